@@ -1,0 +1,301 @@
+/*
+ * beatbox.h -- C ABI of the B200 rigid-body step library (libbeatbox.so).
+ *
+ * This is the drop-in boundary for beat-box's per-step rigid-body pipeline.  The
+ * reference exposes that pipeline as the C++ class beatbox::RigidBodyManager
+ * (src/rigid_body_manager.hpp:12-264), fed by SceneManager::load_scene
+ * (src/scene_manager.hpp:825-929) and configured by StatusManager
+ * (src/status_manager.hpp:204-373).  Each entry point below names the reference
+ * interface it replaces.  Plain pointers and sizes only; no exceptions cross this
+ * boundary; every function returns a bb_status (0 = OK) unless stated otherwise.
+ *
+ * Threading: a bb_world is used by one host thread at a time.  bb_step() enqueues
+ * work on the world's CUDA stream and returns; bb_sync() waits for it.  Readback
+ * functions synchronise the world's stream before copying.
+ */
+#ifndef BEATBOX_H
+#define BEATBOX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+typedef int32_t bb_status;
+#define BB_OK 0
+#define BB_E_INVALID 1      /* bad argument or call order */
+#define BB_E_CAPACITY 2     /* a per-step buffer (pairs, manifolds) overflowed; reserve more */
+#define BB_E_CUDA 3         /* a CUDA runtime call failed; see bb_last_error_string() */
+#define BB_E_DEVICE_LIMIT 4 /* a bounded device loop (spin, traversal stack) gave up */
+#define BB_E_BUDGET 5       /* serving admission refused: HBM budget exhausted */
+#define BB_E_UNSUPPORTED 6  /* feature of the reference not provided by this build */
+
+/* ---- body flags: the reference RigidBodyFlag bits (include/shared.inl:94-100) ----- */
+#define BB_BODY_DYNAMIC (1u << 1)
+#define BB_BODY_GRAVITY (1u << 2)
+#define BB_BODY_SLEEPING (1u << 3)
+
+/* ---- shapes ---------------------------------------------------------------------- */
+#define BB_SHAPE_BOX 0u    /* reference OBB body: RigidBody::minimum/maximum (shared.inl:349-352) */
+#define BB_SHAPE_SPHERE 1u /* no reference counterpart: written from first principles */
+
+/* ---- inertia construction modes for bb_add_bodies -------------------------------- */
+#define BB_INERTIA_PHYSICAL 0u  /* solid box / sphere inverse inertia from mass */
+#define BB_INERTIA_REFERENCE 1u /* cuboid_get_inverse_intertia(inv_mass, min, max): the reference
+                                   scene builder passes inverse mass as mass
+                                   (src/scene_manager.hpp:861, include/math.hpp:106-130) */
+#define BB_INERTIA_EXPLICIT 2u  /* use bb_body_desc.inv_inertia (body-frame diagonal) as given */
+
+/* ---- solver types: SimSolverType (include/shared.inl:210-216) ---------------------- */
+#define BB_SOLVER_PGS 0u      /* Baumgarte PGS: only on the reference's per-island path */
+#define BB_SOLVER_PGS_SOFT 1u /* soft-step PGS on graph colours (reference default PGS family) */
+#define BB_SOLVER_AVBD 2u     /* augmented vertex block descent (reference default solver) */
+
+/* ---- sim flags: SimFlag (include/shared.inl:150-161) -------------------------------- */
+#define BB_SIM_ACCUM_IMPULSE (1u << 0)
+#define BB_SIM_FRICTION (1u << 1)
+#define BB_SIM_WARM_STARTING (1u << 2)
+#define BB_SIM_ADVECTION (1u << 3)
+#define BB_SIM_DEBUG_INFO (1u << 4)
+#define BB_SIM_USE_GRAPH_COLORING (1u << 5)
+#define BB_SIM_SLEEPING_ENABLED (1u << 7)
+/* reference defaults (src/rigid_body_manager.hpp:140-147) */
+#define BB_SIM_DEFAULT_FLAGS                                                                        \
+  (BB_SIM_ACCUM_IMPULSE | BB_SIM_FRICTION | BB_SIM_WARM_STARTING | BB_SIM_ADVECTION |               \
+   BB_SIM_DEBUG_INFO | BB_SIM_USE_GRAPH_COLORING | BB_SIM_SLEEPING_ENABLED)
+
+/* ---- reference arithmetic kept as switchable behaviours ----------------------------
+ * Each bit reproduces one piece of the reference step's arithmetic exactly.  Clearing a
+ * bit selects the physically consistent formula instead.                             */
+#define BB_QUIRK_GRAVITY_IMPULSE (1u << 0)   /* PGS advect: v += g*dt*inv_mass (apply_impulse,
+                                                src/shaders/extensions.slang:127-134,169-178) */
+#define BB_QUIRK_SAT_FRAME (1u << 1)         /* box-box SAT relative rotation C = R_A*R_B^T
+                                                (collision_detection.slang:572) */
+#define BB_QUIRK_INERTIA_TRANSPOSE (1u << 2) /* world inverse inertia R^T*I^-1*R
+                                                (extensions.slang:184-188) */
+#define BB_QUIRKS_REFERENCE (BB_QUIRK_GRAVITY_IMPULSE | BB_QUIRK_SAT_FRAME | BB_QUIRK_INERTIA_TRANSPOSE)
+#define BB_QUIRKS_PHYSICAL 0u
+
+/* ---- Morton normalisation box ---------------------------------------------------- */
+#define BB_BOUNDS_FIXED 0u /* use bb_solver_params.world_min / world_extent (reference: -64, 128,
+                              src/shaders/simulation/RB_sim.slang:96-101) */
+#define BB_BOUNDS_AUTO 1u  /* per substep: min/max of body positions */
+
+/* Solver and material parameters.  Every reference constant is a field whose default (from
+ * bb_default_solver_params) is the reference value; replaces StatusManager::set_solver /
+ * flag toggles (src/status_manager.hpp:204-373) and the compile-time constants of
+ * include/shared.inl:77-83,760-839 and include/defines.hpp:352-364. */
+typedef struct bb_solver_params {
+  uint32_t solver;             /* BB_SOLVER_* (default AVBD) */
+  uint32_t flags;              /* BB_SIM_* (default BB_SIM_DEFAULT_FLAGS) */
+  uint32_t quirks;             /* BB_QUIRK_* (default BB_QUIRKS_REFERENCE) */
+  uint32_t iterations;         /* PGS solve sweeps per substep (reference create() arg, default 5) */
+  uint32_t relax_iterations;   /* PGS relax sweeps per substep (reference: = iterations) */
+  uint32_t gc_rounds;          /* edge-colouring rounds (RBM GRAPH_COLOR_MAX_ROUNDS = 32) */
+  float gravity;               /* y acceleration, default -9.81 */
+  float linear_damping;        /* 0.1 /s */
+  float angular_damping;       /* 0.1 /s */
+  float contact_hertz;         /* MIN_CONTACT_HERTZ = 30 */
+  float penetration_cap;       /* narrow-phase depth floor, -0.25 */
+  /* sleeping (shared.inl:793-797, RB_sim.slang:556-737) */
+  float sleep_lin_vel2;        /* 0.0144 */
+  float sleep_ang_vel2;        /* 0.0225 */
+  uint32_t sleep_steps;        /* 30 */
+  /* AVBD (shared.inl:798-838) */
+  uint32_t avbd_iterations;    /* 10 */
+  float avbd_beta;             /* 1e5 */
+  float avbd_gamma;            /* 0.99 */
+  float avbd_k_min;            /* 1 */
+  float avbd_k_max;            /* 1e9 */
+  float avbd_margin;           /* 0.0005 */
+  float avbd_stick_thresh;     /* 0.01 */
+  float avbd_stick_slop;       /* 0.001 */
+  uint32_t avbd_color_rounds;  /* 16 */
+  uint32_t avbd_shock_layers;  /* 12 */
+  uint32_t avbd_post_stab_sweeps; /* 4 */
+  /* Morton normalisation */
+  uint32_t bounds_mode;        /* BB_BOUNDS_* */
+  float world_min[3];          /* default -64 */
+  float world_extent[3];       /* default 128 */
+} bb_solver_params;
+
+/* World creation.  max_bodies sizes the body arrays; pair_capacity and contact capacity
+ * are derived from pairs_per_body (pairs <= pairs_per_body * max_bodies). */
+typedef struct bb_world_desc {
+  uint32_t max_bodies;
+  uint32_t pairs_per_body; /* 0 = default (16) */
+  int32_t device;          /* CUDA device ordinal; -1 = current */
+  void* stream;            /* cudaStream_t to run on; NULL = the world creates its own */
+} bb_world_desc;
+
+/* One body.  Replaces the RigidBody initialiser used by SceneManager scenes
+ * (src/scene_manager.hpp:114-823) plus the id / mass / inertia assignment of
+ * load_scene (src/scene_manager.hpp:850-887). */
+typedef struct bb_body_desc {
+  float position[3];
+  float rotation[4];     /* quaternion x, y, z, w (reference Quaternion{v, w}) */
+  float velocity[3];
+  float omega[3];
+  uint32_t shape;        /* handle from bb_add_box_shape / bb_add_sphere_shape */
+  uint32_t flags;        /* BB_BODY_* */
+  float mass;            /* > 0: used as given; 0: density * volume (0 density = static) */
+  float density;
+  float friction;
+  float restitution;     /* stored; unused by the reference solvers (solvers.slang:49-56) */
+  uint32_t inertia_mode; /* BB_INERTIA_* */
+  float inv_inertia[3];  /* body-frame diagonal, BB_INERTIA_EXPLICIT only */
+} bb_body_desc;
+
+/* Per-step counters: the reference SimConfig readback (src/rigid_body_manager.cpp:1681-1693,
+ * include/shared.inl:571-665) plus this build's capacity and error reporting. */
+typedef struct bb_step_stats {
+  uint32_t body_count;
+  uint32_t active_body_count;
+  uint32_t pair_count;            /* broad_phase_collision_count */
+  uint32_t manifold_count;        /* g_c_info.collision_count */
+  uint32_t contact_count;
+  uint32_t island_count;
+  uint32_t graph_color_count;     /* colours used by the edge colouring */
+  uint32_t graph_color_overflow;  /* manifolds solved by the serial overflow bucket */
+  uint32_t graph_color_violations;
+  uint32_t avbd_color_count;
+  uint32_t avbd_violations;
+  uint32_t sleeping_count;
+  uint32_t fresh_contacts;        /* dbg_fresh: contacts that failed warm-start matching */
+  uint32_t stick_count;           /* avbd_stick_count */
+  float max_penetration;          /* deepest contact penetration (positive metres) */
+  uint32_t error_flags;           /* BB_ERRF_* bits raised on the device */
+  uint32_t pair_capacity;
+  uint32_t substeps_run;
+} bb_step_stats;
+
+/* device error bits (bb_step_stats.error_flags) */
+#define BB_ERRF_PAIR_OVERFLOW (1u << 0)
+#define BB_ERRF_STACK_OVERFLOW (1u << 1)
+#define BB_ERRF_SPIN_LIMIT (1u << 2)
+#define BB_ERRF_CAS_LIMIT (1u << 3)
+#define BB_ERRF_CONTACT_OVERFLOW (1u << 4)
+
+/* intermediate buffers readable with bb_debug_read (for parity tests and tools) */
+#define BB_DBG_MORTON 1u       /* u32 x N: Morton code of body order[i] (previous sorted order) */
+#define BB_DBG_SORTED_KEYS 2u  /* u32 x N */
+#define BB_DBG_SORTED_IDS 3u   /* u32 x N: body id at each sorted position */
+#define BB_DBG_LBVH_CHILD 4u   /* i32 x 2(N-1): left, right of internal nodes; >= N-1 = leaf */
+#define BB_DBG_LEAF_AABB 5u    /* f32 x 6N: min xyz, max xyz per sorted leaf */
+#define BB_DBG_NODE_AABB 6u    /* f32 x 6(N-1) */
+#define BB_DBG_PAIRS 7u        /* u32 x 2P: (sorted a, sorted b), a < b */
+#define BB_DBG_MANIFOLDS 8u    /* bb_manifold_info x M */
+#define BB_DBG_CONTACTS 9u     /* bb_contact_info x 8M (slot j of manifold m at 8m+j) */
+#define BB_DBG_EDGE_COLORS 10u /* u32 x M (0xFFFFFFFF = overflow) */
+#define BB_DBG_BODY_COLORS 11u /* u32 x N by body id (AVBD colouring) */
+#define BB_DBG_ISLANDS 12u     /* u32 x N by body id (0xFFFFFFFF = static / no island) */
+#define BB_DBG_SUPPORT_DEPTH 13u /* u32 x N by body id (AVBD shock-propagation depth) */
+
+typedef struct bb_manifold_info {
+  uint32_t body_a;       /* body ids; a has the lower sorted position this substep */
+  uint32_t body_b;
+  int32_t key;           /* SAT axis (0-14), 20 sphere-sphere, 21/22 box-sphere */
+  int32_t contact_count;
+  float normal[3];       /* from a towards b */
+  uint32_t color;        /* edge colour */
+  float tangent[2][3];
+} bb_manifold_info;
+
+typedef struct bb_contact_info {
+  float position[3];
+  float penetration;     /* <= 0 when overlapping */
+  float normal_impulse;  /* PGS impulse, or AVBD lambda */
+  float tangent_impulse[2];
+  uint32_t feature;      /* packed feature pair: in_ref | out_ref<<8 | in_inc<<16 | out_inc<<24 */
+  uint32_t warm_start;   /* persistence counter (0 = fresh) */
+  float penalty;         /* AVBD normal penalty k (mass_coefficient) */
+} bb_contact_info;
+
+/* ---- entry points ------------------------------------------------------------------ */
+
+/* Fill p with the reference defaults listed in bb_solver_params.  No reference
+ * counterpart: the reference compiles these in. */
+void bb_default_solver_params(bb_solver_params* p);
+
+/* Replaces RigidBodyManager::RigidBodyManager + create()
+ * (src/rigid_body_manager.hpp:14-18, src/rigid_body_manager.cpp:6-283). */
+bb_status bb_world_create(const bb_world_desc* desc, void** out_world);
+/* Replaces RigidBodyManager::~RigidBodyManager (src/rigid_body_manager.hpp:16). */
+bb_status bb_world_destroy(void* world);
+
+/* Shape table.  The reference stores the box extents in each RigidBody (min/max,
+ * shared.inl:351-352); here bodies reference a shape handle. */
+bb_status bb_add_box_shape(void* world, float hx, float hy, float hz, uint32_t* out_shape);
+bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape);
+
+/* Append n bodies; their ids are consecutive from *out_first_id.  Replaces the body
+ * push + id/mass/inertia assignment of SceneManager::load_scene
+ * (src/scene_manager.hpp:850-887) and RBM::update_active_rigid_body_list
+ * (src/rigid_body_manager.cpp:90-119,1695-1712). */
+bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t n, uint32_t* out_first_id);
+
+/* Change the friction/restitution of bodies [first, first+n).  No separate reference
+ * entry point (materials are per body, shared.inl:360-361). */
+bb_status bb_set_material(void* world, uint32_t first, uint32_t n, float friction, float restitution);
+
+/* Replaces StatusManager::set_solver + flag toggles (src/status_manager.hpp:204-373),
+ * RBM::set_sim_flags/clear_sim_flags/set_sim_type (src/rigid_body_manager.hpp:22-40). */
+bb_status bb_set_solver_params(void* world, const bb_solver_params* params);
+bb_status bb_get_solver_params(void* world, bb_solver_params* params);
+
+/* Advance every body by dt in `substeps` full pipeline passes of h = dt/substeps.
+ * Replaces RigidBodyManager::simulate (src/rigid_body_manager.cpp:1606-1622), which runs
+ * one pass at the fixed TIME_STEP.  Asynchronous on the world's stream. */
+bb_status bb_step(void* world, float dt, uint32_t substeps);
+/* Wait for queued steps; returns BB_E_CAPACITY / BB_E_DEVICE_LIMIT if a step raised an
+ * error flag (see bb_step_stats.error_flags). */
+bb_status bb_sync(void* world);
+
+/* Read / overwrite body state by id (any pointer may be NULL).  position 3N, rotation 4N
+ * (x y z w), velocity 3N, omega 3N.  The reference never reads bodies back to the host
+ * (transforms go to the TLAS, src/shaders/AS_mngr.slang:5-36). */
+bb_status bb_read_state(void* world, float* position, float* rotation, float* velocity, float* omega);
+bb_status bb_write_state(void* world, const float* position, const float* rotation,
+                         const float* velocity, const float* omega);
+/* Per-body flags (BB_BODY_*, including SLEEPING) by id. */
+bb_status bb_read_flags(void* world, uint32_t* flags);
+uint32_t bb_body_count(void* world);
+
+/* Replaces RBM::read_back_sim_config (src/rigid_body_manager.cpp:1681-1693). */
+bb_status bb_read_stats(void* world, bb_step_stats* stats);
+
+/* Replaces RBM::skip_warm_starting_once (src/rigid_body_manager.hpp:29-31). */
+bb_status bb_skip_warm_starting_once(void* world);
+
+/* Run the collision front end of one substep on the current state without moving bodies:
+ * Morton codes, radix sort, LBVH build + refit, broad phase (stage = 1), and the narrow
+ * phase with warm-start matching (stage = 2).  Results are readable with bb_debug_read.
+ * No reference counterpart (the reference only runs the whole task graph). */
+bb_status bb_debug_collide(void* world, uint32_t stage);
+/* Copy an intermediate buffer (BB_DBG_*) of the last substep to host memory.  *count
+ * receives the element count; at most max_bytes are written. */
+bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_bytes, uint64_t* count);
+
+/* CUDA stream the world runs on (cudaStream_t). */
+void* bb_world_stream(void* world);
+/* Per-stage device timing (ms, summed over substeps since the last reset) for profiling.
+ * names: a NUL-separated list of stage names, written to names (may be NULL). */
+bb_status bb_set_profiling(void* world, int32_t enabled);
+bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint32_t* n_stages,
+                              char* names, uint32_t names_bytes);
+/* Number of kernels this library launched on the world's stream since creation. */
+uint64_t bb_kernel_launch_count(void* world);
+
+/* Last error message of the calling thread (static storage, never NULL). */
+const char* bb_last_error_string(void);
+/* Library version string. */
+const char* bb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEATBOX_H */
