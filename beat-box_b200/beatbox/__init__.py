@@ -1,0 +1,404 @@
+"""beatbox -- Python host side of the B200 rigid-body step library (libbeatbox.so).
+
+``World`` wraps the C ABI of include/beatbox.h with numpy arrays.  ``RigidBodyManager`` mirrors
+the reference's class of that name (src/rigid_body_manager.hpp:12-70): create / simulate /
+read_back_sim_config / set_sim_flags / clear_sim_flags / set_sim_type /
+skip_warm_starting_once, so code written against the reference's manager reads the same.
+
+The library is CUDA-only: importing works anywhere, but creating a world needs the built
+libbeatbox.so and a GPU, and fails loudly otherwise (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import scenes  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libbeatbox.so")
+
+# status codes and flags (include/beatbox.h)
+OK, E_INVALID, E_CAPACITY, E_CUDA, E_DEVICE_LIMIT, E_BUDGET, E_UNSUPPORTED = range(7)
+BODY_DYNAMIC, BODY_GRAVITY, BODY_SLEEPING = 1 << 1, 1 << 2, 1 << 3
+SHAPE_BOX, SHAPE_SPHERE = 0, 1
+INERTIA_PHYSICAL, INERTIA_REFERENCE, INERTIA_EXPLICIT = 0, 1, 2
+SOLVER_PGS, SOLVER_PGS_SOFT, SOLVER_AVBD = 0, 1, 2
+SIM_ACCUM_IMPULSE, SIM_FRICTION, SIM_WARM_STARTING, SIM_ADVECTION = 1, 2, 4, 8
+SIM_DEBUG_INFO, SIM_USE_GRAPH_COLORING, SIM_SLEEPING_ENABLED = 16, 32, 128
+SIM_DEFAULT_FLAGS = SIM_ACCUM_IMPULSE | SIM_FRICTION | SIM_WARM_STARTING | SIM_ADVECTION | SIM_DEBUG_INFO | \
+    SIM_USE_GRAPH_COLORING | SIM_SLEEPING_ENABLED
+QUIRK_GRAVITY_IMPULSE, QUIRK_SAT_FRAME, QUIRK_INERTIA_TRANSPOSE = 1, 2, 4
+QUIRKS_REFERENCE, QUIRKS_PHYSICAL = 7, 0
+BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
+DBG = dict(morton=1, sorted_keys=2, sorted_ids=3, lbvh_child=4, leaf_aabb=5, node_aabb=6, pairs=7,
+           manifolds=8, contacts=9, edge_colors=10, body_colors=11, islands=12, support_depth=13)
+
+
+class BeatboxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"beatbox error {code}: {msg}")
+        self.code = code
+
+
+class SolverParams(ctypes.Structure):
+    _fields_ = [
+        ("solver", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("quirks", ctypes.c_uint32),
+        ("iterations", ctypes.c_uint32), ("relax_iterations", ctypes.c_uint32), ("gc_rounds", ctypes.c_uint32),
+        ("gravity", ctypes.c_float), ("linear_damping", ctypes.c_float), ("angular_damping", ctypes.c_float),
+        ("contact_hertz", ctypes.c_float), ("penetration_cap", ctypes.c_float),
+        ("sleep_lin_vel2", ctypes.c_float), ("sleep_ang_vel2", ctypes.c_float), ("sleep_steps", ctypes.c_uint32),
+        ("avbd_iterations", ctypes.c_uint32), ("avbd_beta", ctypes.c_float), ("avbd_gamma", ctypes.c_float),
+        ("avbd_k_min", ctypes.c_float), ("avbd_k_max", ctypes.c_float), ("avbd_margin", ctypes.c_float),
+        ("avbd_stick_thresh", ctypes.c_float), ("avbd_stick_slop", ctypes.c_float),
+        ("avbd_color_rounds", ctypes.c_uint32), ("avbd_shock_layers", ctypes.c_uint32),
+        ("avbd_post_stab_sweeps", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
+        ("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3),
+    ]
+
+
+class WorldDesc(ctypes.Structure):
+    _fields_ = [("max_bodies", ctypes.c_uint32), ("pairs_per_body", ctypes.c_uint32), ("device", ctypes.c_int32),
+                ("stream", ctypes.c_void_p)]
+
+
+class BodyDesc(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float * 3), ("rotation", ctypes.c_float * 4), ("velocity", ctypes.c_float * 3),
+                ("omega", ctypes.c_float * 3), ("shape", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("mass", ctypes.c_float), ("density", ctypes.c_float), ("friction", ctypes.c_float),
+                ("restitution", ctypes.c_float), ("inertia_mode", ctypes.c_uint32), ("inv_inertia", ctypes.c_float * 3)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "body_count", "active_body_count", "pair_count", "manifold_count", "contact_count", "island_count",
+        "graph_color_count", "graph_color_overflow", "graph_color_violations", "avbd_color_count",
+        "avbd_violations", "sleeping_count", "fresh_contacts", "stick_count")] + [
+        ("max_penetration", ctypes.c_float), ("error_flags", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
+        ("substeps_run", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+MANIFOLD_DTYPE = np.dtype([("body_a", "<u4"), ("body_b", "<u4"), ("key", "<i4"), ("contact_count", "<i4"),
+                           ("normal", "<f4", 3), ("color", "<u4"), ("tangent", "<f4", (2, 3))])
+CONTACT_DTYPE = np.dtype([("position", "<f4", 3), ("penetration", "<f4"), ("normal_impulse", "<f4"),
+                          ("tangent_impulse", "<f4", 2), ("feature", "<u4"), ("warm_start", "<u4"),
+                          ("penalty", "<f4")])
+
+# exported symbols of include/beatbox.h: name -> (restype, argtypes)
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_SIG = {
+    "bb_default_solver_params": (None, [ctypes.POINTER(SolverParams)]),
+    "bb_world_create": (ctypes.c_int32, [ctypes.POINTER(WorldDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "bb_world_destroy": (ctypes.c_int32, [_P]),
+    "bb_add_box_shape": (ctypes.c_int32, [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.POINTER(_U32)]),
+    "bb_add_sphere_shape": (ctypes.c_int32, [_P, ctypes.c_float, ctypes.POINTER(_U32)]),
+    "bb_add_bodies": (ctypes.c_int32, [_P, ctypes.POINTER(BodyDesc), _U32, ctypes.POINTER(_U32)]),
+    "bb_set_material": (ctypes.c_int32, [_P, _U32, _U32, ctypes.c_float, ctypes.c_float]),
+    "bb_set_solver_params": (ctypes.c_int32, [_P, ctypes.POINTER(SolverParams)]),
+    "bb_get_solver_params": (ctypes.c_int32, [_P, ctypes.POINTER(SolverParams)]),
+    "bb_step": (ctypes.c_int32, [_P, ctypes.c_float, _U32]),
+    "bb_sync": (ctypes.c_int32, [_P]),
+    "bb_read_state": (ctypes.c_int32, [_P, _P, _P, _P, _P]),
+    "bb_write_state": (ctypes.c_int32, [_P, _P, _P, _P, _P]),
+    "bb_read_flags": (ctypes.c_int32, [_P, _P]),
+    "bb_body_count": (_U32, [_P]),
+    "bb_read_stats": (ctypes.c_int32, [_P, ctypes.POINTER(StepStats)]),
+    "bb_skip_warm_starting_once": (ctypes.c_int32, [_P]),
+    "bb_debug_collide": (ctypes.c_int32, [_P, _U32]),
+    "bb_debug_read": (ctypes.c_int32, [_P, _U32, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "bb_world_stream": (ctypes.c_void_p, [_P]),
+    "bb_set_profiling": (ctypes.c_int32, [_P, ctypes.c_int32]),
+    "bb_read_stage_times": (ctypes.c_int32, [_P, _P, _U32, ctypes.POINTER(_U32), _P, _U32]),
+    "bb_kernel_launch_count": (ctypes.c_uint64, [_P]),
+    "bb_last_error_string": (ctypes.c_char_p, []),
+    "bb_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load libbeatbox.so (building it first if it is missing and nvcc is available)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("_bb_build", os.path.join(PKG, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    L = ctypes.CDLL(path)
+    for name, (res, args) in _SIG.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(code: int):
+    if code != OK:
+        raise BeatboxError(code, _lib.bb_last_error_string().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def default_params() -> SolverParams:
+    p = SolverParams()
+    load_library().bb_default_solver_params(ctypes.byref(p))
+    return p
+
+
+def make_params(**kw) -> SolverParams:
+    p = default_params()
+    for k, v in kw.items():
+        if k in ("world_min", "world_extent"):
+            getattr(p, k)[:] = [float(x) for x in v]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+class World:
+    """One simulated world on the GPU (wraps bb_world_*)."""
+
+    def __init__(self, max_bodies: int, pairs_per_body: int = 16, device: int = -1, stream: int | None = None):
+        L = load_library()
+        desc = WorldDesc(max_bodies, pairs_per_body, device, stream)
+        h = ctypes.c_void_p()
+        _check(L.bb_world_create(ctypes.byref(desc), ctypes.byref(h)))
+        self.h = h
+        self.L = L
+        self._shape_cache: dict = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bb_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- construction --------------------------------------------------------------------
+    def add_box_shape(self, hx: float, hy: float, hz: float) -> int:
+        out = _U32()
+        _check(self.L.bb_add_box_shape(self.h, hx, hy, hz, ctypes.byref(out)))
+        return out.value
+
+    def add_sphere_shape(self, r: float) -> int:
+        out = _U32()
+        _check(self.L.bb_add_sphere_shape(self.h, r, ctypes.byref(out)))
+        return out.value
+
+    def _shape_for(self, shape: int, half) -> int:
+        key = (int(shape), float(half[0]), float(half[1]), float(half[2]))
+        h = self._shape_cache.get(key)
+        if h is None:
+            h = self.add_box_shape(*key[1:]) if shape == SHAPE_BOX else self.add_sphere_shape(key[1])
+            self._shape_cache[key] = h
+        return h
+
+    def add_scene(self, scene: dict, inertia_mode: int = INERTIA_EXPLICIT) -> int:
+        """Add every body of a beatbox.scenes dict; masses and inverse inertias are taken from
+        the scene (the oracle gets the same arrays)."""
+        n = int(scene["n"])
+        descs = (BodyDesc * n)()
+        for i in range(n):
+            d = descs[i]
+            d.position[:] = scene["pos"][i].tolist()
+            d.rotation[:] = scene["quat"][i].tolist()
+            d.velocity[:] = scene["vel"][i].tolist()
+            d.omega[:] = scene["omega"][i].tolist()
+            d.shape = self._shape_for(int(scene["shape"][i]), scene["half"][i])
+            d.flags = int(scene["flags"][i])
+            d.mass = float(scene["mass"][i])
+            d.density = 0.0
+            d.friction = float(scene["friction"][i])
+            d.restitution = float(scene["restitution"][i])
+            d.inertia_mode = inertia_mode
+            d.inv_inertia[:] = scene["inv_inertia"][i].tolist()
+        first = _U32()
+        _check(self.L.bb_add_bodies(self.h, descs, n, ctypes.byref(first)))
+        return first.value
+
+    def add_bodies(self, descs) -> int:
+        arr = (BodyDesc * len(descs))(*descs)
+        first = _U32()
+        _check(self.L.bb_add_bodies(self.h, arr, len(descs), ctypes.byref(first)))
+        return first.value
+
+    def set_material(self, first: int, n: int, friction: float, restitution: float = 0.0):
+        _check(self.L.bb_set_material(self.h, first, n, friction, restitution))
+
+    # ---- parameters --------------------------------------------------------------------
+    @property
+    def params(self) -> SolverParams:
+        p = SolverParams()
+        _check(self.L.bb_get_solver_params(self.h, ctypes.byref(p)))
+        return p
+
+    def set_params(self, p: SolverParams | None = None, **kw):
+        p = p if p is not None else self.params
+        for k, v in kw.items():
+            if k in ("world_min", "world_extent"):
+                getattr(p, k)[:] = [float(x) for x in v]
+            else:
+                setattr(p, k, v)
+        _check(self.L.bb_set_solver_params(self.h, ctypes.byref(p)))
+
+    # ---- stepping ------------------------------------------------------------------------
+    def step(self, dt: float, substeps: int = 1):
+        _check(self.L.bb_step(self.h, ctypes.c_float(dt), substeps))
+
+    def sync(self):
+        _check(self.L.bb_sync(self.h))
+
+    def skip_warm_starting_once(self):
+        _check(self.L.bb_skip_warm_starting_once(self.h))
+
+    @property
+    def n(self) -> int:
+        return int(self.L.bb_body_count(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.L.bb_world_stream(self.h)
+
+    def launches(self) -> int:
+        return int(self.L.bb_kernel_launch_count(self.h))
+
+    # ---- readback ------------------------------------------------------------------------
+    def read_state(self, out: dict | None = None) -> dict:
+        n = self.n
+        out = out or dict(pos=np.empty((n, 3), np.float32), quat=np.empty((n, 4), np.float32),
+                          vel=np.empty((n, 3), np.float32), omega=np.empty((n, 3), np.float32))
+        _check(self.L.bb_read_state(self.h, _ptr(out["pos"]), _ptr(out["quat"]), _ptr(out["vel"]), _ptr(out["omega"])))
+        return out
+
+    def write_state(self, pos=None, quat=None, vel=None, omega=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)  # noqa: E731
+        pos, quat, vel, omega = c(pos), c(quat), c(vel), c(omega)
+        _check(self.L.bb_write_state(self.h, _ptr(pos), _ptr(quat), _ptr(vel), _ptr(omega)))
+
+    def read_flags(self) -> np.ndarray:
+        f = np.empty(self.n, np.uint32)
+        _check(self.L.bb_read_flags(self.h, _ptr(f)))
+        return f
+
+    def stats(self) -> dict:
+        s = StepStats()
+        _check(self.L.bb_read_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def debug_collide(self, stage: int):
+        _check(self.L.bb_debug_collide(self.h, stage))
+
+    def debug_read(self, which: str):
+        code = DBG[which]
+        cnt = ctypes.c_uint64()
+        _check(self.L.bb_debug_read(self.h, code, None, 0, ctypes.byref(cnt)))
+        n = cnt.value
+        if which in ("leaf_aabb", "node_aabb"):
+            buf = np.empty(n, np.float32)
+        elif which == "lbvh_child":
+            buf = np.empty(n, np.int32)
+        elif which == "manifolds":
+            buf = np.empty(n, MANIFOLD_DTYPE)
+        elif which == "contacts":
+            buf = np.empty(n, CONTACT_DTYPE)
+        else:
+            buf = np.empty(n, np.uint32)
+        _check(self.L.bb_debug_read(self.h, code, _ptr(buf), buf.nbytes, ctypes.byref(cnt)))
+        return buf
+
+    # ---- profiling --------------------------------------------------------------------------
+    def set_profiling(self, on: bool):
+        _check(self.L.bb_set_profiling(self.h, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        ms = np.zeros(32, np.float32)
+        ns = _U32()
+        names = ctypes.create_string_buffer(1024)
+        _check(self.L.bb_read_stage_times(self.h, _ptr(ms), 32, ctypes.byref(ns), names, 1024))
+        nm = names.raw.split(b"\0")[: ns.value]
+        return {k.decode(): float(v) for k, v in zip(nm, ms[: ns.value])}
+
+
+def world_from_scene(scene: dict, params: SolverParams | None = None, pairs_per_body: int = 16, **kw) -> World:
+    """World holding every body of a scene, with its Morton bounds applied."""
+    w = World(int(scene["n"]), pairs_per_body=pairs_per_body)
+    w.add_scene(scene)
+    p = params if params is not None else default_params()
+    if scene.get("bounds") is not None:
+        p.world_min[:] = scene["bounds"][0]
+        p.world_extent[:] = scene["bounds"][1]
+    w.set_params(p, **kw)
+    return w
+
+
+class RigidBodyManager:
+    """Drop-in for the reference's beatbox::RigidBodyManager (src/rigid_body_manager.hpp:12-70).
+
+    simulate() advances one fixed step (TIME_STEP = 0.01667 s, include/defines.hpp:354) in
+    ``substeps`` pipeline passes; read_back_sim_config() returns the SimConfig-style counters.
+    """
+
+    TIME_STEP = 0.01667
+
+    def __init__(self, max_bodies: int = 1024, pairs_per_body: int = 16):
+        self.world = World(max_bodies, pairs_per_body=pairs_per_body)
+        self._sim_config: dict = {}
+        self.substeps = 1
+
+    def create(self, name: str = "", iterations: int = 5) -> bool:
+        self.world.set_params(iterations=iterations, relax_iterations=iterations)
+        return True
+
+    def simulate(self) -> bool:
+        self.world.step(self.TIME_STEP, self.substeps)
+        return True
+
+    def read_back_sim_config(self) -> bool:
+        self._sim_config = self.world.stats()
+        return True
+
+    def get_sim_config_reference(self) -> dict:
+        return self._sim_config
+
+    def skip_warm_starting_once(self):
+        self.world.skip_warm_starting_once()
+
+    def get_sim_flags(self) -> int:
+        return int(self.world.params.flags)
+
+    def set_sim_flags(self, flags: int) -> int:
+        p = self.world.params
+        p.flags |= flags
+        self.world.set_params(p)
+        return int(p.flags)
+
+    def clear_sim_flags(self, flags: int) -> int:
+        p = self.world.params
+        p.flags &= ~flags
+        self.world.set_params(p)
+        return int(p.flags)
+
+    def set_sim_type(self, solver: int):
+        self.world.set_params(solver=solver)
+
+    def get_sim_type(self) -> int:
+        return int(self.world.params.solver)

@@ -1,0 +1,255 @@
+// bb_bvh.cu -- Morton codes, radix sort, Karras LBVH build, atomic bottom-up refit and the
+// broad phase.
+//
+// Reference: entry_generate_morton_codes (src/shaders/simulation/RB_sim.slang:75-111),
+// MortonCodeGenerator (src/shaders/simulation/LBVH.slang:4-32), entry_generate_hierarchy_
+// linear_bvh + LBVH::determine_range/find_split/delta (RB_sim.slang:206-278, LBVH.slang:
+// 155-221), entry_build/convert_bounding_boxes_linear_bvh (RB_sim.slang:282-349),
+// entry_broad_phase + LBVH::broad_phase (RB_sim.slang:413-437, LBVH.slang:223-286).
+//
+// B200 design: the body state is never gathered into Morton order (the reference copies its
+// 184-byte AoS bodies every step, RB_sim.slang:351-386); the sort carries body ids and every
+// later stage indexes the SoA arrays by id.  Keys are emitted in the previous substep's
+// sorted order, so ties break exactly like the reference's scratch-array order.  The refit
+// uses one arrival counter per internal node (second arriver merges) instead of the
+// reference's O(N depth) per-leaf atomic min/max walk; float min/max is exact, so the boxes
+// are identical.  The broad phase traverses left-first and prunes subtrees whose leaf range
+// ends at or before the query, so each query emits its partners j > i in ascending order and
+// the pair list comes out sorted by (a, b) with no global atomic per pair.
+#include "bb_common.cuh"
+#include "bb_kernels.cuh"
+
+// ---- FP32-exact geometry (no contraction) -------------------------------------------------
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+__device__ __forceinline__ float morton_axis(float p, float mn, float ext) {
+  float x = __fdiv_rn(__fsub_rn(p, mn), ext);
+  x = __fmul_rn(x, 1024.0f);
+  x = fminf(fmaxf(x, 0.0f), 1023.0f);
+  return x;
+}
+__device__ __forceinline__ uint32_t morton_code(float3 p, const float wmin[3], const float wext[3]) {
+  uint32_t xx = expand_bits(__float2uint_rz(morton_axis(p.x, wmin[0], wext[0])));
+  uint32_t yy = expand_bits(__float2uint_rz(morton_axis(p.y, wmin[1], wext[1])));
+  uint32_t zz = expand_bits(__float2uint_rz(morton_axis(p.z, wmin[2], wext[2])));
+  return xx * 4 + yy * 2 + zz;
+}
+
+// RigidBody::get_AABB_from_OBB (src/shaders/extensions.slang:195-210): the 8 corners of the
+// box rotated by the quaternion sandwich q c q* (include/shared.inl:455-475) plus position.
+__device__ __forceinline__ void leaf_box(float4 shp, float4 p4, float4 q4, float4& mn, float4& mx) {
+  uint32_t type = __float_as_uint(shp.w);
+  if (type == BB_SHAPE_SPHERE) {
+    float r = shp.x;
+    mn = make_float4(__fsub_rn(p4.x, r), __fsub_rn(p4.y, r), __fsub_rn(p4.z, r), 0.f);
+    mx = make_float4(__fadd_rn(p4.x, r), __fadd_rn(p4.y, r), __fadd_rn(p4.z, r), 0.f);
+    return;
+  }
+  Quatf q = q_from(q4);
+  Quatf qc = q_conj(q);
+  float lo[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+  float hi[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    Quatf c{(i & 1) ? shp.x : -shp.x, (i & 2) ? shp.y : -shp.y, (i & 4) ? shp.z : -shp.z, 0.f};
+    Quatf r = q_mul_exact(q_mul_exact(q, c), qc);
+    float w[3] = {__fadd_rn(r.x, p4.x), __fadd_rn(r.y, p4.y), __fadd_rn(r.z, p4.z)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = w[k] < lo[k] ? w[k] : lo[k];
+      hi[k] = w[k] > hi[k] ? w[k] : hi[k];
+    }
+  }
+  mn = make_float4(lo[0], lo[1], lo[2], 0.f);
+  mx = make_float4(hi[0], hi[1], hi[2], 0.f);
+}
+
+__device__ __forceinline__ bool box_overlap(float4 amn, float4 amx, float4 bmn, float4 bmx) {
+  return amn.x <= bmx.x && amx.x >= bmn.x && amn.y <= bmx.y && amx.y >= bmn.y && amn.z <= bmx.z && amx.z >= bmn.z;
+}
+
+// ---- kernels ---------------------------------------------------------------------------------
+__global__ void k_bounds(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = d.pos[i];
+  atomicMin(&d.ctr->bounds_min[0], f2ord(p.x));
+  atomicMin(&d.ctr->bounds_min[1], f2ord(p.y));
+  atomicMin(&d.ctr->bounds_min[2], f2ord(p.z));
+  atomicMax(&d.ctr->bounds_max[0], f2ord(p.x));
+  atomicMax(&d.ctr->bounds_max[1], f2ord(p.y));
+  atomicMax(&d.ctr->bounds_max[2], f2ord(p.z));
+}
+
+// keys[0][i] = Morton code of body vals[0][i] (the previous substep's sorted order).
+__global__ void k_morton(const DevState d, uint32_t n, Params p) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float wmin[3], wext[3];
+  if (p.bounds_mode == BB_BOUNDS_AUTO) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float lo = ord2f(d.ctr->bounds_min[k]), hi = ord2f(d.ctr->bounds_max[k]);
+      float e = __fsub_rn(hi, lo);
+      wmin[k] = lo;
+      wext[k] = e > 0.0f ? e : 1.0f;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      wmin[k] = p.world_min[k];
+      wext[k] = p.world_extent[k];
+    }
+  }
+  uint32_t id = d.vals[0][i];
+  d.keys[0][i] = morton_code(f3(d.pos[id]), wmin, wext);
+}
+
+__device__ __forceinline__ int clz_delta(const uint32_t* codes, int n, int i, uint32_t ci, int j) {
+  if (j < 0 || j > n - 1) return -1;
+  uint32_t cj = codes[j];
+  if (ci == cj) return 32 + __clz(uint32_t(i ^ j));
+  return __clz(ci ^ cj);
+}
+
+// leaves in sorted order + Karras internal nodes (LBVH.slang:155-221, RB_sim.slang:206-278)
+__global__ void k_build(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t* codes = d.keys[0];
+  uint32_t id = d.vals[0][i];
+  d.rank[id] = i;
+  float4 mn, mx;
+  leaf_box(d.shape[id], d.pos[id], d.rot[id], mn, mx);
+  uint32_t leaf = n - 1 + i;
+  d.node_box[2 * leaf] = mn;
+  d.node_box[2 * leaf + 1] = mx;
+  if (i == 0) d.parent[0] = -1;
+  if (i + 1 >= n) return;
+  const int N = int(n), idx = int(i);
+  uint32_t code = codes[idx];
+  int dl = clz_delta(codes, N, idx, code, idx - 1);
+  int dr = clz_delta(codes, N, idx, code, idx + 1);
+  int dir = dr >= dl ? 1 : -1;
+  int dmin = min(dl, dr);
+  int lmax = 2;
+  while (clz_delta(codes, N, idx, code, idx + lmax * dir) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t > 0; t >>= 1)
+    if (clz_delta(codes, N, idx, code, idx + (l + t) * dir) > dmin) l += t;
+  int j = idx + l * dir;
+  int first = min(idx, j), last = max(idx, j);
+  uint32_t fc = codes[first];
+  int common = clz_delta(codes, N, first, fc, last);
+  int split = first, step = last - first;
+  do {
+    step = (step + 1) >> 1;
+    int ns = split + step;
+    if (ns < last && clz_delta(codes, N, first, fc, ns) > common) split = ns;
+  } while (step > 1);
+  int ca = split == first ? N - 1 + split : split;
+  int cb = split + 1 == last ? N - 1 + split + 1 : split + 1;
+  d.child[i] = make_int2(ca, cb);
+  d.parent[ca] = idx;
+  d.parent[cb] = idx;
+  d.range_last[i] = last;
+  d.visit[i] = 0;
+}
+
+// bottom-up refit: the second child to arrive at a node merges both boxes and climbs on
+__global__ void k_refit(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || n < 2) return;
+  int node = d.parent[n - 1 + i];
+  uint32_t guard = 0;
+  while (node >= 0) {
+    __threadfence();
+    if (atomicAdd(&d.visit[node], 1u) == 0u) return;  // first arriver: sibling not ready
+    __threadfence();
+    int2 c = d.child[node];
+    float4 amn = __ldcg(&d.node_box[2 * c.x]), amx = __ldcg(&d.node_box[2 * c.x + 1]);
+    float4 bmn = __ldcg(&d.node_box[2 * c.y]), bmx = __ldcg(&d.node_box[2 * c.y + 1]);
+    float4 mn = make_float4(bmn.x < amn.x ? bmn.x : amn.x, bmn.y < amn.y ? bmn.y : amn.y,
+                            bmn.z < amn.z ? bmn.z : amn.z, 0.f);
+    float4 mx = make_float4(bmx.x > amx.x ? bmx.x : amx.x, bmx.y > amx.y ? bmx.y : amx.y,
+                            bmx.z > amx.z ? bmx.z : amx.z, 0.f);
+    __stcg(&d.node_box[2 * node], mn);
+    __stcg(&d.node_box[2 * node + 1], mx);
+    node = d.parent[node];
+    if (++guard > 128u) {  // a Karras tree over 30-bit codes + 32 index bits is < 64 deep
+      raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+      return;
+    }
+  }
+}
+
+// Left-first traversal for sorted query i.  EMIT=false counts, EMIT=true writes.
+template <bool EMIT>
+__global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (n < 2) {
+    if (!EMIT) d.pair_cnt[i] = 0;
+    return;
+  }
+  const int N = int(n);
+  const int leaf0 = N - 1;
+  float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
+  uint32_t out = EMIT ? d.pair_off[i] : 0u;
+  const uint32_t cap = d.pair_capacity;
+  uint32_t count = 0;
+  int stack[BB_BVH_STACK];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    int node = stack[--sp];
+    if (node >= leaf0) {
+      if (EMIT) {
+        uint32_t k = out + count;
+        if (k < cap) d.pairs[k] = make_uint2(i, uint32_t(node - leaf0));
+        else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+      }
+      ++count;
+      continue;
+    }
+    int2 c = d.child[node];
+    int kids[2] = {c.y, c.x};  // right first: the left child is popped first
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      int ch = kids[k];
+      bool take;
+      if (ch >= leaf0) take = (ch - leaf0) > int(i);
+      else take = d.range_last[ch] > int(i);
+      if (!take) continue;
+      float4 bmn = d.node_box[2 * ch], bmx = d.node_box[2 * ch + 1];
+      if (!box_overlap(qmn, qmx, bmn, bmx)) continue;
+      if (sp < BB_BVH_STACK) stack[sp++] = ch;
+      else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+    }
+  }
+  if (!EMIT) d.pair_cnt[i] = count;
+}
+
+void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
+                  int cur) {
+  (void)cur;
+  if (n == 0) return;
+  const int T = BB_THREADS;
+  uint32_t blocks = (n + T - 1) / T;
+  if (p.bounds_mode == BB_BOUNDS_AUTO) k_bounds<<<blocks, T, 0, s>>>(d, n);
+  k_morton<<<blocks, T, 0, s>>>(d, n, p);
+  uint32_t* keys[2] = {d.keys[0], d.keys[1]};
+  uint32_t* vals[2] = {d.vals[0], d.vals[1]};
+  bb_launch_sort(s, keys, vals, nullptr, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms);
+  k_build<<<blocks, T, 0, s>>>(d, n);
+  k_refit<<<blocks, T, 0, s>>>(d, n);
+  uint32_t bb = (n + 127) / 128;
+  k_broad<false><<<bb, 128, 0, s>>>(d, n);
+  bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr);
+  k_broad<true><<<bb, 128, 0, s>>>(d, n);
+}

@@ -1,0 +1,269 @@
+// bb_common.cuh -- shared device definitions of the B200 rigid-body step.
+//
+// Layout (all arrays in HBM, indexed by body id unless noted):
+//   pos      float4  position.xyz, inverse mass
+//   rot      float4  quaternion x y z w
+//   vel      float4  linear velocity.xyz, mass
+//   omega    float4  angular velocity.xyz, 0
+//   pvel     float4  previous-step velocity (AVBD adaptive warm start)
+//   shape    float4  half extents (sphere: radius in x), w = shape type bits
+//   iinv     float4  body-frame inverse inertia diagonal.xyz, friction
+//   flags    u32     BB_BODY_* ; sleep u32 timer (bit 31 = partner veto)
+// Manifolds live in pair slots (one slot per broad-phase pair); slot p owns contact rows
+// 8p .. 8p+7.  A compact list man_slot[m] (pair order) names the slots that collided.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/beatbox.h"
+
+#define BB_MAX_CONTACTS 8
+#define BB_MAX_COLORS 32
+#define BB_UNCOLORED 0xFFFFFFFFu
+#define BB_NONE 0xFFFFFFFFu
+#define BB_SLEEP_VETO 0x80000000u
+#define BB_SLEEP_MASK 0x7FFFFFFFu
+#define BB_SPIN_LIMIT (1u << 22)
+#define BB_BVH_STACK 64
+
+#define BB_KEY_SPHERE_SPHERE 20
+#define BB_KEY_BOX_SPHERE 21
+#define BB_KEY_SPHERE_BOX 22
+
+// ---- device counters (one struct per world, zeroed per substep where noted) ---------
+struct DevCounters {
+  uint32_t n_bodies;       // host-set
+  uint32_t n_dynamic;      // host-set
+  uint32_t pair_count;     // broad phase output (per substep)
+  uint32_t manifold_count; // per substep
+  uint32_t contact_count;
+  uint32_t fresh;
+  uint32_t max_pen_bits;   // float bits of the deepest penetration (positive)
+  uint32_t island_count;
+  uint32_t sleeping;
+  uint32_t gc_colors;
+  uint32_t gc_overflow;
+  uint32_t gc_violations;
+  uint32_t gc_uncolored;   // working counter of the colouring rounds
+  uint32_t avbd_colors;
+  uint32_t avbd_violations;
+  uint32_t stick;
+  uint32_t error_flags;    // sticky until read
+  uint32_t gc_epoch;       // colouring round epoch (never reset)
+  uint32_t barrier_count;  // grid barrier
+  uint32_t barrier_gen;
+  uint32_t bounds_min[3];  // BB_BOUNDS_AUTO: ordered-float min/max of positions
+  uint32_t bounds_max[3];
+  uint32_t avbd_body_count;
+  uint32_t substeps;       // substeps run since the last stats read
+  uint32_t pad[6];
+};
+
+// ---- pointers of one world's device state ------------------------------------------------
+struct DevState {
+  // bodies
+  float4 *pos, *rot, *vel, *omega, *pvel, *shape, *iinv;
+  uint32_t *flags, *sleep;
+  float4* iw;  // world inverse inertia cache: 2 float4 per body (xx xy xz yy | yz zz - -)
+  // front end
+  uint32_t *keys[2], *vals[2];  // vals[0] holds the sorted ids (= next substep's order)
+  uint32_t* rank;               // body id -> sorted position
+  float4* node_box;             // 2 float4 per node (min, max); internal 0..N-2, leaves N-1..
+  int2* child;                  // internal node children
+  int32_t* parent;              // parent of every node (root: -1)
+  int32_t* range_last;          // last leaf covered by each internal node
+  uint32_t* visit;              // refit arrival counters
+  uint32_t *pair_cnt, *pair_off;  // per query
+  uint2* pairs;                 // (sorted a, sorted b)
+  // manifolds (two buffers: [cur], [prev] chosen by parity)
+  uint2* m_bodies[2];    // body ids (a, b) per slot
+  int2* m_keycc[2];      // key, contact count per slot
+  float4* m_normal[2];   // normal.xyz, error (int bits)
+  float4* m_t0[2];
+  float4* m_t1[2];
+  float4* m_anchor_a[2]; // body positions at narrow-phase time
+  float4* m_anchor_b[2];
+  uint32_t* man_slot[2]; // compact manifold -> slot
+  uint32_t* man_count_prev; // not used (count kept in counters)
+  // contacts (8 per slot)
+  float4* c_pos[2];      // position.xyz, penetration
+  float4* c_lam[2];      // normal impulse / lambda, tangent impulse 0/1, AVBD normal penalty k
+  float4* c_kt[2];       // AVBD tangent penalties 0/1, stick (bits), warm-start count (bits)
+  float4* c_anc_a[2];    // AVBD local anchor on a .xyz, feature pair (bits)
+  float4* c_anc_b[2];    // AVBD local anchor on b .xyz, 0
+  // PGS rows (current only)
+  float4 *c_r1, *c_r2, *c_k;
+  // per-body manifold lists (CSR over compact manifold indices) [cur], [prev]
+  uint32_t* csr_start[2];
+  uint32_t* csr_list[2];
+  uint32_t* csr_cursor;
+  uint32_t* hit;         // per pair slot: 1 if it produced a manifold
+  uint32_t* man_index;   // per pair slot: exclusive scan of hit
+  // islands
+  uint32_t *uf_parent, *is_root, *root_rank, *island;
+  // colouring
+  uint32_t* gc_color;    // per compact manifold
+  uint32_t* gc_pid;      // pair-identity hash
+  uint32_t* gc_choice;
+  uint32_t* gc_mask;     // per body
+  unsigned long long* gc_owner; // per body x 32 colours: (epoch << 32) | priority
+  uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies
+  uint32_t* bucket_start; // 34 + 32*L entries
+  // AVBD
+  uint32_t* body_color;   // per body
+  uint32_t* body_color_round;
+  float4 *a_pos_start, *a_rot_start, *a_pos_tilde, *a_rot_tilde;
+  uint32_t* a_depth;
+  uint32_t *a_bucket_keys[2], *a_bucket_vals[2];
+  uint32_t* a_bucket_start;
+  // scan / sort scratch
+  uint32_t* scan_status;  // decoupled look-back status words
+  uint32_t* scan_tile_ctr;
+  uint32_t* sort_hist;    // 4 x 256 global digit histograms
+  uint32_t* sort_status;  // tiles x 256 per pass
+  uint32_t* sort_tile_ctr;
+  DevCounters* ctr;
+  uint32_t pair_capacity;
+  uint32_t body_capacity;
+};
+
+// ---- small vector helpers -------------------------------------------------------------------
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float4 f4(float3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ float comp(float3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+__device__ __forceinline__ void set_comp(float3& a, int i, float v) {
+  if (i == 0) a.x = v;
+  else if (i == 1) a.y = v;
+  else a.z = v;
+}
+
+struct Quatf {
+  float x, y, z, w;
+};
+__device__ __forceinline__ Quatf q_from(float4 a) { return Quatf{a.x, a.y, a.z, a.w}; }
+__device__ __forceinline__ float4 q_to4(Quatf q) { return make_float4(q.x, q.y, q.z, q.w); }
+__device__ __forceinline__ Quatf q_conj(Quatf q) { return Quatf{-q.x, -q.y, -q.z, q.w}; }
+// Hamilton product (include/math.hpp:357-364), contraction allowed.
+__device__ __forceinline__ Quatf q_mul(Quatf a, Quatf b) {
+  return Quatf{a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y + a.y * b.w + a.z * b.x - a.x * b.z,
+               a.w * b.z + a.z * b.w + a.x * b.y - a.y * b.x, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z};
+}
+__device__ __forceinline__ Quatf q_normalize(Quatf q) {
+  float m = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+  return Quatf{q.x / m, q.y / m, q.z / m, q.w / m};
+}
+__device__ __forceinline__ float3 q_rotate(Quatf q, float3 v) {  // q v q*
+  Quatf r = q_mul(q_mul(q, Quatf{v.x, v.y, v.z, 0.f}), q_conj(q));
+  return make_float3(r.x, r.y, r.z);
+}
+__device__ __forceinline__ float3 q_rotate_inv(Quatf q, float3 v) {  // q* v q
+  Quatf r = q_mul(q_mul(q_conj(q), Quatf{v.x, v.y, v.z, 0.f}), q);
+  return make_float3(r.x, r.y, r.z);
+}
+
+// Exact (no contraction) Hamilton product for the bit-exact AABB path: the reference order
+// ((a + b) + c) - d with every product rounded separately.
+__device__ __forceinline__ float ex4(float a1, float b1, float a2, float b2, float a3, float b3, float a4, float b4) {
+  return __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(a1, b1), __fmul_rn(a2, b2)), __fmul_rn(a3, b3)), __fmul_rn(a4, b4));
+}
+__device__ __forceinline__ Quatf q_mul_exact(Quatf a, Quatf b) {
+  Quatf r;
+  r.x = ex4(a.w, b.x, a.x, b.w, a.y, b.z, a.z, b.y);
+  r.y = ex4(a.w, b.y, a.y, b.w, a.z, b.x, a.x, b.z);
+  r.z = ex4(a.w, b.z, a.z, b.w, a.x, b.y, a.y, b.x);
+  r.w = __fsub_rn(__fsub_rn(__fsub_rn(__fmul_rn(a.w, b.w), __fmul_rn(a.x, b.x)), __fmul_rn(a.y, b.y)),
+                  __fmul_rn(a.z, b.z));
+  return r;
+}
+
+// 3x3 symmetric helpers: world inverse inertia stored as (xx, xy, xz, yy) (yz, zz).
+struct Sym3 {
+  float xx, xy, xz, yy, yz, zz;
+};
+__device__ __forceinline__ float3 sym_mul(const Sym3& s, float3 v) {
+  return make_float3(s.xx * v.x + s.xy * v.y + s.xz * v.z, s.xy * v.x + s.yy * v.y + s.yz * v.z,
+                     s.xz * v.x + s.yz * v.y + s.zz * v.z);
+}
+// Rotation matrix rows of to_matrix (include/math.hpp:287-304).
+__device__ __forceinline__ void q_matrix(Quatf q, float m[3][3]) {
+  float x2 = q.x + q.x, y2 = q.y + q.y, z2 = q.z + q.z;
+  float xx = q.x * x2, xy = q.x * y2, xz = q.x * z2, yy = q.y * y2, yz = q.y * z2, zz = q.z * z2;
+  float wx = q.w * x2, wy = q.w * y2, wz = q.w * z2;
+  m[0][0] = 1.f - (yy + zz); m[0][1] = xy - wz; m[0][2] = xz + wy;
+  m[1][0] = xy + wz; m[1][1] = 1.f - (xx + zz); m[1][2] = yz - wx;
+  m[2][0] = xz - wy; m[2][1] = yz + wx; m[2][2] = 1.f - (xx + yy);
+}
+// World inverse inertia from the body-frame diagonal d.  transpose_quirk: R^T D R
+// (get_transformed_inertia, extensions.slang:184-188); else R D R^T.
+__device__ __forceinline__ Sym3 world_inv_inertia(Quatf q, float3 d, bool transpose_quirk) {
+  float R[3][3];
+  q_matrix(q, R);
+  float M[3][3];  // rows of the matrix S with world = S^T D S
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) M[i][j] = transpose_quirk ? R[i][j] : R[j][i];
+  // world[a][b] = sum_k M[k][a] d_k M[k][b]
+  float dd[3] = {d.x, d.y, d.z};
+  Sym3 s;
+  auto e = [&](int a, int b) { return M[0][a] * dd[0] * M[0][b] + M[1][a] * dd[1] * M[1][b] + M[2][a] * dd[2] * M[2][b]; };
+  s.xx = e(0, 0); s.xy = e(0, 1); s.xz = e(0, 2); s.yy = e(1, 1); s.yz = e(1, 2); s.zz = e(2, 2);
+  return s;
+}
+
+__device__ __forceinline__ void raise_error(DevCounters* c, uint32_t bit) { atomicOr(&c->error_flags, bit); }
+
+// order-preserving float <-> uint (include/math.hpp:228-256)
+__device__ __forceinline__ uint32_t f2ord(float f) {
+  uint32_t u = __float_as_uint(f);
+  uint32_t mask = uint32_t(-int32_t(u >> 31)) | 0x80000000u;
+  return u ^ mask;
+}
+__device__ __forceinline__ float ord2f(uint32_t v) {
+  uint32_t mask = ((v >> 31) - 1u) | 0x80000000u;
+  return __uint_as_float(v ^ mask);
+}
+
+// ---- grid barrier for persistent cooperative kernels ------------------------------------
+// Sense by generation counter; the spin is bounded: on timeout the block raises
+// BB_ERRF_SPIN_LIMIT and every later barrier returns at once (results are then invalid and
+// the host reports BB_E_DEVICE_LIMIT).
+__device__ __forceinline__ void grid_barrier(DevCounters* c) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* gen = &c->barrier_gen;
+    uint32_t g = *gen;
+    __threadfence();
+    uint32_t arrived = atomicAdd(&c->barrier_count, 1u);
+    if (arrived == gridDim.x - 1) {
+      c->barrier_count = 0;
+      __threadfence();
+      atomicAdd(&c->barrier_gen, 1u);
+    } else {
+      uint32_t spins = 0;
+      while (*gen == g) {
+        if (++spins > BB_SPIN_LIMIT || (*(volatile uint32_t*)&c->error_flags & BB_ERRF_SPIN_LIMIT)) {
+          atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// kernel-side solver parameters (a plain copy of bb_solver_params)
+typedef bb_solver_params Params;
+
+// ---- host-side launch helpers (defined in bb_world.cu) ----------------------------------
+#define BB_THREADS 256

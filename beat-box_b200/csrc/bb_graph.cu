@@ -1,0 +1,304 @@
+// bb_graph.cu -- advect, union-find islands, neighbourhood sleeping, edge colouring of the
+// contact graph and the colour buckets the PGS sweeps run over.
+//
+// Reference: entry_rigid_body_sim / RigidBody::advect (src/shaders/simulation/RB_sim.slang:
+// 518-554, src/shaders/extensions.slang:127-139); IslandBuilder (src/shaders/simulation/
+// islands.slang:153-302); entry_sleep_reduce/veto/apply (RB_sim.slang:556-737); graph
+// colouring (src/shaders/simulation/coloring.slang:25-292, rounds RBM:1332-1342).
+//
+// B200 design: the 32 bid/commit colouring rounds (96 dispatches in the reference) run in
+// one persistent cooperative kernel with a grid barrier between phases and stop as soon as
+// every manifold is coloured.  The per-(body, colour) owner cell holds (epoch << 32 | prio)
+// in 64 bits, so it never needs the reference's per-round reset pass.  The colour buckets
+// are one stable onesweep pass keyed by colour, so every colour sweep later reads a compact
+// list instead of scanning all manifolds (RB_sim.slang:1416-1419).
+#include "bb_common.cuh"
+#include "bb_kernels.cuh"
+
+// ---- advect (PGS family) ---------------------------------------------------------------------
+__global__ void k_advect(const DevState d, Params p, uint32_t n, float h) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t f = d.flags[i];
+  if (!(f & BB_BODY_DYNAMIC) || (f & BB_BODY_SLEEPING)) return;
+  float4 v = d.vel[i];
+  if (f & BB_BODY_GRAVITY) {
+    float dv = p.gravity * h;
+    if (p.quirks & BB_QUIRK_GRAVITY_IMPULSE) dv *= d.pos[i].w;  // impulse g*dt scaled by 1/m
+    v.y += dv;
+  }
+  float lin = expf(-h * p.linear_damping), ang = expf(-h * p.angular_damping);
+  d.vel[i] = make_float4(v.x * lin, v.y * lin, v.z * lin, v.w);
+  float4 w = d.omega[i];
+  d.omega[i] = make_float4(w.x * ang, w.y * ang, w.z * ang, w.w);
+}
+
+void bb_advect(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int sms) {
+  (void)sms;
+  if (p.solver == BB_SOLVER_AVBD || !(p.flags & BB_SIM_ADVECTION) || n == 0) return;
+  k_advect<<<(n + BB_THREADS - 1) / BB_THREADS, BB_THREADS, 0, s>>>(d, p, n, h);
+}
+
+// ---- islands ---------------------------------------------------------------------------------
+__global__ void k_uf_init(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  d.uf_parent[i] = (d.flags[i] & BB_BODY_DYNAMIC) ? i : BB_NONE;
+}
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, DevCounters* c) {
+  uint32_t guard = 0;
+  for (;;) {
+    uint32_t px = atomicAdd(&parent[x], 0u);
+    if (px == x) return x;
+    x = px;
+    if (++guard > (1u << 24)) {
+      raise_error(c, BB_ERRF_CAS_LIMIT);
+      return x;
+    }
+  }
+}
+// IslandBuilder::link_bodies (islands.slang:153-213): link the higher root under the lower
+__global__ void k_uf_link(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+    if (!(d.flags[b.x] & BB_BODY_DYNAMIC) || !(d.flags[b.y] & BB_BODY_DYNAMIC)) continue;
+    uint32_t ra = b.x, rb = b.y;
+    for (uint32_t tries = 0;; ++tries) {
+      ra = uf_find(d.uf_parent, ra, d.ctr);
+      rb = uf_find(d.uf_parent, rb, d.ctr);
+      if (ra == rb) break;
+      uint32_t lo = min(ra, rb), hi = max(ra, rb);
+      if (atomicCAS(&d.uf_parent[hi], hi, lo) == hi) break;
+      if (tries > 4096u) {
+        raise_error(d.ctr, BB_ERRF_CAS_LIMIT);
+        break;
+      }
+    }
+  }
+}
+__global__ void k_uf_roots(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t r = d.uf_parent[i];
+  if (r == BB_NONE) {
+    d.is_root[i] = 0;
+    return;
+  }
+  r = uf_find(d.uf_parent, i, d.ctr);
+  d.island[i] = r;  // root for now; rank applied by k_island_ids
+  d.is_root[i] = r == i ? 1u : 0u;
+}
+__global__ void k_island_ids(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  d.island[i] = d.uf_parent[i] == BB_NONE ? BB_NONE : d.root_rank[d.island[i]];
+}
+
+void bb_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
+                int cur) {
+  (void)p;
+  if (n == 0) return;
+  const int T = BB_THREADS;
+  uint32_t blocks = (n + T - 1) / T;
+  k_uf_init<<<blocks, T, 0, s>>>(d, n);
+  k_uf_link<<<sms * 8, T, 0, s>>>(d, cur);
+  k_uf_roots<<<blocks, T, 0, s>>>(d, n);
+  bb_launch_scan(s, d.is_root, d.root_rank, nullptr, n, &d.ctr->island_count, sc.scan_status + 3 * sc.scan_tiles,
+                 sc.scan_tile_ctr + 3, d.ctr);
+  k_island_ids<<<blocks, T, 0, s>>>(d, n);
+}
+
+// ---- sleeping (RB_sim.slang:556-737) --------------------------------------------------------
+__global__ void k_sleep_reduce(const DevState d, Params p, uint32_t n, int cur) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t f = d.flags[i];
+  if (!(f & BB_BODY_DYNAMIC)) return;
+  if (!(p.flags & BB_SIM_SLEEPING_ENABLED)) {
+    d.sleep[i] = 0;
+    d.flags[i] = f & ~BB_BODY_SLEEPING;
+    return;
+  }
+  bool contactless = d.csr_start[cur][i] == d.csr_start[cur][i + 1];
+  if (contactless && (f & BB_BODY_SLEEPING)) {
+    uint32_t t = d.sleep[i] & BB_SLEEP_MASK;
+    d.sleep[i] = t >= 10u ? t - 10u : 0u;
+    return;
+  }
+  float3 v = f3(d.vel[i]), w = f3(d.omega[i]);
+  float lin2 = dot3(v, v), ang2 = dot3(w, w);
+  uint32_t timer = d.sleep[i] & BB_SLEEP_MASK;
+  bool calm = lin2 < p.sleep_lin_vel2 && ang2 < p.sleep_ang_vel2;
+  d.sleep[i] = calm ? min(timer + 1u, p.sleep_steps) : (timer >= 4u ? timer - 4u : 0u);
+}
+__global__ void k_sleep_veto(const DevState d, Params p, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    uint32_t slot = d.man_slot[cur][m];
+    uint2 b = d.m_bodies[cur][slot];
+    uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+    bool ad = fa & BB_BODY_DYNAMIC, bd = fb & BB_BODY_DYNAMIC;
+    bool a_loud = ad && (d.sleep[b.x] & BB_SLEEP_MASK) < p.sleep_steps;
+    bool b_loud = bd && (d.sleep[b.y] & BB_SLEEP_MASK) < p.sleep_steps;
+    int32_t err = __float_as_int(d.m_normal[cur][slot].w);
+    bool stalled = err != 0x7FFFFFFF && abs(err) < 10;
+    bool deep = false;
+    if (!stalled) {
+      int cc = d.m_keycc[cur][slot].y;
+      for (int c = 0; c < cc; ++c)
+        if (d.c_pos[cur][slot * BB_MAX_CONTACTS + c].w < -0.05f) {
+          deep = true;
+          break;
+        }
+    }
+    if ((a_loud || deep) && bd) atomicOr(&d.sleep[b.y], BB_SLEEP_VETO);
+    if ((b_loud || deep) && ad) atomicOr(&d.sleep[b.x], BB_SLEEP_VETO);
+  }
+}
+__global__ void k_sleep_apply(const DevState d, uint32_t n, Params p) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t f = d.flags[i];
+  if (!(f & BB_BODY_DYNAMIC)) return;
+  uint32_t t = d.sleep[i];
+  bool vetoed = (t & BB_SLEEP_VETO) != 0;
+  bool quiet = (t & BB_SLEEP_MASK) >= p.sleep_steps;
+  bool was = (f & BB_BODY_SLEEPING) != 0;
+  if (quiet && !vetoed) {
+    if (!was) {
+      float4 v = d.vel[i];
+      d.vel[i] = make_float4(0.f, 0.f, 0.f, v.w);
+      d.omega[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      d.flags[i] = f | BB_BODY_SLEEPING;
+    }
+    atomicAdd(&d.ctr->sleeping, 1u);
+  } else if (was) {
+    d.flags[i] = f & ~BB_BODY_SLEEPING;
+  }
+}
+
+void bb_sleep(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, int sms, int cur) {
+  if (n == 0) return;
+  const int T = BB_THREADS;
+  uint32_t blocks = (n + T - 1) / T;
+  k_sleep_reduce<<<blocks, T, 0, s>>>(d, p, n, cur);
+  if (!(p.flags & BB_SIM_SLEEPING_ENABLED)) return;
+  k_sleep_veto<<<sms * 8, T, 0, s>>>(d, p, cur);
+  k_sleep_apply<<<blocks, T, 0, s>>>(d, n, p);
+}
+
+// ---- edge colouring ------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t gc_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ uint32_t gc_priority(uint32_t pid, uint32_t round) {
+  uint32_t h = gc_hash(pid + round * 0x85ebca6bu) & 0xFFFu;
+  if (h == 0u) h = 1u;
+  return (h << 20) | (pid & 0xFFFFFu);
+}
+
+// Persistent cooperative kernel: init, then rounds r = 1..gc_rounds of
+//   bid:    every uncoloured manifold takes the lowest colour free on both dynamic bodies
+//           (gc_pick_color, coloring.slang:95-103) and atomically maxes its priority
+//           (gc_priority, :130-138) into owner[body][colour];
+//   commit: a manifold that won on both bodies takes the colour (:179-212).
+// Finally writes the (colour, manifold) keys of the bucket sort.
+__global__ void __launch_bounds__(BB_THREADS) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
+  DevCounters* c = d.ctr;
+  const uint32_t M = c->manifold_count;
+  const uint32_t epoch = c->gc_epoch;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  uint32_t* uncol = &c->pad[0];  // two alternating per-round counters
+  for (uint32_t i = tid; i < n; i += stride) d.gc_mask[i] = 0;
+  for (uint32_t m = tid; m < M; m += stride) {
+    uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+    int key = d.m_keycc[cur][d.man_slot[cur][m]].x;
+    uint32_t lo = min(b.x, b.y), hi = max(b.x, b.y);
+    d.gc_pid[m] = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
+    d.gc_color[m] = BB_UNCOLORED;
+  }
+  if (tid == 0) {
+    uncol[1] = 0;
+    c->gc_colors = 0;
+  }
+  grid_barrier(c);
+  for (uint32_t r = 1; r <= p.gc_rounds; ++r) {
+    const unsigned long long tag = (unsigned long long)(epoch + r) << 32;
+    uint32_t mine = 0;
+    for (uint32_t m = tid; m < M; m += stride) {
+      if (d.gc_color[m] != BB_UNCOLORED) continue;
+      ++mine;
+      uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+      bool sa = !(d.flags[b.x] & BB_BODY_DYNAMIC), sb = !(d.flags[b.y] & BB_BODY_DYNAMIC);
+      uint32_t avail = ~((sa ? 0u : d.gc_mask[b.x]) | (sb ? 0u : d.gc_mask[b.y]));
+      uint32_t col = avail == 0u ? BB_MAX_COLORS : uint32_t(__ffs(avail) - 1);
+      d.gc_choice[m] = col;
+      if (col >= BB_MAX_COLORS) continue;
+      unsigned long long v = tag | gc_priority(d.gc_pid[m], r);
+      if (!sa) atomicMax(&d.gc_owner[size_t(b.x) * BB_MAX_COLORS + col], v);
+      if (!sb) atomicMax(&d.gc_owner[size_t(b.y) * BB_MAX_COLORS + col], v);
+    }
+    if (mine) atomicAdd(&uncol[r & 1], mine);
+    grid_barrier(c);
+    if (*(volatile uint32_t*)&uncol[r & 1] == 0u) break;
+    if (tid == 0) uncol[(r + 1) & 1] = 0;
+    for (uint32_t m = tid; m < M; m += stride) {
+      if (d.gc_color[m] != BB_UNCOLORED) continue;
+      uint32_t col = d.gc_choice[m];
+      if (col >= BB_MAX_COLORS) continue;
+      uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+      bool sa = !(d.flags[b.x] & BB_BODY_DYNAMIC), sb = !(d.flags[b.y] & BB_BODY_DYNAMIC);
+      unsigned long long v = tag | gc_priority(d.gc_pid[m], r);
+      bool wa = sa || d.gc_owner[size_t(b.x) * BB_MAX_COLORS + col] == v;
+      bool wb = sb || d.gc_owner[size_t(b.y) * BB_MAX_COLORS + col] == v;
+      if (wa && wb) {
+        d.gc_color[m] = col;
+        if (!sa) atomicOr(&d.gc_mask[b.x], 1u << col);
+        if (!sb) atomicOr(&d.gc_mask[b.y], 1u << col);
+        atomicMax(&c->gc_colors, col + 1u);
+      }
+    }
+    grid_barrier(c);
+  }
+  uint32_t over = 0;
+  for (uint32_t m = tid; m < M; m += stride) {
+    uint32_t col = d.gc_color[m];
+    if (col == BB_UNCOLORED) ++over;
+    d.bucket_keys[0][m] = col == BB_UNCOLORED ? BB_MAX_COLORS : col;
+    d.bucket_vals[0][m] = m;
+  }
+  if (over) atomicAdd(&c->gc_overflow, over);
+  if (tid == 0) c->gc_epoch = epoch + 64u;
+}
+
+// bucket_start[0..33]: start of colour c (32 = overflow), [33] = M
+__global__ void k_bucket_starts(const uint32_t* hist_scan, const uint32_t* n_ptr, uint32_t* starts, int nb) {
+  int t = threadIdx.x;
+  if (t < nb) starts[t] = hist_scan[t];
+  if (t == nb) starts[t] = *n_ptr;
+}
+
+int bb_edge_coloring_blocks(int sms) { return bb_coop_blocks((const void*)k_edge_color, BB_THREADS, sms); }
+
+void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
+                      int sms, int cur, int coop_blocks) {
+  Params pp = p;
+  int cc = cur;
+  uint32_t nn = n;
+  DevState dd = d;
+  void* args[] = {&dd, &pp, &cc, &nn};
+  bb_launch_coop((const void*)k_edge_color, coop_blocks, BB_THREADS, args, s);
+  // stable bucket sort of manifold ids by colour (one 8-bit digit)
+  uint32_t* keys[2] = {d.bucket_keys[0], d.bucket_keys[1]};
+  uint32_t* vals[2] = {d.bucket_vals[0], d.bucket_vals[1]};
+  uint32_t* hist = sc.sort_hist + 2 * 4 * 256;
+  bb_launch_sort(s, keys, vals, &d.ctr->manifold_count, d.pair_capacity, 1, 0, hist, sc.sort_status + 4 * sc.sort_tiles * 256,
+                 sc.sort_tile_ctr + 4, d.ctr, sms);
+  k_bucket_starts<<<1, 64, 0, s>>>(hist + 4 * 256, &d.ctr->manifold_count, d.bucket_start, BB_MAX_COLORS + 1);
+}

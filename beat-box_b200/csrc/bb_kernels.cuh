@@ -1,0 +1,54 @@
+// bb_kernels.cuh -- host-side launchers of the step's kernels (one .cu file per stage).
+#pragma once
+#include "bb_common.cuh"
+
+// bb_scan_sort.cu
+void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint32_t n_cap,
+                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr);
+uint32_t bb_scan_tiles(uint32_t n_cap);
+uint32_t bb_sort_tiles(uint32_t n_cap);
+void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,
+                    int passes, int shift0, uint32_t* hist, uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr,
+                    int sms);
+
+// Scratch bookkeeping shared by the stages of one substep.
+struct StepScratch {
+  unsigned long long* scan_status;  // n_scans x scan_tiles
+  uint32_t* scan_tile_ctr;          // n_scans
+  uint32_t scan_tiles;
+  uint32_t* sort_hist;              // n_sorts x (2 x 4 x 256)
+  uint32_t* sort_status;            // n_sorts x 4 x sort_tiles x 256
+  uint32_t* sort_tile_ctr;          // n_sorts x 4
+  uint32_t sort_tiles;
+};
+
+// bb_bvh.cu: Morton codes -> sort -> Karras LBVH -> refit -> broad phase
+void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
+                  int cur);
+
+// bb_narrow.cu: narrow phase + warm start + manifold compaction + per-body lists
+void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
+                     int sms, int cur, bool warm);
+
+// bb_graph.cu: advect, islands, sleeping, edge colouring + colour buckets
+void bb_advect(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int sms);
+void bb_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
+                int cur);
+void bb_sleep(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, int sms, int cur);
+void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
+                      int sms, int cur, int coop_blocks);
+
+// bb_solve.cu: PGS_SOFT and AVBD solvers
+void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
+                       int coop_blocks, int sms);
+void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,
+                   int sms, int cur, int coop_blocks);
+
+// co-resident block counts of the persistent cooperative kernels
+int bb_edge_coloring_blocks(int sms);
+int bb_pgs_soft_blocks(int sms);
+int bb_avbd_blocks(int sms);
+
+// occupancy helpers (bb_world.cu)
+int bb_coop_blocks(const void* kernel, int threads, int sms);
+cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s);

@@ -1,0 +1,632 @@
+// bb_narrow.cu -- narrow phase with persistent-contact warm start, manifold compaction and
+// per-body manifold lists.
+//
+// Reference: narrow_phase (src/shaders/simulation/collision_detection.slang:1514-1755),
+// OBBvsOBBCollision (:5-877: SAT :562-740, incident face :123-243, reference edges :245-336,
+// clipping :352-449, edge contact :456-548), find_old_collision (:914-963),
+// Manifold::compute_basis / update_from_old (src/shaders/extensions.slang:262-473),
+// body_link_manifold (collision_detection.slang:881-905).
+//
+// B200 design: one thread per broad-phase pair writes its manifold into the pair's own slot
+// (no atomic append), a scan over the hit flags gives the compact manifold order (= pair
+// order), and each dynamic body gets a CSR list of its manifolds in ascending order built by
+// count / scan / fill / per-body sort.  Warm-start lookup walks the previous substep's CSR
+// list of the pair's dynamic body, which finds the same (unique) old manifold as the
+// reference's linked-list walk.
+#include "bb_common.cuh"
+#include "bb_kernels.cuh"
+
+namespace {
+
+enum : uint32_t {
+  POS_X_POS_Y = 0, POS_X_NEG_Y = 1, POS_X_POS_Z = 2, POS_X_NEG_Z = 3, NEG_X_POS_Y = 4, NEG_X_NEG_Y = 5,
+  NEG_X_POS_Z = 6, NEG_X_NEG_Z = 7, POS_Y_POS_Z = 8, POS_Y_NEG_Z = 9, NEG_Y_POS_Z = 10, NEG_Y_NEG_Z = 11
+};
+
+// feature pair packed in one word: in_ref | out_ref << 8 | in_inc << 16 | out_inc << 24
+__device__ __forceinline__ uint32_t fp_pack(uint32_t ir, uint32_t orf, uint32_t ii, uint32_t oi) {
+  return (ir & 255u) | ((orf & 255u) << 8) | ((ii & 255u) << 16) | ((oi & 255u) << 24);
+}
+__device__ __forceinline__ uint32_t fp_in_ref(uint32_t f) { return f & 255u; }
+__device__ __forceinline__ uint32_t fp_out_ref(uint32_t f) { return (f >> 8) & 255u; }
+__device__ __forceinline__ uint32_t fp_in_inc(uint32_t f) { return (f >> 16) & 255u; }
+__device__ __forceinline__ uint32_t fp_out_inc(uint32_t f) { return (f >> 24) & 255u; }
+__device__ __forceinline__ uint32_t fp_set_in_ref(uint32_t f, uint32_t v) { return (f & ~255u) | (v & 255u); }
+__device__ __forceinline__ uint32_t fp_set_out_ref(uint32_t f, uint32_t v) { return (f & ~(255u << 8)) | ((v & 255u) << 8); }
+__device__ __forceinline__ uint32_t fp_swap_roles(uint32_t f) {
+  return fp_pack(fp_in_inc(f), fp_out_inc(f), fp_in_ref(f), fp_out_ref(f));
+}
+
+// Slang-semantics transform: rows of r are the body axes; vectors multiply from the left.
+struct Xf {
+  float r[3][3];
+  float3 p;
+};
+__device__ __forceinline__ float3 xf_rotate(const Xf& t, float3 v) {
+  return make_float3(v.x * t.r[0][0] + v.y * t.r[1][0] + v.z * t.r[2][0], v.x * t.r[0][1] + v.y * t.r[1][1] + v.z * t.r[2][1],
+                     v.x * t.r[0][2] + v.y * t.r[1][2] + v.z * t.r[2][2]);
+}
+__device__ __forceinline__ float3 xf_rotate_t(const Xf& t, float3 v) {
+  return make_float3(t.r[0][0] * v.x + t.r[0][1] * v.y + t.r[0][2] * v.z, t.r[1][0] * v.x + t.r[1][1] * v.y + t.r[1][2] * v.z,
+                     t.r[2][0] * v.x + t.r[2][1] * v.y + t.r[2][2] * v.z);
+}
+__device__ __forceinline__ float3 xf_transform(const Xf& t, float3 v) { return xf_rotate(t, v) + t.p; }
+__device__ __forceinline__ float3 xf_transform_t(const Xf& t, float3 v) { return xf_rotate_t(t, v - t.p); }
+__device__ __forceinline__ float3 row3(const float m[3][3], int i) { return make_float3(m[i][0], m[i][1], m[i][2]); }
+__device__ __forceinline__ float3 col3(const float m[3][3], int j) { return make_float3(m[0][j], m[1][j], m[2][j]); }
+
+__device__ __forceinline__ void body_axes(Quatf q, float r[3][3]) {
+  float R[3][3];
+  q_matrix(q, R);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r[i][j] = R[j][i];
+}
+
+struct CV {
+  float3 v;
+  uint32_t f;
+};
+
+struct Contacts {
+  int cc;
+  int key;
+  float3 normal;
+  float3 pos[BB_MAX_CONTACTS];
+  float pen[BB_MAX_CONTACTS];
+  uint32_t fp[BB_MAX_CONTACTS];
+};
+
+// compute_incident_face (collision_detection.slang:123-243)
+__device__ void incident_face(const Xf& itx, float3 e, float3 n, CV out[4]) {
+  n = -xf_rotate_t(itx, n);
+  float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+  float3 v[4];
+  uint32_t fi[4][2];
+  auto set = [&](uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, uint32_t c0, uint32_t c1, uint32_t d0, uint32_t d1) {
+    fi[0][0] = a0; fi[0][1] = a1; fi[1][0] = b0; fi[1][1] = b1; fi[2][0] = c0; fi[2][1] = c1; fi[3][0] = d0; fi[3][1] = d1;
+  };
+  if (ax > ay && ax > az) {
+    if (n.x > 0.f) {
+      v[0] = make_float3(e.x, e.y, -e.z); v[1] = make_float3(e.x, e.y, e.z); v[2] = make_float3(e.x, -e.y, e.z); v[3] = make_float3(e.x, -e.y, -e.z);
+      set(POS_Y_NEG_Z, POS_X_NEG_Y, POS_X_NEG_Y, POS_Y_POS_Z, POS_Y_POS_Z, NEG_X_NEG_Z, NEG_X_NEG_Z, POS_Y_NEG_Z);
+    } else {
+      v[0] = make_float3(-e.x, -e.y, e.z); v[1] = make_float3(-e.x, e.y, e.z); v[2] = make_float3(-e.x, e.y, -e.z); v[3] = make_float3(-e.x, -e.y, -e.z);
+      set(NEG_X_NEG_Y, NEG_Y_NEG_Z, NEG_Y_NEG_Z, POS_X_NEG_Z, POS_X_NEG_Z, NEG_Y_POS_Z, NEG_Y_POS_Z, NEG_X_NEG_Y);
+    }
+  } else if (ay > ax && ay > az) {
+    if (n.y > 0.f) {
+      v[0] = make_float3(-e.x, e.y, e.z); v[1] = make_float3(e.x, e.y, e.z); v[2] = make_float3(e.x, e.y, -e.z); v[3] = make_float3(-e.x, e.y, -e.z);
+      set(POS_X_NEG_Z, POS_X_POS_Y, POS_X_POS_Y, POS_X_NEG_Y, POS_X_NEG_Y, POS_X_POS_Z, POS_X_POS_Z, POS_X_NEG_Z);
+    } else {
+      v[0] = make_float3(e.x, -e.y, e.z); v[1] = make_float3(-e.x, -e.y, e.z); v[2] = make_float3(-e.x, -e.y, -e.z); v[3] = make_float3(e.x, -e.y, -e.z);
+      set(NEG_X_NEG_Z, NEG_X_POS_Y, NEG_X_POS_Y, NEG_X_NEG_Y, NEG_X_NEG_Y, NEG_X_POS_Z, NEG_X_POS_Z, NEG_X_NEG_Z);
+    }
+  } else {
+    if (n.z > 0.f) {
+      v[0] = make_float3(-e.x, e.y, e.z); v[1] = make_float3(-e.x, -e.y, e.z); v[2] = make_float3(e.x, -e.y, e.z); v[3] = make_float3(e.x, e.y, e.z);
+      set(POS_X_POS_Y, NEG_Y_NEG_Z, NEG_Y_NEG_Z, NEG_X_POS_Y, NEG_X_POS_Y, POS_Y_POS_Z, POS_Y_POS_Z, POS_X_POS_Y);
+    } else {
+      v[0] = make_float3(e.x, -e.y, -e.z); v[1] = make_float3(-e.x, -e.y, -e.z); v[2] = make_float3(-e.x, e.y, -e.z); v[3] = make_float3(e.x, e.y, -e.z);
+      set(POS_Y_NEG_Z, NEG_X_POS_Z, NEG_X_POS_Z, NEG_Y_POS_Z, NEG_Y_POS_Z, POS_X_POS_Z, POS_X_POS_Z, POS_Y_NEG_Z);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    out[i].v = xf_transform(itx, v[i]);
+    out[i].f = fp_pack(0u, 0u, fi[i][0], fi[i][1]);
+  }
+}
+
+// compute_reference_edges_and_basis (collision_detection.slang:245-336)
+__device__ void reference_edges(float3 er, const Xf& rtx, float3 n, int axis, uint32_t clip[4], Xf& basis, float3& e) {
+  n = xf_rotate_t(rtx, n);
+  if (axis > 2) axis -= 3;
+  float3 r0 = row3(rtx.r, 0), r1 = row3(rtx.r, 1), r2 = row3(rtx.r, 2);
+  float3 b0, b1, b2;
+  if (axis == 0) {
+    if (n.x > 0.f) { clip[0] = POS_X_NEG_Y; clip[1] = POS_Y_POS_Z; clip[2] = NEG_X_NEG_Z; clip[3] = POS_Y_NEG_Z; e = make_float3(er.y, er.z, er.x); b0 = r1; b1 = r2; b2 = r0; }
+    else { clip[0] = NEG_Y_NEG_Z; clip[1] = POS_X_NEG_Z; clip[2] = NEG_Y_POS_Z; clip[3] = NEG_X_NEG_Y; e = make_float3(er.z, er.y, er.x); b0 = r2; b1 = r1; b2 = -r0; }
+  } else if (axis == 1) {
+    if (n.y > 0.f) { clip[0] = POS_X_POS_Y; clip[1] = POS_X_NEG_Y; clip[2] = POS_X_POS_Z; clip[3] = POS_X_NEG_Z; e = make_float3(er.z, er.x, er.y); b0 = r2; b1 = r0; b2 = r1; }
+    else { clip[0] = NEG_X_POS_Y; clip[1] = NEG_X_NEG_Y; clip[2] = NEG_X_POS_Z; clip[3] = NEG_X_NEG_Z; e = make_float3(er.z, er.x, er.y); b0 = r2; b1 = -r0; b2 = -r1; }
+  } else {
+    if (n.z > 0.f) { clip[0] = NEG_Y_NEG_Z; clip[1] = NEG_X_POS_Y; clip[2] = POS_Y_POS_Z; clip[3] = POS_X_POS_Y; e = make_float3(er.y, er.x, er.z); b0 = -r1; b1 = r0; b2 = r2; }
+    else { clip[0] = NEG_X_POS_Z; clip[1] = NEG_Y_POS_Z; clip[2] = POS_X_POS_Z; clip[3] = POS_Y_NEG_Z; e = make_float3(er.y, er.x, er.z); b0 = -r1; b1 = -r0; b2 = -r2; }
+  }
+  basis.r[0][0] = b0.x; basis.r[0][1] = b0.y; basis.r[0][2] = b0.z;
+  basis.r[1][0] = b1.x; basis.r[1][1] = b1.y; basis.r[1][2] = b1.z;
+  basis.r[2][0] = b2.x; basis.r[2][1] = b2.y; basis.r[2][2] = b2.z;
+  basis.p = rtx.p;
+}
+
+// ortographic_clip (collision_detection.slang:352-387); output capped at 8
+__device__ int ortho_clip(float sign, float e, int axis, uint32_t clip_edge, const CV* in, int in_count, CV* out) {
+  const float TH = 0.005f;
+  int oc = 0;
+  CV a = in[in_count - 1];
+  for (int i = 0; i < in_count; ++i) {
+    CV b = in[i];
+    float da = sign * comp(a.v, axis) - e;
+    float db = sign * comp(b.v, axis) - e;
+    bool on_a = da < TH && da > -TH, on_b = db < TH && db > -TH;
+    if ((da < 0.f && db < 0.f) || on_a || on_b) {
+      if (oc < BB_MAX_CONTACTS) out[oc++] = b;
+    } else if (da < 0.f && db >= 0.f) {
+      CV cv;
+      cv.f = fp_set_out_ref(b.f, clip_edge);
+      cv.v = a.v + (b.v - a.v) * (da / (da - db));
+      if (oc < BB_MAX_CONTACTS) out[oc++] = cv;
+    } else if (da >= 0.f && db < 0.f) {
+      CV cv;
+      cv.f = fp_set_in_ref(a.f, clip_edge);
+      cv.v = a.v + (b.v - a.v) * (da / (da - db));
+      if (oc < BB_MAX_CONTACTS) out[oc++] = cv;
+      if (oc < BB_MAX_CONTACTS) out[oc++] = b;
+    }
+    a = b;
+  }
+  return oc;
+}
+
+__device__ __forceinline__ float c_sign(float x) { return x < 0.f ? -1.f : 1.f; }
+
+// support_edge (collision_detection.slang:456-497)
+__device__ void support_edge(const Xf& tx, float3 e, float3 n, float3& ca, float3& cb) {
+  n = xf_rotate_t(tx, n);
+  float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+  int axis = (ax <= ay && ax <= az) ? 0 : ((ay <= ax && ay <= az) ? 1 : 2);
+  float3 v0 = make_float3(c_sign(n.x) * e.x, c_sign(n.y) * e.y, c_sign(n.z) * e.z), v1 = v0;
+  set_comp(v0, axis, comp(e, axis));
+  set_comp(v1, axis, -comp(e, axis));
+  ca = xf_transform(tx, v0);
+  cb = xf_transform(tx, v1);
+}
+
+// edges_contact (collision_detection.slang:499-548)
+__device__ void edges_contact(float3 pa, float3 qa, float3 pb, float3 qb, float3& ca, float3& cb) {
+  float3 da = qa - pa, db = qb - pb, r = pa - pb;
+  float a = dot3(da, da), e = dot3(db, db), f = dot3(db, r), c = dot3(da, r), b = dot3(da, db);
+  float denom = a * e - b * b;
+  if (denom == 0.f) {
+    float t = fminf(fmaxf(dot3(r, da) / a, 0.f), 1.f);
+    ca = pa + da * t;
+    float u = fminf(fmaxf(dot3(ca - pb, db) / e, 0.f), 1.f);
+    cb = pb + db * u;
+    return;
+  }
+  float ta = fminf(fmaxf((b * f - c * e) / denom, 0.f), 1.f);
+  float tb = (b * ta + f) / e;
+  if (tb < 0.f) {
+    tb = 0.f;
+    ta = fminf(fmaxf(-c / a, 0.f), 1.f);
+  } else if (tb > 1.f) {
+    tb = 1.f;
+    ta = fminf(fmaxf((b - c) / a, 0.f), 1.f);
+  }
+  ca = pa + da * ta;
+  cb = pb + db * tb;
+}
+
+// OBBvsOBBCollision::collision_detection (collision_detection.slang:562-876)
+__device__ bool box_box(Quatf qa, float3 pa, float3 ea, Quatf qb, float3 pb, float3 eb, bool sat_quirk, Contacts& out) {
+  out.cc = 0;
+  out.key = -1;
+  Xf txa, txb;
+  body_axes(qa, txa.r);
+  txa.p = pa;
+  body_axes(qb, txb.r);
+  txb.p = pb;
+  float C[3][3], aC[3][3];
+  bool parallel = false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float v;
+      if (sat_quirk) v = txa.r[0][i] * txb.r[0][j] + txa.r[1][i] * txb.r[1][j] + txa.r[2][i] * txb.r[2][j];
+      else v = txb.r[i][0] * txa.r[j][0] + txb.r[i][1] * txa.r[j][1] + txb.r[i][2] * txa.r[j][2];
+      C[i][j] = v;
+      aC[i][j] = fabsf(v);
+      if (aC[i][j] > 0.9998f) parallel = true;
+    }
+  float3 t = q_rotate_inv(qa, pb - pa);
+  float a_max = -3.402823466e+38f, b_max = -3.402823466e+38f, e_max = -3.402823466e+38f;
+  int a_axis = -1, b_axis = -1, e_axis = -1;
+  float3 n_a = make_float3(0, 0, 0), n_b = n_a, n_e = n_a;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float s = fabsf(comp(t, i)) - (comp(ea, i) + dot3(col3(aC, i), eb));
+    if (s > 0.f) return false;
+    if (s > a_max) { a_max = s; a_axis = i; n_a = row3(txa.r, i); }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float proj = dot3(t, row3(C, i));
+    float s = fabsf(proj) - (comp(eb, i) + dot3(row3(aC, i), ea));
+    if (s > 0.f) return false;
+    if (s > b_max) { b_max = s; b_axis = 3 + i; n_b = row3(txb.r, i); }
+  }
+  if (!parallel) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+        float rA = comp(ea, i1) * aC[j][i2] + comp(ea, i2) * aC[j][i1];
+        float rB = comp(eb, j1) * aC[j2][i] + comp(eb, j2) * aC[j1][i];
+        float s = fabsf(comp(t, i2) * C[j][i1] - comp(t, i1) * C[j][i2]) - (rA + rB);
+        float3 axis = make_float3(0, 0, 0);
+        set_comp(axis, i1, -C[j][i2]);
+        set_comp(axis, i2, C[j][i1]);
+        if (s > 0.f) return false;
+        float l = 1.0f / len3(axis);
+        s *= l;
+        if (s > e_max) { e_max = s; e_axis = 6 + i * 3 + j; n_e = axis * l; }
+      }
+    }
+  }
+  int axis;
+  float s_max;
+  float3 normal;
+  float face_max = fmaxf(a_max, b_max);
+  if (0.95f * e_max > face_max + 0.01f) { axis = e_axis; s_max = e_max; normal = n_e; }
+  else if (0.95f * b_max > a_max + 0.01f) { axis = b_axis; s_max = b_max; normal = n_b; }
+  else { axis = a_axis; s_max = a_max; normal = n_a; }
+  if (dot3(normal, pb - pa) < 0.f) normal = -normal;
+  if (axis == -1) return false;
+  if (axis <= 5) {
+    const Xf& rtx = axis <= 2 ? txa : txb;
+    const Xf& itx = axis <= 2 ? txb : txa;
+    float3 er = axis <= 2 ? ea : eb, ei = axis <= 2 ? eb : ea;
+    bool flip = axis > 2;
+    if (flip) normal = -normal;
+    CV inc[4];
+    incident_face(itx, ei, normal, inc);
+    uint32_t clip[4];
+    Xf basis;
+    float3 e;
+    reference_edges(er, rtx, normal, axis, clip, basis, e);
+    CV in[BB_MAX_CONTACTS], outv[BB_MAX_CONTACTS];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      in[i].v = xf_transform_t(basis, inc[i].v);
+      in[i].f = inc[i].f;
+    }
+    int oc = ortho_clip(1.f, e.x, 0, clip[0], in, 4, outv);
+    if (oc == 0) return false;
+    int ic = ortho_clip(1.f, e.y, 1, clip[1], outv, oc, in);
+    if (ic == 0) return false;
+    oc = ortho_clip(-1.f, e.x, 0, clip[2], in, ic, outv);
+    if (oc == 0) return false;
+    ic = ortho_clip(-1.f, e.y, 1, clip[3], outv, oc, in);
+    if (ic == 0) return false;
+    int n = 0;
+    for (int i = 0; i < ic; ++i) {
+      float dd = in[i].v.z - e.z;
+      if (dd <= 0.f) {
+        out.pos[n] = xf_transform(basis, in[i].v);
+        out.pen[n] = dd;
+        out.fp[n] = flip ? fp_swap_roles(in[i].f) : in[i].f;
+        ++n;
+      }
+    }
+    if (n > 0) {
+      out.cc = n;
+      out.normal = flip ? -normal : normal;
+    }
+  } else {
+    normal = xf_rotate(txa, normal);
+    if (dot3(normal, pb - pa) < 0.f) normal = -normal;
+    float3 p0, q0, p1, q1, ca, cb;
+    support_edge(txa, ea, normal, p0, q0);
+    support_edge(txb, eb, -normal, p1, q1);
+    edges_contact(p0, q0, p1, q1, ca, cb);
+    out.cc = 1;
+    out.normal = normal;
+    out.pos[0] = (ca + cb) * 0.5f;
+    out.pen[0] = s_max;
+    out.fp[0] = fp_pack(axis, axis, axis, axis);
+  }
+  out.key = axis;
+  return out.cc > 0;
+}
+
+// Sphere contacts (first principles; the reference has no sphere collider).
+__device__ bool sphere_sphere(float3 pa, float ra, float3 pb, float rb, Contacts& out) {
+  float3 d = pb - pa;
+  float dist = len3(d);
+  if (dist > ra + rb) return false;
+  float3 n = dist > 1e-9f ? d * (1.0f / dist) : make_float3(0, 1, 0);
+  float pen = dist - (ra + rb);
+  out.cc = 1;
+  out.key = BB_KEY_SPHERE_SPHERE;
+  out.normal = n;
+  out.pen[0] = pen;
+  out.pos[0] = pa + n * (ra + pen * 0.5f);
+  out.fp[0] = fp_pack(BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE);
+  return true;
+}
+__device__ bool box_sphere_core(Quatf qx, float3 px, float3 e, float3 ps, float r, float3& n, float& pen, float3& pos) {
+  float3 c = q_rotate_inv(qx, ps - px);
+  float3 q = make_float3(fminf(fmaxf(c.x, -e.x), e.x), fminf(fmaxf(c.y, -e.y), e.y), fminf(fmaxf(c.z, -e.z), e.z));
+  bool inside = fabsf(c.x) < e.x && fabsf(c.y) < e.y && fabsf(c.z) < e.z;
+  if (!inside) {
+    float3 dl = c - q;
+    float dist = len3(dl);
+    if (dist > r) return false;
+    float3 nl = dist > 1e-9f ? dl * (1.0f / dist) : make_float3(0, 1, 0);
+    n = q_rotate(qx, nl);
+    pen = dist - r;
+    pos = ((px + q_rotate(qx, q)) + (ps - n * r)) * 0.5f;
+    return true;
+  }
+  int ax = 0;
+  float best = e.x - fabsf(c.x);
+  if (e.y - fabsf(c.y) < best) { best = e.y - fabsf(c.y); ax = 1; }
+  if (e.z - fabsf(c.z) < best) { best = e.z - fabsf(c.z); ax = 2; }
+  float3 nl = make_float3(0, 0, 0);
+  float sg = comp(c, ax) < 0.f ? -1.f : 1.f;
+  set_comp(nl, ax, sg);
+  n = q_rotate(qx, nl);
+  pen = -best - r;
+  float3 face = c;
+  set_comp(face, ax, sg * comp(e, ax));
+  pos = ((px + q_rotate(qx, face)) + (ps - n * r)) * 0.5f;
+  return true;
+}
+
+__device__ __forceinline__ uint32_t warm_inc(uint32_t w) { return min(255u, w + 1u); }
+
+}  // namespace
+
+// Narrow phase + warm start: one thread per pair.
+__global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int cur, int warm) {
+  const int prv = cur ^ 1;
+  const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x) {
+    uint2 pr = d.pairs[k];
+    uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
+    uint32_t fa = d.flags[ida], fb = d.flags[idb];
+    d.hit[k] = 0;
+    d.m_keycc[cur][k] = make_int2(-1, 0);
+    if (!(fa & BB_BODY_DYNAMIC) && !(fb & BB_BODY_DYNAMIC)) continue;  // static-static (:1525)
+    float4 pa4 = d.pos[ida], pb4 = d.pos[idb];
+    float4 sa = d.shape[ida], sb = d.shape[idb];
+    Quatf qa = q_from(d.rot[ida]), qb = q_from(d.rot[idb]);
+    float3 pa = f3(pa4), pb = f3(pb4);
+    uint32_t ta = __float_as_uint(sa.w), tb = __float_as_uint(sb.w);
+    Contacts m;
+    bool hit;
+    if (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) {
+      hit = box_box(qa, pa, f3(sa), qb, pb, f3(sb), (p.quirks & BB_QUIRK_SAT_FRAME) != 0, m);
+    } else if (ta == BB_SHAPE_SPHERE && tb == BB_SHAPE_SPHERE) {
+      hit = sphere_sphere(pa, sa.x, pb, sb.x, m);
+    } else {
+      float3 n, pos;
+      float pen;
+      if (ta == BB_SHAPE_BOX) {
+        hit = box_sphere_core(qa, pa, f3(sa), pb, sb.x, n, pen, pos);
+        m.key = BB_KEY_BOX_SPHERE;
+      } else {
+        hit = box_sphere_core(qb, pb, f3(sb), pa, sa.x, n, pen, pos);
+        n = -n;
+        m.key = BB_KEY_SPHERE_BOX;
+      }
+      if (hit) {
+        m.cc = 1;
+        m.normal = n;
+        m.pen[0] = pen;
+        m.pos[0] = pos;
+        m.fp[0] = fp_pack(m.key, m.key, m.key, m.key);
+      }
+    }
+    if (!hit) continue;
+    // compute_basis (extensions.slang:262-272)
+    float3 n = m.normal, t0;
+    if (fabsf(n.x) > fabsf(n.y)) t0 = make_float3(n.z, 0.f, -n.x);
+    else t0 = make_float3(0.f, -n.z, n.y);
+    t0 = t0 * (1.0f / len3(t0));
+    float3 t1 = cross3(t0, n);
+    // new contacts; inherited fields start at zero
+    float3 cpos[BB_MAX_CONTACTS];
+    float cpen[BB_MAX_CONTACTS];
+    uint32_t cfp[BB_MAX_CONTACTS], cwarm[BB_MAX_CONTACTS], cstick[BB_MAX_CONTACTS];
+    float4 clam[BB_MAX_CONTACTS];
+    float2 ckt[BB_MAX_CONTACTS];
+    float3 canca[BB_MAX_CONTACTS], cancb[BB_MAX_CONTACTS];
+    const int cc = m.cc;
+    for (int c = 0; c < cc; ++c) {
+      cpos[c] = m.pos[c];
+      cpen[c] = fmaxf(m.pen[c], p.penetration_cap);  // extraction cap (:1575-1578)
+      cfp[c] = m.fp[c];
+      cwarm[c] = 0;
+      cstick[c] = 0;
+      clam[c] = make_float4(0, 0, 0, 0);
+      ckt[c] = make_float2(0, 0);
+      canca[c] = make_float3(0, 0, 0);
+      cancb[c] = make_float3(0, 0, 0);
+    }
+    int32_t err = 0x7FFFFFFF;
+    if (warm) {
+      // find the pair's manifold of the previous substep on the dynamic body's list
+      uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb;
+      uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
+      uint32_t old_slot = BB_NONE;
+      bool swapped = false;
+      for (uint32_t e = s0; e < s1; ++e) {
+        uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
+        uint2 ob = d.m_bodies[prv][os];
+        if ((ob.x == ida && ob.y == idb) || (ob.x == idb && ob.y == ida)) {
+          old_slot = os;
+          swapped = ob.x != ida;
+          break;
+        }
+      }
+      if (old_slot != BB_NONE) {
+        // Manifold::update_from_old (extensions.slang:306-473)
+        int2 okc = d.m_keycc[prv][old_slot];
+        float4 on4 = d.m_normal[prv][old_slot];
+        float sgn = swapped ? -1.f : 1.f;
+        bool cross_key = m.key != okc.x || swapped;
+        bool go = !cross_key || dot3(n, f3(on4) * sgn) > 0.7f;
+        if (go) {
+          const int occ = okc.y;
+          uint32_t used_old = 0, matched_new = 0;
+          const uint32_t ob = old_slot * BB_MAX_CONTACTS;
+          if (!cross_key) {
+            for (int i = 0; i < cc; ++i) {
+              for (int j = 0; j < occ; ++j) {
+                if (used_old & (1u << j)) continue;
+                float4 op = d.c_pos[prv][ob + j];
+                uint32_t ofp = __float_as_uint(d.c_anc_a[prv][ob + j].w);
+                bool feat = fp_in_inc(ofp) == fp_in_inc(cfp[i]) && fp_out_inc(ofp) == fp_out_inc(cfp[i]);
+                float3 dp = f3(op) - cpos[i];
+                bool close = dot3(dp, dp) < 0.1f * 0.1f;
+                if (feat && close) {
+                  float4 ol = d.c_lam[prv][ob + j];
+                  float4 okt = d.c_kt[prv][ob + j];
+                  clam[i] = ol;
+                  ckt[i] = make_float2(okt.x, okt.y);
+                  cstick[i] = __float_as_uint(okt.z);
+                  if (cstick[i] != 0) {
+                    canca[i] = f3(d.c_anc_a[prv][ob + j]);
+                    cancb[i] = f3(d.c_anc_b[prv][ob + j]);
+                  }
+                  float3 d2 = cpos[i] - f3(op);
+                  if (dot3(d2, d2) < 0.01f) cpos[i] = f3(op);
+                  cwarm[i] = warm_inc(__float_as_uint(okt.w));
+                  used_old |= 1u << j;
+                  matched_new |= 1u << i;
+                  break;
+                }
+              }
+            }
+          }
+          for (int round = 0; round < cc; ++round) {
+            float best = 0.1225f;
+            int bi = -1, bj = -1;
+            for (int i = 0; i < cc; ++i) {
+              if (matched_new & (1u << i)) continue;
+              for (int j = 0; j < occ; ++j) {
+                if (used_old & (1u << j)) continue;
+                float3 dp = cpos[i] - f3(d.c_pos[prv][ob + j]);
+                float d2 = dot3(dp, dp);
+                if (d2 < best) { best = d2; bi = i; bj = j; }
+              }
+            }
+            if (bi < 0) break;
+            float4 ol = d.c_lam[prv][ob + bj];
+            float4 okt = d.c_kt[prv][ob + bj];
+            clam[bi] = make_float4(ol.x, ol.y * sgn, ol.z, ol.w);
+            ckt[bi] = make_float2(okt.x, okt.y);
+            cstick[bi] = __float_as_uint(okt.z);
+            float4 oaa = d.c_anc_a[prv][ob + bj];
+            if (cstick[bi] != 0) {
+              float3 aa = f3(oaa), ab = f3(d.c_anc_b[prv][ob + bj]);
+              canca[bi] = swapped ? ab : aa;
+              cancb[bi] = swapped ? aa : ab;
+            }
+            cfp[bi] = __float_as_uint(oaa.w);
+            cwarm[bi] = warm_inc(__float_as_uint(okt.w));
+            matched_new |= 1u << bi;
+            used_old |= 1u << bj;
+          }
+          float deep_new = 0.f, deep_old = 0.f;
+          for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, cpen[i]);
+          for (int j = 0; j < occ; ++j) deep_old = fminf(deep_old, d.c_pos[prv][ob + j].w);
+          err = int32_t(fminf(fmaxf((deep_new - deep_old) * 10000.0f, -32000.0f), 32000.0f));
+        }
+      }
+    }
+    d.m_bodies[cur][k] = make_uint2(ida, idb);
+    d.m_keycc[cur][k] = make_int2(m.key, cc);
+    d.m_normal[cur][k] = f4(n, __int_as_float(err));
+    d.m_t0[cur][k] = f4(t0, 0.f);
+    d.m_t1[cur][k] = f4(t1, 0.f);
+    d.m_anchor_a[cur][k] = make_float4(pa.x, pa.y, pa.z, 0.f);
+    d.m_anchor_b[cur][k] = make_float4(pb.x, pb.y, pb.z, 0.f);
+    const uint32_t cb = k * BB_MAX_CONTACTS;
+    for (int c = 0; c < cc; ++c) {
+      d.c_pos[cur][cb + c] = f4(cpos[c], cpen[c]);
+      d.c_lam[cur][cb + c] = clam[c];
+      d.c_kt[cur][cb + c] = make_float4(ckt[c].x, ckt[c].y, __uint_as_float(cstick[c]), __uint_as_float(cwarm[c]));
+      d.c_anc_a[cur][cb + c] = f4(canca[c], __uint_as_float(cfp[c]));
+      d.c_anc_b[cur][cb + c] = f4(cancb[c], 0.f);
+    }
+    d.hit[k] = 1;
+  }
+}
+
+// man_slot[man_index[k]] = k for every slot that collided; per-manifold statistics.
+__global__ void k_compact(const DevState d, int cur) {
+  const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x) {
+    if (!d.hit[k]) continue;
+    d.man_slot[cur][d.man_index[k]] = k;
+    int cc = d.m_keycc[cur][k].y;
+    uint32_t fresh = 0;
+    float deep = 0.f;
+    for (int c = 0; c < cc; ++c) {
+      const uint32_t ci = k * BB_MAX_CONTACTS + c;
+      if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
+      deep = fmaxf(deep, -d.c_pos[cur][ci].w);
+    }
+    atomicAdd(&d.ctr->contact_count, uint32_t(cc));
+    if (fresh) atomicAdd(&d.ctr->fresh, fresh);
+    if (deep > 0.f) atomicMax(&d.ctr->max_pen_bits, __float_as_uint(deep));
+  }
+}
+
+// per-body manifold lists: count, (scan), fill, sort
+__global__ void k_csr_count(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+    if (d.flags[b.x] & BB_BODY_DYNAMIC) atomicAdd(&d.csr_cursor[b.x], 1u);
+    if (d.flags[b.y] & BB_BODY_DYNAMIC) atomicAdd(&d.csr_cursor[b.y], 1u);
+  }
+}
+__global__ void k_csr_fill(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+    if (d.flags[b.x] & BB_BODY_DYNAMIC) d.csr_list[cur][d.csr_start[cur][b.x] + atomicAdd(&d.csr_cursor[b.x], 1u)] = m;
+    if (d.flags[b.y] & BB_BODY_DYNAMIC) d.csr_list[cur][d.csr_start[cur][b.y] + atomicAdd(&d.csr_cursor[b.y], 1u)] = m;
+  }
+}
+__global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
+  uint32_t* L = d.csr_list[cur];
+  for (uint32_t a = s0 + 1; a < s1; ++a) {
+    uint32_t v = L[a];
+    uint32_t b = a;
+    while (b > s0 && L[b - 1] > v) {
+      L[b] = L[b - 1];
+      --b;
+    }
+    L[b] = v;
+  }
+}
+
+void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
+                     int cur, bool warm) {
+  const int T = BB_THREADS;
+  int grid = sms * 8;
+  k_narrow<<<sms * 16, 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
+  // compact order: exclusive scan of the hit flags over the pair slots
+  bb_launch_scan(s, d.hit, d.man_index, &d.ctr->pair_count, d.pair_capacity, &d.ctr->manifold_count,
+                 sc.scan_status + sc.scan_tiles, sc.scan_tile_ctr + 1, d.ctr);
+  k_compact<<<grid, T, 0, s>>>(d, cur);
+  // per-body lists
+  cudaMemsetAsync(d.csr_cursor, 0, sizeof(uint32_t) * (n + 1), s);
+  k_csr_count<<<grid, T, 0, s>>>(d, cur);
+  bb_launch_scan(s, d.csr_cursor, d.csr_start[cur], nullptr, n + 1, nullptr, sc.scan_status + 2 * sc.scan_tiles,
+                 sc.scan_tile_ctr + 2, d.ctr);
+  cudaMemsetAsync(d.csr_cursor, 0, sizeof(uint32_t) * (n + 1), s);
+  k_csr_fill<<<grid, T, 0, s>>>(d, cur);
+  k_csr_sort<<<(n + T - 1) / T, T, 0, s>>>(d, cur, n);
+}

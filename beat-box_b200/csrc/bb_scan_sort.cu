@@ -1,0 +1,263 @@
+// bb_scan_sort.cu -- single-pass prefix scan and onesweep LSD radix sort.
+//
+// Replaces the reference's radix sort (histogram + scatter per 8-bit digit with a host
+// transfer between passes, src/shaders/simulation/RB_sim.slang:113-203,
+// src/shaders/simulation/LBVH.slang:34-152, RBM:1288-1295) with:
+//   * one histogram kernel that counts all digit positions in a single read of the keys,
+//   * one onesweep kernel per digit: tiles of 2048 keys rank themselves with warp-level
+//     multisplit (__match_any_sync), publish per-digit tile totals, and resolve their global
+//     offsets by decoupled look-back over the preceding tiles.
+// Both are stable, so the result equals a stable sort by key -- the reference's semantics.
+// Element counts are read from device memory so the kernels can sit in a CUDA graph.
+#include "bb_common.cuh"
+#include "bb_kernels.cuh"
+
+namespace {
+constexpr int kThreads = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kThreads * kItems;  // 2048
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1u;
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// exclusive scan of n u32 values: out[i] = sum(in[0..i)), *total = sum(in)
+__global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                   const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
+                                                   uint32_t* total, unsigned long long* status, uint32_t* tile_ctr,
+                                                   DevCounters* ctr) {
+  __shared__ uint32_t s_tile, s_excl;
+  __shared__ uint32_t s_warp[kThreads / 32];
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
+  __syncthreads();
+  const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kTile;
+  if (base >= n && !(n == 0 && tile == 0)) return;
+  uint32_t v[kItems];
+  uint32_t local = 0;
+  const uint32_t i0 = base + threadIdx.x * kItems;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    uint32_t i = i0 + k;
+    v[k] = i < n ? in[i] : 0u;
+    local += v[k];
+  }
+  // block exclusive scan of the per-thread sums
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kThreads / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kThreads / 32) s_warp[lane] = w;  // inclusive warp sums
+  }
+  __syncthreads();
+  uint32_t block_total = s_warp[kThreads / 32 - 1];
+  uint32_t excl_in_block = x - local + (warp > 0 ? s_warp[warp - 1] : 0u);
+  // decoupled look-back by thread 0
+  if (threadIdx.x == 0) {
+    volatile unsigned long long* st = status;
+    if (tile == 0) {
+      st[0] = (2ull << 32) | block_total;
+      s_excl = 0;
+    } else {
+      st[tile] = (1ull << 32) | block_total;
+      uint32_t excl = 0;
+      int32_t j = int32_t(tile) - 1;
+      uint32_t spins = 0;
+      while (j >= 0) {
+        unsigned long long w = st[j];
+        uint32_t flag = uint32_t(w >> 32);
+        if (flag == 0) {
+          if (++spins > BB_SPIN_LIMIT) {
+            raise_error(ctr, BB_ERRF_SPIN_LIMIT);
+            break;
+          }
+          continue;
+        }
+        excl += uint32_t(w);
+        if (flag == 2) break;
+        --j;
+      }
+      st[tile] = (2ull << 32) | (excl + block_total);
+      s_excl = excl;
+    }
+  }
+  __syncthreads();
+  uint32_t run = s_excl + excl_in_block;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    uint32_t i = i0 + k;
+    if (i < n) out[i] = run;
+    run += v[k];
+  }
+  // the tile holding element n-1 (or tile 0 when n == 0) publishes the total
+  if (total && threadIdx.x == 0 && (n == 0 ? tile == 0 : (n - 1) / kTile == tile)) *total = s_excl + block_total;
+}
+
+// ---------------------------------------------------------------------------------------
+// global digit histograms of `passes` 8-bit digits starting at bit shift0
+__global__ void __launch_bounds__(kThreads) k_sort_hist(const uint32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
+                                                        uint32_t* hist, int passes, int shift0) {
+  __shared__ uint32_t s_hist[4][256];
+  for (int i = threadIdx.x; i < 4 * 256; i += kThreads) (&s_hist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
+  for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+    uint32_t k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(k >> (shift0 + 8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int p = 0; p < passes; ++p) {
+    uint32_t c = s_hist[p][threadIdx.x];
+    if (c) atomicAdd(&hist[p * 256 + threadIdx.x], c);
+  }
+}
+
+// exclusive scan of each 256-bin histogram row in place into hist_scan (count rows kept)
+__global__ void k_sort_hist_scan(const uint32_t* hist, uint32_t* hist_scan, int passes) {
+  __shared__ uint32_t s[256];
+  for (int p = 0; p < passes; ++p) {
+    uint32_t v = hist[p * 256 + threadIdx.x];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+      uint32_t y = threadIdx.x >= uint32_t(o) ? s[threadIdx.x - o] : 0u;
+      __syncthreads();
+      s[threadIdx.x] += y;
+      __syncthreads();
+    }
+    hist_scan[p * 256 + threadIdx.x] = s[threadIdx.x] - v;
+    __syncthreads();
+  }
+}
+
+// one stable onesweep pass on digit (key >> shift) & 255
+__global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in,
+                                                       const uint32_t* __restrict__ vals_in,
+                                                       uint32_t* __restrict__ keys_out,
+                                                       uint32_t* __restrict__ vals_out,
+                                                       const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
+                                                       const uint32_t* __restrict__ digit_start, int shift,
+                                                       uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp_hist[kThreads / 32][256];
+  __shared__ uint32_t s_offset[256];
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
+  for (int i = threadIdx.x; i < (kThreads / 32) * 256; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kTile;
+  if (base >= n) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t key[kItems], val[kItems], rank[kItems], dig[kItems];
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    uint32_t i = base + warp * (32 * kItems) + k * 32 + lane;
+    bool ok = i < n;
+    key[k] = ok ? keys_in[i] : 0u;
+    val[k] = ok ? vals_in[i] : 0u;
+    dig[k] = ok ? ((key[k] >> shift) & 255u) : 256u;
+  }
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    uint32_t d = dig[k];
+    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    uint32_t prior = d < 256u ? s_warp_hist[warp][d] : 0u;
+    rank[k] = prior + __popc(peers & lt_mask);
+    __syncwarp();
+    if (d < 256u && lane == __ffs(peers) - 1) s_warp_hist[warp][d] = prior + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: exclusive prefix over warps, tile total
+  const uint32_t t = threadIdx.x;
+  uint32_t sum = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) {
+    uint32_t c = s_warp_hist[w][t];
+    s_warp_hist[w][t] = sum;
+    sum += c;
+  }
+  volatile uint32_t* st = status;
+  uint32_t excl = 0;
+  if (tile == 0) {
+    st[t] = kFlagPrefix | sum;
+  } else {
+    st[tile * 256 + t] = kFlagAgg | sum;
+    int32_t j = int32_t(tile) - 1;
+    uint32_t spins = 0;
+    while (j >= 0) {
+      uint32_t w = st[j * 256 + t];
+      uint32_t flag = w & ~kValMask;
+      if (flag == 0) {
+        if (++spins > BB_SPIN_LIMIT) {
+          raise_error(ctr, BB_ERRF_SPIN_LIMIT);
+          break;
+        }
+        continue;
+      }
+      excl += w & kValMask;
+      if (flag == kFlagPrefix) break;
+      --j;
+    }
+    st[tile * 256 + t] = kFlagPrefix | (excl + sum);
+  }
+  s_offset[t] = digit_start[t] + excl;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    uint32_t d = dig[k];
+    if (d < 256u) {
+      uint32_t dst = s_offset[d] + s_warp_hist[warp][d] + rank[k];
+      keys_out[dst] = key[k];
+      vals_out[dst] = val[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// host launchers
+void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint32_t n_cap,
+                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr) {
+  uint32_t tiles = (n_cap + kTile - 1) / kTile;
+  if (tiles == 0) tiles = 1;
+  k_scan<<<tiles, kThreads, 0, s>>>(in, out, n_dev, n_cap, total, status, tile_ctr, ctr);
+}
+
+uint32_t bb_scan_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
+uint32_t bb_sort_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
+
+// Sorts `passes` digits of (keys, vals) in place between buffers 0 and 1; result in buffer
+// passes % 2.  hist: 2 x 4 x 256 words (counts, exclusive starts); status: passes x tiles x
+// 256 words, zeroed; tile_ctr: passes words, zeroed.
+void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,
+                    int passes, int shift0, uint32_t* hist, uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr,
+                    int sms) {
+  uint32_t tiles = (n_cap + kTile - 1) / kTile;
+  if (tiles == 0) tiles = 1;
+  int hblocks = sms * 4;
+  k_sort_hist<<<hblocks, kThreads, 0, s>>>(keys[0], n_dev, n_cap, hist, passes, shift0);
+  k_sort_hist_scan<<<1, 256, 0, s>>>(hist, hist + 4 * 256, passes);
+  for (int p = 0; p < passes; ++p) {
+    int in = p & 1, out = in ^ 1;
+    k_onesweep<<<tiles, kThreads, 0, s>>>(keys[in], vals[in], keys[out], vals[out], n_dev, n_cap,
+                                          hist + 4 * 256 + p * 256, shift0 + 8 * p,
+                                          status + size_t(p) * tiles * 256, tile_ctr + p, ctr);
+  }
+}

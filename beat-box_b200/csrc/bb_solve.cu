@@ -1,0 +1,815 @@
+// bb_solve.cu -- PGS_SOFT and AVBD contact solvers.
+//
+// Reference: PGS_SOFT::pre_step / solve (src/shaders/simulation/solvers.slang:142-279) run
+// per colour (RB_sim.slang:1408-1578) in the order of RBM:1369-1389 (pre-step, I solve sweeps,
+// integrate positions RB_sim.slang:1287-1326, I relax sweeps), each sweep colours 0..31 then
+// the serial overflow bucket.  AVBD (src/shaders/simulation/avbd.slang): body colouring
+// (:812-981), prepare (:70-128), warm start (:390-473), support depth (:667-724), primal
+// (:478-658) with the 6x6 LDL^T of avbd_solve6 (:329-387), dual (:728-808), finalize
+// (:132-202), post-stabilisation sweeps (RBM:1400-1425).
+//
+// B200 design: each solver phase is ONE persistent cooperative kernel that walks compact
+// colour buckets and separates colours with a grid barrier, instead of the reference's
+// (2I+1) x 33 dispatches that each scan every manifold and filter by colour.  Contact rows
+// are 64-byte float4 groups per contact; body velocities and the world inverse inertia are
+// float4 loads.  The 6x6 block solve stays in registers.
+#include "bb_common.cuh"
+#include <algorithm>
+
+#include "bb_kernels.cuh"
+
+// ---------------------------------------------------------------------------------------
+// PGS_SOFT
+struct BodyVel {
+  float3 v, w;
+};
+
+__device__ __forceinline__ Sym3 load_iw(const DevState& d, uint32_t i) {
+  float4 a = d.iw[2 * i], b = d.iw[2 * i + 1];
+  return Sym3{a.x, a.y, a.z, a.w, b.x, b.y};
+}
+__device__ __forceinline__ void store_iw(const DevState& d, uint32_t i, const Sym3& s) {
+  d.iw[2 * i] = make_float4(s.xx, s.xy, s.xz, s.yy);
+  d.iw[2 * i + 1] = make_float4(s.yz, s.zz, 0.f, 0.f);
+}
+__device__ __forceinline__ bool awake(uint32_t f) { return (f & BB_BODY_DYNAMIC) && !(f & BB_BODY_SLEEPING); }
+
+// Quaternion integration (extensions.slang:148-166)
+__device__ __forceinline__ Quatf apply_angular_velocity(Quatf rot, float3 w, float dt) {
+  float angle = len3(w) * dt;
+  Quatf q;
+  if (angle > 0.0001f) {
+    float3 axis = w * (1.0f / len3(w));
+    float half = angle / 2.0f;
+    float sh, ch;
+    sincosf(half, &sh, &ch);
+    q = Quatf{axis.x * sh, axis.y * sh, axis.z * sh, ch};
+  } else {
+    float3 dr = w * dt * 0.5f;
+    q = Quatf{dr.x, dr.y, dr.z, 1.0f};
+  }
+  return q_normalize(q_mul(q, rot));
+}
+
+// PGS_SOFT::pre_step (solvers.slang:143-196)
+__device__ void pgs_pre_step(const DevState& d, const Params& p, int cur, uint32_t m, float h, float hertz) {
+  const uint32_t slot = d.man_slot[cur][m];
+  const uint2 b = d.m_bodies[cur][slot];
+  const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+  if (!awake(fa) && !awake(fb)) return;
+  const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
+  const Sym3 IA = load_iw(d, b.x), IB = load_iw(d, b.y);
+  float3 va = f3(d.vel[b.x]), wa = f3(d.omega[b.x]), vb = f3(d.vel[b.y]), wb = f3(d.omega[b.y]);
+  const float3 n = f3(d.m_normal[cur][slot]);
+  const float3 t0 = f3(d.m_t0[cur][slot]), t1 = f3(d.m_t1[cur][slot]);
+  const float3 aa = f3(d.m_anchor_a[cur][slot]), ab = f3(d.m_anchor_b[cur][slot]);
+  const int cc = d.m_keycc[cur][slot].y;
+  const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
+  const float ch = (ima == 0.f || imb == 0.f) ? 2.0f * hertz : hertz;
+  const float zeta = 10.0f;
+  const float omega = 2.0f * 3.14159265359f * ch;
+  const float c = h * omega * (2.0f * zeta + h * omega);
+  const float bf = omega / (2.0f * zeta + h * omega);
+  const float icoef = 1.0f / (1.0f + c);
+  const float mcoef = c * icoef;
+  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
+  for (int j = 0; j < cc; ++j) {
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    const float4 pp = d.c_pos[cur][ci];
+    const float3 r1 = f3(pp) - aa, r2 = f3(pp) - ab;
+    float3 rn1 = cross3(r1, n), rn2 = cross3(r2, n);
+    float kn = ima + imb + dot3(rn1, sym_mul(IA, rn1)) + dot3(rn2, sym_mul(IB, rn2));
+    float nmass = kn == 0.f ? 0.f : 1.0f / kn;
+    float tm[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      float3 t = k == 0 ? t0 : t1;
+      float3 rt1 = cross3(r1, t), rt2 = cross3(r2, t);
+      float kt = ima + imb + dot3(rt1, sym_mul(IA, rt1)) + dot3(rt2, sym_mul(IB, rt2));
+      tm[k] = kt == 0.f ? 0.f : 1.0f / kt;
+    }
+    const float pen = pp.w;
+    const float bias_value = pen > 0.f ? pen * inv_h : fmaxf(bf * pen, -4.0f);
+    d.c_r1[ci] = f4(r1, nmass);
+    d.c_r2[ci] = f4(r2, tm[0]);
+    d.c_k[ci] = make_float4(tm[1], bias_value, mcoef, icoef);
+    float4 lam = d.c_lam[cur][ci];
+    // the reference writes its mass coefficient / tangent masses into the persistent contact
+    d.c_lam[cur][ci] = make_float4(lam.x, lam.y, lam.z, mcoef);
+    float4 kt4 = d.c_kt[cur][ci];
+    d.c_kt[cur][ci] = make_float4(tm[0], tm[1], kt4.z, kt4.w);
+    if (accum) {
+      float3 P = n * lam.x;
+      if (fric) P = P + t0 * lam.y + t1 * lam.z;
+      va = va - P * ima;
+      wa = wa - sym_mul(IA, cross3(r1, P));
+      vb = vb + P * imb;
+      wb = wb + sym_mul(IB, cross3(r2, P));
+    }
+  }
+  if (fa & BB_BODY_DYNAMIC) {
+    d.vel[b.x] = f4(va, d.vel[b.x].w);
+    d.omega[b.x] = f4(wa, 0.f);
+  }
+  if (fb & BB_BODY_DYNAMIC) {
+    d.vel[b.y] = f4(vb, d.vel[b.y].w);
+    d.omega[b.y] = f4(wb, 0.f);
+  }
+}
+
+// PGS_SOFT::solve (solvers.slang:199-278)
+__device__ void pgs_solve(const DevState& d, const Params& p, int cur, uint32_t m, bool use_bias) {
+  const uint32_t slot = d.man_slot[cur][m];
+  const uint2 b = d.m_bodies[cur][slot];
+  const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+  if (!awake(fa) && !awake(fb)) return;
+  const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
+  const Sym3 IA = load_iw(d, b.x), IB = load_iw(d, b.y);
+  float4 va4 = d.vel[b.x], vb4 = d.vel[b.y];
+  float3 va = f3(va4), wa = f3(d.omega[b.x]), vb = f3(vb4), wb = f3(d.omega[b.y]);
+  const float mu = sqrtf(d.iinv[b.x].w * d.iinv[b.y].w);
+  const float3 n = f3(d.m_normal[cur][slot]);
+  const float3 t0 = f3(d.m_t0[cur][slot]), t1 = f3(d.m_t1[cur][slot]);
+  const int cc = d.m_keycc[cur][slot].y;
+  const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
+  for (int j = 0; j < cc; ++j) {
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    const float4 R1 = d.c_r1[ci], R2 = d.c_r2[ci], K = d.c_k[ci];
+    float4 lam = d.c_lam[cur][ci];
+    const float3 r1 = f3(R1), r2 = f3(R2);
+    float3 rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
+    if (fric) {
+      float imp_t[2] = {lam.y, lam.z};
+      const float tmass[2] = {R2.w, K.x};
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const float3 t = k == 0 ? t0 : t1;
+        float tv = dot3(rv, t);
+        float ti = tmass[k] * -tv;
+        float maxf = mu * lam.x;
+        if (accum) {
+          float old = imp_t[k];
+          imp_t[k] = fminf(fmaxf(old + ti, -maxf), maxf);
+          ti = imp_t[k] - old;
+        } else {
+          ti = fminf(fmaxf(ti, -maxf), maxf);
+        }
+        float3 P = t * ti;
+        va = va - P * ima;
+        wa = wa - sym_mul(IA, cross3(r1, P));
+        vb = vb + P * imb;
+        wb = wb + sym_mul(IB, cross3(r2, P));
+      }
+      lam.y = imp_t[0];
+      lam.z = imp_t[1];
+    }
+    rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
+    float vn = dot3(rv, n);
+    float bias = 0.f, ms = 1.f, is = 0.f;
+    if (K.y > 0.f) {
+      bias = K.y;
+    } else if (use_bias) {
+      bias = K.y;
+      ms = K.z;
+      is = K.w;
+    }
+    float imp = -R1.w * ms * (vn + bias) - is * lam.x;
+    if (accum) {
+      float old = lam.x;
+      lam.x = fmaxf(old + imp, 0.f);
+      imp = lam.x - old;
+    } else {
+      imp = fmaxf(imp, 0.f);
+    }
+    float3 P = n * imp;
+    va = va - P * ima;
+    wa = wa - sym_mul(IA, cross3(r1, P));
+    vb = vb + P * imb;
+    wb = wb + sym_mul(IB, cross3(r2, P));
+    d.c_lam[cur][ci] = lam;
+  }
+  if (fa & BB_BODY_DYNAMIC) {
+    d.vel[b.x] = f4(va, va4.w);
+    d.omega[b.x] = f4(wa, 0.f);
+  }
+  if (fb & BB_BODY_DYNAMIC) {
+    d.vel[b.y] = f4(vb, vb4.w);
+    d.omega[b.y] = f4(wb, 0.f);
+  }
+}
+
+// sweep over colours 0..C-1 and the overflow bucket; phase 0 pre-step, 1 solve, 2 relax
+__device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int phase, float h, float hertz) {
+  const uint32_t C = d.ctr->gc_colors;
+  const uint32_t* list = d.bucket_vals[1];
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (uint32_t c = 0; c < C; ++c) {
+    uint32_t s0 = d.bucket_start[c], s1 = d.bucket_start[c + 1];
+    if (s0 == s1) continue;
+    for (uint32_t k = s0 + tid; k < s1; k += stride) {
+      uint32_t m = list[k];
+      if (phase == 0) pgs_pre_step(d, p, cur, m, h, hertz);
+      else pgs_solve(d, p, cur, m, phase == 1);
+    }
+    grid_barrier(d.ctr);
+  }
+  uint32_t o0 = d.bucket_start[BB_MAX_COLORS], o1 = d.bucket_start[BB_MAX_COLORS + 1];
+  if (o0 != o1) {
+    if (tid == 0) {
+      for (uint32_t k = o0; k < o1; ++k) {
+        uint32_t m = list[k];
+        if (phase == 0) pgs_pre_step(d, p, cur, m, h, hertz);
+        else pgs_solve(d, p, cur, m, phase == 1);
+      }
+    }
+    grid_barrier(d.ctr);
+  }
+}
+
+__global__ void __launch_bounds__(BB_THREADS) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
+  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
+  const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
+  for (uint32_t i = tid; i < n; i += stride) store_iw(d, i, world_inv_inertia(q_from(d.rot[i]), f3(d.iinv[i]), tq));
+  grid_barrier(d.ctr);
+  pgs_sweep(d, p, cur, 0, h, hertz);
+  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, h, hertz);
+  if (p.flags & BB_SIM_ADVECTION) {
+    for (uint32_t i = tid; i < n; i += stride) {
+      if (!awake(d.flags[i])) continue;
+      float4 ps = d.pos[i];
+      float3 v = f3(d.vel[i]);
+      d.pos[i] = make_float4(ps.x + v.x * h, ps.y + v.y * h, ps.z + v.z * h, ps.w);
+      Quatf q = apply_angular_velocity(q_from(d.rot[i]), f3(d.omega[i]), h);
+      d.rot[i] = q_to4(q);
+      store_iw(d, i, world_inv_inertia(q, f3(d.iinv[i]), tq));
+    }
+    grid_barrier(d.ctr);
+  }
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, h, hertz);
+}
+
+int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_THREADS, sms); }
+
+void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
+                       int coop_blocks, int sms) {
+  (void)sms;
+  DevState dd = d;
+  Params pp = p;
+  int cc = cur;
+  uint32_t nn = n;
+  float hh = h;
+  void* args[] = {&dd, &pp, &cc, &nn, &hh};
+  bb_launch_coop((const void*)k_pgs_soft, coop_blocks, BB_THREADS, args, s);
+}
+
+// ---------------------------------------------------------------------------------------
+// AVBD
+__device__ __forceinline__ uint32_t avbd_priority(uint32_t body, uint32_t round) {
+  uint32_t x = body * 0x9e3779b9u + round * 0x85ebca6bu;
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return ((x & 0xFFFu) << 20) | (body & 0xFFFFFu);
+}
+__device__ __forceinline__ float3 small_angle_delta(Quatf now, Quatf start) {
+  Quatf dq = q_mul(now, q_conj(start));
+  float sg = dq.w < 0.f ? -1.f : 1.f;
+  return make_float3(dq.x, dq.y, dq.z) * (2.0f * sg);
+}
+__device__ __forceinline__ float3 avbd_q_rotate(Quatf q, float3 u) {
+  float3 qv = make_float3(q.x, q.y, q.z);
+  return u + 2.0f * cross3(qv, cross3(qv, u) + u * q.w);
+}
+
+// Jones-Plassmann colouring with start-of-round semantics: body_color holds
+// ((round + 1) << 8) | colour while the kernel runs, so a neighbour coloured in the current
+// round still counts as uncoloured.
+__global__ void __launch_bounds__(BB_THREADS) k_avbd_color(const DevState d, Params p, int cur, uint32_t n) {
+  DevCounters* c = d.ctr;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  uint32_t* uncol = &c->pad[2];
+  for (uint32_t i = tid; i < n; i += stride) d.body_color[i] = BB_UNCOLORED;
+  if (tid == 0) {
+    uncol[0] = 0;
+    uncol[1] = 0;
+    c->avbd_colors = 0;
+  }
+  grid_barrier(c);
+  for (uint32_t rd = 0; rd < p.avbd_color_rounds; ++rd) {
+    uint32_t left = 0;
+    for (uint32_t i = tid; i < n; i += stride) {
+      if (d.body_color[i] != BB_UNCOLORED || !(d.flags[i] & BB_BODY_DYNAMIC)) continue;
+      const uint32_t mine = avbd_priority(i, rd);
+      uint32_t used = 0;
+      bool wait = false;
+      const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
+      for (uint32_t e = s0; e < s1 && !wait; ++e) {
+        uint2 b = d.m_bodies[cur][d.man_slot[cur][d.csr_list[cur][e]]];
+        uint32_t q = b.x == i ? b.y : b.x;
+        if (q == i || !(d.flags[q] & BB_BODY_DYNAMIC)) continue;
+        uint32_t pc = *(volatile uint32_t*)&d.body_color[q];
+        bool unc = pc == BB_UNCOLORED || (pc >> 8) == rd + 1u;
+        if (unc) {
+          if (avbd_priority(q, rd) > mine) wait = true;
+        } else {
+          used |= 1u << (pc & 255u);
+        }
+      }
+      if (wait || used == 0xFFFFFFFFu) {
+        ++left;
+        continue;
+      }
+      uint32_t col = uint32_t(__ffs(~used) - 1);
+      d.body_color[i] = ((rd + 1u) << 8) | col;
+      atomicMax(&c->avbd_colors, col + 1u);
+    }
+    if (left) atomicAdd(&uncol[rd & 1], left);
+    grid_barrier(c);
+    if (*(volatile uint32_t*)&uncol[rd & 1] == 0u) break;
+    if (tid == 0) uncol[(rd + 1) & 1] = 0;
+    grid_barrier(c);
+  }
+  for (uint32_t i = tid; i < n; i += stride) {
+    uint32_t v = d.body_color[i];
+    d.body_color[i] = v == BB_UNCOLORED ? BB_UNCOLORED : (v & 255u);
+  }
+}
+
+__global__ void k_avbd_prepare(const DevState d, Params p, uint32_t n, float dt) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t f = d.flags[i];
+  if (!awake(f)) return;
+  float3 w = f3(d.omega[i]);
+  float om = len3(w);
+  if (om > 50.0f) {
+    w = w * (50.0f / om);
+    d.omega[i] = f4(w, 0.f);
+  }
+  float grav = (f & BB_BODY_GRAVITY) ? p.gravity : 0.f;
+  float4 ps = d.pos[i];
+  float3 pos = f3(ps), v = f3(d.vel[i]);
+  Quatf q = q_from(d.rot[i]);
+  d.a_pos_start[i] = f4(pos, 0.f);
+  d.a_rot_start[i] = q_to4(q);
+  d.a_pos_tilde[i] = f4(pos + v * dt + make_float3(0.f, grav, 0.f) * (dt * dt), 0.f);
+  Quatf qt = apply_angular_velocity(q, w, dt);
+  d.a_rot_tilde[i] = q_to4(qt);
+  float aw = 0.f;
+  if (fabsf(grav) > 1e-6f) {
+    float ay = (v.y - d.pvel[i].y) / dt;
+    float sg = grav > 0.f ? 1.f : -1.f;
+    aw = fminf(fmaxf(ay * sg / fabsf(grav), 0.f), 1.f);
+  }
+  d.pos[i] = f4(pos + v * dt + make_float3(0.f, grav, 0.f) * (aw * dt * dt), ps.w);
+  d.rot[i] = q_to4(qt);
+}
+
+__global__ void k_avbd_warmstart(const DevState d, Params p, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  const bool warm = p.flags & BB_SIM_WARM_STARTING;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    const uint32_t slot = d.man_slot[cur][m];
+    const uint2 b = d.m_bodies[cur][slot];
+    bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
+    float3 c1 = d1 ? f3(d.a_pos_start[b.x]) : f3(d.pos[b.x]);
+    float3 c2 = d2 ? f3(d.a_pos_start[b.y]) : f3(d.pos[b.y]);
+    Quatf q1c = q_conj(d1 ? q_from(d.a_rot_start[b.x]) : q_from(d.rot[b.x]));
+    Quatf q2c = q_conj(d2 ? q_from(d.a_rot_start[b.y]) : q_from(d.rot[b.y]));
+    const int cc = d.m_keycc[cur][slot].y;
+    uint32_t sticks = 0;
+    for (int j = 0; j < cc; ++j) {
+      const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+      float4 lam = d.c_lam[cur][ci];
+      float4 kt = d.c_kt[cur][ci];
+      uint32_t wcount = __float_as_uint(kt.w), stick = __float_as_uint(kt.z);
+      bool matched = wcount != 0u && warm;
+      if (!matched) {
+        lam = make_float4(0.f, 0.f, 0.f, p.avbd_k_min);
+        kt.x = kt.y = p.avbd_k_min;
+        stick = 0;
+      } else {
+        lam.w = fminf(fmaxf(lam.w * p.avbd_gamma, p.avbd_k_min), p.avbd_k_max);
+        lam.x = fminf(lam.x, 0.f);
+        kt.x = fminf(fmaxf(kt.x * p.avbd_gamma, p.avbd_k_min), p.avbd_k_max);
+        kt.y = fminf(fmaxf(kt.y * p.avbd_gamma, p.avbd_k_min), p.avbd_k_max);
+      }
+      bool sticking = matched && stick != 0u;
+      if (!sticking) {
+        float4 cp = d.c_pos[cur][ci];
+        float4 aa = d.c_anc_a[cur][ci];
+        d.c_anc_a[cur][ci] = f4(avbd_q_rotate(q1c, f3(cp) - c1), aa.w);
+        d.c_anc_b[cur][ci] = f4(avbd_q_rotate(q2c, f3(cp) - c2), 0.f);
+      } else {
+        ++sticks;
+      }
+      d.c_lam[cur][ci] = lam;
+      d.c_kt[cur][ci] = make_float4(kt.x, kt.y, __uint_as_float(stick), kt.w);
+    }
+    if (sticks) atomicAdd(&d.ctr->stick, sticks);
+  }
+}
+
+__global__ void k_avbd_depth_reset(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  d.a_depth[i] = awake(d.flags[i]) ? BB_NONE : 0u;
+}
+__global__ void k_avbd_depth_relax(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    const uint32_t slot = d.man_slot[cur][m];
+    if (d.m_keycc[cur][slot].y <= 0) continue;
+    const uint2 b = d.m_bodies[cur][slot];
+    uint32_t d1 = *(volatile uint32_t*)&d.a_depth[b.x], d2 = *(volatile uint32_t*)&d.a_depth[b.y];
+    if (d2 != BB_NONE && d2 + 1u < d1) atomicMin(&d.a_depth[b.x], d2 + 1u);
+    if (d1 != BB_NONE && d1 + 1u < d2) atomicMin(&d.a_depth[b.y], d1 + 1u);
+  }
+}
+
+// bucket keys of awake coloured bodies: pass 0 = colour (main sweeps),
+// pass 1 = min(depth, L-1) * 32 + colour (post-stabilisation cascade); others sort last
+__global__ void k_avbd_keys(const DevState d, Params p, uint32_t n, int post) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t col = d.body_color[i];
+  uint32_t key = 0xFFFFu;
+  if (awake(d.flags[i]) && col < BB_MAX_COLORS) {
+    if (post) {
+      uint32_t layer = min(d.a_depth[i], p.avbd_shock_layers - 1u);
+      key = layer * BB_MAX_COLORS + col;
+    } else {
+      key = col;
+    }
+  }
+  d.a_bucket_keys[0][i] = key;
+  d.a_bucket_vals[0][i] = i;
+}
+// starts[v] = first sorted position with key >= v, for v in [0, nb]
+__global__ void k_lower_bounds(const uint32_t* keys, uint32_t n, uint32_t* starts, uint32_t nb) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v > nb) return;
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (keys[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  starts[v] = lo;
+}
+
+struct AvbdCtx {
+  float dt;
+};
+
+__device__ float avbd_contact_C(const DevState& d, const Params& p, int cur, uint32_t slot, uint32_t ci, uint2 b,
+                                bool d1, bool d2, float alpha, float3 n, float3& rr1, float3& rr2) {
+  float4 cp = d.c_pos[cur][ci];
+  float3 c1 = d1 ? f3(d.a_pos_start[b.x]) : f3(d.pos[b.x]);
+  float3 c2 = d2 ? f3(d.a_pos_start[b.y]) : f3(d.pos[b.y]);
+  rr1 = f3(cp) - c1;
+  rr2 = f3(cp) - c2;
+  float C = (cp.w + p.avbd_margin) * (1.0f - alpha);
+  if (d1) {
+    float3 dp = f3(d.pos[b.x]) - c1;
+    float3 dth = small_angle_delta(q_from(d.rot[b.x]), q_from(d.a_rot_start[b.x]));
+    C -= dot3(n, dp + cross3(dth, rr1));
+  }
+  if (d2) {
+    float3 dp = f3(d.pos[b.y]) - c2;
+    float3 dth = small_angle_delta(q_from(d.rot[b.y]), q_from(d.a_rot_start[b.y]));
+    C += dot3(n, dp + cross3(dth, rr2));
+  }
+  (void)slot;
+  return C;
+}
+
+__device__ float avbd_dir_C(const DevState& d, const Params& p, int cur, uint32_t ci, uint2 b, bool d1, bool d2,
+                            float alpha, float3 dir, float3& ar1, float3& ar2, float& C0t) {
+  float3 c1 = d1 ? f3(d.a_pos_start[b.x]) : f3(d.pos[b.x]);
+  float3 c2 = d2 ? f3(d.a_pos_start[b.y]) : f3(d.pos[b.y]);
+  Quatf q1 = d1 ? q_from(d.a_rot_start[b.x]) : q_from(d.rot[b.x]);
+  Quatf q2 = d2 ? q_from(d.a_rot_start[b.y]) : q_from(d.rot[b.y]);
+  ar1 = avbd_q_rotate(q1, f3(d.c_anc_a[cur][ci]));
+  ar2 = avbd_q_rotate(q2, f3(d.c_anc_b[cur][ci]));
+  C0t = dot3(dir, (c2 + ar2) - (c1 + ar1));
+  float sg = C0t > 0.f ? 1.f : (C0t < 0.f ? -1.f : 0.f);
+  float c0e = sg * fmaxf(0.f, fabsf(C0t) - p.avbd_stick_slop);
+  float C = c0e * (1.0f - alpha);
+  if (d1) {
+    float3 dp = f3(d.pos[b.x]) - c1;
+    float3 dth = small_angle_delta(q_from(d.rot[b.x]), q_from(d.a_rot_start[b.x]));
+    C -= dot3(dir, dp + cross3(dth, ar1));
+  }
+  if (d2) {
+    float3 dp = f3(d.pos[b.y]) - c2;
+    float3 dth = small_angle_delta(q_from(d.rot[b.y]), q_from(d.a_rot_start[b.y]));
+    C += dot3(dir, dp + cross3(dth, ar2));
+  }
+  return C;
+}
+
+// entry_avbd_primal (avbd.slang:478-658): Gauss-Newton step of body i on its 6 DoF.
+__device__ void avbd_primal(const DevState& d, const Params& p, int cur, uint32_t i, float dt, float alpha) {
+  const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
+  const float inv_dt2 = dt > 0.f ? 1.0f / (dt * dt) : 0.f;
+  const float m_lin = d.vel[i].w * inv_dt2;
+  Quatf rot = q_from(d.rot[i]);
+  Sym3 wi = world_inv_inertia(rot, f3(d.iinv[i]), tq);
+  // avbd_inverse3 (avbd.slang:309-326) of the symmetric world inverse inertia
+  float3 c0 = make_float3(wi.xx, wi.xy, wi.xz), c1 = make_float3(wi.xy, wi.yy, wi.yz), c2 = make_float3(wi.xz, wi.yz, wi.zz);
+  float3 r0 = cross3(c1, c2), r1 = cross3(c2, c0), r2 = cross3(c0, c1);
+  float det = dot3(c0, r0);
+  float inv = fabsf(det) > 1e-12f ? 1.0f / det : 0.f;
+  r0 = r0 * inv;
+  r1 = r1 * inv;
+  r2 = r2 * inv;
+  float H[6][6];
+  float g[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    g[a] = 0.f;
+#pragma unroll
+    for (int bb = 0; bb < 6; ++bb) H[a][bb] = 0.f;
+  }
+  H[0][0] = H[1][1] = H[2][2] = m_lin;
+  float Iw[3][3] = {{r0.x, r0.y, r0.z}, {r1.x, r1.y, r1.z}, {r2.x, r2.y, r2.z}};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) H[3 + a][3 + bb] = Iw[a][bb] * inv_dt2;
+  float3 dpos = f3(d.pos[i]) - f3(d.a_pos_tilde[i]);
+  float3 dth = small_angle_delta(rot, q_from(d.a_rot_tilde[i]));
+  g[0] = m_lin * dpos.x;
+  g[1] = m_lin * dpos.y;
+  g[2] = m_lin * dpos.z;
+  float3 ga = make_float3(Iw[0][0] * dth.x + Iw[0][1] * dth.y + Iw[0][2] * dth.z,
+                          Iw[1][0] * dth.x + Iw[1][1] * dth.y + Iw[1][2] * dth.z,
+                          Iw[2][0] * dth.x + Iw[2][1] * dth.y + Iw[2][2] * dth.z) * inv_dt2;
+  g[3] = ga.x;
+  g[4] = ga.y;
+  g[5] = ga.z;
+  const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
+  for (uint32_t e = s0; e < s1; ++e) {
+    const uint32_t slot = d.man_slot[cur][d.csr_list[cur][e]];
+    const uint2 b = d.m_bodies[cur][slot];
+    const bool i1 = b.x == i;
+    const bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
+    const float mu = sqrtf(fmaxf(d.iinv[b.x].w, 0.f) * fmaxf(d.iinv[b.y].w, 0.f));
+    const float3 n = f3(d.m_normal[cur][slot]);
+    const float3 td[2] = {f3(d.m_t0[cur][slot]), f3(d.m_t1[cur][slot])};
+    const int cc = d.m_keycc[cur][slot].y;
+    for (int j = 0; j < cc; ++j) {
+      const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+      float3 rr1, rr2;
+      float C = avbd_contact_C(d, p, cur, slot, ci, b, d1, d2, alpha, n, rr1, rr2);
+      const float4 lam = d.c_lam[cur][ci];
+      const float4 kt = d.c_kt[cur][ci];
+      float f = fminf(lam.w * C + lam.x, 0.f);
+      float3 Jl = i1 ? -n : n;
+      float3 Ja = i1 ? -cross3(rr1, n) : cross3(rr2, n);
+      float J[6] = {Jl.x, Jl.y, Jl.z, Ja.x, Ja.y, Ja.z};
+#pragma unroll
+      for (int a = 0; a < 6; ++a) g[a] += f * J[a];
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 6; ++bb) H[a][bb] += lam.w * J[a] * J[bb];
+      const float bound = mu * fabsf(lam.x);
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        float3 ar1, ar2;
+        float C0t;
+        float Ct = avbd_dir_C(d, p, cur, ci, b, d1, d2, alpha, td[t], ar1, ar2, C0t);
+        const float ktt = t == 0 ? kt.x : kt.y;
+        const float lt = t == 0 ? lam.y : lam.z;
+        float ft = fminf(fmaxf(ktt * Ct + lt, -bound), bound);
+        float3 Jlt = i1 ? -td[t] : td[t];
+        float3 Jat = i1 ? -cross3(ar1, td[t]) : cross3(ar2, td[t]);
+        float Jt[6] = {Jlt.x, Jlt.y, Jlt.z, Jat.x, Jat.y, Jat.z};
+#pragma unroll
+        for (int a = 0; a < 6; ++a) g[a] += ft * Jt[a];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+          for (int bb = 0; bb < 6; ++bb) H[a][bb] += ktt * Jt[a] * Jt[bb];
+      }
+    }
+  }
+  // avbd_solve6: in-place LDL^T, diagonal floor 1e-8
+  float x[6], rhs[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) rhs[a] = -g[a];
+#pragma unroll
+  for (int jj = 0; jj < 6; ++jj) {
+    float dd = H[jj][jj];
+#pragma unroll
+    for (int kk = 0; kk < 6; ++kk)
+      if (kk < jj) dd -= H[jj][kk] * H[jj][kk] * H[kk][kk];
+    dd = fmaxf(dd, 1e-8f);
+    H[jj][jj] = dd;
+#pragma unroll
+    for (int ii = 0; ii < 6; ++ii) {
+      if (ii > jj) {
+        float s = H[ii][jj];
+#pragma unroll
+        for (int kk = 0; kk < 6; ++kk)
+          if (kk < jj) s -= H[ii][kk] * H[jj][kk] * H[kk][kk];
+        H[ii][jj] = s / dd;
+      }
+    }
+  }
+#pragma unroll
+  for (int ii = 0; ii < 6; ++ii) {
+    float s = rhs[ii];
+#pragma unroll
+    for (int kk = 0; kk < 6; ++kk)
+      if (kk < ii) s -= H[ii][kk] * rhs[kk];
+    rhs[ii] = s;
+  }
+#pragma unroll
+  for (int ii = 0; ii < 6; ++ii) rhs[ii] /= H[ii][ii];
+#pragma unroll
+  for (int ii = 5; ii >= 0; --ii) {
+    float s = rhs[ii];
+#pragma unroll
+    for (int kk = 0; kk < 6; ++kk)
+      if (kk > ii) s -= H[kk][ii] * x[kk];
+    x[ii] = s;
+  }
+  float4 ps = d.pos[i];
+  d.pos[i] = make_float4(ps.x + x[0], ps.y + x[1], ps.z + x[2], ps.w);
+  Quatf dq{x[3] * 0.5f, x[4] * 0.5f, x[5] * 0.5f, 1.0f};
+  d.rot[i] = q_to4(q_normalize(q_mul(dq, rot)));
+}
+
+// entry_avbd_dual (avbd.slang:728-808)
+__device__ void avbd_dual(const DevState& d, const Params& p, int cur, uint32_t m) {
+  const uint32_t slot = d.man_slot[cur][m];
+  const uint2 b = d.m_bodies[cur][slot];
+  const bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
+  if (!d1 && !d2) return;
+  const float mu = sqrtf(fmaxf(d.iinv[b.x].w, 0.f) * fmaxf(d.iinv[b.y].w, 0.f));
+  const float3 n = f3(d.m_normal[cur][slot]);
+  const float3 td[2] = {f3(d.m_t0[cur][slot]), f3(d.m_t1[cur][slot])};
+  const int cc = d.m_keycc[cur][slot].y;
+  for (int j = 0; j < cc; ++j) {
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    float3 rr1, rr2;
+    float C = avbd_contact_C(d, p, cur, slot, ci, b, d1, d2, 1.0f, n, rr1, rr2);
+    float4 lam = d.c_lam[cur][ci];
+    float4 kt = d.c_kt[cur][ci];
+    const float lam0 = lam.x, k = lam.w;
+    float nl = fminf(k * C + lam0, 0.f);
+    lam.x = nl;
+    if (nl < 0.f) lam.w = fminf(k + p.avbd_beta * fabsf(C), p.avbd_k_max);
+    const float bound = mu * fabsf(lam0);
+    bool stick_ok = true;
+    float drift2 = 0.f;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      float3 ar1, ar2;
+      float C0t;
+      float Ct = avbd_dir_C(d, p, cur, ci, b, d1, d2, 1.0f, td[t], ar1, ar2, C0t);
+      float lt = t == 0 ? lam.y : lam.z;
+      float ktt = t == 0 ? kt.x : kt.y;
+      float nlt = fminf(fmaxf(ktt * Ct + lt, -bound), bound);
+      if (t == 0) lam.y = nlt;
+      else lam.z = nlt;
+      if (nlt > -bound && nlt < bound) {
+        float nk = fminf(ktt + p.avbd_beta * fabsf(Ct), p.avbd_k_max);
+        if (t == 0) kt.x = nk;
+        else kt.y = nk;
+      } else {
+        stick_ok = false;
+      }
+      drift2 += C0t * C0t;
+    }
+    uint32_t stick = (stick_ok && drift2 < p.avbd_stick_thresh * p.avbd_stick_thresh) ? 1u : 0u;
+    d.c_lam[cur][ci] = lam;
+    d.c_kt[cur][ci] = make_float4(kt.x, kt.y, __uint_as_float(stick), kt.w);
+  }
+}
+
+// entry_avbd_finalize (avbd.slang:132-202)
+__device__ void avbd_finalize(const DevState& d, int cur, uint32_t i, float dt) {
+  const float inv_dt = dt > 0.f ? 1.0f / dt : 0.f;
+  float4 v4 = d.vel[i];
+  d.pvel[i] = v4;
+  float3 v = (f3(d.pos[i]) - f3(d.a_pos_start[i])) * inv_dt;
+  Quatf dq = q_mul(q_from(d.rot[i]), q_conj(q_from(d.a_rot_start[i])));
+  float sg = dq.w < 0.f ? -1.f : 1.f;
+  float3 w = make_float3(dq.x, dq.y, dq.z) * (2.0f * sg * inv_dt);
+  if (dot3(v, v) < 0.09f && dot3(w, w) < 0.16f && d.csr_start[cur][i + 1] - d.csr_start[cur][i] >= 3u) {
+    v = v * 0.9f;
+    w = w * 0.9f;
+  }
+  d.vel[i] = f4(v, v4.w);
+  d.omega[i] = f4(w, 0.f);
+}
+
+// persistent solve: main iterations (colour sweeps + dual), finalize, post-stabilisation
+__global__ void __launch_bounds__(BB_THREADS) k_avbd_solve(const DevState d, Params p, int cur, uint32_t n, float dt,
+                                                           int phase) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const uint32_t* list = d.a_bucket_vals[1];
+  if (phase == 0) {
+    const uint32_t C = d.ctr->avbd_colors;
+    const uint32_t M = d.ctr->manifold_count;
+    for (uint32_t it = 0; it < p.avbd_iterations; ++it) {
+      for (uint32_t c = 0; c < C; ++c) {
+        uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
+        if (s0 == s1) continue;
+        for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 1.0f);
+        grid_barrier(d.ctr);
+      }
+      for (uint32_t m = tid; m < M; m += stride) avbd_dual(d, p, cur, m);
+      grid_barrier(d.ctr);
+    }
+    for (uint32_t i = tid; i < n; i += stride)
+      if (awake(d.flags[i])) avbd_finalize(d, cur, i, dt);
+  } else if (phase == 1) {
+    const uint32_t nb = p.avbd_shock_layers * BB_MAX_COLORS;
+    for (uint32_t key = 0; key < nb; ++key) {
+      uint32_t s0 = d.a_bucket_start[key], s1 = d.a_bucket_start[key + 1];
+      if (s0 == s1) continue;
+      for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 0.0f);
+      grid_barrier(d.ctr);
+    }
+  } else {
+    const uint32_t C = d.ctr->avbd_colors;
+    for (uint32_t sw = 1; sw < p.avbd_post_stab_sweeps; ++sw) {
+      for (uint32_t c = 0; c < C; ++c) {
+        uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
+        if (s0 == s1) continue;
+        for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 0.0f);
+        grid_barrier(d.ctr);
+      }
+    }
+  }
+}
+
+// Scratch of the body bucket sorts (every region is zeroed once per substep and used once):
+// histogram region `region` (2048 words each), status / tile-counter slots from `slot`.
+static void avbd_buckets(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
+                         int sms, int post, int region, int slot) {
+  const int T = BB_THREADS;
+  uint32_t blocks = (n + T - 1) / T;
+  k_avbd_keys<<<blocks, T, 0, s>>>(d, p, n, post);
+  uint32_t* keys[2] = {d.a_bucket_keys[0], d.a_bucket_keys[1]};
+  uint32_t* vals[2] = {d.a_bucket_vals[0], d.a_bucket_vals[1]};
+  uint32_t* hist = sc.sort_hist + size_t(region) * 2 * 4 * 256;
+  // post keys need 9 bits; three 8-bit passes (the third sees only zero digits, so it keeps
+  // the order) leave the result in buffer 1 like the one-pass colour sort
+  bb_launch_sort(s, keys, vals, nullptr, n, post ? 3 : 1, 0, hist, sc.sort_status + size_t(slot) * sc.sort_tiles * 256,
+                 sc.sort_tile_ctr + slot, d.ctr, sms);
+  uint32_t nb = post ? p.avbd_shock_layers * BB_MAX_COLORS : BB_MAX_COLORS;
+  k_lower_bounds<<<(nb + 1 + 127) / 128, 128, 0, s>>>(d.a_bucket_keys[1], n, d.a_bucket_start, nb);
+}
+
+int bb_avbd_blocks(int sms) {
+  return std::min(bb_coop_blocks((const void*)k_avbd_color, BB_THREADS, sms),
+                  bb_coop_blocks((const void*)k_avbd_solve, BB_THREADS, sms));
+}
+
+void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,
+                   int sms, int cur, int coop_blocks) {
+  if (n == 0) return;
+  const int T = BB_THREADS;
+  uint32_t blocks = (n + T - 1) / T;
+  {
+    DevState dd = d;
+    Params pp = p;
+    int cc = cur;
+    uint32_t nn = n;
+    void* args[] = {&dd, &pp, &cc, &nn};
+    bb_launch_coop((const void*)k_avbd_color, coop_blocks, T, args, s);
+  }
+  k_avbd_prepare<<<blocks, T, 0, s>>>(d, p, n, h);
+  k_avbd_warmstart<<<sms * 8, T, 0, s>>>(d, p, cur);
+  k_avbd_depth_reset<<<blocks, T, 0, s>>>(d, n);
+  for (uint32_t k = 0; k < p.avbd_shock_layers; ++k) k_avbd_depth_relax<<<sms * 8, T, 0, s>>>(d, cur);
+  DevState dd = d;
+  Params pp = p;
+  int cc = cur;
+  uint32_t nn = n;
+  float hh = h;
+  int phase = 0;
+  void* args[] = {&dd, &pp, &cc, &nn, &hh, &phase};
+  avbd_buckets(s, d, p, n, sc, sms, 0, 2, 5);
+  bb_launch_coop((const void*)k_avbd_solve, coop_blocks, T, args, s);
+  avbd_buckets(s, d, p, n, sc, sms, 1, 3, 6);  // slots 6, 7, 8
+  int phase1 = 1;
+  void* args1[] = {&dd, &pp, &cc, &nn, &hh, &phase1};
+  bb_launch_coop((const void*)k_avbd_solve, coop_blocks, T, args1, s);
+  if (p.avbd_post_stab_sweeps > 1) {
+    avbd_buckets(s, d, p, n, sc, sms, 0, 4, 9);
+    int phase2 = 2;
+    void* args2[] = {&dd, &pp, &cc, &nn, &hh, &phase2};
+    bb_launch_coop((const void*)k_avbd_solve, coop_blocks, T, args2, s);
+  }
+}

@@ -1,0 +1,841 @@
+// bb_world.cu -- the world object behind the C ABI of include/beatbox.h.
+//
+// Replaces RigidBodyManager (src/rigid_body_manager.{hpp,cpp}): buffer allocation
+// (RBM:121-283), the per-step program (RBM:1284-1427, here the substep sequence in
+// World::substep) and the SimConfig readback (RBM:1681-1693).  Bodies are added through
+// bb_add_bodies, which restates SceneManager::load_scene's id / mass / inertia assignment
+// (src/scene_manager.hpp:850-887).
+//
+// Execution: a step of S substeps is captured once into a CUDA graph keyed by
+// (S, buffer parity, warm start, dt, parameters) and replayed; all per-substep counts stay on
+// the device.  Persistent solver kernels are launched cooperatively.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "bb_common.cuh"
+#include "bb_kernels.cuh"
+
+namespace {
+thread_local std::string g_last_error = "no error";
+bb_status fail(bb_status code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+#define CU(call)                                                                                       \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess) return fail(BB_E_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct Shape {
+  uint32_t type;
+  float half[3];
+};
+
+template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& err) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    err = e;
+    return nullptr;
+  }
+  cudaMemset(p, 0, n * sizeof(T));
+  owned.push_back(p);
+  return static_cast<T*>(p);
+}
+
+uint64_t fnv(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+  const uint8_t* b = static_cast<const uint8_t*>(data);
+  for (size_t i = 0; i < bytes; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+}  // namespace
+
+int bb_coop_blocks(const void* kernel, int threads, int sms) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  return sms * std::min(per_sm, 2);
+}
+
+cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, kernel, args);
+}
+
+__global__ void k_begin_substep(DevCounters* c) {
+  if (threadIdx.x != 0) return;
+  c->pair_count = 0;
+  c->manifold_count = 0;
+  c->contact_count = 0;
+  c->fresh = 0;
+  c->max_pen_bits = 0;
+  c->island_count = 0;
+  c->sleeping = 0;
+  c->gc_colors = 0;
+  c->gc_overflow = 0;
+  c->gc_violations = 0;
+  c->avbd_colors = 0;
+  c->avbd_violations = 0;
+  c->stick = 0;
+  c->barrier_count = 0;
+  for (int k = 0; k < 3; ++k) {
+    c->bounds_min[k] = 0xFFFFFFFFu;
+    c->bounds_max[k] = 0u;
+  }
+  for (int k = 0; k < 6; ++k) c->pad[k] = 0;
+  c->substeps += 1;
+}
+
+struct bb_world_impl {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint32_t cap_n = 0, cap_p = 0, n = 0, n_dyn = 0;
+  std::vector<Shape> shapes;
+  std::vector<float> restitution;
+  bb_solver_params params;
+  DevState d = {};
+  StepScratch sc = {};
+  std::vector<void*> owned;
+  int parity = 0;    // manifold buffer of the last committed substep
+  int last_cur = 0;  // manifold buffer the last (partial or full) substep wrote
+  bool skip_warm_once = false;
+  bool ran_any = false;
+  int coop_edge = 0, coop_pgs = 0, coop_avbd = 0;
+  size_t scratch_bytes = 0;
+  void* scratch_base = nullptr;
+  // graph cache
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+  };
+  std::map<std::tuple<uint32_t, int, int, uint32_t, uint64_t, uint32_t>, GraphEntry> graphs;
+  bool use_graphs = true;
+  uint64_t launches = 0;
+  // profiling
+  bool profiling = false;
+  std::vector<std::string> stage_names;
+  std::vector<float> stage_ms;
+
+  ~bb_world_impl() {
+    for (auto& g : graphs)
+      if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+    for (void* p : owned) cudaFree(p);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+
+  bb_status allocate() {
+    cudaError_t err = cudaSuccess;
+    const size_t N = cap_n + 1, P = cap_p;
+    const size_t C = P * BB_MAX_CONTACTS;
+    auto f4 = [&](size_t k) { return dalloc<float4>(k, owned, err); };
+    auto u32 = [&](size_t k) { return dalloc<uint32_t>(k, owned, err); };
+    d.pos = f4(N); d.rot = f4(N); d.vel = f4(N); d.omega = f4(N); d.pvel = f4(N); d.shape = f4(N); d.iinv = f4(N);
+    d.flags = u32(N); d.sleep = u32(N); d.iw = f4(2 * N);
+    for (int k = 0; k < 2; ++k) { d.keys[k] = u32(N); d.vals[k] = u32(N); }
+    d.rank = u32(N);
+    d.node_box = f4(4 * N);
+    d.child = dalloc<int2>(N, owned, err);
+    d.parent = dalloc<int32_t>(2 * N, owned, err);
+    d.range_last = dalloc<int32_t>(N, owned, err);
+    d.visit = u32(N);
+    d.pair_cnt = u32(N); d.pair_off = u32(N + 1);
+    d.pairs = dalloc<uint2>(P, owned, err);
+    for (int k = 0; k < 2; ++k) {
+      d.m_bodies[k] = dalloc<uint2>(P, owned, err);
+      d.m_keycc[k] = dalloc<int2>(P, owned, err);
+      d.m_normal[k] = f4(P); d.m_t0[k] = f4(P); d.m_t1[k] = f4(P); d.m_anchor_a[k] = f4(P); d.m_anchor_b[k] = f4(P);
+      d.man_slot[k] = u32(P);
+      d.c_pos[k] = f4(C); d.c_lam[k] = f4(C); d.c_kt[k] = f4(C); d.c_anc_a[k] = f4(C); d.c_anc_b[k] = f4(C);
+      d.csr_start[k] = u32(N + 1);
+      d.csr_list[k] = u32(2 * P);
+    }
+    d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
+    d.csr_cursor = u32(N + 1);
+    d.hit = u32(P); d.man_index = u32(P);
+    d.uf_parent = u32(N); d.is_root = u32(N); d.root_rank = u32(N); d.island = u32(N);
+    d.gc_color = u32(P); d.gc_pid = u32(P); d.gc_choice = u32(P); d.gc_mask = u32(N);
+    d.gc_owner = dalloc<unsigned long long>(N * BB_MAX_COLORS, owned, err);
+    for (int k = 0; k < 2; ++k) { d.bucket_keys[k] = u32(P); d.bucket_vals[k] = u32(P); }
+    d.bucket_start = u32(64);
+    d.body_color = u32(N); d.body_color_round = u32(N);
+    d.a_pos_start = f4(N); d.a_rot_start = f4(N); d.a_pos_tilde = f4(N); d.a_rot_tilde = f4(N);
+    d.a_depth = u32(N);
+    for (int k = 0; k < 2; ++k) { d.a_bucket_keys[k] = u32(N); d.a_bucket_vals[k] = u32(N); }
+    d.a_bucket_start = u32(64 * BB_MAX_COLORS + 2);
+    d.ctr = dalloc<DevCounters>(1, owned, err);
+    d.pair_capacity = cap_p;
+    d.body_capacity = cap_n;
+    // scratch zeroed at every substep: scan status (4 scans), sort hists / status (10 slots)
+    sc.scan_tiles = bb_scan_tiles(std::max<size_t>(P, N + 1));
+    sc.sort_tiles = bb_sort_tiles(std::max<size_t>(P, N));
+    size_t scan_words = size_t(4) * sc.scan_tiles;  // 64-bit
+    size_t sort_status_words = size_t(10) * sc.sort_tiles * 256;
+    size_t hist_words = 10 * 4 * 256;
+    scratch_bytes = scan_words * 8 + 16 * 4 + hist_words * 4 + sort_status_words * 4 + 16 * 4;
+    char* base = static_cast<char*>(static_cast<void*>(dalloc<uint8_t>(scratch_bytes + 256, owned, err)));
+    if (err != cudaSuccess) return fail(BB_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+    scratch_base = base;
+    sc.scan_status = reinterpret_cast<unsigned long long*>(base);
+    base += scan_words * 8;
+    sc.scan_tile_ctr = reinterpret_cast<uint32_t*>(base);
+    base += 16 * 4;
+    sc.sort_hist = reinterpret_cast<uint32_t*>(base);
+    base += hist_words * 4;
+    sc.sort_status = reinterpret_cast<uint32_t*>(base);
+    base += sort_status_words * 4;
+    sc.sort_tile_ctr = reinterpret_cast<uint32_t*>(base);
+    return BB_OK;
+  }
+
+  void reset_contacts() {
+    cudaMemsetAsync(d.csr_start[0], 0, sizeof(uint32_t) * (cap_n + 2), stream);
+    cudaMemsetAsync(d.csr_start[1], 0, sizeof(uint32_t) * (cap_n + 2), stream);
+    std::vector<uint32_t> ident(n);
+    for (uint32_t i = 0; i < n; ++i) ident[i] = i;
+    cudaMemcpyAsync(d.vals[0], ident.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream);
+    cudaStreamSynchronize(stream);
+  }
+
+  void invalidate_graphs() {
+    for (auto& g : graphs)
+      if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+    graphs.clear();
+  }
+
+  // one full pipeline pass (RBM:1284-1427) at h; commit = flip the manifold parity
+  void substep(float h, bool warm, uint32_t stop_stage, bool commit) {
+    const int cur = parity ^ 1;
+    k_begin_substep<<<1, 32, 0, stream>>>(d.ctr);
+    cudaMemsetAsync(scratch_base, 0, scratch_bytes, stream);
+    bb_front_end(stream, d, params, n, sc, sms, cur);
+    if (stop_stage >= 2) bb_narrow_phase(stream, d, params, n, sc, sms, cur, warm);
+    last_cur = cur;
+    if (stop_stage < 3) return;
+    bb_advect(stream, d, params, n, h, sms);
+    bb_islands(stream, d, params, n, sc, sms, cur);
+    bb_sleep(stream, d, params, n, sms, cur);
+    bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
+    if (params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(stream, d, params, n, h, cur, coop_pgs, sms);
+    else if (params.solver == BB_SOLVER_AVBD) bb_solve_avbd(stream, d, params, n, h, sc, sms, cur, coop_avbd);
+    if (commit) parity = cur;
+  }
+};
+
+using World = bb_world_impl;
+
+static World* W(void* w) { return static_cast<World*>(w); }
+
+extern "C" {
+
+const char* bb_last_error_string(void) { return g_last_error.c_str(); }
+const char* bb_version(void) { return "beatbox-b200 0.1 (sm_100a)"; }
+
+void bb_default_solver_params(bb_solver_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->solver = BB_SOLVER_AVBD;
+  p->flags = BB_SIM_DEFAULT_FLAGS;
+  p->quirks = BB_QUIRKS_REFERENCE;
+  p->iterations = 5;
+  p->relax_iterations = 5;
+  p->gc_rounds = 32;
+  p->gravity = -9.81f;
+  p->linear_damping = 0.1f;
+  p->angular_damping = 0.1f;
+  p->contact_hertz = 30.0f;
+  p->penetration_cap = -0.25f;
+  p->sleep_lin_vel2 = 0.0144f;
+  p->sleep_ang_vel2 = 0.0225f;
+  p->sleep_steps = 30;
+  p->avbd_iterations = 10;
+  p->avbd_beta = 100000.0f;
+  p->avbd_gamma = 0.99f;
+  p->avbd_k_min = 1.0f;
+  p->avbd_k_max = 1000000000.0f;
+  p->avbd_margin = 0.0005f;
+  p->avbd_stick_thresh = 0.01f;
+  p->avbd_stick_slop = 0.001f;
+  p->avbd_color_rounds = 16;
+  p->avbd_shock_layers = 12;
+  p->avbd_post_stab_sweeps = 4;
+  p->bounds_mode = BB_BOUNDS_FIXED;
+  for (int k = 0; k < 3; ++k) {
+    p->world_min[k] = -64.0f;
+    p->world_extent[k] = 128.0f;
+  }
+}
+
+bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
+  if (!desc || !out_world || desc->max_bodies == 0) return fail(BB_E_INVALID, "bb_world_create: bad arguments");
+  World* w = new World();
+  if (desc->device >= 0) {
+    cudaError_t e = cudaSetDevice(desc->device);
+    if (e != cudaSuccess) {
+      delete w;
+      return fail(BB_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+  }
+  cudaGetDevice(&w->device);
+  cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device);
+  if (desc->stream) {
+    w->stream = static_cast<cudaStream_t>(desc->stream);
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete w;
+      return fail(BB_E_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    w->own_stream = true;
+  }
+  w->cap_n = desc->max_bodies;
+  uint32_t ppb = desc->pairs_per_body ? desc->pairs_per_body : 16;
+  w->cap_p = uint32_t(std::min<uint64_t>(uint64_t(ppb) * w->cap_n + 1024, 0x3FFFFFFFull));
+  bb_default_solver_params(&w->params);
+  bb_status st = w->allocate();
+  if (st != BB_OK) {
+    delete w;
+    return st;
+  }
+  w->coop_edge = bb_edge_coloring_blocks(w->sms);
+  w->coop_pgs = bb_pgs_soft_blocks(w->sms);
+  w->coop_avbd = bb_avbd_blocks(w->sms);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    delete w;
+    return fail(BB_E_CUDA, std::string("create: ") + cudaGetErrorString(e));
+  }
+  *out_world = w;
+  return BB_OK;
+}
+
+bb_status bb_world_destroy(void* world) {
+  if (!world) return fail(BB_E_INVALID, "bb_world_destroy: null world");
+  cudaStreamSynchronize(W(world)->stream);
+  delete W(world);
+  return BB_OK;
+}
+
+void* bb_world_stream(void* world) { return world ? W(world)->stream : nullptr; }
+uint32_t bb_body_count(void* world) { return world ? W(world)->n : 0; }
+
+bb_status bb_add_box_shape(void* world, float hx, float hy, float hz, uint32_t* out_shape) {
+  if (!world || !out_shape || !(hx > 0) || !(hy > 0) || !(hz > 0)) return fail(BB_E_INVALID, "bb_add_box_shape: bad arguments");
+  W(world)->shapes.push_back(Shape{BB_SHAPE_BOX, {hx, hy, hz}});
+  *out_shape = uint32_t(W(world)->shapes.size() - 1);
+  return BB_OK;
+}
+
+bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape) {
+  if (!world || !out_shape || !(radius > 0)) return fail(BB_E_INVALID, "bb_add_sphere_shape: bad arguments");
+  W(world)->shapes.push_back(Shape{BB_SHAPE_SPHERE, {radius, radius, radius}});
+  *out_shape = uint32_t(W(world)->shapes.size() - 1);
+  return BB_OK;
+}
+
+bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id) {
+  World* w = W(world);
+  if (!w || (!bodies && count)) return fail(BB_E_INVALID, "bb_add_bodies: bad arguments");
+  if (uint64_t(w->n) + count > w->cap_n) return fail(BB_E_CAPACITY, "bb_add_bodies: max_bodies exceeded");
+  std::vector<float4> pos(count), rot(count), vel(count), om(count), shp(count), ii(count);
+  std::vector<uint32_t> fl(count), zero(count, 0);
+  uint32_t ndyn = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const bb_body_desc& b = bodies[i];
+    if (b.shape >= w->shapes.size()) return fail(BB_E_INVALID, "bb_add_bodies: unknown shape handle");
+    const Shape& s = w->shapes[b.shape];
+    bool dyn = (b.flags & BB_BODY_DYNAMIC) != 0;
+    double vol = s.type == BB_SHAPE_BOX ? 8.0 * s.half[0] * s.half[1] * s.half[2]
+                                        : 4.0 / 3.0 * 3.14159265358979 * double(s.half[0]) * s.half[0] * s.half[0];
+    float mass = b.mass > 0 ? b.mass : float(b.density * vol);
+    if (!dyn) mass = 0;
+    if (dyn && !(mass > 0)) return fail(BB_E_INVALID, "bb_add_bodies: dynamic body needs mass or density");
+    float inv_mass = dyn ? 1.0f / mass : 0.0f;
+    float inv_i[3] = {0, 0, 0};
+    if (dyn) {
+      if (b.inertia_mode == BB_INERTIA_EXPLICIT) {
+        for (int k = 0; k < 3; ++k) inv_i[k] = b.inv_inertia[k];
+      } else if (b.inertia_mode == BB_INERTIA_REFERENCE) {
+        // cuboid_get_inverse_intertia(inv_mass, min, max) (include/math.hpp:106-130)
+        float w_ = 2 * s.half[0], h_ = 2 * s.half[1], d_ = 2 * s.half[2];
+        float t = 1.0f / 12.0f;
+        inv_i[0] = 1.0f / (t * inv_mass * (h_ * h_ + d_ * d_));
+        inv_i[1] = 1.0f / (t * inv_mass * (w_ * w_ + d_ * d_));
+        inv_i[2] = 1.0f / (t * inv_mass * (w_ * w_ + h_ * h_));
+      } else if (s.type == BB_SHAPE_BOX) {
+        double w_ = 2.0 * s.half[0], h_ = 2.0 * s.half[1], d_ = 2.0 * s.half[2];
+        inv_i[0] = float(12.0 / (mass * (h_ * h_ + d_ * d_)));
+        inv_i[1] = float(12.0 / (mass * (w_ * w_ + d_ * d_)));
+        inv_i[2] = float(12.0 / (mass * (w_ * w_ + h_ * h_)));
+      } else {
+        float v = float(5.0 / (2.0 * mass * double(s.half[0]) * s.half[0]));
+        inv_i[0] = inv_i[1] = inv_i[2] = v;
+      }
+    }
+    pos[i] = make_float4(b.position[0], b.position[1], b.position[2], inv_mass);
+    rot[i] = make_float4(b.rotation[0], b.rotation[1], b.rotation[2], b.rotation[3]);
+    vel[i] = make_float4(b.velocity[0], b.velocity[1], b.velocity[2], mass);
+    om[i] = make_float4(b.omega[0], b.omega[1], b.omega[2], 0.f);
+    uint32_t tbits = s.type;
+    float tf;
+    std::memcpy(&tf, &tbits, 4);
+    shp[i] = make_float4(s.half[0], s.half[1], s.half[2], tf);
+    ii[i] = make_float4(inv_i[0], inv_i[1], inv_i[2], b.friction);
+    fl[i] = b.flags & (BB_BODY_DYNAMIC | BB_BODY_GRAVITY | BB_BODY_SLEEPING);
+    if (dyn) ++ndyn;
+    w->restitution.push_back(b.restitution);
+  }
+  const uint32_t o = w->n;
+  cudaStreamSynchronize(w->stream);
+  CU(cudaMemcpy(w->d.pos + o, pos.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.rot + o, rot.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.vel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.pvel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.omega + o, om.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.shape + o, shp.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.iinv + o, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.flags + o, fl.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.sleep + o, zero.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  w->n += count;
+  w->n_dyn += ndyn;
+  if (out_first_id) *out_first_id = o;
+  // new bodies restart the persistent state (sorted order, warm-start contacts), as a scene
+  // load does in the reference
+  w->reset_contacts();
+  w->invalidate_graphs();
+  uint32_t nn[2] = {w->n, w->n_dyn};
+  CU(cudaMemcpy(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice));
+  return BB_OK;
+}
+
+bb_status bb_set_material(void* world, uint32_t first, uint32_t count, float friction, float restitution) {
+  World* w = W(world);
+  if (!w || uint64_t(first) + count > w->n) return fail(BB_E_INVALID, "bb_set_material: bad range");
+  cudaStreamSynchronize(w->stream);
+  std::vector<float4> ii(count);
+  CU(cudaMemcpy(ii.data(), w->d.iinv + first, count * sizeof(float4), cudaMemcpyDeviceToHost));
+  for (auto& v : ii) v.w = friction;
+  CU(cudaMemcpy(w->d.iinv + first, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  for (uint32_t i = 0; i < count; ++i) w->restitution[first + i] = restitution;
+  return BB_OK;
+}
+
+bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
+  World* w = W(world);
+  if (!w || !p) return fail(BB_E_INVALID, "bb_set_solver_params: bad arguments");
+  if (p->solver == BB_SOLVER_PGS)
+    return fail(BB_E_UNSUPPORTED, "BB_SOLVER_PGS runs only on the reference's per-island path, not provided");
+  if (p->solver > BB_SOLVER_AVBD) return fail(BB_E_INVALID, "unknown solver");
+  if (p->gc_rounds > 63 || p->avbd_shock_layers == 0 || p->avbd_shock_layers > 64)
+    return fail(BB_E_INVALID, "gc_rounds <= 63 and 1 <= avbd_shock_layers <= 64 required");
+  if (!(p->flags & BB_SIM_USE_GRAPH_COLORING))
+    return fail(BB_E_UNSUPPORTED, "the per-island solve path (USE_GRAPH_COLORING off) is not provided");
+  for (int k = 0; k < 3; ++k)
+    if (!(p->world_extent[k] > 0)) return fail(BB_E_INVALID, "world_extent must be positive");
+  w->params = *p;
+  return BB_OK;
+}
+
+bb_status bb_get_solver_params(void* world, bb_solver_params* p) {
+  if (!world || !p) return fail(BB_E_INVALID, "bb_get_solver_params: bad arguments");
+  *p = W(world)->params;
+  return BB_OK;
+}
+
+bb_status bb_skip_warm_starting_once(void* world) {
+  if (!world) return fail(BB_E_INVALID, "null world");
+  W(world)->skip_warm_once = true;
+  return BB_OK;
+}
+
+bb_status bb_step(void* world, float dt, uint32_t substeps) {
+  World* w = W(world);
+  if (!w || !(dt > 0) || substeps == 0 || substeps > 64) return fail(BB_E_INVALID, "bb_step: bad arguments");
+  if (w->n == 0) return BB_OK;
+  const float h = dt / float(substeps);
+  const bool warm_first = (w->params.flags & BB_SIM_WARM_STARTING) && !w->skip_warm_once;
+  const bool warm_rest = (w->params.flags & BB_SIM_WARM_STARTING) != 0;
+  w->skip_warm_once = false;
+  uint32_t hbits;
+  std::memcpy(&hbits, &h, 4);
+  auto key = std::make_tuple(substeps, w->parity, warm_first ? 1 : 0, w->n, fnv(&w->params, sizeof(w->params)), hbits);
+  if (w->use_graphs && !w->profiling) {
+    auto it = w->graphs.find(key);
+    if (it == w->graphs.end()) {
+      int parity0 = w->parity;
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (uint32_t s = 0; s < substeps; ++s) w->substep(h, s == 0 ? warm_first : warm_rest, 99, true);
+        e = cudaStreamEndCapture(w->stream, &g);
+      }
+      w->parity = parity0;
+      World::GraphEntry ge;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&ge.exec, g, 0);
+      if (e == cudaSuccess) {
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (auto nd : nodes) {
+          cudaGraphNodeType t;
+          cudaGraphNodeGetType(nd, &t);
+          if (t == cudaGraphNodeTypeKernel) ++ge.kernels;
+        }
+      }
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        w->use_graphs = false;  // fall back to direct launches from now on
+      } else {
+        it = w->graphs.emplace(key, ge).first;
+      }
+    }
+    if (w->use_graphs) {
+      CU(cudaGraphLaunch(it->second.exec, w->stream));
+      w->launches += it->second.kernels;
+      for (uint32_t s = 0; s < substeps; ++s) w->parity ^= 1;
+      w->last_cur = w->parity;
+      w->ran_any = true;
+      return BB_OK;
+    }
+  }
+  if (w->profiling) {
+    // per-stage timing: run the substeps stage by stage with events
+    static const char* names[] = {"front_end", "narrow_phase", "advect", "islands", "sleep", "edge_coloring", "solve"};
+    if (w->stage_ms.size() != 7) {
+      w->stage_ms.assign(7, 0.f);
+      w->stage_names.assign(names, names + 7);
+    }
+    for (uint32_t s = 0; s < substeps; ++s) {
+      const int cur = w->parity ^ 1;
+      cudaEvent_t ev[8];
+      for (auto& e : ev) cudaEventCreate(&e);
+      k_begin_substep<<<1, 32, 0, w->stream>>>(w->d.ctr);
+      cudaMemsetAsync(w->scratch_base, 0, w->scratch_bytes, w->stream);
+      cudaEventRecord(ev[0], w->stream);
+      bb_front_end(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur);
+      cudaEventRecord(ev[1], w->stream);
+      bb_narrow_phase(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, s == 0 ? warm_first : warm_rest);
+      cudaEventRecord(ev[2], w->stream);
+      bb_advect(w->stream, w->d, w->params, w->n, h, w->sms);
+      cudaEventRecord(ev[3], w->stream);
+      bb_islands(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur);
+      cudaEventRecord(ev[4], w->stream);
+      bb_sleep(w->stream, w->d, w->params, w->n, w->sms, cur);
+      cudaEventRecord(ev[5], w->stream);
+      bb_edge_coloring(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_edge);
+      cudaEventRecord(ev[6], w->stream);
+      if (w->params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->coop_pgs, w->sms);
+      else bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
+      cudaEventRecord(ev[7], w->stream);
+      CU(cudaEventSynchronize(ev[7]));
+      for (int k = 0; k < 7; ++k) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        w->stage_ms[k] += ms;
+      }
+      for (auto& e : ev) cudaEventDestroy(e);
+      w->parity = cur;
+      w->last_cur = cur;
+    }
+    w->ran_any = true;
+    return BB_OK;
+  }
+  for (uint32_t s = 0; s < substeps; ++s) w->substep(h, s == 0 ? warm_first : warm_rest, 99, true);
+  w->ran_any = true;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(BB_E_CUDA, std::string("bb_step: ") + cudaGetErrorString(e));
+  return BB_OK;
+}
+
+bb_status bb_sync(void* world) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  CU(cudaStreamSynchronize(w->stream));
+  uint32_t flags = 0;
+  CU(cudaMemcpy(&flags, &w->d.ctr->error_flags, 4, cudaMemcpyDeviceToHost));
+  if (flags & (BB_ERRF_PAIR_OVERFLOW | BB_ERRF_CONTACT_OVERFLOW))
+    return fail(BB_E_CAPACITY, "pair capacity exceeded: create the world with a larger pairs_per_body");
+  if (flags & (BB_ERRF_SPIN_LIMIT | BB_ERRF_STACK_OVERFLOW | BB_ERRF_CAS_LIMIT))
+    return fail(BB_E_DEVICE_LIMIT, "a bounded device loop gave up (error flags " + std::to_string(flags) + ")");
+  return BB_OK;
+}
+
+bb_status bb_read_state(void* world, float* position, float* rotation, float* velocity, float* omega) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  CU(cudaStreamSynchronize(w->stream));
+  const uint32_t n = w->n;
+  std::vector<float4> tmp(n);
+  auto rd3 = [&](float4* src, float* dst) -> bb_status {
+    if (!dst) return BB_OK;
+    CU(cudaMemcpy(tmp.data(), src, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+      dst[3 * i] = tmp[i].x;
+      dst[3 * i + 1] = tmp[i].y;
+      dst[3 * i + 2] = tmp[i].z;
+    }
+    return BB_OK;
+  };
+  bb_status s;
+  if ((s = rd3(w->d.pos, position)) != BB_OK) return s;
+  if ((s = rd3(w->d.vel, velocity)) != BB_OK) return s;
+  if ((s = rd3(w->d.omega, omega)) != BB_OK) return s;
+  if (rotation) CU(cudaMemcpy(rotation, w->d.rot, n * sizeof(float4), cudaMemcpyDeviceToHost));
+  return BB_OK;
+}
+
+bb_status bb_write_state(void* world, const float* position, const float* rotation, const float* velocity,
+                         const float* omega) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  CU(cudaStreamSynchronize(w->stream));
+  const uint32_t n = w->n;
+  std::vector<float4> tmp(n);
+  auto wr3 = [&](float4* dstd, const float* src) -> bb_status {
+    if (!src) return BB_OK;
+    CU(cudaMemcpy(tmp.data(), dstd, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+      tmp[i].x = src[3 * i];
+      tmp[i].y = src[3 * i + 1];
+      tmp[i].z = src[3 * i + 2];
+    }
+    CU(cudaMemcpy(dstd, tmp.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    return BB_OK;
+  };
+  bb_status s;
+  if ((s = wr3(w->d.pos, position)) != BB_OK) return s;
+  if ((s = wr3(w->d.vel, velocity)) != BB_OK) return s;
+  if ((s = wr3(w->d.omega, omega)) != BB_OK) return s;
+  if (rotation) CU(cudaMemcpy(w->d.rot, rotation, n * sizeof(float4), cudaMemcpyHostToDevice));
+  return BB_OK;
+}
+
+bb_status bb_read_flags(void* world, uint32_t* flags) {
+  World* w = W(world);
+  if (!w || !flags) return fail(BB_E_INVALID, "bad arguments");
+  CU(cudaStreamSynchronize(w->stream));
+  CU(cudaMemcpy(flags, w->d.flags, w->n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return BB_OK;
+}
+
+bb_status bb_read_stats(void* world, bb_step_stats* s) {
+  World* w = W(world);
+  if (!w || !s) return fail(BB_E_INVALID, "bad arguments");
+  CU(cudaStreamSynchronize(w->stream));
+  DevCounters c;
+  CU(cudaMemcpy(&c, w->d.ctr, sizeof(c), cudaMemcpyDeviceToHost));
+  std::memset(s, 0, sizeof(*s));
+  s->body_count = w->n;
+  s->active_body_count = w->n_dyn;
+  s->pair_count = c.pair_count;
+  s->manifold_count = c.manifold_count;
+  s->contact_count = c.contact_count;
+  s->island_count = c.island_count;
+  s->graph_color_count = c.gc_colors;
+  s->graph_color_overflow = c.gc_overflow;
+  s->graph_color_violations = c.gc_violations;
+  s->avbd_color_count = c.avbd_colors;
+  s->avbd_violations = c.avbd_violations;
+  s->sleeping_count = c.sleeping;
+  s->fresh_contacts = c.fresh;
+  s->stick_count = c.stick;
+  float mp;
+  std::memcpy(&mp, &c.max_pen_bits, 4);
+  s->max_penetration = mp;
+  s->error_flags = c.error_flags;
+  s->pair_capacity = w->cap_p;
+  s->substeps_run = c.substeps;
+  return BB_OK;
+}
+
+bb_status bb_debug_collide(void* world, uint32_t stage) {
+  World* w = W(world);
+  if (!w || stage < 1 || stage > 2) return fail(BB_E_INVALID, "bb_debug_collide: stage must be 1 or 2");
+  if (w->n == 0) return BB_OK;
+  bool warm = (w->params.flags & BB_SIM_WARM_STARTING) && !w->skip_warm_once;
+  w->substep(0.0f, warm, stage, false);
+  CU(cudaStreamSynchronize(w->stream));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(BB_E_CUDA, std::string("bb_debug_collide: ") + cudaGetErrorString(e));
+  return BB_OK;
+}
+
+bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_bytes, uint64_t* count) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  CU(cudaStreamSynchronize(w->stream));
+  DevCounters c;
+  CU(cudaMemcpy(&c, w->d.ctr, sizeof(c), cudaMemcpyDeviceToHost));
+  const uint32_t n = w->n;
+  const int cur = w->last_cur;
+  const uint32_t P = std::min(c.pair_count, w->cap_p), M = c.manifold_count;
+  std::vector<uint8_t> out;
+  uint64_t cnt = 0;
+  auto grab = [&](const void* src, size_t bytes) -> bb_status {
+    out.resize(bytes);
+    if (bytes) CU(cudaMemcpy(out.data(), src, bytes, cudaMemcpyDeviceToHost));
+    return BB_OK;
+  };
+  bb_status st = BB_OK;
+  switch (which) {
+    case BB_DBG_MORTON: {
+      // keys[0] holds the sorted codes and vals[0] the ids: scatter back to id order
+      std::vector<uint32_t> keys(n), ids(n);
+      CU(cudaMemcpy(keys.data(), w->d.keys[0], n * 4, cudaMemcpyDeviceToHost));
+      CU(cudaMemcpy(ids.data(), w->d.vals[0], n * 4, cudaMemcpyDeviceToHost));
+      std::vector<uint32_t> by_id(n);
+      for (uint32_t i = 0; i < n; ++i) by_id[ids[i]] = keys[i];
+      out.resize(4 * n);
+      std::memcpy(out.data(), by_id.data(), 4 * n);
+      cnt = n;
+      break;
+    }
+    case BB_DBG_SORTED_KEYS: st = grab(w->d.keys[0], 4 * n); cnt = n; break;
+    case BB_DBG_SORTED_IDS: st = grab(w->d.vals[0], 4 * n); cnt = n; break;
+    case BB_DBG_LBVH_CHILD: st = grab(w->d.child, n > 1 ? 8 * (n - 1) : 0); cnt = n > 1 ? 2 * (n - 1) : 0; break;
+    case BB_DBG_LEAF_AABB:
+    case BB_DBG_NODE_AABB: {
+      uint32_t first = which == BB_DBG_LEAF_AABB ? n - 1 : 0, count_ = which == BB_DBG_LEAF_AABB ? n : (n > 0 ? n - 1 : 0);
+      std::vector<float4> box(2 * count_);
+      if (count_) CU(cudaMemcpy(box.data(), w->d.node_box + 2 * first, box.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+      out.resize(24 * count_);
+      float* o = reinterpret_cast<float*>(out.data());
+      for (uint32_t i = 0; i < count_; ++i) {
+        o[6 * i] = box[2 * i].x; o[6 * i + 1] = box[2 * i].y; o[6 * i + 2] = box[2 * i].z;
+        o[6 * i + 3] = box[2 * i + 1].x; o[6 * i + 4] = box[2 * i + 1].y; o[6 * i + 5] = box[2 * i + 1].z;
+      }
+      cnt = 6ull * count_;
+      break;
+    }
+    case BB_DBG_PAIRS: st = grab(w->d.pairs, 8ull * P); cnt = 2ull * P; break;
+    case BB_DBG_MANIFOLDS:
+    case BB_DBG_CONTACTS:
+    case BB_DBG_EDGE_COLORS: {
+      std::vector<uint32_t> slot(M), color(M);
+      if (M) CU(cudaMemcpy(slot.data(), w->d.man_slot[cur], 4 * M, cudaMemcpyDeviceToHost));
+      if (which == BB_DBG_EDGE_COLORS) {
+        if (M) CU(cudaMemcpy(color.data(), w->d.gc_color, 4 * M, cudaMemcpyDeviceToHost));
+        out.resize(4 * M);
+        std::memcpy(out.data(), color.data(), 4 * M);
+        cnt = M;
+        break;
+      }
+      if (which == BB_DBG_MANIFOLDS) {
+        std::vector<uint2> bodies(P);
+        std::vector<int2> kc(P);
+        std::vector<float4> nrm(P), t0(P), t1(P);
+        if (P) {
+          CU(cudaMemcpy(bodies.data(), w->d.m_bodies[cur], 8 * P, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(kc.data(), w->d.m_keycc[cur], 8 * P, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(nrm.data(), w->d.m_normal[cur], 16 * P, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(t0.data(), w->d.m_t0[cur], 16 * P, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(t1.data(), w->d.m_t1[cur], 16 * P, cudaMemcpyDeviceToHost));
+        }
+        if (M) CU(cudaMemcpy(color.data(), w->d.gc_color, 4 * M, cudaMemcpyDeviceToHost));
+        out.resize(sizeof(bb_manifold_info) * M);
+        bb_manifold_info* mi = reinterpret_cast<bb_manifold_info*>(out.data());
+        for (uint32_t m = 0; m < M; ++m) {
+          uint32_t s = slot[m];
+          mi[m].body_a = bodies[s].x;
+          mi[m].body_b = bodies[s].y;
+          mi[m].key = kc[s].x;
+          mi[m].contact_count = kc[s].y;
+          mi[m].normal[0] = nrm[s].x; mi[m].normal[1] = nrm[s].y; mi[m].normal[2] = nrm[s].z;
+          mi[m].color = color[m];
+          mi[m].tangent[0][0] = t0[s].x; mi[m].tangent[0][1] = t0[s].y; mi[m].tangent[0][2] = t0[s].z;
+          mi[m].tangent[1][0] = t1[s].x; mi[m].tangent[1][1] = t1[s].y; mi[m].tangent[1][2] = t1[s].z;
+        }
+        cnt = M;
+        break;
+      }
+      const size_t C = size_t(P) * BB_MAX_CONTACTS;
+      std::vector<float4> cp(C), cl(C), ck(C), ca(C);
+      std::vector<int2> kc(P);
+      if (P) {
+        CU(cudaMemcpy(cp.data(), w->d.c_pos[cur], 16 * C, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(cl.data(), w->d.c_lam[cur], 16 * C, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(ck.data(), w->d.c_kt[cur], 16 * C, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(ca.data(), w->d.c_anc_a[cur], 16 * C, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(kc.data(), w->d.m_keycc[cur], 8 * P, cudaMemcpyDeviceToHost));
+      }
+      out.assign(sizeof(bb_contact_info) * 8 * size_t(M), 0);
+      bb_contact_info* ci = reinterpret_cast<bb_contact_info*>(out.data());
+      for (uint32_t m = 0; m < M; ++m) {
+        uint32_t s = slot[m];
+        for (int j = 0; j < kc[s].y; ++j) {
+          size_t k = size_t(s) * BB_MAX_CONTACTS + j;
+          bb_contact_info& o = ci[8 * size_t(m) + j];
+          o.position[0] = cp[k].x; o.position[1] = cp[k].y; o.position[2] = cp[k].z;
+          o.penetration = cp[k].w;
+          o.normal_impulse = cl[k].x;
+          o.tangent_impulse[0] = cl[k].y;
+          o.tangent_impulse[1] = cl[k].z;
+          std::memcpy(&o.feature, &ca[k].w, 4);
+          std::memcpy(&o.warm_start, &ck[k].w, 4);
+          o.penalty = cl[k].w;
+        }
+      }
+      cnt = 8ull * M;
+      break;
+    }
+    case BB_DBG_BODY_COLORS: st = grab(w->d.body_color, 4 * n); cnt = n; break;
+    case BB_DBG_ISLANDS: st = grab(w->d.island, 4 * n); cnt = n; break;
+    case BB_DBG_SUPPORT_DEPTH: st = grab(w->d.a_depth, 4 * n); cnt = n; break;
+    default: return fail(BB_E_INVALID, "bb_debug_read: unknown buffer");
+  }
+  if (st != BB_OK) return st;
+  if (dst) std::memcpy(dst, out.data(), std::min<uint64_t>(out.size(), max_bytes));
+  if (count) *count = cnt;
+  return BB_OK;
+}
+
+bb_status bb_set_profiling(void* world, int32_t enabled) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  w->profiling = enabled != 0;
+  w->stage_ms.assign(w->stage_ms.size(), 0.f);
+  return BB_OK;
+}
+
+bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint32_t* n_stages, char* names,
+                              uint32_t names_bytes) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  CU(cudaStreamSynchronize(w->stream));
+  uint32_t ns = uint32_t(w->stage_ms.size());
+  if (n_stages) *n_stages = ns;
+  for (uint32_t k = 0; k < ns && k < max_stages && ms; ++k) ms[k] = w->stage_ms[k];
+  if (names && names_bytes) {
+    std::string all;
+    for (auto& s : w->stage_names) {
+      all += s;
+      all.push_back('\0');
+    }
+    std::memcpy(names, all.data(), std::min<size_t>(all.size(), names_bytes));
+  }
+  return BB_OK;
+}
+
+uint64_t bb_kernel_launch_count(void* world) { return world ? W(world)->launches : 0; }
+
+}  // extern "C"

@@ -180,7 +180,7 @@ typedef struct bb_step_stats {
 #define BB_ERRF_CONTACT_OVERFLOW (1u << 4)
 
 /* intermediate buffers readable with bb_debug_read (for parity tests and tools) */
-#define BB_DBG_MORTON 1u       /* u32 x N: Morton code of body order[i] (previous sorted order) */
+#define BB_DBG_MORTON 1u       /* u32 x N: Morton code of each body, by body id */
 #define BB_DBG_SORTED_KEYS 2u  /* u32 x N */
 #define BB_DBG_SORTED_IDS 3u   /* u32 x N: body id at each sorted position */
 #define BB_DBG_LBVH_CHILD 4u   /* i32 x 2(N-1): left, right of internal nodes; >= N-1 = leaf */

@@ -48,7 +48,12 @@ template <class R> uint64_t debug_read(World<R>& w, uint32_t which, void* dst, u
   auto put = [&](const void* src, uint64_t bytes) { std::memcpy(dst, src, std::min(bytes, max_bytes)); };
   const uint64_t N = w.n();
   switch (which) {
-    case BB_DBG_MORTON: put(w.morton.data(), 4 * w.morton.size()); return w.morton.size();
+    case BB_DBG_MORTON: {
+      std::vector<uint32_t> by_id(w.sorted_keys.size());
+      for (size_t i = 0; i < w.sorted_keys.size(); ++i) by_id[w.sorted_ids[i]] = w.sorted_keys[i];
+      put(by_id.data(), 4 * by_id.size());
+      return by_id.size();
+    }
     case BB_DBG_SORTED_KEYS: put(w.sorted_keys.data(), 4 * w.sorted_keys.size()); return w.sorted_keys.size();
     case BB_DBG_SORTED_IDS: put(w.sorted_ids.data(), 4 * w.sorted_ids.size()); return w.sorted_ids.size();
     case BB_DBG_LBVH_CHILD: put(w.child.data(), 4 * w.child.size()); return w.child.size();

@@ -983,6 +983,7 @@ template <class R> class World {
   void collide(uint32_t stage) {
     front_end();
     if (stage >= 2) narrow_phase();
+    order = sorted_ids;  // the sorted order seeds the next sort's tie order, as in a substep
   }
 
   void publish() {
