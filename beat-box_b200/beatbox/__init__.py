@@ -253,6 +253,8 @@ class World:
 
     def set_params(self, p: SolverParams | None = None, **kw):
         p = p if p is not None else self.params
+        if not isinstance(p, SolverParams):  # a layout-identical struct (e.g. the oracle's)
+            p = SolverParams.from_buffer_copy(bytes(p))
         for k, v in kw.items():
             if k in ("world_min", "world_extent"):
                 getattr(p, k)[:] = [float(x) for x in v]
@@ -343,6 +345,8 @@ def world_from_scene(scene: dict, params: SolverParams | None = None, pairs_per_
     w = World(int(scene["n"]), pairs_per_body=pairs_per_body)
     w.add_scene(scene)
     p = params if params is not None else default_params()
+    if not isinstance(p, SolverParams):
+        p = SolverParams.from_buffer_copy(bytes(p))
     if scene.get("bounds") is not None:
         p.world_min[:] = scene["bounds"][0]
         p.world_extent[:] = scene["bounds"][1]

@@ -188,25 +188,45 @@ __global__ void k_refit(const DevState d, uint32_t n) {
   }
 }
 
+// A query that visits more than BB_BP_BUDGET nodes (a huge static body: floor, walls) is
+// handed to k_broad_heavy, which splits its traversal over a block.
+#define BB_BP_BUDGET 512u
+#define BB_HEAVY_CAP 1024u
+#define BB_FRONTIER 256
+
 // Left-first traversal for sorted query i.  EMIT=false counts, EMIT=true writes.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (n < 2) {
-    if (!EMIT) d.pair_cnt[i] = 0;
+    if (!EMIT) {
+      d.pair_cnt[i] = 0;
+      d.is_heavy[i] = 0;
+    }
     return;
   }
+  if (EMIT && d.is_heavy[i]) return;
   const int N = int(n);
   const int leaf0 = N - 1;
   float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
   uint32_t out = EMIT ? d.pair_off[i] : 0u;
   const uint32_t cap = d.pair_capacity;
-  uint32_t count = 0;
+  uint32_t count = 0, visits = 0;
+  bool budgeted = !EMIT;
   int stack[BB_BVH_STACK];
   int sp = 0;
   stack[sp++] = 0;
   while (sp > 0) {
+    if (budgeted && ++visits > BB_BP_BUDGET) {
+      uint32_t slot = atomicAdd(&d.ctr->pad[4], 1u);
+      if (slot < BB_HEAVY_CAP) {
+        d.heavy_list[slot] = i;
+        d.is_heavy[i] = 1;
+        return;  // pair_cnt[i] is written by k_broad_heavy
+      }
+      budgeted = false;  // heavy list full: finish serially
+    }
     int node = stack[--sp];
     if (node >= leaf0) {
       if (EMIT) {
@@ -232,7 +252,136 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
       else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
     }
   }
-  if (!EMIT) d.pair_cnt[i] = count;
+  if (!EMIT) {
+    d.pair_cnt[i] = count;
+    d.is_heavy[i] = 0;
+  }
+}
+
+__device__ __forceinline__ bool bp_take(const DevState& d, int ch, int leaf0, int qi, float4 qmn, float4 qmx) {
+  bool take = ch >= leaf0 ? (ch - leaf0) > qi : d.range_last[ch] > qi;
+  return take && box_overlap(qmn, qmx, d.node_box[2 * ch], d.node_box[2 * ch + 1]);
+}
+
+// block-wide exclusive scan of one value per thread (blockDim.x == BB_FRONTIER)
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < BB_FRONTIER / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < BB_FRONTIER / 32) s_warp[lane] = w;
+  }
+  __syncthreads();
+  total = s_warp[BB_FRONTIER / 32 - 1];
+  uint32_t excl = x - v + (warp > 0 ? s_warp[warp - 1] : 0u);
+  __syncthreads();
+  return excl;
+}
+
+// One block per heavy query: expand an ordered frontier of overlapping subtrees level by
+// level (each level a block scan, so left-to-right order is kept), then every thread walks
+// one frontier subtree left-first.  Per-thread counts are scanned so the emitted pairs keep
+// ascending partner order.
+template <bool EMIT>
+__global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, uint32_t n) {
+  __shared__ int s_fr[2][BB_FRONTIER];
+  __shared__ uint32_t s_warp[BB_FRONTIER / 32];
+  __shared__ uint32_t s_size;
+  const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
+  if (blockIdx.x >= hc) return;
+  const uint32_t qi = d.heavy_list[blockIdx.x];
+  const int N = int(n), leaf0 = N - 1;
+  const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
+  const int t = threadIdx.x;
+  if (t == 0) {
+    s_fr[0][0] = 0;
+    s_size = 1;
+  }
+  __syncthreads();
+  int cur = 0;
+  for (int level = 0; level < 64; ++level) {
+    const uint32_t size = s_size;
+    const int node = t < int(size) ? s_fr[cur][t] : -1;
+    int kid[2] = {-1, -1};
+    uint32_t c = 0;
+    if (node >= leaf0) {
+      kid[c++] = node;  // a leaf entry stays in place
+    } else if (node >= 0) {
+      int2 ch = d.child[node];
+      if (bp_take(d, ch.x, leaf0, int(qi), qmn, qmx)) kid[c++] = ch.x;
+      if (bp_take(d, ch.y, leaf0, int(qi), qmn, qmx)) kid[c++] = ch.y;
+    }
+    uint32_t total;
+    const uint32_t pos = block_excl_scan(c, s_warp, total);
+    if (total > BB_FRONTIER || total == 0) break;  // uniform: keep the current frontier
+    bool internal = false;
+    for (uint32_t k = 0; k < c; ++k) {
+      s_fr[cur ^ 1][pos + k] = kid[k];
+      internal |= kid[k] < leaf0;
+    }
+    const int more = __syncthreads_or(internal);
+    cur ^= 1;
+    if (t == 0) s_size = total;
+    __syncthreads();
+    if (!more) break;
+  }
+  const uint32_t size = s_size;
+  // count (and emit) the leaves under frontier entry t, left-first
+  const int root = t < int(size) ? s_fr[cur][t] : -1;
+  uint32_t count = 0;
+  uint32_t out = 0;
+  for (int pass = EMIT ? 0 : 1; pass < 2; ++pass) {
+    // EMIT: pass 0 counts (for the scan), pass 1 writes
+    uint32_t cnt = 0;
+    if (root >= 0) {
+      int stack[BB_BVH_STACK];
+      int sp = 0;
+      stack[sp++] = root;
+      while (sp > 0) {
+        int node = stack[--sp];
+        if (node >= leaf0) {
+          if (EMIT && pass == 1) {
+            uint32_t k = out + cnt;
+            if (k < d.pair_capacity) d.pairs[k] = make_uint2(qi, uint32_t(node - leaf0));
+            else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+          }
+          ++cnt;
+          continue;
+        }
+        int2 c = d.child[node];
+        if (bp_take(d, c.y, leaf0, int(qi), qmn, qmx)) {
+          if (sp < BB_BVH_STACK) stack[sp++] = c.y;
+          else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+        }
+        if (bp_take(d, c.x, leaf0, int(qi), qmn, qmx)) {
+          if (sp < BB_BVH_STACK) stack[sp++] = c.x;
+          else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+        }
+      }
+    }
+    count = cnt;
+    if (EMIT && pass == 0) {
+      uint32_t total;
+      out = d.pair_off[qi] + block_excl_scan(cnt, s_warp, total);
+    }
+  }
+  if (!EMIT) {
+    uint32_t total;
+    block_excl_scan(count, s_warp, total);
+    if (t == 0) d.pair_cnt[qi] = total;
+  }
 }
 
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
@@ -249,7 +398,10 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   k_build<<<blocks, T, 0, s>>>(d, n);
   k_refit<<<blocks, T, 0, s>>>(d, n);
   uint32_t bb = (n + 127) / 128;
+  uint32_t hb = min(n, BB_HEAVY_CAP);
   k_broad<false><<<bb, 128, 0, s>>>(d, n);
+  k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n);
   bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr);
   k_broad<true><<<bb, 128, 0, s>>>(d, n);
+  k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n);
 }

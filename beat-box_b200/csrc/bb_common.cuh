@@ -74,6 +74,7 @@ struct DevState {
   int32_t* range_last;          // last leaf covered by each internal node
   uint32_t* visit;              // refit arrival counters
   uint32_t *pair_cnt, *pair_off;  // per query
+  uint32_t *is_heavy, *heavy_list;  // queries over the visit budget (block-cooperative)
   uint2* pairs;                 // (sorted a, sorted b)
   // manifolds (two buffers: [cur], [prev] chosen by parity)
   uint2* m_bodies[2];    // body ids (a, b) per slot
@@ -123,6 +124,7 @@ struct DevState {
   uint32_t* sort_status;  // tiles x 256 per pass
   uint32_t* sort_tile_ctr;
   DevCounters* ctr;
+  float* staging;  // host state exchange: rot 4N | pos 3N | vel 3N | omega 3N
   uint32_t pair_capacity;
   uint32_t body_capacity;
 };
@@ -236,28 +238,34 @@ __device__ __forceinline__ float ord2f(uint32_t v) {
 // Sense by generation counter; the spin is bounded: on timeout the block raises
 // BB_ERRF_SPIN_LIMIT and every later barrier returns at once (results are then invalid and
 // the host reports BB_E_DEVICE_LIMIT).
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ __forceinline__ void grid_barrier(DevCounters* c) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile uint32_t* gen = &c->barrier_gen;
-    uint32_t g = *gen;
-    __threadfence();
+    uint32_t g = ld_acquire_gpu(&c->barrier_gen);
+    fence_acq_rel_gpu();  // publish this block's writes (cumulative over the CTA barrier)
     uint32_t arrived = atomicAdd(&c->barrier_count, 1u);
     if (arrived == gridDim.x - 1) {
       c->barrier_count = 0;
-      __threadfence();
+      fence_acq_rel_gpu();
       atomicAdd(&c->barrier_gen, 1u);
     } else {
       uint32_t spins = 0;
-      while (*gen == g) {
-        if (++spins > BB_SPIN_LIMIT || (*(volatile uint32_t*)&c->error_flags & BB_ERRF_SPIN_LIMIT)) {
+      while (ld_acquire_gpu(&c->barrier_gen) == g) {
+        if (++spins > BB_SPIN_LIMIT) {
           atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
           break;
         }
-        __nanosleep(32);
+        if ((spins & 1023u) == 0u && (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT)) break;
       }
     }
-    __threadfence();
+    fence_acq_rel_gpu();
   }
   __syncthreads();
 }
@@ -267,3 +275,5 @@ typedef bb_solver_params Params;
 
 // ---- host-side launch helpers (defined in bb_world.cu) ----------------------------------
 #define BB_THREADS 256
+// persistent cooperative kernels: one 512-thread block per SM (fewer barrier participants)
+#define BB_COOP_THREADS 512

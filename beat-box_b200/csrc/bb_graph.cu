@@ -209,7 +209,7 @@ __device__ __forceinline__ uint32_t gc_priority(uint32_t pid, uint32_t round) {
 //           (gc_priority, :130-138) into owner[body][colour];
 //   commit: a manifold that won on both bodies takes the colour (:179-212).
 // Finally writes the (colour, manifold) keys of the bucket sort.
-__global__ void __launch_bounds__(BB_THREADS) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
+__global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
   DevCounters* c = d.ctr;
   const uint32_t M = c->manifold_count;
   const uint32_t epoch = c->gc_epoch;
@@ -284,7 +284,7 @@ __global__ void k_bucket_starts(const uint32_t* hist_scan, const uint32_t* n_ptr
   if (t == nb) starts[t] = *n_ptr;
 }
 
-int bb_edge_coloring_blocks(int sms) { return bb_coop_blocks((const void*)k_edge_color, BB_THREADS, sms); }
+int bb_edge_coloring_blocks(int sms) { return bb_coop_blocks((const void*)k_edge_color, BB_COOP_THREADS, sms); }
 
 void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
                       int sms, int cur, int coop_blocks) {
@@ -293,7 +293,7 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
   uint32_t nn = n;
   DevState dd = d;
   void* args[] = {&dd, &pp, &cc, &nn};
-  bb_launch_coop((const void*)k_edge_color, coop_blocks, BB_THREADS, args, s);
+  bb_launch_coop((const void*)k_edge_color, coop_blocks, BB_COOP_THREADS, args, s);
   // stable bucket sort of manifold ids by colour (one 8-bit digit)
   uint32_t* keys[2] = {d.bucket_keys[0], d.bucket_keys[1]};
   uint32_t* vals[2] = {d.bucket_vals[0], d.bucket_vals[1]};

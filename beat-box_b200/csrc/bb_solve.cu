@@ -226,7 +226,7 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int phase
   }
 }
 
-__global__ void __launch_bounds__(BB_THREADS) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
+__global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
   const float inv_h = h > 0.f ? 1.0f / h : 0.f;
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(BB_THREADS) k_pgs_soft(const DevState d, Param
   for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, h, hertz);
 }
 
-int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_THREADS, sms); }
+int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_COOP_THREADS, sms); }
 
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                        int coop_blocks, int sms) {
@@ -261,7 +261,7 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
-  bb_launch_coop((const void*)k_pgs_soft, coop_blocks, BB_THREADS, args, s);
+  bb_launch_coop((const void*)k_pgs_soft, coop_blocks, BB_COOP_THREADS, args, s);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -288,7 +288,7 @@ __device__ __forceinline__ float3 avbd_q_rotate(Quatf q, float3 u) {
 // Jones-Plassmann colouring with start-of-round semantics: body_color holds
 // ((round + 1) << 8) | colour while the kernel runs, so a neighbour coloured in the current
 // round still counts as uncoloured.
-__global__ void __launch_bounds__(BB_THREADS) k_avbd_color(const DevState d, Params p, int cur, uint32_t n) {
+__global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevState d, Params p, int cur, uint32_t n) {
   DevCounters* c = d.ctr;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* uncol = &c->pad[2];
@@ -713,7 +713,7 @@ __device__ void avbd_finalize(const DevState& d, int cur, uint32_t i, float dt) 
 }
 
 // persistent solve: main iterations (colour sweeps + dual), finalize, post-stabilisation
-__global__ void __launch_bounds__(BB_THREADS) k_avbd_solve(const DevState d, Params p, int cur, uint32_t n, float dt,
+__global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevState d, Params p, int cur, uint32_t n, float dt,
                                                            int phase) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const uint32_t* list = d.a_bucket_vals[1];
@@ -772,8 +772,8 @@ static void avbd_buckets(cudaStream_t s, const DevState& d, const Params& p, uin
 }
 
 int bb_avbd_blocks(int sms) {
-  return std::min(bb_coop_blocks((const void*)k_avbd_color, BB_THREADS, sms),
-                  bb_coop_blocks((const void*)k_avbd_solve, BB_THREADS, sms));
+  return std::min(bb_coop_blocks((const void*)k_avbd_color, BB_COOP_THREADS, sms),
+                  bb_coop_blocks((const void*)k_avbd_solve, BB_COOP_THREADS, sms));
 }
 
 void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,
@@ -787,7 +787,7 @@ void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t 
     int cc = cur;
     uint32_t nn = n;
     void* args[] = {&dd, &pp, &cc, &nn};
-    bb_launch_coop((const void*)k_avbd_color, coop_blocks, T, args, s);
+    bb_launch_coop((const void*)k_avbd_color, coop_blocks, BB_COOP_THREADS, args, s);
   }
   k_avbd_prepare<<<blocks, T, 0, s>>>(d, p, n, h);
   k_avbd_warmstart<<<sms * 8, T, 0, s>>>(d, p, cur);
@@ -801,15 +801,15 @@ void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t 
   int phase = 0;
   void* args[] = {&dd, &pp, &cc, &nn, &hh, &phase};
   avbd_buckets(s, d, p, n, sc, sms, 0, 2, 5);
-  bb_launch_coop((const void*)k_avbd_solve, coop_blocks, T, args, s);
+  bb_launch_coop((const void*)k_avbd_solve, coop_blocks, BB_COOP_THREADS, args, s);
   avbd_buckets(s, d, p, n, sc, sms, 1, 3, 6);  // slots 6, 7, 8
   int phase1 = 1;
   void* args1[] = {&dd, &pp, &cc, &nn, &hh, &phase1};
-  bb_launch_coop((const void*)k_avbd_solve, coop_blocks, T, args1, s);
+  bb_launch_coop((const void*)k_avbd_solve, coop_blocks, BB_COOP_THREADS, args1, s);
   if (p.avbd_post_stab_sweeps > 1) {
     avbd_buckets(s, d, p, n, sc, sms, 0, 4, 9);
     int phase2 = 2;
     void* args2[] = {&dd, &pp, &cc, &nn, &hh, &phase2};
-    bb_launch_coop((const void*)k_avbd_solve, coop_blocks, T, args2, s);
+    bb_launch_coop((const void*)k_avbd_solve, coop_blocks, BB_COOP_THREADS, args2, s);
   }
 }

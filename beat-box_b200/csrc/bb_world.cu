@@ -62,7 +62,7 @@ int bb_coop_blocks(const void* kernel, int threads, int sms) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
   if (per_sm < 1) per_sm = 1;
-  return sms * std::min(per_sm, 2);
+  return sms * std::min(per_sm, 1);
 }
 
 cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s) {
@@ -77,6 +77,34 @@ cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** a
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelExC(&cfg, kernel, args);
+}
+
+// state exchange with the host through one staging buffer: rot 4N | pos 3N | vel 3N | omega 3N
+// (rotations first: float4 accesses need the 16-byte-aligned base)
+__global__ void k_pack_state(const DevState d, uint32_t n, float* st) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = d.pos[i], q = d.rot[i], v = d.vel[i], w = d.omega[i];
+  float* Q = st;
+  float* P = st + 4 * size_t(n);
+  float* V = st + 7 * size_t(n);
+  float* W = st + 10 * size_t(n);
+  P[3 * i] = p.x; P[3 * i + 1] = p.y; P[3 * i + 2] = p.z;
+  reinterpret_cast<float4*>(Q)[i] = q;
+  V[3 * i] = v.x; V[3 * i + 1] = v.y; V[3 * i + 2] = v.z;
+  W[3 * i] = w.x; W[3 * i + 1] = w.y; W[3 * i + 2] = w.z;
+}
+__global__ void k_unpack_state(const DevState d, uint32_t n, const float* st, uint32_t mask) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* Q = st;
+  const float* P = st + 4 * size_t(n);
+  const float* V = st + 7 * size_t(n);
+  const float* W = st + 10 * size_t(n);
+  if (mask & 1) d.pos[i] = make_float4(P[3 * i], P[3 * i + 1], P[3 * i + 2], d.pos[i].w);
+  if (mask & 2) d.rot[i] = reinterpret_cast<const float4*>(Q)[i];
+  if (mask & 4) d.vel[i] = make_float4(V[3 * i], V[3 * i + 1], V[3 * i + 2], d.vel[i].w);
+  if (mask & 8) d.omega[i] = make_float4(W[3 * i], W[3 * i + 1], W[3 * i + 2], 0.f);
 }
 
 __global__ void k_begin_substep(DevCounters* c) {
@@ -158,6 +186,7 @@ struct bb_world_impl {
     d.range_last = dalloc<int32_t>(N, owned, err);
     d.visit = u32(N);
     d.pair_cnt = u32(N); d.pair_off = u32(N + 1);
+    d.is_heavy = u32(N); d.heavy_list = u32(1024);
     d.pairs = dalloc<uint2>(P, owned, err);
     for (int k = 0; k < 2; ++k) {
       d.m_bodies[k] = dalloc<uint2>(P, owned, err);
@@ -182,6 +211,7 @@ struct bb_world_impl {
     for (int k = 0; k < 2; ++k) { d.a_bucket_keys[k] = u32(N); d.a_bucket_vals[k] = u32(N); }
     d.a_bucket_start = u32(64 * BB_MAX_COLORS + 2);
     d.ctr = dalloc<DevCounters>(1, owned, err);
+    d.staging = dalloc<float>(13 * N + 4, owned, err);
     d.pair_capacity = cap_p;
     d.body_capacity = cap_n;
     // scratch zeroed at every substep: scan status (4 scans), sort hists / status (10 slots)
@@ -580,27 +610,20 @@ bb_status bb_sync(void* world) {
   return BB_OK;
 }
 
+// Device pack + one async copy per array on the world's stream (host memory should be pinned
+// for full PCIe / C2C bandwidth; pageable memory works, slower).
 bb_status bb_read_state(void* world, float* position, float* rotation, float* velocity, float* omega) {
   World* w = W(world);
   if (!w) return fail(BB_E_INVALID, "null world");
-  CU(cudaStreamSynchronize(w->stream));
   const uint32_t n = w->n;
-  std::vector<float4> tmp(n);
-  auto rd3 = [&](float4* src, float* dst) -> bb_status {
-    if (!dst) return BB_OK;
-    CU(cudaMemcpy(tmp.data(), src, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-      dst[3 * i] = tmp[i].x;
-      dst[3 * i + 1] = tmp[i].y;
-      dst[3 * i + 2] = tmp[i].z;
-    }
-    return BB_OK;
-  };
-  bb_status s;
-  if ((s = rd3(w->d.pos, position)) != BB_OK) return s;
-  if ((s = rd3(w->d.vel, velocity)) != BB_OK) return s;
-  if ((s = rd3(w->d.omega, omega)) != BB_OK) return s;
-  if (rotation) CU(cudaMemcpy(rotation, w->d.rot, n * sizeof(float4), cudaMemcpyDeviceToHost));
+  if (n == 0) return BB_OK;
+  float* st = w->d.staging;
+  k_pack_state<<<(n + 255) / 256, 256, 0, w->stream>>>(w->d, n, st);
+  if (position) CU(cudaMemcpyAsync(position, st + 4ull * n, 12ull * n, cudaMemcpyDeviceToHost, w->stream));
+  if (rotation) CU(cudaMemcpyAsync(rotation, st, 16ull * n, cudaMemcpyDeviceToHost, w->stream));
+  if (velocity) CU(cudaMemcpyAsync(velocity, st + 7ull * n, 12ull * n, cudaMemcpyDeviceToHost, w->stream));
+  if (omega) CU(cudaMemcpyAsync(omega, st + 10ull * n, 12ull * n, cudaMemcpyDeviceToHost, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
 
@@ -608,25 +631,17 @@ bb_status bb_write_state(void* world, const float* position, const float* rotati
                          const float* omega) {
   World* w = W(world);
   if (!w) return fail(BB_E_INVALID, "null world");
-  CU(cudaStreamSynchronize(w->stream));
   const uint32_t n = w->n;
-  std::vector<float4> tmp(n);
-  auto wr3 = [&](float4* dstd, const float* src) -> bb_status {
-    if (!src) return BB_OK;
-    CU(cudaMemcpy(tmp.data(), dstd, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-      tmp[i].x = src[3 * i];
-      tmp[i].y = src[3 * i + 1];
-      tmp[i].z = src[3 * i + 2];
-    }
-    CU(cudaMemcpy(dstd, tmp.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    return BB_OK;
-  };
-  bb_status s;
-  if ((s = wr3(w->d.pos, position)) != BB_OK) return s;
-  if ((s = wr3(w->d.vel, velocity)) != BB_OK) return s;
-  if ((s = wr3(w->d.omega, omega)) != BB_OK) return s;
-  if (rotation) CU(cudaMemcpy(w->d.rot, rotation, n * sizeof(float4), cudaMemcpyHostToDevice));
+  if (n == 0) return BB_OK;
+  float* st = w->d.staging;
+  uint32_t mask = 0;
+  if (position) { CU(cudaMemcpyAsync(st + 4ull * n, position, 12ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 1; }
+  if (rotation) { CU(cudaMemcpyAsync(st, rotation, 16ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 2; }
+  if (velocity) { CU(cudaMemcpyAsync(st + 7ull * n, velocity, 12ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 4; }
+  if (omega) { CU(cudaMemcpyAsync(st + 10ull * n, omega, 12ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 8; }
+  k_unpack_state<<<(n + 255) / 256, 256, 0, w->stream>>>(w->d, n, st, mask);
+  // the caller may reuse its buffers as soon as this returns
+  CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
 

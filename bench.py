@@ -1,0 +1,340 @@
+"""Benchmark of the B200 rigid-body step (body-steps/s), one JSON line on rank 0.
+
+Workload (default): 100,000 mixed bodies (60% boxes with half extents U[0.2, 0.8], 40% spheres
+with lognormal radii) dropped from a 60x60x200 m column into a 5-wall container; FP32 state,
+dt = 1/60 s, 4 substeps, PGS_SOFT 10 solve + 10 relax iterations, physical arithmetic (the
+reference's gravity / SAT-frame / inertia quirks off).  Synthetic seeded scene (seed 0): no
+public dataset exists for this workload.  A "step" is one bb_step(dt, 4) of the whole world.
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the world's
+stream; L2 is flushed (256 MB write) before every timed step, outside the events.  Multi-GPU
+(torchrun): a single world does not shard, so every rank steps its own replica; the time is
+the max over ranks and value = all ranks' body-steps / that time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solver pgs|avbd]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "beat-box_b200"))
+
+import numpy as np  # noqa: E402
+
+from beatbox import scenes  # noqa: E402
+
+DT = 1.0 / 60.0
+SUBSTEPS = 4
+N_BODIES = 100_000
+L2_BYTES = 126 * 1024 * 1024
+
+
+def workload(args):
+    sc = scenes.mixed_column(n_bodies=args.bodies, seed=0)
+    name = (f"mixed_column_{args.bodies // 1000}k: {args.bodies} bodies (60% boxes / 40% spheres) in a "
+            f"60x60x200 m column, 5-wall container, dt=1/60, {SUBSTEPS} substeps, ")
+    if args.solver == "pgs":
+        name += "PGS_SOFT 10 iterations"
+    else:
+        name += "AVBD 4 iterations (beta=10)"
+    return sc, name
+
+
+def solver_fields(args) -> dict:
+    if args.solver == "pgs":
+        return dict(solver=1, iterations=10, relax_iterations=10, quirks=0)
+    return dict(solver=2, avbd_iterations=4, avbd_beta=10.0, quirks=0)
+
+
+def sample_clocks(dev: int):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                                 "-i", str(dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except (OSError, FileNotFoundError):
+        return None
+
+
+def finish_clocks(proc) -> dict:
+    if proc is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    proc.terminate()
+    try:
+        out, _ = proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        out, _ = proc.communicate()
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.strip().splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx.append(float(f[2]))
+        except ValueError:
+            continue
+        for k, nm in enumerate(names):
+            if f[5 + k].lower().startswith("active"):
+                reasons.add(nm)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks() -> dict:
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+def solver_bytes(st: dict, n: int, args) -> float:
+    """Algorithmic HBM bytes of one solver launch (one substep), SoA float4 model: body
+    state 64 B, props 48 B, contact row 64 B, manifold header 32 B."""
+    M, K = st["manifold_count"], st["contact_count"]
+    if args.solver == "pgs":
+        it = 10
+        pre = 64 * K + 4 * 32 * M + 2 * 48 * M
+        sweep = 64 * K + 128 * M
+        return pre + 2 * it * sweep + 128 * n
+    it = 4
+    sweeps = it + 12 + 3  # main iterations + post-stabilisation (cascade + plain sweeps)
+    return 2 * 192 * n + sweeps * (64 * n + 2 * (32 * M + 64 * K)) + it * (32 * M + 76 * K)
+
+
+def run_reference(args, rank: int, world_size: int):
+    """Times the reference's CPU implementation of the step: the oracle (a restatement of the
+    reference's Slang passes; the reference itself needs Vulkan/Daxa and cannot run here) in
+    FP32 on all host cores."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    pyoracle.build()
+    sc, name = workload(args)
+    threads = os.cpu_count() or 1
+    p = pyoracle.default_params()
+    for k, v in solver_fields(args).items():
+        setattr(p, k, v)
+    p.world_min[:] = sc["bounds"][0]
+    p.world_extent[:] = sc["bounds"][1]
+    o = pyoracle.Oracle(sc, double=False, threads=threads, params=p)
+    budget = args.ref_budget_s
+    t0 = time.time()
+    warm = 0
+    for _ in range(args.warmup):
+        o.step(DT, SUBSTEPS)
+        warm += 1
+        if time.time() - t0 > budget / 3:
+            break
+    t1 = time.time()
+    steps = 0
+    while steps < args.steps:
+        o.step(DT, SUBSTEPS)
+        steps += 1
+        if time.time() - t1 > budget:
+            break
+    el = time.time() - t1
+    v = sc["n"] * steps / el
+    sample = (f"{steps} of {args.steps} timed steps (after {warm} warm-up steps) of the full {sc['n']}-body world, "
+              f"FP32 oracle, {threads} threads")
+    line = {"impl": "reference", "metric": "body-steps/s", "value": v, "unit": "body-steps/s", "n_gpus": world_size,
+            "steps": steps, "warmup": warm, "ms_per_step": 1000 * el / max(steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+            "config": {"workload": name, "bodies": sc["n"], "substeps": SUBSTEPS, "dt": DT},
+            "cpu_baseline": {"value": v, "unit": "body-steps/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world_size: int, local_rank: int):
+    import torch
+
+    import beatbox as bb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    sc, name = workload(args)
+    fields = solver_fields(args)
+
+    def make_world():
+        w = bb.World(sc["n"], pairs_per_body=16, device=local_rank)
+        w.add_scene(sc)
+        p = bb.default_params()
+        p.world_min[:] = sc["bounds"][0]
+        p.world_extent[:] = sc["bounds"][1]
+        w.set_params(p, **fields)
+        return w
+
+    w = make_world()
+    stream = torch.cuda.ExternalStream(w.stream)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    for _ in range(args.warmup):
+        w.step(DT, SUBSTEPS)
+    w.sync()
+    warm_state = w.read_state()
+    warm_flags = w.read_flags()
+    n = w.n
+    launches0 = w.launches()
+    clocks = sample_clocks(local_rank)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        evs[k][0].record(stream)
+        w.step(DT, SUBSTEPS)
+        evs[k][1].record(stream)
+    w.sync()
+    torch.cuda.synchronize()
+    clk = finish_clocks(clocks)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    launches = w.launches() - launches0
+    stats = w.stats()
+    t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world_size * n * args.steps / (max_ms / 1000.0)
+
+    # end to end through the public API with pinned host buffers: upload state, step, read back
+    w2 = make_world()
+    for _ in range(args.warmup):
+        w2.step(DT, SUBSTEPS)
+    w2.sync()
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32).pin_memory().numpy()  # noqa: E731
+    host = {k: pin(v.shape) for k, v in warm_state.items()}
+    for k in host:
+        host[k][...] = w2.read_state()[k]
+    e2e_steps = max(1, min(args.steps, 60))
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        w2.write_state(host["pos"], host["quat"], host["vel"], host["omega"])
+        w2.step(DT, SUBSTEPS)
+        w2.read_state(host)
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world_size * n * e2e_steps / float(e2e_t.item())
+    io_bytes = n * (12 + 16 + 12 + 12)
+    w2.close()
+
+    # roofline of the dominant stage: per-stage CUDA-event times over a profiled pass
+    prof_steps = max(1, min(args.steps, 20))
+    w.set_profiling(True)
+    for _ in range(prof_steps):
+        w.step(DT, SUBSTEPS)
+    w.sync()
+    stages = w.stage_times()
+    w.set_profiling(False)
+    st_now = w.stats()
+    launches_per_stage = prof_steps * SUBSTEPS
+    dom = max(stages, key=stages.get) if stages else "solve"
+    pk = peaks()
+    peak_gbs = float(pk.get("hbm_gbs", 6650.0))
+    solve_ms = stages.get("solve", 0.0) / launches_per_stage
+    sb = solver_bytes(st_now, n, args)
+    achieved = sb / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else 0.0
+    roof = {"kernel": "solve (k_pgs_soft)" if args.solver == "pgs" else "solve (AVBD kernels)", "bound": "hbm",
+            "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
+            "peak_source": "measured" if not pk.get("fallback") else "fallback", "traffic": None,
+            "algorithmic_bytes_per_launch": sb, "ms_per_launch": solve_ms,
+            "stage_ms_per_substep": {k: v / launches_per_stage for k, v in stages.items()}, "dominant_stage": dom}
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, sc, warm_state, warm_flags)
+    if rank == 0:
+        line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world_size,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded scene, seed 0)",
+                "config": {"workload": name, "bodies": n, "substeps": SUBSTEPS, "dt": DT,
+                           "parallelism": f"replicas x{world_size}", "l2": "flushed before every timed step",
+                           "timed_steps": f"steps {args.warmup}..{args.warmup + args.steps - 1} from the initial column"},
+                "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": io_bytes,
+                        "d2h_bytes_per_step": io_bytes, "steps": e2e_steps,
+                        "what": "bb_write_state + bb_step + bb_read_state with pinned host buffers"},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "step_stats": stats}
+        print(json.dumps(line), flush=True)
+    w.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args, sc, state, flags) -> dict:
+    """Oracle (FP32, all host threads) continued from the GPU's post-warm-up state for about
+    15 s of CPU time: a bounded sample of the timed workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    pyoracle.build()
+    sc2 = dict(sc)
+    sc2["pos"], sc2["quat"], sc2["vel"], sc2["omega"] = state["pos"], state["quat"], state["vel"], state["omega"]
+    sc2["flags"] = flags
+    threads = os.cpu_count() or 1
+    p = pyoracle.default_params()
+    for k, v in solver_fields(args).items():
+        setattr(p, k, v)
+    p.world_min[:] = sc["bounds"][0]
+    p.world_extent[:] = sc["bounds"][1]
+    o = pyoracle.Oracle(sc2, double=False, threads=threads, params=p)
+    t0 = time.time()
+    steps = 0
+    while steps < args.steps and (steps == 0 or time.time() - t0 < 15.0):
+        o.step(DT, SUBSTEPS)
+        steps += 1
+    el = time.time() - t0
+    return {"value": sc["n"] * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of the {sc['n']}-body world continued from the GPU state after "
+                      f"{args.warmup} warm-up steps (cold warm start), FP32 oracle"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solver", default="pgs", choices=["pgs", "avbd"])
+    ap.add_argument("--bodies", type=int, default=N_BODIES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world_size)
+    else:
+        run_ours(args, rank, world_size, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,273 @@
+"""GPU parity tests: the CUDA library (through its C ABI) against the oracle.
+
+Tolerances:
+  * bit-exact: Morton codes, sorted keys and ids, LBVH topology, leaf and node boxes, pairs,
+    manifold identities (bodies, SAT key, contact count), edge and body colourings;
+  * narrow-phase geometry (FP32 kernel vs FP64 oracle): normals 1e-5, contact points and
+    depths 1e-4 m;
+  * one step from a contact-rich state: relative error <= 1e-4 of the world's scale for
+    positions and 2e-4 (abs floor 2e-4 m/s) for velocities;
+  * 300 steps: aggregate statistics within bands (see test_300_step_statistics).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import beatbox as bb
+from beatbox import scenes
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+
+
+def oracle_for(po, sc, params):
+    return po.Oracle(sc, params=params)
+
+
+def params_for(po, sc, **kw):
+    p = po.default_params()
+    for k, v in kw.items():
+        setattr(p, k, v)
+    if sc.get("bounds") is not None:
+        p.world_min[:] = sc["bounds"][0]
+        p.world_extent[:] = sc["bounds"][1]
+    return p
+
+
+def oread(o, code, dtype):
+    cnt, buf = o.debug_read(code)
+    itemsize = np.dtype(dtype).itemsize
+    if code == 8:
+        return buf[: cnt * bb.MANIFOLD_DTYPE.itemsize].view(bb.MANIFOLD_DTYPE)
+    if code == 9:
+        return buf[: cnt * bb.CONTACT_DTYPE.itemsize].view(bb.CONTACT_DTYPE)
+    return buf[: cnt * itemsize].view(dtype)
+
+
+def dup_scene():
+    """Bodies sharing Morton cells (duplicate codes exercise the index tie-break)."""
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50])
+    pos = np.array([[0.01 * (k % 3), 0.6 + 0.02 * (k // 3), 0.0] for k in range(12)])
+    sb.add(pos, np.tile([0, 0, 0, 1.0], (12, 1)), np.full((12, 3), 0.05), 0,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1.0)
+    return sb.build()
+
+
+def single_scene(n):
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50])
+    if n > 1:
+        sb.add([[0, 0.45, 0]] * (n - 1), [[0, 0, 0, 1]] * (n - 1), [[0.5] * 3] * (n - 1), 0,
+               scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1.0)
+    return sb.build()
+
+
+FRONT_SCENES = {
+    "box_grid_1000": lambda: scenes.box_grid(),
+    "mixed_2000": lambda: scenes.mixed_column(n_bodies=2000, seed=1),
+    "pyramids_2x1000": lambda: scenes.pyramids(n_pyramids=2, boxes_per=1000),
+    "duplicates": dup_scene,
+    "one_body": lambda: single_scene(1),
+    "two_bodies": lambda: single_scene(2),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FRONT_SCENES))
+@pytest.mark.parametrize("bounds", [bb.BOUNDS_FIXED, bb.BOUNDS_AUTO])
+def test_front_end_bit_exact(oracle_lib, name, bounds):
+    sc = FRONT_SCENES[name]()
+    p = params_for(oracle_lib, sc, bounds_mode=bounds)
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    w.debug_collide(1)
+    o.collide(1)
+    assert np.array_equal(w.debug_read("morton"), oread(o, 1, np.uint32))
+    assert np.array_equal(w.debug_read("sorted_keys"), oread(o, 2, np.uint32))
+    assert np.array_equal(w.debug_read("sorted_ids"), oread(o, 3, np.uint32))
+    assert np.array_equal(w.debug_read("lbvh_child"), oread(o, 4, np.int32))
+    assert np.array_equal(w.debug_read("leaf_aabb"), oread(o, 5, np.float32))
+    assert np.array_equal(w.debug_read("node_aabb"), oread(o, 6, np.float32))
+    assert np.array_equal(w.debug_read("pairs"), oread(o, 7, np.uint32))
+    # a second collide starts from the new sorted order on both sides
+    w.debug_collide(1)
+    o.collide(1)
+    assert np.array_equal(w.debug_read("sorted_ids"), oread(o, 3, np.uint32))
+    assert np.array_equal(w.debug_read("pairs"), oread(o, 7, np.uint32))
+
+
+@pytest.mark.parametrize("name,quirks", [("box_grid_1000", 0), ("box_grid_1000", 7), ("mixed_2000", 0),
+                                         ("mixed_2000", 7), ("pyramids_2x1000", 0)])
+def test_narrow_phase_matches_oracle(oracle_lib, name, quirks):
+    sc = FRONT_SCENES[name]()
+    if name == "mixed_2000":  # drop the column onto itself so boxes and spheres touch
+        sc = dict(sc)
+        pos = sc["pos"].copy()
+        pos[5:, 1] = 0.5 + (pos[5:, 1] - 1.0) * 0.02
+        sc["pos"] = pos
+    p = params_for(oracle_lib, sc, quirks=quirks)
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    w.debug_collide(2)
+    o.collide(2)
+    gm, rm = w.debug_read("manifolds"), oread(o, 8, None)
+    assert len(gm) == len(rm) and len(gm) > 0
+    assert np.array_equal(gm["body_a"], rm["body_a"]) and np.array_equal(gm["body_b"], rm["body_b"])
+    assert np.array_equal(gm["key"], rm["key"])
+    assert np.array_equal(gm["contact_count"], rm["contact_count"])
+    assert np.abs(gm["normal"] - rm["normal"]).max() < 1e-5
+    gc, rc = w.debug_read("contacts"), oread(o, 9, None)
+    mask = np.repeat(np.arange(8)[None, :], len(gm), 0) < gm["contact_count"][:, None]
+    mask = mask.ravel()
+    assert np.abs(gc["position"][mask] - rc["position"][mask]).max() < 1e-4
+    assert np.abs(gc["penetration"][mask] - rc["penetration"][mask]).max() < 1e-4
+    assert np.array_equal(gc["feature"][mask], rc["feature"][mask])
+
+
+def settled(po, sc, solver, quirks, steps):
+    """A contact-rich state: the FP64 oracle run for `steps` steps, as float32 arrays."""
+    p = params_for(po, sc, solver=solver, quirks=quirks, iterations=8, relax_iterations=8, avbd_iterations=4)
+    o = oracle_for(po, sc, p)
+    for _ in range(steps):
+        o.step(DT, 4)
+    st = o.state()
+    sc2 = dict(sc)
+    sc2["pos"], sc2["quat"] = st["pos"].astype(np.float32), st["quat"].astype(np.float32)
+    sc2["vel"], sc2["omega"] = st["vel"].astype(np.float32), st["omega"].astype(np.float32)
+    sc2["flags"] = sc["flags"].copy()  # everyone awake
+    return sc2, p
+
+
+@pytest.mark.parametrize("solver", [bb.SOLVER_PGS_SOFT, bb.SOLVER_AVBD])
+@pytest.mark.parametrize("quirks", [bb.QUIRKS_PHYSICAL, bb.QUIRKS_REFERENCE])
+def test_one_step_state_within_tolerance(oracle_lib, solver, quirks):
+    base = scenes.box_grid(n_side=6, layers=4, density=5.0 if solver == bb.SOLVER_AVBD else 1000.0)
+    sc, p = settled(oracle_lib, base, solver, quirks, 45)
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    o.step(DT, 4)
+    w.step(DT, 4)
+    w.sync()
+    assert w.stats()["manifold_count"] > 50
+    # identical colourings of the last substep (same manifolds -> same colours)
+    assert np.array_equal(w.debug_read("edge_colors"), oread(o, 10, np.uint32))
+    g, r = w.read_state(), o.state()
+    dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+    pos_scale = np.abs(r["pos"][dyn]).max()
+    perr = np.abs(g["pos"][dyn] - r["pos"][dyn]).max() / pos_scale
+    vscale = max(np.abs(r["vel"][dyn]).max(), 1.0)
+    verr = np.abs(g["vel"][dyn] - r["vel"][dyn]).max()
+    assert perr < 1e-4, perr
+    assert verr < 2e-4 * vscale, verr
+
+
+def energy_stats(state, sc):
+    dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+    m = sc["mass"][dyn].astype(np.float64)
+    v = state["vel"][dyn].astype(np.float64)
+    y = state["pos"][dyn, 1].astype(np.float64)
+    return dict(ke=float(0.5 * (m * (v ** 2).sum(1)).sum()), pe=float((m * 9.81 * y).sum()),
+                mom=float(np.abs((m[:, None] * v).sum(0)).sum()), ymean=float(y.mean()))
+
+
+def test_300_step_statistics(oracle_lib):
+    """1,000-box grid, PGS 8 iterations, 4 substeps, 300 steps: GPU (FP32) vs oracle (FP64).
+    The trajectories are chaotic, so aggregate quantities are compared:
+    mean height within 2 cm, potential energy within 1%, max penetration within 1 cm,
+    sleeping fraction within 0.1, final kinetic energy both small."""
+    sc = scenes.box_grid()
+    p = params_for(oracle_lib, sc, solver=1, quirks=0, iterations=8, relax_iterations=8)
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    for _ in range(300):
+        w.step(DT, 4)
+        o.step(DT, 4)
+    w.sync()
+    g, r = energy_stats(w.read_state(), sc), energy_stats(o.state(), sc)
+    gs, rs = w.stats(), o.stats()
+    assert abs(g["ymean"] - r["ymean"]) < 0.02
+    assert abs(g["pe"] - r["pe"]) / r["pe"] < 0.01
+    assert abs(gs["max_penetration"] - rs["max_penetration"]) < 0.01
+    assert abs(gs["sleeping_count"] - rs["sleeping_count"]) <= 100
+    assert g["ke"] < 1e-2 * r["pe"] and r["ke"] < 1e-2 * r["pe"]
+    assert gs["error_flags"] == 0 and gs["graph_color_overflow"] == 0
+
+
+def test_steps_are_deterministic(oracle_lib):
+    sc = scenes.mixed_column(n_bodies=3000, seed=2)
+    outs = []
+    for _ in range(2):
+        p = params_for(oracle_lib, sc, solver=1, quirks=0)
+        w = bb.world_from_scene(sc, params=p)
+        for _ in range(40):
+            w.step(DT, 4)
+        outs.append(w.read_state())
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k])
+
+
+def test_avbd_colouring_valid_and_matches_oracle(oracle_lib):
+    sc = scenes.box_grid(n_side=6, layers=4, density=5.0)
+    sc2, p = settled(oracle_lib, sc, bb.SOLVER_AVBD, 0, 30)
+    w = bb.world_from_scene(sc2, params=p)
+    o = oracle_for(oracle_lib, sc2, p)
+    w.step(DT, 1)
+    o.step(DT, 1)
+    gcol, rcol = w.debug_read("body_colors"), oread(o, 11, np.uint32)
+    assert np.array_equal(gcol, rcol)
+    st = w.stats()
+    assert st["avbd_color_count"] == o.stats()["avbd_color_count"] > 0
+    # validity: no manifold joins two dynamic bodies of the same colour
+    man = w.debug_read("manifolds")
+    dyn = (sc2["flags"] & bb.BODY_DYNAMIC) != 0
+    both = dyn[man["body_a"]] & dyn[man["body_b"]]
+    assert np.all(gcol[man["body_a"][both]] != gcol[man["body_b"][both]])
+
+
+def test_capacity_overflow_is_reported(oracle_lib):
+    sc = scenes.pyramids(n_pyramids=1, boxes_per=1000)
+    w = bb.World(sc["n"], pairs_per_body=1)
+    w.add_scene(sc)
+    w.step(DT, 1)
+    with pytest.raises(bb.BeatboxError) as e:
+        w.sync()
+    assert e.value.code == bb.E_CAPACITY
+
+
+def test_invalid_arguments_are_rejected():
+    w = bb.World(8)
+    with pytest.raises(bb.BeatboxError) as e:
+        w.step(0.0, 1)
+    assert e.value.code == bb.E_INVALID
+    with pytest.raises(bb.BeatboxError) as e:
+        w.set_params(solver=bb.SOLVER_PGS)
+    assert e.value.code == bb.E_UNSUPPORTED
+    with pytest.raises(bb.BeatboxError):
+        w.add_box_shape(-1.0, 1.0, 1.0)
+
+
+def test_rigid_body_manager_facade():
+    m = bb.RigidBodyManager(max_bodies=64)
+    assert m.create("test", iterations=6)
+    sc = scenes.box_grid(n_side=3, layers=2)
+    m.world.add_scene(sc)
+    m.set_sim_type(bb.SOLVER_PGS_SOFT)
+    m.clear_sim_flags(bb.SIM_SLEEPING_ENABLED)
+    assert not (m.get_sim_flags() & bb.SIM_SLEEPING_ENABLED)
+    for _ in range(10):
+        assert m.simulate()
+    assert m.read_back_sim_config()
+    cfg = m.get_sim_config_reference()
+    assert cfg["body_count"] == sc["n"] and cfg["error_flags"] == 0
+
+
+def test_state_roundtrip_and_write():
+    sc = scenes.box_grid(n_side=3, layers=2)
+    w = bb.world_from_scene(sc)
+    st = w.read_state()
+    assert np.allclose(st["pos"], sc["pos"]) and np.allclose(st["quat"], sc["quat"])
+    newpos = st["pos"] + 1.0
+    w.write_state(pos=newpos)
+    assert np.allclose(w.read_state()["pos"], newpos)
