@@ -34,6 +34,7 @@ SIM_DEFAULT_FLAGS = SIM_ACCUM_IMPULSE | SIM_FRICTION | SIM_WARM_STARTING | SIM_A
 QUIRK_GRAVITY_IMPULSE, QUIRK_SAT_FRAME, QUIRK_INERTIA_TRANSPOSE = 1, 2, 4
 QUIRKS_REFERENCE, QUIRKS_PHYSICAL = 7, 0
 BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
+SCHEDULE_DATAFLOW, SCHEDULE_COLOUR_BARRIER = 0, 1
 DBG = dict(morton=1, sorted_keys=2, sorted_ids=3, lbvh_child=4, leaf_aabb=5, node_aabb=6, pairs=7,
            manifolds=8, contacts=9, edge_colors=10, body_colors=11, islands=12, support_depth=13)
 
@@ -55,7 +56,7 @@ class SolverParams(ctypes.Structure):
         ("avbd_k_min", ctypes.c_float), ("avbd_k_max", ctypes.c_float), ("avbd_margin", ctypes.c_float),
         ("avbd_stick_thresh", ctypes.c_float), ("avbd_stick_slop", ctypes.c_float),
         ("avbd_color_rounds", ctypes.c_uint32), ("avbd_shock_layers", ctypes.c_uint32),
-        ("avbd_post_stab_sweeps", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
+        ("avbd_post_stab_sweeps", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
         ("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3),
     ]
 
@@ -70,6 +71,10 @@ class BodyDesc(ctypes.Structure):
                 ("omega", ctypes.c_float * 3), ("shape", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("mass", ctypes.c_float), ("density", ctypes.c_float), ("friction", ctypes.c_float),
                 ("restitution", ctypes.c_float), ("inertia_mode", ctypes.c_uint32), ("inv_inertia", ctypes.c_float * 3)]
+
+
+class BatchWorldDesc(ctypes.Structure):
+    _fields_ = [("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3)]
 
 
 class StepStats(ctypes.Structure):
@@ -100,6 +105,9 @@ _SIG = {
     "bb_add_box_shape": (ctypes.c_int32, [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.POINTER(_U32)]),
     "bb_add_sphere_shape": (ctypes.c_int32, [_P, ctypes.c_float, ctypes.POINTER(_U32)]),
     "bb_add_bodies": (ctypes.c_int32, [_P, ctypes.POINTER(BodyDesc), _U32, ctypes.POINTER(_U32)]),
+    "bb_add_world": (ctypes.c_int32, [_P, ctypes.POINTER(BatchWorldDesc), ctypes.POINTER(BodyDesc), _U32,
+                                      ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "bb_world_count": (_U32, [_P]),
     "bb_set_material": (ctypes.c_int32, [_P, _U32, _U32, ctypes.c_float, ctypes.c_float]),
     "bb_set_solver_params": (ctypes.c_int32, [_P, ctypes.POINTER(SolverParams)]),
     "bb_get_solver_params": (ctypes.c_int32, [_P, ctypes.POINTER(SolverParams)]),
@@ -117,6 +125,7 @@ _SIG = {
     "bb_set_profiling": (ctypes.c_int32, [_P, ctypes.c_int32]),
     "bb_read_stage_times": (ctypes.c_int32, [_P, _P, _U32, ctypes.POINTER(_U32), _P, _U32]),
     "bb_kernel_launch_count": (ctypes.c_uint64, [_P]),
+    "bb_radix_sort_pairs": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_last_error_string": (ctypes.c_char_p, []),
     "bb_version": (ctypes.c_char_p, []),
 }
@@ -212,9 +221,7 @@ class World:
             self._shape_cache[key] = h
         return h
 
-    def add_scene(self, scene: dict, inertia_mode: int = INERTIA_EXPLICIT) -> int:
-        """Add every body of a beatbox.scenes dict; masses and inverse inertias are taken from
-        the scene (the oracle gets the same arrays)."""
+    def _scene_descs(self, scene: dict, inertia_mode: int):
         n = int(scene["n"])
         descs = (BodyDesc * n)()
         for i in range(n):
@@ -231,9 +238,30 @@ class World:
             d.restitution = float(scene["restitution"][i])
             d.inertia_mode = inertia_mode
             d.inv_inertia[:] = scene["inv_inertia"][i].tolist()
+        return descs, n
+
+    def add_scene(self, scene: dict, inertia_mode: int = INERTIA_EXPLICIT) -> int:
+        """Add every body of a beatbox.scenes dict; masses and inverse inertias are taken from
+        the scene (the oracle gets the same arrays)."""
+        descs, n = self._scene_descs(scene, inertia_mode)
         first = _U32()
         _check(self.L.bb_add_bodies(self.h, descs, n, ctypes.byref(first)))
         return first.value
+
+    def add_world(self, scene: dict, world_min, world_extent, inertia_mode: int = INERTIA_EXPLICIT):
+        """Append a scene as an independent world of a batch (bodies of different worlds
+        never collide).  Returns (world index, first body id)."""
+        descs, n = self._scene_descs(scene, inertia_mode)
+        wd = BatchWorldDesc()
+        wd.world_min[:] = [float(v) for v in world_min]
+        wd.world_extent[:] = [float(v) for v in world_extent]
+        wi, first = _U32(), _U32()
+        _check(self.L.bb_add_world(self.h, ctypes.byref(wd), descs, n, ctypes.byref(wi), ctypes.byref(first)))
+        return wi.value, first.value
+
+    @property
+    def n_worlds(self) -> int:
+        return int(self.L.bb_world_count(self.h))
 
     def add_bodies(self, descs) -> int:
         arr = (BodyDesc * len(descs))(*descs)

@@ -107,14 +107,36 @@ __global__ void k_morton(const DevState d, uint32_t n, Params p) {
     }
   }
   uint32_t id = d.vals[0][i];
+  if (d.n_worlds >= 1) {  // batched worlds: each world normalises by its own box
+    uint32_t w = d.world_of[id];
+    float4 a = d.world_bounds[2 * w], b = d.world_bounds[2 * w + 1];
+    wmin[0] = a.x; wmin[1] = a.y; wmin[2] = a.z;
+    wext[0] = b.x; wext[1] = b.y; wext[2] = b.z;
+  }
   d.keys[0][i] = morton_code(f3(d.pos[id]), wmin, wext);
 }
 
-__device__ __forceinline__ int clz_delta(const uint32_t* codes, int n, int i, uint32_t ci, int j) {
+// world of every sorted position (batched worlds only)
+__global__ void k_sorted_world(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d.sworld[i] = d.world_of[d.vals[0][i]];
+}
+
+// LBVH::delta (LBVH.slang:158-170) on the key (world, code): with batched worlds the world id
+// forms the 32 high bits, so a pair of different worlds shares fewer prefix bits than any pair
+// inside one world, and each world's range is one subtree.  sw == nullptr: single world.
+__device__ __forceinline__ int clz_delta(const uint32_t* codes, const uint32_t* sw, int n, int i, uint32_t ci,
+                                         uint32_t wi, int j) {
   if (j < 0 || j > n - 1) return -1;
+  int base = 0;
+  if (sw) {
+    uint32_t wj = sw[j];
+    if (wi != wj) return __clz(wi ^ wj);
+    base = 32;
+  }
   uint32_t cj = codes[j];
-  if (ci == cj) return 32 + __clz(uint32_t(i ^ j));
-  return __clz(ci ^ cj);
+  if (ci == cj) return base + 32 + __clz(uint32_t(i ^ j));
+  return base + __clz(ci ^ cj);
 }
 
 // leaves in sorted order + Karras internal nodes (LBVH.slang:155-221, RB_sim.slang:206-278)
@@ -122,6 +144,7 @@ __global__ void k_build(const DevState d, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t* codes = d.keys[0];
+  const uint32_t* sw = d.n_worlds > 1 ? d.sworld : nullptr;
   uint32_t id = d.vals[0][i];
   d.rank[id] = i;
   float4 mn, mx;
@@ -133,24 +156,26 @@ __global__ void k_build(const DevState d, uint32_t n) {
   if (i + 1 >= n) return;
   const int N = int(n), idx = int(i);
   uint32_t code = codes[idx];
-  int dl = clz_delta(codes, N, idx, code, idx - 1);
-  int dr = clz_delta(codes, N, idx, code, idx + 1);
+  uint32_t wi = sw ? sw[idx] : 0u;
+  int dl = clz_delta(codes, sw, N, idx, code, wi, idx - 1);
+  int dr = clz_delta(codes, sw, N, idx, code, wi, idx + 1);
   int dir = dr >= dl ? 1 : -1;
   int dmin = min(dl, dr);
   int lmax = 2;
-  while (clz_delta(codes, N, idx, code, idx + lmax * dir) > dmin) lmax <<= 1;
+  while (clz_delta(codes, sw, N, idx, code, wi, idx + lmax * dir) > dmin) lmax <<= 1;
   int l = 0;
   for (int t = lmax >> 1; t > 0; t >>= 1)
-    if (clz_delta(codes, N, idx, code, idx + (l + t) * dir) > dmin) l += t;
+    if (clz_delta(codes, sw, N, idx, code, wi, idx + (l + t) * dir) > dmin) l += t;
   int j = idx + l * dir;
   int first = min(idx, j), last = max(idx, j);
   uint32_t fc = codes[first];
-  int common = clz_delta(codes, N, first, fc, last);
+  uint32_t fw = sw ? sw[first] : 0u;
+  int common = clz_delta(codes, sw, N, first, fc, fw, last);
   int split = first, step = last - first;
   do {
     step = (step + 1) >> 1;
     int ns = split + step;
-    if (ns < last && clz_delta(codes, N, first, fc, ns) > common) split = ns;
+    if (ns < last && clz_delta(codes, sw, N, first, fc, fw, ns) > common) split = ns;
   } while (step > 1);
   int ca = split == first ? N - 1 + split : split;
   int cb = split + 1 == last ? N - 1 + split + 1 : split + 1;
@@ -158,6 +183,7 @@ __global__ void k_build(const DevState d, uint32_t n) {
   d.parent[ca] = idx;
   d.parent[cb] = idx;
   d.range_last[i] = last;
+  d.range_first[i] = first;
   d.visit[i] = 0;
 }
 
@@ -194,6 +220,19 @@ __global__ void k_refit(const DevState d, uint32_t n) {
 #define BB_HEAVY_CAP 1024u
 #define BB_FRONTIER 256
 
+// Child ch is worth visiting from query qi: it holds leaves in (qi, wend) and its box
+// overlaps the query box.  wend = n for one world; the end of the query's world otherwise.
+__device__ __forceinline__ bool bp_take(const DevState& d, int ch, int leaf0, int qi, int wend, float4 qmn, float4 qmx) {
+  bool take = ch >= leaf0 ? ((ch - leaf0) > qi && (ch - leaf0) < wend)
+                          : (d.range_last[ch] > qi && d.range_first[ch] < wend);
+  return take && box_overlap(qmn, qmx, d.node_box[2 * ch], d.node_box[2 * ch + 1]);
+}
+__device__ __forceinline__ int world_end(const DevState& d, uint32_t qi, uint32_t n) {
+  if (d.n_worlds <= 1) return int(n);
+  uint32_t w = d.sworld[qi];
+  return int(d.world_first[w] + d.world_count[w]);
+}
+
 // Left-first traversal for sorted query i.  EMIT=false counts, EMIT=true writes.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
@@ -210,6 +249,7 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
   const int N = int(n);
   const int leaf0 = N - 1;
   float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
+  const int wend = world_end(d, i, n);
   uint32_t out = EMIT ? d.pair_off[i] : 0u;
   const uint32_t cap = d.pair_capacity;
   uint32_t count = 0, visits = 0;
@@ -242,12 +282,7 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       int ch = kids[k];
-      bool take;
-      if (ch >= leaf0) take = (ch - leaf0) > int(i);
-      else take = d.range_last[ch] > int(i);
-      if (!take) continue;
-      float4 bmn = d.node_box[2 * ch], bmx = d.node_box[2 * ch + 1];
-      if (!box_overlap(qmn, qmx, bmn, bmx)) continue;
+      if (!bp_take(d, ch, leaf0, int(i), wend, qmn, qmx)) continue;
       if (sp < BB_BVH_STACK) stack[sp++] = ch;
       else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
     }
@@ -256,11 +291,6 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
     d.pair_cnt[i] = count;
     d.is_heavy[i] = 0;
   }
-}
-
-__device__ __forceinline__ bool bp_take(const DevState& d, int ch, int leaf0, int qi, float4 qmn, float4 qmx) {
-  bool take = ch >= leaf0 ? (ch - leaf0) > qi : d.range_last[ch] > qi;
-  return take && box_overlap(qmn, qmx, d.node_box[2 * ch], d.node_box[2 * ch + 1]);
 }
 
 // block-wide exclusive scan of one value per thread (blockDim.x == BB_FRONTIER)
@@ -304,6 +334,7 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
   const uint32_t qi = d.heavy_list[blockIdx.x];
   const int N = int(n), leaf0 = N - 1;
   const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
+  const int wend = world_end(d, qi, n);
   const int t = threadIdx.x;
   if (t == 0) {
     s_fr[0][0] = 0;
@@ -320,8 +351,8 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
       kid[c++] = node;  // a leaf entry stays in place
     } else if (node >= 0) {
       int2 ch = d.child[node];
-      if (bp_take(d, ch.x, leaf0, int(qi), qmn, qmx)) kid[c++] = ch.x;
-      if (bp_take(d, ch.y, leaf0, int(qi), qmn, qmx)) kid[c++] = ch.y;
+      if (bp_take(d, ch.x, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.x;
+      if (bp_take(d, ch.y, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.y;
     }
     uint32_t total;
     const uint32_t pos = block_excl_scan(c, s_warp, total);
@@ -361,11 +392,11 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
           continue;
         }
         int2 c = d.child[node];
-        if (bp_take(d, c.y, leaf0, int(qi), qmn, qmx)) {
+        if (bp_take(d, c.y, leaf0, int(qi), wend, qmn, qmx)) {
           if (sp < BB_BVH_STACK) stack[sp++] = c.y;
           else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
         }
-        if (bp_take(d, c.x, leaf0, int(qi), qmn, qmx)) {
+        if (bp_take(d, c.x, leaf0, int(qi), wend, qmn, qmx)) {
           if (sp < BB_BVH_STACK) stack[sp++] = c.x;
           else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
         }
@@ -394,7 +425,14 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   k_morton<<<blocks, T, 0, s>>>(d, n, p);
   uint32_t* keys[2] = {d.keys[0], d.keys[1]};
   uint32_t* vals[2] = {d.vals[0], d.vals[1]};
-  bb_launch_sort(s, keys, vals, nullptr, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms);
+  if (d.n_worlds > 1) {
+    // stable sort by code, then by world id (two digits of world_of[id]): key order (world, code)
+    bb_launch_sort(s, keys, vals, nullptr, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms,
+                   d.world_of, 2);
+    k_sorted_world<<<blocks, T, 0, s>>>(d, n);
+  } else {
+    bb_launch_sort(s, keys, vals, nullptr, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms);
+  }
   k_build<<<blocks, T, 0, s>>>(d, n);
   k_refit<<<blocks, T, 0, s>>>(d, n);
   uint32_t bb = (n + 127) / 128;

@@ -57,6 +57,8 @@ struct DevCounters {
   uint32_t avbd_body_count;
   uint32_t substeps;       // substeps run since the last stats read
   uint32_t pad[6];
+  uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
+                           // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD
 };
 
 // ---- pointers of one world's device state ------------------------------------------------
@@ -94,6 +96,13 @@ struct DevState {
   float4* c_anc_b[2];    // AVBD local anchor on b .xyz, 0
   // PGS rows (current only)
   float4 *c_r1, *c_r2, *c_k;
+  // dataflow schedule: per compact manifold (slot, a, b, rank_a | rank_b << 16); per-body counters
+  uint4* flow_rec;
+  uint32_t* flow_counter;
+  // barrier schedule: colour-ordered items, rec = (slot, a, b, cc | dyn_a << 8 | dyn_b << 9 |
+  // skip << 10), mass = (inverse mass a, inverse mass b, friction, -)
+  uint4* pgs_rec;
+  float4* pgs_mass;
   // per-body manifold lists (CSR over compact manifold indices) [cur], [prev]
   uint32_t* csr_start[2];
   uint32_t* csr_list[2];
@@ -123,6 +132,15 @@ struct DevState {
   uint32_t* sort_hist;    // 4 x 256 global digit histograms
   uint32_t* sort_status;  // tiles x 256 per pass
   uint32_t* sort_tile_ctr;
+  // batched worlds (n_worlds > 1): world w owns body ids [world_first[w], +world_count[w]),
+  // which is also its range of sorted positions (keys sort by (world, Morton code))
+  uint32_t n_worlds;
+  uint32_t* world_of;     // per body
+  uint32_t* world_first;  // per world
+  uint32_t* world_count;  // per world
+  float4* world_bounds;   // per world: (min.xyz, -), (extent.xyz, -)
+  uint32_t* sworld;       // world of each sorted position
+  int32_t* range_first;   // first leaf covered by each internal node
   DevCounters* ctr;
   float* staging;  // host state exchange: rot 4N | pos 3N | vel 3N | omega 3N
   uint32_t pair_capacity;
@@ -223,6 +241,12 @@ __device__ __forceinline__ Sym3 world_inv_inertia(Quatf q, float3 d, bool transp
 
 __device__ __forceinline__ void raise_error(DevCounters* c, uint32_t bit) { atomicOr(&c->error_flags, bit); }
 
+// id of a body inside its own world (batched worlds hash world-local ids, so a world's
+// colouring does not depend on where it sits in the batch)
+__device__ __forceinline__ uint32_t local_id(const DevState& d, uint32_t id) {
+  return d.n_worlds > 1 ? id - d.world_first[d.world_of[id]] : id;
+}
+
 // order-preserving float <-> uint (include/math.hpp:228-256)
 __device__ __forceinline__ uint32_t f2ord(float f) {
   uint32_t u = __float_as_uint(f);
@@ -266,6 +290,32 @@ __device__ __forceinline__ void grid_barrier(DevCounters* c) {
       }
     }
     fence_acq_rel_gpu();
+  }
+  __syncthreads();
+}
+
+// Grid barrier on a monotonic arrival counter that is zero when the kernel starts (one counter
+// per persistent launch of a substep): block thread 0 publishes the block's writes and adds one
+// without waiting for a reply, then polls until all blocks of this epoch arrived.  Two round
+// trips fewer than the generation barrier above (no generation read, no atomic reply).
+__device__ __forceinline__ void red_relaxed_add(uint32_t* p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void grid_sync(DevCounters* c, uint32_t* count, uint32_t& epoch) {
+  __syncthreads();
+  ++epoch;
+  if (threadIdx.x == 0) {
+    fence_acq_rel_gpu();  // release this block's writes (cumulative over the CTA barrier)
+    red_relaxed_add(count, 1u);
+    const uint32_t target = epoch * gridDim.x;
+    uint32_t spins = 0;
+    while (ld_acquire_gpu(count) < target) {
+      if (++spins > BB_SPIN_LIMIT) {
+        atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
+        break;
+      }
+      if ((spins & 1023u) == 0u && (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT)) break;
+    }
   }
   __syncthreads();
 }

@@ -219,7 +219,8 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_edge_color(const DevStat
   for (uint32_t m = tid; m < M; m += stride) {
     uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
     int key = d.m_keycc[cur][d.man_slot[cur][m]].x;
-    uint32_t lo = min(b.x, b.y), hi = max(b.x, b.y);
+    const uint32_t la = local_id(d, b.x), lb = local_id(d, b.y);
+    uint32_t lo = min(la, lb), hi = max(la, lb);
     d.gc_pid[m] = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
     d.gc_color[m] = BB_UNCOLORED;
   }
@@ -297,8 +298,9 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
   // stable bucket sort of manifold ids by colour (one 8-bit digit)
   uint32_t* keys[2] = {d.bucket_keys[0], d.bucket_keys[1]};
   uint32_t* vals[2] = {d.bucket_vals[0], d.bucket_vals[1]};
-  uint32_t* hist = sc.sort_hist + 2 * 4 * 256;
-  bb_launch_sort(s, keys, vals, &d.ctr->manifold_count, d.pair_capacity, 1, 0, hist, sc.sort_status + 4 * sc.sort_tiles * 256,
-                 sc.sort_tile_ctr + 4, d.ctr, sms);
-  k_bucket_starts<<<1, 64, 0, s>>>(hist + 4 * 256, &d.ctr->manifold_count, d.bucket_start, BB_MAX_COLORS + 1);
+  // scratch: histogram region 1, status / tile-counter slot 6 (the front-end sort uses 0..5)
+  uint32_t* hist = sc.sort_hist + 1 * BB_HIST_REGION;
+  bb_launch_sort(s, keys, vals, &d.ctr->manifold_count, d.pair_capacity, 1, 0, hist,
+                 sc.sort_status + 6 * size_t(sc.sort_tiles) * 256, sc.sort_tile_ctr + 6, d.ctr, sms);
+  k_bucket_starts<<<1, 64, 0, s>>>(hist + 8 * 256, &d.ctr->manifold_count, d.bucket_start, BB_MAX_COLORS + 1);
 }

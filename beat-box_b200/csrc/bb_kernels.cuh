@@ -7,9 +7,14 @@ void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uin
                     uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr);
 uint32_t bb_scan_tiles(uint32_t n_cap);
 uint32_t bb_sort_tiles(uint32_t n_cap);
+// hist regions are BB_HIST_REGION words: 8 rows of counts + 8 rows of exclusive starts
+#define BB_HIST_REGION (2 * 8 * 256)
 void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,
                     int passes, int shift0, uint32_t* hist, uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr,
-                    int sms);
+                    int sms, const uint32_t* lut = nullptr, int lut_passes = 0);
+void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* dst_keys[2],
+                       uint32_t* dst_vals[2], uint32_t n, int passes, uint32_t* hist, uint32_t* status,
+                       uint32_t* tile_ctr, DevCounters* ctr, int sms);
 
 // Scratch bookkeeping shared by the stages of one substep.
 struct StepScratch {
@@ -43,6 +48,15 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
                        int coop_blocks, int sms);
 void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,
                    int sms, int cur, int coop_blocks);
+
+// thread-local last-error message behind bb_last_error_string (bb_world.cu)
+bb_status bb_fail(bb_status code, const char* msg);
+
+// stand-alone radix sort helpers (bb_sort_api.cu)
+bb_status bb_check_sort_args(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                             uint32_t n, uint32_t key_bits);
+void bb_sort_carve(char* base, uint32_t n, int passes, DevCounters** ctr, uint32_t** hist, uint32_t** tile_ctr,
+                   uint32_t** status, uint32_t** tmp_keys, uint32_t** tmp_vals, size_t* zero_bytes);
 
 // co-resident block counts of the persistent cooperative kernels
 int bb_edge_coloring_blocks(int sms);

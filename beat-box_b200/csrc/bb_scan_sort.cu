@@ -108,26 +108,33 @@ __global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------------------
-// global digit histograms of `passes` 8-bit digits starting at bit shift0
+// Global histograms of `passes` 8-bit key digits starting at bit shift0, followed by
+// `lut_passes` digits of lut[value] (world ids in batched worlds).  Rows: up to 8.
 __global__ void __launch_bounds__(kThreads) k_sort_hist(const uint32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vals,
+                                                        const uint32_t* __restrict__ lut,
                                                         const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
-                                                        uint32_t* hist, int passes, int shift0) {
-  __shared__ uint32_t s_hist[4][256];
-  for (int i = threadIdx.x; i < 4 * 256; i += kThreads) (&s_hist[0][0])[i] = 0;
+                                                        uint32_t* hist, int passes, int lut_passes, int shift0) {
+  __shared__ uint32_t s_hist[8][256];
+  for (int i = threadIdx.x; i < 8 * 256; i += kThreads) (&s_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
   for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
     uint32_t k = keys[i];
     for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(k >> (shift0 + 8 * p)) & 255u], 1u);
+    if (lut_passes) {
+      uint32_t w = lut[vals[i]];
+      for (int p = 0; p < lut_passes; ++p) atomicAdd(&s_hist[passes + p][(w >> (8 * p)) & 255u], 1u);
+    }
   }
   __syncthreads();
-  for (int p = 0; p < passes; ++p) {
+  for (int p = 0; p < passes + lut_passes; ++p) {
     uint32_t c = s_hist[p][threadIdx.x];
     if (c) atomicAdd(&hist[p * 256 + threadIdx.x], c);
   }
 }
 
-// exclusive scan of each 256-bin histogram row in place into hist_scan (count rows kept)
+// exclusive scan of each 256-bin histogram row into hist_scan (count rows kept)
 __global__ void k_sort_hist_scan(const uint32_t* hist, uint32_t* hist_scan, int passes) {
   __shared__ uint32_t s[256];
   for (int p = 0; p < passes; ++p) {
@@ -145,14 +152,16 @@ __global__ void k_sort_hist_scan(const uint32_t* hist, uint32_t* hist_scan, int 
   }
 }
 
-// one stable onesweep pass on digit (key >> shift) & 255
+// one stable onesweep pass on digit (key >> shift) & 255, or (lut[value] >> shift) & 255
+// when lut is given
 __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in,
                                                        const uint32_t* __restrict__ vals_in,
                                                        uint32_t* __restrict__ keys_out,
                                                        uint32_t* __restrict__ vals_out,
                                                        const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
                                                        const uint32_t* __restrict__ digit_start, int shift,
-                                                       uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr) {
+                                                       const uint32_t* __restrict__ lut, uint32_t* status,
+                                                       uint32_t* tile_ctr, DevCounters* ctr) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_hist[kThreads / 32][256];
   __shared__ uint32_t s_offset[256];
@@ -172,7 +181,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     bool ok = i < n;
     key[k] = ok ? keys_in[i] : 0u;
     val[k] = ok ? vals_in[i] : 0u;
-    dig[k] = ok ? ((key[k] >> shift) & 255u) : 256u;
+    dig[k] = ok ? (((lut ? lut[val[k]] : key[k]) >> shift) & 255u) : 256u;
   }
 #pragma unroll
   for (int k = 0; k < kItems; ++k) {
@@ -243,21 +252,47 @@ void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uin
 uint32_t bb_scan_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
 uint32_t bb_sort_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
 
-// Sorts `passes` digits of (keys, vals) in place between buffers 0 and 1; result in buffer
-// passes % 2.  hist: 2 x 4 x 256 words (counts, exclusive starts); status: passes x tiles x
-// 256 words, zeroed; tile_ctr: passes words, zeroed.
+// Sorts `passes` digits: pass 0 reads (keys_in, vals_in); pass k writes buffer
+// dst[(passes - 1 - k) & 1] and the next pass reads it, so the last pass lands in dst[0].
+// hist: 2 x 4 x 256 words (counts, exclusive starts), zeroed; status: passes x tiles x 256
+// words, zeroed; tile_ctr: passes words, zeroed.
+void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* dst_keys[2],
+                       uint32_t* dst_vals[2], uint32_t n, int passes, uint32_t* hist, uint32_t* status,
+                       uint32_t* tile_ctr, DevCounters* ctr, int sms) {
+  uint32_t tiles = (n + kTile - 1) / kTile;
+  if (tiles == 0) tiles = 1;
+  k_sort_hist<<<sms * 4, kThreads, 0, s>>>(keys_in, vals_in, nullptr, nullptr, n, hist, passes, 0, 0);
+  k_sort_hist_scan<<<1, 256, 0, s>>>(hist, hist + 8 * 256, passes);
+  const uint32_t* ik = keys_in;
+  const uint32_t* iv = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    int o = (passes - 1 - p) & 1;
+    k_onesweep<<<tiles, kThreads, 0, s>>>(ik, iv, dst_keys[o], dst_vals[o], nullptr, n, hist + 8 * 256 + p * 256, 8 * p,
+                                          nullptr, status + size_t(p) * tiles * 256, tile_ctr + p, ctr);
+    ik = dst_keys[o];
+    iv = dst_vals[o];
+  }
+}
+
+// Sorts `passes` key digits (from bit shift0) and then `lut_passes` digits of lut[value] in
+// place between buffers 0 and 1; result in buffer (passes + lut_passes) % 2.  hist: one region
+// of 2 x 8 x 256 words (counts, exclusive starts), zeroed; status: (passes + lut_passes) x
+// tiles x 256 words, zeroed; tile_ctr: one word per pass, zeroed.
 void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,
                     int passes, int shift0, uint32_t* hist, uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr,
-                    int sms) {
+                    int sms, const uint32_t* lut, int lut_passes) {
   uint32_t tiles = (n_cap + kTile - 1) / kTile;
   if (tiles == 0) tiles = 1;
-  int hblocks = sms * 4;
-  k_sort_hist<<<hblocks, kThreads, 0, s>>>(keys[0], n_dev, n_cap, hist, passes, shift0);
-  k_sort_hist_scan<<<1, 256, 0, s>>>(hist, hist + 4 * 256, passes);
-  for (int p = 0; p < passes; ++p) {
+  const int total = passes + (lut ? lut_passes : 0);
+  k_sort_hist<<<sms * 4, kThreads, 0, s>>>(keys[0], vals[0], lut, n_dev, n_cap, hist, passes, lut ? lut_passes : 0,
+                                           shift0);
+  k_sort_hist_scan<<<1, 256, 0, s>>>(hist, hist + 8 * 256, total);
+  for (int p = 0; p < total; ++p) {
     int in = p & 1, out = in ^ 1;
+    bool by_lut = p >= passes;
     k_onesweep<<<tiles, kThreads, 0, s>>>(keys[in], vals[in], keys[out], vals[out], n_dev, n_cap,
-                                          hist + 4 * 256 + p * 256, shift0 + 8 * p,
-                                          status + size_t(p) * tiles * 256, tile_ctr + p, ctr);
+                                          hist + 8 * 256 + p * 256, by_lut ? 8 * (p - passes) : shift0 + 8 * p,
+                                          by_lut ? lut : nullptr, status + size_t(p) * tiles * 256, tile_ctr + p,
+                                          ctr);
   }
 }

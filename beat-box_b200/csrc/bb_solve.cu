@@ -51,10 +51,122 @@ __device__ __forceinline__ Quatf apply_angular_velocity(Quatf rot, float3 w, flo
   return q_normalize(q_mul(q, rot));
 }
 
-// PGS_SOFT::pre_step (solvers.slang:143-196)
-__device__ void pgs_pre_step(const DevState& d, const Params& p, int cur, uint32_t m, float h, float hertz) {
-  const uint32_t slot = d.man_slot[cur][m];
-  const uint2 b = d.m_bodies[cur][slot];
+// ---- PGS_SOFT arithmetic of one contact, shared by both schedules (same expressions, so the
+// schedules agree bit for bit) -------------------------------------------------------------
+
+// soft-constraint coefficients of a manifold (solvers.slang:150-158)
+struct SoftCoef {
+  float bf, mcoef, icoef, inv_h;
+};
+__device__ __forceinline__ SoftCoef pgs_soft_coef(float ima, float imb, float h, float hertz) {
+  const float ch = (ima == 0.f || imb == 0.f) ? 2.0f * hertz : hertz;
+  const float zeta = 10.0f;
+  const float omega = 2.0f * 3.14159265359f * ch;
+  const float c = h * omega * (2.0f * zeta + h * omega);
+  SoftCoef s;
+  s.bf = omega / (2.0f * zeta + h * omega);
+  s.icoef = 1.0f / (1.0f + c);
+  s.mcoef = c * s.icoef;
+  s.inv_h = h > 0.f ? 1.0f / h : 0.f;
+  return s;
+}
+
+// rows of one contact (solvers.slang:160-190): R1 = (r1, normal mass), R2 = (r2, tangent
+// mass 0), K = (tangent mass 1, bias, mass coefficient, impulse coefficient)
+__device__ __forceinline__ void pgs_contact_rows(float4 pp, float3 aa, float3 ab, float3 n, float3 t0, float3 t1,
+                                                 float ima, float imb, const Sym3& IA, const Sym3& IB,
+                                                 const SoftCoef& s, float4& R1, float4& R2, float4& K) {
+  const float3 r1 = f3(pp) - aa, r2 = f3(pp) - ab;
+  float3 rn1 = cross3(r1, n), rn2 = cross3(r2, n);
+  float kn = ima + imb + dot3(rn1, sym_mul(IA, rn1)) + dot3(rn2, sym_mul(IB, rn2));
+  float nmass = kn == 0.f ? 0.f : 1.0f / kn;
+  float tm[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    float3 t = k == 0 ? t0 : t1;
+    float3 rt1 = cross3(r1, t), rt2 = cross3(r2, t);
+    float kt = ima + imb + dot3(rt1, sym_mul(IA, rt1)) + dot3(rt2, sym_mul(IB, rt2));
+    tm[k] = kt == 0.f ? 0.f : 1.0f / kt;
+  }
+  const float pen = pp.w;
+  const float bias_value = pen > 0.f ? pen * s.inv_h : fmaxf(s.bf * pen, -4.0f);
+  R1 = f4(r1, nmass);
+  R2 = f4(r2, tm[0]);
+  K = make_float4(tm[1], bias_value, s.mcoef, s.icoef);
+}
+
+// warm start of one contact: apply the accumulated impulse (solvers.slang:191-195)
+__device__ __forceinline__ void pgs_contact_warm(float3 r1, float3 r2, float4 lam, float3 n, float3 t0, float3 t1,
+                                                 bool fric, float ima, float imb, const Sym3& IA, const Sym3& IB,
+                                                 float3& va, float3& wa, float3& vb, float3& wb) {
+  float3 P = n * lam.x;
+  if (fric) P = P + t0 * lam.y + t1 * lam.z;
+  va = va - P * ima;
+  wa = wa - sym_mul(IA, cross3(r1, P));
+  vb = vb + P * imb;
+  wb = wb + sym_mul(IB, cross3(r2, P));
+}
+
+// one contact of PGS_SOFT::solve (solvers.slang:209-277): two friction rows, then the normal row
+__device__ __forceinline__ void pgs_contact_solve(float4 R1, float4 R2, float4 K, float4& lam, float3 n, float3 t0,
+                                                  float3 t1, float mu, bool use_bias, bool accum, bool fric, float ima,
+                                                  float imb, const Sym3& IA, const Sym3& IB, float3& va, float3& wa,
+                                                  float3& vb, float3& wb) {
+  const float3 r1 = f3(R1), r2 = f3(R2);
+  float3 rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
+  if (fric) {
+    float imp_t[2] = {lam.y, lam.z};
+    const float tmass[2] = {R2.w, K.x};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const float3 t = k == 0 ? t0 : t1;
+      float tv = dot3(rv, t);
+      float ti = tmass[k] * -tv;
+      float maxf = mu * lam.x;
+      if (accum) {
+        float old = imp_t[k];
+        imp_t[k] = fminf(fmaxf(old + ti, -maxf), maxf);
+        ti = imp_t[k] - old;
+      } else {
+        ti = fminf(fmaxf(ti, -maxf), maxf);
+      }
+      float3 P = t * ti;
+      va = va - P * ima;
+      wa = wa - sym_mul(IA, cross3(r1, P));
+      vb = vb + P * imb;
+      wb = wb + sym_mul(IB, cross3(r2, P));
+    }
+    lam.y = imp_t[0];
+    lam.z = imp_t[1];
+  }
+  rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
+  float vn = dot3(rv, n);
+  float bias = 0.f, ms = 1.f, is = 0.f;
+  if (K.y > 0.f) {
+    bias = K.y;
+  } else if (use_bias) {
+    bias = K.y;
+    ms = K.z;
+    is = K.w;
+  }
+  float imp = -R1.w * ms * (vn + bias) - is * lam.x;
+  if (accum) {
+    float old = lam.x;
+    lam.x = fmaxf(old + imp, 0.f);
+    imp = lam.x - old;
+  } else {
+    imp = fmaxf(imp, 0.f);
+  }
+  float3 P = n * imp;
+  va = va - P * ima;
+  wa = wa - sym_mul(IA, cross3(r1, P));
+  vb = vb + P * imb;
+  wb = wb + sym_mul(IB, cross3(r2, P));
+}
+
+// PGS_SOFT::pre_step (solvers.slang:143-196) of one manifold slot: rows, then warm start
+__device__ void pgs_pre_step_slot(const DevState& d, const Params& p, int cur, uint32_t slot, uint2 b, float h,
+                                  float hertz) {
   const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
   if (!awake(fa) && !awake(fb)) return;
   const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
@@ -65,47 +177,20 @@ __device__ void pgs_pre_step(const DevState& d, const Params& p, int cur, uint32
   const float3 aa = f3(d.m_anchor_a[cur][slot]), ab = f3(d.m_anchor_b[cur][slot]);
   const int cc = d.m_keycc[cur][slot].y;
   const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
-  const float ch = (ima == 0.f || imb == 0.f) ? 2.0f * hertz : hertz;
-  const float zeta = 10.0f;
-  const float omega = 2.0f * 3.14159265359f * ch;
-  const float c = h * omega * (2.0f * zeta + h * omega);
-  const float bf = omega / (2.0f * zeta + h * omega);
-  const float icoef = 1.0f / (1.0f + c);
-  const float mcoef = c * icoef;
-  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
+  const SoftCoef s = pgs_soft_coef(ima, imb, h, hertz);
   for (int j = 0; j < cc; ++j) {
     const uint32_t ci = slot * BB_MAX_CONTACTS + j;
-    const float4 pp = d.c_pos[cur][ci];
-    const float3 r1 = f3(pp) - aa, r2 = f3(pp) - ab;
-    float3 rn1 = cross3(r1, n), rn2 = cross3(r2, n);
-    float kn = ima + imb + dot3(rn1, sym_mul(IA, rn1)) + dot3(rn2, sym_mul(IB, rn2));
-    float nmass = kn == 0.f ? 0.f : 1.0f / kn;
-    float tm[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      float3 t = k == 0 ? t0 : t1;
-      float3 rt1 = cross3(r1, t), rt2 = cross3(r2, t);
-      float kt = ima + imb + dot3(rt1, sym_mul(IA, rt1)) + dot3(rt2, sym_mul(IB, rt2));
-      tm[k] = kt == 0.f ? 0.f : 1.0f / kt;
-    }
-    const float pen = pp.w;
-    const float bias_value = pen > 0.f ? pen * inv_h : fmaxf(bf * pen, -4.0f);
-    d.c_r1[ci] = f4(r1, nmass);
-    d.c_r2[ci] = f4(r2, tm[0]);
-    d.c_k[ci] = make_float4(tm[1], bias_value, mcoef, icoef);
+    float4 R1, R2, K;
+    pgs_contact_rows(d.c_pos[cur][ci], aa, ab, n, t0, t1, ima, imb, IA, IB, s, R1, R2, K);
+    d.c_r1[ci] = R1;
+    d.c_r2[ci] = R2;
+    d.c_k[ci] = K;
     float4 lam = d.c_lam[cur][ci];
     // the reference writes its mass coefficient / tangent masses into the persistent contact
-    d.c_lam[cur][ci] = make_float4(lam.x, lam.y, lam.z, mcoef);
+    d.c_lam[cur][ci] = make_float4(lam.x, lam.y, lam.z, s.mcoef);
     float4 kt4 = d.c_kt[cur][ci];
-    d.c_kt[cur][ci] = make_float4(tm[0], tm[1], kt4.z, kt4.w);
-    if (accum) {
-      float3 P = n * lam.x;
-      if (fric) P = P + t0 * lam.y + t1 * lam.z;
-      va = va - P * ima;
-      wa = wa - sym_mul(IA, cross3(r1, P));
-      vb = vb + P * imb;
-      wb = wb + sym_mul(IB, cross3(r2, P));
-    }
+    d.c_kt[cur][ci] = make_float4(R2.w, K.x, kt4.z, kt4.w);
+    if (accum) pgs_contact_warm(f3(R1), f3(R2), lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
   }
   if (fa & BB_BODY_DYNAMIC) {
     d.vel[b.x] = f4(va, d.vel[b.x].w);
@@ -117,10 +202,8 @@ __device__ void pgs_pre_step(const DevState& d, const Params& p, int cur, uint32
   }
 }
 
-// PGS_SOFT::solve (solvers.slang:199-278)
-__device__ void pgs_solve(const DevState& d, const Params& p, int cur, uint32_t m, bool use_bias) {
-  const uint32_t slot = d.man_slot[cur][m];
-  const uint2 b = d.m_bodies[cur][slot];
+// PGS_SOFT::solve (solvers.slang:199-278) of one manifold slot
+__device__ void pgs_solve_slot(const DevState& d, const Params& p, int cur, uint32_t slot, uint2 b, bool use_bias) {
   const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
   if (!awake(fa) && !awake(fb)) return;
   const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
@@ -134,58 +217,9 @@ __device__ void pgs_solve(const DevState& d, const Params& p, int cur, uint32_t 
   const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
   for (int j = 0; j < cc; ++j) {
     const uint32_t ci = slot * BB_MAX_CONTACTS + j;
-    const float4 R1 = d.c_r1[ci], R2 = d.c_r2[ci], K = d.c_k[ci];
     float4 lam = d.c_lam[cur][ci];
-    const float3 r1 = f3(R1), r2 = f3(R2);
-    float3 rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
-    if (fric) {
-      float imp_t[2] = {lam.y, lam.z};
-      const float tmass[2] = {R2.w, K.x};
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const float3 t = k == 0 ? t0 : t1;
-        float tv = dot3(rv, t);
-        float ti = tmass[k] * -tv;
-        float maxf = mu * lam.x;
-        if (accum) {
-          float old = imp_t[k];
-          imp_t[k] = fminf(fmaxf(old + ti, -maxf), maxf);
-          ti = imp_t[k] - old;
-        } else {
-          ti = fminf(fmaxf(ti, -maxf), maxf);
-        }
-        float3 P = t * ti;
-        va = va - P * ima;
-        wa = wa - sym_mul(IA, cross3(r1, P));
-        vb = vb + P * imb;
-        wb = wb + sym_mul(IB, cross3(r2, P));
-      }
-      lam.y = imp_t[0];
-      lam.z = imp_t[1];
-    }
-    rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
-    float vn = dot3(rv, n);
-    float bias = 0.f, ms = 1.f, is = 0.f;
-    if (K.y > 0.f) {
-      bias = K.y;
-    } else if (use_bias) {
-      bias = K.y;
-      ms = K.z;
-      is = K.w;
-    }
-    float imp = -R1.w * ms * (vn + bias) - is * lam.x;
-    if (accum) {
-      float old = lam.x;
-      lam.x = fmaxf(old + imp, 0.f);
-      imp = lam.x - old;
-    } else {
-      imp = fmaxf(imp, 0.f);
-    }
-    float3 P = n * imp;
-    va = va - P * ima;
-    wa = wa - sym_mul(IA, cross3(r1, P));
-    vb = vb + P * imb;
-    wb = wb + sym_mul(IB, cross3(r2, P));
+    pgs_contact_solve(d.c_r1[ci], d.c_r2[ci], d.c_k[ci], lam, n, t0, t1, mu, use_bias, accum, fric, ima, imb, IA, IB,
+                      va, wa, vb, wb);
     d.c_lam[cur][ci] = lam;
   }
   if (fa & BB_BODY_DYNAMIC) {
@@ -198,70 +232,348 @@ __device__ void pgs_solve(const DevState& d, const Params& p, int cur, uint32_t 
   }
 }
 
-// sweep over colours 0..C-1 and the overflow bucket; phase 0 pre-step, 1 solve, 2 relax
-__device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int phase, float h, float hertz) {
-  const uint32_t C = d.ctr->gc_colors;
-  const uint32_t* list = d.bucket_vals[1];
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  for (uint32_t c = 0; c < C; ++c) {
-    uint32_t s0 = d.bucket_start[c], s1 = d.bucket_start[c + 1];
-    if (s0 == s1) continue;
-    for (uint32_t k = s0 + tid; k < s1; k += stride) {
-      uint32_t m = list[k];
-      if (phase == 0) pgs_pre_step(d, p, cur, m, h, hertz);
-      else pgs_solve(d, p, cur, m, phase == 1);
+// integrate one body (RB_sim.slang:1287-1326) and refresh its world inverse inertia
+__device__ __forceinline__ void pgs_integrate(const DevState& d, uint32_t i, float h, bool tq) {
+  float4 ps = d.pos[i];
+  float3 v = f3(d.vel[i]);
+  d.pos[i] = make_float4(ps.x + v.x * h, ps.y + v.y * h, ps.z + v.z * h, ps.w);
+  Quatf q = apply_angular_velocity(q_from(d.rot[i]), f3(d.omega[i]), h);
+  d.rot[i] = q_to4(q);
+  store_iw(d, i, world_inv_inertia(q, f3(d.iinv[i]), tq));
+}
+
+// ---------------------------------------------------------------------------------------
+// PGS_SOFT, colour-barrier schedule: one persistent cooperative kernel.
+//
+// Every sweep walks the colour buckets in order with a grid barrier after each colour; item k
+// of a colour (a manifold) always belongs to the same thread, so the thread can load the
+// next colour's item -- its record, contact frame, rows and impulses, none of which another
+// thread writes -- BEFORE the barrier, and after the barrier only the two bodies' velocities
+// and inertias remain to be fetched: one memory round trip per colour on the critical path.
+#define BB_PGS_THREADS 256  // one block per SM: up to 255 registers for the held item
+#define BB_PGS_PF 4         // contacts of an item held in registers across the barrier
+#define BB_PGS_SKIP (1u << 10)
+
+struct PgsItem {
+  uint4 rec;    // slot, body a, body b, contact count | dynamic a << 8 | dynamic b << 9 | skip << 10
+  float4 mass;  // inverse mass a, inverse mass b, friction, -
+  float4 n, t0, t1;
+  float4 R1[BB_PGS_PF], R2[BB_PGS_PF], K[BB_PGS_PF], lam[BB_PGS_PF];
+};
+
+__device__ __forceinline__ void pgs_item_load(const DevState& d, int cur, uint32_t k, PgsItem& x) {
+  x.rec = d.pgs_rec[k];
+  x.mass = d.pgs_mass[k];
+  if (x.rec.w & BB_PGS_SKIP) return;
+  const uint32_t slot = x.rec.x, cc = x.rec.w & 0xFFu;
+  x.n = d.m_normal[cur][slot];
+  x.t0 = d.m_t0[cur][slot];
+  x.t1 = d.m_t1[cur][slot];
+#pragma unroll
+  for (int j = 0; j < BB_PGS_PF; ++j) {
+    if (uint32_t(j) < cc) {
+      const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+      x.R1[j] = d.c_r1[ci];
+      x.R2[j] = d.c_r2[ci];
+      x.K[j] = d.c_k[ci];
+      x.lam[j] = d.c_lam[cur][ci];
     }
-    grid_barrier(d.ctr);
-  }
-  uint32_t o0 = d.bucket_start[BB_MAX_COLORS], o1 = d.bucket_start[BB_MAX_COLORS + 1];
-  if (o0 != o1) {
-    if (tid == 0) {
-      for (uint32_t k = o0; k < o1; ++k) {
-        uint32_t m = list[k];
-        if (phase == 0) pgs_pre_step(d, p, cur, m, h, hertz);
-        else pgs_solve(d, p, cur, m, phase == 1);
-      }
-    }
-    grid_barrier(d.ctr);
   }
 }
 
-__global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
+// item record + rows of colour-ordered item k (the pre-step's row half; no body is touched)
+__device__ void pgs_item_build(const DevState& d, int cur, uint32_t k, uint32_t m, float h, float hertz) {
+  const uint32_t slot = d.man_slot[cur][m];
+  const uint2 b = d.m_bodies[cur][slot];
+  const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+  const uint32_t cc = uint32_t(d.m_keycc[cur][slot].y);
+  const bool skip = !awake(fa) && !awake(fb);
+  const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
+  d.pgs_rec[k] = make_uint4(slot, b.x, b.y,
+                            cc | ((fa & BB_BODY_DYNAMIC) ? 1u << 8 : 0u) | ((fb & BB_BODY_DYNAMIC) ? 1u << 9 : 0u) |
+                                (skip ? BB_PGS_SKIP : 0u));
+  d.pgs_mass[k] = make_float4(ima, imb, sqrtf(d.iinv[b.x].w * d.iinv[b.y].w), 0.f);
+  if (skip) return;
+  const Sym3 IA = load_iw(d, b.x), IB = load_iw(d, b.y);
+  const float3 n = f3(d.m_normal[cur][slot]);
+  const float3 t0 = f3(d.m_t0[cur][slot]), t1 = f3(d.m_t1[cur][slot]);
+  const float3 aa = f3(d.m_anchor_a[cur][slot]), ab = f3(d.m_anchor_b[cur][slot]);
+  const SoftCoef s = pgs_soft_coef(ima, imb, h, hertz);
+  for (uint32_t j = 0; j < cc; ++j) {
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    float4 R1, R2, K;
+    pgs_contact_rows(d.c_pos[cur][ci], aa, ab, n, t0, t1, ima, imb, IA, IB, s, R1, R2, K);
+    d.c_r1[ci] = R1;
+    d.c_r2[ci] = R2;
+    d.c_k[ci] = K;
+    const float4 lam = d.c_lam[cur][ci];
+    d.c_lam[cur][ci] = make_float4(lam.x, lam.y, lam.z, s.mcoef);
+    const float4 kt4 = d.c_kt[cur][ci];
+    d.c_kt[cur][ci] = make_float4(R2.w, K.x, kt4.z, kt4.w);
+  }
+}
+
+// mode 0: warm start, 1: solve sweep (soft bias), 2: relax sweep
+__device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p, int cur, PgsItem& x, int mode) {
+  if (x.rec.w & BB_PGS_SKIP) return;
+  const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
+  if (mode == 0 && !accum) return;
+  const uint32_t a = x.rec.y, b = x.rec.z, slot = x.rec.x, cc = x.rec.w & 0xFFu;
+  float4 va4 = d.vel[a], vb4 = d.vel[b];
+  float3 va = f3(va4), wa = f3(d.omega[a]), vb = f3(vb4), wb = f3(d.omega[b]);
+  const Sym3 IA = load_iw(d, a), IB = load_iw(d, b);
+  const float ima = x.mass.x, imb = x.mass.y, mu = x.mass.z;
+  const float3 n = f3(x.n), t0 = f3(x.t0), t1 = f3(x.t1);
+#pragma unroll
+  for (int j = 0; j < BB_PGS_PF; ++j) {
+    if (uint32_t(j) < cc) {
+      if (mode == 0) {
+        pgs_contact_warm(f3(x.R1[j]), f3(x.R2[j]), x.lam[j], n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
+      } else {
+        pgs_contact_solve(x.R1[j], x.R2[j], x.K[j], x.lam[j], n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA,
+                          IB, va, wa, vb, wb);
+        d.c_lam[cur][slot * BB_MAX_CONTACTS + j] = x.lam[j];
+      }
+    }
+  }
+  for (uint32_t j = BB_PGS_PF; j < cc; ++j) {  // contacts beyond the register-held ones
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    float4 lam = d.c_lam[cur][ci];
+    if (mode == 0) {
+      pgs_contact_warm(f3(d.c_r1[ci]), f3(d.c_r2[ci]), lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
+    } else {
+      pgs_contact_solve(d.c_r1[ci], d.c_r2[ci], d.c_k[ci], lam, n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA,
+                        IB, va, wa, vb, wb);
+      d.c_lam[cur][ci] = lam;
+    }
+  }
+  if (x.rec.w & (1u << 8)) {
+    d.vel[a] = f4(va, va4.w);
+    d.omega[a] = f4(wa, 0.f);
+  }
+  if (x.rec.w & (1u << 9)) {
+    d.vel[b] = f4(vb, vb4.w);
+    d.omega[b] = f4(wb, 0.f);
+  }
+}
+
+// one sweep over colours 0..C-1 and the overflow bucket.  On entry x holds this thread's first
+// item of colour 0; on exit it holds the same for the next sweep.
+__device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode, const uint32_t* bs, uint32_t C,
+                          PgsItem& x, uint32_t& epoch) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  uint32_t* sync = &d.ctr->sync_count[1];
+  for (uint32_t c = 0; c < C; ++c) {
+    const uint32_t end = bs[c + 1];
+    for (uint32_t k = bs[c] + tid; k < end;) {
+      pgs_item_run(d, p, cur, x, mode);
+      k += stride;
+      if (k < end) pgs_item_load(d, cur, k, x);
+    }
+    const uint32_t cn = c + 1 < C ? c + 1 : 0u;
+    if (bs[cn] + tid < bs[cn + 1]) pgs_item_load(d, cur, bs[cn] + tid, x);
+    grid_sync(d.ctr, sync, epoch);
+  }
+  const uint32_t o0 = bs[BB_MAX_COLORS], o1 = bs[BB_MAX_COLORS + 1];
+  if (o0 != o1) {  // overflow bucket: serial, in manifold order
+    if (tid == 0) {
+      for (uint32_t k = o0; k < o1; ++k) {
+        PgsItem y;
+        pgs_item_load(d, cur, k, y);
+        pgs_item_run(d, p, cur, y, mode);
+      }
+    }
+    grid_sync(d.ctr, sync, epoch);
+  }
+}
+
+__global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
+  __shared__ uint32_t bs[BB_MAX_COLORS + 2];
+  if (threadIdx.x < BB_MAX_COLORS + 2) bs[threadIdx.x] = d.bucket_start[threadIdx.x];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
   const float inv_h = h > 0.f ? 1.0f / h : 0.f;
   const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
+  uint32_t* sync = &d.ctr->sync_count[1];
+  uint32_t epoch = 0;
   for (uint32_t i = tid; i < n; i += stride) store_iw(d, i, world_inv_inertia(q_from(d.rot[i]), f3(d.iinv[i]), tq));
-  grid_barrier(d.ctr);
-  pgs_sweep(d, p, cur, 0, h, hertz);
-  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, h, hertz);
+  grid_sync(d.ctr, sync, epoch);  // also makes bs visible block-wide
+  const uint32_t C = d.ctr->gc_colors;
+  const uint32_t* list = d.bucket_vals[1];
+  // records and rows, each item by the thread that runs it in every sweep (no barrier needed)
+  for (uint32_t c = 0; c < C; ++c)
+    for (uint32_t k = bs[c] + tid; k < bs[c + 1]; k += stride) pgs_item_build(d, cur, k, list[k], h, hertz);
+  if (tid == 0)
+    for (uint32_t k = bs[BB_MAX_COLORS]; k < bs[BB_MAX_COLORS + 1]; ++k) pgs_item_build(d, cur, k, list[k], h, hertz);
+  PgsItem x;
+  if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, cur, bs[0] + tid, x);
+  pgs_sweep(d, p, cur, 0, bs, C, x, epoch);
+  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, C, x, epoch);
   if (p.flags & BB_SIM_ADVECTION) {
-    for (uint32_t i = tid; i < n; i += stride) {
-      if (!awake(d.flags[i])) continue;
-      float4 ps = d.pos[i];
-      float3 v = f3(d.vel[i]);
-      d.pos[i] = make_float4(ps.x + v.x * h, ps.y + v.y * h, ps.z + v.z * h, ps.w);
-      Quatf q = apply_angular_velocity(q_from(d.rot[i]), f3(d.omega[i]), h);
-      d.rot[i] = q_to4(q);
-      store_iw(d, i, world_inv_inertia(q, f3(d.iinv[i]), tq));
-    }
-    grid_barrier(d.ctr);
+    for (uint32_t i = tid; i < n; i += stride)
+      if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
+    grid_sync(d.ctr, sync, epoch);
   }
-  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, h, hertz);
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, C, x, epoch);
 }
 
-int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_COOP_THREADS, sms); }
+int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_PGS_THREADS, sms); }
+
+
+// ---------------------------------------------------------------------------------------
+// PGS_SOFT, dataflow schedule.
+//
+// The per-colour sweeps give every body b the ordered sequence L_b of the manifolds touching
+// it, sorted by (colour, manifold) with the overflow bucket last; one sweep processes L_b in
+// that order, and a manifold's result depends only on its two bodies' states.  So instead of a
+// grid barrier after each colour, each dynamic body carries a sequence counter: the item
+// (phase f, manifold M) waits until counter[b] == f*deg(b) + rank_b(M) (+1 after the integrate
+// item in the relax phases) for both its dynamic bodies, runs, and releases +1 on each.  The
+// outcome is bit-identical to the barrier schedule.  Items are dequeued by warps in queue order
+// (phase, colour, manifold), which is a topological order of the waits, so the schedule cannot
+// deadlock even without co-residency: every wait points at an item dequeued earlier.  Bucket
+// sizes are padded to 32 so a warp's chunk never straddles two colours.
+__device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void flow_wait(DevCounters* c, const uint32_t* ctr, uint32_t target) {
+  uint32_t spins = 0;
+  while (ld_acquire_gpu(ctr) < target) {
+    if (++spins > BB_SPIN_LIMIT) {
+      atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
+      return;
+    }
+  }
+}
+
+// per compact manifold: (slot, body a, body b, rank_a | rank_b << 16) where rank_x is the
+// manifold's position in L_x (colour-major, then manifold order)
+__global__ void k_flow_prep(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    const uint32_t slot = d.man_slot[cur][m];
+    const uint2 b = d.m_bodies[cur][slot];
+    const uint32_t cm = min(d.gc_color[m], uint32_t(BB_MAX_COLORS));
+    uint32_t rank[2] = {0, 0};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const uint32_t x = k == 0 ? b.x : b.y;
+      if (!(d.flags[x] & BB_BODY_DYNAMIC)) continue;
+      const uint32_t s0 = d.csr_start[cur][x], s1 = d.csr_start[cur][x + 1];
+      uint32_t r = 0;
+      for (uint32_t e = s0; e < s1; ++e) {
+        const uint32_t m2 = d.csr_list[cur][e];
+        const uint32_t c2 = min(d.gc_color[m2], uint32_t(BB_MAX_COLORS));
+        r += (c2 < cm || (c2 == cm && m2 < m)) ? 1u : 0u;
+      }
+      rank[k] = r;
+    }
+    d.flow_rec[m] = make_uint4(slot, b.x, b.y, (rank[0] & 0xFFFFu) | (rank[1] << 16));
+  }
+}
+
+// world inverse inertia cache and zeroed sequence counters
+__global__ void k_flow_init(const DevState d, Params p, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  store_iw(d, i, world_inv_inertia(q_from(d.rot[i]), f3(d.iinv[i]), p.quirks & BB_QUIRK_INERTIA_TRANSPOSE));
+  d.flow_counter[i] = 0;
+}
+
+__global__ void __launch_bounds__(256) k_pgs_flow(const DevState d, Params p, int cur, uint32_t n, float h) {
+  __shared__ uint32_t s_pre[BB_MAX_COLORS + 2];    // padded bucket prefix
+  __shared__ uint32_t s_start[BB_MAX_COLORS + 2];  // real bucket starts
+  if (threadIdx.x < BB_MAX_COLORS + 2) s_start[threadIdx.x] = d.bucket_start[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int c = 0; c <= BB_MAX_COLORS; ++c) {
+      s_pre[c] = acc;
+      acc += (s_start[c + 1] - s_start[c] + 31u) & ~31u;
+    }
+    s_pre[BB_MAX_COLORS + 1] = acc;
+  }
+  __syncthreads();
+  const uint32_t L = s_pre[BB_MAX_COLORS + 1];
+  const uint32_t I = p.iterations, Ir = p.relax_iterations;
+  const uint32_t npad = (n + 31u) & ~31u;
+  const uint64_t solve_end = uint64_t(L) * (1 + I);
+  const uint64_t integ_end = solve_end + npad;
+  const uint64_t total = integ_end + uint64_t(L) * Ir;
+  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
+  const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
+  const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
+  const bool advect = p.flags & BB_SIM_ADVECTION;
+  const uint32_t* list = d.bucket_vals[1];
+  const int lane = threadIdx.x & 31;
+  uint32_t* head = &d.ctr->pad[5];
+  for (;;) {
+    uint32_t q0 = 0;
+    if (lane == 0) q0 = atomicAdd(head, 32u);
+    q0 = __shfl_sync(0xFFFFFFFFu, q0, 0);
+    if (uint64_t(q0) >= total) break;
+    const uint64_t q = uint64_t(q0) + lane;
+    if (q >= total) continue;
+    if (q >= solve_end && q < integ_end) {
+      // integrate body i after its pre-step and solve items (RB_sim.slang:1287-1326)
+      const uint32_t i = uint32_t(q - solve_end);
+      if (i >= n || !(d.flags[i] & BB_BODY_DYNAMIC)) continue;
+      const uint32_t deg = d.csr_start[cur][i + 1] - d.csr_start[cur][i];
+      flow_wait(d.ctr, &d.flow_counter[i], (1 + I) * deg);
+      if (advect && awake(d.flags[i])) pgs_integrate(d, i, h, tq);
+      red_release_add(&d.flow_counter[i], 1u);
+      continue;
+    }
+    uint32_t phase, r;
+    if (q < solve_end) {
+      phase = uint32_t(q / L);
+      r = uint32_t(q % L);
+    } else {
+      const uint64_t q2 = q - integ_end;
+      phase = 1 + I + uint32_t(q2 / L);
+      r = uint32_t(q2 % L);
+    }
+    int c = 0;  // bucket: last c with s_pre[c] <= r
+#pragma unroll
+    for (int stepw = 32; stepw > 0; stepw >>= 1)
+      if (c + stepw <= BB_MAX_COLORS && s_pre[c + stepw] <= r) c += stepw;
+    const uint32_t o = r - s_pre[c];
+    if (o >= s_start[c + 1] - s_start[c]) continue;  // padding
+    const uint32_t m = list[s_start[c] + o];
+    const uint4 rec = d.flow_rec[m];
+    const uint2 b = make_uint2(rec.y, rec.z);
+    const bool da = d.flags[b.x] & BB_BODY_DYNAMIC, db = d.flags[b.y] & BB_BODY_DYNAMIC;
+    const uint32_t extra = phase > I ? 1u : 0u;
+    if (da) {
+      const uint32_t deg = d.csr_start[cur][b.x + 1] - d.csr_start[cur][b.x];
+      flow_wait(d.ctr, &d.flow_counter[b.x], phase * deg + (rec.w & 0xFFFFu) + extra);
+    }
+    if (db) {
+      const uint32_t deg = d.csr_start[cur][b.y + 1] - d.csr_start[cur][b.y];
+      flow_wait(d.ctr, &d.flow_counter[b.y], phase * deg + (rec.w >> 16) + extra);
+    }
+    if (phase == 0) pgs_pre_step_slot(d, p, cur, rec.x, b, h, hertz);
+    else pgs_solve_slot(d, p, cur, rec.x, b, phase <= I);
+    if (da) red_release_add(&d.flow_counter[b.x], 1u);
+    if (db) red_release_add(&d.flow_counter[b.y], 1u);
+  }
+}
 
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                        int coop_blocks, int sms) {
-  (void)sms;
+  if (p.schedule == BB_SCHEDULE_DATAFLOW) {
+    k_flow_prep<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
+    k_flow_init<<<(n + BB_THREADS - 1) / BB_THREADS, BB_THREADS, 0, s>>>(d, p, n);
+    k_pgs_flow<<<sms * 8, 256, 0, s>>>(d, p, cur, n, h);
+    return;
+  }
   DevState dd = d;
   Params pp = p;
   int cc = cur;
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
-  bb_launch_coop((const void*)k_pgs_soft, coop_blocks, BB_COOP_THREADS, args, s);
+  bb_launch_coop((const void*)k_pgs_soft, coop_blocks, BB_PGS_THREADS, args, s);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -303,7 +615,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevStat
     uint32_t left = 0;
     for (uint32_t i = tid; i < n; i += stride) {
       if (d.body_color[i] != BB_UNCOLORED || !(d.flags[i] & BB_BODY_DYNAMIC)) continue;
-      const uint32_t mine = avbd_priority(i, rd);
+      const uint32_t mine = avbd_priority(local_id(d, i), rd);
       uint32_t used = 0;
       bool wait = false;
       const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
@@ -314,7 +626,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevStat
         uint32_t pc = *(volatile uint32_t*)&d.body_color[q];
         bool unc = pc == BB_UNCOLORED || (pc >> 8) == rd + 1u;
         if (unc) {
-          if (avbd_priority(q, rd) > mine) wait = true;
+          if (avbd_priority(local_id(d, q), rd) > mine) wait = true;
         } else {
           used |= 1u << (pc & 255u);
         }
@@ -762,7 +1074,7 @@ static void avbd_buckets(cudaStream_t s, const DevState& d, const Params& p, uin
   k_avbd_keys<<<blocks, T, 0, s>>>(d, p, n, post);
   uint32_t* keys[2] = {d.a_bucket_keys[0], d.a_bucket_keys[1]};
   uint32_t* vals[2] = {d.a_bucket_vals[0], d.a_bucket_vals[1]};
-  uint32_t* hist = sc.sort_hist + size_t(region) * 2 * 4 * 256;
+  uint32_t* hist = sc.sort_hist + size_t(region) * BB_HIST_REGION;
   // post keys need 9 bits; three 8-bit passes (the third sees only zero digits, so it keeps
   // the order) leave the result in buffer 1 like the one-pass colour sort
   bb_launch_sort(s, keys, vals, nullptr, n, post ? 3 : 1, 0, hist, sc.sort_status + size_t(slot) * sc.sort_tiles * 256,
@@ -800,14 +1112,14 @@ void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t 
   float hh = h;
   int phase = 0;
   void* args[] = {&dd, &pp, &cc, &nn, &hh, &phase};
-  avbd_buckets(s, d, p, n, sc, sms, 0, 2, 5);
+  avbd_buckets(s, d, p, n, sc, sms, 0, 2, 7);
   bb_launch_coop((const void*)k_avbd_solve, coop_blocks, BB_COOP_THREADS, args, s);
-  avbd_buckets(s, d, p, n, sc, sms, 1, 3, 6);  // slots 6, 7, 8
+  avbd_buckets(s, d, p, n, sc, sms, 1, 3, 8);  // slots 8, 9, 10
   int phase1 = 1;
   void* args1[] = {&dd, &pp, &cc, &nn, &hh, &phase1};
   bb_launch_coop((const void*)k_avbd_solve, coop_blocks, BB_COOP_THREADS, args1, s);
   if (p.avbd_post_stab_sweeps > 1) {
-    avbd_buckets(s, d, p, n, sc, sms, 0, 4, 9);
+    avbd_buckets(s, d, p, n, sc, sms, 0, 4, 11);
     int phase2 = 2;
     void* args2[] = {&dd, &pp, &cc, &nn, &hh, &phase2};
     bb_launch_coop((const void*)k_avbd_solve, coop_blocks, BB_COOP_THREADS, args2, s);

@@ -58,6 +58,8 @@ uint64_t fnv(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull
 }
 }  // namespace
 
+bb_status bb_fail(bb_status code, const char* msg) { return fail(code, msg); }
+
 int bb_coop_blocks(const void* kernel, int threads, int sms) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
@@ -128,6 +130,7 @@ __global__ void k_begin_substep(DevCounters* c) {
     c->bounds_max[k] = 0u;
   }
   for (int k = 0; k < 6; ++k) c->pad[k] = 0;
+  for (int k = 0; k < 8; ++k) c->sync_count[k] = 0;
   c->substeps += 1;
 }
 
@@ -198,6 +201,15 @@ struct bb_world_impl {
       d.csr_list[k] = u32(2 * P);
     }
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
+    d.flow_rec = dalloc<uint4>(P, owned, err);
+    d.pgs_rec = dalloc<uint4>(P, owned, err);
+    d.pgs_mass = f4(P);
+    d.flow_counter = u32(N);
+    d.range_first = dalloc<int32_t>(N, owned, err);
+    d.sworld = u32(N);
+    d.world_of = u32(N); d.world_first = u32(N); d.world_count = u32(N);
+    d.world_bounds = f4(2 * N);
+    d.n_worlds = 0;
     d.csr_cursor = u32(N + 1);
     d.hit = u32(P); d.man_index = u32(P);
     d.uf_parent = u32(N); d.is_root = u32(N); d.root_rank = u32(N); d.island = u32(N);
@@ -218,8 +230,8 @@ struct bb_world_impl {
     sc.scan_tiles = bb_scan_tiles(std::max<size_t>(P, N + 1));
     sc.sort_tiles = bb_sort_tiles(std::max<size_t>(P, N));
     size_t scan_words = size_t(4) * sc.scan_tiles;  // 64-bit
-    size_t sort_status_words = size_t(10) * sc.sort_tiles * 256;
-    size_t hist_words = 10 * 4 * 256;
+    size_t sort_status_words = size_t(12) * sc.sort_tiles * 256;
+    size_t hist_words = 5 * BB_HIST_REGION;
     scratch_bytes = scan_words * 8 + 16 * 4 + hist_words * 4 + sort_status_words * 4 + 16 * 4;
     char* base = static_cast<char*>(static_cast<void*>(dalloc<uint8_t>(scratch_bytes + 256, owned, err)));
     if (err != cudaSuccess) return fail(BB_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
@@ -381,8 +393,7 @@ bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape) {
   return BB_OK;
 }
 
-bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id) {
-  World* w = W(world);
+static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id) {
   if (!w || (!bodies && count)) return fail(BB_E_INVALID, "bb_add_bodies: bad arguments");
   if (uint64_t(w->n) + count > w->cap_n) return fail(BB_E_CAPACITY, "bb_add_bodies: max_bodies exceeded");
   std::vector<float4> pos(count), rot(count), vel(count), om(count), shp(count), ii(count);
@@ -455,6 +466,39 @@ bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t count,
   CU(cudaMemcpy(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice));
   return BB_OK;
 }
+
+bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id) {
+  World* w = W(world);
+  if (w && w->d.n_worlds > 0) return fail(BB_E_INVALID, "bb_add_bodies: this object holds batched worlds");
+  return add_bodies_impl(w, bodies, count, out_first_id);
+}
+
+bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_body_desc* bodies, uint32_t count,
+                       uint32_t* out_world_index, uint32_t* out_first_id) {
+  World* w = W(world);
+  if (!w || !desc || count == 0) return fail(BB_E_INVALID, "bb_add_world: bad arguments");
+  if (w->d.n_worlds == 0 && w->n > 0) return fail(BB_E_INVALID, "bb_add_world: object already holds a plain world");
+  for (int k = 0; k < 3; ++k)
+    if (!(desc->world_extent[k] > 0)) return fail(BB_E_INVALID, "bb_add_world: world_extent must be positive");
+  uint32_t first = 0;
+  bb_status st = add_bodies_impl(w, bodies, count, &first);
+  if (st != BB_OK) return st;
+  const uint32_t widx = w->d.n_worlds;
+  std::vector<uint32_t> wof(count, widx);
+  CU(cudaMemcpy(w->d.world_of + first, wof.data(), 4ull * count, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.world_first + widx, &first, 4, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(w->d.world_count + widx, &count, 4, cudaMemcpyHostToDevice));
+  float4 bnd[2] = {make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
+                   make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f)};
+  CU(cudaMemcpy(w->d.world_bounds + 2 * widx, bnd, sizeof(bnd), cudaMemcpyHostToDevice));
+  w->d.n_worlds = widx + 1;
+  w->invalidate_graphs();
+  if (out_world_index) *out_world_index = widx;
+  if (out_first_id) *out_first_id = first;
+  return BB_OK;
+}
+
+uint32_t bb_world_count(void* world) { return world ? W(world)->d.n_worlds : 0; }
 
 bb_status bb_set_material(void* world, uint32_t first, uint32_t count, float friction, float restitution) {
   World* w = W(world);

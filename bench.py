@@ -37,19 +37,36 @@ L2_BYTES = 126 * 1024 * 1024
 
 
 def workload(args):
-    sc = scenes.mixed_column(n_bodies=args.bodies, seed=0)
-    name = (f"mixed_column_{args.bodies // 1000}k: {args.bodies} bodies (60% boxes / 40% spheres) in a "
-            f"60x60x200 m column, 5-wall container, dt=1/60, {SUBSTEPS} substeps, ")
+    if args.scene == "pyramids":
+        n_pyr = max(1, args.bodies // 1000)
+        sc = scenes.pyramids(n_pyramids=n_pyr, boxes_per=1000, seed=0)
+        name = (f"pyramids_{n_pyr}x1000: {n_pyr} pyramids of 1000 unit boxes (base 18x18) on a 32x32 grid, "
+                f"velocity N(0, 0.01) m/s, dt=1/60, {SUBSTEPS} substeps, ")
+    else:
+        sc = scenes.mixed_column(n_bodies=args.bodies, seed=0)
+        name = (f"mixed_column_{args.bodies // 1000}k: {args.bodies} bodies (60% boxes / 40% spheres) in a "
+                f"60x60x200 m column, 5-wall container, dt=1/60, {SUBSTEPS} substeps, ")
     if args.solver == "pgs":
-        name += "PGS_SOFT 10 iterations"
+        name += f"PGS_SOFT 10 iterations ({args.schedule} schedule)"
     else:
         name += "AVBD 4 iterations (beta=10)"
     return sc, name
 
 
+def run_steps(args) -> int:
+    """Length of the configuration's run: 600 steps for the mixed column, 300 for the pyramids."""
+    return 300 if args.scene == "pyramids" else 600
+
+
+def timed_window(args) -> int:
+    """First timed step: centred on the run, never before the W warm-up steps."""
+    return max(args.warmup, run_steps(args) // 2 - args.steps // 2)
+
+
 def solver_fields(args) -> dict:
     if args.solver == "pgs":
-        return dict(solver=1, iterations=10, relax_iterations=10, quirks=0)
+        return dict(solver=1, iterations=10, relax_iterations=10, quirks=0,
+                    schedule=0 if args.schedule == "dataflow" else 1)
     return dict(solver=2, avbd_iterations=4, avbd_beta=10.0, quirks=0)
 
 
@@ -131,13 +148,12 @@ def run_reference(args, rank: int, world_size: int):
     p.world_extent[:] = sc["bounds"][1]
     o = pyoracle.Oracle(sc, double=False, threads=threads, params=p)
     budget = args.ref_budget_s
+    first = timed_window(args)
     t0 = time.time()
-    warm = 0
-    for _ in range(args.warmup):
+    done = 0  # untimed steps: pre-roll to the timed window (bounded by the budget), then warm-up
+    while done < first and (first - done <= args.warmup or time.time() - t0 < budget):
         o.step(DT, SUBSTEPS)
-        warm += 1
-        if time.time() - t0 > budget / 3:
-            break
+        done += 1
     t1 = time.time()
     steps = 0
     while steps < args.steps:
@@ -147,8 +163,10 @@ def run_reference(args, rank: int, world_size: int):
             break
     el = time.time() - t1
     v = sc["n"] * steps / el
-    sample = (f"{steps} of {args.steps} timed steps (after {warm} warm-up steps) of the full {sc['n']}-body world, "
-              f"FP32 oracle, {threads} threads")
+    sample = (f"steps {done}..{done + steps - 1} of the {run_steps(args)}-step run ({steps} of the {args.steps} "
+              f"timed steps; the window starts at step {first}, fewer if the {budget:.0f} s pre-roll budget ran out) "
+              f"of the full {sc['n']}-body world, FP32 oracle, {threads} threads")
+    warm = done
     line = {"impl": "reference", "metric": "body-steps/s", "value": v, "unit": "body-steps/s", "n_gpus": world_size,
             "steps": steps, "warmup": warm, "ms_per_step": 1000 * el / max(steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
@@ -183,12 +201,20 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         w.set_params(p, **fields)
         return w
 
+    # The configuration is a run of RUN_STEPS steps whose cost per step grows as the pile forms;
+    # K timed steps are centred on that run (untimed pre-roll first), so a short K still
+    # measures a representative part of it, and K >= RUN_STEPS - W times the whole run.
+    first = timed_window(args)
+
+    def roll(world):
+        for _ in range(first):
+            world.step(DT, SUBSTEPS)
+        world.sync()
+
     w = make_world()
     stream = torch.cuda.ExternalStream(w.stream)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
-    for _ in range(args.warmup):
-        w.step(DT, SUBSTEPS)
-    w.sync()
+    roll(w)
     warm_state = w.read_state()
     warm_flags = w.read_flags()
     n = w.n
@@ -219,14 +245,12 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
 
     # end to end through the public API with pinned host buffers: upload state, step, read back
     w2 = make_world()
-    for _ in range(args.warmup):
-        w2.step(DT, SUBSTEPS)
-    w2.sync()
+    roll(w2)  # the same deterministic history: both measurements cover the same steps
     pin = lambda shape: torch.empty(shape, dtype=torch.float32).pin_memory().numpy()  # noqa: E731
     host = {k: pin(v.shape) for k, v in warm_state.items()}
     for k in host:
         host[k][...] = w2.read_state()[k]
-    e2e_steps = max(1, min(args.steps, 60))
+    e2e_steps = args.steps  # the same steps as the device-timed run
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
@@ -274,7 +298,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                 "data": "synthetic (seeded scene, seed 0)",
                 "config": {"workload": name, "bodies": n, "substeps": SUBSTEPS, "dt": DT,
                            "parallelism": f"replicas x{world_size}", "l2": "flushed before every timed step",
-                           "timed_steps": f"steps {args.warmup}..{args.warmup + args.steps - 1} from the initial column"},
+                           "timed_steps": f"steps {first}..{first + args.steps - 1} of the {run_steps(args)}-step run "
+                                          f"(the last {args.warmup} untimed steps before them are the warm-up)"},
                 "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": io_bytes,
                         "d2h_bytes_per_step": io_bytes, "steps": e2e_steps,
                         "what": "bb_write_state + bb_step + bb_read_state with pinned host buffers"},
@@ -323,6 +348,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="pgs", choices=["pgs", "avbd"])
     ap.add_argument("--bodies", type=int, default=N_BODIES)
+    ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids"],
+                    help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids")
+    ap.add_argument("--schedule", default="dataflow", choices=["dataflow", "barrier"],
+                    help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget-s", type=float, default=150.0)
     args = ap.parse_args()

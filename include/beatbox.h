@@ -84,6 +84,14 @@ typedef int32_t bb_status;
                               src/shaders/simulation/RB_sim.slang:96-101) */
 #define BB_BOUNDS_AUTO 1u  /* per substep: min/max of body positions */
 
+/* ---- colour-sweep schedules ------------------------------------------------------------
+ * DATAFLOW: every (sweep, manifold) item waits on per-body sequence counters for exactly the
+ * items that precede it on its two bodies in (sweep, colour, manifold) order -- the order the
+ * reference's per-colour dispatches impose -- so no grid-wide barrier is needed.
+ * COLOUR_BARRIER: one grid barrier between colours, as the reference's dispatch sequence. */
+#define BB_SCHEDULE_DATAFLOW 0u
+#define BB_SCHEDULE_COLOUR_BARRIER 1u
+
 /* Solver and material parameters.  Every reference constant is a field whose default (from
  * bb_default_solver_params) is the reference value; replaces StatusManager::set_solver /
  * flag toggles (src/status_manager.hpp:204-373) and the compile-time constants of
@@ -116,6 +124,8 @@ typedef struct bb_solver_params {
   uint32_t avbd_color_rounds;  /* 16 */
   uint32_t avbd_shock_layers;  /* 12 */
   uint32_t avbd_post_stab_sweeps; /* 4 */
+  /* execution schedule of the colour sweeps (results are identical either way) */
+  uint32_t schedule;           /* BB_SCHEDULE_* (default BB_SCHEDULE_DATAFLOW) */
   /* Morton normalisation */
   uint32_t bounds_mode;        /* BB_BOUNDS_* */
   float world_min[3];          /* default -64 */
@@ -237,6 +247,20 @@ bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape);
  * (src/rigid_body_manager.cpp:90-119,1695-1712). */
 bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t n, uint32_t* out_first_id);
 
+/* Batched worlds: append an independent world of n bodies (its own ground included) to a
+ * world object; bodies of different worlds never interact.  Ids stay consecutive per world
+ * (*out_first_id); keys sort by (world, Morton code), the LBVH keeps each world in one subtree,
+ * and colouring priorities use world-local ids, so every world evolves exactly as it would
+ * alone.  world_min/world_extent: the world's Morton normalisation box.  Not mixable with
+ * bb_add_bodies on the same object.  No reference counterpart (the reference is one world). */
+typedef struct bb_batch_world_desc {
+  float world_min[3];
+  float world_extent[3];
+} bb_batch_world_desc;
+bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_body_desc* bodies, uint32_t n,
+                       uint32_t* out_world_index, uint32_t* out_first_id);
+uint32_t bb_world_count(void* world);
+
 /* Change the friction/restitution of bodies [first, first+n).  No separate reference
  * entry point (materials are per body, shared.inl:360-361). */
 bb_status bb_set_material(void* world, uint32_t first, uint32_t n, float friction, float restitution);
@@ -288,6 +312,15 @@ bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint3
                               char* names, uint32_t names_bytes);
 /* Number of kernels this library launched on the world's stream since creation. */
 uint64_t bb_kernel_launch_count(void* world);
+
+/* Stable LSD radix sort of n (key, value) pairs held in DEVICE memory: keys_out/vals_out
+ * receive the pairs ordered by the low key_bits (1..32) of the key, ties kept in input order.
+ * The step's Morton-code sort (onesweep with decoupled look-back), exposed on caller arrays;
+ * the reference sorts inside its task graph (src/shaders/simulation/RB_sim.slang:113-203,
+ * LBVH.slang:34-152).  Asynchronous on `stream` (cudaStream_t, NULL = legacy default).
+ * Its scratch is allocated with cudaMalloc on first use per device and reused afterwards. */
+bb_status bb_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                              uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
 
 /* Last error message of the calling thread (static storage, never NULL). */
 const char* bb_last_error_string(void);

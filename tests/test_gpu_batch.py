@@ -1,0 +1,148 @@
+"""GPU tests of the batched-worlds mode and of the two PGS schedules.
+
+Both are pure reorganisations of the same arithmetic, so the bar is bitwise equality:
+  * a world stepped inside a batch equals the same world stepped alone (its body ids are
+    shifted by the world's first id; every hash, sort and traversal works on world-local
+    ids and per-world ranges);
+  * the dataflow PGS schedule (per-body sequence counters) equals the colour-barrier
+    schedule (grid barrier between colours), since every body still sees its constraints
+    in colour order.
+"""
+import numpy as np
+import pytest
+
+import beatbox as bb
+from beatbox import scenes
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+
+
+def scene_bounds(sc, margin=4.0):
+    if sc.get("bounds") is not None:
+        return sc["bounds"]
+    lo = sc["pos"].min(axis=0) - margin
+    hi = sc["pos"].max(axis=0) + margin
+    return lo.tolist(), np.maximum(hi - lo, 1.0).tolist()
+
+
+def small_column(seed):
+    return scenes.mixed_column(n_bodies=400, seed=seed)
+
+
+def tiny_stack():
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50])
+    sb.add([[0, 0.5 + 1.0 * k, 0] for k in range(5)], [[0, 0, 0, 1]] * 5, [[0.5] * 3] * 5, 0,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1.0)
+    return sb.build()
+
+
+WORLDS = [
+    lambda: scenes.box_grid(n_side=5, layers=3),
+    lambda: small_column(3),
+    tiny_stack,
+    lambda: scenes.pyramids(n_pyramids=2, boxes_per=55, gap=-0.002),
+    lambda: small_column(4),
+]
+
+
+def params(solver, **kw):
+    p = bb.make_params(solver=solver, quirks=bb.QUIRKS_PHYSICAL, **kw)
+    if solver == bb.SOLVER_AVBD:
+        p.avbd_iterations = 4
+    return p
+
+
+def run_batch(scs, p, steps, substeps):
+    total = sum(int(s["n"]) for s in scs)
+    w = bb.World(total)
+    firsts = []
+    for k, sc in enumerate(scs):
+        lo, ext = scene_bounds(sc)
+        wi, first = w.add_world(sc, lo, ext)
+        assert wi == k
+        firsts.append(first)
+    assert w.n_worlds == len(scs)
+    w.set_params(p)
+    for _ in range(steps):
+        w.step(DT, substeps)
+    st = w.read_state()
+    stats = w.stats()
+    w.close()
+    return [{k: v[f:f + int(sc["n"])] for k, v in st.items()} for f, sc in zip(firsts, scs)], stats
+
+
+@pytest.mark.parametrize("solver", [bb.SOLVER_PGS_SOFT, bb.SOLVER_AVBD])
+def test_batched_world_equals_world_alone(solver):
+    scs = [f() for f in WORLDS]
+    p = params(solver)
+    batch, stats = run_batch(scs, p, steps=30, substeps=2)
+    assert stats["error_flags"] == 0
+    for k, sc in enumerate(scs):
+        alone, _ = run_batch([sc], p, steps=30, substeps=2)
+        for key in alone[0]:
+            assert np.array_equal(batch[k][key], alone[0][key]), (k, key)
+
+
+def test_overlapping_worlds_never_interact():
+    """Three copies of one scene occupying the same space: with no cross-world pairs every
+    copy evolves exactly like the scene alone."""
+    sc = small_column(5)
+    p = params(bb.SOLVER_PGS_SOFT)
+    batch, _ = run_batch([sc, sc, sc], p, steps=40, substeps=2)
+    alone, _ = run_batch([sc], p, steps=40, substeps=2)
+    for k in range(3):
+        for key in alone[0]:
+            assert np.array_equal(batch[k][key], alone[0][key]), (k, key)
+
+
+def test_batched_pairs_stay_inside_worlds():
+    scs = [small_column(6), small_column(6)]
+    total = sum(int(s["n"]) for s in scs)
+    w = bb.World(total)
+    for sc in scs:
+        w.add_world(sc, *scene_bounds(sc))
+    w.set_params(params(bb.SOLVER_PGS_SOFT))
+    for _ in range(20):
+        w.step(DT, 1)
+    w.debug_collide(2)
+    man = w.debug_read("manifolds")
+    n0 = int(scs[0]["n"])
+    assert len(man) > 0
+    wa = man["body_a"] >= n0
+    wb = man["body_b"] >= n0
+    assert np.array_equal(wa, wb)
+    assert 0 < wa.sum() < len(man)
+
+
+def test_mixing_plain_and_batched_is_rejected():
+    sc = tiny_stack()
+    w = bb.World(64)
+    w.add_world(sc, *scene_bounds(sc))
+    with pytest.raises(bb.BeatboxError):
+        w.add_scene(sc)
+    w.close()
+    w = bb.World(64)
+    w.add_scene(sc)
+    with pytest.raises(bb.BeatboxError):
+        w.add_world(sc, *scene_bounds(sc))
+    w.close()
+
+
+@pytest.mark.parametrize("name", ["mixed_3000", "pyramids_4x300"])
+def test_dataflow_schedule_equals_colour_barrier(name):
+    sc = (scenes.mixed_column(n_bodies=3000, seed=2) if name == "mixed_3000"
+          else scenes.pyramids(n_pyramids=4, boxes_per=300, gap=-0.002))
+    outs = []
+    for schedule in (bb.SCHEDULE_DATAFLOW, bb.SCHEDULE_COLOUR_BARRIER):
+        p = params(bb.SOLVER_PGS_SOFT, schedule=schedule)
+        w = bb.world_from_scene(sc, params=p)
+        for _ in range(40):
+            w.step(DT, 4)
+        outs.append(w.read_state())
+        assert w.stats()["error_flags"] == 0
+        w.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k

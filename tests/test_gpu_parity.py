@@ -68,7 +68,7 @@ def single_scene(n):
 FRONT_SCENES = {
     "box_grid_1000": lambda: scenes.box_grid(),
     "mixed_2000": lambda: scenes.mixed_column(n_bodies=2000, seed=1),
-    "pyramids_2x1000": lambda: scenes.pyramids(n_pyramids=2, boxes_per=1000),
+    "pyramids_2x1000": lambda: scenes.pyramids(n_pyramids=2, boxes_per=1000, gap=-0.002),
     "duplicates": dup_scene,
     "one_body": lambda: single_scene(1),
     "two_bodies": lambda: single_scene(2),
@@ -227,7 +227,8 @@ def test_avbd_colouring_valid_and_matches_oracle(oracle_lib):
 
 
 def test_capacity_overflow_is_reported(oracle_lib):
-    sc = scenes.pyramids(n_pyramids=1, boxes_per=1000)
+    # overlapping boxes: every box pairs with up to 26 neighbours, far above one pair per body
+    sc = scenes.pyramids(n_pyramids=1, boxes_per=1000, gap=-0.002)
     w = bb.World(sc["n"], pairs_per_body=1)
     w.add_scene(sc)
     w.step(DT, 1)
