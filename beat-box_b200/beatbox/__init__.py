@@ -35,6 +35,7 @@ QUIRK_GRAVITY_IMPULSE, QUIRK_SAT_FRAME, QUIRK_INERTIA_TRANSPOSE = 1, 2, 4
 QUIRKS_REFERENCE, QUIRKS_PHYSICAL = 7, 0
 BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
 SCHEDULE_DATAFLOW, SCHEDULE_COLOUR_BARRIER = 0, 1
+SORT_STATIC_MAX_KEYS = 262144
 DBG = dict(morton=1, sorted_keys=2, sorted_ids=3, lbvh_child=4, leaf_aabb=5, node_aabb=6, pairs=7,
            manifolds=8, contacts=9, edge_colors=10, body_colors=11, islands=12, support_depth=13)
 
@@ -126,6 +127,7 @@ _SIG = {
     "bb_read_stage_times": (ctypes.c_int32, [_P, _P, _U32, ctypes.POINTER(_U32), _P, _U32]),
     "bb_kernel_launch_count": (ctypes.c_uint64, [_P]),
     "bb_radix_sort_pairs": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
+    "bb_radix_sort_pairs_static": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_last_error_string": (ctypes.c_char_p, []),
     "bb_version": (ctypes.c_char_p, []),
 }

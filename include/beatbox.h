@@ -322,6 +322,17 @@ uint64_t bb_kernel_launch_count(void* world);
 bb_status bb_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                               uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
 
+/* bb_radix_sort_pairs with the same results that allocates nothing: its scratch (about 2.6 MB)
+ * is a fixed device array in the library, so n is limited to BB_SORT_STATIC_MAX_KEYS (larger n
+ * returns BB_E_INVALID).  The first call on a device (with that device current) looks the
+ * array's address up; make it before any stream capture.  Every call clears the part of the
+ * scratch that must start at zero on `stream` itself.  Calls on one device share the scratch:
+ * calls that overlap in time (different streams without ordering, several host threads) race
+ * and give wrong results.  No counterpart in the reference. */
+#define BB_SORT_STATIC_MAX_KEYS 262144u
+bb_status bb_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                     uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
+
 /* Last error message of the calling thread (static storage, never NULL). */
 const char* bb_last_error_string(void);
 /* Library version string. */
