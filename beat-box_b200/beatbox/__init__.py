@@ -57,7 +57,8 @@ class SolverParams(ctypes.Structure):
         ("avbd_k_min", ctypes.c_float), ("avbd_k_max", ctypes.c_float), ("avbd_margin", ctypes.c_float),
         ("avbd_stick_thresh", ctypes.c_float), ("avbd_stick_slop", ctypes.c_float),
         ("avbd_color_rounds", ctypes.c_uint32), ("avbd_shock_layers", ctypes.c_uint32),
-        ("avbd_post_stab_sweeps", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
+        ("avbd_post_stab_sweeps", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("broad_threads", ctypes.c_uint32),
+        ("narrow_blocks_per_sm", ctypes.c_uint32), ("flow_blocks_per_sm", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
         ("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3),
     ]
 
@@ -72,6 +73,13 @@ class BodyDesc(ctypes.Structure):
                 ("omega", ctypes.c_float * 3), ("shape", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("mass", ctypes.c_float), ("density", ctypes.c_float), ("friction", ctypes.c_float),
                 ("restitution", ctypes.c_float), ("inertia_mode", ctypes.c_uint32), ("inv_inertia", ctypes.c_float * 3)]
+
+
+BODY_DTYPE = np.dtype([("position", "<f4", 3), ("rotation", "<f4", 4), ("velocity", "<f4", 3), ("omega", "<f4", 3),
+                       ("shape", "<u4"), ("flags", "<u4"), ("mass", "<f4"), ("density", "<f4"),
+                       ("friction", "<f4"), ("restitution", "<f4"), ("inertia_mode", "<u4"),
+                       ("inv_inertia", "<f4", 3)])
+assert BODY_DTYPE.itemsize == ctypes.sizeof(BodyDesc)
 
 
 class BatchWorldDesc(ctypes.Structure):
@@ -128,6 +136,7 @@ _SIG = {
     "bb_kernel_launch_count": (ctypes.c_uint64, [_P]),
     "bb_radix_sort_pairs": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_radix_sort_pairs_static": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
+    "bb_autotune": (ctypes.c_int32, [_P, ctypes.c_float, _U32, _U32, ctypes.POINTER(SolverParams)]),
     "bb_last_error_string": (ctypes.c_char_p, []),
     "bb_version": (ctypes.c_char_p, []),
 }
@@ -224,22 +233,22 @@ class World:
         return h
 
     def _scene_descs(self, scene: dict, inertia_mode: int):
+        """bb_body_desc array of a scene, filled column-wise through a numpy view."""
         n = int(scene["n"])
         descs = (BodyDesc * n)()
-        for i in range(n):
-            d = descs[i]
-            d.position[:] = scene["pos"][i].tolist()
-            d.rotation[:] = scene["quat"][i].tolist()
-            d.velocity[:] = scene["vel"][i].tolist()
-            d.omega[:] = scene["omega"][i].tolist()
-            d.shape = self._shape_for(int(scene["shape"][i]), scene["half"][i])
-            d.flags = int(scene["flags"][i])
-            d.mass = float(scene["mass"][i])
-            d.density = 0.0
-            d.friction = float(scene["friction"][i])
-            d.restitution = float(scene["restitution"][i])
-            d.inertia_mode = inertia_mode
-            d.inv_inertia[:] = scene["inv_inertia"][i].tolist()
+        a = np.frombuffer(descs, dtype=BODY_DTYPE, count=n)
+        a["position"] = scene["pos"]
+        a["rotation"] = scene["quat"]
+        a["velocity"] = scene["vel"]
+        a["omega"] = scene["omega"]
+        a["shape"] = [self._shape_for(int(t), h) for t, h in zip(scene["shape"].tolist(), scene["half"].tolist())]
+        a["flags"] = scene["flags"]
+        a["mass"] = scene["mass"]
+        a["density"] = 0.0
+        a["friction"] = scene["friction"]
+        a["restitution"] = scene["restitution"]
+        a["inertia_mode"] = inertia_mode
+        a["inv_inertia"] = scene["inv_inertia"]
         return descs, n
 
     def add_scene(self, scene: dict, inertia_mode: int = INERTIA_EXPLICIT) -> int:
@@ -295,6 +304,14 @@ class World:
     # ---- stepping ------------------------------------------------------------------------
     def step(self, dt: float, substeps: int = 1):
         _check(self.L.bb_step(self.h, ctypes.c_float(dt), substeps))
+
+    def autotune(self, dt: float, substeps: int = 1, trial_steps: int = 2) -> dict:
+        """Time launch geometries / schedules on this world (each trial step advances it) and keep
+        the fastest; returns the chosen tunables."""
+        p = SolverParams()
+        _check(self.L.bb_autotune(self.h, dt, substeps, trial_steps, ctypes.byref(p)))
+        return dict(schedule=p.schedule, broad_threads=p.broad_threads, narrow_blocks_per_sm=p.narrow_blocks_per_sm,
+                    flow_blocks_per_sm=p.flow_blocks_per_sm)
 
     def sync(self):
         _check(self.L.bb_sync(self.h))

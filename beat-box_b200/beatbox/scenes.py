@@ -252,3 +252,42 @@ def pyramids(n_pyramids: int = 1000, boxes_per: int = 1000, seed: int = 0, densi
            density, friction=friction, vel=vel)
     sb.bounds = ([-extent / 2 - 12, -2.0, -extent / 2 - 12], [extent + 24, extent + 24, extent + 24])
     return sb.build()
+
+
+def pile(n_bodies: int, seed: int = 0, sphere_fraction: float = 0.4, density: float = 1000.0,
+         friction: float = 0.5, inertia: str = "physical") -> dict:
+    """A config-1 style pile scaled to n_bodies: unit boxes (half extent 0.5) and spheres
+    (radius 0.5) in a jittered grid, side = ceil(n^(1/3)) columns per axis and as many layers as
+    needed, 1.1 m spacing, 0.1 m above the ground top, per-axis jitter U(+-0.05), yaw U[0, 2 pi);
+    a random sphere_fraction of the slots holds spheres.  Ground: static box centred at
+    (0, -50, 0), half extent 50.  The scene's Morton box covers the pile with a 4 m margin."""
+    side = max(1, int(math.ceil(n_bodies ** (1.0 / 3.0) - 1e-9)))
+    per_layer = side * side
+    k = np.arange(n_bodies)
+    ly, rem = np.divmod(k, per_layer)
+    lz, lx = np.divmod(rem, side)
+    off = (side - 1) * 1.1 * 0.5
+    pos = np.stack([lx * 1.1 - off, 0.6 + ly * 1.1, lz * 1.1 - off], axis=1).astype(np.float64)
+    pos += np.stack([uniform(seed, 1 + a, n_bodies, -0.05, 0.05) for a in range(3)], axis=1)
+    quat = yaw_rotations(uniform(seed, 4, n_bodies, 0.0, 2 * math.pi))
+    is_sph = uniform(seed, 5, n_bodies) < sphere_fraction
+    flags = BODY_DYNAMIC | BODY_GRAVITY
+    sb = SceneBuilder(inertia)
+    sb.add_static_box([0.0, -50.0, 0.0], [50.0, 50.0, 50.0], friction=friction)
+    box = ~is_sph
+    if box.any():
+        sb.add(pos[box], quat[box], np.full((int(box.sum()), 3), 0.5), SHAPE_BOX, flags, density * 1.0,
+               friction=friction)
+    if is_sph.any():
+        ns = int(is_sph.sum())
+        sb.add(pos[is_sph], quat[is_sph], np.full((ns, 3), 0.5), SHAPE_SPHERE, flags,
+               density * (4.0 / 3.0) * math.pi * 0.125, friction=friction)
+    height = 0.6 + (int(ly.max()) + 1) * 1.1
+    sb.bounds = ([-off - 4.0, -4.0, -off - 4.0], [2 * off + 8.0, height + 8.0, 2 * off + 8.0])
+    return sb.build()
+
+
+def batch_sizes(n_worlds: int, seed: int = 0, lo: int = 16, hi: int = 2048) -> np.ndarray:
+    """Body counts of a batch: floor(exp(U(ln lo, ln hi))) per world."""
+    u = uniform(seed, 90, n_worlds, math.log(lo), math.log(hi))
+    return np.floor(np.exp(u)).astype(np.int64)

@@ -217,6 +217,7 @@ __global__ void k_refit(const DevState d, uint32_t n) {
 // A query that visits more than BB_BP_BUDGET nodes (a huge static body: floor, walls) is
 // handed to k_broad_heavy, which splits its traversal over a block.
 #define BB_BP_BUDGET 512u
+#define BB_BP_STAGE 16u  // partners per query kept from the counting traversal
 #define BB_HEAVY_CAP 1024u
 #define BB_FRONTIER 256
 
@@ -233,7 +234,9 @@ __device__ __forceinline__ int world_end(const DevState& d, uint32_t qi, uint32_
   return int(d.world_first[w] + d.world_count[w]);
 }
 
-// Left-first traversal for sorted query i.  EMIT=false counts, EMIT=true writes.
+// Left-first traversal for sorted query i.  EMIT=false counts every partner and keeps the first
+// BB_BP_STAGE of them in bp_stage (so k_broad_copy can place them once offsets are known);
+// EMIT=true re-walks only the queries that had more (is_heavy == 2) and writes their pairs.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
     }
     return;
   }
-  if (EMIT && d.is_heavy[i]) return;
+  if (EMIT && d.is_heavy[i] != 2u) return;
   const int N = int(n);
   const int leaf0 = N - 1;
   float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
@@ -273,6 +276,8 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
         uint32_t k = out + count;
         if (k < cap) d.pairs[k] = make_uint2(i, uint32_t(node - leaf0));
         else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+      } else if (count < BB_BP_STAGE) {
+        d.bp_stage[size_t(i) * BB_BP_STAGE + count] = uint32_t(node - leaf0);
       }
       ++count;
       continue;
@@ -289,7 +294,20 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
   }
   if (!EMIT) {
     d.pair_cnt[i] = count;
-    d.is_heavy[i] = 0;
+    d.is_heavy[i] = count > BB_BP_STAGE ? 2u : 0u;
+  }
+}
+
+// pairs of the queries whose partners all fit in bp_stage, one thread per staged slot
+__global__ void k_broad_copy(const DevState d, uint32_t n) {
+  const size_t total = size_t(n) * BB_BP_STAGE;
+  const uint32_t cap = d.pair_capacity;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t i = uint32_t(t / BB_BP_STAGE), k = uint32_t(t % BB_BP_STAGE);
+    if (d.is_heavy[i] != 0u || k >= d.pair_cnt[i]) continue;
+    const uint32_t o = d.pair_off[i] + k;
+    if (o < cap) d.pairs[o] = make_uint2(i, d.bp_stage[t]);
+    else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
   }
 }
 
@@ -435,11 +453,13 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   }
   k_build<<<blocks, T, 0, s>>>(d, n);
   k_refit<<<blocks, T, 0, s>>>(d, n);
-  uint32_t bb = (n + 127) / 128;
+  const uint32_t bt = p.broad_threads ? p.broad_threads : 128u;
+  uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);
-  k_broad<false><<<bb, 128, 0, s>>>(d, n);
+  k_broad<false><<<bb, bt, 0, s>>>(d, n);
   k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n);
   bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr);
-  k_broad<true><<<bb, 128, 0, s>>>(d, n);
+  k_broad_copy<<<sms * 16, 256, 0, s>>>(d, n);
+  k_broad<true><<<bb, bt, 0, s>>>(d, n);
   k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n);
 }

@@ -55,7 +55,7 @@ struct DevCounters {
   uint32_t bounds_min[3];  // BB_BOUNDS_AUTO: ordered-float min/max of positions
   uint32_t bounds_max[3];
   uint32_t avbd_body_count;
-  uint32_t substeps;       // substeps run since the last stats read
+  uint32_t substeps;       // substeps run since the world was created
   uint32_t pad[6];
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD
@@ -76,7 +76,8 @@ struct DevState {
   int32_t* range_last;          // last leaf covered by each internal node
   uint32_t* visit;              // refit arrival counters
   uint32_t *pair_cnt, *pair_off;  // per query
-  uint32_t *is_heavy, *heavy_list;  // queries over the visit budget (block-cooperative)
+  uint32_t *is_heavy, *heavy_list;  // 1: over the visit budget (block-cooperative), 2: staging spilled
+  uint32_t* bp_stage;           // first 16 partners of each query (counting traversal)
   uint2* pairs;                 // (sorted a, sorted b)
   // manifolds (two buffers: [cur], [prev] chosen by parity)
   uint2* m_bodies[2];    // body ids (a, b) per slot
@@ -103,6 +104,9 @@ struct DevState {
   // skip << 10), mass = (inverse mass a, inverse mass b, friction, -)
   uint4* pgs_rec;
   float4* pgs_mass;
+  float4* pgs_frame;   // 3 per item: normal, tangent 0, tangent 1
+  float4* pgs_lam;     // compact impulses, pgs_coff[k] + j
+  uint32_t *pgs_cnt, *pgs_coff, *pgs_slot;
   // per-body manifold lists (CSR over compact manifold indices) [cur], [prev]
   uint32_t* csr_start[2];
   uint32_t* csr_list[2];
@@ -115,6 +119,7 @@ struct DevState {
   uint32_t* gc_color;    // per compact manifold
   uint32_t* gc_pid;      // pair-identity hash
   uint32_t* gc_choice;
+  uint4* gc_rec;         // per compact manifold: body a, body b, pair hash, static bits
   uint32_t* gc_mask;     // per body
   unsigned long long* gc_owner; // per body x 32 colours: (epoch << 32) | priority
   uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies

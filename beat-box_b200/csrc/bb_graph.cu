@@ -45,17 +45,32 @@ __global__ void k_uf_init(const DevState d, uint32_t n) {
   if (i >= n) return;
   d.uf_parent[i] = (d.flags[i] & BB_BODY_DYNAMIC) ? i : BB_NONE;
 }
+__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Root of x with path halving.  A tree's root is its smallest id (links hang the larger root
+// under the smaller), so the final roots do not depend on the order of the links.  Halving
+// only rewrites parents of non-roots, and only to an ancestor; roots change only by the CAS in
+// k_uf_link, so the two kinds of write never touch the same word.
 __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, DevCounters* c) {
+  uint32_t p = ld_relaxed_gpu(&parent[x]);
   uint32_t guard = 0;
-  for (;;) {
-    uint32_t px = atomicAdd(&parent[x], 0u);
-    if (px == x) return x;
-    x = px;
+  while (p != x) {
+    const uint32_t gp = ld_relaxed_gpu(&parent[p]);
+    if (gp != p) st_relaxed_gpu(&parent[x], gp);
+    x = p;
+    p = gp;
     if (++guard > (1u << 24)) {
       raise_error(c, BB_ERRF_CAS_LIMIT);
       return x;
     }
   }
+  return x;
 }
 // IslandBuilder::link_bodies (islands.slang:153-213): link the higher root under the lower
 __global__ void k_uf_link(const DevState d, int cur) {
@@ -63,13 +78,14 @@ __global__ void k_uf_link(const DevState d, int cur) {
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
     uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
     if (!(d.flags[b.x] & BB_BODY_DYNAMIC) || !(d.flags[b.y] & BB_BODY_DYNAMIC)) continue;
-    uint32_t ra = b.x, rb = b.y;
-    for (uint32_t tries = 0;; ++tries) {
-      ra = uf_find(d.uf_parent, ra, d.ctr);
-      rb = uf_find(d.uf_parent, rb, d.ctr);
-      if (ra == rb) break;
-      uint32_t lo = min(ra, rb), hi = max(ra, rb);
-      if (atomicCAS(&d.uf_parent[hi], hi, lo) == hi) break;
+    uint32_t ra = uf_find(d.uf_parent, b.x, d.ctr), rb = uf_find(d.uf_parent, b.y, d.ctr);
+    for (uint32_t tries = 0; ra != rb; ++tries) {
+      const uint32_t lo = min(ra, rb), hi = max(ra, rb);
+      const uint32_t old = atomicCAS(&d.uf_parent[hi], hi, lo);
+      if (old == hi) break;
+      // hi was linked meanwhile: continue from its new root
+      if (hi == ra) ra = uf_find(d.uf_parent, old, d.ctr);
+      else rb = uf_find(d.uf_parent, old, d.ctr);
       if (tries > 4096u) {
         raise_error(d.ctr, BB_ERRF_CAS_LIMIT);
         break;
@@ -209,63 +225,73 @@ __device__ __forceinline__ uint32_t gc_priority(uint32_t pid, uint32_t round) {
 //           (gc_priority, :130-138) into owner[body][colour];
 //   commit: a manifold that won on both bodies takes the colour (:179-212).
 // Finally writes the (colour, manifold) keys of the bucket sort.
-__global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
+// Persistent colouring kernel.  Each manifold's bodies, static bits and pair hash are packed
+// into one record up front, so a round touches rec -> body masks -> owner words only; the
+// grid barrier is the arrival-counter kind (counter 0 of the substep).
+#define BB_GC_THREADS 1024
+__global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
   DevCounters* c = d.ctr;
   const uint32_t M = c->manifold_count;
   const uint32_t epoch = c->gc_epoch;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* uncol = &c->pad[0];  // two alternating per-round counters
+  uint32_t* sync = &c->sync_count[0];
+  uint32_t ep = 0;
   for (uint32_t i = tid; i < n; i += stride) d.gc_mask[i] = 0;
   for (uint32_t m = tid; m < M; m += stride) {
-    uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
-    int key = d.m_keycc[cur][d.man_slot[cur][m]].x;
+    const uint32_t slot = d.man_slot[cur][m];
+    uint2 b = d.m_bodies[cur][slot];
+    int key = d.m_keycc[cur][slot].x;
     const uint32_t la = local_id(d, b.x), lb = local_id(d, b.y);
     uint32_t lo = min(la, lb), hi = max(la, lb);
-    d.gc_pid[m] = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
+    const uint32_t pid = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
+    d.gc_pid[m] = pid;
     d.gc_color[m] = BB_UNCOLORED;
+    const uint32_t st = ((d.flags[b.x] & BB_BODY_DYNAMIC) ? 0u : 1u) | ((d.flags[b.y] & BB_BODY_DYNAMIC) ? 0u : 2u);
+    d.gc_rec[m] = make_uint4(b.x, b.y, pid, st);
   }
   if (tid == 0) {
     uncol[1] = 0;
     c->gc_colors = 0;
   }
-  grid_barrier(c);
+  grid_sync(c, sync, ep);
   for (uint32_t r = 1; r <= p.gc_rounds; ++r) {
     const unsigned long long tag = (unsigned long long)(epoch + r) << 32;
     uint32_t mine = 0;
     for (uint32_t m = tid; m < M; m += stride) {
       if (d.gc_color[m] != BB_UNCOLORED) continue;
       ++mine;
-      uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
-      bool sa = !(d.flags[b.x] & BB_BODY_DYNAMIC), sb = !(d.flags[b.y] & BB_BODY_DYNAMIC);
-      uint32_t avail = ~((sa ? 0u : d.gc_mask[b.x]) | (sb ? 0u : d.gc_mask[b.y]));
+      const uint4 rec = d.gc_rec[m];
+      const bool sa = rec.w & 1u, sb = rec.w & 2u;
+      uint32_t avail = ~((sa ? 0u : d.gc_mask[rec.x]) | (sb ? 0u : d.gc_mask[rec.y]));
       uint32_t col = avail == 0u ? BB_MAX_COLORS : uint32_t(__ffs(avail) - 1);
       d.gc_choice[m] = col;
       if (col >= BB_MAX_COLORS) continue;
-      unsigned long long v = tag | gc_priority(d.gc_pid[m], r);
-      if (!sa) atomicMax(&d.gc_owner[size_t(b.x) * BB_MAX_COLORS + col], v);
-      if (!sb) atomicMax(&d.gc_owner[size_t(b.y) * BB_MAX_COLORS + col], v);
+      unsigned long long v = tag | gc_priority(rec.z, r);
+      if (!sa) atomicMax(&d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col], v);
+      if (!sb) atomicMax(&d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col], v);
     }
     if (mine) atomicAdd(&uncol[r & 1], mine);
-    grid_barrier(c);
+    grid_sync(c, sync, ep);
     if (*(volatile uint32_t*)&uncol[r & 1] == 0u) break;
     if (tid == 0) uncol[(r + 1) & 1] = 0;
     for (uint32_t m = tid; m < M; m += stride) {
       if (d.gc_color[m] != BB_UNCOLORED) continue;
       uint32_t col = d.gc_choice[m];
       if (col >= BB_MAX_COLORS) continue;
-      uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
-      bool sa = !(d.flags[b.x] & BB_BODY_DYNAMIC), sb = !(d.flags[b.y] & BB_BODY_DYNAMIC);
-      unsigned long long v = tag | gc_priority(d.gc_pid[m], r);
-      bool wa = sa || d.gc_owner[size_t(b.x) * BB_MAX_COLORS + col] == v;
-      bool wb = sb || d.gc_owner[size_t(b.y) * BB_MAX_COLORS + col] == v;
+      const uint4 rec = d.gc_rec[m];
+      const bool sa = rec.w & 1u, sb = rec.w & 2u;
+      unsigned long long v = tag | gc_priority(rec.z, r);
+      bool wa = sa || d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col] == v;
+      bool wb = sb || d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col] == v;
       if (wa && wb) {
         d.gc_color[m] = col;
-        if (!sa) atomicOr(&d.gc_mask[b.x], 1u << col);
-        if (!sb) atomicOr(&d.gc_mask[b.y], 1u << col);
+        if (!sa) atomicOr(&d.gc_mask[rec.x], 1u << col);
+        if (!sb) atomicOr(&d.gc_mask[rec.y], 1u << col);
         atomicMax(&c->gc_colors, col + 1u);
       }
     }
-    grid_barrier(c);
+    grid_sync(c, sync, ep);
   }
   uint32_t over = 0;
   for (uint32_t m = tid; m < M; m += stride) {
@@ -285,7 +311,7 @@ __global__ void k_bucket_starts(const uint32_t* hist_scan, const uint32_t* n_ptr
   if (t == nb) starts[t] = *n_ptr;
 }
 
-int bb_edge_coloring_blocks(int sms) { return bb_coop_blocks((const void*)k_edge_color, BB_COOP_THREADS, sms); }
+int bb_edge_coloring_blocks(int sms) { return bb_coop_blocks((const void*)k_edge_color, BB_GC_THREADS, sms); }
 
 void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
                       int sms, int cur, int coop_blocks) {
@@ -294,7 +320,7 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
   uint32_t nn = n;
   DevState dd = d;
   void* args[] = {&dd, &pp, &cc, &nn};
-  bb_launch_coop((const void*)k_edge_color, coop_blocks, BB_COOP_THREADS, args, s);
+  bb_launch_coop((const void*)k_edge_color, coop_blocks, BB_GC_THREADS, args, s);
   // stable bucket sort of manifold ids by colour (one 8-bit digit)
   uint32_t* keys[2] = {d.bucket_keys[0], d.bucket_keys[1]};
   uint32_t* vals[2] = {d.bucket_vals[0], d.bucket_vals[1]};

@@ -616,7 +616,7 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
                      int cur, bool warm) {
   const int T = BB_THREADS;
   int grid = sms * 8;
-  k_narrow<<<sms * 16, 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
+  k_narrow<<<sms * (p.narrow_blocks_per_sm ? p.narrow_blocks_per_sm : 16u), 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
   // compact order: exclusive scan of the hit flags over the pair slots
   bb_launch_scan(s, d.hit, d.man_index, &d.ctr->pair_count, d.pair_capacity, &d.ctr->manifold_count,
                  sc.scan_status + sc.scan_tiles, sc.scan_tile_ctr + 1, d.ctr);

@@ -254,60 +254,81 @@ __device__ __forceinline__ void pgs_integrate(const DevState& d, uint32_t i, flo
 #define BB_PGS_PF 4         // contacts of an item held in registers across the barrier
 #define BB_PGS_SKIP (1u << 10)
 
+// The kernel works on a compact copy in colour order: item k's record, masses and contact frame
+// at index k, its contacts' rows (c_r1, c_r2, c_k reused with compact indexing) and impulses
+// (pgs_lam) at pgs_coff[k] + j.  The impulses go back to the persistent slot-indexed contacts
+// when the kernel ends.  Dense arrays keep the per-sweep working set (about 80 B per manifold,
+// 64 B per contact, 64 B per body) resident in L2.
 struct PgsItem {
-  uint4 rec;    // slot, body a, body b, contact count | dynamic a << 8 | dynamic b << 9 | skip << 10
+  uint4 rec;    // contact offset, body a, body b, contact count | dynamic a << 8 | dynamic b << 9 | skip << 10
   float4 mass;  // inverse mass a, inverse mass b, friction, -
   float4 n, t0, t1;
   float4 R1[BB_PGS_PF], R2[BB_PGS_PF], K[BB_PGS_PF], lam[BB_PGS_PF];
 };
 
-__device__ __forceinline__ void pgs_item_load(const DevState& d, int cur, uint32_t k, PgsItem& x) {
+__device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, PgsItem& x) {
   x.rec = d.pgs_rec[k];
   x.mass = d.pgs_mass[k];
-  if (x.rec.w & BB_PGS_SKIP) return;
-  const uint32_t slot = x.rec.x, cc = x.rec.w & 0xFFu;
-  x.n = d.m_normal[cur][slot];
-  x.t0 = d.m_t0[cur][slot];
-  x.t1 = d.m_t1[cur][slot];
+  x.n = d.pgs_frame[3 * k];
+  x.t0 = d.pgs_frame[3 * k + 1];
+  x.t1 = d.pgs_frame[3 * k + 2];
+  const uint32_t c0 = x.rec.x, cc = x.rec.w & 0xFFu;
 #pragma unroll
   for (int j = 0; j < BB_PGS_PF; ++j) {
     if (uint32_t(j) < cc) {
-      const uint32_t ci = slot * BB_MAX_CONTACTS + j;
-      x.R1[j] = d.c_r1[ci];
-      x.R2[j] = d.c_r2[ci];
-      x.K[j] = d.c_k[ci];
-      x.lam[j] = d.c_lam[cur][ci];
+      x.R1[j] = d.c_r1[c0 + j];
+      x.R2[j] = d.c_r2[c0 + j];
+      x.K[j] = d.c_k[c0 + j];
+      x.lam[j] = d.pgs_lam[c0 + j];
     }
   }
 }
 
-// item record + rows of colour-ordered item k (the pre-step's row half; no body is touched)
+// contacts per colour-ordered item (0 for items whose bodies both sleep): scanned into pgs_coff
+__global__ void k_pgs_count(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  const uint32_t* list = d.bucket_vals[1];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+    const uint32_t slot = d.man_slot[cur][list[k]];
+    const uint2 b = d.m_bodies[cur][slot];
+    const bool skip = !awake(d.flags[b.x]) && !awake(d.flags[b.y]);
+    d.pgs_cnt[k] = skip ? 0u : uint32_t(d.m_keycc[cur][slot].y);
+  }
+}
+
+// compact record + rows of colour-ordered item k (the pre-step's row half; no body is touched)
 __device__ void pgs_item_build(const DevState& d, int cur, uint32_t k, uint32_t m, float h, float hertz) {
   const uint32_t slot = d.man_slot[cur][m];
   const uint2 b = d.m_bodies[cur][slot];
   const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
-  const uint32_t cc = uint32_t(d.m_keycc[cur][slot].y);
+  const uint32_t cc = d.pgs_cnt[k];  // 0 when both bodies sleep
+  const uint32_t c0 = d.pgs_coff[k];
   const bool skip = !awake(fa) && !awake(fb);
   const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
-  d.pgs_rec[k] = make_uint4(slot, b.x, b.y,
+  d.pgs_rec[k] = make_uint4(c0, b.x, b.y,
                             cc | ((fa & BB_BODY_DYNAMIC) ? 1u << 8 : 0u) | ((fb & BB_BODY_DYNAMIC) ? 1u << 9 : 0u) |
                                 (skip ? BB_PGS_SKIP : 0u));
   d.pgs_mass[k] = make_float4(ima, imb, sqrtf(d.iinv[b.x].w * d.iinv[b.y].w), 0.f);
+  d.pgs_slot[k] = slot;
   if (skip) return;
+  const float4 n4 = d.m_normal[cur][slot], t04 = d.m_t0[cur][slot], t14 = d.m_t1[cur][slot];
+  d.pgs_frame[3 * k] = n4;
+  d.pgs_frame[3 * k + 1] = t04;
+  d.pgs_frame[3 * k + 2] = t14;
   const Sym3 IA = load_iw(d, b.x), IB = load_iw(d, b.y);
-  const float3 n = f3(d.m_normal[cur][slot]);
-  const float3 t0 = f3(d.m_t0[cur][slot]), t1 = f3(d.m_t1[cur][slot]);
+  const float3 n = f3(n4), t0 = f3(t04), t1 = f3(t14);
   const float3 aa = f3(d.m_anchor_a[cur][slot]), ab = f3(d.m_anchor_b[cur][slot]);
   const SoftCoef s = pgs_soft_coef(ima, imb, h, hertz);
   for (uint32_t j = 0; j < cc; ++j) {
     const uint32_t ci = slot * BB_MAX_CONTACTS + j;
     float4 R1, R2, K;
     pgs_contact_rows(d.c_pos[cur][ci], aa, ab, n, t0, t1, ima, imb, IA, IB, s, R1, R2, K);
-    d.c_r1[ci] = R1;
-    d.c_r2[ci] = R2;
-    d.c_k[ci] = K;
+    d.c_r1[c0 + j] = R1;
+    d.c_r2[c0 + j] = R2;
+    d.c_k[c0 + j] = K;
     const float4 lam = d.c_lam[cur][ci];
-    d.c_lam[cur][ci] = make_float4(lam.x, lam.y, lam.z, s.mcoef);
+    // the reference writes its mass coefficient / tangent masses into the persistent contact
+    d.pgs_lam[c0 + j] = make_float4(lam.x, lam.y, lam.z, s.mcoef);
     const float4 kt4 = d.c_kt[cur][ci];
     d.c_kt[cur][ci] = make_float4(R2.w, K.x, kt4.z, kt4.w);
   }
@@ -318,7 +339,7 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
   if (x.rec.w & BB_PGS_SKIP) return;
   const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
   if (mode == 0 && !accum) return;
-  const uint32_t a = x.rec.y, b = x.rec.z, slot = x.rec.x, cc = x.rec.w & 0xFFu;
+  const uint32_t a = x.rec.y, b = x.rec.z, c0 = x.rec.x, cc = x.rec.w & 0xFFu;
   float4 va4 = d.vel[a], vb4 = d.vel[b];
   float3 va = f3(va4), wa = f3(d.omega[a]), vb = f3(vb4), wb = f3(d.omega[b]);
   const Sym3 IA = load_iw(d, a), IB = load_iw(d, b);
@@ -332,19 +353,19 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
       } else {
         pgs_contact_solve(x.R1[j], x.R2[j], x.K[j], x.lam[j], n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA,
                           IB, va, wa, vb, wb);
-        d.c_lam[cur][slot * BB_MAX_CONTACTS + j] = x.lam[j];
+        d.pgs_lam[c0 + j] = x.lam[j];
       }
     }
   }
   for (uint32_t j = BB_PGS_PF; j < cc; ++j) {  // contacts beyond the register-held ones
-    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
-    float4 lam = d.c_lam[cur][ci];
+    const uint32_t ci = c0 + j;
+    float4 lam = d.pgs_lam[ci];
     if (mode == 0) {
       pgs_contact_warm(f3(d.c_r1[ci]), f3(d.c_r2[ci]), lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
     } else {
       pgs_contact_solve(d.c_r1[ci], d.c_r2[ci], d.c_k[ci], lam, n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA,
                         IB, va, wa, vb, wb);
-      d.c_lam[cur][ci] = lam;
+      d.pgs_lam[ci] = lam;
     }
   }
   if (x.rec.w & (1u << 8)) {
@@ -368,10 +389,10 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
     for (uint32_t k = bs[c] + tid; k < end;) {
       pgs_item_run(d, p, cur, x, mode);
       k += stride;
-      if (k < end) pgs_item_load(d, cur, k, x);
+      if (k < end) pgs_item_load(d, k, x);
     }
     const uint32_t cn = c + 1 < C ? c + 1 : 0u;
-    if (bs[cn] + tid < bs[cn + 1]) pgs_item_load(d, cur, bs[cn] + tid, x);
+    if (bs[cn] + tid < bs[cn + 1]) pgs_item_load(d, bs[cn] + tid, x);
     grid_sync(d.ctr, sync, epoch);
   }
   const uint32_t o0 = bs[BB_MAX_COLORS], o1 = bs[BB_MAX_COLORS + 1];
@@ -379,7 +400,7 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
     if (tid == 0) {
       for (uint32_t k = o0; k < o1; ++k) {
         PgsItem y;
-        pgs_item_load(d, cur, k, y);
+        pgs_item_load(d, k, y);
         pgs_item_run(d, p, cur, y, mode);
       }
     }
@@ -406,7 +427,7 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d
   if (tid == 0)
     for (uint32_t k = bs[BB_MAX_COLORS]; k < bs[BB_MAX_COLORS + 1]; ++k) pgs_item_build(d, cur, k, list[k], h, hertz);
   PgsItem x;
-  if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, cur, bs[0] + tid, x);
+  if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, bs[0] + tid, x);
   pgs_sweep(d, p, cur, 0, bs, C, x, epoch);
   for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, C, x, epoch);
   if (p.flags & BB_SIM_ADVECTION) {
@@ -415,6 +436,14 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d
     grid_sync(d.ctr, sync, epoch);
   }
   for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, C, x, epoch);
+  // impulses back to the persistent contacts (every sweep ended with a grid barrier)
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t k = tid; k < M; k += stride) {
+    const uint32_t cc = d.pgs_cnt[k];
+    if (cc == 0) continue;
+    const uint32_t slot = d.pgs_slot[k], c0 = d.pgs_coff[k];
+    for (uint32_t j = 0; j < cc; ++j) d.c_lam[cur][slot * BB_MAX_CONTACTS + j] = d.pgs_lam[c0 + j];
+  }
 }
 
 int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_PGS_THREADS, sms); }
@@ -560,13 +589,16 @@ __global__ void __launch_bounds__(256) k_pgs_flow(const DevState d, Params p, in
 }
 
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
-                       int coop_blocks, int sms) {
+                       const StepScratch& sc, int coop_blocks, int sms) {
   if (p.schedule == BB_SCHEDULE_DATAFLOW) {
     k_flow_prep<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
     k_flow_init<<<(n + BB_THREADS - 1) / BB_THREADS, BB_THREADS, 0, s>>>(d, p, n);
-    k_pgs_flow<<<sms * 8, 256, 0, s>>>(d, p, cur, n, h);
+    k_pgs_flow<<<sms * (p.flow_blocks_per_sm ? p.flow_blocks_per_sm : 8u), 256, 0, s>>>(d, p, cur, n, h);
     return;
   }
+  k_pgs_count<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
+  bb_launch_scan(s, d.pgs_cnt, d.pgs_coff, &d.ctr->manifold_count, d.pair_capacity, nullptr,
+                 sc.scan_status + 4 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 4, d.ctr);
   DevState dd = d;
   Params pp = p;
   int cc = cur;
@@ -604,13 +636,15 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevStat
   DevCounters* c = d.ctr;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* uncol = &c->pad[2];
+  uint32_t* sync = &c->sync_count[2];
+  uint32_t ep = 0;
   for (uint32_t i = tid; i < n; i += stride) d.body_color[i] = BB_UNCOLORED;
   if (tid == 0) {
     uncol[0] = 0;
     uncol[1] = 0;
     c->avbd_colors = 0;
   }
-  grid_barrier(c);
+  grid_sync(c, sync, ep);
   for (uint32_t rd = 0; rd < p.avbd_color_rounds; ++rd) {
     uint32_t left = 0;
     for (uint32_t i = tid; i < n; i += stride) {
@@ -640,10 +674,10 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevStat
       atomicMax(&c->avbd_colors, col + 1u);
     }
     if (left) atomicAdd(&uncol[rd & 1], left);
-    grid_barrier(c);
+    grid_sync(c, sync, ep);
     if (*(volatile uint32_t*)&uncol[rd & 1] == 0u) break;
     if (tid == 0) uncol[(rd + 1) & 1] = 0;
-    grid_barrier(c);
+    grid_sync(c, sync, ep);
   }
   for (uint32_t i = tid; i < n; i += stride) {
     uint32_t v = d.body_color[i];
@@ -1029,6 +1063,8 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
                                                            int phase) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const uint32_t* list = d.a_bucket_vals[1];
+  uint32_t* sync = &d.ctr->sync_count[3 + phase];
+  uint32_t ep = 0;
   if (phase == 0) {
     const uint32_t C = d.ctr->avbd_colors;
     const uint32_t M = d.ctr->manifold_count;
@@ -1037,10 +1073,10 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
         uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
         if (s0 == s1) continue;
         for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 1.0f);
-        grid_barrier(d.ctr);
+        grid_sync(d.ctr, sync, ep);
       }
       for (uint32_t m = tid; m < M; m += stride) avbd_dual(d, p, cur, m);
-      grid_barrier(d.ctr);
+      grid_sync(d.ctr, sync, ep);
     }
     for (uint32_t i = tid; i < n; i += stride)
       if (awake(d.flags[i])) avbd_finalize(d, cur, i, dt);
@@ -1050,7 +1086,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
       uint32_t s0 = d.a_bucket_start[key], s1 = d.a_bucket_start[key + 1];
       if (s0 == s1) continue;
       for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 0.0f);
-      grid_barrier(d.ctr);
+      grid_sync(d.ctr, sync, ep);
     }
   } else {
     const uint32_t C = d.ctr->avbd_colors;
@@ -1059,7 +1095,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
         uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
         if (s0 == s1) continue;
         for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 0.0f);
-        grid_barrier(d.ctr);
+        grid_sync(d.ctr, sync, ep);
       }
     }
   }

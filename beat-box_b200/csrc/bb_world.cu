@@ -109,6 +109,13 @@ __global__ void k_unpack_state(const DevState d, uint32_t n, const float* st, ui
   if (mask & 8) d.omega[i] = make_float4(W[3 * i], W[3 * i + 1], W[3 * i + 2], 0.f);
 }
 
+__global__ void k_extend_contacts(const DevState d, uint32_t o, uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  d.vals[0][o + i] = o + i;
+  for (int k = 0; k < 2; ++k) d.csr_start[k][o + 1 + i] = d.csr_start[k][o];
+}
+
 __global__ void k_begin_substep(DevCounters* c) {
   if (threadIdx.x != 0) return;
   c->pair_count = 0;
@@ -190,6 +197,7 @@ struct bb_world_impl {
     d.visit = u32(N);
     d.pair_cnt = u32(N); d.pair_off = u32(N + 1);
     d.is_heavy = u32(N); d.heavy_list = u32(1024);
+    d.bp_stage = u32(size_t(N) * 16);
     d.pairs = dalloc<uint2>(P, owned, err);
     for (int k = 0; k < 2; ++k) {
       d.m_bodies[k] = dalloc<uint2>(P, owned, err);
@@ -203,7 +211,11 @@ struct bb_world_impl {
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
     d.flow_rec = dalloc<uint4>(P, owned, err);
     d.pgs_rec = dalloc<uint4>(P, owned, err);
+    d.gc_rec = dalloc<uint4>(P, owned, err);
     d.pgs_mass = f4(P);
+    d.pgs_frame = f4(3 * P);
+    d.pgs_lam = f4(8 * P);
+    d.pgs_cnt = u32(P); d.pgs_coff = u32(P); d.pgs_slot = u32(P);
     d.flow_counter = u32(N);
     d.range_first = dalloc<int32_t>(N, owned, err);
     d.sworld = u32(N);
@@ -226,10 +238,10 @@ struct bb_world_impl {
     d.staging = dalloc<float>(13 * N + 4, owned, err);
     d.pair_capacity = cap_p;
     d.body_capacity = cap_n;
-    // scratch zeroed at every substep: scan status (4 scans), sort hists / status (10 slots)
+    // scratch zeroed at every substep: scan status (5 scans), sort hists / status (12 slots)
     sc.scan_tiles = bb_scan_tiles(std::max<size_t>(P, N + 1));
     sc.sort_tiles = bb_sort_tiles(std::max<size_t>(P, N));
-    size_t scan_words = size_t(4) * sc.scan_tiles;  // 64-bit
+    size_t scan_words = size_t(5) * sc.scan_tiles;  // 64-bit
     size_t sort_status_words = size_t(12) * sc.sort_tiles * 256;
     size_t hist_words = 5 * BB_HIST_REGION;
     scratch_bytes = scan_words * 8 + 16 * 4 + hist_words * 4 + sort_status_words * 4 + 16 * 4;
@@ -257,6 +269,13 @@ struct bb_world_impl {
     cudaStreamSynchronize(stream);
   }
 
+  // bodies [o, o + count) were appended: they start with empty contact lists and take the
+  // next sorted positions; existing bodies keep their warm-start state and order
+  void extend_contacts(uint32_t o, uint32_t count) {
+    k_extend_contacts<<<(count + 255) / 256, 256, 0, stream>>>(d, o, count);
+    cudaStreamSynchronize(stream);
+  }
+
   void invalidate_graphs() {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
@@ -276,7 +295,7 @@ struct bb_world_impl {
     bb_islands(stream, d, params, n, sc, sms, cur);
     bb_sleep(stream, d, params, n, sms, cur);
     bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
-    if (params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(stream, d, params, n, h, cur, coop_pgs, sms);
+    if (params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, sms);
     else if (params.solver == BB_SOLVER_AVBD) bb_solve_avbd(stream, d, params, n, h, sc, sms, cur, coop_avbd);
     if (commit) parity = cur;
   }
@@ -319,6 +338,10 @@ void bb_default_solver_params(bb_solver_params* p) {
   p->avbd_color_rounds = 16;
   p->avbd_shock_layers = 12;
   p->avbd_post_stab_sweeps = 4;
+  p->schedule = BB_SCHEDULE_COLOUR_BARRIER;
+  p->broad_threads = 128;
+  p->narrow_blocks_per_sm = 16;
+  p->flow_blocks_per_sm = 8;
   p->bounds_mode = BB_BOUNDS_FIXED;
   for (int k = 0; k < 3; ++k) {
     p->world_min[k] = -64.0f;
@@ -393,7 +416,8 @@ bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape) {
   return BB_OK;
 }
 
-static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id) {
+static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id,
+                                 bool keep_contacts = false) {
   if (!w || (!bodies && count)) return fail(BB_E_INVALID, "bb_add_bodies: bad arguments");
   if (uint64_t(w->n) + count > w->cap_n) return fail(BB_E_CAPACITY, "bb_add_bodies: max_bodies exceeded");
   std::vector<float4> pos(count), rot(count), vel(count), om(count), shp(count), ii(count);
@@ -459,8 +483,9 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
   w->n_dyn += ndyn;
   if (out_first_id) *out_first_id = o;
   // new bodies restart the persistent state (sorted order, warm-start contacts), as a scene
-  // load does in the reference
-  w->reset_contacts();
+  // load does in the reference; a world added to a batch leaves the other worlds' state alone
+  if (keep_contacts) w->extend_contacts(o, count);
+  else w->reset_contacts();
   w->invalidate_graphs();
   uint32_t nn[2] = {w->n, w->n_dyn};
   CU(cudaMemcpy(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice));
@@ -481,7 +506,7 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
   for (int k = 0; k < 3; ++k)
     if (!(desc->world_extent[k] > 0)) return fail(BB_E_INVALID, "bb_add_world: world_extent must be positive");
   uint32_t first = 0;
-  bb_status st = add_bodies_impl(w, bodies, count, &first);
+  bb_status st = add_bodies_impl(w, bodies, count, &first, w->d.n_worlds > 0);
   if (st != BB_OK) return st;
   const uint32_t widx = w->d.n_worlds;
   std::vector<uint32_t> wof(count, widx);
@@ -524,7 +549,14 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
     return fail(BB_E_UNSUPPORTED, "the per-island solve path (USE_GRAPH_COLORING off) is not provided");
   for (int k = 0; k < 3; ++k)
     if (!(p->world_extent[k] > 0)) return fail(BB_E_INVALID, "world_extent must be positive");
+  if (p->schedule > BB_SCHEDULE_COLOUR_BARRIER) return fail(BB_E_INVALID, "unknown schedule");
+  if ((p->broad_threads != 0 && p->broad_threads != 32 && p->broad_threads != 64 && p->broad_threads != 128) ||
+      p->narrow_blocks_per_sm > 64 || p->flow_blocks_per_sm > 8)
+    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, flow <= 8)");
   w->params = *p;
+  if (!w->params.broad_threads) w->params.broad_threads = 128;
+  if (!w->params.narrow_blocks_per_sm) w->params.narrow_blocks_per_sm = 16;
+  if (!w->params.flow_blocks_per_sm) w->params.flow_blocks_per_sm = 8;
   return BB_OK;
 }
 
@@ -618,7 +650,7 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
       cudaEventRecord(ev[5], w->stream);
       bb_edge_coloring(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_edge);
       cudaEventRecord(ev[6], w->stream);
-      if (w->params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->coop_pgs, w->sms);
+      if (w->params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->sms);
       else bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
       cudaEventRecord(ev[7], w->stream);
       CU(cudaEventSynchronize(ev[7]));
@@ -898,3 +930,73 @@ bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint3
 uint64_t bb_kernel_launch_count(void* world) { return world ? W(world)->launches : 0; }
 
 }  // extern "C"
+
+// ---- autotuner ------------------------------------------------------------------------------
+// Coordinate descent over the launch-geometry fields and the colour-sweep schedule of
+// bb_solver_params.  Every candidate computes bit-identical results, so the trial steps are
+// ordinary steps of the world (they advance it; call this in place of warm-up steps).  Each
+// candidate gets one untimed step (graph capture) and `trial_steps` steps timed with CUDA
+// events on the world's stream.
+bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_steps, bb_solver_params* chosen) {
+  World* w = W(world);
+  if (!w || !(dt > 0) || substeps == 0 || trial_steps == 0) return fail(BB_E_INVALID, "bb_autotune: bad arguments");
+  if (w->n == 0) {
+    if (chosen) *chosen = w->params;
+    return BB_OK;
+  }
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  bb_solver_params best = w->params;
+  auto trial = [&](const bb_solver_params& cand, float* ms) -> bb_status {
+    bb_status st = bb_set_solver_params(world, &cand);
+    if (st != BB_OK) return st;
+    st = bb_step(world, dt, substeps);
+    if (st != BB_OK) return st;
+    CU(cudaEventRecord(e0, w->stream));
+    for (uint32_t k = 0; k < trial_steps; ++k) {
+      st = bb_step(world, dt, substeps);
+      if (st != BB_OK) return st;
+    }
+    CU(cudaEventRecord(e1, w->stream));
+    CU(cudaEventSynchronize(e1));
+    CU(cudaEventElapsedTime(ms, e0, e1));
+    return bb_sync(world);
+  };
+  float best_ms = 0.f;
+  bb_status st = trial(best, &best_ms);
+  struct Axis {
+    uint32_t bb_solver_params::*field;
+    std::vector<uint32_t> values;
+    bool pgs_only, dataflow_only;
+  };
+  const std::vector<Axis> axes = {
+      {&bb_solver_params::schedule, {BB_SCHEDULE_DATAFLOW, BB_SCHEDULE_COLOUR_BARRIER}, true, false},
+      {&bb_solver_params::flow_blocks_per_sm, {2, 4, 8}, true, true},
+      {&bb_solver_params::broad_threads, {32, 64, 128}, false, false},
+      {&bb_solver_params::narrow_blocks_per_sm, {4, 8, 16, 32}, false, false},
+  };
+  for (const Axis& ax : axes) {
+    if (st != BB_OK) break;
+    if (ax.pgs_only && best.solver != BB_SOLVER_PGS_SOFT) continue;
+    if (ax.dataflow_only && best.schedule != BB_SCHEDULE_DATAFLOW) continue;
+    for (uint32_t v : ax.values) {
+      if (best.*ax.field == v) continue;
+      bb_solver_params cand = best;
+      cand.*ax.field = v;
+      float ms = 0.f;
+      st = trial(cand, &ms);
+      if (st != BB_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = cand;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != BB_OK) return st;
+  st = bb_set_solver_params(world, &best);
+  if (chosen) *chosen = best;
+  return st;
+}

@@ -340,6 +340,146 @@ def cpu_baseline(args, sc, state, flags) -> dict:
                       f"{args.warmup} warm-up steps (cold warm start), FP32 oracle"}
 
 
+def batched_scenes(n_worlds: int):
+    """Config-4 batch: world k is a pile of floor(exp(U(ln 16, ln 2048))) bodies, seed k + 1."""
+    sizes = scenes.batch_sizes(n_worlds, seed=0)
+    return [scenes.pile(int(nw), seed=k + 1) for k, nw in enumerate(sizes)]
+
+
+def balanced_share(sizes, rank: int, world_size: int):
+    """Greedy body-count-balanced assignment of worlds to ranks (largest first)."""
+    load = [0] * world_size
+    mine = []
+    for k in sorted(range(len(sizes)), key=lambda k: -sizes[k]):
+        r = min(range(world_size), key=lambda r: load[r])
+        load[r] += sizes[k]
+        if r == rank:
+            mine.append(k)
+    return sorted(mine)
+
+
+def run_batched(args, rank: int, world_size: int, local_rank: int):
+    """Config 4: thousands of independent worlds stepped as one batch (world-prefixed Morton
+    keys, one CUDA-graph launch per step), against the same worlds stepped one at a time through
+    the plain single-world path with the same kernels."""
+    import torch
+
+    import beatbox as bb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    all_scs = batched_scenes(args.worlds)
+    sizes = [int(sc["n"]) for sc in all_scs]
+    scs = [all_scs[k] for k in balanced_share(sizes, rank, world_size)]
+    total = sum(int(sc["n"]) for sc in scs)
+    p = bb.make_params(solver=bb.SOLVER_PGS_SOFT, iterations=8, relax_iterations=8, quirks=bb.QUIRKS_PHYSICAL)
+    w = bb.World(total, pairs_per_body=8, device=local_rank)
+    for sc in scs:
+        w.add_world(sc, *sc["bounds"])
+    w.set_params(p)
+    run = 120
+    first = max(args.warmup, run // 2 - args.steps // 2)
+    tune = w.autotune(DT, SUBSTEPS, trial_steps=1)  # its trial steps are ordinary steps of the run
+    tuned = w.stats()["substeps_run"] // SUBSTEPS
+    for _ in range(max(0, first - tuned)):
+        w.step(DT, SUBSTEPS)
+    w.sync()
+    done = max(first, tuned)
+    stream = torch.cuda.ExternalStream(w.stream)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    clocks = sample_clocks(local_rank)
+    launches0 = w.launches()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        evs[k][0].record(stream)
+        w.step(DT, SUBSTEPS)
+        evs[k][1].record(stream)
+    w.sync()
+    torch.cuda.synchronize()
+    clk = finish_clocks(clocks)
+    batch_ms = sum(a.elapsed_time(b) for a, b in evs)
+    launches = w.launches() - launches0
+    st = w.stats()
+    t = torch.tensor([batch_ms], device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    value = sum(sizes) * args.steps / (float(t.item()) / 1000.0)
+
+    # end to end: upload all worlds' state, step, read it back (pinned host buffers)
+    host = {k: torch.empty(v.shape, dtype=torch.float32).pin_memory().numpy() for k, v in w.read_state().items()}
+    for k, v in w.read_state().items():
+        host[k][...] = v
+    t0 = time.perf_counter()
+    e2e_steps = min(args.steps, 20)
+    for _ in range(e2e_steps):
+        w.write_state(host["pos"], host["quat"], host["vel"], host["omega"])
+        w.step(DT, SUBSTEPS)
+        w.read_state(host)
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = sum(sizes) * e2e_steps / float(e2e_t.item())
+    w.close()
+
+    # plain path: every plain_stride-th of this rank's worlds alone, same kernels, same step window
+    plain_bodies = 0
+    plain_ms = 0.0
+    ks = 3
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for sc in scs[:: args.plain_stride]:
+        pw = bb.world_from_scene(sc, params=p, pairs_per_body=8)
+        for _ in range(done):
+            pw.step(DT, SUBSTEPS)
+        pw.sync()
+        ps = torch.cuda.ExternalStream(pw.stream)
+        ev0.record(ps)
+        for _ in range(ks):
+            pw.step(DT, SUBSTEPS)
+        ev1.record(ps)
+        pw.sync()
+        plain_ms += ev0.elapsed_time(ev1)
+        plain_bodies += int(sc["n"]) * ks
+        pw.close()
+    plain_value = plain_bodies / (plain_ms / 1000.0) if plain_ms > 0 else None
+    if rank == 0:
+        line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world_size,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(t.item()) / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded piles, seeds 1..worlds)",
+                "config": {"workload": f"batched_{args.worlds}: {args.worlds} worlds of floor(exp(U(ln 16, ln 2048))) "
+                                       f"bodies ({sum(sizes)} in total), config-1 piles (60% unit boxes / 40% "
+                                       f"spheres r=0.5) each over its own ground, dt=1/60, {SUBSTEPS} substeps, "
+                                       "PGS_SOFT 8 iterations, autotuned",
+                           "worlds": args.worlds, "bodies": sum(sizes), "parallelism": f"worlds split over {world_size} GPU(s)",
+                           "l2": "flushed before every timed step",
+                           "timed_steps": f"steps {done}..{done + args.steps - 1} of the {run}-step run",
+                           "tuning": tune},
+                "plain": {"value": plain_value, "unit": "body-steps/s",
+                          "sample": f"every {args.plain_stride}th world alone through the single-world path, "
+                                    f"{ks} steps each after the same {done}-step roll, device time"},
+                "batched_over_plain": (value / world_size) / plain_value if plain_value else None,
+                "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": total * 52,
+                        "d2h_bytes_per_step": total * 52, "steps": e2e_steps,
+                        "what": "bb_write_state + bb_step + bb_read_state of the whole batch, pinned host buffers"},
+                "gpu_launches": launches, "clocks": clk, "step_stats": st}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -350,8 +490,12 @@ def main():
     ap.add_argument("--bodies", type=int, default=N_BODIES)
     ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids"],
                     help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids")
-    ap.add_argument("--schedule", default="dataflow", choices=["dataflow", "barrier"],
+    ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched"],
+                    help="plain: one world (default); batched: config-4 batch of independent worlds")
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--plain-stride", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget-s", type=float, default=150.0)
     args = ap.parse_args()
@@ -361,6 +505,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world_size)
+    elif args.mode == "batched":
+        run_batched(args, rank, world_size, local_rank)
     else:
         run_ours(args, rank, world_size, local_rank)
 

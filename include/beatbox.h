@@ -125,7 +125,11 @@ typedef struct bb_solver_params {
   uint32_t avbd_shock_layers;  /* 12 */
   uint32_t avbd_post_stab_sweeps; /* 4 */
   /* execution schedule of the colour sweeps (results are identical either way) */
-  uint32_t schedule;           /* BB_SCHEDULE_* (default BB_SCHEDULE_DATAFLOW) */
+  uint32_t schedule;           /* BB_SCHEDULE_* (default BB_SCHEDULE_COLOUR_BARRIER) */
+  /* launch geometry (results are identical for every value; 0 = default; bb_autotune picks) */
+  uint32_t broad_threads;        /* broad-phase block size: 32, 64 or 128 (default 128) */
+  uint32_t narrow_blocks_per_sm; /* narrow-phase grid, 128-thread blocks per SM: 1..64 (default 16) */
+  uint32_t flow_blocks_per_sm;   /* dataflow PGS grid, 256-thread blocks per SM: 1..8 (default 8) */
   /* Morton normalisation */
   uint32_t bounds_mode;        /* BB_BOUNDS_* */
   float world_min[3];          /* default -64 */
@@ -179,7 +183,7 @@ typedef struct bb_step_stats {
   float max_penetration;          /* deepest contact penetration (positive metres) */
   uint32_t error_flags;           /* BB_ERRF_* bits raised on the device */
   uint32_t pair_capacity;
-  uint32_t substeps_run;
+  uint32_t substeps_run;          /* substeps run since the world was created */
 } bb_step_stats;
 
 /* device error bits (bb_step_stats.error_flags) */
@@ -332,6 +336,14 @@ bb_status bb_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, 
 #define BB_SORT_STATIC_MAX_KEYS 262144u
 bb_status bb_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                      uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
+
+/* Pick the launch geometry and colour-sweep schedule of this world by timing candidates
+ * (coordinate descent over bb_solver_params.schedule, flow_blocks_per_sm, broad_threads,
+ * narrow_blocks_per_sm).  All candidates give bit-identical results, so the trial steps are
+ * ordinary steps (about 12 x (trial_steps + 1) of them): use it in place of warm-up.  The
+ * winner is set on the world and copied to *chosen (may be NULL).  The reference has no
+ * autotuner (its dispatch sizes are fixed in the task graph, src/rigid_body_manager.cpp:1284-1427). */
+bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_steps, bb_solver_params* chosen);
 
 /* Last error message of the calling thread (static storage, never NULL). */
 const char* bb_last_error_string(void);

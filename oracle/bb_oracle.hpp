@@ -204,7 +204,10 @@ inline void default_params(bb_solver_params* p) {
   p->avbd_color_rounds = 16;
   p->avbd_shock_layers = 12;
   p->avbd_post_stab_sweeps = 4;
-  p->schedule = BB_SCHEDULE_DATAFLOW;  // execution detail of the CUDA library; ignored here
+  p->schedule = BB_SCHEDULE_COLOUR_BARRIER;  // execution details of the CUDA library; ignored here
+  p->broad_threads = 128;
+  p->narrow_blocks_per_sm = 16;
+  p->flow_blocks_per_sm = 8;
   p->bounds_mode = BB_BOUNDS_FIXED;
   for (int i = 0; i < 3; ++i) {
     p->world_min[i] = -64.0f;

@@ -146,3 +146,43 @@ def test_dataflow_schedule_equals_colour_barrier(name):
         w.close()
     for k in outs[0]:
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_world_added_to_a_running_batch_leaves_the_others_unchanged():
+    """Serving pattern: world B joins after A has run 10 steps; A continues exactly as alone
+    (its warm-start contacts and sort order survive the join) and B runs as if alone."""
+    a, b = small_column(7), tiny_stack()
+    p = params(bb.SOLVER_PGS_SOFT)
+    w = bb.World(int(a["n"]) + int(b["n"]))
+    w.add_world(a, *scene_bounds(a))
+    w.set_params(p)
+    for _ in range(10):
+        w.step(DT, 2)
+    _, fb = w.add_world(b, *scene_bounds(b))
+    for _ in range(10):
+        w.step(DT, 2)
+    st = w.read_state()
+    w.close()
+    alone_a, _ = run_batch([a], p, steps=20, substeps=2)
+    alone_b, _ = run_batch([b], p, steps=10, substeps=2)
+    na = int(a["n"])
+    for key in st:
+        assert np.array_equal(st[key][:na], alone_a[0][key]), key
+        assert np.array_equal(st[key][fb:fb + int(b["n"])], alone_b[0][key]), key
+
+
+def test_autotune_keeps_results_bit_identical():
+    sc = scenes.mixed_column(n_bodies=2000, seed=3)
+    p = params(bb.SOLVER_PGS_SOFT)
+    w = bb.world_from_scene(sc, params=p)
+    tuned = w.autotune(DT, 2, trial_steps=1)
+    steps = w.stats()["substeps_run"] // 2
+    assert steps >= 4 and set(tuned) >= {"schedule", "broad_threads", "narrow_blocks_per_sm"}
+    for _ in range(5):
+        w.step(DT, 2)
+    ref = bb.world_from_scene(sc, params=p)
+    for _ in range(steps + 5):
+        ref.step(DT, 2)
+    a, b = w.read_state(), ref.read_state()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
