@@ -86,6 +86,35 @@ class BatchWorldDesc(ctypes.Structure):
     _fields_ = [("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3)]
 
 
+class ShapeDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_uint32), ("half", ctypes.c_float * 3)]
+
+
+class ServerDesc(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_active", ctypes.c_uint32),
+                ("pairs_per_body", ctypes.c_uint32), ("device", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("world", ctypes.c_uint64), ("shapes", ctypes.POINTER(ShapeDesc)), ("n_shapes", ctypes.c_uint32),
+                ("bodies", ctypes.POINTER(BodyDesc)), ("n_bodies", ctypes.c_uint32),
+                ("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3),
+                ("params", SolverParams), ("dt", ctypes.c_float), ("substeps", ctypes.c_uint32),
+                ("steps", ctypes.c_uint32)]
+
+
+class RequestStatus(ctypes.Structure):
+    _fields_ = [("done", ctypes.c_uint32), ("result", ctypes.c_int32), ("submit_s", ctypes.c_double),
+                ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("body_steps", ctypes.c_uint64), ("evictions", ctypes.c_uint64), ("worlds_created", ctypes.c_uint64),
+                ("resident_bytes", ctypes.c_uint64), ("active", ctypes.c_uint32), ("queued", ctypes.c_uint32),
+                ("resident_worlds", ctypes.c_uint32), ("known_worlds", ctypes.c_uint32)]
+
+
 class StepStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in (
         "body_count", "active_body_count", "pair_count", "manifold_count", "contact_count", "island_count",
@@ -137,6 +166,16 @@ _SIG = {
     "bb_radix_sort_pairs": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_radix_sort_pairs_static": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_autotune": (ctypes.c_int32, [_P, ctypes.c_float, _U32, _U32, ctypes.POINTER(SolverParams)]),
+    "bb_world_device_bytes": (ctypes.c_uint64, [_P]),
+    "bb_world_clear": (ctypes.c_int32, [_P]),
+    "bb_world_bytes_for": (ctypes.c_uint64, [_U32, _U32]),
+    "bb_server_create": (ctypes.c_int32, [ctypes.POINTER(ServerDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "bb_server_destroy": (ctypes.c_int32, [_P]),
+    "bb_server_submit": (ctypes.c_int32, [_P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
+    "bb_server_poll": (ctypes.c_int32, [_P, ctypes.c_uint64, ctypes.POINTER(RequestStatus)]),
+    "bb_server_wait": (ctypes.c_int32, [_P, ctypes.c_uint64, ctypes.POINTER(RequestStatus)]),
+    "bb_server_read_state": (ctypes.c_int32, [_P, ctypes.c_uint64, _P, _P, _P, _P, ctypes.POINTER(_U32)]),
+    "bb_server_get_stats": (ctypes.c_int32, [_P, ctypes.POINTER(ServerStats)]),
     "bb_last_error_string": (ctypes.c_char_p, []),
     "bb_version": (ctypes.c_char_p, []),
 }
@@ -399,6 +438,109 @@ def world_from_scene(scene: dict, params: SolverParams | None = None, pairs_per_
         p.world_extent[:] = scene["bounds"][1]
     w.set_params(p, **kw)
     return w
+
+
+def scene_request_arrays(scene: dict, inertia_mode: int = INERTIA_EXPLICIT):
+    """(shapes, bodies) ctypes arrays of a scene for a server request: one shape per distinct
+    (type, half extents), body.shape indexing the shape table."""
+    table: dict = {}
+    idx = []
+    for t, h in zip(scene["shape"].tolist(), scene["half"].tolist()):
+        key = (int(t), float(h[0]), float(h[1]), float(h[2]))
+        if key not in table:
+            table[key] = len(table)
+        idx.append(table[key])
+    shapes = (ShapeDesc * len(table))()
+    for key, k in table.items():
+        shapes[k].type = key[0]
+        shapes[k].half[:] = key[1:]
+    n = int(scene["n"])
+    bodies = (BodyDesc * n)()
+    a = np.frombuffer(bodies, dtype=BODY_DTYPE, count=n)
+    a["position"] = scene["pos"]
+    a["rotation"] = scene["quat"]
+    a["velocity"] = scene["vel"]
+    a["omega"] = scene["omega"]
+    a["shape"] = idx
+    a["flags"] = scene["flags"]
+    a["mass"] = scene["mass"]
+    a["friction"] = scene["friction"]
+    a["restitution"] = scene["restitution"]
+    a["inertia_mode"] = inertia_mode
+    a["inv_inertia"] = scene["inv_inertia"]
+    return shapes, bodies
+
+
+class Server:
+    """Serving loop (bb_server_*): step requests for device-resident worlds, admitted by an HBM
+    budget, overlapping on the device."""
+
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 64, pairs_per_body: int = 8, device: int = -1):
+        self.L = load_library()
+        d = ServerDesc(hbm_budget_bytes, max_active, pairs_per_body, device)
+        h = ctypes.c_void_p()
+        _check(self.L.bb_server_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def close(self):
+        if self.h:
+            _check(self.L.bb_server_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, world: int, steps: int, params: SolverParams, dt: float = 1.0 / 60.0, substeps: int = 1,
+               scene: dict | None = None, arrays=None) -> int:
+        """Queue `steps` steps of world `world`; a new world needs `scene` (or prebuilt `arrays`
+        from scene_request_arrays, plus scene for its bounds)."""
+        r = Request()
+        r.world = world
+        r.params = params if isinstance(params, SolverParams) else SolverParams.from_buffer_copy(bytes(params))
+        r.dt = dt
+        r.substeps = substeps
+        r.steps = steps
+        if scene is not None:
+            shapes, bodies = arrays if arrays is not None else scene_request_arrays(scene)
+            r.shapes = ctypes.cast(shapes, ctypes.POINTER(ShapeDesc))
+            r.n_shapes = len(shapes)
+            r.bodies = ctypes.cast(bodies, ctypes.POINTER(BodyDesc))
+            r.n_bodies = len(bodies)
+            b = scene.get("bounds") or ([-64.0] * 3, [128.0] * 3)
+            r.world_min[:] = [float(v) for v in b[0]]
+            r.world_extent[:] = [float(v) for v in b[1]]
+        t = ctypes.c_uint64()
+        _check(self.L.bb_server_submit(self.h, ctypes.byref(r), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int) -> dict:
+        st = RequestStatus()
+        _check(self.L.bb_server_poll(self.h, ticket, ctypes.byref(st)))
+        return dict(done=bool(st.done), result=st.result, submit_s=st.submit_s, start_s=st.start_s,
+                    finish_s=st.finish_s)
+
+    def wait(self, ticket: int) -> dict:
+        st = RequestStatus()
+        _check(self.L.bb_server_wait(self.h, ticket, ctypes.byref(st)))
+        return dict(done=bool(st.done), result=st.result, submit_s=st.submit_s, start_s=st.start_s,
+                    finish_s=st.finish_s)
+
+    def read_state(self, world: int, n: int) -> dict:
+        out = dict(pos=np.empty((n, 3), np.float32), quat=np.empty((n, 4), np.float32),
+                   vel=np.empty((n, 3), np.float32), omega=np.empty((n, 3), np.float32))
+        cnt = _U32()
+        _check(self.L.bb_server_read_state(self.h, world, _ptr(out["pos"]), _ptr(out["quat"]), _ptr(out["vel"]),
+                                           _ptr(out["omega"]), ctypes.byref(cnt)))
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(self.L.bb_server_get_stats(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
 
 
 class RigidBodyManager:

@@ -216,9 +216,9 @@ __global__ void k_refit(const DevState d, uint32_t n) {
 
 // A query that visits more than BB_BP_BUDGET nodes (a huge static body: floor, walls) is
 // handed to k_broad_heavy, which splits its traversal over a block.
-#define BB_BP_BUDGET 512u
-#define BB_BP_STAGE 16u  // partners per query kept from the counting traversal
-#define BB_HEAVY_CAP 1024u
+#define BB_BP_BUDGET 128u  // a serial walk longer than this sets the kernel's tail: hand it off
+#define BB_BP_STAGE 32u   // partners per query kept from the counting traversal
+#define BB_HEAVY_CAP 8192u
 #define BB_FRONTIER 256
 
 // Child ch is worth visiting from query qi: it holds leaves in (qi, wend) and its box

@@ -77,7 +77,7 @@ struct DevState {
   uint32_t* visit;              // refit arrival counters
   uint32_t *pair_cnt, *pair_off;  // per query
   uint32_t *is_heavy, *heavy_list;  // 1: over the visit budget (block-cooperative), 2: staging spilled
-  uint32_t* bp_stage;           // first 16 partners of each query (counting traversal)
+  uint32_t* bp_stage;           // first 32 partners of each query (counting traversal)
   uint2* pairs;                 // (sorted a, sorted b)
   // manifolds (two buffers: [cur], [prev] chosen by parity)
   uint2* m_bodies[2];    // body ids (a, b) per slot

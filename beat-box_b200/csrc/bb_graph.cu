@@ -40,11 +40,6 @@ void bb_advect(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, f
 }
 
 // ---- islands ---------------------------------------------------------------------------------
-__global__ void k_uf_init(const DevState d, uint32_t n) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  d.uf_parent[i] = (d.flags[i] & BB_BODY_DYNAMIC) ? i : BB_NONE;
-}
 __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
   uint32_t v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -53,73 +48,85 @@ __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
 __device__ __forceinline__ void st_relaxed_gpu(uint32_t* p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// Root of x with path halving.  A tree's root is its smallest id (links hang the larger root
-// under the smaller), so the final roots do not depend on the order of the links.  Halving
-// only rewrites parents of non-roots, and only to an ancestor; roots change only by the CAS in
-// k_uf_link, so the two kinds of write never touch the same word.
-__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, DevCounters* c) {
-  uint32_t p = ld_relaxed_gpu(&parent[x]);
-  uint32_t guard = 0;
-  while (p != x) {
-    const uint32_t gp = ld_relaxed_gpu(&parent[p]);
-    if (gp != p) st_relaxed_gpu(&parent[x], gp);
-    x = p;
-    p = gp;
-    if (++guard > (1u << 24)) {
-      raise_error(c, BB_ERRF_CAS_LIMIT);
-      return x;
-    }
+
+// Connected components in synchronous rounds inside one persistent kernel (counter 7 of the
+// substep's grid barriers): every round hooks, for each contact between two dynamic bodies,
+// the larger of the two parents under the smaller (atomicMin, so parents only decrease and
+// the forest stays acyclic), then lets every body jump one level (parent <- grandparent).  At
+// the fixpoint every body points at the smallest id of its component -- the same roots as the
+// reference's link-to-lower union-find (islands.slang:153-213) -- after O(log diameter)
+// rounds, with no serial walk of a long chain by any one thread.
+#define BB_CC_THREADS 512
+#define BB_CC_MAX_ROUNDS 96u
+__global__ void __launch_bounds__(BB_CC_THREADS, 1) k_components(const DevState d, int cur, uint32_t n) {
+  DevCounters* c = d.ctr;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const uint32_t M = c->manifold_count;
+  uint32_t* sync = &c->sync_count[7];
+  uint32_t* changed = &c->pad[2];  // two alternating per-round flags (the AVBD colouring reuses them later)
+  uint32_t ep = 0;
+  uint32_t* parent = d.uf_parent;
+  for (uint32_t i = tid; i < n; i += stride) parent[i] = (d.flags[i] & BB_BODY_DYNAMIC) ? i : BB_NONE;
+  if (tid == 0) {
+    changed[0] = 0;
+    changed[1] = 0;
   }
-  return x;
-}
-// IslandBuilder::link_bodies (islands.slang:153-213): link the higher root under the lower
-__global__ void k_uf_link(const DevState d, int cur) {
-  const uint32_t M = d.ctr->manifold_count;
-  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
-    uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
-    if (!(d.flags[b.x] & BB_BODY_DYNAMIC) || !(d.flags[b.y] & BB_BODY_DYNAMIC)) continue;
-    uint32_t ra = uf_find(d.uf_parent, b.x, d.ctr), rb = uf_find(d.uf_parent, b.y, d.ctr);
-    for (uint32_t tries = 0; ra != rb; ++tries) {
-      const uint32_t lo = min(ra, rb), hi = max(ra, rb);
-      const uint32_t old = atomicCAS(&d.uf_parent[hi], hi, lo);
-      if (old == hi) break;
-      // hi was linked meanwhile: continue from its new root
-      if (hi == ra) ra = uf_find(d.uf_parent, old, d.ctr);
-      else rb = uf_find(d.uf_parent, old, d.ctr);
-      if (tries > 4096u) {
-        raise_error(d.ctr, BB_ERRF_CAS_LIMIT);
-        break;
+  grid_sync(c, sync, ep);
+  uint32_t r = 0;
+  for (; r < BB_CC_MAX_ROUNDS; ++r) {
+    uint32_t any = 0;
+    for (uint32_t m = tid; m < M; m += stride) {
+      const uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+      const uint32_t pa = ld_relaxed_gpu(&parent[b.x]), pb = ld_relaxed_gpu(&parent[b.y]);
+      if (pa == BB_NONE || pb == BB_NONE || pa == pb) continue;
+      atomicMin(&parent[max(pa, pb)], min(pa, pb));
+      any = 1;
+    }
+    grid_sync(c, sync, ep);
+    for (uint32_t i = tid; i < n; i += stride) {
+      const uint32_t p = parent[i];
+      if (p == BB_NONE) continue;
+      const uint32_t pp = ld_relaxed_gpu(&parent[p]);
+      if (pp != p) {  // only this thread writes parent[i] in this pass
+        st_relaxed_gpu(&parent[i], pp);
+        any = 1;
       }
     }
+    if (any) atomicOr(&changed[r & 1], 1u);
+    grid_sync(c, sync, ep);
+    const bool more = *(volatile uint32_t*)&changed[r & 1] != 0u;
+    if (tid == 0) changed[(r + 1) & 1] = 0;
+    if (!more) break;
+    grid_sync(c, sync, ep);  // the reset above lands before anyone flags the next round
+  }
+  if (r == BB_CC_MAX_ROUNDS && tid == 0) raise_error(c, BB_ERRF_CAS_LIMIT);
+  for (uint32_t i = tid; i < n; i += stride) {
+    const uint32_t p = parent[i];
+    d.island[i] = p;  // root; rank applied by k_island_ids
+    d.is_root[i] = p == i ? 1u : 0u;
   }
 }
-__global__ void k_uf_roots(const DevState d, uint32_t n) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t r = d.uf_parent[i];
-  if (r == BB_NONE) {
-    d.is_root[i] = 0;
-    return;
-  }
-  r = uf_find(d.uf_parent, i, d.ctr);
-  d.island[i] = r;  // root for now; rank applied by k_island_ids
-  d.is_root[i] = r == i ? 1u : 0u;
-}
+
 __global__ void k_island_ids(const DevState d, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   d.island[i] = d.uf_parent[i] == BB_NONE ? BB_NONE : d.root_rank[d.island[i]];
 }
 
+int bb_components_blocks(int sms) { return bb_coop_blocks((const void*)k_components, BB_CC_THREADS, sms); }
+
 void bb_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
-                int cur) {
+                int cur, int coop_blocks) {
   (void)p;
+  (void)sms;
   if (n == 0) return;
   const int T = BB_THREADS;
   uint32_t blocks = (n + T - 1) / T;
-  k_uf_init<<<blocks, T, 0, s>>>(d, n);
-  k_uf_link<<<sms * 8, T, 0, s>>>(d, cur);
-  k_uf_roots<<<blocks, T, 0, s>>>(d, n);
+  DevState dd = d;
+  int cc = cur;
+  uint32_t nn = n;
+  void* args[] = {&dd, &cc, &nn};
+  bb_launch_coop((const void*)k_components, coop_blocks, BB_CC_THREADS, args, s);
   bb_launch_scan(s, d.is_root, d.root_rank, nullptr, n, &d.ctr->island_count, sc.scan_status + 3 * sc.scan_tiles,
                  sc.scan_tile_ctr + 3, d.ctr);
   k_island_ids<<<blocks, T, 0, s>>>(d, n);

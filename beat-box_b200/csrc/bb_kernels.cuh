@@ -38,7 +38,8 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
 // bb_graph.cu: advect, islands, sleeping, edge colouring + colour buckets
 void bb_advect(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int sms);
 void bb_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
-                int cur);
+                int cur, int coop_blocks);
+int bb_components_blocks(int sms);
 void bb_sleep(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, int sms, int cur);
 void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
                       int sms, int cur, int coop_blocks);

@@ -38,9 +38,14 @@ struct Shape {
   float half[3];
 };
 
+thread_local size_t t_alloc_bytes = 0;  // device bytes allocated by dalloc on this thread
+thread_local bool t_count_only = false;  // dalloc only counts (bb_world_bytes_for)
+
 template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& err) {
   void* p = nullptr;
   if (n == 0) n = 1;
+  t_alloc_bytes += n * sizeof(T);
+  if (t_count_only) return nullptr;
   cudaError_t e = cudaMalloc(&p, n * sizeof(T));
   if (e != cudaSuccess) {
     err = e;
@@ -157,9 +162,10 @@ struct bb_world_impl {
   int last_cur = 0;  // manifold buffer the last (partial or full) substep wrote
   bool skip_warm_once = false;
   bool ran_any = false;
-  int coop_edge = 0, coop_pgs = 0, coop_avbd = 0;
+  int coop_edge = 0, coop_pgs = 0, coop_avbd = 0, coop_cc = 0;
   size_t scratch_bytes = 0;
   void* scratch_base = nullptr;
+  size_t dev_bytes = 0;  // device memory held by this world
   // graph cache
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
@@ -196,8 +202,8 @@ struct bb_world_impl {
     d.range_last = dalloc<int32_t>(N, owned, err);
     d.visit = u32(N);
     d.pair_cnt = u32(N); d.pair_off = u32(N + 1);
-    d.is_heavy = u32(N); d.heavy_list = u32(1024);
-    d.bp_stage = u32(size_t(N) * 16);
+    d.is_heavy = u32(N); d.heavy_list = u32(8192);
+    d.bp_stage = u32(size_t(N) * 32);
     d.pairs = dalloc<uint2>(P, owned, err);
     for (int k = 0; k < 2; ++k) {
       d.m_bodies[k] = dalloc<uint2>(P, owned, err);
@@ -292,7 +298,7 @@ struct bb_world_impl {
     last_cur = cur;
     if (stop_stage < 3) return;
     bb_advect(stream, d, params, n, h, sms);
-    bb_islands(stream, d, params, n, sc, sms, cur);
+    bb_islands(stream, d, params, n, sc, sms, cur, coop_cc);
     bb_sleep(stream, d, params, n, sms, cur);
     bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
     if (params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, sms);
@@ -375,14 +381,22 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   uint32_t ppb = desc->pairs_per_body ? desc->pairs_per_body : 16;
   w->cap_p = uint32_t(std::min<uint64_t>(uint64_t(ppb) * w->cap_n + 1024, 0x3FFFFFFFull));
   bb_default_solver_params(&w->params);
+  t_alloc_bytes = 0;
   bb_status st = w->allocate();
+  w->dev_bytes = t_alloc_bytes;
   if (st != BB_OK) {
     delete w;
     return st;
   }
-  w->coop_edge = bb_edge_coloring_blocks(w->sms);
-  w->coop_pgs = bb_pgs_soft_blocks(w->sms);
-  w->coop_avbd = bb_avbd_blocks(w->sms);
+  // persistent grids sized to the world's capacity (about 3 manifolds per body), so the kernels
+  // of small worlds on other streams can run beside each other; results do not depend on it
+  auto fit = [](int max_blocks, uint64_t items, int threads) {
+    return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(max_blocks), (items + threads - 1) / threads)));
+  };
+  w->coop_edge = fit(bb_edge_coloring_blocks(w->sms), 3ull * w->cap_n, 1024);
+  w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), 3ull * w->cap_n, 256);
+  w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n, 512);
+  w->coop_cc = fit(bb_components_blocks(w->sms), 2ull * w->cap_n, BB_THREADS * 2);
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     delete w;
@@ -400,6 +414,41 @@ bb_status bb_world_destroy(void* world) {
 }
 
 void* bb_world_stream(void* world) { return world ? W(world)->stream : nullptr; }
+uint64_t bb_world_device_bytes(void* world) { return world ? W(world)->dev_bytes : 0; }
+
+uint64_t bb_world_bytes_for(uint32_t max_bodies, uint32_t pairs_per_body) {
+  World probe;
+  probe.cap_n = max_bodies;
+  const uint32_t ppb = pairs_per_body ? pairs_per_body : 16;
+  probe.cap_p = uint32_t(std::min<uint64_t>(uint64_t(ppb) * max_bodies + 1024, 0x3FFFFFFFull));
+  t_alloc_bytes = 0;
+  t_count_only = true;
+  probe.allocate();
+  t_count_only = false;
+  probe.owned.clear();
+  return t_alloc_bytes;
+}
+
+// Remove every body and shape; allocations, stream and parameters stay (for reuse of a world
+// object by a server).  Persistent contact state restarts as for a new world.
+bb_status bb_world_clear(void* world) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "bb_world_clear: null world");
+  CU(cudaStreamSynchronize(w->stream));
+  w->n = 0;
+  w->n_dyn = 0;
+  w->shapes.clear();
+  w->restitution.clear();
+  w->d.n_worlds = 0;
+  w->parity = 0;
+  w->last_cur = 0;
+  w->skip_warm_once = false;
+  w->ran_any = false;
+  w->invalidate_graphs();
+  uint32_t nn[2] = {0, 0};
+  CU(cudaMemcpy(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice));
+  return BB_OK;
+}
 uint32_t bb_body_count(void* world) { return world ? W(world)->n : 0; }
 
 bb_status bb_add_box_shape(void* world, float hx, float hy, float hz, uint32_t* out_shape) {
@@ -644,7 +693,7 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
       cudaEventRecord(ev[2], w->stream);
       bb_advect(w->stream, w->d, w->params, w->n, h, w->sms);
       cudaEventRecord(ev[3], w->stream);
-      bb_islands(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur);
+      bb_islands(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_cc);
       cudaEventRecord(ev[4], w->stream);
       bb_sleep(w->stream, w->d, w->params, w->n, w->sms, cur);
       cudaEventRecord(ev[5], w->stream);

@@ -480,6 +480,79 @@ def run_batched(args, rank: int, world_size: int, local_rank: int):
         dist.destroy_process_group()
 
 
+def run_served(args, rank: int, world_size: int, local_rank: int):
+    """Config 5: Poisson arrivals of step requests for worlds of 64..50,000 bodies (log-uniform;
+    config-1 piles), 1..120 steps each, PGS_SOFT or AVBD 50/50, half of them creating a world and
+    half continuing an existing one; worlds stay on the device between requests, admission by a
+    120 GB HBM budget.  For each arrival rate a fixed number of requests is submitted in real time
+    and served to completion; throughput and p50/p99 request latency are reported per rate."""
+    import numpy as np
+    import torch
+
+    import beatbox as bb
+
+    torch.cuda.set_device(local_rank)
+    rng = np.random.default_rng(5)
+    n_templates = 48
+    sizes = np.floor(np.exp(rng.uniform(np.log(64), np.log(50000), n_templates))).astype(int)
+    templates = [scenes.pile(int(nb), seed=200 + k) for k, nb in enumerate(sizes)]
+    arrays = [bb.scene_request_arrays(sc) for sc in templates]
+    p_pgs = bb.make_params(solver=bb.SOLVER_PGS_SOFT, iterations=10, relax_iterations=10, quirks=bb.QUIRKS_PHYSICAL)
+    p_avbd = bb.make_params(solver=bb.SOLVER_AVBD, avbd_iterations=4, avbd_beta=10.0, quirks=bb.QUIRKS_PHYSICAL)
+    srv = bb.Server(hbm_budget_bytes=120 << 30, max_active=args.max_active, pairs_per_body=8, device=local_rank)
+    clocks = sample_clocks(local_rank)
+    rates = [float(x) for x in args.rates.split(",")]
+    per_rate = []
+    next_key = 1
+    known = []  # (key, template) of worlds created so far
+    for lam in rates:
+        tickets = []
+        bodies = 0
+        t_start = time.perf_counter()
+        t_next = t_start
+        for _ in range(args.requests):
+            t_next += rng.exponential(1.0 / lam)
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            steps = int(rng.integers(1, 121))
+            params = p_pgs if rng.random() < 0.5 else p_avbd
+            if not known or rng.random() < 0.5:
+                k = int(rng.integers(0, n_templates))
+                key = next_key
+                next_key += 1
+                known.append((key, k))
+                tk = srv.submit(key, steps, params, DT, SUBSTEPS, scene=templates[k], arrays=arrays[k])
+            else:
+                key, k = known[int(rng.integers(0, len(known)))]
+                tk = srv.submit(key, steps, params, DT, SUBSTEPS)
+            tickets.append(tk)
+            bodies += int(templates[k]["n"]) * steps
+        res = [srv.wait(t) for t in tickets]
+        ok = [r for r in res if r["result"] == bb.OK]
+        lat = np.array([r["finish_s"] - r["submit_s"] for r in ok])
+        span = max(r["finish_s"] for r in res) - min(r["submit_s"] for r in res)
+        per_rate.append({"rate_req_s": lam, "requests": len(res), "failed": len(res) - len(ok),
+                         "body_steps_per_s": bodies / span if span > 0 else None,
+                         "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
+                         "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
+                         "submit_window_s": time.perf_counter() - t_start})
+    clk = finish_clocks(clocks)
+    st = srv.stats()
+    srv.close()
+    best = max(per_rate, key=lambda r: r["body_steps_per_s"] or 0)
+    line = {"metric": "body-steps/s", "value": best["body_steps_per_s"], "unit": "body-steps/s", "n_gpus": 1,
+            "steps": args.requests, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded piles and arrivals)",
+            "config": {"workload": "served: Poisson arrivals, worlds of floor(exp(U(ln 64, ln 50000))) bodies "
+                                   "(config-1 piles), 1..120 steps per request, PGS_SOFT 10 / AVBD 4 50/50, half new "
+                                   "worlds, 120 GB HBM budget, dt=1/60, 4 substeps",
+                       "rates_req_s": rates, "requests_per_rate": args.requests, "max_active": args.max_active},
+            "per_rate": per_rate, "server": st, "clocks": clk,
+            "value_is": "the best per-rate throughput (body-steps of the requests / first submit to last finish)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -492,8 +565,12 @@ def main():
                     help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids")
     ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched"],
-                    help="plain: one world (default); batched: config-4 batch of independent worlds")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: one world (default); batched: config-4 batch of independent worlds; "
+                         "served: config-5 serving loop")
+    ap.add_argument("--rates", default="200,500,1000,2000,5000")
+    ap.add_argument("--requests", type=int, default=150, help="requests per arrival rate (served mode)")
+    ap.add_argument("--max-active", type=int, default=64)
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--plain-stride", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -507,6 +584,9 @@ def main():
         run_reference(args, rank, world_size)
     elif args.mode == "batched":
         run_batched(args, rank, world_size, local_rank)
+    elif args.mode == "served":
+        if rank == 0:
+            run_served(args, rank, world_size, local_rank)
     else:
         run_ours(args, rank, world_size, local_rank)
 

@@ -314,6 +314,15 @@ void* bb_world_stream(void* world);
 bb_status bb_set_profiling(void* world, int32_t enabled);
 bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint32_t* n_stages,
                               char* names, uint32_t names_bytes);
+/* Device memory held by the world (all its buffers), in bytes; bb_world_bytes_for gives the
+ * same figure for a world not yet created.  No reference counterpart. */
+uint64_t bb_world_device_bytes(void* world);
+uint64_t bb_world_bytes_for(uint32_t max_bodies, uint32_t pairs_per_body);
+/* Remove all bodies and shapes, keeping the world's buffers, stream and parameters, so the
+ * object can hold a different scene (bodies added next restart the persistent state).  No
+ * reference counterpart (the reference reloads a scene into fixed buffers, RBM:224-254). */
+bb_status bb_world_clear(void* world);
+
 /* Number of kernels this library launched on the world's stream since creation. */
 uint64_t bb_kernel_launch_count(void* world);
 
@@ -344,6 +353,67 @@ bb_status bb_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* va
  * winner is set on the world and copied to *chosen (may be NULL).  The reference has no
  * autotuner (its dispatch sizes are fixed in the task graph, src/rigid_body_manager.cpp:1284-1427). */
 bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_steps, bb_solver_params* chosen);
+
+/* ---- serving loop ---------------------------------------------------------------------
+ * Step requests for many worlds, kept resident on the device between requests, admitted by an
+ * HBM budget; requests that arrive while others run start as soon as a slot and memory are
+ * free, and their steps overlap on the device (one stream per world).  A request either
+ * creates a world (its key not seen before; shapes and bodies given) or continues one.  A
+ * world runs its requests one after another in submission order; its result does not depend
+ * on the other requests in flight.  Idle worlds may be evicted to make room: their body state
+ * is kept on the host and reloaded (warm-start contacts restart).  No reference counterpart:
+ * the reference steps one scene per frame from its render loop (src/renderer_manager.cpp:254). */
+typedef struct bb_shape_desc {
+  uint32_t type;   /* BB_SHAPE_BOX or BB_SHAPE_SPHERE */
+  float half[3];   /* half extents; sphere radius in half[0] */
+} bb_shape_desc;
+
+typedef struct bb_server_desc {
+  uint64_t hbm_budget_bytes; /* device memory the server may hold in worlds */
+  uint32_t max_active;       /* requests in flight at once (0 = 64) */
+  uint32_t pairs_per_body;   /* pair capacity of the worlds it creates (0 = 8) */
+  int32_t device;            /* -1 = current device */
+} bb_server_desc;
+
+typedef struct bb_request {
+  uint64_t world;               /* caller's world key */
+  const bb_shape_desc* shapes;  /* new world: shape table (body.shape indexes it); else NULL */
+  uint32_t n_shapes;
+  const bb_body_desc* bodies;   /* new world: its bodies (copied by submit); else NULL */
+  uint32_t n_bodies;
+  float world_min[3];           /* new world: Morton normalisation box */
+  float world_extent[3];
+  bb_solver_params params;      /* this request's solver settings (Morton box fields ignored) */
+  float dt;
+  uint32_t substeps;
+  uint32_t steps;               /* bb_step(dt, substeps) calls */
+} bb_request;
+
+typedef struct bb_request_status {
+  uint32_t done;     /* 1 once finished */
+  bb_status result;  /* BB_OK, BB_E_BUDGET (the world can never fit the budget), ... */
+  double submit_s;   /* server clock, seconds since bb_server_create */
+  double start_s;
+  double finish_s;
+} bb_request_status;
+
+typedef struct bb_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t body_steps;       /* bodies x steps of the completed requests */
+  uint64_t evictions, worlds_created;
+  uint64_t resident_bytes;   /* device bytes held in resident and pooled worlds */
+  uint32_t active, queued, resident_worlds, known_worlds;
+} bb_server_stats;
+
+bb_status bb_server_create(const bb_server_desc* desc, void** out_server);
+bb_status bb_server_destroy(void* server); /* finishes queued requests first */
+bb_status bb_server_submit(void* server, const bb_request* req, uint64_t* out_ticket);
+bb_status bb_server_poll(void* server, uint64_t ticket, bb_request_status* out);
+bb_status bb_server_wait(void* server, uint64_t ticket, bb_request_status* out);
+/* Body state of a world after its last finished request (waits for a running one). */
+bb_status bb_server_read_state(void* server, uint64_t world, float* position, float* rotation, float* velocity,
+                               float* omega, uint32_t* n_bodies);
+bb_status bb_server_get_stats(void* server, bb_server_stats* out);
 
 /* Last error message of the calling thread (static storage, never NULL). */
 const char* bb_last_error_string(void);

@@ -1,0 +1,87 @@
+"""GPU tests of the serving loop (bb_server_*): every world's result is the same alone and in
+the mix of concurrent requests (bitwise), eviction under a tight HBM budget keeps requests
+completing, and a world that can never fit the budget is refused with BB_E_BUDGET."""
+import numpy as np
+import pytest
+
+import beatbox as bb
+from beatbox import scenes
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+GB = 1 << 30
+
+
+def req_params(k):
+    p = bb.make_params(solver=bb.SOLVER_PGS_SOFT if k % 2 == 0 else bb.SOLVER_AVBD, quirks=bb.QUIRKS_PHYSICAL,
+                       iterations=8, relax_iterations=8)
+    p.avbd_iterations = 4
+    return p
+
+
+WORLD_SIZES = [64, 150, 400, 900, 2000, 97]
+# (world index, steps) in submission order: worlds get several requests, interleaved
+PLAN = [(0, 5), (1, 12), (2, 3), (3, 8), (4, 6), (0, 7), (5, 20), (2, 9), (1, 4), (3, 2), (0, 3), (4, 5)]
+
+
+def run_plan(server, worlds, plan):
+    tickets = []
+    seen = set()
+    for j, (w, steps) in enumerate(plan):
+        sc = worlds[w] if w not in seen else None
+        seen.add(w)
+        tickets.append(server.submit(1000 + w, steps, req_params(j), DT, 2, scene=sc))
+    res = [server.wait(t) for t in tickets]
+    return res
+
+
+def test_each_world_is_the_same_alone_and_in_the_mix():
+    worlds = [scenes.pile(n, seed=k + 1) for k, n in enumerate(WORLD_SIZES)]
+    mix = bb.Server(hbm_budget_bytes=40 * GB, max_active=16)
+    res = run_plan(mix, worlds, PLAN)
+    assert all(r["done"] and r["result"] == bb.OK for r in res)
+    st = mix.stats()
+    assert st["completed"] == len(PLAN) and st["evictions"] == 0
+    assert st["body_steps"] == sum(int(worlds[w]["n"]) * s for w, s in PLAN)
+    mixed = {w: mix.read_state(1000 + w, int(worlds[w]["n"])) for w in range(len(worlds))}
+    mix.close()
+    for w in range(len(worlds)):
+        alone = bb.Server(hbm_budget_bytes=40 * GB, max_active=1)
+        plan_w = [(k, s) for k, (ww, s) in enumerate(PLAN) if ww == w]
+        seen = False
+        for j, s in plan_w:  # same request sequence, same request parameters, nothing else in flight
+            alone.wait(alone.submit(1000 + w, s, req_params(j), DT, 2, scene=None if seen else worlds[w]))
+            seen = True
+        a = alone.read_state(1000 + w, int(worlds[w]["n"]))
+        alone.close()
+        for key in a:
+            assert np.array_equal(a[key], mixed[w][key]), (w, key)
+
+
+def test_tight_budget_evicts_idle_worlds_and_keeps_serving():
+    worlds = [scenes.pile(n, seed=50 + k) for k, n in enumerate([1500, 1800, 1200, 1600])]
+    probe = bb.World(2048, pairs_per_body=8)
+    per_world = probe.L.bb_world_device_bytes(probe.h)
+    probe.close()
+    srv = bb.Server(hbm_budget_bytes=int(2.5 * per_world), max_active=4)
+    tickets = []
+    for rnd in range(3):
+        for w, sc in enumerate(worlds):
+            tickets.append(srv.submit(7 + w, 3, req_params(rnd), DT, 2, scene=sc if rnd == 0 else None))
+    res = [srv.wait(t) for t in tickets]
+    assert all(r["result"] == bb.OK for r in res)
+    st = srv.stats()
+    assert st["evictions"] > 0 and st["resident_bytes"] <= 2.5 * per_world
+    for w, sc in enumerate(worlds):
+        s = srv.read_state(7 + w, int(sc["n"]))
+        assert np.isfinite(s["pos"]).all() and (s["pos"][1:, 1] > -1.0).all()
+    srv.close()
+
+
+def test_world_larger_than_the_budget_is_refused():
+    srv = bb.Server(hbm_budget_bytes=1 << 20, max_active=2)
+    t = srv.submit(1, 2, req_params(0), DT, 1, scene=scenes.pile(500, seed=3))
+    r = srv.wait(t)
+    assert r["done"] and r["result"] == bb.E_BUDGET
+    srv.close()
