@@ -110,6 +110,7 @@ struct DevState {
   // per-body manifold lists (CSR over compact manifold indices) [cur], [prev]
   uint32_t* csr_start[2];
   uint32_t* csr_list[2];
+  uint32_t* csr_partner[2];  // other body of each list entry
   uint32_t* csr_cursor;
   uint32_t* hit;         // per pair slot: 1 if it produced a manifold
   uint32_t* man_index;   // per pair slot: exclusive scan of hit

@@ -452,17 +452,16 @@ __global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int 
     if (warm) {
       // find the pair's manifold of the previous substep on the dynamic body's list
       uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb;
+      const uint32_t other = x == ida ? idb : ida;
       uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
       uint32_t old_slot = BB_NONE;
       bool swapped = false;
       for (uint32_t e = s0; e < s1; ++e) {
-        uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
-        uint2 ob = d.m_bodies[prv][os];
-        if ((ob.x == ida && ob.y == idb) || (ob.x == idb && ob.y == ida)) {
-          old_slot = os;
-          swapped = ob.x != ida;
-          break;
-        }
+        if (d.csr_partner[prv][e] != other) continue;
+        const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
+        old_slot = os;
+        swapped = d.m_bodies[prv][os].x != ida;
+        break;
       }
       if (old_slot != BB_NONE) {
         // Manifold::update_from_old (extensions.slang:306-473)
@@ -609,6 +608,11 @@ __global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
       --b;
     }
     L[b] = v;
+  }
+  // partner body of every entry, so lookups by pair scan one contiguous array
+  for (uint32_t e = s0; e < s1; ++e) {
+    const uint2 b = d.m_bodies[cur][d.man_slot[cur][L[e]]];
+    d.csr_partner[cur][e] = b.x == i ? b.y : b.x;
   }
 }
 

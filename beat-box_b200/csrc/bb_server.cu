@@ -111,7 +111,7 @@ struct bb_server_impl {
       WorldRec* lru = nullptr;
       for (auto& kv : worlds) {
         WorldRec* wr = kv.second.get();
-        if (wr->world && !wr->busy && (!lru || wr->last_use < lru->last_use)) lru = wr;
+        if (!wr->busy && wr->world && (!lru || wr->last_use < lru->last_use)) lru = wr;
       }
       if (!lru) return false;
       evict(lru);
@@ -138,64 +138,57 @@ struct bb_server_impl {
     ++st.evictions;
   }
 
-  // make `wr` resident: a pooled or new world object of its class, shapes and bodies loaded
-  bb_status materialise(WorldRec* wr) {
-    const uint32_t n = uint32_t(wr->bodies.size());
-    wr->cls = class_of(n);
-    void* w = nullptr;
-    bb_status s = BB_OK;
-    auto it = pool.find(wr->cls);
-    if (it != pool.end() && !it->second.empty()) {
-      w = it->second.back();
-      it->second.pop_back();
-      s = bb_world_clear(w);
-    } else {
-      if (!make_room(bytes_of_class(wr->cls))) return BB_E_BUDGET;
-      bb_world_desc wd = {};
-      wd.max_bodies = 1u << wr->cls;
-      wd.pairs_per_body = desc.pairs_per_body ? desc.pairs_per_body : 8;
-      wd.device = desc.device;
-      s = bb_world_create(&wd, &w);
-      if (s != BB_OK) return s;
-      const uint64_t b = bb_world_device_bytes(w);
-      class_bytes[wr->cls] = b;
-      held_bytes += b;
-      ++st.worlds_created;
-    }
-    for (const bb_shape_desc& sh : wr->shapes) {  // handles come out as 0, 1, 2, ... in order
-      uint32_t h = 0;
-      if (s != BB_OK) break;
-      s = sh.type == BB_SHAPE_SPHERE ? bb_add_sphere_shape(w, sh.half[0], &h)
-                                     : bb_add_box_shape(w, sh.half[0], sh.half[1], sh.half[2], &h);
-    }
-    uint32_t first = 0;
-    if (s == BB_OK) s = bb_add_bodies(w, wr->bodies.data(), n, &first);
-    if (s != BB_OK) {
-      pool[wr->cls].push_back(w);
-      return s;
-    }
-    wr->world = w;
-    return BB_OK;
-  }
+  // Admission reserves what request q needs while the lock is held: a pooled world object of
+  // its class, or budget for a new one.  The slow part (creating the world, loading bodies,
+  // enqueueing the steps) runs after the lock is released, so submitters never wait on it.
+  struct Start {
+    Req* q = nullptr;
+    void* pooled = nullptr;  // reused world object (cleared before use)
+    uint64_t reserved = 0;   // budget reserved for a new world object
+    bb_status result = BB_OK;
+  };
 
-  // start request q on its world: parameters, all steps, completion event
-  bb_status start(Req* q) {
+  // outside the lock: materialise the world if needed, set parameters, enqueue all steps
+  void run_start(Start& sp) {
+    Req* q = sp.q;
     WorldRec* wr = q->w;
+    bb_status s = BB_OK;
     if (!wr->world) {
-      bb_status s = materialise(wr);
-      if (s != BB_OK) return s;
+      void* w = sp.pooled;
+      if (w) {
+        s = bb_world_clear(w);
+      } else {
+        bb_world_desc wd = {};
+        wd.max_bodies = 1u << wr->cls;
+        wd.pairs_per_body = desc.pairs_per_body ? desc.pairs_per_body : 8;
+        wd.device = desc.device;
+        s = bb_world_create(&wd, &w);
+        if (s != BB_OK) w = nullptr;
+      }
+      for (size_t k = 0; k < wr->shapes.size() && s == BB_OK; ++k) {  // handles come out as 0, 1, 2, ...
+        const bb_shape_desc& sh = wr->shapes[k];
+        uint32_t h = 0;
+        s = sh.type == BB_SHAPE_SPHERE ? bb_add_sphere_shape(w, sh.half[0], &h)
+                                       : bb_add_box_shape(w, sh.half[0], sh.half[1], sh.half[2], &h);
+      }
+      uint32_t first = 0;
+      if (s == BB_OK) s = bb_add_bodies(w, wr->bodies.data(), uint32_t(wr->bodies.size()), &first);
+      sp.pooled = w;  // the object now held for this world (nullptr if creation failed)
+      if (s != BB_OK) {
+        sp.result = s;
+        return;
+      }
     }
+    void* w = wr->world ? wr->world : sp.pooled;
     bb_solver_params p = q->r.params;
     std::memcpy(p.world_min, wr->wmin, sizeof(p.world_min));
     std::memcpy(p.world_extent, wr->wext, sizeof(p.world_extent));
     p.bounds_mode = BB_BOUNDS_FIXED;
-    bb_status s = bb_set_solver_params(wr->world, &p);
-    for (uint32_t k = 0; k < q->r.steps && s == BB_OK; ++k) s = bb_step(wr->world, q->r.dt, q->r.substeps);
-    if (s != BB_OK) return s;
-    if (cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming) != cudaSuccess) return BB_E_CUDA;
-    if (cudaEventRecord(q->ev, static_cast<cudaStream_t>(bb_world_stream(wr->world))) != cudaSuccess)
-      return BB_E_CUDA;
-    return BB_OK;
+    s = bb_set_solver_params(w, &p);
+    for (uint32_t k = 0; k < q->r.steps && s == BB_OK; ++k) s = bb_step(w, q->r.dt, q->r.substeps);
+    if (s == BB_OK && cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming) != cudaSuccess) s = BB_E_CUDA;
+    if (s == BB_OK && cudaEventRecord(q->ev, static_cast<cudaStream_t>(bb_world_stream(w))) != cudaSuccess) s = BB_E_CUDA;
+    sp.result = s;
   }
 
   void finish(Req* q, bb_status result) {
@@ -217,6 +210,7 @@ struct bb_server_impl {
 
   void loop() {
     if (desc.device >= 0) cudaSetDevice(desc.device);
+    std::vector<Start> todo;
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
       // retire finished requests
@@ -232,35 +226,65 @@ struct bb_server_impl {
         }
       }
       // admit in arrival order; a world runs one request at a time (later ones wait in order)
+      todo.clear();
       const uint32_t slots = desc.max_active ? desc.max_active : 64;
-      for (auto it = queue.begin(); it != queue.end() && active.size() < slots;) {
+      for (auto it = queue.begin(); it != queue.end() && active.size() + todo.size() < slots;) {
         Req* q = *it;
-        if (q->w->busy) {
+        WorldRec* wr = q->w;
+        if (wr->busy) {
           ++it;
           continue;
         }
-        if (!q->w->world) {
-          const uint64_t need = bytes_of_class(class_of(uint32_t(q->w->bodies.size())));
-          if (need > desc.hbm_budget_bytes) {  // can never fit
-            it = queue.erase(it);
-            q->start_s = now();
-            finish(q, BB_E_BUDGET);
-            continue;
-          }
-          if (!make_room(need)) {  // wait for running requests to free memory
-            ++it;
-            continue;
+        Start sp;
+        sp.q = q;
+        if (!wr->world) {
+          wr->cls = class_of(uint32_t(wr->bodies.size()));
+          auto pit = pool.find(wr->cls);
+          if (pit != pool.end() && !pit->second.empty()) {
+            sp.pooled = pit->second.back();
+            pit->second.pop_back();
+          } else {
+            const uint64_t need = bytes_of_class(wr->cls);
+            if (need > desc.hbm_budget_bytes) {  // can never fit
+              it = queue.erase(it);
+              q->start_s = now();
+              finish(q, BB_E_BUDGET);
+              continue;
+            }
+            if (!make_room(need)) {  // wait for running requests to free memory
+              ++it;
+              continue;
+            }
+            held_bytes += need;
+            sp.reserved = need;
           }
         }
-        q->w->busy = true;
+        wr->busy = true;
         q->start_s = now();
-        bb_status s = start(q);
         it = queue.erase(it);
-        if (s != BB_OK) {
-          finish(q, s);
-          continue;
+        todo.push_back(sp);
+      }
+      if (!todo.empty()) {
+        lk.unlock();
+        for (Start& sp : todo) run_start(sp);
+        lk.lock();
+        for (Start& sp : todo) {
+          Req* q = sp.q;
+          WorldRec* wr = q->w;
+          if (sp.reserved) {  // a new world object: account its real size
+            held_bytes -= sp.reserved;
+            if (sp.pooled) {
+              held_bytes += bb_world_device_bytes(sp.pooled);
+              ++st.worlds_created;
+            }
+          }
+          if (!wr->world && sp.pooled) {
+            if (sp.result == BB_OK) wr->world = sp.pooled;
+            else pool[wr->cls].push_back(sp.pooled);
+          }
+          if (sp.result != BB_OK) finish(q, sp.result);
+          else active.push_back(q);
         }
-        active.push_back(q);
       }
       st.resident_bytes = held_bytes;
       st.active = uint32_t(active.size());

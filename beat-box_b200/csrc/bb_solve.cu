@@ -393,7 +393,11 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
     }
     const uint32_t cn = c + 1 < C ? c + 1 : 0u;
     if (bs[cn] + tid < bs[cn + 1]) pgs_item_load(d, bs[cn] + tid, x);
-    grid_sync(d.ctr, sync, epoch);
+    // Two consecutive colours that both fit in block 0 (items map to threads by their index in
+    // the colour) need only a CTA barrier between them: every item and every body write of both
+    // lives in block 0.  The test reads shared bucket starts, so every block decides alike.
+    if (c + 1 < C && bs[c + 1] - bs[c] <= blockDim.x && bs[c + 2] - bs[c + 1] <= blockDim.x) __syncthreads();
+    else grid_sync(d.ctr, sync, epoch);
   }
   const uint32_t o0 = bs[BB_MAX_COLORS], o1 = bs[BB_MAX_COLORS + 1];
   if (o0 != o1) {  // overflow bucket: serial, in manifold order
@@ -654,8 +658,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevStat
       bool wait = false;
       const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
       for (uint32_t e = s0; e < s1 && !wait; ++e) {
-        uint2 b = d.m_bodies[cur][d.man_slot[cur][d.csr_list[cur][e]]];
-        uint32_t q = b.x == i ? b.y : b.x;
+        const uint32_t q = d.csr_partner[cur][e];
         if (q == i || !(d.flags[q] & BB_BODY_DYNAMIC)) continue;
         uint32_t pc = *(volatile uint32_t*)&d.body_color[q];
         bool unc = pc == BB_UNCOLORED || (pc >> 8) == rd + 1u;

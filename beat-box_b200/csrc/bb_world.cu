@@ -213,6 +213,7 @@ struct bb_world_impl {
       d.c_pos[k] = f4(C); d.c_lam[k] = f4(C); d.c_kt[k] = f4(C); d.c_anc_a[k] = f4(C); d.c_anc_b[k] = f4(C);
       d.csr_start[k] = u32(N + 1);
       d.csr_list[k] = u32(2 * P);
+      d.csr_partner[k] = u32(2 * P);
     }
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
     d.flow_rec = dalloc<uint4>(P, owned, err);

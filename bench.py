@@ -537,6 +537,7 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
                          "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
                          "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
                          "submit_window_s": time.perf_counter() - t_start})
+        print(json.dumps({"progress": per_rate[-1], "server": srv.stats()}), file=sys.stderr, flush=True)
     clk = finish_clocks(clocks)
     st = srv.stats()
     srv.close()
@@ -569,7 +570,7 @@ def main():
                     help="plain: one world (default); batched: config-4 batch of independent worlds; "
                          "served: config-5 serving loop")
     ap.add_argument("--rates", default="200,500,1000,2000,5000")
-    ap.add_argument("--requests", type=int, default=150, help="requests per arrival rate (served mode)")
+    ap.add_argument("--requests", type=int, default=60, help="requests per arrival rate (served mode)")
     ap.add_argument("--max-active", type=int, default=64)
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--plain-stride", type=int, default=16)
