@@ -326,6 +326,32 @@ __device__ __forceinline__ void grid_sync(DevCounters* c, uint32_t* count, uint3
   __syncthreads();
 }
 
+// grid_sync split in two: arrive publishes this block's writes and counts it in; wait returns
+// once every block of the epoch has arrived.  Work placed between them must neither read what
+// other blocks write in this epoch nor write what they read.
+__device__ __forceinline__ void grid_arrive(uint32_t* count, uint32_t& epoch) {
+  __syncthreads();
+  ++epoch;
+  if (threadIdx.x == 0) {
+    fence_acq_rel_gpu();
+    red_relaxed_add(count, 1u);
+  }
+}
+__device__ __forceinline__ void grid_wait(DevCounters* c, const uint32_t* count, uint32_t epoch) {
+  if (threadIdx.x == 0) {
+    const uint32_t target = epoch * gridDim.x;
+    uint32_t spins = 0;
+    while (ld_acquire_gpu(count) < target) {
+      if (++spins > BB_SPIN_LIMIT) {
+        atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
+        break;
+      }
+      if ((spins & 1023u) == 0u && (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT)) break;
+    }
+  }
+  __syncthreads();
+}
+
 // kernel-side solver parameters (a plain copy of bb_solver_params)
 typedef bb_solver_params Params;
 

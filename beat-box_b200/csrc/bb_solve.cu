@@ -266,6 +266,25 @@ struct PgsItem {
   float4 R1[BB_PGS_PF], R2[BB_PGS_PF], K[BB_PGS_PF], lam[BB_PGS_PF];
 };
 
+// item k given its record (loaded ahead): masses, frame, rows, impulses
+__device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k, uint4 rec, PgsItem& x) {
+  x.rec = rec;
+  x.mass = d.pgs_mass[k];
+  x.n = d.pgs_frame[3 * k];
+  x.t0 = d.pgs_frame[3 * k + 1];
+  x.t1 = d.pgs_frame[3 * k + 2];
+  const uint32_t c0 = rec.x, cc = rec.w & 0xFFu;
+#pragma unroll
+  for (int j = 0; j < BB_PGS_PF; ++j) {
+    if (uint32_t(j) < cc) {
+      x.R1[j] = d.c_r1[c0 + j];
+      x.R2[j] = d.c_r2[c0 + j];
+      x.K[j] = d.c_k[c0 + j];
+      x.lam[j] = d.pgs_lam[c0 + j];
+    }
+  }
+}
+
 __device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, PgsItem& x) {
   x.rec = d.pgs_rec[k];
   x.mass = d.pgs_mass[k];
@@ -379,9 +398,15 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
 }
 
 // one sweep over colours 0..C-1 and the overflow bucket.  On entry x holds this thread's first
-// item of colour 0; on exit it holds the same for the next sweep.
+// item of colour 0 and rec_next the record of its first item of colour 1 (or of colour 0 when
+// C == 1); on exit both are set the same way for the next sweep.  Records run one colour ahead
+// of the rest of the item, so the loads issued between barrier arrival and wait never wait on
+// an address; and they are issued after this block's arrival, so the arrival's fence does not
+// wait for them either.
+__device__ __forceinline__ uint32_t pgs_next_colour(uint32_t c, uint32_t C) { return c + 1 < C ? c + 1 : 0u; }
+
 __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode, const uint32_t* bs, uint32_t C,
-                          PgsItem& x, uint32_t& epoch) {
+                          PgsItem& x, uint4& rec_next, uint32_t& epoch) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* sync = &d.ctr->sync_count[1];
   for (uint32_t c = 0; c < C; ++c) {
@@ -391,13 +416,17 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
       k += stride;
       if (k < end) pgs_item_load(d, k, x);
     }
-    const uint32_t cn = c + 1 < C ? c + 1 : 0u;
-    if (bs[cn] + tid < bs[cn + 1]) pgs_item_load(d, bs[cn] + tid, x);
+    const uint32_t cn = pgs_next_colour(c, C), cnn = pgs_next_colour(cn, C);
+    const uint32_t kn = bs[cn] + tid, knn = bs[cnn] + tid;
     // Two consecutive colours that both fit in block 0 (items map to threads by their index in
     // the colour) need only a CTA barrier between them: every item and every body write of both
     // lives in block 0.  The test reads shared bucket starts, so every block decides alike.
-    if (c + 1 < C && bs[c + 1] - bs[c] <= blockDim.x && bs[c + 2] - bs[c + 1] <= blockDim.x) __syncthreads();
-    else grid_sync(d.ctr, sync, epoch);
+    const bool local = c + 1 < C && bs[c + 1] - bs[c] <= blockDim.x && bs[c + 2] - bs[c + 1] <= blockDim.x;
+    if (!local) grid_arrive(sync, epoch);
+    if (kn < bs[cn + 1]) pgs_item_load_rest(d, kn, rec_next, x);
+    if (knn < bs[cnn + 1]) rec_next = d.pgs_rec[knn];
+    if (local) __syncthreads();
+    else grid_wait(d.ctr, sync, epoch);
   }
   const uint32_t o0 = bs[BB_MAX_COLORS], o1 = bs[BB_MAX_COLORS + 1];
   if (o0 != o1) {  // overflow bucket: serial, in manifold order
@@ -431,15 +460,20 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d
   if (tid == 0)
     for (uint32_t k = bs[BB_MAX_COLORS]; k < bs[BB_MAX_COLORS + 1]; ++k) pgs_item_build(d, cur, k, list[k], h, hertz);
   PgsItem x;
+  uint4 rec_next = make_uint4(0, 0, 0, 0);
   if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, bs[0] + tid, x);
-  pgs_sweep(d, p, cur, 0, bs, C, x, epoch);
-  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, C, x, epoch);
+  if (C > 0) {
+    const uint32_t c1 = pgs_next_colour(0, C);
+    if (bs[c1] + tid < bs[c1 + 1]) rec_next = d.pgs_rec[bs[c1] + tid];
+  }
+  pgs_sweep(d, p, cur, 0, bs, C, x, rec_next, epoch);
+  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, C, x, rec_next, epoch);
   if (p.flags & BB_SIM_ADVECTION) {
     for (uint32_t i = tid; i < n; i += stride)
       if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
     grid_sync(d.ctr, sync, epoch);
   }
-  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, C, x, epoch);
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, C, x, rec_next, epoch);
   // impulses back to the persistent contacts (every sweep ended with a grid barrier)
   const uint32_t M = d.ctr->manifold_count;
   for (uint32_t k = tid; k < M; k += stride) {
