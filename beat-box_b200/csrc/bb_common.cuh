@@ -58,7 +58,10 @@ struct DevCounters {
   uint32_t substeps;       // substeps run since the world was created
   uint32_t pad[6];
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
-                           // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD
+                           // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
+                           // 7 connected components
+  uint32_t np_counts[2];   // narrow-phase work lists: box-box pairs, pairs with a sphere
+  uint32_t pad2[6];
 };
 
 // ---- pointers of one world's device state ------------------------------------------------
@@ -79,6 +82,7 @@ struct DevState {
   uint32_t *is_heavy, *heavy_list;  // 1: over the visit budget (block-cooperative), 2: staging spilled
   uint32_t* bp_stage;           // first 32 partners of each query (counting traversal)
   uint2* pairs;                 // (sorted a, sorted b)
+  uint32_t* np_list;            // narrow-phase work list (pair indices; see k_np_classify)
   // manifolds (two buffers: [cur], [prev] chosen by parity)
   uint2* m_bodies[2];    // body ids (a, b) per slot
   int2* m_keycc[2];      // key, contact count per slot

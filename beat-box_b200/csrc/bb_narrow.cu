@@ -381,17 +381,52 @@ __device__ __forceinline__ uint32_t warm_inc(uint32_t w) { return min(255u, w + 
 
 }  // namespace
 
-// Narrow phase + warm start: one thread per pair.
+// Work lists of the narrow phase: box-box pairs from the front of np_list, pairs with a sphere
+// from the back, static-static pairs (:1525) nowhere.  Every slot starts as "no manifold".
+// Grouping by shape keeps the warps of k_narrow on one code path (the box-box clip is long,
+// the sphere cases short); the outputs go to each pair's own slot, so the order in which the
+// lists fill does not matter.
+__global__ void k_np_classify(const DevState d, int cur) {
+  const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
+  const int lane = threadIdx.x & 31;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < P; base += gridDim.x * blockDim.x) {
+    const uint32_t k = base + threadIdx.x;
+    int kind = -1;  // 0 box-box, 1 with a sphere
+    if (k < P) {
+      d.hit[k] = 0;
+      d.m_keycc[cur][k] = make_int2(-1, 0);
+      const uint2 pr = d.pairs[k];
+      const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
+      if ((d.flags[ida] & BB_BODY_DYNAMIC) || (d.flags[idb] & BB_BODY_DYNAMIC)) {
+        const uint32_t ta = __float_as_uint(d.shape[ida].w), tb = __float_as_uint(d.shape[idb].w);
+        kind = (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1;
+      }
+    }
+#pragma unroll
+    for (int kd = 0; kd < 2; ++kd) {
+      const unsigned mask = __ballot_sync(0xFFFFFFFFu, kind == kd);
+      if (!mask) continue;
+      uint32_t off = 0;
+      if (lane == 0) off = atomicAdd(&d.ctr->np_counts[kd], uint32_t(__popc(mask)));
+      off = __shfl_sync(0xFFFFFFFFu, off, 0);
+      if (kind == kd) {
+        const uint32_t r = off + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+        d.np_list[kd == 0 ? r : P - 1 - r] = k;
+      }
+    }
+  }
+}
+
+// Narrow phase + warm start: one thread per listed pair.
 __global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int cur, int warm) {
   const int prv = cur ^ 1;
   const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x) {
+  const uint32_t nbb = d.ctr->np_counts[0], ntot = nbb + d.ctr->np_counts[1];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += gridDim.x * blockDim.x) {
+    const uint32_t k = d.np_list[t < nbb ? t : P - 1 - (t - nbb)];
     uint2 pr = d.pairs[k];
     uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
-    uint32_t fa = d.flags[ida], fb = d.flags[idb];
-    d.hit[k] = 0;
-    d.m_keycc[cur][k] = make_int2(-1, 0);
-    if (!(fa & BB_BODY_DYNAMIC) && !(fb & BB_BODY_DYNAMIC)) continue;  // static-static (:1525)
+    const uint32_t fa = d.flags[ida];
     float4 pa4 = d.pos[ida], pb4 = d.pos[idb];
     float4 sa = d.shape[ida], sb = d.shape[idb];
     Quatf qa = q_from(d.rot[ida]), qb = q_from(d.rot[idb]);
@@ -620,6 +655,7 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
                      int cur, bool warm) {
   const int T = BB_THREADS;
   int grid = sms * 8;
+  k_np_classify<<<sms * 8, 256, 0, s>>>(d, cur);
   k_narrow<<<sms * (p.narrow_blocks_per_sm ? p.narrow_blocks_per_sm : 16u), 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
   // compact order: exclusive scan of the hit flags over the pair slots
   bb_launch_scan(s, d.hit, d.man_index, &d.ctr->pair_count, d.pair_capacity, &d.ctr->manifold_count,

@@ -143,6 +143,8 @@ __global__ void k_begin_substep(DevCounters* c) {
   }
   for (int k = 0; k < 6; ++k) c->pad[k] = 0;
   for (int k = 0; k < 8; ++k) c->sync_count[k] = 0;
+  c->np_counts[0] = 0;
+  c->np_counts[1] = 0;
   c->substeps += 1;
 }
 
@@ -218,6 +220,7 @@ struct bb_world_impl {
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
     d.flow_rec = dalloc<uint4>(P, owned, err);
     d.pgs_rec = dalloc<uint4>(P, owned, err);
+    d.np_list = u32(P);
     d.gc_rec = dalloc<uint4>(P, owned, err);
     d.pgs_mass = f4(P);
     d.pgs_frame = f4(3 * P);
