@@ -314,6 +314,7 @@ __device__ __forceinline__ void red_relaxed_add(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ void grid_sync(DevCounters* c, uint32_t* count, uint32_t& epoch) {
   __syncthreads();
   ++epoch;
+  if (gridDim.x == 1) return;  // one block: the CTA barrier is the grid barrier
   if (threadIdx.x == 0) {
     fence_acq_rel_gpu();  // release this block's writes (cumulative over the CTA barrier)
     red_relaxed_add(count, 1u);
@@ -336,13 +337,13 @@ __device__ __forceinline__ void grid_sync(DevCounters* c, uint32_t* count, uint3
 __device__ __forceinline__ void grid_arrive(uint32_t* count, uint32_t& epoch) {
   __syncthreads();
   ++epoch;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && gridDim.x > 1) {
     fence_acq_rel_gpu();
     red_relaxed_add(count, 1u);
   }
 }
 __device__ __forceinline__ void grid_wait(DevCounters* c, const uint32_t* count, uint32_t epoch) {
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && gridDim.x > 1) {
     const uint32_t target = epoch * gridDim.x;
     uint32_t spins = 0;
     while (ld_acquire_gpu(count) < target) {

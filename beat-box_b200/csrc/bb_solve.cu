@@ -251,7 +251,6 @@ __device__ __forceinline__ void pgs_integrate(const DevState& d, uint32_t i, flo
 // thread writes -- BEFORE the barrier, and after the barrier only the two bodies' velocities
 // and inertias remain to be fetched: one memory round trip per colour on the critical path.
 #define BB_PGS_THREADS 256  // one block per SM: up to 255 registers for the held item
-#define BB_PGS_PF 4         // contacts of an item held in registers across the barrier
 #define BB_PGS_SKIP (1u << 10)
 
 // The kernel works on a compact copy in colour order: item k's record, masses and contact frame
@@ -259,15 +258,17 @@ __device__ __forceinline__ void pgs_integrate(const DevState& d, uint32_t i, flo
 // (pgs_lam) at pgs_coff[k] + j.  The impulses go back to the persistent slot-indexed contacts
 // when the kernel ends.  Dense arrays keep the per-sweep working set (about 80 B per manifold,
 // 64 B per contact, 64 B per body) resident in L2.
+template <int PF>  // contacts of an item held in registers across the barrier
 struct PgsItem {
   uint4 rec;    // contact offset, body a, body b, contact count | dynamic a << 8 | dynamic b << 9 | skip << 10
   float4 mass;  // inverse mass a, inverse mass b, friction, -
   float4 n, t0, t1;
-  float4 R1[BB_PGS_PF], R2[BB_PGS_PF], K[BB_PGS_PF], lam[BB_PGS_PF];
+  float4 R1[PF], R2[PF], K[PF], lam[PF];
 };
 
 // item k given its record (loaded ahead): masses, frame, rows, impulses
-__device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k, uint4 rec, PgsItem& x) {
+template <int PF>
+__device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k, uint4 rec, PgsItem<PF>& x) {
   x.rec = rec;
   x.mass = d.pgs_mass[k];
   x.n = d.pgs_frame[3 * k];
@@ -275,7 +276,7 @@ __device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k
   x.t1 = d.pgs_frame[3 * k + 2];
   const uint32_t c0 = rec.x, cc = rec.w & 0xFFu;
 #pragma unroll
-  for (int j = 0; j < BB_PGS_PF; ++j) {
+  for (int j = 0; j < PF; ++j) {
     if (uint32_t(j) < cc) {
       x.R1[j] = d.c_r1[c0 + j];
       x.R2[j] = d.c_r2[c0 + j];
@@ -285,7 +286,8 @@ __device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k
   }
 }
 
-__device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, PgsItem& x) {
+template <int PF>
+__device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, PgsItem<PF>& x) {
   x.rec = d.pgs_rec[k];
   x.mass = d.pgs_mass[k];
   x.n = d.pgs_frame[3 * k];
@@ -293,7 +295,7 @@ __device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, Pgs
   x.t1 = d.pgs_frame[3 * k + 2];
   const uint32_t c0 = x.rec.x, cc = x.rec.w & 0xFFu;
 #pragma unroll
-  for (int j = 0; j < BB_PGS_PF; ++j) {
+  for (int j = 0; j < PF; ++j) {
     if (uint32_t(j) < cc) {
       x.R1[j] = d.c_r1[c0 + j];
       x.R2[j] = d.c_r2[c0 + j];
@@ -354,7 +356,8 @@ __device__ void pgs_item_build(const DevState& d, int cur, uint32_t k, uint32_t 
 }
 
 // mode 0: warm start, 1: solve sweep (soft bias), 2: relax sweep
-__device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p, int cur, PgsItem& x, int mode) {
+template <int PF>
+__device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p, int cur, PgsItem<PF>& x, int mode) {
   if (x.rec.w & BB_PGS_SKIP) return;
   const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
   if (mode == 0 && !accum) return;
@@ -365,7 +368,7 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
   const float ima = x.mass.x, imb = x.mass.y, mu = x.mass.z;
   const float3 n = f3(x.n), t0 = f3(x.t0), t1 = f3(x.t1);
 #pragma unroll
-  for (int j = 0; j < BB_PGS_PF; ++j) {
+  for (int j = 0; j < PF; ++j) {
     if (uint32_t(j) < cc) {
       if (mode == 0) {
         pgs_contact_warm(f3(x.R1[j]), f3(x.R2[j]), x.lam[j], n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
@@ -376,7 +379,7 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
       }
     }
   }
-  for (uint32_t j = BB_PGS_PF; j < cc; ++j) {  // contacts beyond the register-held ones
+  for (uint32_t j = PF; j < cc; ++j) {  // contacts beyond the register-held ones
     const uint32_t ci = c0 + j;
     float4 lam = d.pgs_lam[ci];
     if (mode == 0) {
@@ -405,8 +408,9 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
 // wait for them either.
 __device__ __forceinline__ uint32_t pgs_next_colour(uint32_t c, uint32_t C) { return c + 1 < C ? c + 1 : 0u; }
 
+template <int PF>
 __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode, const uint32_t* bs, uint32_t C,
-                          PgsItem& x, uint4& rec_next, uint32_t& epoch) {
+                          PgsItem<PF>& x, uint4& rec_next, uint32_t& epoch) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* sync = &d.ctr->sync_count[1];
   for (uint32_t c = 0; c < C; ++c) {
@@ -432,7 +436,7 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
   if (o0 != o1) {  // overflow bucket: serial, in manifold order
     if (tid == 0) {
       for (uint32_t k = o0; k < o1; ++k) {
-        PgsItem y;
+        PgsItem<PF> y;
         pgs_item_load(d, k, y);
         pgs_item_run(d, p, cur, y, mode);
       }
@@ -441,7 +445,10 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
   }
 }
 
-__global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
+// PF = 4 for large worlds (one 255-register block per SM); PF = 1 for small worlds, whose few
+// blocks then need only part of an SM and can run beside other worlds' kernels
+template <int PF>
+__global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   __shared__ uint32_t bs[BB_MAX_COLORS + 2];
   if (threadIdx.x < BB_MAX_COLORS + 2) bs[threadIdx.x] = d.bucket_start[threadIdx.x];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
@@ -459,7 +466,7 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d
     for (uint32_t k = bs[c] + tid; k < bs[c + 1]; k += stride) pgs_item_build(d, cur, k, list[k], h, hertz);
   if (tid == 0)
     for (uint32_t k = bs[BB_MAX_COLORS]; k < bs[BB_MAX_COLORS + 1]; ++k) pgs_item_build(d, cur, k, list[k], h, hertz);
-  PgsItem x;
+  PgsItem<PF> x;
   uint4 rec_next = make_uint4(0, 0, 0, 0);
   if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, bs[0] + tid, x);
   if (C > 0) {
@@ -484,7 +491,7 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, 1) k_pgs_soft(const DevState d
   }
 }
 
-int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft, BB_PGS_THREADS, sms); }
+int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft<4>, BB_PGS_THREADS, sms); }
 
 
 // ---------------------------------------------------------------------------------------
@@ -643,7 +650,8 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
-  bb_launch_coop((const void*)k_pgs_soft, coop_blocks, BB_PGS_THREADS, args, s);
+  const void* kern = coop_blocks > 16 ? (const void*)k_pgs_soft<4> : (const void*)k_pgs_soft<1>;
+  bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s);
 }
 
 // ---------------------------------------------------------------------------------------

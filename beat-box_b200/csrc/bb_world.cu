@@ -392,15 +392,17 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
     delete w;
     return st;
   }
-  // persistent grids sized to the world's capacity (about 3 manifolds per body), so the kernels
-  // of small worlds on other streams can run beside each other; results do not depend on it
+  // Persistent grids sized to the world's capacity: about one thread per item of the largest
+  // colour (~half the bodies) for the sweeps, about one per body for colouring and components.
+  // A small world then runs on a block or two (its barriers become CTA barriers) and leaves
+  // the rest of the GPU to other worlds' streams.  Results do not depend on the grid.
   auto fit = [](int max_blocks, uint64_t items, int threads) {
     return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(max_blocks), (items + threads - 1) / threads)));
   };
-  w->coop_edge = fit(bb_edge_coloring_blocks(w->sms), 3ull * w->cap_n, 1024);
-  w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), 3ull * w->cap_n, 256);
-  w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n, 512);
-  w->coop_cc = fit(bb_components_blocks(w->sms), 2ull * w->cap_n, BB_THREADS * 2);
+  w->coop_edge = fit(bb_edge_coloring_blocks(w->sms), w->cap_n, 1024);
+  w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), w->cap_n / 2, 256);
+  w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n / 2, 512);
+  w->coop_cc = fit(bb_components_blocks(w->sms), w->cap_n, 512);
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     delete w;

@@ -508,6 +508,7 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
     for lam in rates:
         tickets = []
         bodies = 0
+        submit_s = []
         t_start = time.perf_counter()
         t_next = t_start
         for _ in range(args.requests):
@@ -522,10 +523,13 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
                 key = next_key
                 next_key += 1
                 known.append((key, k))
+                t_call = time.perf_counter()
                 tk = srv.submit(key, steps, params, DT, SUBSTEPS, scene=templates[k], arrays=arrays[k])
             else:
                 key, k = known[int(rng.integers(0, len(known)))]
+                t_call = time.perf_counter()
                 tk = srv.submit(key, steps, params, DT, SUBSTEPS)
+            submit_s.append(time.perf_counter() - t_call)
             tickets.append(tk)
             bodies += int(templates[k]["n"]) * steps
         res = [srv.wait(t) for t in tickets]
@@ -536,7 +540,10 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
                          "body_steps_per_s": bodies / span if span > 0 else None,
                          "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
                          "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
-                         "submit_window_s": time.perf_counter() - t_start})
+                         "submit_window_s": time.perf_counter() - t_start,
+                         "submit_call_ms_max": 1000 * max(submit_s),
+                         "queue_wait_ms_p50": float(np.percentile([r["start_s"] - r["submit_s"] for r in res], 50) * 1000),
+                         "run_ms_p50": float(np.percentile([r["finish_s"] - r["start_s"] for r in res], 50) * 1000)})
         print(json.dumps({"progress": per_rate[-1], "server": srv.stats()}), file=sys.stderr, flush=True)
     clk = finish_clocks(clocks)
     st = srv.stats()
