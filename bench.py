@@ -42,20 +42,30 @@ def workload(args):
         sc = scenes.pyramids(n_pyramids=n_pyr, boxes_per=1000, seed=0)
         name = (f"pyramids_{n_pyr}x1000: {n_pyr} pyramids of 1000 unit boxes (base 18x18) on a 32x32 grid, "
                 f"velocity N(0, 0.01) m/s, dt=1/60, {SUBSTEPS} substeps, ")
+    elif args.scene == "box_grid":
+        sc = scenes.box_grid(n_side=10, seed=0)
+        sc["bounds"] = ([-64.0] * 3, [128.0] * 3)  # the reference's Morton box
+        name = (f"box_grid_1000: 1000 unit boxes (10x10x10, 1.1 m spacing, jitter 0.05 m, random yaw) "
+                f"dropped on a ground box, dt=1/60, {SUBSTEPS} substeps, ")
     else:
         sc = scenes.mixed_column(n_bodies=args.bodies, seed=0)
         name = (f"mixed_column_{args.bodies // 1000}k: {args.bodies} bodies (60% boxes / 40% spheres) in a "
                 f"60x60x200 m column, 5-wall container, dt=1/60, {SUBSTEPS} substeps, ")
     if args.solver == "pgs":
-        name += f"PGS_SOFT 10 iterations ({args.schedule} schedule)"
+        name += f"PGS_SOFT {pgs_iterations(args)} iterations ({args.schedule} schedule)"
     else:
         name += "AVBD 4 iterations (beta=10)"
     return sc, name
 
 
 def run_steps(args) -> int:
-    """Length of the configuration's run: 600 steps for the mixed column, 300 for the pyramids."""
-    return 300 if args.scene == "pyramids" else 600
+    """Length of the configuration's run: 600 steps for the mixed column, 300 for the others."""
+    return 600 if args.scene == "mixed_column" else 300
+
+
+def pgs_iterations(args) -> int:
+    """PGS solve (and relax) iterations: 8 for the 1000-box grid, 10 for the others."""
+    return 8 if args.scene == "box_grid" else 10
 
 
 def timed_window(args) -> int:
@@ -65,7 +75,7 @@ def timed_window(args) -> int:
 
 def solver_fields(args) -> dict:
     if args.solver == "pgs":
-        return dict(solver=1, iterations=10, relax_iterations=10, quirks=0,
+        return dict(solver=1, iterations=pgs_iterations(args), relax_iterations=pgs_iterations(args), quirks=0,
                     schedule=0 if args.schedule == "dataflow" else 1)
     return dict(solver=2, avbd_iterations=4, avbd_beta=10.0, quirks=0)
 
@@ -569,8 +579,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="pgs", choices=["pgs", "avbd"])
     ap.add_argument("--bodies", type=int, default=N_BODIES)
-    ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids"],
-                    help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids")
+    ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids", "box_grid"],
+                    help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids; "
+                         "box_grid: the 1000-box grid")
     ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
