@@ -61,7 +61,8 @@ struct DevCounters {
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
                            // 7 connected components
   uint32_t np_counts[2];   // narrow-phase work lists: box-box pairs, pairs with a sphere
-  uint32_t pad2[6];
+  uint32_t gc_list_n[2];   // edge colouring: sizes of the alternating uncoloured-manifold lists
+  uint32_t pad2[4];
 };
 
 // ---- pointers of one world's device state ------------------------------------------------
@@ -125,6 +126,7 @@ struct DevState {
   uint32_t* gc_pid;      // pair-identity hash
   uint32_t* gc_choice;
   uint4* gc_rec;         // per compact manifold: body a, body b, pair hash, static bits
+  uint32_t* gc_list[2];  // manifolds still uncoloured after a round (alternating)
   uint32_t* gc_mask;     // per body
   unsigned long long* gc_owner; // per body x 32 colours: (epoch << 32) | priority
   uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies

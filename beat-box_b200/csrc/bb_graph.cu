@@ -241,7 +241,6 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   const uint32_t M = c->manifold_count;
   const uint32_t epoch = c->gc_epoch;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  uint32_t* uncol = &c->pad[0];  // two alternating per-round counters
   uint32_t* sync = &c->sync_count[0];
   uint32_t ep = 0;
   for (uint32_t i = tid; i < n; i += stride) d.gc_mask[i] = 0;
@@ -258,16 +257,23 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
     d.gc_rec[m] = make_uint4(b.x, b.y, pid, st);
   }
   if (tid == 0) {
-    uncol[1] = 0;
     c->gc_colors = 0;
+    c->gc_list_n[0] = 0;
   }
   grid_sync(c, sync, ep);
+  // Round r bids and commits over the manifolds still uncoloured when it starts: all of them in
+  // round 1, afterwards the list the previous round's commit left (in any order: a round's
+  // outcome depends only on its set, since the highest priority wins every contested colour).
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
   for (uint32_t r = 1; r <= p.gc_rounds; ++r) {
+    const uint32_t* L = r == 1 ? nullptr : d.gc_list[r & 1];
+    const uint32_t nL = r == 1 ? M : *(volatile uint32_t*)&c->gc_list_n[r & 1];
+    if (nL == 0) break;
+    if (tid == 0) c->gc_list_n[(r + 1) & 1] = 0;  // the list this round fills (last read two rounds ago)
     const unsigned long long tag = (unsigned long long)(epoch + r) << 32;
-    uint32_t mine = 0;
-    for (uint32_t m = tid; m < M; m += stride) {
-      if (d.gc_color[m] != BB_UNCOLORED) continue;
-      ++mine;
+    for (uint32_t i = tid; i < nL; i += stride) {
+      const uint32_t m = L ? L[i] : i;
       const uint4 rec = d.gc_rec[m];
       const bool sa = rec.w & 1u, sb = rec.w & 2u;
       uint32_t avail = ~((sa ? 0u : d.gc_mask[rec.x]) | (sb ? 0u : d.gc_mask[rec.y]));
@@ -278,24 +284,37 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
       if (!sa) atomicMax(&d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col], v);
       if (!sb) atomicMax(&d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col], v);
     }
-    if (mine) atomicAdd(&uncol[r & 1], mine);
     grid_sync(c, sync, ep);
-    if (*(volatile uint32_t*)&uncol[r & 1] == 0u) break;
-    if (tid == 0) uncol[(r + 1) & 1] = 0;
-    for (uint32_t m = tid; m < M; m += stride) {
-      if (d.gc_color[m] != BB_UNCOLORED) continue;
-      uint32_t col = d.gc_choice[m];
-      if (col >= BB_MAX_COLORS) continue;
-      const uint4 rec = d.gc_rec[m];
-      const bool sa = rec.w & 1u, sb = rec.w & 2u;
-      unsigned long long v = tag | gc_priority(rec.z, r);
-      bool wa = sa || d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col] == v;
-      bool wb = sb || d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col] == v;
-      if (wa && wb) {
-        d.gc_color[m] = col;
-        if (!sa) atomicOr(&d.gc_mask[rec.x], 1u << col);
-        if (!sb) atomicOr(&d.gc_mask[rec.y], 1u << col);
-        atomicMax(&c->gc_colors, col + 1u);
+    uint32_t* next = d.gc_list[(r + 1) & 1];
+    for (uint32_t base = warp0; base < nL; base += stride) {  // warp-uniform trip count
+      const uint32_t i = base + lane;
+      bool keep = false;
+      uint32_t m = 0;
+      if (i < nL) {
+        m = L ? L[i] : i;
+        const uint32_t col = d.gc_choice[m];
+        keep = true;
+        if (col < BB_MAX_COLORS) {
+          const uint4 rec = d.gc_rec[m];
+          const bool sa = rec.w & 1u, sb = rec.w & 2u;
+          unsigned long long v = tag | gc_priority(rec.z, r);
+          bool wa = sa || d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col] == v;
+          bool wb = sb || d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col] == v;
+          if (wa && wb) {
+            d.gc_color[m] = col;
+            if (!sa) atomicOr(&d.gc_mask[rec.x], 1u << col);
+            if (!sb) atomicOr(&d.gc_mask[rec.y], 1u << col);
+            atomicMax(&c->gc_colors, col + 1u);
+            keep = false;
+          }
+        }
+      }
+      const unsigned mask = __ballot_sync(0xFFFFFFFFu, keep);
+      if (mask) {
+        uint32_t off = 0;
+        if (lane == 0) off = atomicAdd(&c->gc_list_n[(r + 1) & 1], uint32_t(__popc(mask)));
+        off = __shfl_sync(0xFFFFFFFFu, off, 0);
+        if (keep) next[off + __popc(mask & ((1u << lane) - 1u))] = m;
       }
     }
     grid_sync(c, sync, ep);

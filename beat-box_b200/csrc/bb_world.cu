@@ -145,6 +145,8 @@ __global__ void k_begin_substep(DevCounters* c) {
   for (int k = 0; k < 8; ++k) c->sync_count[k] = 0;
   c->np_counts[0] = 0;
   c->np_counts[1] = 0;
+  c->gc_list_n[0] = 0;
+  c->gc_list_n[1] = 0;
   c->substeps += 1;
 }
 
@@ -222,6 +224,7 @@ struct bb_world_impl {
     d.pgs_rec = dalloc<uint4>(P, owned, err);
     d.np_list = u32(P);
     d.gc_rec = dalloc<uint4>(P, owned, err);
+    d.gc_list[0] = u32(P); d.gc_list[1] = u32(P);
     d.pgs_mass = f4(P);
     d.pgs_frame = f4(3 * P);
     d.pgs_lam = f4(8 * P);
