@@ -54,21 +54,68 @@ __device__ __forceinline__ Quatf apply_angular_velocity(Quatf rot, float3 w, flo
 // ---- PGS_SOFT arithmetic of one contact, shared by both schedules (same expressions, so the
 // schedules agree bit for bit) -------------------------------------------------------------
 
+// Every operation below is an explicitly rounded intrinsic (fma where a product feeds a sum),
+// so the compiler has nothing left to contract: each inlined copy of this arithmetic -- the
+// barrier schedule's register-held and streamed contacts, the dataflow schedule -- produces
+// the same bits.
+__device__ __forceinline__ float3 xadd(float3 a, float3 b) {
+  return make_float3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 xsub(float3 a, float3 b) {
+  return make_float3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 xscale(float3 a, float s) {
+  return make_float3(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s));
+}
+__device__ __forceinline__ float3 xaxpy(float3 a, float s, float3 y) {  // a * s + y
+  return make_float3(__fmaf_rn(a.x, s, y.x), __fmaf_rn(a.y, s, y.y), __fmaf_rn(a.z, s, y.z));
+}
+__device__ __forceinline__ float xdot(float3 a, float3 b) {
+  return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+__device__ __forceinline__ float3 xcross(float3 a, float3 b) {
+  return make_float3(__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+                     __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float3 xsym(const Sym3& s, float3 v) {
+  return make_float3(__fmaf_rn(s.xz, v.z, __fmaf_rn(s.xy, v.y, __fmul_rn(s.xx, v.x))),
+                     __fmaf_rn(s.yz, v.z, __fmaf_rn(s.yy, v.y, __fmul_rn(s.xy, v.x))),
+                     __fmaf_rn(s.zz, v.z, __fmaf_rn(s.yz, v.y, __fmul_rn(s.xz, v.x))));
+}
+// v_a -= P m_a, w_a -= I_a (r1 x P), v_b += P m_b, w_b += I_b (r2 x P)
+__device__ __forceinline__ void xapply(float3 P, float3 r1, float3 r2, float ima, float imb, const Sym3& IA,
+                                       const Sym3& IB, float3& va, float3& wa, float3& vb, float3& wb) {
+  va = xaxpy(P, -ima, va);
+  wa = xsub(wa, xsym(IA, xcross(r1, P)));
+  vb = xaxpy(P, imb, vb);
+  wb = xadd(wb, xsym(IB, xcross(r2, P)));
+}
+
 // soft-constraint coefficients of a manifold (solvers.slang:150-158)
 struct SoftCoef {
   float bf, mcoef, icoef, inv_h;
 };
 __device__ __forceinline__ SoftCoef pgs_soft_coef(float ima, float imb, float h, float hertz) {
-  const float ch = (ima == 0.f || imb == 0.f) ? 2.0f * hertz : hertz;
+  const float ch = (ima == 0.f || imb == 0.f) ? __fmul_rn(2.0f, hertz) : hertz;
   const float zeta = 10.0f;
-  const float omega = 2.0f * 3.14159265359f * ch;
-  const float c = h * omega * (2.0f * zeta + h * omega);
+  const float omega = __fmul_rn(2.0f * 3.14159265359f, ch);
+  const float ho = __fmul_rn(h, omega);
+  const float den = __fadd_rn(2.0f * zeta, ho);
+  const float c = __fmul_rn(ho, den);
   SoftCoef s;
-  s.bf = omega / (2.0f * zeta + h * omega);
-  s.icoef = 1.0f / (1.0f + c);
-  s.mcoef = c * s.icoef;
-  s.inv_h = h > 0.f ? 1.0f / h : 0.f;
+  s.bf = __fdiv_rn(omega, den);
+  s.icoef = __fdiv_rn(1.0f, __fadd_rn(1.0f, c));
+  s.mcoef = __fmul_rn(c, s.icoef);
+  s.inv_h = h > 0.f ? __fdiv_rn(1.0f, h) : 0.f;
   return s;
+}
+
+// effective mass of one row along direction u: 1 / (m_a + m_b + (r1 x u) I_a (r1 x u) + ...)
+__device__ __forceinline__ float xrow_mass(float3 r1, float3 r2, float3 u, float ima, float imb, const Sym3& IA,
+                                           const Sym3& IB) {
+  const float3 c1 = xcross(r1, u), c2 = xcross(r2, u);
+  const float k = __fadd_rn(__fadd_rn(__fadd_rn(ima, imb), xdot(c1, xsym(IA, c1))), xdot(c2, xsym(IB, c2)));
+  return k == 0.f ? 0.f : __fdiv_rn(1.0f, k);
 }
 
 // rows of one contact (solvers.slang:160-190): R1 = (r1, normal mass), R2 = (r2, tangent
@@ -76,35 +123,29 @@ __device__ __forceinline__ SoftCoef pgs_soft_coef(float ima, float imb, float h,
 __device__ __forceinline__ void pgs_contact_rows(float4 pp, float3 aa, float3 ab, float3 n, float3 t0, float3 t1,
                                                  float ima, float imb, const Sym3& IA, const Sym3& IB,
                                                  const SoftCoef& s, float4& R1, float4& R2, float4& K) {
-  const float3 r1 = f3(pp) - aa, r2 = f3(pp) - ab;
-  float3 rn1 = cross3(r1, n), rn2 = cross3(r2, n);
-  float kn = ima + imb + dot3(rn1, sym_mul(IA, rn1)) + dot3(rn2, sym_mul(IB, rn2));
-  float nmass = kn == 0.f ? 0.f : 1.0f / kn;
-  float tm[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    float3 t = k == 0 ? t0 : t1;
-    float3 rt1 = cross3(r1, t), rt2 = cross3(r2, t);
-    float kt = ima + imb + dot3(rt1, sym_mul(IA, rt1)) + dot3(rt2, sym_mul(IB, rt2));
-    tm[k] = kt == 0.f ? 0.f : 1.0f / kt;
-  }
+  const float3 r1 = xsub(f3(pp), aa), r2 = xsub(f3(pp), ab);
+  const float nmass = xrow_mass(r1, r2, n, ima, imb, IA, IB);
+  const float tm0 = xrow_mass(r1, r2, t0, ima, imb, IA, IB);
+  const float tm1 = xrow_mass(r1, r2, t1, ima, imb, IA, IB);
   const float pen = pp.w;
-  const float bias_value = pen > 0.f ? pen * s.inv_h : fmaxf(s.bf * pen, -4.0f);
+  const float bias_value = pen > 0.f ? __fmul_rn(pen, s.inv_h) : fmaxf(__fmul_rn(s.bf, pen), -4.0f);
   R1 = f4(r1, nmass);
-  R2 = f4(r2, tm[0]);
-  K = make_float4(tm[1], bias_value, s.mcoef, s.icoef);
+  R2 = f4(r2, tm0);
+  K = make_float4(tm1, bias_value, s.mcoef, s.icoef);
 }
 
 // warm start of one contact: apply the accumulated impulse (solvers.slang:191-195)
 __device__ __forceinline__ void pgs_contact_warm(float3 r1, float3 r2, float4 lam, float3 n, float3 t0, float3 t1,
                                                  bool fric, float ima, float imb, const Sym3& IA, const Sym3& IB,
                                                  float3& va, float3& wa, float3& vb, float3& wb) {
-  float3 P = n * lam.x;
-  if (fric) P = P + t0 * lam.y + t1 * lam.z;
-  va = va - P * ima;
-  wa = wa - sym_mul(IA, cross3(r1, P));
-  vb = vb + P * imb;
-  wb = wb + sym_mul(IB, cross3(r2, P));
+  float3 P = xscale(n, lam.x);
+  if (fric) P = xaxpy(t1, lam.z, xaxpy(t0, lam.y, P));
+  xapply(P, r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
+}
+
+// relative velocity at the contact: (v_b + w_b x r2) - (v_a + w_a x r1)
+__device__ __forceinline__ float3 xrel(float3 r1, float3 r2, float3 va, float3 wa, float3 vb, float3 wb) {
+  return xsub(xadd(vb, xcross(wb, r2)), xadd(va, xcross(wa, r1)));
 }
 
 // one contact of PGS_SOFT::solve (solvers.slang:209-277): two friction rows, then the normal row
@@ -113,34 +154,28 @@ __device__ __forceinline__ void pgs_contact_solve(float4 R1, float4 R2, float4 K
                                                   float imb, const Sym3& IA, const Sym3& IB, float3& va, float3& wa,
                                                   float3& vb, float3& wb) {
   const float3 r1 = f3(R1), r2 = f3(R2);
-  float3 rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
   if (fric) {
+    const float3 rv = xrel(r1, r2, va, wa, vb, wb);
     float imp_t[2] = {lam.y, lam.z};
     const float tmass[2] = {R2.w, K.x};
+    const float maxf = __fmul_rn(mu, lam.x);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const float3 t = k == 0 ? t0 : t1;
-      float tv = dot3(rv, t);
-      float ti = tmass[k] * -tv;
-      float maxf = mu * lam.x;
+      float ti = __fmul_rn(tmass[k], -xdot(rv, t));
       if (accum) {
-        float old = imp_t[k];
-        imp_t[k] = fminf(fmaxf(old + ti, -maxf), maxf);
-        ti = imp_t[k] - old;
+        const float old = imp_t[k];
+        imp_t[k] = fminf(fmaxf(__fadd_rn(old, ti), -maxf), maxf);
+        ti = __fsub_rn(imp_t[k], old);
       } else {
         ti = fminf(fmaxf(ti, -maxf), maxf);
       }
-      float3 P = t * ti;
-      va = va - P * ima;
-      wa = wa - sym_mul(IA, cross3(r1, P));
-      vb = vb + P * imb;
-      wb = wb + sym_mul(IB, cross3(r2, P));
+      xapply(xscale(t, ti), r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
     }
     lam.y = imp_t[0];
     lam.z = imp_t[1];
   }
-  rv = vb + cross3(wb, r2) - va - cross3(wa, r1);
-  float vn = dot3(rv, n);
+  const float vn = xdot(xrel(r1, r2, va, wa, vb, wb), n);
   float bias = 0.f, ms = 1.f, is = 0.f;
   if (K.y > 0.f) {
     bias = K.y;
@@ -149,19 +184,15 @@ __device__ __forceinline__ void pgs_contact_solve(float4 R1, float4 R2, float4 K
     ms = K.z;
     is = K.w;
   }
-  float imp = -R1.w * ms * (vn + bias) - is * lam.x;
+  float imp = __fsub_rn(__fmul_rn(__fmul_rn(-R1.w, ms), __fadd_rn(vn, bias)), __fmul_rn(is, lam.x));
   if (accum) {
-    float old = lam.x;
-    lam.x = fmaxf(old + imp, 0.f);
-    imp = lam.x - old;
+    const float old = lam.x;
+    lam.x = fmaxf(__fadd_rn(old, imp), 0.f);
+    imp = __fsub_rn(lam.x, old);
   } else {
     imp = fmaxf(imp, 0.f);
   }
-  float3 P = n * imp;
-  va = va - P * ima;
-  wa = wa - sym_mul(IA, cross3(r1, P));
-  vb = vb + P * imb;
-  wb = wb + sym_mul(IB, cross3(r2, P));
+  xapply(xscale(n, imp), r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
 }
 
 // PGS_SOFT::pre_step (solvers.slang:143-196) of one manifold slot: rows, then warm start
@@ -233,13 +264,29 @@ __device__ void pgs_solve_slot(const DevState& d, const Params& p, int cur, uint
 }
 
 // integrate one body (RB_sim.slang:1287-1326) and refresh its world inverse inertia
+// Compiled once (not inlined) so both schedules integrate with the same instructions.
+__device__ __noinline__ void pgs_integrate_body(float4* pos, float4* rot, const float4* vel, const float4* omega,
+                                                const float4* iinv, float4* iw, uint32_t i, float h, bool tq) {
+  const float4 ps = pos[i];
+  const float3 v = f3(vel[i]);
+  pos[i] = make_float4(ps.x + v.x * h, ps.y + v.y * h, ps.z + v.z * h, ps.w);
+  const Quatf q = apply_angular_velocity(q_from(rot[i]), f3(omega[i]), h);
+  rot[i] = q_to4(q);
+  const Sym3 s = world_inv_inertia(q, f3(iinv[i]), tq);
+  iw[2 * i] = make_float4(s.xx, s.xy, s.xz, s.yy);
+  iw[2 * i + 1] = make_float4(s.yz, s.zz, 0.f, 0.f);
+}
+__device__ __noinline__ void pgs_world_inertia_body(const float4* rot, const float4* iinv, float4* iw, uint32_t i,
+                                                    bool tq) {
+  const Sym3 s = world_inv_inertia(q_from(rot[i]), f3(iinv[i]), tq);
+  iw[2 * i] = make_float4(s.xx, s.xy, s.xz, s.yy);
+  iw[2 * i + 1] = make_float4(s.yz, s.zz, 0.f, 0.f);
+}
+__device__ __forceinline__ void pgs_world_inertia(const DevState& d, uint32_t i, bool tq) {
+  pgs_world_inertia_body(d.rot, d.iinv, d.iw, i, tq);
+}
 __device__ __forceinline__ void pgs_integrate(const DevState& d, uint32_t i, float h, bool tq) {
-  float4 ps = d.pos[i];
-  float3 v = f3(d.vel[i]);
-  d.pos[i] = make_float4(ps.x + v.x * h, ps.y + v.y * h, ps.z + v.z * h, ps.w);
-  Quatf q = apply_angular_velocity(q_from(d.rot[i]), f3(d.omega[i]), h);
-  d.rot[i] = q_to4(q);
-  store_iw(d, i, world_inv_inertia(q, f3(d.iinv[i]), tq));
+  pgs_integrate_body(d.pos, d.rot, d.vel, d.omega, d.iinv, d.iw, i, h, tq);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -457,7 +504,7 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(co
   const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
   uint32_t* sync = &d.ctr->sync_count[1];
   uint32_t epoch = 0;
-  for (uint32_t i = tid; i < n; i += stride) store_iw(d, i, world_inv_inertia(q_from(d.rot[i]), f3(d.iinv[i]), tq));
+  for (uint32_t i = tid; i < n; i += stride) pgs_world_inertia(d, i, tq);
   grid_sync(d.ctr, sync, epoch);  // also makes bs visible block-wide
   const uint32_t C = d.ctr->gc_colors;
   const uint32_t* list = d.bucket_vals[1];
@@ -550,7 +597,7 @@ __global__ void k_flow_prep(const DevState d, int cur) {
 __global__ void k_flow_init(const DevState d, Params p, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  store_iw(d, i, world_inv_inertia(q_from(d.rot[i]), f3(d.iinv[i]), p.quirks & BB_QUIRK_INERTIA_TRANSPOSE));
+  pgs_world_inertia(d, i, p.quirks & BB_QUIRK_INERTIA_TRANSPOSE);
   d.flow_counter[i] = 0;
 }
 
