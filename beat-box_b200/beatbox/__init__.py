@@ -166,6 +166,10 @@ _SIG = {
     "bb_radix_sort_pairs": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_radix_sort_pairs_static": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_autotune": (ctypes.c_int32, [_P, ctypes.c_float, _U32, _U32, ctypes.POINTER(SolverParams)]),
+    "bb_update_transforms": (ctypes.c_int32, [_P]),
+    "bb_transforms_device": (ctypes.c_void_p, [_P]),
+    "bb_read_transforms": (ctypes.c_int32, [_P, _P]),
+    "bb_read_contact_points": (ctypes.c_int32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
     "bb_world_device_bytes": (ctypes.c_uint64, [_P]),
     "bb_world_clear": (ctypes.c_int32, [_P]),
     "bb_world_bytes_for": (ctypes.c_uint64, [_U32, _U32]),
@@ -381,6 +385,20 @@ class World:
         c = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)  # noqa: E731
         pos, quat, vel, omega = c(pos), c(quat), c(vel), c(omega)
         _check(self.L.bb_write_state(self.h, _ptr(pos), _ptr(quat), _ptr(vel), _ptr(omega)))
+
+    def read_transforms(self) -> np.ndarray:
+        """(n, 3, 4) affine transforms [R | t] of every body (world = R local + t)."""
+        out = np.empty((self.n, 3, 4), np.float32)
+        _check(self.L.bb_read_transforms(self.h, _ptr(out)))
+        return out
+
+    def read_contact_points(self) -> np.ndarray:
+        """(k, 4) contact points of the last substep: position, depth."""
+        cnt = _U32()
+        _check(self.L.bb_read_contact_points(self.h, None, 0, ctypes.byref(cnt)))
+        out = np.empty((cnt.value, 4), np.float32)
+        _check(self.L.bb_read_contact_points(self.h, _ptr(out), cnt.value, ctypes.byref(cnt)))
+        return out
 
     def read_flags(self) -> np.ndarray:
         f = np.empty(self.n, np.uint32)

@@ -121,6 +121,35 @@ __global__ void k_extend_contacts(const DevState d, uint32_t o, uint32_t count) 
   for (int k = 0; k < 2; ++k) d.csr_start[k][o + 1 + i] = d.csr_start[k][o];
 }
 
+// Render feed: per body the affine transform [R | t] (3 x 4, row-major: the layout of a ray
+// tracing instance transform), R from the quaternion (to_matrix, include/math.hpp:292-309),
+// so that world = R * local + t.  The reference writes the same per-body transform into its
+// TLAS instances (src/shaders/AS_mngr.slang:5-36, shared.inl:377-419).
+__global__ void k_transforms(const DevState d, uint32_t n, float* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float R[3][3];
+  q_matrix(q_from(d.rot[i]), R);
+  const float4 p = d.pos[i];
+  float* o = out + 12 * size_t(i);
+  o[0] = R[0][0]; o[1] = R[0][1]; o[2] = R[0][2]; o[3] = p.x;
+  o[4] = R[1][0]; o[5] = R[1][1]; o[6] = R[1][2]; o[7] = p.y;
+  o[8] = R[2][0]; o[9] = R[2][1]; o[10] = R[2][2]; o[11] = p.z;
+}
+
+// Debug contact points of the last substep in manifold order, 8 slots per manifold (position,
+// depth; unused slots get a NaN depth), written into the solver-row scratch (free between steps).
+__global__ void k_contact_points(const DevState d, int cur, float4* out) {
+  const uint32_t M = d.ctr->manifold_count;
+  const size_t total = size_t(M) * BB_MAX_CONTACTS;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t m = uint32_t(t / BB_MAX_CONTACTS), j = uint32_t(t % BB_MAX_CONTACTS);
+    const uint32_t slot = d.man_slot[cur][m];
+    const int cc = d.m_keycc[cur][slot].y;
+    out[t] = int(j) < cc ? d.c_pos[cur][size_t(slot) * BB_MAX_CONTACTS + j] : make_float4(0.f, 0.f, 0.f, __int_as_float(0x7FC00000));
+  }
+}
+
 __global__ void k_begin_substep(DevCounters* c) {
   if (threadIdx.x != 0) return;
   c->pair_count = 0;
@@ -170,6 +199,7 @@ struct bb_world_impl {
   size_t scratch_bytes = 0;
   void* scratch_base = nullptr;
   size_t dev_bytes = 0;  // device memory held by this world
+  float* xforms = nullptr;  // render feed: 12 floats per body
   // graph cache
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
@@ -249,6 +279,7 @@ struct bb_world_impl {
     d.a_bucket_start = u32(64 * BB_MAX_COLORS + 2);
     d.ctr = dalloc<DevCounters>(1, owned, err);
     d.staging = dalloc<float>(13 * N + 4, owned, err);
+    xforms = dalloc<float>(12 * N, owned, err);
     d.pair_capacity = cap_p;
     d.body_capacity = cap_n;
     // scratch zeroed at every substep: scan status (5 scans), sort hists / status (12 slots)
@@ -758,6 +789,49 @@ bb_status bb_read_state(void* world, float* position, float* rotation, float* ve
   if (velocity) CU(cudaMemcpyAsync(velocity, st + 7ull * n, 12ull * n, cudaMemcpyDeviceToHost, w->stream));
   if (omega) CU(cudaMemcpyAsync(omega, st + 10ull * n, 12ull * n, cudaMemcpyDeviceToHost, w->stream));
   CU(cudaStreamSynchronize(w->stream));
+  return BB_OK;
+}
+
+bb_status bb_update_transforms(void* world) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  if (w->n) k_transforms<<<(w->n + 255) / 256, 256, 0, w->stream>>>(w->d, w->n, w->xforms);
+  CU(cudaGetLastError());
+  return BB_OK;
+}
+
+const float* bb_transforms_device(void* world) { return world ? W(world)->xforms : nullptr; }
+
+bb_status bb_read_transforms(void* world, float* transforms) {
+  World* w = W(world);
+  if (!w || (!transforms && w->n)) return fail(BB_E_INVALID, "bb_read_transforms: bad arguments");
+  bb_status st = bb_update_transforms(world);
+  if (st != BB_OK) return st;
+  if (w->n) CU(cudaMemcpyAsync(transforms, w->xforms, 48ull * w->n, cudaMemcpyDeviceToHost, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  return BB_OK;
+}
+
+bb_status bb_read_contact_points(void* world, float* points, uint32_t max_points, uint32_t* count) {
+  World* w = W(world);
+  if (!w || !count || (!points && max_points)) return fail(BB_E_INVALID, "bb_read_contact_points: bad arguments");
+  CU(cudaStreamSynchronize(w->stream));
+  uint32_t M = 0;
+  CU(cudaMemcpy(&M, &w->d.ctr->manifold_count, 4, cudaMemcpyDeviceToHost));
+  *count = 0;
+  if (!w->ran_any || M == 0) return BB_OK;
+  const int cur = w->last_cur;
+  k_contact_points<<<w->sms * 8, 256, 0, w->stream>>>(w->d, cur, w->d.c_r1);
+  std::vector<float4> buf(size_t(M) * BB_MAX_CONTACTS);
+  CU(cudaMemcpyAsync(buf.data(), w->d.c_r1, buf.size() * sizeof(float4), cudaMemcpyDeviceToHost, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  uint32_t k = 0;
+  for (const float4& c : buf) {
+    if (c.w != c.w) continue;  // NaN: unused slot
+    if (k < max_points) std::memcpy(points + 4 * size_t(k), &c, 16);
+    ++k;
+  }
+  *count = k;
   return BB_OK;
 }
 

@@ -415,6 +415,21 @@ bb_status bb_server_read_state(void* server, uint64_t world, float* position, fl
                                float* omega, uint32_t* n_bodies);
 bb_status bb_server_get_stats(void* server, bb_server_stats* out);
 
+/* ---- render feed (no graphics API: device and host buffers) ----------------------------
+ * Per body the 3 x 4 row-major affine transform [R | t] (world = R * local + t), the layout of a
+ * ray-tracing instance transform.  Replaces the TLAS instance update of the reference
+ * (src/shaders/AS_mngr.slang:5-36, include/shared.inl:377-419), which feeds its path tracer.
+ * bb_update_transforms refreshes the device buffer on the world's stream (asynchronous);
+ * bb_transforms_device returns that buffer (12 floats per body id, valid for the world's life);
+ * bb_read_transforms refreshes it and copies it to host memory. */
+bb_status bb_update_transforms(void* world);
+const float* bb_transforms_device(void* world);
+bb_status bb_read_transforms(void* world, float* transforms);
+/* Contact points of the last substep (x, y, z, depth; depth <= 0 on penetration), in manifold
+ * order; up to max_points are copied and *count receives the total.  Replaces the reference's
+ * debug contact-point buffer for its renderer (src/shaders/simulation/RB_sim.slang:1583-1653). */
+bb_status bb_read_contact_points(void* world, float* points, uint32_t max_points, uint32_t* count);
+
 /* Last error message of the calling thread (static storage, never NULL). */
 const char* bb_last_error_string(void);
 /* Library version string. */
