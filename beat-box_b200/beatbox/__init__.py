@@ -112,7 +112,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
                 ("body_steps", ctypes.c_uint64), ("evictions", ctypes.c_uint64), ("worlds_created", ctypes.c_uint64),
                 ("resident_bytes", ctypes.c_uint64), ("active", ctypes.c_uint32), ("queued", ctypes.c_uint32),
-                ("resident_worlds", ctypes.c_uint32), ("known_worlds", ctypes.c_uint32)]
+                ("resident_worlds", ctypes.c_uint32), ("known_worlds", ctypes.c_uint32),
+                ("materialise_s", ctypes.c_double), ("issue_s", ctypes.c_double)]
 
 
 class StepStats(ctypes.Structure):

@@ -146,6 +146,7 @@ struct bb_server_impl {
     void* pooled = nullptr;  // reused world object (cleared before use)
     uint64_t reserved = 0;   // budget reserved for a new world object
     bb_status result = BB_OK;
+    double materialise_s = 0, issue_s = 0;
   };
 
   // outside the lock: materialise the world if needed, set parameters, enqueue all steps
@@ -153,6 +154,7 @@ struct bb_server_impl {
     Req* q = sp.q;
     WorldRec* wr = q->w;
     bb_status s = BB_OK;
+    const auto t0 = Clock::now();
     if (!wr->world) {
       void* w = sp.pooled;
       if (w) {
@@ -180,6 +182,8 @@ struct bb_server_impl {
       }
     }
     void* w = wr->world ? wr->world : sp.pooled;
+    const auto t1 = Clock::now();
+    sp.materialise_s = std::chrono::duration<double>(t1 - t0).count();
     bb_solver_params p = q->r.params;
     std::memcpy(p.world_min, wr->wmin, sizeof(p.world_min));
     std::memcpy(p.world_extent, wr->wext, sizeof(p.world_extent));
@@ -188,6 +192,7 @@ struct bb_server_impl {
     for (uint32_t k = 0; k < q->r.steps && s == BB_OK; ++k) s = bb_step(w, q->r.dt, q->r.substeps);
     if (s == BB_OK && cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming) != cudaSuccess) s = BB_E_CUDA;
     if (s == BB_OK && cudaEventRecord(q->ev, static_cast<cudaStream_t>(bb_world_stream(w))) != cudaSuccess) s = BB_E_CUDA;
+    sp.issue_s = std::chrono::duration<double>(Clock::now() - t1).count();
     sp.result = s;
   }
 
@@ -271,6 +276,8 @@ struct bb_server_impl {
         for (Start& sp : todo) {
           Req* q = sp.q;
           WorldRec* wr = q->w;
+          st.materialise_s += sp.materialise_s;
+          st.issue_s += sp.issue_s;
           if (sp.reserved) {  // a new world object: account its real size
             held_bytes -= sp.reserved;
             if (sp.pooled) {

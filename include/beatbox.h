@@ -403,6 +403,8 @@ typedef struct bb_server_stats {
   uint64_t evictions, worlds_created;
   uint64_t resident_bytes;   /* device bytes held in resident and pooled worlds */
   uint32_t active, queued, resident_worlds, known_worlds;
+  double materialise_s;      /* worker time spent creating / loading worlds */
+  double issue_s;            /* worker time spent enqueueing steps (includes graph captures) */
 } bb_server_stats;
 
 bb_status bb_server_create(const bb_server_desc* desc, void** out_server);
