@@ -41,7 +41,7 @@ struct Shape {
 thread_local size_t t_alloc_bytes = 0;  // device bytes allocated by dalloc on this thread
 thread_local bool t_count_only = false;  // dalloc only counts (bb_world_bytes_for)
 
-template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& err) {
+template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& err, cudaStream_t stream) {
   void* p = nullptr;
   if (n == 0) n = 1;
   t_alloc_bytes += n * sizeof(T);
@@ -51,7 +51,7 @@ template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& e
     err = e;
     return nullptr;
   }
-  cudaMemset(p, 0, n * sizeof(T));
+  cudaMemsetAsync(p, 0, n * sizeof(T), stream);
   owned.push_back(p);
   return static_cast<T*>(p);
 }
@@ -224,24 +224,24 @@ struct bb_world_impl {
     cudaError_t err = cudaSuccess;
     const size_t N = cap_n + 1, P = cap_p;
     const size_t C = P * BB_MAX_CONTACTS;
-    auto f4 = [&](size_t k) { return dalloc<float4>(k, owned, err); };
-    auto u32 = [&](size_t k) { return dalloc<uint32_t>(k, owned, err); };
+    auto f4 = [&](size_t k) { return dalloc<float4>(k, owned, err, stream); };
+    auto u32 = [&](size_t k) { return dalloc<uint32_t>(k, owned, err, stream); };
     d.pos = f4(N); d.rot = f4(N); d.vel = f4(N); d.omega = f4(N); d.pvel = f4(N); d.shape = f4(N); d.iinv = f4(N);
     d.flags = u32(N); d.sleep = u32(N); d.iw = f4(2 * N);
     for (int k = 0; k < 2; ++k) { d.keys[k] = u32(N); d.vals[k] = u32(N); }
     d.rank = u32(N);
     d.node_box = f4(4 * N);
-    d.child = dalloc<int2>(N, owned, err);
-    d.parent = dalloc<int32_t>(2 * N, owned, err);
-    d.range_last = dalloc<int32_t>(N, owned, err);
+    d.child = dalloc<int2>(N, owned, err, stream);
+    d.parent = dalloc<int32_t>(2 * N, owned, err, stream);
+    d.range_last = dalloc<int32_t>(N, owned, err, stream);
     d.visit = u32(N);
     d.pair_cnt = u32(N); d.pair_off = u32(N + 1);
     d.is_heavy = u32(N); d.heavy_list = u32(8192);
     d.bp_stage = u32(size_t(N) * 32);
-    d.pairs = dalloc<uint2>(P, owned, err);
+    d.pairs = dalloc<uint2>(P, owned, err, stream);
     for (int k = 0; k < 2; ++k) {
-      d.m_bodies[k] = dalloc<uint2>(P, owned, err);
-      d.m_keycc[k] = dalloc<int2>(P, owned, err);
+      d.m_bodies[k] = dalloc<uint2>(P, owned, err, stream);
+      d.m_keycc[k] = dalloc<int2>(P, owned, err, stream);
       d.m_normal[k] = f4(P); d.m_t0[k] = f4(P); d.m_t1[k] = f4(P); d.m_anchor_a[k] = f4(P); d.m_anchor_b[k] = f4(P);
       d.man_slot[k] = u32(P);
       d.c_pos[k] = f4(C); d.c_lam[k] = f4(C); d.c_kt[k] = f4(C); d.c_anc_a[k] = f4(C); d.c_anc_b[k] = f4(C);
@@ -250,17 +250,17 @@ struct bb_world_impl {
       d.csr_partner[k] = u32(2 * P);
     }
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
-    d.flow_rec = dalloc<uint4>(P, owned, err);
-    d.pgs_rec = dalloc<uint4>(P, owned, err);
+    d.flow_rec = dalloc<uint4>(P, owned, err, stream);
+    d.pgs_rec = dalloc<uint4>(P, owned, err, stream);
     d.np_list = u32(P);
-    d.gc_rec = dalloc<uint4>(P, owned, err);
+    d.gc_rec = dalloc<uint4>(P, owned, err, stream);
     d.gc_list[0] = u32(P); d.gc_list[1] = u32(P);
     d.pgs_mass = f4(P);
     d.pgs_frame = f4(3 * P);
     d.pgs_lam = f4(8 * P);
     d.pgs_cnt = u32(P); d.pgs_coff = u32(P); d.pgs_slot = u32(P);
     d.flow_counter = u32(N);
-    d.range_first = dalloc<int32_t>(N, owned, err);
+    d.range_first = dalloc<int32_t>(N, owned, err, stream);
     d.sworld = u32(N);
     d.world_of = u32(N); d.world_first = u32(N); d.world_count = u32(N);
     d.world_bounds = f4(2 * N);
@@ -269,7 +269,7 @@ struct bb_world_impl {
     d.hit = u32(P); d.man_index = u32(P);
     d.uf_parent = u32(N); d.is_root = u32(N); d.root_rank = u32(N); d.island = u32(N);
     d.gc_color = u32(P); d.gc_pid = u32(P); d.gc_choice = u32(P); d.gc_mask = u32(N);
-    d.gc_owner = dalloc<unsigned long long>(N * BB_MAX_COLORS, owned, err);
+    d.gc_owner = dalloc<unsigned long long>(N * BB_MAX_COLORS, owned, err, stream);
     for (int k = 0; k < 2; ++k) { d.bucket_keys[k] = u32(P); d.bucket_vals[k] = u32(P); }
     d.bucket_start = u32(64);
     d.body_color = u32(N); d.body_color_round = u32(N);
@@ -277,9 +277,9 @@ struct bb_world_impl {
     d.a_depth = u32(N);
     for (int k = 0; k < 2; ++k) { d.a_bucket_keys[k] = u32(N); d.a_bucket_vals[k] = u32(N); }
     d.a_bucket_start = u32(64 * BB_MAX_COLORS + 2);
-    d.ctr = dalloc<DevCounters>(1, owned, err);
-    d.staging = dalloc<float>(13 * N + 4, owned, err);
-    xforms = dalloc<float>(12 * N, owned, err);
+    d.ctr = dalloc<DevCounters>(1, owned, err, stream);
+    d.staging = dalloc<float>(13 * N + 4, owned, err, stream);
+    xforms = dalloc<float>(12 * N, owned, err, stream);
     d.pair_capacity = cap_p;
     d.body_capacity = cap_n;
     // scratch zeroed at every substep: scan status (5 scans), sort hists / status (12 slots)
@@ -289,7 +289,7 @@ struct bb_world_impl {
     size_t sort_status_words = size_t(12) * sc.sort_tiles * 256;
     size_t hist_words = 5 * BB_HIST_REGION;
     scratch_bytes = scan_words * 8 + 16 * 4 + hist_words * 4 + sort_status_words * 4 + 16 * 4;
-    char* base = static_cast<char*>(static_cast<void*>(dalloc<uint8_t>(scratch_bytes + 256, owned, err)));
+    char* base = static_cast<char*>(static_cast<void*>(dalloc<uint8_t>(scratch_bytes + 256, owned, err, stream)));
     if (err != cudaSuccess) return fail(BB_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
     scratch_base = base;
     sc.scan_status = reinterpret_cast<unsigned long long*>(base);
@@ -437,7 +437,7 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), w->cap_n / 2, 256);
   w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n / 2, 512);
   w->coop_cc = fit(bb_components_blocks(w->sms), w->cap_n, 512);
-  cudaError_t e = cudaDeviceSynchronize();
+  cudaError_t e = cudaStreamSynchronize(w->stream);  // the zero fills (no device-wide wait)
   if (e != cudaSuccess) {
     delete w;
     return fail(BB_E_CUDA, std::string("create: ") + cudaGetErrorString(e));
@@ -486,7 +486,8 @@ bb_status bb_world_clear(void* world) {
   w->ran_any = false;
   w->invalidate_graphs();
   uint32_t nn[2] = {0, 0};
-  CU(cudaMemcpy(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
 uint32_t bb_body_count(void* world) { return world ? W(world)->n : 0; }
@@ -559,15 +560,15 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
   }
   const uint32_t o = w->n;
   cudaStreamSynchronize(w->stream);
-  CU(cudaMemcpy(w->d.pos + o, pos.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.rot + o, rot.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.vel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.pvel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.omega + o, om.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.shape + o, shp.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.iinv + o, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.flags + o, fl.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.sleep + o, zero.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(w->d.pos + o, pos.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.rot + o, rot.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.vel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.pvel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.omega + o, om.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.shape + o, shp.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.iinv + o, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.flags + o, fl.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.sleep + o, zero.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
   w->n += count;
   w->n_dyn += ndyn;
   if (out_first_id) *out_first_id = o;
@@ -577,7 +578,8 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
   else w->reset_contacts();
   w->invalidate_graphs();
   uint32_t nn[2] = {w->n, w->n_dyn};
-  CU(cudaMemcpy(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));  // the host arrays above die on return
   return BB_OK;
 }
 
@@ -599,12 +601,13 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
   if (st != BB_OK) return st;
   const uint32_t widx = w->d.n_worlds;
   std::vector<uint32_t> wof(count, widx);
-  CU(cudaMemcpy(w->d.world_of + first, wof.data(), 4ull * count, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.world_first + widx, &first, 4, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(w->d.world_count + widx, &count, 4, cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(w->d.world_of + first, wof.data(), 4ull * count, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.world_first + widx, &first, 4, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.world_count + widx, &count, 4, cudaMemcpyHostToDevice, w->stream));
   float4 bnd[2] = {make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
                    make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f)};
-  CU(cudaMemcpy(w->d.world_bounds + 2 * widx, bnd, sizeof(bnd), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(w->d.world_bounds + 2 * widx, bnd, sizeof(bnd), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
   w->d.n_worlds = widx + 1;
   w->invalidate_graphs();
   if (out_world_index) *out_world_index = widx;
@@ -621,7 +624,8 @@ bb_status bb_set_material(void* world, uint32_t first, uint32_t count, float fri
   std::vector<float4> ii(count);
   CU(cudaMemcpy(ii.data(), w->d.iinv + first, count * sizeof(float4), cudaMemcpyDeviceToHost));
   for (auto& v : ii) v.w = friction;
-  CU(cudaMemcpy(w->d.iinv + first, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(w->d.iinv + first, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
   for (uint32_t i = 0; i < count; ++i) w->restitution[first + i] = restitution;
   return BB_OK;
 }
