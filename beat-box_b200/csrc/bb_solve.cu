@@ -492,8 +492,9 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
   }
 }
 
-// PF = 4 for large worlds (one 255-register block per SM); PF = 1 for small worlds, whose few
-// blocks then need only part of an SM and can run beside other worlds' kernels
+// PF = 4 contacts held per item (one 255-register block per SM).  Holding fewer would let
+// two blocks share an SM but puts the other contacts' loads on the critical path, one round
+// trip each.
 template <int PF>
 __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   __shared__ uint32_t bs[BB_MAX_COLORS + 2];
@@ -547,13 +548,15 @@ int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft<
 // The per-colour sweeps give every body b the ordered sequence L_b of the manifolds touching
 // it, sorted by (colour, manifold) with the overflow bucket last; one sweep processes L_b in
 // that order, and a manifold's result depends only on its two bodies' states.  So instead of a
-// grid barrier after each colour, each dynamic body carries a sequence counter: the item
-// (phase f, manifold M) waits until counter[b] == f*deg(b) + rank_b(M) (+1 after the integrate
-// item in the relax phases) for both its dynamic bodies, runs, and releases +1 on each.  The
-// outcome is bit-identical to the barrier schedule.  Items are dequeued by warps in queue order
-// (phase, colour, manifold), which is a topological order of the waits, so the schedule cannot
-// deadlock even without co-residency: every wait points at an item dequeued earlier.  Bucket
-// sizes are padded to 32 so a warp's chunk never straddles two colours.
+// grid barrier after each colour, each dynamic body carries a sequence counter: item k of sweep
+// s waits until counter[b] == s * deg(b) + rank_b(k) for both its dynamic bodies, runs, and
+// releases +1 on each.  The outcome is bit-identical to the barrier schedule.
+//
+// The kernel is cooperative (all blocks resident) and thread t owns the items k = t, t + T, ...
+// of the colour-ordered list, which it runs in increasing (sweep, k) order.  Every wait points
+// at an item earlier in that order, owned by a thread that reaches it without waiting on a
+// later item of t, so the schedule cannot deadlock.  The items are the barrier schedule's
+// compact records (built by their owners), so a thread loads its next item while waiting.
 __device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -567,18 +570,19 @@ __device__ __forceinline__ void flow_wait(DevCounters* c, const uint32_t* ctr, u
   }
 }
 
-// per compact manifold: (slot, body a, body b, rank_a | rank_b << 16) where rank_x is the
-// manifold's position in L_x (colour-major, then manifold order)
+// per colour-ordered item k: (rank_a | rank_b << 16, deg_a | deg_b << 16) where rank_x is the
+// item's position in L_x (colour-major, then manifold order) and deg_x = |L_x|
 __global__ void k_flow_prep(const DevState d, int cur) {
   const uint32_t M = d.ctr->manifold_count;
-  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
-    const uint32_t slot = d.man_slot[cur][m];
-    const uint2 b = d.m_bodies[cur][slot];
+  const uint32_t* list = d.bucket_vals[1];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+    const uint32_t m = list[k];
+    const uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
     const uint32_t cm = min(d.gc_color[m], uint32_t(BB_MAX_COLORS));
-    uint32_t rank[2] = {0, 0};
+    uint32_t rank[2] = {0, 0}, deg[2] = {0, 0};
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const uint32_t x = k == 0 ? b.x : b.y;
+    for (int q = 0; q < 2; ++q) {
+      const uint32_t x = q == 0 ? b.x : b.y;
       if (!(d.flags[x] & BB_BODY_DYNAMIC)) continue;
       const uint32_t s0 = d.csr_start[cur][x], s1 = d.csr_start[cur][x + 1];
       uint32_t r = 0;
@@ -587,9 +591,10 @@ __global__ void k_flow_prep(const DevState d, int cur) {
         const uint32_t c2 = min(d.gc_color[m2], uint32_t(BB_MAX_COLORS));
         r += (c2 < cm || (c2 == cm && m2 < m)) ? 1u : 0u;
       }
-      rank[k] = r;
+      rank[q] = r;
+      deg[q] = s1 - s0;
     }
-    d.flow_rec[m] = make_uint4(slot, b.x, b.y, (rank[0] & 0xFFFFu) | (rank[1] << 16));
+    d.flow_rec[k] = make_uint4((rank[0] & 0xFFFFu) | (rank[1] << 16), (deg[0] & 0xFFFFu) | (deg[1] << 16), 0u, 0u);
   }
 }
 
@@ -601,103 +606,88 @@ __global__ void k_flow_init(const DevState d, Params p, uint32_t n) {
   d.flow_counter[i] = 0;
 }
 
-__global__ void __launch_bounds__(256) k_pgs_flow(const DevState d, Params p, int cur, uint32_t n, float h) {
-  __shared__ uint32_t s_pre[BB_MAX_COLORS + 2];    // padded bucket prefix
-  __shared__ uint32_t s_start[BB_MAX_COLORS + 2];  // real bucket starts
-  if (threadIdx.x < BB_MAX_COLORS + 2) s_start[threadIdx.x] = d.bucket_start[threadIdx.x];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t acc = 0;
-    for (int c = 0; c <= BB_MAX_COLORS; ++c) {
-      s_pre[c] = acc;
-      acc += (s_start[c + 1] - s_start[c] + 31u) & ~31u;
-    }
-    s_pre[BB_MAX_COLORS + 1] = acc;
+// one dataflow sweep s (mode 0 warm start, 1 solve, 2 relax) over this thread's items
+template <int PF>
+__device__ void flow_sweep(const DevState& d, const Params& p, int cur, uint32_t s, int mode, uint32_t M, PgsItem<PF>& x,
+                           uint4& fr) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (uint32_t k = tid; k < M; k += stride) {
+    const uint32_t a = x.rec.y, b = x.rec.z;
+    const bool da = x.rec.w & (1u << 8), db = x.rec.w & (1u << 9);
+    if (da) flow_wait(d.ctr, &d.flow_counter[a], s * (fr.y & 0xFFFFu) + (fr.x & 0xFFFFu));
+    if (db) flow_wait(d.ctr, &d.flow_counter[b], s * (fr.y >> 16) + (fr.x >> 16));
+    pgs_item_run(d, p, cur, x, mode);
+    if (da) red_release_add(&d.flow_counter[a], 1u);
+    if (db) red_release_add(&d.flow_counter[b], 1u);
+    // this thread's next item (wrapping to its first for the next sweep)
+    const uint32_t kn = k + stride < M ? k + stride : tid;
+    pgs_item_load(d, kn, x);
+    fr = d.flow_rec[kn];
   }
-  __syncthreads();
-  const uint32_t L = s_pre[BB_MAX_COLORS + 1];
-  const uint32_t I = p.iterations, Ir = p.relax_iterations;
-  const uint32_t npad = (n + 31u) & ~31u;
-  const uint64_t solve_end = uint64_t(L) * (1 + I);
-  const uint64_t integ_end = solve_end + npad;
-  const uint64_t total = integ_end + uint64_t(L) * Ir;
+}
+
+template <int PF>
+__global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_flow(const DevState d, Params p, int cur,
+                                                                               uint32_t n, float h) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
   const float inv_h = h > 0.f ? 1.0f / h : 0.f;
   const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
-  const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
-  const bool advect = p.flags & BB_SIM_ADVECTION;
+  uint32_t* sync = &d.ctr->sync_count[1];
+  uint32_t epoch = 0;
+  const uint32_t M = d.ctr->manifold_count;
   const uint32_t* list = d.bucket_vals[1];
-  const int lane = threadIdx.x & 31;
-  uint32_t* head = &d.ctr->pad[5];
-  for (;;) {
-    uint32_t q0 = 0;
-    if (lane == 0) q0 = atomicAdd(head, 32u);
-    q0 = __shfl_sync(0xFFFFFFFFu, q0, 0);
-    if (uint64_t(q0) >= total) break;
-    const uint64_t q = uint64_t(q0) + lane;
-    if (q >= total) continue;
-    if (q >= solve_end && q < integ_end) {
-      // integrate body i after its pre-step and solve items (RB_sim.slang:1287-1326)
-      const uint32_t i = uint32_t(q - solve_end);
-      if (i >= n || !(d.flags[i] & BB_BODY_DYNAMIC)) continue;
-      const uint32_t deg = d.csr_start[cur][i + 1] - d.csr_start[cur][i];
-      flow_wait(d.ctr, &d.flow_counter[i], (1 + I) * deg);
-      if (advect && awake(d.flags[i])) pgs_integrate(d, i, h, tq);
-      red_release_add(&d.flow_counter[i], 1u);
-      continue;
-    }
-    uint32_t phase, r;
-    if (q < solve_end) {
-      phase = uint32_t(q / L);
-      r = uint32_t(q % L);
-    } else {
-      const uint64_t q2 = q - integ_end;
-      phase = 1 + I + uint32_t(q2 / L);
-      r = uint32_t(q2 % L);
-    }
-    int c = 0;  // bucket: last c with s_pre[c] <= r
-#pragma unroll
-    for (int stepw = 32; stepw > 0; stepw >>= 1)
-      if (c + stepw <= BB_MAX_COLORS && s_pre[c + stepw] <= r) c += stepw;
-    const uint32_t o = r - s_pre[c];
-    if (o >= s_start[c + 1] - s_start[c]) continue;  // padding
-    const uint32_t m = list[s_start[c] + o];
-    const uint4 rec = d.flow_rec[m];
-    const uint2 b = make_uint2(rec.y, rec.z);
-    const bool da = d.flags[b.x] & BB_BODY_DYNAMIC, db = d.flags[b.y] & BB_BODY_DYNAMIC;
-    const uint32_t extra = phase > I ? 1u : 0u;
-    if (da) {
-      const uint32_t deg = d.csr_start[cur][b.x + 1] - d.csr_start[cur][b.x];
-      flow_wait(d.ctr, &d.flow_counter[b.x], phase * deg + (rec.w & 0xFFFFu) + extra);
-    }
-    if (db) {
-      const uint32_t deg = d.csr_start[cur][b.y + 1] - d.csr_start[cur][b.y];
-      flow_wait(d.ctr, &d.flow_counter[b.y], phase * deg + (rec.w >> 16) + extra);
-    }
-    if (phase == 0) pgs_pre_step_slot(d, p, cur, rec.x, b, h, hertz);
-    else pgs_solve_slot(d, p, cur, rec.x, b, phase <= I);
-    if (da) red_release_add(&d.flow_counter[b.x], 1u);
-    if (db) red_release_add(&d.flow_counter[b.y], 1u);
+  for (uint32_t k = tid; k < M; k += stride) pgs_item_build(d, cur, k, list[k], h, hertz);
+  PgsItem<PF> x;
+  uint4 fr = make_uint4(0, 0, 0, 0);
+  if (tid < M) {
+    pgs_item_load(d, tid, x);
+    fr = d.flow_rec[tid];
+  }
+  uint32_t s = 0;
+  flow_sweep(d, p, cur, s++, 0, M, x, fr);
+  for (uint32_t it = 0; it < p.iterations; ++it) flow_sweep(d, p, cur, s++, 1, M, x, fr);
+  if (p.flags & BB_SIM_ADVECTION) {
+    grid_sync(d.ctr, sync, epoch);
+    for (uint32_t i = tid; i < n; i += stride)
+      if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
+    grid_sync(d.ctr, sync, epoch);
+  }
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) flow_sweep(d, p, cur, s++, 2, M, x, fr);
+  grid_sync(d.ctr, sync, epoch);
+  for (uint32_t k = tid; k < M; k += stride) {  // impulses back to the persistent contacts
+    const uint32_t cc = d.pgs_cnt[k];
+    if (cc == 0) continue;
+    const uint32_t slot = d.pgs_slot[k], c0 = d.pgs_coff[k];
+    for (uint32_t j = 0; j < cc; ++j) d.c_lam[cur][slot * BB_MAX_CONTACTS + j] = d.pgs_lam[c0 + j];
   }
 }
 
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                        const StepScratch& sc, int coop_blocks, int sms) {
-  if (p.schedule == BB_SCHEDULE_DATAFLOW) {
-    k_flow_prep<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
-    k_flow_init<<<(n + BB_THREADS - 1) / BB_THREADS, BB_THREADS, 0, s>>>(d, p, n);
-    k_pgs_flow<<<sms * (p.flow_blocks_per_sm ? p.flow_blocks_per_sm : 8u), 256, 0, s>>>(d, p, cur, n, h);
-    return;
-  }
   k_pgs_count<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
   bb_launch_scan(s, d.pgs_cnt, d.pgs_coff, &d.ctr->manifold_count, d.pair_capacity, nullptr,
                  sc.scan_status + 4 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 4, d.ctr);
+  if (p.schedule == BB_SCHEDULE_DATAFLOW) {
+    k_flow_prep<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
+    k_flow_init<<<(n + BB_THREADS - 1) / BB_THREADS, BB_THREADS, 0, s>>>(d, p, n);
+    DevState dd = d;
+    Params pp = p;
+    int cc = cur;
+    uint32_t nn = n;
+    float hh = h;
+    void* args[] = {&dd, &pp, &cc, &nn, &hh};
+    const void* kern = (const void*)k_pgs_flow<4>;
+    bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s);
+    return;
+  }
   DevState dd = d;
   Params pp = p;
   int cc = cur;
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
-  const void* kern = coop_blocks > 16 ? (const void*)k_pgs_soft<4> : (const void*)k_pgs_soft<1>;
+  const void* kern = (const void*)k_pgs_soft<4>;
   bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s);
 }
 

@@ -1108,7 +1108,6 @@ bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_s
   };
   const std::vector<Axis> axes = {
       {&bb_solver_params::schedule, {BB_SCHEDULE_DATAFLOW, BB_SCHEDULE_COLOUR_BARRIER}, true, false},
-      {&bb_solver_params::flow_blocks_per_sm, {2, 4, 8}, true, true},
       {&bb_solver_params::broad_threads, {32, 64, 128}, false, false},
       {&bb_solver_params::narrow_blocks_per_sm, {4, 8, 16, 32}, false, false},
   };
