@@ -13,6 +13,7 @@
 // their body state (pose, velocity, sleep flag) is saved on the host and the world is rebuilt
 // from it when a later request continues it (an evicted world restarts its warm-start state).
 // World objects are pooled by capacity class (powers of two) and reused through bb_world_clear.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -271,7 +272,20 @@ struct bb_server_impl {
       }
       if (!todo.empty()) {
         lk.unlock();
-        for (Start& sp : todo) run_start(sp);
+        // independent worlds: materialise and enqueue them from several host threads (graph
+        // capture and world creation are host-heavy; each world is touched by one thread)
+        const size_t nt = std::min<size_t>(todo.size(), 8);
+        if (nt <= 1) {
+          for (Start& sp : todo) run_start(sp);
+        } else {
+          std::vector<std::thread> th;
+          for (size_t t = 0; t < nt; ++t)
+            th.emplace_back([this, &todo, t, nt] {
+              if (desc.device >= 0) cudaSetDevice(desc.device);
+              for (size_t k = t; k < todo.size(); k += nt) run_start(todo[k]);
+            });
+          for (auto& x : th) x.join();
+        }
         lk.lock();
         for (Start& sp : todo) {
           Req* q = sp.q;
