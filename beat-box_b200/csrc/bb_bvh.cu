@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
   __shared__ uint32_t s_warp[BB_FRONTIER / 32];
   __shared__ uint32_t s_size;
   const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
-  if (blockIdx.x >= hc) return;
+  if (blockIdx.x >= hc || d.hv_n[blockIdx.x] != BB_NONE) return;  // pool path took this query
   const uint32_t qi = d.heavy_list[blockIdx.x];
   const int N = int(n), leaf0 = N - 1;
   const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
@@ -433,6 +433,175 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
   }
 }
 
+// ---- heavy queries over the whole GPU -------------------------------------------------------
+// A query with a huge box (floor, walls) can overlap a large share of all leaves.  One block
+// per heavy query expands an ordered frontier of overlapping subtrees, up to BB_HV_FRONTIER
+// entries, and appends it to a pool; then every pool entry is walked by its own thread (count,
+// scan over the pool, walk again to emit), so one query's walk is spread over the GPU.  The
+// frontier keeps left-to-right order and each entry covers a contiguous leaf range, so the
+// concatenated walks emit ascending partners, as the single-thread traversal does.  A query
+// whose frontier does not fit the pool falls back to k_broad_heavy (hv_n = BB_NONE).
+#define BB_HV_THREADS 1024
+#define BB_HV_PER_THREAD 4
+#define BB_HV_FRONTIER (BB_HV_THREADS * BB_HV_PER_THREAD)
+
+__device__ __forceinline__ uint32_t block_excl_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = s_warp[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_warp[lane] = w;
+  }
+  __syncthreads();
+  total = s_warp[31];
+  const uint32_t excl = x - v + (warp > 0 ? s_warp[warp - 1] : 0u);
+  __syncthreads();
+  return excl;
+}
+
+__global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState d, uint32_t n) {
+  __shared__ int s_fr[2][BB_HV_FRONTIER];
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_size, s_off, s_fits;
+  const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
+  const int N = int(n), leaf0 = N - 1;
+  const int t = threadIdx.x;
+  for (uint32_t slot = blockIdx.x; slot < hc; slot += gridDim.x) {
+    const uint32_t qi = d.heavy_list[slot];
+    const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
+    const int wend = world_end(d, qi, n);
+    if (t == 0) {
+      s_fr[0][0] = 0;
+      s_size = 1;
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int level = 0; level < 64; ++level) {
+      const uint32_t size = s_size;
+      int kid[2 * BB_HV_PER_THREAD];
+      uint32_t c = 0;
+      bool internal = false;
+#pragma unroll
+      for (int e = 0; e < BB_HV_PER_THREAD; ++e) {
+        const uint32_t idx = uint32_t(t) * BB_HV_PER_THREAD + e;
+        if (idx >= size) continue;
+        const int node = s_fr[cur][idx];
+        if (node >= leaf0) {
+          kid[c++] = node;  // a leaf entry stays in place
+        } else {
+          const int2 ch = d.child[node];
+          if (bp_take(d, ch.x, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.x;
+          if (bp_take(d, ch.y, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.y;
+        }
+      }
+      uint32_t total;
+      const uint32_t pos = block_excl_scan_1024(c, s_warp, total);
+      if (total > BB_HV_FRONTIER || total == 0) {  // uniform: keep the current frontier (or none)
+        if (total == 0 && t == 0) s_size = 0;
+        __syncthreads();
+        break;
+      }
+      for (uint32_t k = 0; k < c; ++k) {
+        s_fr[cur ^ 1][pos + k] = kid[k];
+        internal |= kid[k] < leaf0;
+      }
+      const int more = __syncthreads_or(internal);
+      cur ^= 1;
+      if (t == 0) s_size = total;
+      __syncthreads();
+      if (!more) break;
+    }
+    const uint32_t size = s_size;
+    if (t == 0) {
+      const uint32_t off = size ? atomicAdd(&d.ctr->hv_pool_n, size) : 0u;
+      const bool fits = uint64_t(off) + size <= d.hv_cap;
+      s_off = off;
+      s_fits = fits ? 1u : 0u;
+      d.hv_first[slot] = fits ? off : 0u;
+      d.hv_n[slot] = fits ? size : BB_NONE;
+    }
+    __syncthreads();
+    const uint32_t off = s_off;
+    if (s_fits) {
+      for (uint32_t k = t; k < size; k += blockDim.x) {
+        d.hv_pool[off + k] = uint32_t(s_fr[cur][k]);
+        d.hv_slot[off + k] = slot;
+      }
+    } else {  // the reservation ran past the pool: mark the part of it inside the pool unused
+      for (uint32_t k = t; k < size && uint64_t(off) + k < d.hv_cap; k += blockDim.x) d.hv_slot[off + k] = BB_NONE;
+    }
+    __syncthreads();
+  }
+}
+
+// EMIT=false: partners under each pool entry; EMIT=true: write them
+template <bool EMIT>
+__global__ void k_heavy_walk(const DevState d, uint32_t n) {
+  const uint32_t E = min(d.ctr->hv_pool_n, d.hv_cap);
+  const int N = int(n), leaf0 = N - 1;
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+    const uint32_t slot = d.hv_slot[e];
+    if (slot == BB_NONE || d.hv_n[slot] == BB_NONE) {  // the slot's reservation failed (fallback path)
+      if (!EMIT) d.hv_cnt[e] = 0;
+      continue;
+    }
+    const uint32_t qi = d.heavy_list[slot];
+    const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
+    const int wend = world_end(d, qi, n);
+    uint32_t out = 0;
+    if (EMIT) out = d.pair_off[qi] + d.hv_off[e] - d.hv_off[d.hv_first[slot]];
+    uint32_t cnt = 0;
+    int stack[BB_BVH_STACK];
+    int sp = 0;
+    stack[sp++] = int(d.hv_pool[e]);
+    while (sp > 0) {
+      const int node = stack[--sp];
+      if (node >= leaf0) {
+        if (EMIT) {
+          const uint32_t k = out + cnt;
+          if (k < d.pair_capacity) d.pairs[k] = make_uint2(qi, uint32_t(node - leaf0));
+          else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+        }
+        ++cnt;
+        continue;
+      }
+      const int2 c = d.child[node];
+      if (bp_take(d, c.y, leaf0, int(qi), wend, qmn, qmx)) {
+        if (sp < BB_BVH_STACK) stack[sp++] = c.y;
+        else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+      }
+      if (bp_take(d, c.x, leaf0, int(qi), wend, qmn, qmx)) {
+        if (sp < BB_BVH_STACK) stack[sp++] = c.x;
+        else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+      }
+    }
+    if (!EMIT) d.hv_cnt[e] = cnt;
+  }
+}
+
+// pair count of every heavy query with a pool frontier
+__global__ void k_heavy_totals(const DevState d) {
+  const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
+  for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < hc; slot += gridDim.x * blockDim.x) {
+    const uint32_t m = d.hv_n[slot];
+    if (m == BB_NONE) continue;
+    const uint32_t f = d.hv_first[slot];
+    d.pair_cnt[d.heavy_list[slot]] = m ? d.hv_off[f + m - 1] + d.hv_cnt[f + m - 1] - d.hv_off[f] : 0u;
+  }
+}
+
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
                   int cur) {
   (void)cur;
@@ -457,9 +626,15 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);
   k_broad<false><<<bb, bt, 0, s>>>(d, n);
+  k_heavy_frontier<<<min(hb, uint32_t(sms) * 2), BB_HV_THREADS, 0, s>>>(d, n);
+  k_heavy_walk<false><<<sms * 8, 128, 0, s>>>(d, n);
+  bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr, sc.scan_status + 5 * size_t(sc.scan_tiles),
+                 sc.scan_tile_ctr + 5, d.ctr);
+  k_heavy_totals<<<(hb + 255) / 256, 256, 0, s>>>(d);
   k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n);
   bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr);
   k_broad_copy<<<sms * 16, 256, 0, s>>>(d, n);
   k_broad<true><<<bb, bt, 0, s>>>(d, n);
   k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n);
+  k_heavy_walk<true><<<sms * 8, 128, 0, s>>>(d, n);
 }

@@ -62,7 +62,8 @@ struct DevCounters {
                            // 7 connected components
   uint32_t np_counts[2];   // narrow-phase work lists: box-box pairs, pairs with a sphere
   uint32_t gc_list_n[2];   // edge colouring: sizes of the alternating uncoloured-manifold lists
-  uint32_t pad2[4];
+  uint32_t hv_pool_n;      // broad phase: frontier entries of the heavy queries
+  uint32_t pad2[3];
 };
 
 // ---- pointers of one world's device state ------------------------------------------------
@@ -82,6 +83,10 @@ struct DevState {
   uint32_t *pair_cnt, *pair_off;  // per query
   uint32_t *is_heavy, *heavy_list;  // 1: over the visit budget (block-cooperative), 2: staging spilled
   uint32_t* bp_stage;           // first 32 partners of each query (counting traversal)
+  // heavy queries split over the whole GPU: per slot its frontier range in the pool; per pool
+  // entry the subtree root, the slot, the partner count and its exclusive scan
+  uint32_t *hv_first, *hv_n, *hv_pool, *hv_slot, *hv_cnt, *hv_off;
+  uint32_t hv_cap;              // pool entries
   uint2* pairs;                 // (sorted a, sorted b)
   uint32_t* np_list;            // narrow-phase work list (pair indices; see k_np_classify)
   // manifolds (two buffers: [cur], [prev] chosen by parity)

@@ -176,6 +176,7 @@ __global__ void k_begin_substep(DevCounters* c) {
   c->np_counts[1] = 0;
   c->gc_list_n[0] = 0;
   c->gc_list_n[1] = 0;
+  c->hv_pool_n = 0;
   c->substeps += 1;
 }
 
@@ -238,6 +239,9 @@ struct bb_world_impl {
     d.pair_cnt = u32(N); d.pair_off = u32(N + 1);
     d.is_heavy = u32(N); d.heavy_list = u32(8192);
     d.bp_stage = u32(size_t(N) * 32);
+    d.hv_first = u32(8192); d.hv_n = u32(8192);
+    d.hv_cap = uint32_t(P);
+    d.hv_pool = u32(P); d.hv_slot = u32(P); d.hv_cnt = u32(P); d.hv_off = u32(P);
     d.pairs = dalloc<uint2>(P, owned, err, stream);
     for (int k = 0; k < 2; ++k) {
       d.m_bodies[k] = dalloc<uint2>(P, owned, err, stream);
@@ -285,7 +289,7 @@ struct bb_world_impl {
     // scratch zeroed at every substep: scan status (5 scans), sort hists / status (12 slots)
     sc.scan_tiles = bb_scan_tiles(std::max<size_t>(P, N + 1));
     sc.sort_tiles = bb_sort_tiles(std::max<size_t>(P, N));
-    size_t scan_words = size_t(5) * sc.scan_tiles;  // 64-bit
+    size_t scan_words = size_t(6) * sc.scan_tiles;  // 64-bit
     size_t sort_status_words = size_t(12) * sc.sort_tiles * 256;
     size_t hist_words = 5 * BB_HIST_REGION;
     scratch_bytes = scan_words * 8 + 16 * 4 + hist_words * 4 + sort_status_words * 4 + 16 * 4;
