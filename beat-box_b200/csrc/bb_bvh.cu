@@ -626,7 +626,7 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);
   k_broad<false><<<bb, bt, 0, s>>>(d, n);
-  k_heavy_frontier<<<min(hb, uint32_t(sms) * 2), BB_HV_THREADS, 0, s>>>(d, n);
+  k_heavy_frontier<<<hb, BB_HV_THREADS, 0, s>>>(d, n);  // one block per heavy slot
   k_heavy_walk<false><<<sms * 8, 128, 0, s>>>(d, n);
   bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr, sc.scan_status + 5 * size_t(sc.scan_tiles),
                  sc.scan_tile_ctr + 5, d.ctr);
