@@ -66,4 +66,5 @@ int bb_avbd_blocks(int sms);
 
 // occupancy helpers (bb_world.cu)
 int bb_coop_blocks(const void* kernel, int threads, int sms);
-cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s);
+cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s,
+                           size_t smem_bytes = 0);

@@ -313,29 +313,27 @@ struct PgsItem {
   float4 R1[PF], R2[PF], K[PF], lam[PF];
 };
 
-// item k given its record (loaded ahead): masses, frame, rows, impulses
-template <int PF>
-__device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k, uint4 rec, PgsItem<PF>& x) {
-  x.rec = rec;
-  x.mass = d.pgs_mass[k];
-  x.n = d.pgs_frame[3 * k];
-  x.t0 = d.pgs_frame[3 * k + 1];
-  x.t1 = d.pgs_frame[3 * k + 2];
-  const uint32_t c0 = rec.x, cc = rec.w & 0xFFu;
-#pragma unroll
-  for (int j = 0; j < PF; ++j) {
-    if (uint32_t(j) < cc) {
-      x.R1[j] = d.c_r1[c0 + j];
-      x.R2[j] = d.c_r2[c0 + j];
-      x.K[j] = d.c_k[c0 + j];
-      x.lam[j] = d.pgs_lam[c0 + j];
-    }
-  }
+// Contacts beyond the PF register-held ones (up to BB_MAX_CONTACTS - PF) are staged in this
+// thread's slot of dynamic shared memory with cp.async at prefetch time, so the run does not
+// pay one global round trip per extra contact.  Slot layout: [contact][R1, R2, K, lam].
+#define BB_PGS_EXTRA (BB_MAX_CONTACTS - 4)
+#define BB_PGS_SMEM (BB_PGS_THREADS * BB_PGS_EXTRA * 4 * 16)
+__device__ __forceinline__ float4* pgs_extra_slot() {
+  extern __shared__ float4 s_pgs_extra[];
+  return s_pgs_extra + threadIdx.x * (BB_PGS_EXTRA * 4);
 }
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = uint32_t(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <int PF>
-__device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, PgsItem<PF>& x) {
-  x.rec = d.pgs_rec[k];
+// STAGED: extra contacts go to shared memory (the persistent kernels); else they stay in global
+// memory and the run reads them there (the serial overflow path, which must not disturb the
+// slot of the item already prefetched for the next colour).
+template <int PF, bool STAGED>
+__device__ __forceinline__ void pgs_item_fill(const DevState& d, uint32_t k, PgsItem<PF>& x) {
   x.mass = d.pgs_mass[k];
   x.n = d.pgs_frame[3 * k];
   x.t0 = d.pgs_frame[3 * k + 1];
@@ -350,6 +348,30 @@ __device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, Pgs
       x.lam[j] = d.pgs_lam[c0 + j];
     }
   }
+  if (STAGED && cc > uint32_t(PF)) {
+    float4* slot = pgs_extra_slot();
+    for (uint32_t j = PF; j < cc; ++j) {
+      float4* e = slot + (j - PF) * 4;
+      cp_async16(e + 0, d.c_r1 + c0 + j);
+      cp_async16(e + 1, d.c_r2 + c0 + j);
+      cp_async16(e + 2, d.c_k + c0 + j);
+      cp_async16(e + 3, d.pgs_lam + c0 + j);
+    }
+    cp_async_commit();
+  }
+}
+
+// item k given its record (loaded ahead): masses, frame, rows, impulses
+template <int PF, bool STAGED = true>
+__device__ __forceinline__ void pgs_item_load_rest(const DevState& d, uint32_t k, uint4 rec, PgsItem<PF>& x) {
+  x.rec = rec;
+  pgs_item_fill<PF, STAGED>(d, k, x);
+}
+
+template <int PF, bool STAGED = true>
+__device__ __forceinline__ void pgs_item_load(const DevState& d, uint32_t k, PgsItem<PF>& x) {
+  x.rec = d.pgs_rec[k];
+  pgs_item_fill<PF, STAGED>(d, k, x);
 }
 
 // contacts per colour-ordered item (0 for items whose bodies both sleep): scanned into pgs_coff
@@ -403,7 +425,7 @@ __device__ void pgs_item_build(const DevState& d, int cur, uint32_t k, uint32_t 
 }
 
 // mode 0: warm start, 1: solve sweep (soft bias), 2: relax sweep
-template <int PF>
+template <int PF, bool STAGED = true>
 __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p, int cur, PgsItem<PF>& x, int mode) {
   if (x.rec.w & BB_PGS_SKIP) return;
   const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
@@ -426,15 +448,21 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
       }
     }
   }
-  for (uint32_t j = PF; j < cc; ++j) {  // contacts beyond the register-held ones
-    const uint32_t ci = c0 + j;
-    float4 lam = d.pgs_lam[ci];
-    if (mode == 0) {
-      pgs_contact_warm(f3(d.c_r1[ci]), f3(d.c_r2[ci]), lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
-    } else {
-      pgs_contact_solve(d.c_r1[ci], d.c_r2[ci], d.c_k[ci], lam, n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA,
-                        IB, va, wa, vb, wb);
-      d.pgs_lam[ci] = lam;
+  if (cc > uint32_t(PF)) {  // contacts beyond the register-held ones
+    const float4* slot = pgs_extra_slot();
+    if (STAGED) cp_async_wait_all();
+    for (uint32_t j = PF; j < cc; ++j) {
+      const uint32_t ci = c0 + j;
+      const float4* e = slot + (j - PF) * 4;
+      const float4 R1 = STAGED ? e[0] : d.c_r1[ci], R2 = STAGED ? e[1] : d.c_r2[ci];
+      float4 lam = STAGED ? e[3] : d.pgs_lam[ci];
+      if (mode == 0) {
+        pgs_contact_warm(f3(R1), f3(R2), lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
+      } else {
+        const float4 K = STAGED ? e[2] : d.c_k[ci];
+        pgs_contact_solve(R1, R2, K, lam, n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA, IB, va, wa, vb, wb);
+        d.pgs_lam[ci] = lam;
+      }
     }
   }
   if (x.rec.w & (1u << 8)) {
@@ -484,8 +512,8 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
     if (tid == 0) {
       for (uint32_t k = o0; k < o1; ++k) {
         PgsItem<PF> y;
-        pgs_item_load(d, k, y);
-        pgs_item_run(d, p, cur, y, mode);
+        pgs_item_load<PF, false>(d, k, y);
+        pgs_item_run<PF, false>(d, p, cur, y, mode);
       }
     }
     grid_sync(d.ctr, sync, epoch);
@@ -539,7 +567,6 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(co
   }
 }
 
-int bb_pgs_soft_blocks(int sms) { return bb_coop_blocks((const void*)k_pgs_soft<4>, BB_PGS_THREADS, sms); }
 
 
 // ---------------------------------------------------------------------------------------
@@ -663,6 +690,12 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_flow(co
   }
 }
 
+int bb_pgs_soft_blocks(int sms) {
+  cudaFuncSetAttribute((const void*)k_pgs_soft<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM);
+  cudaFuncSetAttribute((const void*)k_pgs_flow<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM);
+  return bb_coop_blocks((const void*)k_pgs_soft<4>, BB_PGS_THREADS, sms);
+}
+
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                        const StepScratch& sc, int coop_blocks, int sms) {
   k_pgs_count<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
@@ -678,7 +711,7 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
     float hh = h;
     void* args[] = {&dd, &pp, &cc, &nn, &hh};
     const void* kern = (const void*)k_pgs_flow<4>;
-    bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s);
+    bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
     return;
   }
   DevState dd = d;
@@ -688,7 +721,7 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
   const void* kern = (const void*)k_pgs_soft<4>;
-  bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s);
+  bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -72,11 +72,12 @@ int bb_coop_blocks(const void* kernel, int threads, int sms) {
   return sms * std::min(per_sm, 1);
 }
 
-cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s) {
+cudaError_t bb_launch_coop(const void* kernel, int blocks, int threads, void** args, cudaStream_t s,
+                           size_t smem_bytes) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(threads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem_bytes;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
