@@ -441,39 +441,13 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
 // frontier keeps left-to-right order and each entry covers a contiguous leaf range, so the
 // concatenated walks emit ascending partners, as the single-thread traversal does.  A query
 // whose frontier does not fit the pool falls back to k_broad_heavy (hv_n = BB_NONE).
-#define BB_HV_THREADS 1024
-#define BB_HV_PER_THREAD 4
+#define BB_HV_THREADS 256  // = BB_FRONTIER, so block_excl_scan serves both kernels
+#define BB_HV_PER_THREAD 16
 #define BB_HV_FRONTIER (BB_HV_THREADS * BB_HV_PER_THREAD)
-
-__device__ __forceinline__ uint32_t block_excl_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t& total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = s_warp[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-      if (lane >= o) w += y;
-    }
-    s_warp[lane] = w;
-  }
-  __syncthreads();
-  total = s_warp[31];
-  const uint32_t excl = x - v + (warp > 0 ? s_warp[warp - 1] : 0u);
-  __syncthreads();
-  return excl;
-}
 
 __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState d, uint32_t n) {
   __shared__ int s_fr[2][BB_HV_FRONTIER];
-  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_warp[BB_FRONTIER / 32];
   __shared__ uint32_t s_size, s_off, s_fits;
   const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
   const int N = int(n), leaf0 = N - 1;
@@ -507,7 +481,7 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
         }
       }
       uint32_t total;
-      const uint32_t pos = block_excl_scan_1024(c, s_warp, total);
+      const uint32_t pos = block_excl_scan(c, s_warp, total);
       if (total > BB_HV_FRONTIER || total == 0) {  // uniform: keep the current frontier (or none)
         if (total == 0 && t == 0) s_size = 0;
         __syncthreads();
