@@ -28,7 +28,7 @@ sys.path.insert(0, os.path.join(ROOT, "beat-box_b200"))
 
 import numpy as np  # noqa: E402
 
-from beatbox import scenes  # noqa: E402
+from beatbox import ranks, scenes  # noqa: E402
 
 DT = 1.0 / 60.0
 SUBSTEPS = 4
@@ -356,18 +356,6 @@ def batched_scenes(n_worlds: int):
     return [scenes.pile(int(nw), seed=k + 1) for k, nw in enumerate(sizes)]
 
 
-def balanced_share(sizes, rank: int, world_size: int):
-    """Greedy body-count-balanced assignment of worlds to ranks (largest first)."""
-    load = [0] * world_size
-    mine = []
-    for k in sorted(range(len(sizes)), key=lambda k: -sizes[k]):
-        r = min(range(world_size), key=lambda r: load[r])
-        load[r] += sizes[k]
-        if r == rank:
-            mine.append(k)
-    return sorted(mine)
-
-
 def run_batched(args, rank: int, world_size: int, local_rank: int):
     """Config 4: thousands of independent worlds stepped as one batch (world-prefixed Morton
     keys, one CUDA-graph launch per step), against the same worlds stepped one at a time through
@@ -386,7 +374,7 @@ def run_batched(args, rank: int, world_size: int, local_rank: int):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     all_scs = batched_scenes(args.worlds)
     sizes = [int(sc["n"]) for sc in all_scs]
-    scs = [all_scs[k] for k in balanced_share(sizes, rank, world_size)]
+    scs = [all_scs[k] for k in ranks.balanced_share(sizes, rank, world_size)]
     total = sum(int(sc["n"]) for sc in scs)
     p = bb.make_params(solver=bb.SOLVER_PGS_SOFT, iterations=8, relax_iterations=8, quirks=bb.QUIRKS_PHYSICAL)
     w = bb.World(total, pairs_per_body=8, device=local_rank)
