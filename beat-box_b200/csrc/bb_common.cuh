@@ -126,6 +126,7 @@ struct DevState {
   uint32_t* man_index;   // per pair slot: exclusive scan of hit
   // islands
   uint32_t *uf_parent, *is_root, *root_rank, *island;
+  uint32_t* island_start;  // per-island path: first sorted manifold of each island
   // colouring
   uint32_t* gc_color;    // per compact manifold
   uint32_t* gc_pid;      // pair-identity hash

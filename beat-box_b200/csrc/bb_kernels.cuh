@@ -45,6 +45,8 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
                       int sms, int cur, int coop_blocks);
 
 // bb_solve.cu: PGS_SOFT and AVBD solvers
+void bb_solve_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
+                      const StepScratch& sc, int sms);
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                        const StepScratch& sc, int coop_blocks, int sms);
 void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,

@@ -725,6 +725,186 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
 }
 
 // ---------------------------------------------------------------------------------------
+// Per-island path (USE_GRAPH_COLORING off, RBM:1390-1399; RB_sim.slang:1122-1406): one thread
+// per contact island runs the island's manifolds serially, in manifold order -- PGS_SOFT's
+// pre-step and solve sweeps, or the Baumgarte PGS of solvers.slang:3-136 -- then all bodies
+// integrate, then (PGS_SOFT only) the relax sweeps run per island again.  Manifolds are grouped
+// by island with a stable sort keyed by the island id of their dynamic body.
+
+// PGS::pre_step (solvers.slang:3-66) of one manifold slot
+__device__ void baum_pre_step_slot(const DevState& d, const Params& p, int cur, uint32_t slot, uint2 b, float inv_h) {
+  const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+  if (!awake(fa) && !awake(fb)) return;
+  const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
+  const Sym3 IA = load_iw(d, b.x), IB = load_iw(d, b.y);
+  float3 va = f3(d.vel[b.x]), wa = f3(d.omega[b.x]), vb = f3(d.vel[b.y]), wb = f3(d.omega[b.y]);
+  const float3 n = f3(d.m_normal[cur][slot]);
+  const float3 t0 = f3(d.m_t0[cur][slot]), t1 = f3(d.m_t1[cur][slot]);
+  const float3 pa = f3(d.pos[b.x]), pb = f3(d.pos[b.y]);
+  const int cc = d.m_keycc[cur][slot].y;
+  const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
+  for (int j = 0; j < cc; ++j) {
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    const float4 pp = d.c_pos[cur][ci];
+    const float3 r1 = xsub(f3(pp), pa), r2 = xsub(f3(pp), pb);
+    const float nmass = xrow_mass(r1, r2, n, ima, imb, IA, IB);
+    const float tm0 = xrow_mass(r1, r2, t0, ima, imb, IA, IB), tm1 = xrow_mass(r1, r2, t1, ima, imb, IA, IB);
+    const float bias = -0.2f * inv_h * fminf(pp.w + 0.01f, 0.f);
+    d.c_r1[ci] = f4(r1, nmass);
+    d.c_r2[ci] = f4(r2, tm0);
+    d.c_k[ci] = make_float4(tm1, bias, 0.f, 0.f);
+    const float4 lam = d.c_lam[cur][ci];
+    if (accum) pgs_contact_warm(r1, r2, lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
+  }
+  if (fa & BB_BODY_DYNAMIC) {
+    d.vel[b.x] = f4(va, d.vel[b.x].w);
+    d.omega[b.x] = f4(wa, 0.f);
+  }
+  if (fb & BB_BODY_DYNAMIC) {
+    d.vel[b.y] = f4(vb, d.vel[b.y].w);
+    d.omega[b.y] = f4(wb, 0.f);
+  }
+}
+
+// PGS::solve (solvers.slang:68-136) of one manifold slot
+__device__ void baum_solve_slot(const DevState& d, const Params& p, int cur, uint32_t slot, uint2 b) {
+  const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+  if (!awake(fa) && !awake(fb)) return;
+  const float ima = d.pos[b.x].w, imb = d.pos[b.y].w;
+  const Sym3 IA = load_iw(d, b.x), IB = load_iw(d, b.y);
+  float4 va4 = d.vel[b.x], vb4 = d.vel[b.y];
+  float3 va = f3(va4), wa = f3(d.omega[b.x]), vb = f3(vb4), wb = f3(d.omega[b.y]);
+  const float mu = sqrtf(d.iinv[b.x].w * d.iinv[b.y].w);
+  const float3 n = f3(d.m_normal[cur][slot]);
+  const float3 t0 = f3(d.m_t0[cur][slot]), t1 = f3(d.m_t1[cur][slot]);
+  const int cc = d.m_keycc[cur][slot].y;
+  const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
+  for (int j = 0; j < cc; ++j) {
+    const uint32_t ci = slot * BB_MAX_CONTACTS + j;
+    const float4 R1 = d.c_r1[ci], R2 = d.c_r2[ci], K = d.c_k[ci];
+    float4 lam = d.c_lam[cur][ci];
+    const float3 r1 = f3(R1), r2 = f3(R2);
+    if (fric) {
+      const float3 rv = xrel(r1, r2, va, wa, vb, wb);
+      const float tmass[2] = {R2.w, K.x};
+      float imp_t[2] = {lam.y, lam.z};
+      const float maxf = mu * lam.x;
+      for (int k = 0; k < 2; ++k) {
+        const float3 t = k == 0 ? t0 : t1;
+        float ti = tmass[k] * -xdot(rv, t);
+        if (accum) {
+          const float old = imp_t[k];
+          imp_t[k] = fminf(fmaxf(old + ti, -maxf), maxf);
+          ti = imp_t[k] - old;
+        } else {
+          ti = fminf(fmaxf(ti, -maxf), maxf);
+        }
+        xapply(xscale(t, ti), r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
+      }
+      lam.y = imp_t[0];
+      lam.z = imp_t[1];
+    }
+    float imp = R1.w * (K.y - xdot(xrel(r1, r2, va, wa, vb, wb), n));
+    if (accum) {
+      const float old = lam.x;
+      lam.x = fmaxf(old + imp, 0.f);
+      imp = lam.x - old;
+    } else {
+      imp = fmaxf(imp, 0.f);
+    }
+    xapply(xscale(n, imp), r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
+    d.c_lam[cur][ci] = lam;
+  }
+  if (fa & BB_BODY_DYNAMIC) {
+    d.vel[b.x] = f4(va, va4.w);
+    d.omega[b.x] = f4(wa, 0.f);
+  }
+  if (fb & BB_BODY_DYNAMIC) {
+    d.vel[b.y] = f4(vb, vb4.w);
+    d.omega[b.y] = f4(wb, 0.f);
+  }
+}
+
+// key of every manifold: the island of its dynamic body
+__global__ void k_island_keys(const DevState d, int cur) {
+  const uint32_t M = d.ctr->manifold_count;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    const uint2 b = d.m_bodies[cur][d.man_slot[cur][m]];
+    const uint32_t ia = d.island[b.x];
+    d.bucket_keys[0][m] = ia != BB_NONE ? ia : d.island[b.y];
+    d.bucket_vals[0][m] = m;
+  }
+}
+// island_start[v] = first sorted position with key >= v, v = 0..island_count
+__global__ void k_island_starts(const DevState d, uint32_t* starts, uint32_t n) {
+  const uint32_t M = d.ctr->manifold_count, nb = d.ctr->island_count;
+  const uint32_t* keys = d.bucket_keys[1];
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= nb && v <= n; v += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = M;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (keys[mid] < v) lo = mid + 1;
+      else hi = mid;
+    }
+    starts[v] = lo;
+  }
+}
+// phase 0: pre-step + solve sweeps; phase 1: relax sweeps (PGS_SOFT)
+__global__ void k_island_solve(const DevState d, Params p, int cur, const uint32_t* starts, float h, int phase) {
+  const uint32_t nb = d.ctr->island_count;
+  const uint32_t* list = d.bucket_vals[1];
+  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
+  const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
+  const bool soft = p.solver == BB_SOLVER_PGS_SOFT;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nb; v += gridDim.x * blockDim.x) {
+    const uint32_t s0 = starts[v], s1 = starts[v + 1];
+    auto each = [&](auto&& fn) {
+      for (uint32_t k = s0; k < s1; ++k) {
+        const uint32_t slot = d.man_slot[cur][list[k]];
+        fn(slot, d.m_bodies[cur][slot]);
+      }
+    };
+    if (phase == 0) {
+      each([&](uint32_t slot, uint2 b) {
+        if (soft) pgs_pre_step_slot(d, p, cur, slot, b, h, hertz);
+        else baum_pre_step_slot(d, p, cur, slot, b, inv_h);
+      });
+      for (uint32_t it = 0; it < p.iterations; ++it)
+        each([&](uint32_t slot, uint2 b) {
+          if (soft) pgs_solve_slot(d, p, cur, slot, b, true);
+          else baum_solve_slot(d, p, cur, slot, b);
+        });
+    } else {
+      for (uint32_t it = 0; it < p.relax_iterations; ++it)
+        each([&](uint32_t slot, uint2 b) { pgs_solve_slot(d, p, cur, slot, b, false); });
+    }
+  }
+}
+__global__ void k_island_integrate(const DevState d, Params p, uint32_t n, float h) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && awake(d.flags[i])) pgs_integrate(d, i, h, p.quirks & BB_QUIRK_INERTIA_TRANSPOSE);
+}
+
+void bb_solve_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
+                      const StepScratch& sc, int sms) {
+  if (n == 0) return;
+  const int T = BB_THREADS;
+  const uint32_t blocks = (n + T - 1) / T;
+  k_flow_init<<<blocks, T, 0, s>>>(d, p, n);  // world inverse inertia of every body
+  k_island_keys<<<sms * 8, T, 0, s>>>(d, cur);
+  uint32_t* keys[2] = {d.bucket_keys[0], d.bucket_keys[1]};
+  uint32_t* vals[2] = {d.bucket_vals[0], d.bucket_vals[1]};
+  // 3 digits (islands < 2^24): histogram region 1 and status slots 6..8 (the colouring's, unused here)
+  uint32_t* hist = sc.sort_hist + 1 * BB_HIST_REGION;
+  bb_launch_sort(s, keys, vals, &d.ctr->manifold_count, d.pair_capacity, 3, 0, hist,
+                 sc.sort_status + 6 * size_t(sc.sort_tiles) * 256, sc.sort_tile_ctr + 6, d.ctr, sms);
+  k_island_starts<<<(n + 1 + T - 1) / T, T, 0, s>>>(d, d.island_start, n);
+  k_island_solve<<<(n + 127) / 128, 128, 0, s>>>(d, p, cur, d.island_start, h, 0);
+  if (p.flags & BB_SIM_ADVECTION) k_island_integrate<<<blocks, T, 0, s>>>(d, p, n, h);
+  if (p.solver == BB_SOLVER_PGS_SOFT) k_island_solve<<<(n + 127) / 128, 128, 0, s>>>(d, p, cur, d.island_start, h, 1);
+}
+
+// ---------------------------------------------------------------------------------------
 // AVBD
 __device__ __forceinline__ uint32_t avbd_priority(uint32_t body, uint32_t round) {
   uint32_t x = body * 0x9e3779b9u + round * 0x85ebca6bu;

@@ -273,6 +273,7 @@ struct bb_world_impl {
     d.csr_cursor = u32(N + 1);
     d.hit = u32(P); d.man_index = u32(P);
     d.uf_parent = u32(N); d.is_root = u32(N); d.root_rank = u32(N); d.island = u32(N);
+    d.island_start = u32(N + 2);
     d.gc_color = u32(P); d.gc_pid = u32(P); d.gc_choice = u32(P); d.gc_mask = u32(N);
     d.gc_owner = dalloc<unsigned long long>(N * BB_MAX_COLORS, owned, err, stream);
     for (int k = 0; k < 2; ++k) { d.bucket_keys[k] = u32(P); d.bucket_vals[k] = u32(P); }
@@ -343,9 +344,11 @@ struct bb_world_impl {
     bb_advect(stream, d, params, n, h, sms);
     bb_islands(stream, d, params, n, sc, sms, cur, coop_cc);
     bb_sleep(stream, d, params, n, sms, cur);
-    bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
-    if (params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, sms);
-    else if (params.solver == BB_SOLVER_AVBD) bb_solve_avbd(stream, d, params, n, h, sc, sms, cur, coop_avbd);
+    const bool coloured = (params.flags & BB_SIM_USE_GRAPH_COLORING) != 0;
+    if (coloured || params.solver == BB_SOLVER_AVBD) bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
+    if (params.solver == BB_SOLVER_AVBD) bb_solve_avbd(stream, d, params, n, h, sc, sms, cur, coop_avbd);
+    else if (!coloured) bb_solve_islands(stream, d, params, n, h, cur, sc, sms);
+    else bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, sms);
     if (commit) parity = cur;
   }
 };
@@ -638,13 +641,11 @@ bb_status bb_set_material(void* world, uint32_t first, uint32_t count, float fri
 bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
   World* w = W(world);
   if (!w || !p) return fail(BB_E_INVALID, "bb_set_solver_params: bad arguments");
-  if (p->solver == BB_SOLVER_PGS)
-    return fail(BB_E_UNSUPPORTED, "BB_SOLVER_PGS runs only on the reference's per-island path, not provided");
+  if (p->solver == BB_SOLVER_PGS && (p->flags & BB_SIM_USE_GRAPH_COLORING))
+    return fail(BB_E_INVALID, "BB_SOLVER_PGS runs on the per-island path only: clear BB_SIM_USE_GRAPH_COLORING");
   if (p->solver > BB_SOLVER_AVBD) return fail(BB_E_INVALID, "unknown solver");
   if (p->gc_rounds > 63 || p->avbd_shock_layers == 0 || p->avbd_shock_layers > 64)
     return fail(BB_E_INVALID, "gc_rounds <= 63 and 1 <= avbd_shock_layers <= 64 required");
-  if (!(p->flags & BB_SIM_USE_GRAPH_COLORING))
-    return fail(BB_E_UNSUPPORTED, "the per-island solve path (USE_GRAPH_COLORING off) is not provided");
   for (int k = 0; k < 3; ++k)
     if (!(p->world_extent[k] > 0)) return fail(BB_E_INVALID, "world_extent must be positive");
   if (p->schedule > BB_SCHEDULE_COLOUR_BARRIER) return fail(BB_E_INVALID, "unknown schedule");
@@ -746,10 +747,13 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
       cudaEventRecord(ev[4], w->stream);
       bb_sleep(w->stream, w->d, w->params, w->n, w->sms, cur);
       cudaEventRecord(ev[5], w->stream);
-      bb_edge_coloring(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_edge);
+      const bool coloured = (w->params.flags & BB_SIM_USE_GRAPH_COLORING) != 0;
+      if (coloured || w->params.solver == BB_SOLVER_AVBD)
+        bb_edge_coloring(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_edge);
       cudaEventRecord(ev[6], w->stream);
-      if (w->params.solver == BB_SOLVER_PGS_SOFT) bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->sms);
-      else bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
+      if (w->params.solver == BB_SOLVER_AVBD) bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
+      else if (!coloured) bb_solve_islands(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->sms);
+      else bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->sms);
       cudaEventRecord(ev[7], w->stream);
       CU(cudaEventSynchronize(ev[7]));
       for (int k = 0; k < 7; ++k) {

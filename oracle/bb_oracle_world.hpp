@@ -597,6 +597,128 @@ template <class R> class World {
     for (uint32_t it = 0; it < p.relax_iterations; ++it) sweep([&](Manifold<R>& m) { pgs_solve(m, false, inv_h); });
   }
 
+  // ---- per-island path (USE_GRAPH_COLORING off): RBM:1390-1399 ----------------------------
+  // PGS::pre_step (solvers.slang:3-66): rows from the arms at pre-step time, Baumgarte bias
+  // -BIAS_FACTOR / h * min(depth + PENETRATION_FACTOR, 0), warm start.
+  void baum_pre_step(Manifold<R>& m, R inv_h) {
+    Body<R>& A = bodies[m.a];
+    Body<R>& B = bodies[m.b];
+    bool accum = (p.flags & BB_SIM_ACCUM_IMPULSE) != 0, fric = (p.flags & BB_SIM_FRICTION) != 0;
+    Mat3<R> IA = world_inv_inertia(A), IB = world_inv_inertia(B);
+    Vec3<R> va = A.vel, wa = A.omega, vb = B.vel, wb = B.omega;
+    for (int i = 0; i < m.cc; ++i) {
+      Contact<R>& c = m.c[i];
+      Vec3<R> r1 = c.pos - A.pos, r2 = c.pos - B.pos;
+      Vec3<R> rn1 = cross(r1, m.normal), rn2 = cross(r2, m.normal);
+      R kn = A.inv_mass + B.inv_mass + dot(rn1, mul_mv(IA, rn1)) + dot(rn2, mul_mv(IB, rn2));
+      c.nmass = kn == 0 ? R(0) : R(1) / kn;
+      for (int j = 0; j < 2; ++j) {
+        Vec3<R> rt1 = cross(r1, m.t[j]), rt2 = cross(r2, m.t[j]);
+        R kt = A.inv_mass + B.inv_mass + dot(rt1, mul_mv(IA, rt1)) + dot(rt2, mul_mv(IB, rt2));
+        c.tmass[j] = kt == 0 ? R(0) : R(1) / kt;
+      }
+      c.bias = -R(0.2) * inv_h * std::min(c.pen + R(0.01), R(0));
+      if (accum) {
+        Vec3<R> P = m.normal * c.ni;
+        if (fric)
+          for (int j = 0; j < 2; ++j) P = P + m.t[j] * c.ti[j];
+        va = va - P * A.inv_mass;
+        wa = wa - mul_mv(IA, cross(r1, P));
+        vb = vb + P * B.inv_mass;
+        wb = wb + mul_mv(IB, cross(r2, P));
+      }
+    }
+    if (is_dyn(A)) { A.vel = va; A.omega = wa; }
+    if (is_dyn(B)) { B.vel = vb; B.omega = wb; }
+  }
+  // PGS::solve (solvers.slang:68-136): friction rows, then the normal row with the Baumgarte bias
+  void baum_solve(Manifold<R>& m) {
+    Body<R>& A = bodies[m.a];
+    Body<R>& B = bodies[m.b];
+    bool accum = (p.flags & BB_SIM_ACCUM_IMPULSE) != 0, fric = (p.flags & BB_SIM_FRICTION) != 0;
+    Mat3<R> IA = world_inv_inertia(A), IB = world_inv_inertia(B);
+    R mu = std::sqrt(A.friction * B.friction);
+    Vec3<R> va = A.vel, wa = A.omega, vb = B.vel, wb = B.omega;
+    for (int i = 0; i < m.cc; ++i) {
+      Contact<R>& c = m.c[i];
+      Vec3<R> r1 = c.pos - A.pos, r2 = c.pos - B.pos;
+      Vec3<R> rv = vb + cross(wb, r2) - va - cross(wa, r1);
+      if (fric) {
+        for (int j = 0; j < 2; ++j) {
+          R ti = c.tmass[j] * -dot(rv, m.t[j]);
+          R maxf = mu * c.ni;
+          if (accum) {
+            R old = c.ti[j];
+            c.ti[j] = std::min(std::max(old + ti, -maxf), maxf);
+            ti = c.ti[j] - old;
+          } else {
+            ti = std::min(std::max(ti, -maxf), maxf);
+          }
+          Vec3<R> P = m.t[j] * ti;
+          va = va - P * A.inv_mass;
+          wa = wa - mul_mv(IA, cross(r1, P));
+          vb = vb + P * B.inv_mass;
+          wb = wb + mul_mv(IB, cross(r2, P));
+        }
+      }
+      rv = vb + cross(wb, r2) - va - cross(wa, r1);
+      R imp = c.nmass * (-dot(rv, m.normal) + c.bias);
+      if (accum) {
+        R old = c.ni;
+        c.ni = std::max(old + imp, R(0));
+        imp = c.ni - old;
+      } else {
+        imp = std::max(imp, R(0));
+      }
+      Vec3<R> P = m.normal * imp;
+      va = va - P * A.inv_mass;
+      wa = wa - mul_mv(IA, cross(r1, P));
+      vb = vb + P * B.inv_mass;
+      wb = wb + mul_mv(IB, cross(r2, P));
+    }
+    if (is_dyn(A)) { A.vel = va; A.omega = wa; }
+    if (is_dyn(B)) { B.vel = vb; B.omega = wb; }
+  }
+  // entry_collision_pre_solver / solver / integrate / solver_relaxation (RB_sim.slang:1122-1406):
+  // each contact island's manifolds serially, islands independent.  A manifold belongs to the
+  // island of its dynamic body; within an island the manifolds run in manifold (pair) order.
+  void solve_islands(R h) {
+    const R inv_h = h > 0 ? R(1) / h : R(0);
+    const R hertz = std::min(R(p.contact_hertz), inv_h * R(0.3333333333333333));
+    const bool soft = p.solver == BB_SOLVER_PGS_SOFT;
+    std::vector<std::vector<uint32_t>> lists(stats.island_count);
+    for (uint32_t mi = 0; mi < manifolds.size(); ++mi) {
+      const Manifold<R>& m = manifolds[mi];
+      uint32_t isl = island[m.a] != MAX_U32 ? island[m.a] : island[m.b];
+      if (isl != MAX_U32) lists[isl].push_back(mi);
+    }
+    auto per_island = [&](auto&& fn) {
+      pool.parallel_for(lists.size(), [&](size_t k) {
+        for (uint32_t mi : lists[k])
+          if (pair_active(manifolds[mi])) fn(manifolds[mi]);
+      }, 16);
+    };
+    per_island([&](Manifold<R>& m) {
+      if (soft) pgs_pre_step(m, h, hertz);
+      else baum_pre_step(m, inv_h);
+    });
+    for (uint32_t it = 0; it < p.iterations; ++it)
+      per_island([&](Manifold<R>& m) {
+        if (soft) pgs_solve(m, true, inv_h);
+        else baum_solve(m);
+      });
+    if (p.flags & BB_SIM_ADVECTION) {
+      pool.parallel_for(n(), [&](size_t i) {
+        Body<R>& r = bodies[i];
+        if (!awake(r)) return;
+        r.pos = r.pos + r.vel * h;
+        r.rot = apply_angular_velocity(r.rot, r.omega, h);
+      }, 1024);
+    }
+    if (soft)
+      for (uint32_t it = 0; it < p.relax_iterations; ++it) per_island([&](Manifold<R>& m) { pgs_solve(m, false, inv_h); });
+  }
+
   // entry_rigid_body_sim / RigidBody::advect (RB_sim.slang:518-554, extensions.slang:127-139)
   void advect(R h) {
     if (p.solver == BB_SOLVER_AVBD || !(p.flags & BB_SIM_ADVECTION)) return;
@@ -1004,8 +1126,10 @@ template <class R> class World {
     advect(h);
     islands();
     sleep();
-    edge_coloring();
+    const bool coloured = (p.flags & BB_SIM_USE_GRAPH_COLORING) != 0;
+    if (coloured || p.solver == BB_SOLVER_AVBD) edge_coloring();
     if (p.solver == BB_SOLVER_AVBD) solve_avbd(h);
+    else if (!coloured) solve_islands(h);
     else if (p.solver == BB_SOLVER_PGS_SOFT) solve_pgs_soft(h);
     publish();
   }

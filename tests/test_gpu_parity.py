@@ -163,6 +163,43 @@ def test_one_step_state_within_tolerance(oracle_lib, solver, quirks):
     assert verr < 2e-4 * vscale, verr
 
 
+@pytest.mark.parametrize("solver", [bb.SOLVER_PGS, bb.SOLVER_PGS_SOFT])
+def test_per_island_path_one_step_within_tolerance(oracle_lib, solver):
+    """USE_GRAPH_COLORING off: every contact island solved serially in manifold order, with the
+    Baumgarte PGS or PGS_SOFT, against the oracle's same schedule."""
+    base = scenes.box_grid(n_side=6, layers=4)
+    sc, p = settled(oracle_lib, base, bb.SOLVER_PGS_SOFT, bb.QUIRKS_PHYSICAL, 45)
+    p.solver = solver
+    p.flags = p.flags & ~bb.SIM_USE_GRAPH_COLORING
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    o.step(DT, 4)
+    w.step(DT, 4)
+    w.sync()
+    st = w.stats()
+    assert st["manifold_count"] > 50 and st["graph_color_count"] == 0 and st["error_flags"] == 0
+    g, r = w.read_state(), o.state()
+    dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+    perr = np.abs(g["pos"][dyn] - r["pos"][dyn]).max() / np.abs(r["pos"][dyn]).max()
+    verr = np.abs(g["vel"][dyn] - r["vel"][dyn]).max()
+    assert perr < 1e-4, perr
+    assert verr < 2e-4 * max(np.abs(r["vel"][dyn]).max(), 1.0), verr
+
+
+def test_per_island_pgs_settles_a_pile():
+    sc = scenes.box_grid(n_side=5, layers=3)
+    p = bb.make_params(solver=bb.SOLVER_PGS, quirks=bb.QUIRKS_PHYSICAL, iterations=8, relax_iterations=8)
+    p.flags = p.flags & ~bb.SIM_USE_GRAPH_COLORING
+    w = bb.world_from_scene(sc, params=p)
+    for _ in range(180):
+        w.step(DT, 4)
+    st = w.read_state()
+    dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+    assert np.abs(st["vel"][dyn]).max() < 0.5
+    assert st["pos"][dyn, 1].min() > 0.3  # resting on the ground, nothing fell through
+    assert w.stats()["error_flags"] == 0
+
+
 def energy_stats(state, sc):
     dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
     m = sc["mass"][dyn].astype(np.float64)
@@ -242,9 +279,9 @@ def test_invalid_arguments_are_rejected():
     with pytest.raises(bb.BeatboxError) as e:
         w.step(0.0, 1)
     assert e.value.code == bb.E_INVALID
-    with pytest.raises(bb.BeatboxError) as e:
+    with pytest.raises(bb.BeatboxError) as e:  # Baumgarte PGS runs on the per-island path only
         w.set_params(solver=bb.SOLVER_PGS)
-    assert e.value.code == bb.E_UNSUPPORTED
+    assert e.value.code == bb.E_INVALID
     with pytest.raises(bb.BeatboxError):
         w.add_box_shape(-1.0, 1.0, 1.0)
 
