@@ -487,15 +487,21 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
         __syncthreads();
         break;
       }
+      uint32_t work = 0;  // leaves under this thread's new internal entries
       for (uint32_t k = 0; k < c; ++k) {
         s_fr[cur ^ 1][pos + k] = kid[k];
-        internal |= kid[k] < leaf0;
+        if (kid[k] < leaf0) {
+          internal = true;
+          work += uint32_t(d.range_last[kid[k]] - d.range_first[kid[k]] + 1);
+        }
       }
       const int more = __syncthreads_or(internal);
       cur ^= 1;
       if (t == 0) s_size = total;
-      __syncthreads();
-      if (!more) break;
+      uint32_t total_work;
+      block_excl_scan(work, s_warp, total_work);  // ends with a CTA barrier
+      // enough entries for the GPU, each with a short walk left: stop expanding
+      if (!more || (total >= BB_FRONTIER && total_work <= 32u * total)) break;
     }
     const uint32_t size = s_size;
     if (t == 0) {

@@ -34,6 +34,10 @@ DT = 1.0 / 60.0
 SUBSTEPS = 4
 N_BODIES = 100_000
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes (read + write) of one k_pgs_soft launch on the 100k mixed column, from one ncu
+# capture at step ~298 of the run (dram__bytes_read.sum + dram__bytes_write.sum; the capture
+# command is in profiles/k_pgs_soft_k_narrow_k_components_mixed_column_100k.md)
+SOLVER_TRAFFIC_MIXED_100K = 114.5e6 + 24.1e6
 
 
 def workload(args):
@@ -294,7 +298,9 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     achieved = sb / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else 0.0
     roof = {"kernel": "solve (k_pgs_soft)" if args.solver == "pgs" else "solve (AVBD kernels)", "bound": "hbm",
             "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
-            "peak_source": "measured" if not pk.get("fallback") else "fallback", "traffic": None,
+            "peak_source": "measured" if not pk.get("fallback") else "fallback",
+            "traffic": (SOLVER_TRAFFIC_MIXED_100K if args.solver == "pgs" and args.scene == "mixed_column"
+                        and args.bodies == N_BODIES else None),
             "algorithmic_bytes_per_launch": sb, "ms_per_launch": solve_ms,
             "stage_ms_per_substep": {k: v / launches_per_stage for k, v in stages.items()}, "dominant_stage": dom}
 
