@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(PKG, "libbeatbox.so")
 # status codes and flags (include/beatbox.h)
 OK, E_INVALID, E_CAPACITY, E_CUDA, E_DEVICE_LIMIT, E_BUDGET, E_UNSUPPORTED = range(7)
 BODY_DYNAMIC, BODY_GRAVITY, BODY_SLEEPING = 1 << 1, 1 << 2, 1 << 3
-SHAPE_BOX, SHAPE_SPHERE = 0, 1
+SHAPE_BOX, SHAPE_SPHERE, SHAPE_VOXEL = 0, 1, 2
 INERTIA_PHYSICAL, INERTIA_REFERENCE, INERTIA_EXPLICIT = 0, 1, 2
 SOLVER_PGS, SOLVER_PGS_SOFT, SOLVER_AVBD = 0, 1, 2
 SIM_ACCUM_IMPULSE, SIM_FRICTION, SIM_WARM_STARTING, SIM_ADVECTION = 1, 2, 4, 8
@@ -37,7 +37,7 @@ BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
 SCHEDULE_DATAFLOW, SCHEDULE_COLOUR_BARRIER = 0, 1
 SORT_STATIC_MAX_KEYS = 262144
 DBG = dict(morton=1, sorted_keys=2, sorted_ids=3, lbvh_child=4, leaf_aabb=5, node_aabb=6, pairs=7,
-           manifolds=8, contacts=9, edge_colors=10, body_colors=11, islands=12, support_depth=13)
+           manifolds=8, contacts=9, edge_colors=10, body_colors=11, islands=12, support_depth=13, body_inertia=14)
 
 
 class BeatboxError(RuntimeError):
@@ -72,13 +72,20 @@ class BodyDesc(ctypes.Structure):
     _fields_ = [("position", ctypes.c_float * 3), ("rotation", ctypes.c_float * 4), ("velocity", ctypes.c_float * 3),
                 ("omega", ctypes.c_float * 3), ("shape", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("mass", ctypes.c_float), ("density", ctypes.c_float), ("friction", ctypes.c_float),
-                ("restitution", ctypes.c_float), ("inertia_mode", ctypes.c_uint32), ("inv_inertia", ctypes.c_float * 3)]
+                ("restitution", ctypes.c_float), ("inertia_mode", ctypes.c_uint32), ("inv_inertia", ctypes.c_float * 3),
+                ("inv_inertia_off", ctypes.c_float * 3)]
+
+
+class VoxelInfo(ctypes.Structure):
+    _fields_ = [("grid_origin", ctypes.c_float * 3), ("box_min", ctypes.c_float * 3), ("box_max", ctypes.c_float * 3),
+                ("solid_count", ctypes.c_uint32), ("surface_count", ctypes.c_uint32), ("unit_mass", ctypes.c_float),
+                ("unit_inv_inertia", ctypes.c_float * 6)]
 
 
 BODY_DTYPE = np.dtype([("position", "<f4", 3), ("rotation", "<f4", 4), ("velocity", "<f4", 3), ("omega", "<f4", 3),
                        ("shape", "<u4"), ("flags", "<u4"), ("mass", "<f4"), ("density", "<f4"),
                        ("friction", "<f4"), ("restitution", "<f4"), ("inertia_mode", "<u4"),
-                       ("inv_inertia", "<f4", 3)])
+                       ("inv_inertia", "<f4", 3), ("inv_inertia_off", "<f4", 3)])
 assert BODY_DTYPE.itemsize == ctypes.sizeof(BodyDesc)
 
 
@@ -143,6 +150,8 @@ _SIG = {
     "bb_world_destroy": (ctypes.c_int32, [_P]),
     "bb_add_box_shape": (ctypes.c_int32, [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.POINTER(_U32)]),
     "bb_add_sphere_shape": (ctypes.c_int32, [_P, ctypes.c_float, ctypes.POINTER(_U32)]),
+    "bb_add_voxel_shape": (ctypes.c_int32, [_P, _U32, _U32, _U32, ctypes.c_float, _P, ctypes.POINTER(_U32)]),
+    "bb_voxel_shape_info": (ctypes.c_int32, [_U32, _U32, _U32, ctypes.c_float, _P, ctypes.POINTER(VoxelInfo), _P, _U32]),
     "bb_add_bodies": (ctypes.c_int32, [_P, ctypes.POINTER(BodyDesc), _U32, ctypes.POINTER(_U32)]),
     "bb_add_world": (ctypes.c_int32, [_P, ctypes.POINTER(BatchWorldDesc), ctypes.POINTER(BodyDesc), _U32,
                                       ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
@@ -268,6 +277,15 @@ class World:
         _check(self.L.bb_add_sphere_shape(self.h, r, ctypes.byref(out)))
         return out.value
 
+    def add_voxel_shape(self, solid, voxel_size: float) -> int:
+        """Voxel shape from an occupancy grid indexed solid[z, y, x] (non-zero = solid)."""
+        g = np.ascontiguousarray(np.asarray(solid) != 0, dtype=np.uint8)
+        nz, ny, nx = g.shape
+        out = _U32()
+        _check(self.L.bb_add_voxel_shape(self.h, nx, ny, nz, float(voxel_size), g.ctypes.data_as(ctypes.c_void_p),
+                                         ctypes.byref(out)))
+        return out.value
+
     def _shape_for(self, shape: int, half) -> int:
         key = (int(shape), float(half[0]), float(half[1]), float(half[2]))
         h = self._shape_cache.get(key)
@@ -285,7 +303,10 @@ class World:
         a["rotation"] = scene["quat"]
         a["velocity"] = scene["vel"]
         a["omega"] = scene["omega"]
-        a["shape"] = [self._shape_for(int(t), h) for t, h in zip(scene["shape"].tolist(), scene["half"].tolist())]
+        vox_handles = [self.add_voxel_shape(v["solid"], v["voxel_size"]) for v in scene.get("voxel_shapes", [])]
+        vidx = scene.get("voxel")
+        a["shape"] = [vox_handles[int(vidx[i])] if int(t) == SHAPE_VOXEL else self._shape_for(int(t), h)
+                      for i, (t, h) in enumerate(zip(scene["shape"].tolist(), scene["half"].tolist()))]
         a["flags"] = scene["flags"]
         a["mass"] = scene["mass"]
         a["density"] = 0.0
@@ -293,6 +314,8 @@ class World:
         a["restitution"] = scene["restitution"]
         a["inertia_mode"] = inertia_mode
         a["inv_inertia"] = scene["inv_inertia"]
+        if "inv_inertia_off" in scene:
+            a["inv_inertia_off"] = scene["inv_inertia_off"]
         return descs, n
 
     def add_scene(self, scene: dict, inertia_mode: int = INERTIA_EXPLICIT) -> int:
@@ -419,7 +442,7 @@ class World:
         cnt = ctypes.c_uint64()
         _check(self.L.bb_debug_read(self.h, code, None, 0, ctypes.byref(cnt)))
         n = cnt.value
-        if which in ("leaf_aabb", "node_aabb"):
+        if which in ("leaf_aabb", "node_aabb", "body_inertia"):
             buf = np.empty(n, np.float32)
         elif which == "lbvh_child":
             buf = np.empty(n, np.int32)
@@ -430,7 +453,7 @@ class World:
         else:
             buf = np.empty(n, np.uint32)
         _check(self.L.bb_debug_read(self.h, code, _ptr(buf), buf.nbytes, ctypes.byref(cnt)))
-        return buf
+        return buf.reshape(-1, 6) if which == "body_inertia" else buf
 
     # ---- profiling --------------------------------------------------------------------------
     def set_profiling(self, on: bool):
@@ -443,6 +466,25 @@ class World:
         _check(self.L.bb_read_stage_times(self.h, _ptr(ms), 32, ctypes.byref(ns), names, 1024))
         nm = names.raw.split(b"\0")[: ns.value]
         return {k.decode(): float(v) for k, v in zip(nm, ms[: ns.value])}
+
+
+def voxel_shape_info(solid, voxel_size: float) -> dict:
+    """What a voxel shape derives from its grid (solid[z, y, x]), computed on the host:
+    grid origin (minus the centre of mass), box min/max, solid and surface counts, mass and
+    inverse inertia (xx yy zz xy xz yz) at density 1, and the packed surface list."""
+    L = load_library()
+    g = np.ascontiguousarray(np.asarray(solid) != 0, dtype=np.uint8)
+    nz, ny, nx = g.shape
+    info = VoxelInfo()
+    _check(L.bb_voxel_shape_info(nx, ny, nz, float(voxel_size), g.ctypes.data_as(ctypes.c_void_p), ctypes.byref(info),
+                                 None, 0))
+    surf = np.zeros(info.surface_count, np.uint32)
+    _check(L.bb_voxel_shape_info(nx, ny, nz, float(voxel_size), g.ctypes.data_as(ctypes.c_void_p), ctypes.byref(info),
+                                 surf.ctypes.data_as(ctypes.c_void_p), len(surf)))
+    return {"grid_origin": np.array(info.grid_origin[:], np.float32), "box_min": np.array(info.box_min[:], np.float32),
+            "box_max": np.array(info.box_max[:], np.float32), "solid_count": int(info.solid_count),
+            "surface_count": int(info.surface_count), "unit_mass": np.float32(info.unit_mass),
+            "unit_inv_inertia": np.array(info.unit_inv_inertia[:], np.float32), "surface": surf}
 
 
 def world_from_scene(scene: dict, params: SolverParams | None = None, pairs_per_body: int = 16, **kw) -> World:
@@ -462,6 +504,8 @@ def world_from_scene(scene: dict, params: SolverParams | None = None, pairs_per_
 def scene_request_arrays(scene: dict, inertia_mode: int = INERTIA_EXPLICIT):
     """(shapes, bodies) ctypes arrays of a scene for a server request: one shape per distinct
     (type, half extents), body.shape indexing the shape table."""
+    if scene.get("voxel_shapes"):
+        raise ValueError("scene_request_arrays: served worlds take box and sphere shapes only")
     table: dict = {}
     idx = []
     for t, h in zip(scene["shape"].tolist(), scene["half"].tolist()):

@@ -9,6 +9,8 @@ They stand in for the workloads the benchmark is quoted on (no public dataset ex
 * ``mixed_column`` -- 100k boxes and spheres in a 60x60x200 m column inside a 5-wall container.
 * ``pyramids``     -- 1,000 box pyramids of 1,000 boxes each on a 32x32 grid.
 * ``batch_worlds`` -- many independent small piles (world id per body).
+* ``voxel_pile``   -- concave voxel bodies (L, cross, hollow frame) dropped on a ground box, the
+                      kind of scene the reference's voxel showcase builds (scene_manager.hpp:574-).
 
 A scene is a dict of numpy arrays, one row per body, ready for ``World.add_bodies`` and for the
 oracle.  Static bodies have mass 0, inverse mass 0 and zero inverse inertia.
@@ -23,6 +25,7 @@ BODY_DYNAMIC = 1 << 1
 BODY_GRAVITY = 1 << 2
 SHAPE_BOX = 0
 SHAPE_SPHERE = 1
+SHAPE_VOXEL = 2
 
 _M64 = (1 << 64) - 1
 
@@ -114,6 +117,7 @@ class SceneBuilder:
     def __init__(self, inertia: str = "physical"):
         self.inertia = inertia
         self.parts: list[dict] = []
+        self.voxel_shapes: list[dict] = []  # {"solid": uint8[z, y, x], "voxel_size": float, "info": ...}
         self.bounds = None  # optional (world_min[3], world_extent[3]) for Morton codes
 
     def add(self, pos, quat, half, shape, flags, mass, friction=0.5, restitution=0.0, vel=None, omega=None):
@@ -141,8 +145,42 @@ class SceneBuilder:
         self.parts.append(dict(
             pos=pos.astype(np.float32), quat=quat.astype(np.float32), half=half.astype(np.float32),
             shape=shape, flags=flags, mass=m32, inv_mass=np.asarray(inv_mass, np.float32), inv_inertia=ii,
+            inv_inertia_off=np.zeros((n, 3), np.float32), voxel=np.zeros(n, np.uint32),
             friction=np.broadcast_to(np.asarray(friction, np.float32), (n,)).copy(),
             restitution=np.broadcast_to(np.asarray(restitution, np.float32), (n,)).copy(),
+            vel=np.zeros((n, 3), np.float32) if vel is None else np.asarray(vel, np.float32).reshape(n, 3),
+            omega=np.zeros((n, 3), np.float32) if omega is None else np.asarray(omega, np.float32).reshape(n, 3),
+        ))
+
+    def add_voxel_shape(self, solid, voxel_size: float) -> int:
+        """Register an occupancy grid solid[z, y, x]; returns its index for add_voxel."""
+        from . import voxel_shape_info  # the library's host build (centre of mass, inertia)
+        g = np.ascontiguousarray(np.asarray(solid) != 0, dtype=np.uint8)
+        self.voxel_shapes.append({"solid": g, "voxel_size": float(voxel_size), "info": voxel_shape_info(g, voxel_size)})
+        return len(self.voxel_shapes) - 1
+
+    def add_voxel(self, pos, quat, shape_index, flags, density=1000.0, friction=0.5, vel=None, omega=None):
+        """Voxel bodies of one registered shape.  Mass = density * unit mass; the inverse inertia
+        (diagonal and off-diagonal) is the shape's unit one scaled by unit_mass / mass in float32,
+        the same arithmetic the library applies to a voxel body added without explicit inertia."""
+        info = self.voxel_shapes[shape_index]["info"]
+        pos = np.asarray(pos, np.float64).reshape(-1, 3)
+        n = pos.shape[0]
+        flags = np.broadcast_to(np.asarray(flags, np.uint32), (n,)).copy()
+        dyn = (flags & BODY_DYNAMIC) != 0
+        mass = np.where(dyn, np.float32(density) * info["unit_mass"], np.float32(0)).astype(np.float32)
+        scale = np.where(dyn, info["unit_mass"] / np.where(dyn, mass, np.float32(1)), np.float32(0)).astype(np.float32)
+        ui = info["unit_inv_inertia"]
+        ii = (ui[None, :3] * scale[:, None]).astype(np.float32)
+        io = (ui[None, 3:] * scale[:, None]).astype(np.float32)
+        half = 0.5 * (info["box_max"] - info["box_min"])
+        self.parts.append(dict(
+            pos=pos.astype(np.float32), quat=np.asarray(quat, np.float64).reshape(n, 4).astype(np.float32),
+            half=np.tile(half.astype(np.float32), (n, 1)), shape=np.full(n, SHAPE_VOXEL, np.uint32), flags=flags,
+            mass=mass, inv_mass=np.where(dyn, np.float32(1) / np.where(dyn, mass, np.float32(1)), 0).astype(np.float32),
+            inv_inertia=ii, inv_inertia_off=io, voxel=np.full(n, shape_index, np.uint32),
+            friction=np.broadcast_to(np.asarray(friction, np.float32), (n,)).copy(),
+            restitution=np.zeros(n, np.float32),
             vel=np.zeros((n, 3), np.float32) if vel is None else np.asarray(vel, np.float32).reshape(n, 3),
             omega=np.zeros((n, 3), np.float32) if omega is None else np.asarray(omega, np.float32).reshape(n, 3),
         ))
@@ -155,6 +193,8 @@ class SceneBuilder:
         scene = {k: np.ascontiguousarray(np.concatenate([p[k] for p in self.parts])) for k in keys}
         scene["n"] = scene["pos"].shape[0]
         scene["bounds"] = self.bounds
+        if self.voxel_shapes:
+            scene["voxel_shapes"] = [{"solid": v["solid"], "voxel_size": v["voxel_size"]} for v in self.voxel_shapes]
         return scene
 
 
@@ -291,3 +331,51 @@ def batch_sizes(n_worlds: int, seed: int = 0, lo: int = 16, hi: int = 2048) -> n
     """Body counts of a batch: floor(exp(U(ln lo, ln hi))) per world."""
     u = uniform(seed, 90, n_worlds, math.log(lo), math.log(hi))
     return np.floor(np.exp(u)).astype(np.int64)
+
+
+# ---- voxel (concave) bodies --------------------------------------------------------------
+def voxel_l_shape(n: int = 4, thick: int = 2) -> np.ndarray:
+    """An L: an n x n x thick slab with the (n-1) x (n-1) upper-right block removed, grid [z, y, x]."""
+    g = np.zeros((thick, n, n), np.uint8)
+    g[:, 0, :] = 1
+    g[:, :, 0] = 1
+    return g
+
+
+def voxel_cross(n: int = 5, thick: int = 1) -> np.ndarray:
+    """A plus sign of arm width 1 in an n x n plane, thick cells deep, grid [z, y, x]."""
+    g = np.zeros((thick, n, n), np.uint8)
+    g[:, n // 2, :] = 1
+    g[:, :, n // 2] = 1
+    return g
+
+
+def voxel_frame(n: int = 5, thick: int = 1) -> np.ndarray:
+    """A hollow square frame (border one cell wide) in an n x n plane, grid [z, y, x]."""
+    g = np.ones((thick, n, n), np.uint8)
+    g[:, 1:-1, 1:-1] = 0
+    return g
+
+
+def voxel_pile(n_bodies: int = 60, seed: int = 0, voxel_size: float = 0.2, density: float = 1000.0,
+               friction: float = 0.5, spacing: float = 1.6, height: float = 1.2, layer: float = 1.5) -> dict:
+    """Concave voxel bodies (L, cross, hollow frame, cycling) with uniform random orientations,
+    jittered on a grid (spacing and layer apart, so no two overlap at the start) over a static
+    ground box (top at y = 0)."""
+    sb = SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50], friction=friction)
+    shapes = [sb.add_voxel_shape(g, voxel_size) for g in (voxel_l_shape(), voxel_cross(), voxel_frame())]
+    per = max(1, int(math.ceil(math.sqrt(n_bodies / 3.0))))
+    k = np.arange(n_bodies)
+    lay, rem = k // (per * per), k % (per * per)
+    gx, gz = rem % per, rem // per
+    half = 0.5 * spacing * (per - 1)
+    pos = np.stack([-half + gx * spacing + uniform(seed, 1, n_bodies, -0.05, 0.05),
+                    height + lay * layer + uniform(seed, 2, n_bodies, 0.0, 0.1),
+                    -half + gz * spacing + uniform(seed, 3, n_bodies, -0.05, 0.05)], axis=1)
+    quat = random_rotations(seed, 10, n_bodies)
+    for si in range(len(shapes)):
+        sel = k % len(shapes) == si
+        if sel.any():
+            sb.add_voxel(pos[sel], quat[sel], shapes[si], BODY_DYNAMIC | BODY_GRAVITY, density, friction)
+    return sb.build()

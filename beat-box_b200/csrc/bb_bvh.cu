@@ -311,8 +311,9 @@ __global__ void k_broad_copy(const DevState d, uint32_t n) {
   }
 }
 
-// block-wide exclusive scan of one value per thread (blockDim.x == BB_FRONTIER)
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+// block-wide exclusive scan of one value per thread (blockDim.x == NT)
+template <int NT>
+__device__ __forceinline__ uint32_t block_scan_nt(uint32_t v, uint32_t* s_warp, uint32_t& total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t x = v;
 #pragma unroll
@@ -323,19 +324,22 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp
   if (lane == 31) s_warp[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    uint32_t w = lane < BB_FRONTIER / 32 ? s_warp[lane] : 0u;
+    uint32_t w = lane < NT / 32 ? s_warp[lane] : 0u;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
       if (lane >= o) w += y;
     }
-    if (lane < BB_FRONTIER / 32) s_warp[lane] = w;
+    if (lane < NT / 32) s_warp[lane] = w;
   }
   __syncthreads();
-  total = s_warp[BB_FRONTIER / 32 - 1];
+  total = s_warp[NT / 32 - 1];
   uint32_t excl = x - v + (warp > 0 ? s_warp[warp - 1] : 0u);
   __syncthreads();
   return excl;
+}
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+  return block_scan_nt<BB_FRONTIER>(v, s_warp, total);
 }
 
 // One block per heavy query: expand an ordered frontier of overlapping subtrees level by
@@ -441,13 +445,15 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
 // frontier keeps left-to-right order and each entry covers a contiguous leaf range, so the
 // concatenated walks emit ascending partners, as the single-thread traversal does.  A query
 // whose frontier does not fit the pool falls back to k_broad_heavy (hv_n = BB_NONE).
-#define BB_HV_THREADS 256  // = BB_FRONTIER, so block_excl_scan serves both kernels
-#define BB_HV_PER_THREAD 16
+// Thread t holds frontier entries [4t, 4t+4); the loads of all four (child, then child range
+// and box) are issued together, so a level costs a few load latencies whatever its size.
+#define BB_HV_THREADS 1024
+#define BB_HV_PER_THREAD 4
 #define BB_HV_FRONTIER (BB_HV_THREADS * BB_HV_PER_THREAD)
 
 __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState d, uint32_t n) {
   __shared__ int s_fr[2][BB_HV_FRONTIER];
-  __shared__ uint32_t s_warp[BB_FRONTIER / 32];
+  __shared__ uint32_t s_warp[BB_HV_THREADS / 32];
   __shared__ uint32_t s_size, s_off, s_fits;
   const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
   const int N = int(n), leaf0 = N - 1;
@@ -464,44 +470,74 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
     int cur = 0;
     for (int level = 0; level < 64; ++level) {
       const uint32_t size = s_size;
-      int kid[2 * BB_HV_PER_THREAD];
-      uint32_t c = 0;
-      bool internal = false;
+      int node[BB_HV_PER_THREAD];
+      int2 ch[BB_HV_PER_THREAD];
 #pragma unroll
       for (int e = 0; e < BB_HV_PER_THREAD; ++e) {
         const uint32_t idx = uint32_t(t) * BB_HV_PER_THREAD + e;
-        if (idx >= size) continue;
-        const int node = s_fr[cur][idx];
-        if (node >= leaf0) {
-          kid[c++] = node;  // a leaf entry stays in place
-        } else {
-          const int2 ch = d.child[node];
-          if (bp_take(d, ch.x, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.x;
-          if (bp_take(d, ch.y, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.y;
-        }
+        node[e] = idx < size ? s_fr[cur][idx] : -1;
       }
+#pragma unroll
+      for (int e = 0; e < BB_HV_PER_THREAD; ++e)
+        ch[e] = (node[e] >= 0 && node[e] < leaf0) ? d.child[node[e]] : make_int2(-1, -1);
+      // take test of both children of every internal entry; leaves stay in place
+      bool tk[2 * BB_HV_PER_THREAD];
+      uint32_t span[2 * BB_HV_PER_THREAD];
+      uint32_t c = 0;
+#pragma unroll
+      for (int e = 0; e < 2 * BB_HV_PER_THREAD; ++e) {
+        const int k = (e & 1) ? ch[e >> 1].y : ch[e >> 1].x;
+        tk[e] = false;
+        span[e] = 0;
+        if (k < 0) continue;
+        bool in_range;
+        if (k >= leaf0) {
+          in_range = (k - leaf0) > int(qi) && (k - leaf0) < wend;
+        } else {
+          const int rf = d.range_first[k], rl = d.range_last[k];
+          in_range = rl > int(qi) && rf < wend;
+          span[e] = uint32_t(rl - rf + 1);
+        }
+        tk[e] = in_range && box_overlap(qmn, qmx, d.node_box[2 * k], d.node_box[2 * k + 1]);
+      }
+#pragma unroll
+      for (int e = 0; e < BB_HV_PER_THREAD; ++e) c += node[e] >= leaf0 ? 1u : uint32_t(tk[2 * e]) + uint32_t(tk[2 * e + 1]);
       uint32_t total;
-      const uint32_t pos = block_excl_scan(c, s_warp, total);
+      uint32_t pos = block_scan_nt<BB_HV_THREADS>(c, s_warp, total);
       if (total > BB_HV_FRONTIER || total == 0) {  // uniform: keep the current frontier (or none)
         if (total == 0 && t == 0) s_size = 0;
         __syncthreads();
         break;
       }
       uint32_t work = 0;  // leaves under this thread's new internal entries
-      for (uint32_t k = 0; k < c; ++k) {
-        s_fr[cur ^ 1][pos + k] = kid[k];
-        if (kid[k] < leaf0) {
-          internal = true;
-          work += uint32_t(d.range_last[kid[k]] - d.range_first[kid[k]] + 1);
+      bool internal = false;
+#pragma unroll
+      for (int e = 0; e < BB_HV_PER_THREAD; ++e) {
+        if (node[e] >= leaf0) {
+          s_fr[cur ^ 1][pos++] = node[e];
+          continue;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (!tk[2 * e + h]) continue;
+          const int k = h ? ch[e].y : ch[e].x;
+          s_fr[cur ^ 1][pos++] = k;
+          if (k < leaf0) {
+            internal = true;
+            work += span[2 * e + h];
+          }
         }
       }
       const int more = __syncthreads_or(internal);
       cur ^= 1;
       if (t == 0) s_size = total;
       uint32_t total_work;
-      block_excl_scan(work, s_warp, total_work);  // ends with a CTA barrier
-      // enough entries for the GPU, each with a short walk left: stop expanding
-      if (!more || (total >= BB_FRONTIER && total_work <= 32u * total)) break;
+      block_scan_nt<BB_HV_THREADS>(work, s_warp, total_work);  // ends with a CTA barrier
+      // stop expanding once the entries are leaves, once a level no longer widens the
+      // frontier (a thin overlap set: walking each entry down is cheaper than a block-wide
+      // level per tree level), or once there are enough entries for the GPU, each with a
+      // short walk left
+      if (!more || total <= size || (total >= BB_FRONTIER && total_work <= 32u * total)) break;
     }
     const uint32_t size = s_size;
     if (t == 0) {
@@ -606,7 +642,8 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);
   k_broad<false><<<bb, bt, 0, s>>>(d, n);
-  k_heavy_frontier<<<hb, BB_HV_THREADS, 0, s>>>(d, n);  // one block per heavy slot
+  // two co-resident 1024-thread blocks per SM loop over the heavy slots
+  k_heavy_frontier<<<min(hb, 2u * uint32_t(sms)), BB_HV_THREADS, 0, s>>>(d, n);
   k_heavy_walk<false><<<sms * 8, 128, 0, s>>>(d, n);
   bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr, sc.scan_status + 5 * size_t(sc.scan_tiles),
                  sc.scan_tile_ctr + 5, d.ctr);

@@ -60,11 +60,26 @@ struct DevCounters {
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
                            // 7 connected components
-  uint32_t np_counts[2];   // narrow-phase work lists: box-box pairs, pairs with a sphere
+  uint32_t np_counts[3];   // narrow-phase work lists: box-box, with a sphere, with a voxel body
   uint32_t gc_list_n[2];   // edge colouring: sizes of the alternating uncoloured-manifold lists
   uint32_t hv_pool_n;      // broad phase: frontier entries of the heavy queries
-  uint32_t pad2[3];
+  uint32_t slot_count;     // worlds with voxel shapes: manifold slots (6 per voxel pair, else 1)
+  uint32_t pad2[1];
 };
+
+// Voxel shape on the device (VoxelShape, include/shared.inl:938-951) with the body-frame box
+// RigidBody::minimum = origin, maximum = hi precomputed on the host.
+struct VoxDev {
+  float ox, oy, oz, vs;   // grid origin (corner of cell 0), cell size
+  float hx, hy, hz;       // grid box maximum
+  uint32_t surf_count;
+  uint32_t dx, dy, dz;    // cells per axis
+  uint32_t occ_off;       // first word of the occupancy bits in vox_occ
+  uint32_t surf_off;      // first entry of the surface list in vox_surf
+  uint32_t pad[3];
+};
+#define BB_SHAPE_KIND(t) ((t) & 0xFFu)
+#define BB_SHAPE_VOXEL_INDEX(t) ((t) >> 8)
 
 // ---- pointers of one world's device state ------------------------------------------------
 struct DevState {
@@ -163,6 +178,17 @@ struct DevState {
   float* staging;  // host state exchange: rot 4N | pos 3N | vel 3N | omega 3N
   uint32_t pair_capacity;
   uint32_t body_capacity;
+  // voxel bodies (shape.w = BB_SHAPE_VOXEL | index << 8) and full inverse inertia
+  const VoxDev* vox;
+  const uint32_t* vox_occ;
+  const uint32_t* vox_surf;
+  uint32_t vox_on;         // the world has voxel shapes: slots are expanded per pair
+  uint32_t full_inertia;   // some body has a non-zero off-diagonal in iinv_off
+  uint32_t* slot_cnt;      // per pair: manifold slots (vox_on)
+  uint32_t* slot_off;      // per pair: first slot
+  uint32_t* slot_pair;     // per slot: pair << 3 | face code
+  uint32_t* vox_list;      // narrow-phase work list of the voxel slots
+  float4* iinv_off;        // per body: body-frame inverse inertia off-diagonal (xy, xz, yz, -)
 };
 
 // ---- small vector helpers -------------------------------------------------------------------
@@ -255,6 +281,33 @@ __device__ __forceinline__ Sym3 world_inv_inertia(Quatf q, float3 d, bool transp
   auto e = [&](int a, int b) { return M[0][a] * dd[0] * M[0][b] + M[1][a] * dd[1] * M[1][b] + M[2][a] * dd[2] * M[2][b]; };
   s.xx = e(0, 0); s.xy = e(0, 1); s.xz = e(0, 2); s.yy = e(1, 1); s.yz = e(1, 2); s.zz = e(2, 2);
   return s;
+}
+
+// Body with a full symmetric body-frame inverse inertia B (diagonal d, off-diagonal o = xy, xz,
+// yz): world = S^T B S with S as above.  Used only for bodies whose o is not zero, so boxes and
+// spheres keep the diagonal formula's bits.
+__device__ __forceinline__ Sym3 world_inv_inertia_full(Quatf q, float3 d, float3 o, bool transpose_quirk) {
+  float R[3][3];
+  q_matrix(q, R);
+  float M[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) M[i][j] = transpose_quirk ? R[i][j] : R[j][i];
+  const float B[3][3] = {{d.x, o.x, o.y}, {o.x, d.y, o.z}, {o.y, o.z, d.z}};
+  float T[3][3];  // B * M
+  for (int k = 0; k < 3; ++k)
+    for (int b = 0; b < 3; ++b) T[k][b] = B[k][0] * M[0][b] + B[k][1] * M[1][b] + B[k][2] * M[2][b];
+  auto e = [&](int a, int b) { return M[0][a] * T[0][b] + M[1][a] * T[1][b] + M[2][a] * T[2][b]; };
+  Sym3 s;
+  s.xx = e(0, 0); s.xy = e(0, 1); s.xz = e(0, 2); s.yy = e(1, 1); s.yz = e(1, 2); s.zz = e(2, 2);
+  return s;
+}
+__device__ __forceinline__ Sym3 body_world_inv_inertia(const float4* iinv, const float4* iinv_off, bool full, uint32_t i,
+                                                       Quatf q, bool tq) {
+  if (full) {
+    const float4 o = iinv_off[i];
+    if (o.x != 0.f || o.y != 0.f || o.z != 0.f) return world_inv_inertia_full(q, f3(iinv[i]), f3(o), tq);
+  }
+  return world_inv_inertia(q, f3(iinv[i]), tq);
 }
 
 __device__ __forceinline__ void raise_error(DevCounters* c, uint32_t bit) { atomicOr(&c->error_flags, bit); }

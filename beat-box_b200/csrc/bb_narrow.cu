@@ -381,29 +381,58 @@ __device__ __forceinline__ uint32_t warm_inc(uint32_t w) { return min(255u, w + 
 
 }  // namespace
 
-// Work lists of the narrow phase: box-box pairs from the front of np_list, pairs with a sphere
-// from the back, static-static pairs (:1525) nowhere.  Every slot starts as "no manifold".
-// Grouping by shape keeps the warps of k_narrow on one code path (the box-box clip is long,
-// the sphere cases short); the outputs go to each pair's own slot, so the order in which the
-// lists fill does not matter.
-__global__ void k_np_classify(const DevState d, int cur) {
+// Manifold slots.  Without voxel shapes a pair owns one slot (slot = pair).  In a world with
+// voxel shapes every pair with a voxel body owns six consecutive slots, one per face direction
+// (code 0..5, key 90 + code), the others one: a scan over the pairs places them, so slot order
+// = (pair, code), which is the manifold order.
+__device__ __forceinline__ uint32_t slot_total(const DevState& d) {
+  return d.vox_on ? min(d.ctr->slot_count, d.pair_capacity) : min(d.ctr->pair_count, d.pair_capacity);
+}
+__device__ __forceinline__ uint32_t slot_pair_of(const DevState& d, uint32_t s) { return d.vox_on ? d.slot_pair[s] >> 3 : s; }
+__device__ __forceinline__ bool pair_has_voxel(const DevState& d, uint32_t k) {
+  const uint2 pr = d.pairs[k];
+  const uint32_t ta = __float_as_uint(d.shape[d.vals[0][pr.x]].w), tb = __float_as_uint(d.shape[d.vals[0][pr.y]].w);
+  return BB_SHAPE_KIND(ta) == BB_SHAPE_VOXEL || BB_SHAPE_KIND(tb) == BB_SHAPE_VOXEL;
+}
+__global__ void k_slot_count(const DevState d) {
   const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x)
+    d.slot_cnt[k] = pair_has_voxel(d, k) ? 6u : 1u;
+}
+__global__ void k_slot_fill(const DevState d) {
+  const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x) {
+    const uint32_t off = d.slot_off[k], c = d.slot_cnt[k];
+    for (uint32_t j = 0; j < c; ++j) {
+      if (off + j < d.pair_capacity) d.slot_pair[off + j] = (k << 3) | j;
+      else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+    }
+  }
+}
+
+// Work lists of the narrow phase: box-box slots from the front of np_list, slots with a sphere
+// from the back, voxel slots in vox_list, static-static pairs (:1525) nowhere.  Every slot
+// starts as "no manifold".  Grouping by shape keeps the warps of k_narrow on one code path
+// (the box-box clip is long, the sphere cases short); the outputs go to each slot's own place,
+// so the order in which the lists fill does not matter.
+__global__ void k_np_classify(const DevState d, int cur) {
+  const uint32_t S = slot_total(d);
   const int lane = threadIdx.x & 31;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < P; base += gridDim.x * blockDim.x) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < S; base += gridDim.x * blockDim.x) {
     const uint32_t k = base + threadIdx.x;
-    int kind = -1;  // 0 box-box, 1 with a sphere
-    if (k < P) {
+    int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body
+    if (k < S) {
       d.hit[k] = 0;
       d.m_keycc[cur][k] = make_int2(-1, 0);
-      const uint2 pr = d.pairs[k];
+      const uint2 pr = d.pairs[slot_pair_of(d, k)];
       const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
       if ((d.flags[ida] & BB_BODY_DYNAMIC) || (d.flags[idb] & BB_BODY_DYNAMIC)) {
-        const uint32_t ta = __float_as_uint(d.shape[ida].w), tb = __float_as_uint(d.shape[idb].w);
-        kind = (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1;
+        const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
+        kind = (ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL) ? 2 : ((ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1);
       }
     }
 #pragma unroll
-    for (int kd = 0; kd < 2; ++kd) {
+    for (int kd = 0; kd < 3; ++kd) {
       const unsigned mask = __ballot_sync(0xFFFFFFFFu, kind == kd);
       if (!mask) continue;
       uint32_t off = 0;
@@ -411,20 +440,165 @@ __global__ void k_np_classify(const DevState d, int cur) {
       off = __shfl_sync(0xFFFFFFFFu, off, 0);
       if (kind == kd) {
         const uint32_t r = off + uint32_t(__popc(mask & ((1u << lane) - 1u)));
-        d.np_list[kd == 0 ? r : P - 1 - r] = k;
+        if (kd == 2) d.vox_list[r] = k;
+        else d.np_list[kd == 0 ? r : S - 1 - r] = k;
       }
     }
   }
 }
 
+// Basis, warm start from the previous substep (Manifold::update_from_old,
+// extensions.slang:306-473, after find_old_collision, collision_detection.slang:914-963) and
+// the write of slot k.  Voxel manifolds (vox) inherit only from the old manifold of the same
+// key in the same body order, match features by the whole voxel/corner id, and keep their
+// own depth caps; other manifolds take the pair's old manifold under any key, either order.
+__device__ __forceinline__ void np_store(const DevState& d, const Params& p, int cur, int warm, uint32_t k,
+                                         uint32_t ida, uint32_t idb, uint32_t fa, float3 pa, float3 pb,
+                                         const Contacts& m, bool vox) {
+  const int prv = cur ^ 1;
+  // compute_basis (extensions.slang:262-272)
+  float3 n = m.normal, t0;
+  if (fabsf(n.x) > fabsf(n.y)) t0 = make_float3(n.z, 0.f, -n.x);
+  else t0 = make_float3(0.f, -n.z, n.y);
+  t0 = t0 * (1.0f / len3(t0));
+  float3 t1 = cross3(t0, n);
+  // new contacts; inherited fields start at zero
+  float3 cpos[BB_MAX_CONTACTS];
+  float cpen[BB_MAX_CONTACTS];
+  uint32_t cfp[BB_MAX_CONTACTS], cwarm[BB_MAX_CONTACTS], cstick[BB_MAX_CONTACTS];
+  float4 clam[BB_MAX_CONTACTS];
+  float2 ckt[BB_MAX_CONTACTS];
+  float3 canca[BB_MAX_CONTACTS], cancb[BB_MAX_CONTACTS];
+  const int cc = m.cc;
+  for (int c = 0; c < cc; ++c) {
+    cpos[c] = m.pos[c];
+    cpen[c] = vox ? m.pen[c] : fmaxf(m.pen[c], p.penetration_cap);  // extraction cap (:1575-1578)
+    cfp[c] = m.fp[c];
+    cwarm[c] = 0;
+    cstick[c] = 0;
+    clam[c] = make_float4(0, 0, 0, 0);
+    ckt[c] = make_float2(0, 0);
+    canca[c] = make_float3(0, 0, 0);
+    cancb[c] = make_float3(0, 0, 0);
+  }
+  int32_t err = 0x7FFFFFFF;
+  if (warm) {
+    // find the pair's manifold of the previous substep on the dynamic body's list
+    uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb;
+    const uint32_t other = x == ida ? idb : ida;
+    uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
+    uint32_t old_slot = BB_NONE;
+    bool swapped = false;
+    for (uint32_t e = s0; e < s1; ++e) {
+      if (d.csr_partner[prv][e] != other) continue;
+      const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
+      if (vox && (d.m_keycc[prv][os].x != m.key || d.m_bodies[prv][os].x != ida)) continue;
+      old_slot = os;
+      swapped = d.m_bodies[prv][os].x != ida;
+      break;
+    }
+    if (old_slot != BB_NONE) {
+      // Manifold::update_from_old (extensions.slang:306-473)
+      int2 okc = d.m_keycc[prv][old_slot];
+      float4 on4 = d.m_normal[prv][old_slot];
+      float sgn = swapped ? -1.f : 1.f;
+      bool cross_key = m.key != okc.x || swapped;
+      bool go = !cross_key || dot3(n, f3(on4) * sgn) > 0.7f;
+      if (go) {
+        const int occ = okc.y;
+        uint32_t used_old = 0, matched_new = 0;
+        const uint32_t ob = old_slot * BB_MAX_CONTACTS;
+        if (!cross_key) {
+          for (int i = 0; i < cc; ++i) {
+            for (int j = 0; j < occ; ++j) {
+              if (used_old & (1u << j)) continue;
+              float4 op = d.c_pos[prv][ob + j];
+              uint32_t ofp = __float_as_uint(d.c_anc_a[prv][ob + j].w);
+              bool feat = vox ? ofp == cfp[i]
+                              : (fp_in_inc(ofp) == fp_in_inc(cfp[i]) && fp_out_inc(ofp) == fp_out_inc(cfp[i]));
+              float3 dp = f3(op) - cpos[i];
+              bool close = dot3(dp, dp) < 0.1f * 0.1f;
+              if (feat && close) {
+                float4 ol = d.c_lam[prv][ob + j];
+                float4 okt = d.c_kt[prv][ob + j];
+                clam[i] = ol;
+                ckt[i] = make_float2(okt.x, okt.y);
+                cstick[i] = __float_as_uint(okt.z);
+                if (cstick[i] != 0) {
+                  canca[i] = f3(d.c_anc_a[prv][ob + j]);
+                  cancb[i] = f3(d.c_anc_b[prv][ob + j]);
+                }
+                float3 d2 = cpos[i] - f3(op);
+                if (dot3(d2, d2) < 0.01f) cpos[i] = f3(op);
+                cwarm[i] = warm_inc(__float_as_uint(okt.w));
+                used_old |= 1u << j;
+                matched_new |= 1u << i;
+                break;
+              }
+            }
+          }
+        }
+        for (int round = 0; round < cc; ++round) {
+          float best = 0.1225f;
+          int bi = -1, bj = -1;
+          for (int i = 0; i < cc; ++i) {
+            if (matched_new & (1u << i)) continue;
+            for (int j = 0; j < occ; ++j) {
+              if (used_old & (1u << j)) continue;
+              float3 dp = cpos[i] - f3(d.c_pos[prv][ob + j]);
+              float d2 = dot3(dp, dp);
+              if (d2 < best) { best = d2; bi = i; bj = j; }
+            }
+          }
+          if (bi < 0) break;
+          float4 ol = d.c_lam[prv][ob + bj];
+          float4 okt = d.c_kt[prv][ob + bj];
+          clam[bi] = make_float4(ol.x, ol.y * sgn, ol.z, ol.w);
+          ckt[bi] = make_float2(okt.x, okt.y);
+          cstick[bi] = __float_as_uint(okt.z);
+          float4 oaa = d.c_anc_a[prv][ob + bj];
+          if (cstick[bi] != 0) {
+            float3 aa = f3(oaa), ab = f3(d.c_anc_b[prv][ob + bj]);
+            canca[bi] = swapped ? ab : aa;
+            cancb[bi] = swapped ? aa : ab;
+          }
+          cfp[bi] = __float_as_uint(oaa.w);
+          cwarm[bi] = warm_inc(__float_as_uint(okt.w));
+          matched_new |= 1u << bi;
+          used_old |= 1u << bj;
+        }
+        float deep_new = 0.f, deep_old = 0.f;
+        for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, cpen[i]);
+        for (int j = 0; j < occ; ++j) deep_old = fminf(deep_old, d.c_pos[prv][ob + j].w);
+        err = int32_t(fminf(fmaxf((deep_new - deep_old) * 10000.0f, -32000.0f), 32000.0f));
+      }
+    }
+  }
+  d.m_bodies[cur][k] = make_uint2(ida, idb);
+  d.m_keycc[cur][k] = make_int2(m.key, cc);
+  d.m_normal[cur][k] = f4(n, __int_as_float(err));
+  d.m_t0[cur][k] = f4(t0, 0.f);
+  d.m_t1[cur][k] = f4(t1, 0.f);
+  d.m_anchor_a[cur][k] = make_float4(pa.x, pa.y, pa.z, 0.f);
+  d.m_anchor_b[cur][k] = make_float4(pb.x, pb.y, pb.z, 0.f);
+  const uint32_t cb = k * BB_MAX_CONTACTS;
+  for (int c = 0; c < cc; ++c) {
+    d.c_pos[cur][cb + c] = f4(cpos[c], cpen[c]);
+    d.c_lam[cur][cb + c] = clam[c];
+    d.c_kt[cur][cb + c] = make_float4(ckt[c].x, ckt[c].y, __uint_as_float(cstick[c]), __uint_as_float(cwarm[c]));
+    d.c_anc_a[cur][cb + c] = f4(canca[c], __uint_as_float(cfp[c]));
+    d.c_anc_b[cur][cb + c] = f4(cancb[c], 0.f);
+  }
+  d.hit[k] = 1;
+}
+
 // Narrow phase + warm start: one thread per listed pair.
 __global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int cur, int warm) {
-  const int prv = cur ^ 1;
-  const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
+  const uint32_t S = slot_total(d);
   const uint32_t nbb = d.ctr->np_counts[0], ntot = nbb + d.ctr->np_counts[1];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += gridDim.x * blockDim.x) {
-    const uint32_t k = d.np_list[t < nbb ? t : P - 1 - (t - nbb)];
-    uint2 pr = d.pairs[k];
+    const uint32_t k = d.np_list[t < nbb ? t : S - 1 - (t - nbb)];
+    uint2 pr = d.pairs[slot_pair_of(d, k)];
     uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
     const uint32_t fa = d.flags[ida];
     float4 pa4 = d.pos[ida], pb4 = d.pos[idb];
@@ -458,145 +632,361 @@ __global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int 
       }
     }
     if (!hit) continue;
-    // compute_basis (extensions.slang:262-272)
-    float3 n = m.normal, t0;
-    if (fabsf(n.x) > fabsf(n.y)) t0 = make_float3(n.z, 0.f, -n.x);
-    else t0 = make_float3(0.f, -n.z, n.y);
-    t0 = t0 * (1.0f / len3(t0));
-    float3 t1 = cross3(t0, n);
-    // new contacts; inherited fields start at zero
-    float3 cpos[BB_MAX_CONTACTS];
-    float cpen[BB_MAX_CONTACTS];
-    uint32_t cfp[BB_MAX_CONTACTS], cwarm[BB_MAX_CONTACTS], cstick[BB_MAX_CONTACTS];
-    float4 clam[BB_MAX_CONTACTS];
-    float2 ckt[BB_MAX_CONTACTS];
-    float3 canca[BB_MAX_CONTACTS], cancb[BB_MAX_CONTACTS];
-    const int cc = m.cc;
-    for (int c = 0; c < cc; ++c) {
-      cpos[c] = m.pos[c];
-      cpen[c] = fmaxf(m.pen[c], p.penetration_cap);  // extraction cap (:1575-1578)
-      cfp[c] = m.fp[c];
-      cwarm[c] = 0;
-      cstick[c] = 0;
-      clam[c] = make_float4(0, 0, 0, 0);
-      ckt[c] = make_float2(0, 0);
-      canca[c] = make_float3(0, 0, 0);
-      cancb[c] = make_float3(0, 0, 0);
+    np_store(d, p, cur, warm, k, ida, idb, fa, pa, pb, m, false);
+  }
+}
+
+// ---- voxel bodies (collision_detection.slang:1001-1512) -----------------------------------------
+// One warp per voxel slot (pair, face code).  The lanes split the sampled body's surface cells;
+// each lane keeps the four extreme-direction winners of its own samples, and a warp reduction
+// picks the winners under the reducer's ranking (score bucket, then depth bucket, then voxel
+// id: a strict total order, since voxel ids are unique in a surface list), so the manifold does
+// not depend on how the samples were split.  Lane 0 then builds the contacts and stores the
+// slot as k_narrow does.
+struct VBody {
+  float3 p;
+  float R[3][3];  // rotation: world = R * local
+  uint32_t kind, vi;
+  float3 lo, hi;  // body-frame box [minimum, maximum]
+};
+__device__ __forceinline__ void vbody(const DevState& d, uint32_t id, VBody& b) {
+  b.p = f3(d.pos[id]);
+  q_matrix(q_from(d.rot[id]), b.R);
+  const float4 s = d.shape[id];
+  const uint32_t t = __float_as_uint(s.w);
+  b.kind = BB_SHAPE_KIND(t);
+  b.vi = BB_SHAPE_VOXEL_INDEX(t);
+  if (b.kind == BB_SHAPE_VOXEL) {
+    const VoxDev& v = d.vox[b.vi];
+    b.lo = make_float3(v.ox, v.oy, v.oz);
+    b.hi = make_float3(v.hx, v.hy, v.hz);
+  } else if (b.kind == BB_SHAPE_SPHERE) {  // read as its bounding cube, as the reference reads any non-voxel body
+    b.lo = make_float3(-s.x, -s.x, -s.x);
+    b.hi = make_float3(s.x, s.x, s.x);
+  } else {
+    b.lo = make_float3(-s.x, -s.y, -s.z);
+    b.hi = make_float3(s.x, s.y, s.z);
+  }
+}
+__device__ __forceinline__ float3 mat_mul(const float R[3][3], float3 v) {
+  return make_float3(R[0][0] * v.x + R[0][1] * v.y + R[0][2] * v.z, R[1][0] * v.x + R[1][1] * v.y + R[1][2] * v.z,
+                     R[2][0] * v.x + R[2][1] * v.y + R[2][2] * v.z);
+}
+__device__ __forceinline__ float3 mat_tmul(const float R[3][3], float3 v) {  // R^T v
+  return make_float3(R[0][0] * v.x + R[1][0] * v.y + R[2][0] * v.z, R[0][1] * v.x + R[1][1] * v.y + R[2][1] * v.z,
+                     R[0][2] * v.x + R[1][2] * v.y + R[2][2] * v.z);
+}
+__device__ __forceinline__ float3 mat_col(const float R[3][3], int k) { return make_float3(R[0][k], R[1][k], R[2][k]); }
+__device__ __forceinline__ float3 axis_vec(uint32_t k, float s) {
+  return make_float3(k == 0 ? s : 0.f, k == 1 ? s : 0.f, k == 2 ? s : 0.f);
+}
+__device__ __forceinline__ bool vox_bit(const DevState& d, const VoxDev& v, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0 || x >= int(v.dx) || y >= int(v.dy) || z >= int(v.dz)) return false;
+  const uint32_t b = uint32_t(x) + uint32_t(y) * v.dx + uint32_t(z) * v.dx * v.dy;
+  return ((__ldg(&d.vox_occ[v.occ_off + b / 32u]) >> (b % 32u)) & 1u) != 0u;
+}
+__device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
+  return uint32_t(x & 0xFF) | (uint32_t(y & 0xFF) << 8) | (uint32_t(z & 0xFF) << 16);
+}
+
+// voxel_obb_prefilter (:1276-1298): face-axis separation of the two boxes, 1 cm margin
+__device__ bool vox_prefilter(const VBody& a, const VBody& b) {
+  const float3 ha = (a.hi - a.lo) * 0.5f, hb = (b.hi - b.lo) * 0.5f;
+  const float3 ca = a.p + mat_mul(a.R, (a.hi + a.lo) * 0.5f), cb = b.p + mat_mul(b.R, (b.hi + b.lo) * 0.5f);
+  const float3 dd = cb - ca;
+  const float haa[3] = {ha.x, ha.y, ha.z}, hbb[3] = {hb.x, hb.y, hb.z};
+  for (int i = 0; i < 3; ++i) {
+    const float3 ai = mat_col(a.R, i), bi = mat_col(b.R, i);
+    const float rb = hbb[0] * fabsf(dot3(ai, mat_col(b.R, 0))) + hbb[1] * fabsf(dot3(ai, mat_col(b.R, 1))) +
+                     hbb[2] * fabsf(dot3(ai, mat_col(b.R, 2)));
+    if (fabsf(dot3(dd, ai)) > haa[i] + rb + 0.01f) return false;
+    const float ra = haa[0] * fabsf(dot3(bi, mat_col(a.R, 0))) + haa[1] * fabsf(dot3(bi, mat_col(a.R, 1))) +
+                     haa[2] * fabsf(dot3(bi, mat_col(a.R, 2)));
+    if (fabsf(dot3(dd, bi)) > hbb[i] + ra + 0.01f) return false;
+  }
+  return true;
+}
+
+// voxel_corner_supported (:1305-1324)
+__device__ bool vox_corner_supported(const DevState& d, float3 pt, float3 n_sep, const VBody& r2, bool s2_vox, uint32_t axk) {
+  if (s2_vox) {
+    const VoxDev& v = d.vox[r2.vi];
+    const float3 l2 = mat_tmul(r2.R, (pt - n_sep * (0.3f * v.vs)) - r2.p);
+    const float3 g = make_float3((l2.x - v.ox) / v.vs, (l2.y - v.oy) / v.vs, (l2.z - v.oz) / v.vs);
+    return vox_bit(d, v, int(floorf(g.x)), int(floorf(g.y)), int(floorf(g.z)));
+  }
+  const float3 half = (r2.hi - r2.lo) * 0.5f, co = (r2.hi + r2.lo) * 0.5f;
+  const float3 l2 = mat_tmul(r2.R, pt - r2.p) - co;
+  const float lu = axk == 0 ? l2.y : l2.x, lv = axk == 2 ? l2.y : l2.z;
+  const float hu = axk == 0 ? half.y : half.x, hv = axk == 2 ? half.y : half.z;
+  return fabsf(lu) <= hu + 0.01f && fabsf(lv) <= hv + 0.01f;
+}
+
+struct VWin {  // one reducer slot
+  float3 pos, nrm;
+  float pen, score;
+  uint32_t fa, fb;
+};
+// rank of a slot's sample: (score bucket desc, depth bucket asc, voxel id asc); empty ranks last
+__device__ __forceinline__ bool vwin_better(bool ea, int sa, int pa, uint32_t fa, bool eb, int sb, int pb, uint32_t fb) {
+  if (ea) return false;
+  if (eb) return true;
+  return sa > sb || (sa == sb && (pa < pb || (pa == pb && fa < fb)));
+}
+
+__global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p, int cur, int warm) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nv = d.ctr->np_counts[2];
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < nv; t += warps) {
+    const uint32_t slot = d.vox_list[t];
+    const uint32_t sp = d.slot_pair[slot];
+    const uint32_t code = sp & 7u;
+    const uint2 pr = d.pairs[sp >> 3];
+    const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
+    VBody A, B;
+    vbody(d, ida, A);
+    vbody(d, idb, B);
+    if (!vox_prefilter(A, B)) continue;  // warp-uniform
+    const bool a_vox = A.kind == BB_SHAPE_VOXEL, b_vox = B.kind == BB_SHAPE_VOXEL;
+    const uint32_t sa_n = a_vox ? d.vox[A.vi].surf_count : 0u, sb_n = b_vox ? d.vox[B.vi].surf_count : 0u;
+    const bool flip = !a_vox || (b_vox && sb_n < sa_n);  // sampled body = B
+    const VBody& r1 = flip ? B : A;
+    const VBody& r2 = flip ? A : B;
+    const bool s2_vox = flip ? a_vox : b_vox;
+    const VoxDev s1 = d.vox[r1.vi];
+    VoxDev s2 = {};
+    if (s2_vox) s2 = d.vox[r2.vi];
+    const float vs1 = s1.vs;
+    // per-axis support radius of a rotated sample cell in r2's frame (:1110-1117)
+    float A12[3][3];  // r2^T r1
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) A12[i][j] = r2.R[0][i] * r1.R[0][j] + r2.R[1][i] * r1.R[1][j] + r2.R[2][i] * r1.R[2][j];
+    const float3 sup = make_float3(fabsf(A12[0][0]) + fabsf(A12[0][1]) + fabsf(A12[0][2]),
+                                   fabsf(A12[1][0]) + fabsf(A12[1][1]) + fabsf(A12[1][2]),
+                                   fabsf(A12[2][0]) + fabsf(A12[2][1]) + fabsf(A12[2][2])) * (0.5f * vs1);
+    const uint32_t axk = code >> 1;
+    const float sgn = (code & 1u) ? 1.f : -1.f;
+    const int isgn = (code & 1u) ? 1 : -1;
+    const float sup_a = comp(sup, int(axk));
+    const float3 half2 = (r2.hi - r2.lo) * 0.5f, co2 = (r2.hi + r2.lo) * 0.5f;
+    const float3 org2 = make_float3(s2.ox, s2.oy, s2.oz);
+    const float vs2 = s2.vs;
+    const float quant = 0.5f * vs1;
+    const float3 n_out = mat_col(r2.R, int(axk)) * sgn;  // the pass's face normal, world frame
+    VWin w[4];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      w[o].pen = 1.0e9f;
+      w[o].score = -1.0e30f;
+      w[o].fa = 0;
+      w[o].fb = 0;
+      w[o].pos = make_float3(0, 0, 0);
+      w[o].nrm = make_float3(0, 0, 0);
     }
-    int32_t err = 0x7FFFFFFF;
-    if (warm) {
-      // find the pair's manifold of the previous substep on the dynamic body's list
-      uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb;
-      const uint32_t other = x == ida ? idb : ida;
-      uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
-      uint32_t old_slot = BB_NONE;
-      bool swapped = false;
-      for (uint32_t e = s0; e < s1; ++e) {
-        if (d.csr_partner[prv][e] != other) continue;
-        const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
-        old_slot = os;
-        swapped = d.m_bodies[prv][os].x != ida;
-        break;
+    uint32_t samples = 0, interior = 0;
+    for (uint32_t i = lane; i < s1.surf_count; i += 32u) {
+      const uint32_t e = __ldg(&d.vox_surf[s1.surf_off + i]);
+      const float3 local = make_float3(s1.ox + (float(e & 0xFFu) + 0.5f) * vs1, s1.oy + (float((e >> 8) & 0xFFu) + 0.5f) * vs1,
+                                       s1.oz + (float((e >> 16) & 0xFFu) + 0.5f) * vs1);
+      const float3 pw = r1.p + mat_mul(r1.R, local);
+      const float3 l2w = mat_tmul(r2.R, pw - r2.p);
+      float pe, su, sv;
+      uint32_t fb;
+      if (s2_vox) {
+        const float3 l2 = l2w;
+        su = axk == 0 ? l2.y : l2.x;
+        sv = axk == 2 ? l2.y : l2.z;
+        const float3 g = make_float3((l2.x - org2.x) / vs2, (l2.y - org2.y) / vs2, (l2.z - org2.z) / vs2);
+        int c[3] = {int(floorf(g.x)), int(floorf(g.y)), int(floorf(g.z))};
+        if (!vox_bit(d, s2, c[0], c[1], c[2])) {
+          // hover band: centre in an empty cell just outside an occupied one (:1155-1183)
+          int ci[3] = {c[0], c[1], c[2]};
+          ci[axk] -= isgn;
+          if (!vox_bit(d, s2, ci[0], ci[1], ci[2])) continue;
+          const float dh = comp(l2, int(axk)) - (comp(org2, int(axk)) + (float(ci[axk]) + 0.5f) * vs2);
+          const float ovh = (0.5f * vs2 + sup_a) - sgn * dh;
+          pe = -ovh;
+          fb = pack_cell(ci[0], ci[1], ci[2]);
+        } else {
+          // cell-face contact (:1185-1222)
+          const float3 dl = l2 - (org2 + (make_float3(float(c[0]), float(c[1]), float(c[2])) + make_float3(0.5f, 0.5f, 0.5f)) * vs2);
+          float best = 1e9f;
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax) {
+            const float di = comp(dl, ax);
+            int nb[3] = {c[0], c[1], c[2]};
+            nb[ax] += di >= 0.f ? 1 : -1;
+            if (vox_bit(d, s2, nb[0], nb[1], nb[2])) continue;
+            const float ov = (0.5f * vs2 + comp(sup, ax)) - fabsf(di);
+            if (ov < best) best = ov;
+          }
+          if (best > 0.5e9f) {
+            ++interior;
+            continue;
+          }
+          int pn[3] = {c[0], c[1], c[2]};
+          pn[axk] += isgn;
+          if (vox_bit(d, s2, pn[0], pn[1], pn[2])) continue;
+          const float ovp = (0.5f * vs2 + sup_a) - sgn * comp(dl, int(axk));
+          if (ovp > best + 0.15f * vs2) continue;
+          pe = -ovp;
+          fb = pack_cell(c[0], c[1], c[2]);
+        }
+      } else {
+        // r2 is a box: sample centre with support radius against the box faces (:1235-1258)
+        const float3 l2 = l2w - co2;
+        su = axk == 0 ? l2.y : l2.x;
+        sv = axk == 2 ? l2.y : l2.z;
+        const float3 q = make_float3(fabsf(l2.x) - half2.x, fabsf(l2.y) - half2.y, fabsf(l2.z) - half2.z);
+        if (q.x > sup.x || q.y > sup.y || q.z > sup.z) continue;
+        const float3 qs = q - sup;
+        const float best_q = fmaxf(qs.x, fmaxf(qs.y, qs.z));
+        const float q_pass = sgn * comp(l2, int(axk)) - comp(half2, int(axk)) - sup_a;
+        if (q_pass < best_q - 0.15f * vs1) continue;
+        pe = q_pass;
+        fb = axk;
       }
-      if (old_slot != BB_NONE) {
-        // Manifold::update_from_old (extensions.slang:306-473)
-        int2 okc = d.m_keycc[prv][old_slot];
-        float4 on4 = d.m_normal[prv][old_slot];
-        float sgn = swapped ? -1.f : 1.f;
-        bool cross_key = m.key != okc.x || swapped;
-        bool go = !cross_key || dot3(n, f3(on4) * sgn) > 0.7f;
-        if (go) {
-          const int occ = okc.y;
-          uint32_t used_old = 0, matched_new = 0;
-          const uint32_t ob = old_slot * BB_MAX_CONTACTS;
-          if (!cross_key) {
-            for (int i = 0; i < cc; ++i) {
-              for (int j = 0; j < occ; ++j) {
-                if (used_old & (1u << j)) continue;
-                float4 op = d.c_pos[prv][ob + j];
-                uint32_t ofp = __float_as_uint(d.c_anc_a[prv][ob + j].w);
-                bool feat = fp_in_inc(ofp) == fp_in_inc(cfp[i]) && fp_out_inc(ofp) == fp_out_inc(cfp[i]);
-                float3 dp = f3(op) - cpos[i];
-                bool close = dot3(dp, dp) < 0.1f * 0.1f;
-                if (feat && close) {
-                  float4 ol = d.c_lam[prv][ob + j];
-                  float4 okt = d.c_kt[prv][ob + j];
-                  clam[i] = ol;
-                  ckt[i] = make_float2(okt.x, okt.y);
-                  cstick[i] = __float_as_uint(okt.z);
-                  if (cstick[i] != 0) {
-                    canca[i] = f3(d.c_anc_a[prv][ob + j]);
-                    cancb[i] = f3(d.c_anc_b[prv][ob + j]);
-                  }
-                  float3 d2 = cpos[i] - f3(op);
-                  if (dot3(d2, d2) < 0.01f) cpos[i] = f3(op);
-                  cwarm[i] = warm_inc(__float_as_uint(okt.w));
-                  used_old |= 1u << j;
-                  matched_new |= 1u << i;
-                  break;
-                }
-              }
-            }
-          }
-          for (int round = 0; round < cc; ++round) {
-            float best = 0.1225f;
-            int bi = -1, bj = -1;
-            for (int i = 0; i < cc; ++i) {
-              if (matched_new & (1u << i)) continue;
-              for (int j = 0; j < occ; ++j) {
-                if (used_old & (1u << j)) continue;
-                float3 dp = cpos[i] - f3(d.c_pos[prv][ob + j]);
-                float d2 = dot3(dp, dp);
-                if (d2 < best) { best = d2; bi = i; bj = j; }
-              }
-            }
-            if (bi < 0) break;
-            float4 ol = d.c_lam[prv][ob + bj];
-            float4 okt = d.c_kt[prv][ob + bj];
-            clam[bi] = make_float4(ol.x, ol.y * sgn, ol.z, ol.w);
-            ckt[bi] = make_float2(okt.x, okt.y);
-            cstick[bi] = __float_as_uint(okt.z);
-            float4 oaa = d.c_anc_a[prv][ob + bj];
-            if (cstick[bi] != 0) {
-              float3 aa = f3(oaa), ab = f3(d.c_anc_b[prv][ob + bj]);
-              canca[bi] = swapped ? ab : aa;
-              cancb[bi] = swapped ? aa : ab;
-            }
-            cfp[bi] = __float_as_uint(oaa.w);
-            cwarm[bi] = warm_inc(__float_as_uint(okt.w));
-            matched_new |= 1u << bi;
-            used_old |= 1u << bj;
-          }
-          float deep_new = 0.f, deep_old = 0.f;
-          for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, cpen[i]);
-          for (int j = 0; j < occ; ++j) deep_old = fminf(deep_old, d.c_pos[prv][ob + j].w);
-          err = int32_t(fminf(fmaxf((deep_new - deep_old) * 10000.0f, -32000.0f), 32000.0f));
+      if (pe >= 0.02f) continue;  // margin band
+      pe = fmaxf(pe, s2_vox ? -0.5f * vs1 : -vs1);  // depth caps (:1262-1266)
+      // VoxelManifoldReducer::add (:1064-1092)
+      const float sc4[4] = {su + sv, su - sv, -su + sv, -su - sv};
+      const int nbk = int(floorf(pe / quant));
+      const uint32_t fa = e & 0xFFFFFFu;
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        const bool empty = w[o].pen > 0.5e9f;
+        const int nbs = int(floorf(sc4[o] / quant));
+        const int obs = empty ? -2147483640 : int(floorf(w[o].score / quant));
+        const int obk = empty ? 0 : int(floorf(w[o].pen / quant));
+        if (empty || nbs > obs || (nbs == obs && (nbk < obk || (nbk == obk && fa < w[o].fa)))) {
+          w[o].pos = pw;
+          w[o].pen = pe;
+          w[o].nrm = n_out;
+          w[o].fa = fa;
+          w[o].fb = fb;
+          w[o].score = sc4[o];
         }
       }
+      ++samples;
     }
-    d.m_bodies[cur][k] = make_uint2(ida, idb);
-    d.m_keycc[cur][k] = make_int2(m.key, cc);
-    d.m_normal[cur][k] = f4(n, __int_as_float(err));
-    d.m_t0[cur][k] = f4(t0, 0.f);
-    d.m_t1[cur][k] = f4(t1, 0.f);
-    d.m_anchor_a[cur][k] = make_float4(pa.x, pa.y, pa.z, 0.f);
-    d.m_anchor_b[cur][k] = make_float4(pb.x, pb.y, pb.z, 0.f);
-    const uint32_t cb = k * BB_MAX_CONTACTS;
-    for (int c = 0; c < cc; ++c) {
-      d.c_pos[cur][cb + c] = f4(cpos[c], cpen[c]);
-      d.c_lam[cur][cb + c] = clam[c];
-      d.c_kt[cur][cb + c] = make_float4(ckt[c].x, ckt[c].y, __uint_as_float(cstick[c]), __uint_as_float(cwarm[c]));
-      d.c_anc_a[cur][cb + c] = f4(canca[c], __uint_as_float(cfp[c]));
-      d.c_anc_b[cur][cb + c] = f4(cancb[c], 0.f);
+    samples = __reduce_add_sync(0xFFFFFFFFu, samples);
+    interior = __reduce_add_sync(0xFFFFFFFFu, interior);
+    // per reducer slot: the best lane's winner
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      bool em = w[o].pen > 0.5e9f;
+      int sb = em ? 0 : int(floorf(w[o].score / quant));
+      int pb = em ? 0 : int(floorf(w[o].pen / quant));
+      uint32_t fa = w[o].fa, src = lane;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const bool oe = __shfl_xor_sync(0xFFFFFFFFu, em, off);
+        const int os = __shfl_xor_sync(0xFFFFFFFFu, sb, off);
+        const int op = __shfl_xor_sync(0xFFFFFFFFu, pb, off);
+        const uint32_t of = __shfl_xor_sync(0xFFFFFFFFu, fa, off);
+        const uint32_t osrc = __shfl_xor_sync(0xFFFFFFFFu, src, off);
+        if (vwin_better(oe, os, op, of, em, sb, pb, fa)) {
+          em = oe;
+          sb = os;
+          pb = op;
+          fa = of;
+          src = osrc;
+        }
+      }
+      w[o].pos.x = __shfl_sync(0xFFFFFFFFu, w[o].pos.x, src);
+      w[o].pos.y = __shfl_sync(0xFFFFFFFFu, w[o].pos.y, src);
+      w[o].pos.z = __shfl_sync(0xFFFFFFFFu, w[o].pos.z, src);
+      w[o].nrm.x = __shfl_sync(0xFFFFFFFFu, w[o].nrm.x, src);
+      w[o].nrm.y = __shfl_sync(0xFFFFFFFFu, w[o].nrm.y, src);
+      w[o].nrm.z = __shfl_sync(0xFFFFFFFFu, w[o].nrm.z, src);
+      w[o].pen = __shfl_sync(0xFFFFFFFFu, w[o].pen, src);
+      w[o].score = __shfl_sync(0xFFFFFFFFu, w[o].score, src);
+      w[o].fa = __shfl_sync(0xFFFFFFFFu, w[o].fa, src);
+      w[o].fb = __shfl_sync(0xFFFFFFFFu, w[o].fb, src);
     }
-    d.hit[k] = 1;
+    if (lane == 0) {  // the manifold and its store: serial, small
+      bool store = true;
+      Contacts m;
+      m.cc = 0;
+      m.key = 90 + int(code);
+      if (samples == 0) {
+        store = code == 0 && interior > 0;
+        // deep-interpenetration rescue (:1487-1506): one centre-to-centre contact
+        const float3 dd = r1.p - r2.p;
+        const float3 n_res = dot3(dd, dd) > 1e-8f ? dd * (1.0f / len3(dd)) : make_float3(0.f, 1.f, 0.f);
+        m.normal = flip ? n_res : -n_res;
+        m.pos[0] = (r1.p + r2.p) * 0.5f;
+        m.pen[0] = -0.5f * vs1;
+        m.fp[0] = 0xFFFFFFu;
+        m.cc = 1;
+      } else {
+        // voxel_emit_manifold (:1330-1448)
+        const float3 n_sep = n_out;
+        m.normal = flip ? n_sep : -n_sep;
+        uint32_t kept[4];
+        float align_k[4];
+        uint32_t kn = 0;
+        for (uint32_t o = 0; o < 4; ++o) {
+          if (w[o].pen >= 0.02f) continue;
+          const float align = dot3(w[o].nrm, n_sep);
+          if (align <= 0.1f) continue;
+          bool dup = false;
+          for (uint32_t q = 0; q < kn; ++q)
+            if (w[kept[q]].fa == w[o].fa) dup = true;
+          if (dup) continue;
+          kept[kn] = o;
+          align_k[kn] = align;
+          ++kn;
+        }
+        const uint32_t reps = kn == 1 ? 4u : (kn == 2 ? 2u : 1u);
+        float3 t1 = cross3(n_sep, fabsf(n_sep.y) < 0.9f ? make_float3(0.f, 1.f, 0.f) : make_float3(1.f, 0.f, 0.f));
+        t1 = t1 * (1.0f / len3(t1));
+        const float3 t2 = cross3(n_sep, t1);
+        const float3 da = (t1 + t2) * (0.318f * vs1), db = (t1 - t2) * (0.318f * vs1);
+        int n_emit = 0;
+        for (uint32_t k2 = 0; k2 < kn; ++k2) {
+          const VWin& wo = w[kept[k2]];
+          const uint32_t vpar = (wo.fa ^ (wo.fa >> 8) ^ (wo.fa >> 16)) & 1u;
+          float3 emitted[4];
+          uint32_t en = 0;
+          for (uint32_t c = 0; c < reps; ++c) {
+            float3 pt = wo.pos;
+            if (reps > 1) {
+              const float3 offv = ((c < 2u) == (vpar == 0u)) ? da : db;
+              const float3 off = offv * ((c & 1u) == 0u ? 1.f : -1.f);
+              pt = wo.pos + off;
+              if (!vox_corner_supported(d, pt, n_sep, r2, s2_vox, axk)) {
+                pt = wo.pos + off * 0.5f;
+                if (!vox_corner_supported(d, pt, n_sep, r2, s2_vox, axk)) pt = wo.pos;
+              }
+            }
+            bool dup = false;
+            for (uint32_t q = 0; q < en; ++q) {
+              const float3 dp = pt - emitted[q];
+              if (dot3(dp, dp) < 1.0e-12f) dup = true;
+            }
+            if (dup) continue;
+            emitted[en++] = pt;
+            m.pos[n_emit] = pt;
+            m.pen[n_emit] = wo.pen * align_k[k2];
+            m.fp[n_emit] = wo.fa | (c << 24);
+            ++n_emit;
+          }
+        }
+        m.cc = n_emit;
+        store = n_emit > 0;
+      }
+      if (store) np_store(d, p, cur, warm, slot, ida, idb, d.flags[ida], A.p, B.p, m, true);
+    }
+    __syncwarp();
   }
 }
 
 // man_slot[man_index[k]] = k for every slot that collided; per-manifold statistics.
 __global__ void k_compact(const DevState d, int cur) {
-  const uint32_t P = min(d.ctr->pair_count, d.pair_capacity);
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x) {
+  const uint32_t S = slot_total(d);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
     if (!d.hit[k]) continue;
     d.man_slot[cur][d.man_index[k]] = k;
     int cc = d.m_keycc[cur][k].y;
@@ -655,11 +1045,18 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
                      int cur, bool warm) {
   const int T = BB_THREADS;
   int grid = sms * 8;
+  if (d.vox_on) {  // six slots per voxel pair: count, scan, fill
+    k_slot_count<<<grid, T, 0, s>>>(d);
+    bb_launch_scan(s, d.slot_cnt, d.slot_off, &d.ctr->pair_count, d.pair_capacity, &d.ctr->slot_count,
+                   sc.scan_status + 6 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 6, d.ctr);
+    k_slot_fill<<<grid, T, 0, s>>>(d);
+  }
   k_np_classify<<<sms * 8, 256, 0, s>>>(d, cur);
   k_narrow<<<sms * (p.narrow_blocks_per_sm ? p.narrow_blocks_per_sm : 16u), 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
-  // compact order: exclusive scan of the hit flags over the pair slots
-  bb_launch_scan(s, d.hit, d.man_index, &d.ctr->pair_count, d.pair_capacity, &d.ctr->manifold_count,
-                 sc.scan_status + sc.scan_tiles, sc.scan_tile_ctr + 1, d.ctr);
+  if (d.vox_on) k_voxel_narrow<<<sms * 8, 256, 0, s>>>(d, p, cur, warm ? 1 : 0);
+  // compact order: exclusive scan of the hit flags over the slots
+  bb_launch_scan(s, d.hit, d.man_index, d.vox_on ? &d.ctr->slot_count : &d.ctr->pair_count, d.pair_capacity,
+                 &d.ctr->manifold_count, sc.scan_status + sc.scan_tiles, sc.scan_tile_ctr + 1, d.ctr);
   k_compact<<<grid, T, 0, s>>>(d, cur);
   // per-body lists
   cudaMemsetAsync(d.csr_cursor, 0, sizeof(uint32_t) * (n + 1), s);

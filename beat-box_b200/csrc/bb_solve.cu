@@ -266,27 +266,28 @@ __device__ void pgs_solve_slot(const DevState& d, const Params& p, int cur, uint
 // integrate one body (RB_sim.slang:1287-1326) and refresh its world inverse inertia
 // Compiled once (not inlined) so both schedules integrate with the same instructions.
 __device__ __noinline__ void pgs_integrate_body(float4* pos, float4* rot, const float4* vel, const float4* omega,
-                                                const float4* iinv, float4* iw, uint32_t i, float h, bool tq) {
+                                                const float4* iinv, const float4* ioff, bool full, float4* iw,
+                                                uint32_t i, float h, bool tq) {
   const float4 ps = pos[i];
   const float3 v = f3(vel[i]);
   pos[i] = make_float4(ps.x + v.x * h, ps.y + v.y * h, ps.z + v.z * h, ps.w);
   const Quatf q = apply_angular_velocity(q_from(rot[i]), f3(omega[i]), h);
   rot[i] = q_to4(q);
-  const Sym3 s = world_inv_inertia(q, f3(iinv[i]), tq);
+  const Sym3 s = body_world_inv_inertia(iinv, ioff, full, i, q, tq);
   iw[2 * i] = make_float4(s.xx, s.xy, s.xz, s.yy);
   iw[2 * i + 1] = make_float4(s.yz, s.zz, 0.f, 0.f);
 }
-__device__ __noinline__ void pgs_world_inertia_body(const float4* rot, const float4* iinv, float4* iw, uint32_t i,
-                                                    bool tq) {
-  const Sym3 s = world_inv_inertia(q_from(rot[i]), f3(iinv[i]), tq);
+__device__ __noinline__ void pgs_world_inertia_body(const float4* rot, const float4* iinv, const float4* ioff,
+                                                    bool full, float4* iw, uint32_t i, bool tq) {
+  const Sym3 s = body_world_inv_inertia(iinv, ioff, full, i, q_from(rot[i]), tq);
   iw[2 * i] = make_float4(s.xx, s.xy, s.xz, s.yy);
   iw[2 * i + 1] = make_float4(s.yz, s.zz, 0.f, 0.f);
 }
 __device__ __forceinline__ void pgs_world_inertia(const DevState& d, uint32_t i, bool tq) {
-  pgs_world_inertia_body(d.rot, d.iinv, d.iw, i, tq);
+  pgs_world_inertia_body(d.rot, d.iinv, d.iinv_off, d.full_inertia != 0, d.iw, i, tq);
 }
 __device__ __forceinline__ void pgs_integrate(const DevState& d, uint32_t i, float h, bool tq) {
-  pgs_integrate_body(d.pos, d.rot, d.vel, d.omega, d.iinv, d.iw, i, h, tq);
+  pgs_integrate_body(d.pos, d.rot, d.vel, d.omega, d.iinv, d.iinv_off, d.full_inertia != 0, d.iw, i, h, tq);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1160,7 +1161,7 @@ __device__ void avbd_primal(const DevState& d, const Params& p, int cur, uint32_
   const float inv_dt2 = dt > 0.f ? 1.0f / (dt * dt) : 0.f;
   const float m_lin = d.vel[i].w * inv_dt2;
   Quatf rot = q_from(d.rot[i]);
-  Sym3 wi = world_inv_inertia(rot, f3(d.iinv[i]), tq);
+  Sym3 wi = body_world_inv_inertia(d.iinv, d.iinv_off, d.full_inertia != 0, i, rot, tq);
   // avbd_inverse3 (avbd.slang:309-326) of the symmetric world inverse inertia
   float3 c0 = make_float3(wi.xx, wi.xy, wi.xz), c1 = make_float3(wi.xy, wi.yy, wi.yz), c2 = make_float3(wi.xz, wi.yz, wi.zz);
   float3 r0 = cross3(c1, c2), r1 = cross3(c2, c0), r2 = cross3(c0, c1);

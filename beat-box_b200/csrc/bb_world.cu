@@ -20,6 +20,7 @@
 
 #include "bb_common.cuh"
 #include "bb_kernels.cuh"
+#include "bb_voxel_build.hpp"
 
 namespace {
 thread_local std::string g_last_error = "no error";
@@ -36,6 +37,9 @@ bb_status fail(bb_status code, const std::string& msg) {
 struct Shape {
   uint32_t type;
   float half[3];
+  uint32_t vox = 0;          // voxel shapes: index in the world's voxel table
+  float unit_mass = 0;       // voxel shapes: mass at density 1
+  float unit_inv[6] = {0, 0, 0, 0, 0, 0};  // voxel shapes: inverse inertia at density 1
 };
 
 thread_local size_t t_alloc_bytes = 0;  // device bytes allocated by dalloc on this thread
@@ -175,6 +179,8 @@ __global__ void k_begin_substep(DevCounters* c) {
   for (int k = 0; k < 8; ++k) c->sync_count[k] = 0;
   c->np_counts[0] = 0;
   c->np_counts[1] = 0;
+  c->np_counts[2] = 0;
+  c->slot_count = 0;
   c->gc_list_n[0] = 0;
   c->gc_list_n[1] = 0;
   c->hv_pool_n = 0;
@@ -210,6 +216,11 @@ struct bb_world_impl {
   std::map<std::tuple<uint32_t, int, int, uint32_t, uint64_t, uint32_t>, GraphEntry> graphs;
   bool use_graphs = true;
   uint64_t launches = 0;
+  // voxel shapes: host copies of the device table and pools
+  std::vector<VoxDev> vox_table;
+  std::vector<uint32_t> vox_occ, vox_surf;
+  void* vox_buf = nullptr;     // device: table | occupancy | surface list
+  void* slot_buf = nullptr;    // device: slot_cnt | slot_off | slot_pair | vox_list (pair capacity each)
   // profiling
   bool profiling = false;
   std::vector<std::string> stage_names;
@@ -219,6 +230,8 @@ struct bb_world_impl {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
     for (void* p : owned) cudaFree(p);
+    if (vox_buf) cudaFree(vox_buf);
+    if (slot_buf) cudaFree(slot_buf);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 
@@ -229,7 +242,7 @@ struct bb_world_impl {
     auto f4 = [&](size_t k) { return dalloc<float4>(k, owned, err, stream); };
     auto u32 = [&](size_t k) { return dalloc<uint32_t>(k, owned, err, stream); };
     d.pos = f4(N); d.rot = f4(N); d.vel = f4(N); d.omega = f4(N); d.pvel = f4(N); d.shape = f4(N); d.iinv = f4(N);
-    d.flags = u32(N); d.sleep = u32(N); d.iw = f4(2 * N);
+    d.flags = u32(N); d.sleep = u32(N); d.iw = f4(2 * N); d.iinv_off = f4(N);
     for (int k = 0; k < 2; ++k) { d.keys[k] = u32(N); d.vals[k] = u32(N); }
     d.rank = u32(N);
     d.node_box = f4(4 * N);
@@ -288,10 +301,10 @@ struct bb_world_impl {
     xforms = dalloc<float>(12 * N, owned, err, stream);
     d.pair_capacity = cap_p;
     d.body_capacity = cap_n;
-    // scratch zeroed at every substep: scan status (5 scans), sort hists / status (12 slots)
+    // scratch zeroed at every substep: scan status (7 scans), sort hists / status (12 slots)
     sc.scan_tiles = bb_scan_tiles(std::max<size_t>(P, N + 1));
     sc.sort_tiles = bb_sort_tiles(std::max<size_t>(P, N));
-    size_t scan_words = size_t(6) * sc.scan_tiles;  // 64-bit
+    size_t scan_words = size_t(7) * sc.scan_tiles;  // 64-bit
     size_t sort_status_words = size_t(12) * sc.sort_tiles * 256;
     size_t hist_words = 5 * BB_HIST_REGION;
     scratch_bytes = scan_words * 8 + 16 * 4 + hist_words * 4 + sort_status_words * 4 + 16 * 4;
@@ -487,6 +500,11 @@ bb_status bb_world_clear(void* world) {
   w->n_dyn = 0;
   w->shapes.clear();
   w->restitution.clear();
+  w->vox_table.clear();
+  w->vox_occ.clear();
+  w->vox_surf.clear();
+  w->d.vox_on = 0;
+  w->d.full_inertia = 0;
   w->d.n_worlds = 0;
   w->parity = 0;
   w->last_cur = 0;
@@ -514,12 +532,96 @@ bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape) {
   return BB_OK;
 }
 
+bb_status bb_voxel_shape_info(uint32_t nx, uint32_t ny, uint32_t nz, float voxel_size, const uint8_t* solid,
+                              bb_voxel_info* out, uint32_t* surface, uint32_t surface_capacity) {
+  VoxelBuild b;
+  if (!out || !voxel_build(nx, ny, nz, voxel_size, solid, b))
+    return fail(BB_E_INVALID, "bb_voxel_shape_info: bad grid (dims 1..256, voxel_size > 0, one solid cell)");
+  for (int k = 0; k < 3; ++k) {
+    out->grid_origin[k] = b.origin[k];
+    out->box_min[k] = b.origin[k];
+    out->box_max[k] = b.hi[k];
+  }
+  out->solid_count = b.solid;
+  out->surface_count = uint32_t(b.surf.size());
+  out->unit_mass = b.unit_mass;
+  for (int k = 0; k < 6; ++k) out->unit_inv_inertia[k] = b.unit_inv[k];
+  if (surface) {
+    if (surface_capacity < b.surf.size()) return fail(BB_E_INVALID, "bb_voxel_shape_info: surface buffer too small");
+    std::memcpy(surface, b.surf.data(), 4 * b.surf.size());
+  }
+  return BB_OK;
+}
+
+// Appends the shape to the world's voxel table and re-uploads table and pools (shapes are
+// added while building a scene, not per step).  The first voxel shape also allocates the
+// per-slot arrays of the narrow phase (six manifold slots per voxel pair).
+bb_status bb_add_voxel_shape(void* world, uint32_t nx, uint32_t ny, uint32_t nz, float voxel_size,
+                             const uint8_t* solid, uint32_t* out_shape) {
+  World* w = W(world);
+  VoxelBuild b;
+  if (!w || !out_shape || !voxel_build(nx, ny, nz, voxel_size, solid, b))
+    return fail(BB_E_INVALID, "bb_add_voxel_shape: bad arguments (dims 1..256, voxel_size > 0, one solid cell)");
+  if (w->vox_table.size() >= (1u << 24)) return fail(BB_E_INVALID, "bb_add_voxel_shape: too many voxel shapes");
+  VoxDev v = {};
+  v.ox = b.origin[0];
+  v.oy = b.origin[1];
+  v.oz = b.origin[2];
+  v.vs = b.vs;
+  v.hx = b.hi[0];
+  v.hy = b.hi[1];
+  v.hz = b.hi[2];
+  v.surf_count = uint32_t(b.surf.size());
+  v.dx = nx;
+  v.dy = ny;
+  v.dz = nz;
+  v.occ_off = uint32_t(w->vox_occ.size());
+  v.surf_off = uint32_t(w->vox_surf.size());
+  w->vox_table.push_back(v);
+  w->vox_occ.insert(w->vox_occ.end(), b.occ.begin(), b.occ.end());
+  w->vox_surf.insert(w->vox_surf.end(), b.surf.begin(), b.surf.end());
+  CU(cudaStreamSynchronize(w->stream));
+  if (!w->slot_buf) {
+    CU(cudaMalloc(&w->slot_buf, 16ull * w->cap_p));
+    uint32_t* sb = static_cast<uint32_t*>(w->slot_buf);
+    w->d.slot_cnt = sb;
+    w->d.slot_off = sb + w->cap_p;
+    w->d.slot_pair = sb + 2ull * w->cap_p;
+    w->d.vox_list = sb + 3ull * w->cap_p;
+    w->dev_bytes += 16ull * w->cap_p;
+  }
+  const size_t tb = sizeof(VoxDev) * w->vox_table.size(), ob = 4 * w->vox_occ.size(), sb = 4 * w->vox_surf.size();
+  if (w->vox_buf) {
+    CU(cudaFree(w->vox_buf));
+    w->vox_buf = nullptr;
+  }
+  CU(cudaMalloc(&w->vox_buf, tb + ob + sb + 16));
+  char* base = static_cast<char*>(w->vox_buf);
+  CU(cudaMemcpyAsync(base, w->vox_table.data(), tb, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(base + tb, w->vox_occ.data(), ob, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(base + tb + ob, w->vox_surf.data(), sb, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  w->d.vox = reinterpret_cast<const VoxDev*>(base);
+  w->d.vox_occ = reinterpret_cast<const uint32_t*>(base + tb);
+  w->d.vox_surf = reinterpret_cast<const uint32_t*>(base + tb + ob);
+  w->d.vox_on = 1;
+  Shape sh{BB_SHAPE_VOXEL, {0.5f * (b.hi[0] - b.origin[0]), 0.5f * (b.hi[1] - b.origin[1]), 0.5f * (b.hi[2] - b.origin[2])}};
+  sh.vox = uint32_t(w->vox_table.size() - 1);
+  sh.unit_mass = b.unit_mass;
+  for (int k = 0; k < 6; ++k) sh.unit_inv[k] = b.unit_inv[k];
+  w->shapes.push_back(sh);
+  w->invalidate_graphs();
+  *out_shape = uint32_t(w->shapes.size() - 1);
+  return BB_OK;
+}
+
 static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id,
                                  bool keep_contacts = false) {
   if (!w || (!bodies && count)) return fail(BB_E_INVALID, "bb_add_bodies: bad arguments");
   if (uint64_t(w->n) + count > w->cap_n) return fail(BB_E_CAPACITY, "bb_add_bodies: max_bodies exceeded");
-  std::vector<float4> pos(count), rot(count), vel(count), om(count), shp(count), ii(count);
+  std::vector<float4> pos(count), rot(count), vel(count), om(count), shp(count), ii(count), io(count);
   std::vector<uint32_t> fl(count), zero(count, 0);
+  bool any_off = false;
   uint32_t ndyn = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const bb_body_desc& b = bodies[i];
@@ -528,14 +630,23 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
     bool dyn = (b.flags & BB_BODY_DYNAMIC) != 0;
     double vol = s.type == BB_SHAPE_BOX ? 8.0 * s.half[0] * s.half[1] * s.half[2]
                                         : 4.0 / 3.0 * 3.14159265358979 * double(s.half[0]) * s.half[0] * s.half[0];
-    float mass = b.mass > 0 ? b.mass : float(b.density * vol);
+    float mass = b.mass > 0 ? b.mass : (s.type == BB_SHAPE_VOXEL ? b.density * s.unit_mass : float(b.density * vol));
     if (!dyn) mass = 0;
     if (dyn && !(mass > 0)) return fail(BB_E_INVALID, "bb_add_bodies: dynamic body needs mass or density");
     float inv_mass = dyn ? 1.0f / mass : 0.0f;
-    float inv_i[3] = {0, 0, 0};
+    float inv_i[3] = {0, 0, 0}, inv_o[3] = {0, 0, 0};
     if (dyn) {
       if (b.inertia_mode == BB_INERTIA_EXPLICIT) {
-        for (int k = 0; k < 3; ++k) inv_i[k] = b.inv_inertia[k];
+        for (int k = 0; k < 3; ++k) {
+          inv_i[k] = b.inv_inertia[k];
+          inv_o[k] = b.inv_inertia_off[k];
+        }
+      } else if (s.type == BB_SHAPE_VOXEL) {
+        const float scale = s.unit_mass / mass;  // inertia scales with mass at fixed shape
+        for (int k = 0; k < 3; ++k) {
+          inv_i[k] = s.unit_inv[k] * scale;
+          inv_o[k] = s.unit_inv[3 + k] * scale;
+        }
       } else if (b.inertia_mode == BB_INERTIA_REFERENCE) {
         // cuboid_get_inverse_intertia(inv_mass, min, max) (include/math.hpp:106-130)
         float w_ = 2 * s.half[0], h_ = 2 * s.half[1], d_ = 2 * s.half[2];
@@ -557,11 +668,13 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
     rot[i] = make_float4(b.rotation[0], b.rotation[1], b.rotation[2], b.rotation[3]);
     vel[i] = make_float4(b.velocity[0], b.velocity[1], b.velocity[2], mass);
     om[i] = make_float4(b.omega[0], b.omega[1], b.omega[2], 0.f);
-    uint32_t tbits = s.type;
+    uint32_t tbits = s.type | (s.type == BB_SHAPE_VOXEL ? s.vox << 8 : 0u);
     float tf;
     std::memcpy(&tf, &tbits, 4);
     shp[i] = make_float4(s.half[0], s.half[1], s.half[2], tf);
     ii[i] = make_float4(inv_i[0], inv_i[1], inv_i[2], b.friction);
+    io[i] = make_float4(inv_o[0], inv_o[1], inv_o[2], 0.f);
+    if (inv_o[0] != 0.f || inv_o[1] != 0.f || inv_o[2] != 0.f) any_off = true;
     fl[i] = b.flags & (BB_BODY_DYNAMIC | BB_BODY_GRAVITY | BB_BODY_SLEEPING);
     if (dyn) ++ndyn;
     w->restitution.push_back(b.restitution);
@@ -575,6 +688,8 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
   CU(cudaMemcpyAsync(w->d.omega + o, om.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.shape + o, shp.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.iinv + o, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.iinv_off + o, io.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  if (any_off) w->d.full_inertia = 1;
   CU(cudaMemcpyAsync(w->d.flags + o, fl.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.sleep + o, zero.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
   w->n += count;
@@ -925,6 +1040,7 @@ bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_byt
   const uint32_t n = w->n;
   const int cur = w->last_cur;
   const uint32_t P = std::min(c.pair_count, w->cap_p), M = c.manifold_count;
+  const uint32_t S = w->d.vox_on ? std::min(c.slot_count, w->cap_p) : P;  // manifold slots
   std::vector<uint8_t> out;
   uint64_t cnt = 0;
   auto grab = [&](const void* src, size_t bytes) -> bb_status {
@@ -977,15 +1093,15 @@ bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_byt
         break;
       }
       if (which == BB_DBG_MANIFOLDS) {
-        std::vector<uint2> bodies(P);
-        std::vector<int2> kc(P);
-        std::vector<float4> nrm(P), t0(P), t1(P);
-        if (P) {
-          CU(cudaMemcpy(bodies.data(), w->d.m_bodies[cur], 8 * P, cudaMemcpyDeviceToHost));
-          CU(cudaMemcpy(kc.data(), w->d.m_keycc[cur], 8 * P, cudaMemcpyDeviceToHost));
-          CU(cudaMemcpy(nrm.data(), w->d.m_normal[cur], 16 * P, cudaMemcpyDeviceToHost));
-          CU(cudaMemcpy(t0.data(), w->d.m_t0[cur], 16 * P, cudaMemcpyDeviceToHost));
-          CU(cudaMemcpy(t1.data(), w->d.m_t1[cur], 16 * P, cudaMemcpyDeviceToHost));
+        std::vector<uint2> bodies(S);
+        std::vector<int2> kc(S);
+        std::vector<float4> nrm(S), t0(S), t1(S);
+        if (S) {
+          CU(cudaMemcpy(bodies.data(), w->d.m_bodies[cur], 8 * S, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(kc.data(), w->d.m_keycc[cur], 8 * S, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(nrm.data(), w->d.m_normal[cur], 16 * S, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(t0.data(), w->d.m_t0[cur], 16 * S, cudaMemcpyDeviceToHost));
+          CU(cudaMemcpy(t1.data(), w->d.m_t1[cur], 16 * S, cudaMemcpyDeviceToHost));
         }
         if (M) CU(cudaMemcpy(color.data(), w->d.gc_color, 4 * M, cudaMemcpyDeviceToHost));
         out.resize(sizeof(bb_manifold_info) * M);
@@ -1004,15 +1120,15 @@ bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_byt
         cnt = M;
         break;
       }
-      const size_t C = size_t(P) * BB_MAX_CONTACTS;
+      const size_t C = size_t(S) * BB_MAX_CONTACTS;
       std::vector<float4> cp(C), cl(C), ck(C), ca(C);
-      std::vector<int2> kc(P);
-      if (P) {
+      std::vector<int2> kc(S);
+      if (S) {
         CU(cudaMemcpy(cp.data(), w->d.c_pos[cur], 16 * C, cudaMemcpyDeviceToHost));
         CU(cudaMemcpy(cl.data(), w->d.c_lam[cur], 16 * C, cudaMemcpyDeviceToHost));
         CU(cudaMemcpy(ck.data(), w->d.c_kt[cur], 16 * C, cudaMemcpyDeviceToHost));
         CU(cudaMemcpy(ca.data(), w->d.c_anc_a[cur], 16 * C, cudaMemcpyDeviceToHost));
-        CU(cudaMemcpy(kc.data(), w->d.m_keycc[cur], 8 * P, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(kc.data(), w->d.m_keycc[cur], 8 * S, cudaMemcpyDeviceToHost));
       }
       out.assign(sizeof(bb_contact_info) * 8 * size_t(M), 0);
       bb_contact_info* ci = reinterpret_cast<bb_contact_info*>(out.data());
@@ -1037,6 +1153,21 @@ bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_byt
     case BB_DBG_BODY_COLORS: st = grab(w->d.body_color, 4 * n); cnt = n; break;
     case BB_DBG_ISLANDS: st = grab(w->d.island, 4 * n); cnt = n; break;
     case BB_DBG_SUPPORT_DEPTH: st = grab(w->d.a_depth, 4 * n); cnt = n; break;
+    case BB_DBG_BODY_INERTIA: {
+      std::vector<float4> ii(n), io(n);
+      if (n) {
+        CU(cudaMemcpy(ii.data(), w->d.iinv, 16ull * n, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(io.data(), w->d.iinv_off, 16ull * n, cudaMemcpyDeviceToHost));
+      }
+      out.resize(24ull * n);
+      float* o = reinterpret_cast<float*>(out.data());
+      for (uint32_t i = 0; i < n; ++i) {
+        o[6 * i] = ii[i].x; o[6 * i + 1] = ii[i].y; o[6 * i + 2] = ii[i].z;
+        o[6 * i + 3] = io[i].x; o[6 * i + 4] = io[i].y; o[6 * i + 5] = io[i].z;
+      }
+      cnt = 6ull * n;
+      break;
+    }
     default: return fail(BB_E_INVALID, "bb_debug_read: unknown buffer");
   }
   if (st != BB_OK) return st;

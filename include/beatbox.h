@@ -41,13 +41,18 @@ typedef int32_t bb_status;
 /* ---- shapes ---------------------------------------------------------------------- */
 #define BB_SHAPE_BOX 0u    /* reference OBB body: RigidBody::minimum/maximum (shared.inl:349-352) */
 #define BB_SHAPE_SPHERE 1u /* no reference counterpart: written from first principles */
+#define BB_SHAPE_VOXEL 2u  /* concave body: occupancy bitmask + surface cells (VoxelShape,
+                              include/shared.inl:938-951; RigidBody::shape_index != 0) */
+#define BB_VOXEL_MAX_DIM 256u /* cells per axis: surface cells pack x | y<<8 | z<<16 */
 
 /* ---- inertia construction modes for bb_add_bodies -------------------------------- */
 #define BB_INERTIA_PHYSICAL 0u  /* solid box / sphere inverse inertia from mass */
 #define BB_INERTIA_REFERENCE 1u /* cuboid_get_inverse_intertia(inv_mass, min, max): the reference
                                    scene builder passes inverse mass as mass
                                    (src/scene_manager.hpp:861, include/math.hpp:106-130) */
-#define BB_INERTIA_EXPLICIT 2u  /* use bb_body_desc.inv_inertia (body-frame diagonal) as given */
+#define BB_INERTIA_EXPLICIT 2u  /* use bb_body_desc.inv_inertia (+ inv_inertia_off) as given */
+/* Voxel bodies always take their inertia from the shape (BB_INERTIA_PHYSICAL and
+ * BB_INERTIA_REFERENCE both mean "from the shape") unless BB_INERTIA_EXPLICIT. */
 
 /* ---- solver types: SimSolverType (include/shared.inl:210-216) ---------------------- */
 #define BB_SOLVER_PGS 0u      /* Baumgarte PGS: only on the reference's per-island path */
@@ -161,6 +166,9 @@ typedef struct bb_body_desc {
   float restitution;     /* stored; unused by the reference solvers (solvers.slang:49-56) */
   uint32_t inertia_mode; /* BB_INERTIA_* */
   float inv_inertia[3];  /* body-frame diagonal, BB_INERTIA_EXPLICIT only */
+  float inv_inertia_off[3]; /* body-frame off-diagonal (xy, xz, yz), BB_INERTIA_EXPLICIT only;
+                               the reference RigidBody::inv_inertia is a full 3x3
+                               (include/shared.inl:366) */
 } bb_body_desc;
 
 /* Per-step counters: the reference SimConfig readback (src/rigid_body_manager.cpp:1681-1693,
@@ -207,6 +215,7 @@ typedef struct bb_step_stats {
 #define BB_DBG_BODY_COLORS 11u /* u32 x N by body id (AVBD colouring) */
 #define BB_DBG_ISLANDS 12u     /* u32 x N by body id (0xFFFFFFFF = static / no island) */
 #define BB_DBG_SUPPORT_DEPTH 13u /* u32 x N by body id (AVBD shock-propagation depth) */
+#define BB_DBG_BODY_INERTIA 14u  /* f32 x 6N by body id: body-frame inverse inertia xx yy zz xy xz yz */
 
 typedef struct bb_manifold_info {
   uint32_t body_a;       /* body ids; a has the lower sorted position this substep */
@@ -244,6 +253,30 @@ bb_status bb_world_destroy(void* world);
  * shared.inl:351-352); here bodies reference a shape handle. */
 bb_status bb_add_box_shape(void* world, float hx, float hy, float hz, uint32_t* out_shape);
 bb_status bb_add_sphere_shape(void* world, float radius, uint32_t* out_shape);
+
+/* Voxel shape from an occupancy grid: solid[x + y*nx + z*nx*ny] != 0 marks a solid cell
+ * (nx, ny, nz <= BB_VOXEL_MAX_DIM, at least one solid cell).  The body origin is the
+ * centre of mass of the solid cells.  Replaces SceneManager::build_voxel_shape
+ * (src/scene_manager.hpp:488-560) and the voxel pools it fills (shared.inl:771-774). */
+bb_status bb_add_voxel_shape(void* world, uint32_t nx, uint32_t ny, uint32_t nz, float voxel_size,
+                             const uint8_t* solid, uint32_t* out_shape);
+
+/* What bb_add_voxel_shape derives from a grid, on the host (no world, no GPU). */
+typedef struct bb_voxel_info {
+  float grid_origin[3];       /* body-frame corner of cell (0,0,0) = minus the centre of mass */
+  float box_min[3];           /* RigidBody::minimum (= grid_origin) */
+  float box_max[3];           /* RigidBody::maximum (= grid_origin + dims * voxel_size) */
+  uint32_t solid_count;
+  uint32_t surface_count;     /* solid cells with an empty face neighbour */
+  float unit_mass;            /* mass at density 1: solid_count * voxel_size^3 */
+  float unit_inv_inertia[6];  /* inverse inertia about the centre of mass at density 1,
+                                 body frame: xx, yy, zz, xy, xz, yz */
+} bb_voxel_info;
+/* surface: NULL, or room for surface_count entries packed x | y<<8 | z<<16 | dir<<24 with dir
+ * the first empty neighbour in the order -x, +x, -y, +y, -z, +z (scene_manager.hpp:536-546).
+ * A body of mass M has inverse inertia unit_inv_inertia * (unit_mass / M) (float). */
+bb_status bb_voxel_shape_info(uint32_t nx, uint32_t ny, uint32_t nz, float voxel_size, const uint8_t* solid,
+                              bb_voxel_info* out, uint32_t* surface, uint32_t surface_capacity);
 
 /* Append n bodies; their ids are consecutive from *out_first_id.  Replaces the body
  * push + id/mass/inertia assignment of SceneManager::load_scene

@@ -104,8 +104,11 @@ template <class R> uint64_t debug_read(World<R>& w, uint32_t which, void* dst, u
           c.normal_impulse = float(s.ni);
           c.tangent_impulse[0] = float(s.ti[0]);
           c.tangent_impulse[1] = float(s.ti[1]);
-          c.feature = (s.fp.in_ref & 0xFF) | ((s.fp.out_ref & 0xFF) << 8) | ((s.fp.in_inc & 0xFF) << 16) |
-                      ((s.fp.out_inc & 0xFF) << 24);
+          // voxel manifolds: the sampled voxel and corner (in_inc); else four 8-bit ids
+          c.feature = (mf.key >= VOXEL_KEY0 && mf.key < VOXEL_KEY0 + 6)
+                          ? s.fp.in_inc
+                          : (s.fp.in_ref & 0xFF) | ((s.fp.out_ref & 0xFF) << 8) | ((s.fp.in_inc & 0xFF) << 16) |
+                                ((s.fp.out_inc & 0xFF) << 24);
           c.warm_start = s.warm;
           c.penalty = float(s.mcoef);
         }
@@ -152,6 +155,54 @@ void* orc_create(uint32_t n, const float* pos, const float* quat, const float* v
 }
 
 void orc_destroy(void* hp) { delete static_cast<Handle*>(hp); }
+
+// Voxel shapes (build_voxel_shape, src/scene_manager.hpp:488-560): returns the shape index.
+uint32_t orc_add_voxel_shape(void* hp, uint32_t nx, uint32_t ny, uint32_t nz, float vs, const uint8_t* solid) {
+  Handle* h = static_cast<Handle*>(hp);
+  uint32_t a = h->dbl ? h->d->voxels.add(nx, ny, nz, vs, solid) : h->f->voxels.add(nx, ny, nz, vs, solid);
+  return a;
+}
+
+// Binds voxel bodies (shape BB_SHAPE_VOXEL) to their shapes and sets the off-diagonal inverse
+// inertia (xy, xz, yz per body; NULL = zero) of dynamic bodies.
+void orc_set_voxel_bodies(void* hp, const uint32_t* voxel_index, const float* inv_inertia_off) {
+  Handle* h = static_cast<Handle*>(hp);
+  auto set = [&](auto& w) {
+    using R = typename std::remove_reference<decltype(w.bodies[0].pos.x)>::type;
+    for (size_t i = 0; i < w.n(); ++i) {
+      auto& b = w.bodies[i];
+      if (b.shape == BB_SHAPE_VOXEL) {
+        b.voxel = voxel_index[i];
+        const VoxelShape& s = w.voxels.shapes[b.voxel];
+        for (int k = 0; k < 3; ++k) {
+          b.lo[k] = s.lo[k];
+          b.hi[k] = s.hi[k];
+        }
+      }
+      if (inv_inertia_off && (b.flags & BB_BODY_DYNAMIC))
+        b.inv_inertia_off = Vec3<R>(inv_inertia_off[3 * i], inv_inertia_off[3 * i + 1], inv_inertia_off[3 * i + 2]);
+    }
+  };
+  if (h->dbl) set(*h->d);
+  else set(*h->f);
+}
+
+// The oracle's build of voxel shape `index`: origin[3], lo[3], hi[3] into f9; solid and
+// surface counts into u2; the surface list into surf (surface-count entries) when not NULL.
+void orc_voxel_shape(void* hp, uint32_t index, float* f9, uint32_t* u2, uint32_t* surf) {
+  Handle* h = static_cast<Handle*>(hp);
+  const VoxelPool& vp = h->dbl ? h->d->voxels : h->f->voxels;
+  const VoxelShape& s = vp.shapes[index];
+  for (int k = 0; k < 3; ++k) {
+    f9[k] = s.origin[k];
+    f9[3 + k] = s.lo[k];
+    f9[6 + k] = s.hi[k];
+  }
+  u2[0] = s.solid;
+  u2[1] = s.surf_count;
+  if (surf)
+    for (uint32_t i = 0; i < s.surf_count; ++i) surf[i] = vp.surf[s.surf_off + i];
+}
 
 void orc_default_params(bb_solver_params* p) { default_params(p); }
 

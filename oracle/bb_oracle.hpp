@@ -31,11 +31,14 @@
 // in FP32 with the reference's operation order; build with -ffp-contract=off.
 #pragma once
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <condition_variable>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -136,10 +139,13 @@ class Pool {
 template <class R> struct Body {
   uint32_t id = 0, flags = 0, shape = BB_SHAPE_BOX;
   float half[3] = {0.5f, 0.5f, 0.5f};  // box half extents; sphere radius in half[0]
+  uint32_t voxel = 0;                  // voxel shape index (BB_SHAPE_VOXEL)
+  float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // voxel bodies: body-frame box [minimum, maximum]
   Vec3<R> pos, vel, omega, prev_vel;
   Quat<R> rot;
   R mass = 0, inv_mass = 0;
-  Vec3<R> inv_inertia;  // body-frame diagonal
+  Vec3<R> inv_inertia;      // body-frame diagonal
+  Vec3<R> inv_inertia_off;  // body-frame off-diagonal (xy, xz, yz); zero for boxes and spheres
   R friction = 0.5, restitution = 0;
   uint32_t sleep_timer = 0;
   uint32_t active_index = MAX_U32;
@@ -247,8 +253,27 @@ inline float fminx(float a, float b) { return b < a ? b : a; }
 inline float fmaxx(float a, float b) { return b > a ? b : a; }
 
 // RigidBody::get_AABB_from_OBB (extensions.slang:195-210): the 8 corners of [min, max]
-// pushed through object_to_world (quaternion sandwich, shared.inl:455-475).  Spheres:
-// centre +- radius.
+// pushed through object_to_world (quaternion sandwich, shared.inl:455-475).  Boxes have
+// [min, max] = [-half, half]; voxel bodies their grid box [lo, hi] (off-centre: the body origin
+// is the centre of mass).  Spheres: centre +- radius.
+inline Aabb leaf_aabb_box(const float lo[3], const float hi[3], const float p[3], const float q[4]) {
+  Aabb a;
+  Quat<float> qq(Vec3<float>(q[0], q[1], q[2]), q[3]);
+  for (int k = 0; k < 3; ++k) {
+    a.mn[k] = FLT_MAX;
+    a.mx[k] = -FLT_MAX;
+  }
+  for (uint32_t i = 0; i < 8; ++i) {
+    Vec3<float> c((i & 1) == 0 ? lo[0] : hi[0], (i & 2) == 0 ? lo[1] : hi[1], (i & 4) == 0 ? lo[2] : hi[2]);
+    Vec3<float> w = rotate_vector(qq, c);
+    float wv[3] = {w.x + p[0], w.y + p[1], w.z + p[2]};
+    for (int k = 0; k < 3; ++k) {
+      a.mn[k] = fminx(a.mn[k], wv[k]);
+      a.mx[k] = fmaxx(a.mx[k], wv[k]);
+    }
+  }
+  return a;
+}
 inline Aabb leaf_aabb(uint32_t shape, const float half[3], const float p[3], const float q[4]) {
   Aabb a;
   if (shape == BB_SHAPE_SPHERE) {
@@ -258,22 +283,8 @@ inline Aabb leaf_aabb(uint32_t shape, const float half[3], const float p[3], con
     }
     return a;
   }
-  Quat<float> qq(Vec3<float>(q[0], q[1], q[2]), q[3]);
-  for (int k = 0; k < 3; ++k) {
-    a.mn[k] = FLT_MAX;
-    a.mx[k] = -FLT_MAX;
-  }
-  for (uint32_t i = 0; i < 8; ++i) {
-    Vec3<float> c((i & 1) == 0 ? -half[0] : half[0], (i & 2) == 0 ? -half[1] : half[1],
-                  (i & 4) == 0 ? -half[2] : half[2]);
-    Vec3<float> w = rotate_vector(qq, c);
-    float wv[3] = {w.x + p[0], w.y + p[1], w.z + p[2]};
-    for (int k = 0; k < 3; ++k) {
-      a.mn[k] = fminx(a.mn[k], wv[k]);
-      a.mx[k] = fmaxx(a.mx[k], wv[k]);
-    }
-  }
-  return a;
+  const float lo[3] = {-half[0], -half[1], -half[2]};
+  return leaf_aabb_box(lo, half, p, q);
 }
 // Aabb::overlap (include/math.hpp:213-217), closed intervals.
 inline bool overlap(const Aabb& a, const Aabb& b) {

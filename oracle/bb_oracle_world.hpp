@@ -5,6 +5,7 @@
 // h = dt / substeps.
 #pragma once
 #include "bb_oracle.hpp"
+#include "bb_oracle_voxel.hpp"
 
 namespace bbo {
 
@@ -18,6 +19,8 @@ template <class R> class World {
   std::vector<uint32_t> order;  // body ids in the previous substep's sorted order
   std::vector<Manifold<R>> prev_manifolds;
   std::unordered_map<uint64_t, uint32_t> prev_pair_index;  // (min id, max id) -> prev manifold
+  std::map<std::tuple<uint32_t, uint32_t, int>, uint32_t> prev_voxel_index;  // (a, b, key) -> prev manifold
+  VoxelPool voxels;
   bool skip_warm_once = false;
 
   // products of the last substep (debug readback)
@@ -40,9 +43,15 @@ template <class R> class World {
 
   // RigidBody::get_transformed_inertia (extensions.slang:184-188): M * D * M^T with
   // M = get_rotation_matrix() = to_matrix()^T  (i.e. R^T D R).  Physical: R D R^T.
+  // A body with a non-zero off-diagonal (voxel bodies) uses its full symmetric matrix.
   Mat3<R> world_inv_inertia(const Body<R>& b) const {
     Mat3<R> Rm = to_matrix(b.rot);
     Mat3<R> D = diag(b.inv_inertia);
+    const Vec3<R>& o = b.inv_inertia_off;
+    if (o.x != R(0) || o.y != R(0) || o.z != R(0)) {
+      D = Mat3<R>::rows(Vec3<R>(b.inv_inertia.x, o.x, o.y), Vec3<R>(o.x, b.inv_inertia.y, o.z),
+                        Vec3<R>(o.y, o.z, b.inv_inertia.z));
+    }
     if (p.quirks & BB_QUIRK_INERTIA_TRANSPOSE) return mul_mm(transpose(Rm), mul_mm(D, Rm));
     return mul_mm(Rm, mul_mm(D, transpose(Rm)));
   }
@@ -104,7 +113,7 @@ template <class R> class World {
       const Body<R>& b = bodies[sorted_ids[i]];
       float pp[3] = {float(b.pos.x), float(b.pos.y), float(b.pos.z)};
       float qq[4] = {float(b.rot.v.x), float(b.rot.v.y), float(b.rot.v.z), float(b.rot.w)};
-      leaf[i] = leaf_aabb(b.shape, b.half, pp, qq);
+      leaf[i] = b.shape == BB_SHAPE_VOXEL ? leaf_aabb_box(b.lo, b.hi, pp, qq) : leaf_aabb(b.shape, b.half, pp, qq);
     }, 1024);
     const int n_ = int(N);
     child.assign(N > 1 ? 2 * (N - 1) : 0, 0);
@@ -206,7 +215,8 @@ template <class R> class World {
   // Narrow phase + warm start (collision_detection.slang:1514-1755).
   void narrow_phase() {
     const size_t P = pair_a.size();
-    std::vector<Manifold<R>> per(P);
+    // up to six manifolds per pair (voxel pairs, one per face direction); one otherwise
+    std::vector<std::array<Manifold<R>, 6>> per(P);
     std::vector<uint8_t> have(P, 0);
     bool warm = (p.flags & BB_SIM_WARM_STARTING) && !skip_warm_once;
     bool quirk = (p.quirks & BB_QUIRK_SAT_FRAME) != 0;
@@ -215,44 +225,57 @@ template <class R> class World {
       const Body<R>& A = bodies[ida];
       const Body<R>& B = bodies[idb];
       if (!is_dyn(A) && !is_dyn(B)) return;  // static-static skip (:1525)
-      SatResult<R> s;
-      bool hit;
-      if (A.shape == BB_SHAPE_BOX && B.shape == BB_SHAPE_BOX) hit = box_box(A, B, quirk, s);
-      else if (A.shape == BB_SHAPE_SPHERE && B.shape == BB_SHAPE_SPHERE) hit = sphere_sphere(A, B, s);
-      else hit = box_sphere(A, B, s);
-      if (!hit) return;
-      Manifold<R>& m = per[k];
-      m.a = ida;
-      m.b = idb;
-      m.sa = pair_a[k];
-      m.sb = pair_b[k];
-      m.key = s.key;
-      m.cc = s.cc;
-      m.normal = s.normal;
-      for (int c = 0; c < s.cc; ++c) {
-        Contact<R> ct;
-        ct.pos = s.pos[c];
-        ct.pen = std::max(s.pen[c], R(p.penetration_cap));  // extraction cap (:1575-1578)
-        ct.fp = s.fp[c];
-        m.c[c] = ct;
-      }
-      m.anchor_a = A.pos;
-      m.anchor_b = B.pos;
-      m.error = 0x7FFFFFFF;
-      compute_basis(m);
-      if (warm) {
-        uint64_t key = (uint64_t(std::min(ida, idb)) << 32) | std::max(ida, idb);
-        auto it = prev_pair_index.find(key);
-        if (it != prev_pair_index.end()) {
-          const Manifold<R>& old = prev_manifolds[it->second];
-          update_from_old(m, old, old.a != ida);
+      const bool vox = A.shape == BB_SHAPE_VOXEL || B.shape == BB_SHAPE_VOXEL;
+      for (uint32_t code = 0; code < (vox ? 6u : 1u); ++code) {
+        SatResult<R> s;
+        bool hit;
+        if (vox) hit = voxel_collide(A, B, code, voxels, s);
+        else if (A.shape == BB_SHAPE_BOX && B.shape == BB_SHAPE_BOX) hit = box_box(A, B, quirk, s);
+        else if (A.shape == BB_SHAPE_SPHERE && B.shape == BB_SHAPE_SPHERE) hit = sphere_sphere(A, B, s);
+        else hit = box_sphere(A, B, s);
+        if (!hit) continue;
+        Manifold<R>& m = per[k][code];
+        m.a = ida;
+        m.b = idb;
+        m.sa = pair_a[k];
+        m.sb = pair_b[k];
+        m.key = s.key;
+        m.cc = s.cc;
+        m.normal = s.normal;
+        for (int c = 0; c < s.cc; ++c) {
+          Contact<R> ct;
+          ct.pos = s.pos[c];
+          // extraction cap of the SAT path (:1575-1578); the voxel path caps its own depths
+          ct.pen = vox ? s.pen[c] : std::max(s.pen[c], R(p.penetration_cap));
+          ct.fp = s.fp[c];
+          m.c[c] = ct;
         }
+        m.anchor_a = A.pos;
+        m.anchor_b = B.pos;
+        m.error = 0x7FFFFFFF;
+        compute_basis(m);
+        if (warm) {
+          // find_old_collision (collision_detection.slang:914-963): voxel manifolds match their
+          // own key in the same body order only; others any key, either order
+          if (vox) {
+            auto it = prev_voxel_index.find(std::make_tuple(ida, idb, m.key));
+            if (it != prev_voxel_index.end()) update_from_old(m, prev_manifolds[it->second], false);
+          } else {
+            uint64_t key = (uint64_t(std::min(ida, idb)) << 32) | std::max(ida, idb);
+            auto it = prev_pair_index.find(key);
+            if (it != prev_pair_index.end()) {
+              const Manifold<R>& old = prev_manifolds[it->second];
+              update_from_old(m, old, old.a != ida);
+            }
+          }
+        }
+        have[k] |= uint8_t(1u << code);
       }
-      have[k] = 1;
     }, 64);
     manifolds.clear();
     for (size_t k = 0; k < P; ++k)
-      if (have[k]) manifolds.push_back(per[k]);
+      for (uint32_t code = 0; code < 6; ++code)
+        if (have[k] & (1u << code)) manifolds.push_back(per[k][code]);
     skip_warm_once = false;
     // per-body manifold lists in ascending manifold order (body_link_manifold :881-905)
     lists.assign(n(), {});
@@ -1112,9 +1135,11 @@ template <class R> class World {
     order = sorted_ids;
     prev_manifolds = manifolds;
     prev_pair_index.clear();
+    prev_voxel_index.clear();
     for (uint32_t m = 0; m < prev_manifolds.size(); ++m) {
       const auto& mf = prev_manifolds[m];
-      prev_pair_index[(uint64_t(std::min(mf.a, mf.b)) << 32) | std::max(mf.a, mf.b)] = m;
+      if (mf.key >= VOXEL_KEY0 && mf.key < VOXEL_KEY0 + 6) prev_voxel_index[std::make_tuple(mf.a, mf.b, mf.key)] = m;
+      else prev_pair_index[(uint64_t(std::min(mf.a, mf.b)) << 32) | std::max(mf.a, mf.b)] = m;
     }
   }
 

@@ -84,6 +84,10 @@ def lib():
         L.orc_morton.restype = ctypes.c_uint32
         L.orc_morton.argtypes = [P, P, P]
         L.orc_leaf_aabb.argtypes = [ctypes.c_uint32, P, P, P, P]
+        L.orc_add_voxel_shape.restype = ctypes.c_uint32
+        L.orc_add_voxel_shape.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, P]
+        L.orc_set_voxel_bodies.argtypes = [P, P, P]
+        L.orc_voxel_shape.argtypes = [P, ctypes.c_uint32, P, P, P]
         L.orc_collide_pair.restype = ctypes.c_int
         L.orc_collide_pair.argtypes = [ctypes.c_uint32, P, P, P, ctypes.c_uint32, P, P, P, ctypes.c_int, P, P, P, P]
         _lib = L
@@ -118,6 +122,14 @@ class Oracle:
                               _ptr(arr["shape"]), _ptr(arr["half"]), _ptr(arr["flags"]), _ptr(arr["mass"]),
                               _ptr(arr["inv_mass"]), _ptr(arr["inv_inertia"]), _ptr(arr["friction"]),
                               _ptr(arr["restitution"]), 1 if double else 0, int(threads))
+        if scene.get("voxel_shapes") or "inv_inertia_off" in scene:
+            for v in scene.get("voxel_shapes", []):
+                g = np.ascontiguousarray(np.asarray(v["solid"]) != 0, dtype=np.uint8)
+                nz, ny, nx = g.shape
+                L.orc_add_voxel_shape(self.h, nx, ny, nz, float(v["voxel_size"]), _ptr(g))
+            vidx = np.ascontiguousarray(scene.get("voxel", np.zeros(n)), dtype=np.uint32)
+            off = np.ascontiguousarray(scene.get("inv_inertia_off", np.zeros((n, 3))), dtype=np.float32)
+            L.orc_set_voxel_bodies(self.h, _ptr(vidx), _ptr(off))
         if params is not None:
             self.set_params(params)
 
@@ -156,6 +168,17 @@ class Oracle:
         buf = np.empty(cap, np.uint8)
         cnt = lib().orc_debug_read(self.h, which, _ptr(buf), buf.nbytes)
         return cnt, buf
+
+
+def voxel_shape(o: "Oracle", index: int) -> dict:
+    """The oracle's own build of a voxel shape: origin, box, counts and surface list."""
+    f9 = np.zeros(9, np.float32)
+    u2 = np.zeros(2, np.uint32)
+    lib().orc_voxel_shape(o.h, index, _ptr(f9), _ptr(u2), None)
+    surf = np.zeros(int(u2[1]), np.uint32)
+    lib().orc_voxel_shape(o.h, index, _ptr(f9), _ptr(u2), _ptr(surf))
+    return {"grid_origin": f9[:3], "box_min": f9[3:6], "box_max": f9[6:], "solid_count": int(u2[0]),
+            "surface_count": int(u2[1]), "surface": surf}
 
 
 def morton(p, wmin, wext) -> int:
