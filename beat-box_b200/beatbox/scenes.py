@@ -363,9 +363,10 @@ def voxel_pile(n_bodies: int = 60, seed: int = 0, voxel_size: float = 0.2, densi
     jittered on a grid (spacing and layer apart, so no two overlap at the start) over a static
     ground box (top at y = 0)."""
     sb = SceneBuilder()
-    sb.add_static_box([0, -50, 0], [50, 50, 50], friction=friction)
-    shapes = [sb.add_voxel_shape(g, voxel_size) for g in (voxel_l_shape(), voxel_cross(), voxel_frame())]
     per = max(1, int(math.ceil(math.sqrt(n_bodies / 3.0))))
+    ground = max(50.0, 0.5 * spacing * per + 10.0)
+    sb.add_static_box([0, -ground, 0], [ground, ground, ground], friction=friction)
+    shapes = [sb.add_voxel_shape(g, voxel_size) for g in (voxel_l_shape(), voxel_cross(), voxel_frame())]
     k = np.arange(n_bodies)
     lay, rem = k // (per * per), k % (per * per)
     gx, gz = rem % per, rem // per
@@ -378,4 +379,7 @@ def voxel_pile(n_bodies: int = 60, seed: int = 0, voxel_size: float = 0.2, densi
         sel = k % len(shapes) == si
         if sel.any():
             sb.add_voxel(pos[sel], quat[sel], shapes[si], BODY_DYNAMIC | BODY_GRAVITY, density, friction)
+    top = height + (int(lay.max()) + 2) * layer if n_bodies else height
+    span = 0.5 * spacing * per + 4.0
+    sb.bounds = ([-span, -2.0, -span], [2 * span, top + 4.0, 2 * span])
     return sb.build()

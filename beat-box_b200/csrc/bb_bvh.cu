@@ -41,8 +41,10 @@ __device__ __forceinline__ uint32_t morton_code(float3 p, const float wmin[3], c
 }
 
 // RigidBody::get_AABB_from_OBB (src/shaders/extensions.slang:195-210): the 8 corners of the
-// box rotated by the quaternion sandwich q c q* (include/shared.inl:455-475) plus position.
-__device__ __forceinline__ void leaf_box(float4 shp, float4 p4, float4 q4, float4& mn, float4& mx) {
+// box [minimum, maximum] rotated by the quaternion sandwich q c q* (include/shared.inl:455-475)
+// plus position.  Boxes have [minimum, maximum] = [-half, half]; voxel bodies their grid box,
+// which is off-centre (the body origin is the centre of mass).
+__device__ __forceinline__ void leaf_box(const DevState& d, float4 shp, float4 p4, float4 q4, float4& mn, float4& mx) {
   uint32_t type = __float_as_uint(shp.w);
   if (type == BB_SHAPE_SPHERE) {
     float r = shp.x;
@@ -50,23 +52,33 @@ __device__ __forceinline__ void leaf_box(float4 shp, float4 p4, float4 q4, float
     mx = make_float4(__fadd_rn(p4.x, r), __fadd_rn(p4.y, r), __fadd_rn(p4.z, r), 0.f);
     return;
   }
+  float lo[3] = {-shp.x, -shp.y, -shp.z}, hi[3] = {shp.x, shp.y, shp.z};
+  if (BB_SHAPE_KIND(type) == BB_SHAPE_VOXEL) {
+    const VoxDev& v = d.vox[BB_SHAPE_VOXEL_INDEX(type)];
+    lo[0] = v.ox;
+    lo[1] = v.oy;
+    lo[2] = v.oz;
+    hi[0] = v.hx;
+    hi[1] = v.hy;
+    hi[2] = v.hz;
+  }
   Quatf q = q_from(q4);
   Quatf qc = q_conj(q);
-  float lo[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
-  float hi[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+  float blo[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+  float bhi[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    Quatf c{(i & 1) ? shp.x : -shp.x, (i & 2) ? shp.y : -shp.y, (i & 4) ? shp.z : -shp.z, 0.f};
+    Quatf c{(i & 1) ? hi[0] : lo[0], (i & 2) ? hi[1] : lo[1], (i & 4) ? hi[2] : lo[2], 0.f};
     Quatf r = q_mul_exact(q_mul_exact(q, c), qc);
     float w[3] = {__fadd_rn(r.x, p4.x), __fadd_rn(r.y, p4.y), __fadd_rn(r.z, p4.z)};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      lo[k] = w[k] < lo[k] ? w[k] : lo[k];
-      hi[k] = w[k] > hi[k] ? w[k] : hi[k];
+      blo[k] = w[k] < blo[k] ? w[k] : blo[k];
+      bhi[k] = w[k] > bhi[k] ? w[k] : bhi[k];
     }
   }
-  mn = make_float4(lo[0], lo[1], lo[2], 0.f);
-  mx = make_float4(hi[0], hi[1], hi[2], 0.f);
+  mn = make_float4(blo[0], blo[1], blo[2], 0.f);
+  mx = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
 __device__ __forceinline__ bool box_overlap(float4 amn, float4 amx, float4 bmn, float4 bmx) {
@@ -148,7 +160,7 @@ __global__ void k_build(const DevState d, uint32_t n) {
   uint32_t id = d.vals[0][i];
   d.rank[id] = i;
   float4 mn, mx;
-  leaf_box(d.shape[id], d.pos[id], d.rot[id], mn, mx);
+  leaf_box(d, d.shape[id], d.pos[id], d.rot[id], mn, mx);
   uint32_t leaf = n - 1 + i;
   d.node_box[2 * leaf] = mn;
   d.node_box[2 * leaf + 1] = mx;
@@ -533,11 +545,11 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
       if (t == 0) s_size = total;
       uint32_t total_work;
       block_scan_nt<BB_HV_THREADS>(work, s_warp, total_work);  // ends with a CTA barrier
-      // stop expanding once the entries are leaves, once a level no longer widens the
-      // frontier (a thin overlap set: walking each entry down is cheaper than a block-wide
-      // level per tree level), or once there are enough entries for the GPU, each with a
-      // short walk left
-      if (!more || total <= size || (total >= BB_FRONTIER && total_work <= 32u * total)) break;
+      // stop expanding once the entries are leaves or each entry's walk is short (32 leaves
+      // under an entry on average), whatever the frontier's width: a thin overlap set (a wall)
+      // then stops after about log2(N / 32) levels instead of descending the whole tree one
+      // block-wide level at a time
+      if (!more || total_work <= 32u * total) break;
     }
     const uint32_t size = s_size;
     if (t == 0) {

@@ -46,6 +46,10 @@ def workload(args):
         sc = scenes.pyramids(n_pyramids=n_pyr, boxes_per=1000, seed=0)
         name = (f"pyramids_{n_pyr}x1000: {n_pyr} pyramids of 1000 unit boxes (base 18x18) on a 32x32 grid, "
                 f"velocity N(0, 0.01) m/s, dt=1/60, {SUBSTEPS} substeps, ")
+    elif args.scene == "voxel_pile":
+        sc = scenes.voxel_pile(n_bodies=args.bodies, seed=0)
+        name = (f"voxel_pile_{args.bodies // 1000}k: {args.bodies} concave voxel bodies (L / cross / frame, "
+                f"0.2 m cells, random orientation) in 3 layers over a ground box, dt=1/60, {SUBSTEPS} substeps, ")
     elif args.scene == "box_grid":
         sc = scenes.box_grid(n_side=10, seed=0)
         sc["bounds"] = ([-64.0] * 3, [128.0] * 3)  # the reference's Morton box
@@ -207,7 +211,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     fields = solver_fields(args)
 
     def make_world():
-        w = bb.World(sc["n"], pairs_per_body=16, device=local_rank)
+        # a voxel pair takes six manifold slots (one per face direction)
+        w = bb.World(sc["n"], pairs_per_body=64 if args.scene == "voxel_pile" else 16, device=local_rank)
         w.add_scene(sc)
         p = bb.default_params()
         p.world_min[:] = sc["bounds"][0]
@@ -573,9 +578,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="pgs", choices=["pgs", "avbd"])
     ap.add_argument("--bodies", type=int, default=N_BODIES)
-    ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids", "box_grid"],
+    ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids", "box_grid", "voxel_pile"],
                     help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids; "
-                         "box_grid: the 1000-box grid")
+                         "box_grid: the 1000-box grid; voxel_pile: concave voxel bodies")
     ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
