@@ -456,11 +456,15 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
 // scan over the pool, walk again to emit), so one query's walk is spread over the GPU.  The
 // frontier keeps left-to-right order and each entry covers a contiguous leaf range, so the
 // concatenated walks emit ascending partners, as the single-thread traversal does.  A query
-// whose frontier does not fit the pool falls back to k_broad_heavy (hv_n = BB_NONE).
+// whose frontier does not fit the pool, or whose world or remaining frontier covers few leaves,
+// goes to k_broad_heavy (hv_n = BB_NONE).
 // Thread t holds frontier entries [4t, 4t+4); the loads of all four (child, then child range
 // and box) are issued together, so a level costs a few load latencies whatever its size.
 #define BB_HV_THREADS 1024
 #define BB_HV_PER_THREAD 4
+// Queries whose world (or remaining frontier) covers at most this many leaves go to the block
+// traversal k_broad_heavy: its 256-entry frontier then leaves at most 512 leaves per walk.
+#define BB_HV_BLOCK_LEAVES (512u * BB_FRONTIER)
 #define BB_HV_FRONTIER (BB_HV_THREADS * BB_HV_PER_THREAD)
 
 __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState d, uint32_t n) {
@@ -474,12 +478,19 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
     const uint32_t qi = d.heavy_list[slot];
     const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
     const int wend = world_end(d, qi, n);
+    const int wbeg = d.n_worlds > 1 ? int(d.world_first[d.sworld[qi]]) : 0;
+    if (uint32_t(wend - wbeg) <= BB_HV_BLOCK_LEAVES) {  // a world this small: block traversal
+      if (t == 0) d.hv_n[slot] = BB_NONE;
+      __syncthreads();
+      continue;
+    }
     if (t == 0) {
       s_fr[0][0] = 0;
       s_size = 1;
     }
     __syncthreads();
     int cur = 0;
+    bool block_path = false;
     for (int level = 0; level < 64; ++level) {
       const uint32_t size = s_size;
       int node[BB_HV_PER_THREAD];
@@ -550,6 +561,17 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
       // then stops after about log2(N / 32) levels instead of descending the whole tree one
       // block-wide level at a time
       if (!more || total_work <= 32u * total) break;
+      // few leaves left under the frontier: a block traversal (k_broad_heavy) costs less than
+      // more levels here plus a pool walk; the pool is for queries over very many leaves
+      if (total_work <= BB_HV_BLOCK_LEAVES) {
+        block_path = true;
+        break;
+      }
+    }
+    if (block_path) {
+      if (t == 0) d.hv_n[slot] = BB_NONE;
+      __syncthreads();
+      continue;
     }
     const uint32_t size = s_size;
     if (t == 0) {

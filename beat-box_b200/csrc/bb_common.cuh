@@ -60,11 +60,10 @@ struct DevCounters {
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
                            // 7 connected components
-  uint32_t np_counts[3];   // narrow-phase work lists: box-box, with a sphere, with a voxel body
+  uint32_t np_counts[4];   // narrow-phase work lists: box-box, with a sphere, voxel pairs, carried
   uint32_t gc_list_n[2];   // edge colouring: sizes of the alternating uncoloured-manifold lists
   uint32_t hv_pool_n;      // broad phase: frontier entries of the heavy queries
   uint32_t slot_count;     // worlds with voxel shapes: manifold slots (6 per voxel pair, else 1)
-  uint32_t pad2[1];
 };
 
 // Voxel shape on the device (VoxelShape, include/shared.inl:938-951) with the body-frame box
@@ -152,6 +151,7 @@ struct DevState {
   unsigned long long* gc_owner; // per body x 32 colours: (epoch << 32) | priority
   uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies
   uint32_t* bucket_start; // 34 + 32*L entries
+  uint32_t* colour_awake; // per colour (32 = overflow): 1 if one of its manifolds has an awake body
   // AVBD
   uint32_t* body_color;   // per body
   uint32_t* body_color_round;
@@ -189,6 +189,8 @@ struct DevState {
   uint32_t* slot_pair;     // per slot: pair << 3 | face code
   uint32_t* vox_list;      // narrow-phase work list of the voxel slots
   float4* iinv_off;        // per body: body-frame inverse inertia off-diagonal (xy, xz, yz, -)
+  uint32_t* frozen;        // per body: 1 if asleep or static at the last narrow phase, state unwritten since
+  uint32_t* carry_list;    // narrow-phase work list of the frozen pairs
 };
 
 // ---- small vector helpers -------------------------------------------------------------------

@@ -410,29 +410,39 @@ __global__ void k_slot_fill(const DevState d) {
   }
 }
 
+__device__ __forceinline__ bool np_awake(uint32_t f) { return (f & BB_BODY_DYNAMIC) && !(f & BB_BODY_SLEEPING); }
+
 // Work lists of the narrow phase: box-box slots from the front of np_list, slots with a sphere
-// from the back, voxel slots in vox_list, static-static pairs (:1525) nowhere.  Every slot
-// starts as "no manifold".  Grouping by shape keeps the warps of k_narrow on one code path
-// (the box-box clip is long, the sphere cases short); the outputs go to each slot's own place,
-// so the order in which the lists fill does not matter.
-__global__ void k_np_classify(const DevState d, int cur) {
+// from the back, voxel pairs (their code-0 slot) in vox_list, frozen pairs (their first slot)
+// in carry_list, static-static pairs (:1525) nowhere.  A pair is frozen when neither body is
+// awake and both were asleep or static at the last narrow phase too, so both poses are those
+// of the previous substep bit for bit.  Every slot starts as "no manifold".  Grouping by shape
+// keeps the warps of k_narrow on one code path (the box-box clip is long, the sphere cases
+// short); the outputs go to each slot's own place, so the order in which the lists fill does
+// not matter.
+__global__ void k_np_classify(const DevState d, int cur, int warm) {
   const uint32_t S = slot_total(d);
   const int lane = threadIdx.x & 31;
   for (uint32_t base = blockIdx.x * blockDim.x; base < S; base += gridDim.x * blockDim.x) {
     const uint32_t k = base + threadIdx.x;
-    int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body
+    int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body, 3 frozen
     if (k < S) {
       d.hit[k] = 0;
       d.m_keycc[cur][k] = make_int2(-1, 0);
       const uint2 pr = d.pairs[slot_pair_of(d, k)];
       const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
-      if ((d.flags[ida] & BB_BODY_DYNAMIC) || (d.flags[idb] & BB_BODY_DYNAMIC)) {
+      const uint32_t fa = d.flags[ida], fb = d.flags[idb];
+      if ((fa & BB_BODY_DYNAMIC) || (fb & BB_BODY_DYNAMIC)) {
         const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
-        kind = (ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL) ? 2 : ((ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1);
+        const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
+        const bool first = !vox || (d.slot_pair[k] & 7u) == 0u;  // a voxel pair is listed once
+        if (warm && !np_awake(fa) && !np_awake(fb) && d.frozen[ida] && d.frozen[idb]) kind = first ? 3 : -1;
+        else if (vox) kind = first ? 2 : -1;
+        else kind = (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1;
       }
     }
 #pragma unroll
-    for (int kd = 0; kd < 3; ++kd) {
+    for (int kd = 0; kd < 4; ++kd) {
       const unsigned mask = __ballot_sync(0xFFFFFFFFu, kind == kd);
       if (!mask) continue;
       uint32_t off = 0;
@@ -440,9 +450,84 @@ __global__ void k_np_classify(const DevState d, int cur) {
       off = __shfl_sync(0xFFFFFFFFu, off, 0);
       if (kind == kd) {
         const uint32_t r = off + uint32_t(__popc(mask & ((1u << lane) - 1u)));
-        if (kd == 2) d.vox_list[r] = k;
+        if (kd == 3) d.carry_list[r] = k;
+        else if (kd == 2) d.vox_list[r] = k;
         else d.np_list[kd == 0 ? r : S - 1 - r] = k;
       }
+    }
+  }
+}
+
+// Carry-over of a frozen pair: its manifold(s) of the previous substep in the same body order
+// (voxel pairs: each face key into its own slot) are kept as they were -- contacts, features,
+// impulses, penalties, stick anchors -- with warm-start counts + 1 and the extraction trend 0,
+// which is what recomputing the same poses and matching every contact by feature gives.  A
+// frozen pair without a manifold last substep goes to the ordinary lists and is computed.
+__device__ __forceinline__ void carry_copy(const DevState& d, int cur, uint32_t os, uint32_t dst, uint32_t ida,
+                                           uint32_t idb) {
+  const int prv = cur ^ 1;
+  const int2 kc = d.m_keycc[prv][os];
+  const float4 n4 = d.m_normal[prv][os];
+  d.m_bodies[cur][dst] = make_uint2(ida, idb);
+  d.m_keycc[cur][dst] = kc;
+  d.m_normal[cur][dst] = make_float4(n4.x, n4.y, n4.z, __int_as_float(0));
+  d.m_t0[cur][dst] = d.m_t0[prv][os];
+  d.m_t1[cur][dst] = d.m_t1[prv][os];
+  const float4 pa = d.pos[ida], pb = d.pos[idb];
+  d.m_anchor_a[cur][dst] = make_float4(pa.x, pa.y, pa.z, 0.f);
+  d.m_anchor_b[cur][dst] = make_float4(pb.x, pb.y, pb.z, 0.f);
+  for (int c = 0; c < kc.y; ++c) {
+    const uint32_t oi = os * BB_MAX_CONTACTS + c, ni = dst * BB_MAX_CONTACTS + c;
+    d.c_pos[cur][ni] = d.c_pos[prv][oi];
+    d.c_lam[cur][ni] = d.c_lam[prv][oi];
+    float4 kt = d.c_kt[prv][oi];
+    kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
+    d.c_kt[cur][ni] = kt;
+    const bool stick = __float_as_uint(kt.z) != 0u;
+    const float4 aa = d.c_anc_a[prv][oi], ab = d.c_anc_b[prv][oi];
+    d.c_anc_a[cur][ni] = stick ? aa : make_float4(0.f, 0.f, 0.f, aa.w);
+    d.c_anc_b[cur][ni] = stick ? make_float4(ab.x, ab.y, ab.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  d.hit[dst] = 1;
+}
+
+__global__ void k_narrow_carry(const DevState d, int cur) {
+  const int prv = cur ^ 1;
+  const uint32_t S = slot_total(d);
+  const uint32_t nc = d.ctr->np_counts[3];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
+    const uint32_t s = d.carry_list[t];
+    const uint2 pr = d.pairs[slot_pair_of(d, s)];
+    const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
+    const uint32_t fa = d.flags[ida];
+    const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
+    const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
+    const uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb, other = x == ida ? idb : ida;
+    const uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
+    bool any = false;
+    for (uint32_t e = s0; e < s1; ++e) {
+      if (d.csr_partner[prv][e] != other) continue;
+      const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
+      if (d.m_bodies[prv][os].x != ida) continue;  // same body order only
+      const int key = d.m_keycc[prv][os].x;
+      if (vox) {
+        if (key < 90 || key > 95) continue;
+        carry_copy(d, cur, os, s + uint32_t(key - 90), ida, idb);
+        any = true;
+      } else {
+        carry_copy(d, cur, os, s, ida, idb);
+        any = true;
+        break;
+      }
+    }
+    if (any) continue;
+    // no manifold last substep: compute the pair with the others
+    if (vox) {
+      d.vox_list[atomicAdd(&d.ctr->np_counts[2], 1u)] = s;
+    } else if (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) {
+      d.np_list[atomicAdd(&d.ctr->np_counts[0], 1u)] = s;
+    } else {
+      d.np_list[S - 1 - atomicAdd(&d.ctr->np_counts[1], 1u)] = s;
     }
   }
 }
@@ -722,27 +807,153 @@ __device__ bool vox_corner_supported(const DevState& d, float3 pt, float3 n_sep,
   return fabsf(lu) <= hu + 0.01f && fabsf(lv) <= hv + 0.01f;
 }
 
-struct VWin {  // one reducer slot
-  float3 pos, nrm;
+struct VWin {  // one reducer slot: the winning sample of one extreme direction
+  float3 pos;
   float pen, score;
   uint32_t fa, fb;
 };
-// rank of a slot's sample: (score bucket desc, depth bucket asc, voxel id asc); empty ranks last
-__device__ __forceinline__ bool vwin_better(bool ea, int sa, int pa, uint32_t fa, bool eb, int sb, int pb, uint32_t fb) {
-  if (ea) return false;
-  if (eb) return true;
-  return sa > sb || (sa == sb && (pa < pb || (pa == pb && fa < fb)));
+// Rank of a reducer slot's sample as two 32-bit words for warp max-reductions: hi = (score
+// bucket + 2^15) << 16 | (2^15 - 1 - depth bucket), lo = 2^24 - fa (lower voxel id wins).  Empty
+// slots rank 0.  Buckets are clamped to 15 bits (|local coordinate| < 3276 half-voxels).
+__device__ __forceinline__ uint32_t vrank_hi(const VWin& w, float quant) {
+  if (w.pen > 0.5e9f) return 0u;
+  const int sb = min(max(int(floorf(w.score / quant)), -32767), 32767);
+  const int pb = min(max(int(floorf(w.pen / quant)), -32767), 32767);
+  return (uint32_t(sb + 32768) << 16) | uint32_t(32767 - pb);
+}
+__device__ __forceinline__ uint32_t vrank_lo(const VWin& w) { return w.pen > 0.5e9f ? 0u : (1u << 24) - w.fa; }
+
+// One sample's code-independent geometry (a surface cell centre of the sampled body).
+struct VSample {
+  float3 pw, l2;  // world position; position in r2's frame (minus r2's box centre when r2 is a box)
+  int c[3];       // r2's cell (voxel r2)
+  bool occ;       // that cell is solid (voxel r2)
+  float best;     // shallowest exit over the near faces (voxel r2, occupied cell); 1e9: interior
+  float3 dl;      // offset from the cell centre (voxel r2, occupied cell)
+  float3 q;       // |l2| - half (box r2)
+  uint32_t fa;    // sampled voxel id
+};
+
+__device__ __forceinline__ void vox_sample_geom(const DevState& d, const VBody& r1, const VoxDev& s1, const VBody& r2,
+                                                bool s2_vox, const VoxDev& s2, float3 sup, float3 half2, float3 co2,
+                                                uint32_t i, VSample& g) {
+  const float vs1 = s1.vs;
+  const uint32_t e = __ldg(&d.vox_surf[s1.surf_off + i]);
+  g.fa = e & 0xFFFFFFu;
+  const float3 local = make_float3(s1.ox + (float(e & 0xFFu) + 0.5f) * vs1, s1.oy + (float((e >> 8) & 0xFFu) + 0.5f) * vs1,
+                                   s1.oz + (float((e >> 16) & 0xFFu) + 0.5f) * vs1);
+  g.pw = r1.p + mat_mul(r1.R, local);
+  const float3 l2w = mat_tmul(r2.R, g.pw - r2.p);
+  if (s2_vox) {
+    g.l2 = l2w;
+    const float vs2 = s2.vs;
+    const float3 gg = make_float3((l2w.x - s2.ox) / vs2, (l2w.y - s2.oy) / vs2, (l2w.z - s2.oz) / vs2);
+    g.c[0] = int(floorf(gg.x));
+    g.c[1] = int(floorf(gg.y));
+    g.c[2] = int(floorf(gg.z));
+    g.occ = vox_bit(d, s2, g.c[0], g.c[1], g.c[2]);
+    g.best = 1e9f;
+    g.dl = make_float3(0.f, 0.f, 0.f);
+    if (g.occ) {
+      // cell-face contact (:1185-1208): the shallowest feasible exit over the near faces
+      const float3 org2 = make_float3(s2.ox, s2.oy, s2.oz);
+      g.dl = l2w - (org2 + (make_float3(float(g.c[0]), float(g.c[1]), float(g.c[2])) + make_float3(0.5f, 0.5f, 0.5f)) * vs2);
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const float di = comp(g.dl, ax);
+        int nb[3] = {g.c[0], g.c[1], g.c[2]};
+        nb[ax] += di >= 0.f ? 1 : -1;
+        if (vox_bit(d, s2, nb[0], nb[1], nb[2])) continue;
+        const float ov = (0.5f * vs2 + comp(sup, ax)) - fabsf(di);
+        if (ov < g.best) g.best = ov;
+      }
+    }
+  } else {
+    g.l2 = l2w - co2;
+    g.q = make_float3(fabsf(g.l2.x) - half2.x, fabsf(g.l2.y) - half2.y, fabsf(g.l2.z) - half2.z);
+  }
 }
 
+// The sample's membership in pass `code` (axis axk, sign sgn) and its depth (:1148-1266);
+// returns false when it does not join.  `interior` is set for occupied cells with no exit.
+__device__ __forceinline__ bool vox_sample_pass(const DevState& d, const VSample& g, bool s2_vox, const VoxDev& s2,
+                                                float3 sup, float3 half2, float vs1, uint32_t axk, float sgn, int isgn,
+                                                float& pe, uint32_t& fb, bool& interior) {
+  interior = false;
+  const float sup_a = comp(sup, int(axk));
+  if (s2_vox) {
+    const float vs2 = s2.vs;
+    if (!g.occ) {
+      // hover band: centre in an empty cell just outside an occupied one (:1155-1183)
+      int ci[3] = {g.c[0], g.c[1], g.c[2]};
+      ci[axk] -= isgn;
+      if (!vox_bit(d, s2, ci[0], ci[1], ci[2])) return false;
+      const float org_a = axk == 0 ? s2.ox : (axk == 1 ? s2.oy : s2.oz);
+      const float dh = comp(g.l2, int(axk)) - (org_a + (float(ci[axk]) + 0.5f) * vs2);
+      const float ovh = (0.5f * vs2 + sup_a) - sgn * dh;
+      pe = -ovh;
+      fb = pack_cell(ci[0], ci[1], ci[2]);
+    } else {
+      if (g.best > 0.5e9f) {
+        interior = true;
+        return false;
+      }
+      int pn[3] = {g.c[0], g.c[1], g.c[2]};
+      pn[axk] += isgn;
+      if (vox_bit(d, s2, pn[0], pn[1], pn[2])) return false;  // the pass axis is no exit here
+      const float ovp = (0.5f * vs2 + sup_a) - sgn * comp(g.dl, int(axk));
+      if (ovp > g.best + 0.15f * vs2) return false;  // dominated by a shallower exit
+      pe = -ovp;
+      fb = pack_cell(g.c[0], g.c[1], g.c[2]);
+    }
+  } else {
+    // r2 is a box: sample centre with support radius against the box faces (:1235-1258)
+    if (g.q.x > sup.x || g.q.y > sup.y || g.q.z > sup.z) return false;
+    const float3 qs = g.q - sup;
+    const float best_q = fmaxf(qs.x, fmaxf(qs.y, qs.z));
+    const float q_pass = sgn * comp(g.l2, int(axk)) - comp(half2, int(axk)) - sup_a;
+    if (q_pass < best_q - 0.15f * vs1) return false;
+    pe = q_pass;
+    fb = axk;
+  }
+  if (pe >= 0.02f) return false;  // margin band
+  pe = fmaxf(pe, s2_vox ? -0.5f * vs1 : -vs1);  // depth caps (:1262-1266)
+  return true;
+}
+
+// VoxelManifoldReducer::add (:1064-1092)
+__device__ __forceinline__ void vox_reduce_add(VWin w[4], float3 pw, float pe, uint32_t fa, uint32_t fb, float su, float sv,
+                                               float quant) {
+  const float sc4[4] = {su + sv, su - sv, -su + sv, -su - sv};
+  const int nbk = int(floorf(pe / quant));
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    const bool empty = w[o].pen > 0.5e9f;
+    const int nbs = int(floorf(sc4[o] / quant));
+    const int obs = empty ? -2147483640 : int(floorf(w[o].score / quant));
+    const int obk = empty ? 0 : int(floorf(w[o].pen / quant));
+    if (empty || nbs > obs || (nbs == obs && (nbk < obk || (nbk == obk && fa < w[o].fa)))) {
+      w[o].pos = pw;
+      w[o].pen = pe;
+      w[o].fa = fa;
+      w[o].fb = fb;
+      w[o].score = sc4[o];
+    }
+  }
+}
+
+// One warp per voxel pair.  The prefilter and each sample's geometry are computed once; the six
+// passes (face codes) then reuse them.  Per pass every lane ranks its own samples, a warp
+// max-reduction of the packed ranks picks each extreme direction's winner, and lane `code`
+// keeps the pass's winners.  Lanes 0..5 then build and store the six manifolds in parallel.
+#define BB_VOX_CACHE 32  // samples whose geometry stays in registers (one per lane)
 __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p, int cur, int warm) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t nv = d.ctr->np_counts[2];
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < nv; t += warps) {
-    const uint32_t slot = d.vox_list[t];
-    const uint32_t sp = d.slot_pair[slot];
-    const uint32_t code = sp & 7u;
-    const uint2 pr = d.pairs[sp >> 3];
+    const uint32_t slot0 = d.vox_list[t];  // the pair's code-0 slot; codes 1..5 follow it
+    const uint2 pr = d.pairs[d.slot_pair[slot0] >> 3];
     const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
     VBody A, B;
     vbody(d, ida, A);
@@ -757,7 +968,7 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
     const VoxDev s1 = d.vox[r1.vi];
     VoxDev s2 = {};
     if (s2_vox) s2 = d.vox[r2.vi];
-    const float vs1 = s1.vs;
+    const float vs1 = s1.vs, quant = 0.5f * vs1;
     // per-axis support radius of a rotated sample cell in r2's frame (:1110-1117)
     float A12[3][3];  // r2^T r1
     for (int i = 0; i < 3; ++i)
@@ -765,153 +976,75 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
     const float3 sup = make_float3(fabsf(A12[0][0]) + fabsf(A12[0][1]) + fabsf(A12[0][2]),
                                    fabsf(A12[1][0]) + fabsf(A12[1][1]) + fabsf(A12[1][2]),
                                    fabsf(A12[2][0]) + fabsf(A12[2][1]) + fabsf(A12[2][2])) * (0.5f * vs1);
-    const uint32_t axk = code >> 1;
-    const float sgn = (code & 1u) ? 1.f : -1.f;
-    const int isgn = (code & 1u) ? 1 : -1;
-    const float sup_a = comp(sup, int(axk));
     const float3 half2 = (r2.hi - r2.lo) * 0.5f, co2 = (r2.hi + r2.lo) * 0.5f;
-    const float3 org2 = make_float3(s2.ox, s2.oy, s2.oz);
-    const float vs2 = s2.vs;
-    const float quant = 0.5f * vs1;
-    const float3 n_out = mat_col(r2.R, int(axk)) * sgn;  // the pass's face normal, world frame
-    VWin w[4];
-#pragma unroll
-    for (int o = 0; o < 4; ++o) {
-      w[o].pen = 1.0e9f;
-      w[o].score = -1.0e30f;
-      w[o].fa = 0;
-      w[o].fb = 0;
-      w[o].pos = make_float3(0, 0, 0);
-      w[o].nrm = make_float3(0, 0, 0);
-    }
-    uint32_t samples = 0, interior = 0;
-    for (uint32_t i = lane; i < s1.surf_count; i += 32u) {
-      const uint32_t e = __ldg(&d.vox_surf[s1.surf_off + i]);
-      const float3 local = make_float3(s1.ox + (float(e & 0xFFu) + 0.5f) * vs1, s1.oy + (float((e >> 8) & 0xFFu) + 0.5f) * vs1,
-                                       s1.oz + (float((e >> 16) & 0xFFu) + 0.5f) * vs1);
-      const float3 pw = r1.p + mat_mul(r1.R, local);
-      const float3 l2w = mat_tmul(r2.R, pw - r2.p);
-      float pe, su, sv;
-      uint32_t fb;
-      if (s2_vox) {
-        const float3 l2 = l2w;
-        su = axk == 0 ? l2.y : l2.x;
-        sv = axk == 2 ? l2.y : l2.z;
-        const float3 g = make_float3((l2.x - org2.x) / vs2, (l2.y - org2.y) / vs2, (l2.z - org2.z) / vs2);
-        int c[3] = {int(floorf(g.x)), int(floorf(g.y)), int(floorf(g.z))};
-        if (!vox_bit(d, s2, c[0], c[1], c[2])) {
-          // hover band: centre in an empty cell just outside an occupied one (:1155-1183)
-          int ci[3] = {c[0], c[1], c[2]};
-          ci[axk] -= isgn;
-          if (!vox_bit(d, s2, ci[0], ci[1], ci[2])) continue;
-          const float dh = comp(l2, int(axk)) - (comp(org2, int(axk)) + (float(ci[axk]) + 0.5f) * vs2);
-          const float ovh = (0.5f * vs2 + sup_a) - sgn * dh;
-          pe = -ovh;
-          fb = pack_cell(ci[0], ci[1], ci[2]);
-        } else {
-          // cell-face contact (:1185-1222)
-          const float3 dl = l2 - (org2 + (make_float3(float(c[0]), float(c[1]), float(c[2])) + make_float3(0.5f, 0.5f, 0.5f)) * vs2);
-          float best = 1e9f;
-#pragma unroll
-          for (int ax = 0; ax < 3; ++ax) {
-            const float di = comp(dl, ax);
-            int nb[3] = {c[0], c[1], c[2]};
-            nb[ax] += di >= 0.f ? 1 : -1;
-            if (vox_bit(d, s2, nb[0], nb[1], nb[2])) continue;
-            const float ov = (0.5f * vs2 + comp(sup, ax)) - fabsf(di);
-            if (ov < best) best = ov;
-          }
-          if (best > 0.5e9f) {
-            ++interior;
-            continue;
-          }
-          int pn[3] = {c[0], c[1], c[2]};
-          pn[axk] += isgn;
-          if (vox_bit(d, s2, pn[0], pn[1], pn[2])) continue;
-          const float ovp = (0.5f * vs2 + sup_a) - sgn * comp(dl, int(axk));
-          if (ovp > best + 0.15f * vs2) continue;
-          pe = -ovp;
-          fb = pack_cell(c[0], c[1], c[2]);
-        }
-      } else {
-        // r2 is a box: sample centre with support radius against the box faces (:1235-1258)
-        const float3 l2 = l2w - co2;
-        su = axk == 0 ? l2.y : l2.x;
-        sv = axk == 2 ? l2.y : l2.z;
-        const float3 q = make_float3(fabsf(l2.x) - half2.x, fabsf(l2.y) - half2.y, fabsf(l2.z) - half2.z);
-        if (q.x > sup.x || q.y > sup.y || q.z > sup.z) continue;
-        const float3 qs = q - sup;
-        const float best_q = fmaxf(qs.x, fmaxf(qs.y, qs.z));
-        const float q_pass = sgn * comp(l2, int(axk)) - comp(half2, int(axk)) - sup_a;
-        if (q_pass < best_q - 0.15f * vs1) continue;
-        pe = q_pass;
-        fb = axk;
-      }
-      if (pe >= 0.02f) continue;  // margin band
-      pe = fmaxf(pe, s2_vox ? -0.5f * vs1 : -vs1);  // depth caps (:1262-1266)
-      // VoxelManifoldReducer::add (:1064-1092)
-      const float sc4[4] = {su + sv, su - sv, -su + sv, -su - sv};
-      const int nbk = int(floorf(pe / quant));
-      const uint32_t fa = e & 0xFFFFFFu;
+    VSample cache;
+    const bool cached = lane < s1.surf_count;
+    if (cached) vox_sample_geom(d, r1, s1, r2, s2_vox, s2, sup, half2, co2, lane, cache);
+    VWin mine[4];  // lane `code`: the winners of pass `code`
+    uint32_t my_samples = 0, my_interior = 0;
+#pragma unroll 1
+    for (uint32_t code = 0; code < 6; ++code) {
+      const uint32_t axk = code >> 1;
+      const float sgn = (code & 1u) ? 1.f : -1.f;
+      const int isgn = (code & 1u) ? 1 : -1;
+      VWin w[4];
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
-        const bool empty = w[o].pen > 0.5e9f;
-        const int nbs = int(floorf(sc4[o] / quant));
-        const int obs = empty ? -2147483640 : int(floorf(w[o].score / quant));
-        const int obk = empty ? 0 : int(floorf(w[o].pen / quant));
-        if (empty || nbs > obs || (nbs == obs && (nbk < obk || (nbk == obk && fa < w[o].fa)))) {
-          w[o].pos = pw;
-          w[o].pen = pe;
-          w[o].nrm = n_out;
-          w[o].fa = fa;
-          w[o].fb = fb;
-          w[o].score = sc4[o];
-        }
+        w[o].pen = 1.0e9f;
+        w[o].score = -1.0e30f;
+        w[o].fa = 0;
+        w[o].fb = 0;
+        w[o].pos = make_float3(0.f, 0.f, 0.f);
       }
-      ++samples;
-    }
-    samples = __reduce_add_sync(0xFFFFFFFFu, samples);
-    interior = __reduce_add_sync(0xFFFFFFFFu, interior);
-    // per reducer slot: the best lane's winner
-#pragma unroll
-    for (int o = 0; o < 4; ++o) {
-      bool em = w[o].pen > 0.5e9f;
-      int sb = em ? 0 : int(floorf(w[o].score / quant));
-      int pb = em ? 0 : int(floorf(w[o].pen / quant));
-      uint32_t fa = w[o].fa, src = lane;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const bool oe = __shfl_xor_sync(0xFFFFFFFFu, em, off);
-        const int os = __shfl_xor_sync(0xFFFFFFFFu, sb, off);
-        const int op = __shfl_xor_sync(0xFFFFFFFFu, pb, off);
-        const uint32_t of = __shfl_xor_sync(0xFFFFFFFFu, fa, off);
-        const uint32_t osrc = __shfl_xor_sync(0xFFFFFFFFu, src, off);
-        if (vwin_better(oe, os, op, of, em, sb, pb, fa)) {
-          em = oe;
-          sb = os;
-          pb = op;
-          fa = of;
-          src = osrc;
+      uint32_t samples = 0, interior = 0;
+      for (uint32_t i = lane; i < s1.surf_count; i += 32u) {
+        VSample g;
+        if (i < BB_VOX_CACHE) g = cache;
+        else vox_sample_geom(d, r1, s1, r2, s2_vox, s2, sup, half2, co2, i, g);
+        float pe;
+        uint32_t fb;
+        bool in;
+        if (!vox_sample_pass(d, g, s2_vox, s2, sup, half2, vs1, axk, sgn, isgn, pe, fb, in)) {
+          interior += in ? 1u : 0u;
+          continue;
         }
+        const float su = axk == 0 ? g.l2.y : g.l2.x, sv = axk == 2 ? g.l2.y : g.l2.z;
+        vox_reduce_add(w, g.pw, pe, g.fa, fb, su, sv, quant);
+        ++samples;
       }
-      w[o].pos.x = __shfl_sync(0xFFFFFFFFu, w[o].pos.x, src);
-      w[o].pos.y = __shfl_sync(0xFFFFFFFFu, w[o].pos.y, src);
-      w[o].pos.z = __shfl_sync(0xFFFFFFFFu, w[o].pos.z, src);
-      w[o].nrm.x = __shfl_sync(0xFFFFFFFFu, w[o].nrm.x, src);
-      w[o].nrm.y = __shfl_sync(0xFFFFFFFFu, w[o].nrm.y, src);
-      w[o].nrm.z = __shfl_sync(0xFFFFFFFFu, w[o].nrm.z, src);
-      w[o].pen = __shfl_sync(0xFFFFFFFFu, w[o].pen, src);
-      w[o].score = __shfl_sync(0xFFFFFFFFu, w[o].score, src);
-      w[o].fa = __shfl_sync(0xFFFFFFFFu, w[o].fa, src);
-      w[o].fb = __shfl_sync(0xFFFFFFFFu, w[o].fb, src);
+      samples = __reduce_add_sync(0xFFFFFFFFu, samples);
+      interior = __reduce_add_sync(0xFFFFFFFFu, interior);
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        const uint32_t hi = vrank_hi(w[o], quant), lo = vrank_lo(w[o]);
+        const uint32_t mh = __reduce_max_sync(0xFFFFFFFFu, hi);
+        const uint32_t ml = __reduce_max_sync(0xFFFFFFFFu, hi == mh ? lo : 0u);
+        const unsigned win = __ballot_sync(0xFFFFFFFFu, hi == mh && lo == ml);
+        const int src = __ffs(win) - 1;
+        VWin b;
+        b.pos.x = __shfl_sync(0xFFFFFFFFu, w[o].pos.x, src);
+        b.pos.y = __shfl_sync(0xFFFFFFFFu, w[o].pos.y, src);
+        b.pos.z = __shfl_sync(0xFFFFFFFFu, w[o].pos.z, src);
+        b.pen = __shfl_sync(0xFFFFFFFFu, w[o].pen, src);
+        b.score = __shfl_sync(0xFFFFFFFFu, w[o].score, src);
+        b.fa = __shfl_sync(0xFFFFFFFFu, w[o].fa, src);
+        b.fb = __shfl_sync(0xFFFFFFFFu, w[o].fb, src);
+        if (lane == code) mine[o] = b;
+      }
+      if (lane == code) {
+        my_samples = samples;
+        my_interior = interior;
+      }
     }
-    if (lane == 0) {  // the manifold and its store: serial, small
+    if (lane < 6) {  // the manifold of pass `lane` and its store: serial, small
+      const uint32_t code = lane, axk = code >> 1;
+      const float3 n_sep = mat_col(r2.R, int(axk)) * ((code & 1u) ? 1.f : -1.f);  // the face normal, world
       bool store = true;
       Contacts m;
       m.cc = 0;
       m.key = 90 + int(code);
-      if (samples == 0) {
-        store = code == 0 && interior > 0;
+      if (my_samples == 0) {
+        store = code == 0 && my_interior > 0;
         // deep-interpenetration rescue (:1487-1506): one centre-to-centre contact
         const float3 dd = r1.p - r2.p;
         const float3 n_res = dot3(dd, dd) > 1e-8f ? dd * (1.0f / len3(dd)) : make_float3(0.f, 1.f, 0.f);
@@ -921,23 +1054,19 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
         m.fp[0] = 0xFFFFFFu;
         m.cc = 1;
       } else {
-        // voxel_emit_manifold (:1330-1448)
-        const float3 n_sep = n_out;
+        // voxel_emit_manifold (:1330-1448); every sample of a pass has the normal n_sep
         m.normal = flip ? n_sep : -n_sep;
+        const float align = dot3(n_sep, n_sep);
         uint32_t kept[4];
-        float align_k[4];
         uint32_t kn = 0;
         for (uint32_t o = 0; o < 4; ++o) {
-          if (w[o].pen >= 0.02f) continue;
-          const float align = dot3(w[o].nrm, n_sep);
+          if (mine[o].pen >= 0.02f) continue;
           if (align <= 0.1f) continue;
           bool dup = false;
           for (uint32_t q = 0; q < kn; ++q)
-            if (w[kept[q]].fa == w[o].fa) dup = true;
+            if (mine[kept[q]].fa == mine[o].fa) dup = true;
           if (dup) continue;
-          kept[kn] = o;
-          align_k[kn] = align;
-          ++kn;
+          kept[kn++] = o;
         }
         const uint32_t reps = kn == 1 ? 4u : (kn == 2 ? 2u : 1u);
         float3 t1 = cross3(n_sep, fabsf(n_sep.y) < 0.9f ? make_float3(0.f, 1.f, 0.f) : make_float3(1.f, 0.f, 0.f));
@@ -946,7 +1075,7 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
         const float3 da = (t1 + t2) * (0.318f * vs1), db = (t1 - t2) * (0.318f * vs1);
         int n_emit = 0;
         for (uint32_t k2 = 0; k2 < kn; ++k2) {
-          const VWin& wo = w[kept[k2]];
+          const VWin& wo = mine[kept[k2]];
           const uint32_t vpar = (wo.fa ^ (wo.fa >> 8) ^ (wo.fa >> 16)) & 1u;
           float3 emitted[4];
           uint32_t en = 0;
@@ -969,7 +1098,7 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
             if (dup) continue;
             emitted[en++] = pt;
             m.pos[n_emit] = pt;
-            m.pen[n_emit] = wo.pen * align_k[k2];
+            m.pen[n_emit] = wo.pen * align;
             m.fp[n_emit] = wo.fa | (c << 24);
             ++n_emit;
           }
@@ -977,7 +1106,7 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
         m.cc = n_emit;
         store = n_emit > 0;
       }
-      if (store) np_store(d, p, cur, warm, slot, ida, idb, d.flags[ida], A.p, B.p, m, true);
+      if (store) np_store(d, p, cur, warm, slot0 + code, ida, idb, d.flags[ida], A.p, B.p, m, true);
     }
     __syncwarp();
   }
@@ -1023,6 +1152,7 @@ __global__ void k_csr_fill(const DevState d, int cur) {
 __global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  d.frozen[i] = np_awake(d.flags[i]) ? 0u : 1u;  // read by the next substep's classification
   uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
   uint32_t* L = d.csr_list[cur];
   for (uint32_t a = s0 + 1; a < s1; ++a) {
@@ -1051,7 +1181,8 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
                    sc.scan_status + 6 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 6, d.ctr);
     k_slot_fill<<<grid, T, 0, s>>>(d);
   }
-  k_np_classify<<<sms * 8, 256, 0, s>>>(d, cur);
+  k_np_classify<<<sms * 8, 256, 0, s>>>(d, cur, warm ? 1 : 0);
+  k_narrow_carry<<<sms * 8, 256, 0, s>>>(d, cur);
   k_narrow<<<sms * (p.narrow_blocks_per_sm ? p.narrow_blocks_per_sm : 16u), 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
   if (d.vox_on) k_voxel_narrow<<<sms * 8, 256, 0, s>>>(d, p, cur, warm ? 1 : 0);
   // compact order: exclusive scan of the hit flags over the slots

@@ -4,9 +4,10 @@
 // transfer between passes, src/shaders/simulation/RB_sim.slang:113-203,
 // src/shaders/simulation/LBVH.slang:34-152, RBM:1288-1295) with:
 //   * one histogram kernel that counts all digit positions in a single read of the keys,
-//   * one onesweep kernel per digit: tiles of 2048 keys rank themselves with warp-level
-//     multisplit (__match_any_sync), publish per-digit tile totals, and resolve their global
-//     offsets by decoupled look-back over the preceding tiles.
+//   * one onesweep kernel per digit: tiles of 4096 keys rank themselves with warp-level
+//     multisplit (__match_any_sync), publish per-digit tile totals, resolve their global
+//     offsets by decoupled look-back over the preceding tiles, reorder the tile by digit in
+//     shared memory and write each digit's run contiguously (coalesced stores).
 // Both are stable, so the result equals a stable sort by key -- the reference's semantics.
 // Element counts are read from device memory so the kernels can sit in a CUDA graph.
 #include "bb_common.cuh"
@@ -15,7 +16,9 @@
 namespace {
 constexpr int kThreads = 256;
 constexpr int kItems = 8;
-constexpr int kTile = kThreads * kItems;  // 2048
+constexpr int kTile = kThreads * kItems;  // 2048 (scan)
+constexpr int kSortItems = BB_SORT_TILE / kThreads;  // 16 keys per thread in a onesweep tile
+static_assert(kSortItems * kThreads == BB_SORT_TILE, "onesweep tile");
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1u;
@@ -164,27 +167,33 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
                                                        uint32_t* tile_ctr, DevCounters* ctr) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_hist[kThreads / 32][256];
-  __shared__ uint32_t s_offset[256];
+  __shared__ uint32_t s_offset[256];  // global position of this tile's first key of digit d
+  __shared__ uint32_t s_local[256];   // tile position of its first key of digit d
+  __shared__ uint32_t s_wsum[kThreads / 32];
+  __shared__ uint32_t s_keys[BB_SORT_TILE];
+  __shared__ uint32_t s_vals[BB_SORT_TILE];
+  __shared__ uint8_t s_dig[BB_SORT_TILE];
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
   for (int i = threadIdx.x; i < (kThreads / 32) * 256; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
   const uint32_t tile = s_tile;
-  const uint32_t base = tile * kTile;
+  const uint32_t base = tile * BB_SORT_TILE;
   if (base >= n) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt_mask = (1u << lane) - 1u;
-  uint32_t key[kItems], val[kItems], rank[kItems], dig[kItems];
+  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems], dig[kSortItems];
 #pragma unroll
-  for (int k = 0; k < kItems; ++k) {
-    uint32_t i = base + warp * (32 * kItems) + k * 32 + lane;
+  for (int k = 0; k < kSortItems; ++k) {
+    uint32_t i = base + warp * (32 * kSortItems) + k * 32 + lane;
     bool ok = i < n;
     key[k] = ok ? keys_in[i] : 0u;
     val[k] = ok ? vals_in[i] : 0u;
     dig[k] = ok ? (((lut ? lut[val[k]] : key[k]) >> shift) & 255u) : 256u;
   }
+  // warp-level multisplit: rank of each key among its warp's keys of the same digit, in order
 #pragma unroll
-  for (int k = 0; k < kItems; ++k) {
+  for (int k = 0; k < kSortItems; ++k) {
     uint32_t d = dig[k];
     uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
     uint32_t prior = d < 256u ? s_warp_hist[warp][d] : 0u;
@@ -194,7 +203,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     __syncwarp();
   }
   __syncthreads();
-  // per digit: exclusive prefix over warps, tile total
+  // per digit t: exclusive prefix over warps, and the tile's count of digit t
   const uint32_t t = threadIdx.x;
   uint32_t sum = 0;
 #pragma unroll
@@ -203,6 +212,21 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     s_warp_hist[w][t] = sum;
     sum += c;
   }
+  // tile-local start of each digit: block exclusive scan of the counts
+  {
+    uint32_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t wo = 0;
+    for (int w = 0; w < warp; ++w) wo += s_wsum[w];
+    s_local[t] = wo + x - sum;
+  }
+  // decoupled look-back: keys of digit t in the preceding tiles
   volatile uint32_t* st = status;
   uint32_t excl = 0;
   if (tile == 0) {
@@ -229,14 +253,25 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
   }
   s_offset[t] = digit_start[t] + excl;
   __syncthreads();
+  // reorder the tile by digit (stable: warps and ranks follow the input order) ...
 #pragma unroll
-  for (int k = 0; k < kItems; ++k) {
+  for (int k = 0; k < kSortItems; ++k) {
     uint32_t d = dig[k];
     if (d < 256u) {
-      uint32_t dst = s_offset[d] + s_warp_hist[warp][d] + rank[k];
-      keys_out[dst] = key[k];
-      vals_out[dst] = val[k];
+      const uint32_t lp = s_local[d] + s_warp_hist[warp][d] + rank[k];
+      s_keys[lp] = key[k];
+      s_vals[lp] = val[k];
+      s_dig[lp] = uint8_t(d);
     }
+  }
+  __syncthreads();
+  // ... and write each digit's run of the tile contiguously
+  const uint32_t nt = min(uint32_t(BB_SORT_TILE), n - base);
+  for (uint32_t i = t; i < nt; i += kThreads) {
+    const uint32_t d = s_dig[i];
+    const uint32_t dst = s_offset[d] + (i - s_local[d]);
+    keys_out[dst] = s_keys[i];
+    vals_out[dst] = s_vals[i];
   }
 }
 
@@ -250,7 +285,7 @@ void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uin
 }
 
 uint32_t bb_scan_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
-uint32_t bb_sort_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
+uint32_t bb_sort_tiles(uint32_t n_cap) { return n_cap / BB_SORT_TILE + 1; }
 
 // Sorts `passes` digits: pass 0 reads (keys_in, vals_in); pass k writes buffer
 // dst[(passes - 1 - k) & 1] and the next pass reads it, so the last pass lands in dst[0].
@@ -259,7 +294,7 @@ uint32_t bb_sort_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }
 void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* dst_keys[2],
                        uint32_t* dst_vals[2], uint32_t n, int passes, uint32_t* hist, uint32_t* status,
                        uint32_t* tile_ctr, DevCounters* ctr, int sms) {
-  uint32_t tiles = (n + kTile - 1) / kTile;
+  uint32_t tiles = (n + BB_SORT_TILE - 1) / BB_SORT_TILE;
   if (tiles == 0) tiles = 1;
   k_sort_hist<<<sms * 4, kThreads, 0, s>>>(keys_in, vals_in, nullptr, nullptr, n, hist, passes, 0, 0);
   k_sort_hist_scan<<<1, 256, 0, s>>>(hist, hist + 8 * 256, passes);
@@ -281,7 +316,7 @@ void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* 
 void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,
                     int passes, int shift0, uint32_t* hist, uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr,
                     int sms, const uint32_t* lut, int lut_passes) {
-  uint32_t tiles = (n_cap + kTile - 1) / kTile;
+  uint32_t tiles = (n_cap + BB_SORT_TILE - 1) / BB_SORT_TILE;
   if (tiles == 0) tiles = 1;
   const int total = passes + (lut ? lut_passes : 0);
   k_sort_hist<<<sms * 4, kThreads, 0, s>>>(keys[0], vals[0], lut, n_dev, n_cap, hist, passes, lut ? lut_passes : 0,

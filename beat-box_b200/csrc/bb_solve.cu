@@ -384,6 +384,7 @@ __global__ void k_pgs_count(const DevState d, int cur) {
     const uint2 b = d.m_bodies[cur][slot];
     const bool skip = !awake(d.flags[b.x]) && !awake(d.flags[b.y]);
     d.pgs_cnt[k] = skip ? 0u : uint32_t(d.m_keycc[cur][slot].y);
+    if (!skip) d.colour_awake[min(d.gc_color[list[k]], uint32_t(BB_MAX_COLORS))] = 1u;
   }
 }
 
@@ -485,23 +486,36 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
 __device__ __forceinline__ uint32_t pgs_next_colour(uint32_t c, uint32_t C) { return c + 1 < C ? c + 1 : 0u; }
 
 template <int PF>
-__device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode, const uint32_t* bs, uint32_t C,
-                          PgsItem<PF>& x, uint4& rec_next, uint32_t& epoch) {
+__device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode, const uint32_t* bs, const uint32_t* aw,
+                          uint32_t C, PgsItem<PF>& x, uint4& rec_next, uint32_t& epoch) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* sync = &d.ctr->sync_count[1];
   for (uint32_t c = 0; c < C; ++c) {
-    const uint32_t end = bs[c + 1];
-    for (uint32_t k = bs[c] + tid; k < end;) {
-      pgs_item_run(d, p, cur, x, mode);
-      k += stride;
-      if (k < end) pgs_item_load(d, k, x);
+    // A colour whose manifolds all sleep has no work (every item is skipped) and needs no
+    // barrier: its neighbours are ordered by the barriers of the colours that do run.
+    const bool run = aw[c] != 0;
+    if (run) {
+      const uint32_t end = bs[c + 1];
+      for (uint32_t k = bs[c] + tid; k < end;) {
+        pgs_item_run(d, p, cur, x, mode);
+        k += stride;
+        if (k < end) pgs_item_load(d, k, x);
+      }
     }
     const uint32_t cn = pgs_next_colour(c, C), cnn = pgs_next_colour(cn, C);
     const uint32_t kn = bs[cn] + tid, knn = bs[cnn] + tid;
-    // Two consecutive colours that both fit in block 0 (items map to threads by their index in
-    // the colour) need only a CTA barrier between them: every item and every body write of both
-    // lives in block 0.  The test reads shared bucket starts, so every block decides alike.
-    const bool local = c + 1 < C && bs[c + 1] - bs[c] <= blockDim.x && bs[c + 2] - bs[c + 1] <= blockDim.x;
+    if (!run) {  // keep the prefetch one colour ahead
+      if (kn < bs[cn + 1]) pgs_item_load_rest(d, kn, rec_next, x);
+      if (knn < bs[cnn + 1]) rec_next = d.pgs_rec[knn];
+      continue;
+    }
+    // This colour and the next one that runs, both fitting in block 0 (items map to threads by
+    // their index in the colour), need only a CTA barrier between them: every item and every
+    // body write of both lives in block 0.  The test reads shared bucket starts and flags, so
+    // every block decides alike.
+    uint32_t ne = c + 1;
+    while (ne < C && !aw[ne]) ++ne;
+    const bool local = ne < C && bs[c + 1] - bs[c] <= blockDim.x && bs[ne + 1] - bs[ne] <= blockDim.x;
     if (!local) grid_arrive(sync, epoch);
     if (kn < bs[cn + 1]) pgs_item_load_rest(d, kn, rec_next, x);
     if (knn < bs[cnn + 1]) rec_next = d.pgs_rec[knn];
@@ -527,7 +541,9 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
 template <int PF>
 __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   __shared__ uint32_t bs[BB_MAX_COLORS + 2];
+  __shared__ uint32_t aw[BB_MAX_COLORS + 1];
   if (threadIdx.x < BB_MAX_COLORS + 2) bs[threadIdx.x] = d.bucket_start[threadIdx.x];
+  if (threadIdx.x < BB_MAX_COLORS + 1) aw[threadIdx.x] = d.colour_awake[threadIdx.x];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
   const float inv_h = h > 0.f ? 1.0f / h : 0.f;
@@ -550,14 +566,14 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(co
     const uint32_t c1 = pgs_next_colour(0, C);
     if (bs[c1] + tid < bs[c1 + 1]) rec_next = d.pgs_rec[bs[c1] + tid];
   }
-  pgs_sweep(d, p, cur, 0, bs, C, x, rec_next, epoch);
-  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, C, x, rec_next, epoch);
+  pgs_sweep(d, p, cur, 0, bs, aw, C, x, rec_next, epoch);
+  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, aw, C, x, rec_next, epoch);
   if (p.flags & BB_SIM_ADVECTION) {
     for (uint32_t i = tid; i < n; i += stride)
       if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
     grid_sync(d.ctr, sync, epoch);
   }
-  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, C, x, rec_next, epoch);
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, aw, C, x, rec_next, epoch);
   // impulses back to the persistent contacts (every sweep ended with a grid barrier)
   const uint32_t M = d.ctr->manifold_count;
   for (uint32_t k = tid; k < M; k += stride) {
@@ -699,6 +715,7 @@ int bb_pgs_soft_blocks(int sms) {
 
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                        const StepScratch& sc, int coop_blocks, int sms) {
+  cudaMemsetAsync(d.colour_awake, 0, sizeof(uint32_t) * (BB_MAX_COLORS + 1), s);
   k_pgs_count<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
   bb_launch_scan(s, d.pgs_cnt, d.pgs_coff, &d.ctr->manifold_count, d.pair_capacity, nullptr,
                  sc.scan_status + 4 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 4, d.ctr);

@@ -11,7 +11,7 @@
 #include "bb_kernels.cuh"
 
 namespace {
-constexpr uint32_t kTile = 2048;
+constexpr uint32_t kTile = BB_SORT_TILE;
 
 struct SortScratch {
   int device = -1;

@@ -13,7 +13,7 @@
 #include "bb_kernels.cuh"
 
 namespace {
-constexpr uint32_t kTile = 2048;  // keys per onesweep tile (must match bb_scan_sort.cu)
+constexpr uint32_t kTile = BB_SORT_TILE;  // keys per onesweep tile
 constexpr uint32_t kMaxKeys = BB_SORT_STATIC_MAX_KEYS;
 constexpr int kMaxPasses = 4;
 constexpr size_t kCounterBytes = (sizeof(DevCounters) + 255) / 256 * 256;

@@ -123,6 +123,7 @@ __global__ void k_extend_contacts(const DevState d, uint32_t o, uint32_t count) 
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   d.vals[0][o + i] = o + i;
+  d.frozen[o + i] = 0;
   for (int k = 0; k < 2; ++k) d.csr_start[k][o + 1 + i] = d.csr_start[k][o];
 }
 
@@ -180,6 +181,7 @@ __global__ void k_begin_substep(DevCounters* c) {
   c->np_counts[0] = 0;
   c->np_counts[1] = 0;
   c->np_counts[2] = 0;
+  c->np_counts[3] = 0;
   c->slot_count = 0;
   c->gc_list_n[0] = 0;
   c->gc_list_n[1] = 0;
@@ -242,7 +244,7 @@ struct bb_world_impl {
     auto f4 = [&](size_t k) { return dalloc<float4>(k, owned, err, stream); };
     auto u32 = [&](size_t k) { return dalloc<uint32_t>(k, owned, err, stream); };
     d.pos = f4(N); d.rot = f4(N); d.vel = f4(N); d.omega = f4(N); d.pvel = f4(N); d.shape = f4(N); d.iinv = f4(N);
-    d.flags = u32(N); d.sleep = u32(N); d.iw = f4(2 * N); d.iinv_off = f4(N);
+    d.flags = u32(N); d.sleep = u32(N); d.iw = f4(2 * N); d.iinv_off = f4(N); d.frozen = u32(N);
     for (int k = 0; k < 2; ++k) { d.keys[k] = u32(N); d.vals[k] = u32(N); }
     d.rank = u32(N);
     d.node_box = f4(4 * N);
@@ -270,7 +272,7 @@ struct bb_world_impl {
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
     d.flow_rec = dalloc<uint4>(P, owned, err, stream);
     d.pgs_rec = dalloc<uint4>(P, owned, err, stream);
-    d.np_list = u32(P);
+    d.np_list = u32(P); d.carry_list = u32(P);
     d.gc_rec = dalloc<uint4>(P, owned, err, stream);
     d.gc_list[0] = u32(P); d.gc_list[1] = u32(P);
     d.pgs_mass = f4(P);
@@ -291,6 +293,7 @@ struct bb_world_impl {
     d.gc_owner = dalloc<unsigned long long>(N * BB_MAX_COLORS, owned, err, stream);
     for (int k = 0; k < 2; ++k) { d.bucket_keys[k] = u32(P); d.bucket_vals[k] = u32(P); }
     d.bucket_start = u32(64);
+    d.colour_awake = u32(BB_MAX_COLORS + 1);
     d.body_color = u32(N); d.body_color_round = u32(N);
     d.a_pos_start = f4(N); d.a_rot_start = f4(N); d.a_pos_tilde = f4(N); d.a_rot_tilde = f4(N);
     d.a_depth = u32(N);
@@ -324,6 +327,7 @@ struct bb_world_impl {
   }
 
   void reset_contacts() {
+    cudaMemsetAsync(d.frozen, 0, sizeof(uint32_t) * (cap_n + 1), stream);
     cudaMemsetAsync(d.csr_start[0], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     cudaMemsetAsync(d.csr_start[1], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     std::vector<uint32_t> ident(n);
@@ -767,6 +771,9 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
   if ((p->broad_threads != 0 && p->broad_threads != 32 && p->broad_threads != 64 && p->broad_threads != 128) ||
       p->narrow_blocks_per_sm > 64 || p->flow_blocks_per_sm > 8)
     return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, flow <= 8)");
+  // contact geometry depends on these: no pair keeps last substep's manifolds as they were
+  if (p->quirks != w->params.quirks || p->penetration_cap != w->params.penetration_cap)
+    CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * (w->cap_n + 1), w->stream));
   w->params = *p;
   if (!w->params.broad_threads) w->params.broad_threads = 128;
   if (!w->params.narrow_blocks_per_sm) w->params.narrow_blocks_per_sm = 16;
@@ -976,6 +983,8 @@ bb_status bb_write_state(void* world, const float* position, const float* rotati
   if (velocity) { CU(cudaMemcpyAsync(st + 7ull * n, velocity, 12ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 4; }
   if (omega) { CU(cudaMemcpyAsync(st + 10ull * n, omega, 12ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 8; }
   k_unpack_state<<<(n + 255) / 256, 256, 0, w->stream>>>(w->d, n, st, mask);
+  // moved poses: no body keeps last substep's manifolds as they were
+  if (mask & 3u) CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * n, w->stream));
   // the caller may reuse its buffers as soon as this returns
   CU(cudaStreamSynchronize(w->stream));
   return BB_OK;

@@ -66,6 +66,41 @@ def workload(args):
     return sc, name
 
 
+def sort_roofline(local_rank: int, peak_gbs: float, n: int = 1 << 26, reps: int = 5) -> dict:
+    """The onesweep pair sort (the step's a4 kernels, through bb_radix_sort_pairs) on 2^26 random
+    32-bit keys with 32-bit values, 1 GB in and out, so every pass streams from HBM.  Algorithmic
+    bytes: one histogram read of the keys (4 B/key) plus 4 passes reading and writing keys and
+    values (16 B/key each), 68 B/key.  CUDA events on the stream the sort runs on; the mean of
+    `reps` sorts after one warm-up sort."""
+    import torch
+
+    import beatbox as bb
+
+    L = bb.load_library()
+    dev = f"cuda:{local_rank}"
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    keys = torch.randint(0, 2 ** 31 - 1, (n,), device=dev, dtype=torch.int64, generator=g).to(torch.int32)
+    vals = torch.arange(n, device=dev, dtype=torch.int32)
+    ko, vo = torch.empty_like(keys), torch.empty_like(vals)
+    s = torch.cuda.current_stream()
+    args = [keys.data_ptr(), vals.data_ptr(), ko.data_ptr(), vo.data_ptr(), n, 32, s.cuda_stream]
+    bb._check(L.bb_radix_sort_pairs(*args))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        bb._check(L.bb_radix_sort_pairs(*args))
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    ok = bool(torch.all(ko[1:].to(torch.int64) >= ko[:-1].to(torch.int64)).item())
+    achieved = 68.0 * n / (ms / 1000.0) / 1e9
+    return {"kernel": "k_sort_hist + 4x k_onesweep (bb_radix_sort_pairs)", "bound": "hbm", "keys": n,
+            "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
+            "ms_per_sort": ms, "algorithmic_bytes_per_key": 68, "sorted": ok}
+
+
 def run_steps(args) -> int:
     """Length of the configuration's run: 600 steps for the mixed column, 300 for the others."""
     return 600 if args.scene == "mixed_column" else 300
@@ -309,6 +344,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
             "algorithmic_bytes_per_launch": sb, "ms_per_launch": solve_ms,
             "stage_ms_per_substep": {k: v / launches_per_stage for k, v in stages.items()}, "dominant_stage": dom}
 
+    sort_roof = sort_roofline(local_rank, peak_gbs) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, sc, warm_state, warm_flags)
@@ -324,7 +361,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                 "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": io_bytes,
                         "d2h_bytes_per_step": io_bytes, "steps": e2e_steps,
                         "what": "bb_write_state + bb_step + bb_read_state with pinned host buffers"},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": launches, "roofline": roof, "sort_roofline": sort_roof, "cpu_baseline": cpu,
+                "clocks": clk,
                 "step_stats": stats}
         print(json.dumps(line), flush=True)
     w.close()

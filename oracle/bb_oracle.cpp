@@ -40,6 +40,7 @@ void load(World<R>& w, uint32_t n, const float* pos, const float* quat, const fl
     b.restitution = restitution[i];
   }
   w.order.clear();
+  w.frozen.clear();
   w.prev_manifolds.clear();
   w.prev_pair_index.clear();
 }
@@ -208,8 +209,13 @@ void orc_default_params(bb_solver_params* p) { default_params(p); }
 
 void orc_set_params(void* hp, const bb_solver_params* p) {
   Handle* h = static_cast<Handle*>(hp);
-  if (h->dbl) h->d->p = *p;
-  else h->f->p = *p;
+  auto set = [&](auto& w) {
+    // contact geometry depends on these: no pair keeps last substep's manifolds as they were
+    if (p->quirks != w.p.quirks || p->penetration_cap != w.p.penetration_cap) w.frozen.clear();
+    w.p = *p;
+  };
+  if (h->dbl) set(*h->d);
+  else set(*h->f);
 }
 
 void orc_step(void* hp, float dt, uint32_t substeps) {
@@ -222,6 +228,13 @@ void orc_collide(void* hp, uint32_t stage) {
   Handle* h = static_cast<Handle*>(hp);
   if (h->dbl) h->d->collide(stage);
   else h->f->collide(stage);
+}
+
+// 0: frozen pairs recompute their contacts like every other pair (for tests of the carry-over)
+void orc_set_carry_frozen(void* hp, int on) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (h->dbl) h->d->carry_frozen = on != 0;
+  else h->f->carry_frozen = on != 0;
 }
 
 void orc_skip_warm_starting_once(void* hp) {

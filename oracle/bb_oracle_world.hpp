@@ -21,6 +21,10 @@ template <class R> class World {
   std::unordered_map<uint64_t, uint32_t> prev_pair_index;  // (min id, max id) -> prev manifold
   std::map<std::tuple<uint32_t, uint32_t, int>, uint32_t> prev_voxel_index;  // (a, b, key) -> prev manifold
   VoxelPool voxels;
+  // frozen[i]: body i was asleep or static at the last narrow phase (its pose has not changed
+  // since); carry_frozen: pairs of frozen, non-awake bodies carry their manifolds over
+  std::vector<uint8_t> frozen;
+  bool carry_frozen = true;
   bool skip_warm_once = false;
 
   // products of the last substep (debug readback)
@@ -212,6 +216,49 @@ template <class R> class World {
   }
 
   // ------------------------------------------------------------------------------------
+  // Carry-over of a frozen pair (neither body awake, both asleep or static at the last narrow
+  // phase as well, so both poses are bit for bit those of the previous substep): instead of
+  // recomputing its contacts and matching them against last substep's, the previous
+  // manifold(s) of the pair in the same body order are kept as they were -- contacts, features,
+  // impulses, penalties -- with warm-start counts + 1 and the extraction trend 0, as a
+  // recomputation whose contacts all match by feature gives.  Returns false (recompute) when
+  // the pair had no manifold last substep.
+  bool carry_pair(size_t k, uint32_t ida, uint32_t idb, bool vox, std::array<Manifold<R>, 6>& out, uint8_t& have) {
+    auto carry = [&](const Manifold<R>& old, Manifold<R>& m) {
+      m = old;
+      m.sa = pair_a[k];
+      m.sb = pair_b[k];
+      m.anchor_a = bodies[ida].pos;
+      m.anchor_b = bodies[idb].pos;
+      m.error = 0;
+      m.color = MAX_U32;
+      for (int c = 0; c < m.cc; ++c) {
+        m.c[c].warm = std::min(255u, m.c[c].warm + 1u);
+        if (m.c[c].stick == 0) {
+          m.c[c].anchor_a = Vec3<R>();
+          m.c[c].anchor_b = Vec3<R>();
+        }
+      }
+    };
+    if (vox) {
+      bool any = false;
+      for (uint32_t code = 0; code < 6; ++code) {
+        auto it = prev_voxel_index.find(std::make_tuple(ida, idb, VOXEL_KEY0 + int(code)));
+        if (it == prev_voxel_index.end()) continue;
+        carry(prev_manifolds[it->second], out[code]);
+        have |= uint8_t(1u << code);
+        any = true;
+      }
+      return any;
+    }
+    auto it = prev_pair_index.find((uint64_t(std::min(ida, idb)) << 32) | std::max(ida, idb));
+    if (it == prev_pair_index.end() || prev_manifolds[it->second].a != ida) return false;
+    carry(prev_manifolds[it->second], out[0]);
+    have = 1;
+    return true;
+  }
+
+  // ------------------------------------------------------------------------------------
   // Narrow phase + warm start (collision_detection.slang:1514-1755).
   void narrow_phase() {
     const size_t P = pair_a.size();
@@ -226,6 +273,9 @@ template <class R> class World {
       const Body<R>& B = bodies[idb];
       if (!is_dyn(A) && !is_dyn(B)) return;  // static-static skip (:1525)
       const bool vox = A.shape == BB_SHAPE_VOXEL || B.shape == BB_SHAPE_VOXEL;
+      if (warm && carry_frozen && !awake(A) && !awake(B) && frozen.size() == n() && frozen[ida] && frozen[idb] &&
+          carry_pair(k, ida, idb, vox, per[k], have[k]))
+        return;
       for (uint32_t code = 0; code < (vox ? 6u : 1u); ++code) {
         SatResult<R> s;
         bool hit;
@@ -276,6 +326,8 @@ template <class R> class World {
     for (size_t k = 0; k < P; ++k)
       for (uint32_t code = 0; code < 6; ++code)
         if (have[k] & (1u << code)) manifolds.push_back(per[k][code]);
+    frozen.assign(n(), 0);
+    for (size_t i = 0; i < n(); ++i) frozen[i] = awake(bodies[i]) ? 0 : 1;
     skip_warm_once = false;
     // per-body manifold lists in ascending manifold order (body_link_manifold :881-905)
     lists.assign(n(), {});

@@ -77,6 +77,7 @@ def lib():
         L.orc_step.argtypes = [P, ctypes.c_float, ctypes.c_uint32]
         L.orc_collide.argtypes = [P, ctypes.c_uint32]
         L.orc_skip_warm_starting_once.argtypes = [P]
+        L.orc_set_carry_frozen.argtypes = [P, ctypes.c_int]
         L.orc_read_state.argtypes = [P, P, P, P, P, P]
         L.orc_read_stats.argtypes = [P, ctypes.POINTER(StepStats)]
         L.orc_debug_read.restype = ctypes.c_uint64
@@ -146,6 +147,9 @@ class Oracle:
 
     def collide(self, stage: int):
         lib().orc_collide(self.h, stage)
+
+    def set_carry_frozen(self, on: bool):
+        lib().orc_set_carry_frozen(self.h, 1 if on else 0)
 
     def skip_warm_starting_once(self):
         lib().orc_skip_warm_starting_once(self.h)

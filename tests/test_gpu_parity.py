@@ -309,3 +309,53 @@ def test_state_roundtrip_and_write():
     newpos = st["pos"] + 1.0
     w.write_state(pos=newpos)
     assert np.allclose(w.read_state()["pos"], newpos)
+
+
+def resting_scene():
+    """Boxes resting on the ground from the start (a 4 x 4 grid of singles and one 2-box stack):
+    they fall asleep after the quiet-time threshold, on the GPU and in the oracle alike."""
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50])
+    g = np.arange(16)
+    pos = np.stack([-2.4 + 1.6 * (g % 4), np.full(16, 0.499), -2.4 + 1.6 * (g // 4)], 1)
+    pos = np.vstack([pos, [[4.0, 0.499, 0.0], [4.0, 1.498, 0.0]]])
+    sb.add(pos, np.tile([0, 0, 0, 1.0], (18, 1)), np.full((18, 3), 0.5), scenes.SHAPE_BOX,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1000.0)
+    return sb.build()
+
+
+@pytest.mark.parametrize("solver", [bb.SOLVER_PGS_SOFT, bb.SOLVER_PGS])
+def test_sleeping_bodies_carry_their_manifolds_like_the_oracle(oracle_lib, solver):
+    """Bodies that fall asleep during the run: from the second substep they sleep, their frozen
+    pairs carry their manifolds over (impulses, features, warm-start counts + 1) on both sides.
+    Sleep counts, manifold identities, features and warm-start counts match the oracle bit for
+    bit, and the sleeping bodies do not move."""
+    sc = resting_scene()
+    p = params_for(oracle_lib, sc, solver=solver, quirks=0, iterations=8, relax_iterations=8)
+    if solver == bb.SOLVER_PGS:  # Baumgarte PGS runs on the per-island path
+        p.flags = p.flags & ~bb.SIM_USE_GRAPH_COLORING
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    for _ in range(50):
+        w.step(DT, 4)
+        o.step(DT, 4)
+    before = w.read_state()
+    for _ in range(10):
+        w.step(DT, 4)
+        o.step(DT, 4)
+    w.sync()
+    gs, rs = w.stats(), o.stats()
+    assert gs["sleeping_count"] == rs["sleeping_count"] == 18
+    gm, rm = w.debug_read("manifolds"), oread(o, 8, None)
+    assert len(gm) == len(rm) == 18
+    for f in ("body_a", "body_b", "key", "contact_count"):
+        assert np.array_equal(gm[f], rm[f]), f
+    gc, rc = w.debug_read("contacts"), oread(o, 9, None)
+    mask = (np.arange(8)[None, :] < gm["contact_count"][:, None]).ravel()
+    assert np.array_equal(gc["feature"][mask], rc["feature"][mask])
+    assert np.array_equal(gc["warm_start"][mask], rc["warm_start"][mask])
+    assert (gc["warm_start"][mask] > 200).all()  # every contact inherited since the first substeps
+    assert np.abs(gc["position"][mask] - rc["position"][mask]).max() < 1e-4
+    after = w.read_state()
+    for k in before:
+        assert np.array_equal(before[k], after[k]), k  # asleep: frozen in place

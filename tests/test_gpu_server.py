@@ -85,3 +85,59 @@ def test_world_larger_than_the_budget_is_refused():
     r = srv.wait(t)
     assert r["done"] and r["result"] == bb.E_BUDGET
     srv.close()
+
+
+def test_served_worlds_match_the_fp64_oracle_on_a_sampled_one_percent(oracle_lib):
+    """Poisson arrivals of new and continued worlds (config-5 style, scaled down); a seeded 1% of
+    the new worlds (at least one) take a single-step request and are never continued, so their
+    served state after the request is compared with the FP64 oracle's one step of the same
+    scene and parameters: the one-step tolerance (positions 1e-4 of the world's scale,
+    velocities 2e-4 of max(|v|, 1) m/s)."""
+    import time
+
+    rng = np.random.default_rng(11)
+    sizes = np.floor(np.exp(rng.uniform(np.log(64), np.log(3000), 12))).astype(int)
+    templates = [scenes.pile(int(n), seed=300 + k) for k, n in enumerate(sizes)]
+    srv = bb.Server(hbm_budget_bytes=40 * GB, max_active=16)
+    known, sampled, tickets = [], [], []
+    next_key = 1
+    for j in range(200):
+        time.sleep(float(rng.exponential(1.0 / 2000.0)))
+        params = req_params(j)
+        if not known or rng.random() < 0.5:
+            k = int(rng.integers(0, len(templates)))
+            key = next_key
+            next_key += 1
+            if rng.random() < 0.01:
+                sampled.append((key, k, params))
+                tickets.append(srv.submit(key, 1, params, DT, 2, scene=templates[k]))
+                continue
+            known.append((key, k))
+            tickets.append(srv.submit(key, int(rng.integers(1, 30)), params, DT, 2, scene=templates[k]))
+        else:
+            key, k = known[int(rng.integers(0, len(known)))]
+            tickets.append(srv.submit(key, int(rng.integers(1, 30)), params, DT, 2))
+        if j == 199 and not sampled:  # at least one sampled world, submitted while others run
+            k = int(rng.integers(0, len(templates)))
+            sampled.append((next_key, k, req_params(j + 1)))
+            tickets.append(srv.submit(next_key, 1, req_params(j + 1), DT, 2, scene=templates[k]))
+            next_key += 1
+    res = [srv.wait(t) for t in tickets]
+    assert all(r["result"] == bb.OK for r in res)
+    assert sampled
+    for key, k, params in sampled:
+        sc = templates[k]
+        g = srv.read_state(key, int(sc["n"]))
+        p = oracle_lib.SolverParams.from_buffer_copy(bytes(params))
+        b = sc.get("bounds") or ([-64.0] * 3, [128.0] * 3)  # the Morton box the server applies
+        p.world_min[:] = b[0]
+        p.world_extent[:] = b[1]
+        o = oracle_lib.Oracle(sc, params=p)
+        o.step(DT, 2)
+        r = o.state()
+        dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+        perr = np.abs(g["pos"][dyn] - r["pos"][dyn]).max() / np.abs(r["pos"][dyn]).max()
+        verr = np.abs(g["vel"][dyn] - r["vel"][dyn]).max()
+        assert perr < 1e-4, (key, perr)
+        assert verr < 2e-4 * max(np.abs(r["vel"][dyn]).max(), 1.0), (key, verr)
+    srv.close()

@@ -221,3 +221,32 @@ def test_scene4_coulomb_outcome(oracle_lib, theta, mu):
         assert slid > 0.3
     else:
         assert abs(slid) < 0.05
+
+
+@pytest.mark.parametrize("solver", [1, 2])
+@pytest.mark.parametrize("scene", ["boxes", "voxels"])
+def test_frozen_pairs_carry_over_gives_the_recomputed_result(oracle_lib, solver, scene):
+    """Pairs whose bodies were asleep (or static) at the last narrow phase and still are keep
+    their manifolds instead of recomputing them; on piles that fall asleep this gives the same
+    bits as recomputing every pair (states and contacts)."""
+    import beatbox as bb
+
+    sc = scenes.box_grid(n_side=4, layers=2) if scene == "boxes" else scenes.voxel_pile(9, seed=2)
+    out = []
+    for carry in (True, False):
+        p = oracle_lib.default_params()
+        p.quirks = 0
+        p.solver = solver
+        p.iterations = p.relax_iterations = 8
+        p.avbd_iterations = 4
+        o = oracle_lib.Oracle(sc, params=p, threads=4)
+        o.set_carry_frozen(carry)
+        for _ in range(300):
+            o.step(1.0 / 60.0, 4)
+        cnt, buf = o.debug_read(9)
+        out.append((o.state(), buf[: cnt * bb.CONTACT_DTYPE.itemsize].copy(), o.stats()["sleeping_count"]))
+    (a, ca, sa), (b, cb, sb) = out
+    assert sa > 0 and sa == sb
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(ca, cb)
