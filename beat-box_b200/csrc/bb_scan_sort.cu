@@ -122,14 +122,38 @@ __global__ void __launch_bounds__(kThreads) k_sort_hist(const uint32_t* __restri
   for (int i = threadIdx.x; i < 8 * 256; i += kThreads) (&s_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
-  for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
-    uint32_t k = keys[i];
+  auto count = [&](uint32_t k, uint32_t v) {
     for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(k >> (shift0 + 8 * p)) & 255u], 1u);
     if (lut_passes) {
-      uint32_t w = lut[vals[i]];
+      uint32_t w = lut[v];
       for (int p = 0; p < lut_passes; ++p) atomicAdd(&s_hist[passes + p][(w >> (8 * p)) & 255u], 1u);
     }
+  };
+  // four keys per 16-byte load, two loads in flight per thread; arrays that do not start on a
+  // 16-byte boundary (caller pointers into a buffer) take the scalar loop for every key
+  const bool aligned = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0 &&
+                       (!lut_passes || (reinterpret_cast<uintptr_t>(vals) & 15u) == 0);
+  const uint32_t n4 = aligned ? n / 4 : 0u, stride = gridDim.x * kThreads;
+  const uint4* k4 = reinterpret_cast<const uint4*>(keys);
+  const uint4* v4 = reinterpret_cast<const uint4*>(vals);
+  uint32_t q = blockIdx.x * kThreads + threadIdx.x;
+  for (; q + stride < n4; q += 2 * stride) {
+    const uint4 a = k4[q], b = k4[q + stride];
+    uint4 va = make_uint4(0, 0, 0, 0), vb = make_uint4(0, 0, 0, 0);
+    if (lut_passes) {
+      va = v4[q];
+      vb = v4[q + stride];
+    }
+    count(a.x, va.x); count(a.y, va.y); count(a.z, va.z); count(a.w, va.w);
+    count(b.x, vb.x); count(b.y, vb.y); count(b.z, vb.z); count(b.w, vb.w);
   }
+  if (q < n4) {
+    const uint4 a = k4[q];
+    const uint4 va = lut_passes ? v4[q] : make_uint4(0, 0, 0, 0);
+    count(a.x, va.x); count(a.y, va.y); count(a.z, va.z); count(a.w, va.w);
+  }
+  for (uint32_t r = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; r < n; r += stride)  // the rest
+    count(keys[r], lut_passes ? vals[r] : 0u);
   __syncthreads();
   for (int p = 0; p < passes + lut_passes; ++p) {
     uint32_t c = s_hist[p][threadIdx.x];
@@ -157,14 +181,51 @@ __global__ void k_sort_hist_scan(const uint32_t* hist, uint32_t* hist_scan, int 
 
 // one stable onesweep pass on digit (key >> shift) & 255, or (lut[value] >> shift) & 255
 // when lut is given
-__global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in,
-                                                       const uint32_t* __restrict__ vals_in,
-                                                       uint32_t* __restrict__ keys_out,
-                                                       uint32_t* __restrict__ vals_out,
-                                                       const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
-                                                       const uint32_t* __restrict__ digit_start, int shift,
-                                                       const uint32_t* __restrict__ lut, uint32_t* status,
-                                                       uint32_t* tile_ctr, DevCounters* ctr) {
+__device__ __forceinline__ uint32_t sort_digit(uint32_t key, uint32_t val, const uint32_t* __restrict__ lut, int shift) {
+  return ((lut ? lut[val] : key) >> shift) & 255u;
+}
+
+// Decoupled look-back for digit t of tile `tile`: the sum of digit t over all preceding tiles.
+// The status words of 8 predecessors are loaded at once and walked in order (aggregates are
+// added until an inclusive prefix), so a chain of tiles still in flight costs one load
+// latency per 8 tiles instead of one per tile.  A word not yet published is re-read.
+constexpr int kLookback = 8;
+__device__ __forceinline__ uint32_t sort_lookback(volatile uint32_t* st, uint32_t tile, uint32_t t, DevCounters* ctr) {
+  uint32_t excl = 0, spins = 0;
+  int32_t j = int32_t(tile) - 1;
+  while (j >= 0) {
+    uint32_t w[kLookback];
+#pragma unroll
+    for (int k = 0; k < kLookback; ++k) {
+      w[k] = 2u << 30;  // before tile 0: an empty inclusive prefix
+      if (j - k >= 0) w[k] = st[uint32_t(j - k) * 256u + t];
+    }
+    int k = 0;
+    for (; k < kLookback; ++k) {
+      const uint32_t flag = w[k] & ~kValMask;
+      if (flag == 0) break;  // not yet published: re-read from here
+      excl += w[k] & kValMask;
+      if (flag == kFlagPrefix) return excl;
+    }
+    j -= k;
+    if (k < kLookback && ++spins > BB_SPIN_LIMIT) {
+      raise_error(ctr, BB_ERRF_SPIN_LIMIT);
+      return excl;
+    }
+  }
+  return excl;
+}
+
+// one stable onesweep pass on digit (key >> shift) & 255, or (lut[value] >> shift) & 255
+// when lut is given
+__global__ void __launch_bounds__(kThreads, 3) k_onesweep(const uint32_t* __restrict__ keys_in,
+                                                          const uint32_t* __restrict__ vals_in,
+                                                          uint32_t* __restrict__ keys_out,
+                                                          uint32_t* __restrict__ vals_out,
+                                                          const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
+                                                          const uint32_t* __restrict__ digit_start, int shift,
+                                                          const uint32_t* __restrict__ lut, uint32_t* status,
+                                                          uint32_t* tile_ctr, DevCounters* ctr) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp_hist[kThreads / 32][256];
   __shared__ uint32_t s_offset[256];  // global position of this tile's first key of digit d
@@ -182,19 +243,18 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
   if (base >= n) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt_mask = (1u << lane) - 1u;
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems], dig[kSortItems];
+  const uint32_t first = base + warp * (32 * kSortItems) + lane;
+  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
-    uint32_t i = base + warp * (32 * kSortItems) + k * 32 + lane;
-    bool ok = i < n;
-    key[k] = ok ? keys_in[i] : 0u;
-    val[k] = ok ? vals_in[i] : 0u;
-    dig[k] = ok ? (((lut ? lut[val[k]] : key[k]) >> shift) & 255u) : 256u;
+    const uint32_t i = first + k * 32;
+    key[k] = i < n ? keys_in[i] : 0u;
+    val[k] = i < n ? vals_in[i] : 0u;
   }
   // warp-level multisplit: rank of each key among its warp's keys of the same digit, in order
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
-    uint32_t d = dig[k];
+    const uint32_t d = first + k * 32 < n ? sort_digit(key[k], val[k], lut, shift) : 256u;
     uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
     uint32_t prior = d < 256u ? s_warp_hist[warp][d] : 0u;
     rank[k] = prior + __popc(peers & lt_mask);
@@ -212,6 +272,9 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     s_warp_hist[w][t] = sum;
     sum += c;
   }
+  volatile uint32_t* st = status;
+  // publish the tile's counts first, so that later tiles can look past this one early
+  st[tile * 256 + t] = (tile == 0 ? kFlagPrefix : kFlagAgg) | sum;
   // tile-local start of each digit: block exclusive scan of the counts
   {
     uint32_t x = sum;
@@ -226,29 +289,10 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     for (int w = 0; w < warp; ++w) wo += s_wsum[w];
     s_local[t] = wo + x - sum;
   }
-  // decoupled look-back: keys of digit t in the preceding tiles
-  volatile uint32_t* st = status;
+  // keys of digit t in the preceding tiles
   uint32_t excl = 0;
-  if (tile == 0) {
-    st[t] = kFlagPrefix | sum;
-  } else {
-    st[tile * 256 + t] = kFlagAgg | sum;
-    int32_t j = int32_t(tile) - 1;
-    uint32_t spins = 0;
-    while (j >= 0) {
-      uint32_t w = st[j * 256 + t];
-      uint32_t flag = w & ~kValMask;
-      if (flag == 0) {
-        if (++spins > BB_SPIN_LIMIT) {
-          raise_error(ctr, BB_ERRF_SPIN_LIMIT);
-          break;
-        }
-        continue;
-      }
-      excl += w & kValMask;
-      if (flag == kFlagPrefix) break;
-      --j;
-    }
+  if (tile > 0) {
+    excl = sort_lookback(st, tile, t, ctr);
     st[tile * 256 + t] = kFlagPrefix | (excl + sum);
   }
   s_offset[t] = digit_start[t] + excl;
@@ -256,8 +300,8 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
   // reorder the tile by digit (stable: warps and ranks follow the input order) ...
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
-    uint32_t d = dig[k];
-    if (d < 256u) {
+    if (first + k * 32 < n) {
+      const uint32_t d = sort_digit(key[k], val[k], lut, shift);
       const uint32_t lp = s_local[d] + s_warp_hist[warp][d] + rank[k];
       s_keys[lp] = key[k];
       s_vals[lp] = val[k];

@@ -34,7 +34,7 @@ def expected(keys, vals, bits):
     return keys[order], vals[order]
 
 
-@pytest.mark.parametrize("n", [1, 2, 2047, 2048, 2049, 100_003])
+@pytest.mark.parametrize("n", [1, 2, 2047, 2048, 2049, 4095, 4096, 4097, 100_003, 1_000_003])
 @pytest.mark.parametrize("bits", [8, 30, 32])
 def test_radix_sort_pairs_matches_stable_sort(n, bits):
     lib = bb.load_library()
@@ -49,6 +49,26 @@ def test_radix_sort_pairs_matches_stable_sort(n, bits):
     assert np.array_equal(gk, ek)
     # inputs untouched
     assert np.array_equal(kin.cpu().numpy().view(np.uint32), keys)
+
+
+def test_radix_sort_pairs_on_unaligned_views():
+    """Inputs that start 4 bytes into a buffer (no 16-byte alignment) sort the same."""
+    import torch
+
+    lib = bb.load_library()
+    n = 70_001
+    rng = np.random.default_rng(7)
+    keys = rng.integers(0, 1 << 31, n + 1, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n + 1, dtype=np.uint32)
+    kin = torch.from_numpy(keys.view(np.int32)).cuda()[1:]
+    vin = torch.from_numpy(vals.view(np.int32)).cuda()[1:]
+    kout, vout = torch.full_like(kin, -1), torch.full_like(vin, -1)
+    torch.cuda.synchronize()
+    assert lib.bb_radix_sort_pairs(dptr(kin), dptr(vin), dptr(kout), dptr(vout), n, 32, None) == bb.OK
+    torch.cuda.synchronize()
+    ek, ev = expected(keys[1:], vals[1:], 32)
+    assert np.array_equal(kout.cpu().numpy().view(np.uint32), ek)
+    assert np.array_equal(vout.cpu().numpy().view(np.uint32), ev)
 
 
 def test_radix_sort_pairs_rejects_bad_arguments():
