@@ -359,12 +359,12 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp
 // one frontier subtree left-first.  Per-thread counts are scanned so the emitted pairs keep
 // ascending partner order.
 template <bool EMIT>
-__global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, uint32_t n) {
+__global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, uint32_t n, int all) {
   __shared__ int s_fr[2][BB_FRONTIER];
   __shared__ uint32_t s_warp[BB_FRONTIER / 32];
   __shared__ uint32_t s_size;
   const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
-  if (blockIdx.x >= hc || d.hv_n[blockIdx.x] != BB_NONE) return;  // pool path took this query
+  if (blockIdx.x >= hc || (!all && d.hv_n[blockIdx.x] != BB_NONE)) return;  // pool path took this query
   const uint32_t qi = d.heavy_list[blockIdx.x];
   const int N = int(n), leaf0 = N - 1;
   const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
@@ -653,7 +653,7 @@ __global__ void k_heavy_totals(const DevState d) {
 }
 
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
-                  int cur) {
+                  int cur, uint32_t max_world_bodies) {
   (void)cur;
   if (n == 0) return;
   const int T = BB_THREADS;
@@ -676,16 +676,22 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);
   k_broad<false><<<bb, bt, 0, s>>>(d, n);
-  // two co-resident 1024-thread blocks per SM loop over the heavy slots
-  k_heavy_frontier<<<min(hb, 2u * uint32_t(sms)), BB_HV_THREADS, 0, s>>>(d, n);
-  k_heavy_walk<false><<<sms * 8, 128, 0, s>>>(d, n);
-  bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr, sc.scan_status + 5 * size_t(sc.scan_tiles),
-                 sc.scan_tile_ctr + 5, d.ctr);
-  k_heavy_totals<<<(hb + 255) / 256, 256, 0, s>>>(d);
-  k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n);
+  // The frontier pool is for worlds over BB_HV_BLOCK_LEAVES bodies; when no world is that large
+  // every heavy query takes the block traversal and the pool kernels are not launched at all
+  // (their GPU-wide 1024-thread blocks would only stall other streams' work).
+  const bool pool = max_world_bodies > BB_HV_BLOCK_LEAVES;
+  if (pool) {
+    // two co-resident 1024-thread blocks per SM loop over the heavy slots
+    k_heavy_frontier<<<min(hb, 2u * uint32_t(sms)), BB_HV_THREADS, 0, s>>>(d, n);
+    k_heavy_walk<false><<<sms * 8, 128, 0, s>>>(d, n);
+    bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr,
+                   sc.scan_status + 5 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 5, d.ctr);
+    k_heavy_totals<<<(hb + 255) / 256, 256, 0, s>>>(d);
+  }
+  k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n, pool ? 0 : 1);
   bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr);
   k_broad_copy<<<sms * 16, 256, 0, s>>>(d, n);
   k_broad<true><<<bb, bt, 0, s>>>(d, n);
-  k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n);
-  k_heavy_walk<true><<<sms * 8, 128, 0, s>>>(d, n);
+  k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n, pool ? 0 : 1);
+  if (pool) k_heavy_walk<true><<<sms * 8, 128, 0, s>>>(d, n);
 }

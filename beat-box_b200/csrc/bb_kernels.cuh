@@ -30,7 +30,8 @@ struct StepScratch {
 
 // bb_bvh.cu: Morton codes -> sort -> Karras LBVH -> refit -> broad phase
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
-                  int cur);
+                  int cur,
+                  uint32_t max_world_bodies);
 
 // bb_narrow.cu: narrow phase + warm start + manifold compaction + per-body lists
 void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,

@@ -538,8 +538,8 @@ __global__ void k_narrow_carry(const DevState d, int cur) {
 // key in the same body order, match features by the whole voxel/corner id, and keep their
 // own depth caps; other manifolds take the pair's old manifold under any key, either order.
 __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int cur, int warm, uint32_t k,
-                                         uint32_t ida, uint32_t idb, uint32_t fa, float3 pa, float3 pb,
-                                         const Contacts& m, bool vox) {
+                                         uint32_t ida, uint32_t idb, uint32_t fa, float3 pa, float3 pb, Contacts& m,
+                                         bool vox) {
   const int prv = cur ^ 1;
   // compute_basis (extensions.slang:262-272)
   float3 n = m.normal, t0;
@@ -547,25 +547,24 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
   else t0 = make_float3(0.f, -n.z, n.y);
   t0 = t0 * (1.0f / len3(t0));
   float3 t1 = cross3(t0, n);
-  // new contacts; inherited fields start at zero
-  float3 cpos[BB_MAX_CONTACTS];
-  float cpen[BB_MAX_CONTACTS];
-  uint32_t cfp[BB_MAX_CONTACTS], cwarm[BB_MAX_CONTACTS], cstick[BB_MAX_CONTACTS];
-  float4 clam[BB_MAX_CONTACTS];
-  float2 ckt[BB_MAX_CONTACTS];
-  float3 canca[BB_MAX_CONTACTS], cancb[BB_MAX_CONTACTS];
   const int cc = m.cc;
-  for (int c = 0; c < cc; ++c) {
-    cpos[c] = m.pos[c];
-    cpen[c] = vox ? m.pen[c] : fmaxf(m.pen[c], p.penetration_cap);  // extraction cap (:1575-1578)
-    cfp[c] = m.fp[c];
-    cwarm[c] = 0;
-    cstick[c] = 0;
-    clam[c] = make_float4(0, 0, 0, 0);
-    ckt[c] = make_float2(0, 0);
-    canca[c] = make_float3(0, 0, 0);
-    cancb[c] = make_float3(0, 0, 0);
-  }
+  for (int c = 0; c < cc; ++c) m.pen[c] = vox ? m.pen[c] : fmaxf(m.pen[c], p.penetration_cap);  // extraction cap (:1575-1578)
+  // Each new contact records the old contact it inherits from (src, -1: none) and whether the
+  // proximity pass gave it (pass2: then the old features, the tangent sign and anchor roles of
+  // a swapped pair apply); the inherited fields are read from the old contact when written.
+  uint32_t src_lo = 0xFFFFFFFFu, src_hi = 0xFFFFFFFFu;  // 8 x 8-bit old index, 0xFF = none
+  auto set_src = [&](int i, int j) {
+    if (i < 4) src_lo = (src_lo & ~(0xFFu << (8 * i))) | (uint32_t(j) << (8 * i));
+    else src_hi = (src_hi & ~(0xFFu << (8 * (i - 4)))) | (uint32_t(j) << (8 * (i - 4)));
+  };
+  auto get_src = [&](int i) -> int {
+    const uint32_t v = i < 4 ? (src_lo >> (8 * i)) & 0xFFu : (src_hi >> (8 * (i - 4))) & 0xFFu;
+    return v == 0xFFu ? -1 : int(v);
+  };
+  uint32_t pass2 = 0;
+  uint32_t ob = 0;
+  bool swapped = false;
+  float sgn = 1.f;
   int32_t err = 0x7FFFFFFF;
   if (warm) {
     // find the pair's manifold of the previous substep on the dynamic body's list
@@ -573,7 +572,6 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
     const uint32_t other = x == ida ? idb : ida;
     uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
     uint32_t old_slot = BB_NONE;
-    bool swapped = false;
     for (uint32_t e = s0; e < s1; ++e) {
       if (d.csr_partner[prv][e] != other) continue;
       const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
@@ -586,36 +584,27 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
       // Manifold::update_from_old (extensions.slang:306-473)
       int2 okc = d.m_keycc[prv][old_slot];
       float4 on4 = d.m_normal[prv][old_slot];
-      float sgn = swapped ? -1.f : 1.f;
+      sgn = swapped ? -1.f : 1.f;
       bool cross_key = m.key != okc.x || swapped;
       bool go = !cross_key || dot3(n, f3(on4) * sgn) > 0.7f;
       if (go) {
         const int occ = okc.y;
         uint32_t used_old = 0, matched_new = 0;
-        const uint32_t ob = old_slot * BB_MAX_CONTACTS;
+        ob = old_slot * BB_MAX_CONTACTS;
         if (!cross_key) {
           for (int i = 0; i < cc; ++i) {
             for (int j = 0; j < occ; ++j) {
               if (used_old & (1u << j)) continue;
               float4 op = d.c_pos[prv][ob + j];
               uint32_t ofp = __float_as_uint(d.c_anc_a[prv][ob + j].w);
-              bool feat = vox ? ofp == cfp[i]
-                              : (fp_in_inc(ofp) == fp_in_inc(cfp[i]) && fp_out_inc(ofp) == fp_out_inc(cfp[i]));
-              float3 dp = f3(op) - cpos[i];
+              bool feat = vox ? ofp == m.fp[i]
+                              : (fp_in_inc(ofp) == fp_in_inc(m.fp[i]) && fp_out_inc(ofp) == fp_out_inc(m.fp[i]));
+              float3 dp = f3(op) - m.pos[i];
               bool close = dot3(dp, dp) < 0.1f * 0.1f;
               if (feat && close) {
-                float4 ol = d.c_lam[prv][ob + j];
-                float4 okt = d.c_kt[prv][ob + j];
-                clam[i] = ol;
-                ckt[i] = make_float2(okt.x, okt.y);
-                cstick[i] = __float_as_uint(okt.z);
-                if (cstick[i] != 0) {
-                  canca[i] = f3(d.c_anc_a[prv][ob + j]);
-                  cancb[i] = f3(d.c_anc_b[prv][ob + j]);
-                }
-                float3 d2 = cpos[i] - f3(op);
-                if (dot3(d2, d2) < 0.01f) cpos[i] = f3(op);
-                cwarm[i] = warm_inc(__float_as_uint(okt.w));
+                set_src(i, j);
+                float3 d2 = m.pos[i] - f3(op);
+                if (dot3(d2, d2) < 0.01f) m.pos[i] = f3(op);
                 used_old |= 1u << j;
                 matched_new |= 1u << i;
                 break;
@@ -630,30 +619,19 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
             if (matched_new & (1u << i)) continue;
             for (int j = 0; j < occ; ++j) {
               if (used_old & (1u << j)) continue;
-              float3 dp = cpos[i] - f3(d.c_pos[prv][ob + j]);
+              float3 dp = m.pos[i] - f3(d.c_pos[prv][ob + j]);
               float d2 = dot3(dp, dp);
               if (d2 < best) { best = d2; bi = i; bj = j; }
             }
           }
           if (bi < 0) break;
-          float4 ol = d.c_lam[prv][ob + bj];
-          float4 okt = d.c_kt[prv][ob + bj];
-          clam[bi] = make_float4(ol.x, ol.y * sgn, ol.z, ol.w);
-          ckt[bi] = make_float2(okt.x, okt.y);
-          cstick[bi] = __float_as_uint(okt.z);
-          float4 oaa = d.c_anc_a[prv][ob + bj];
-          if (cstick[bi] != 0) {
-            float3 aa = f3(oaa), ab = f3(d.c_anc_b[prv][ob + bj]);
-            canca[bi] = swapped ? ab : aa;
-            cancb[bi] = swapped ? aa : ab;
-          }
-          cfp[bi] = __float_as_uint(oaa.w);
-          cwarm[bi] = warm_inc(__float_as_uint(okt.w));
+          set_src(bi, bj);
+          pass2 |= 1u << bi;
           matched_new |= 1u << bi;
           used_old |= 1u << bj;
         }
         float deep_new = 0.f, deep_old = 0.f;
-        for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, cpen[i]);
+        for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, m.pen[i]);
         for (int j = 0; j < occ; ++j) deep_old = fminf(deep_old, d.c_pos[prv][ob + j].w);
         err = int32_t(fminf(fmaxf((deep_new - deep_old) * 10000.0f, -32000.0f), 32000.0f));
       }
@@ -668,11 +646,32 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
   d.m_anchor_b[cur][k] = make_float4(pb.x, pb.y, pb.z, 0.f);
   const uint32_t cb = k * BB_MAX_CONTACTS;
   for (int c = 0; c < cc; ++c) {
-    d.c_pos[cur][cb + c] = f4(cpos[c], cpen[c]);
-    d.c_lam[cur][cb + c] = clam[c];
-    d.c_kt[cur][cb + c] = make_float4(ckt[c].x, ckt[c].y, __uint_as_float(cstick[c]), __uint_as_float(cwarm[c]));
-    d.c_anc_a[cur][cb + c] = f4(canca[c], __uint_as_float(cfp[c]));
-    d.c_anc_b[cur][cb + c] = f4(cancb[c], 0.f);
+    // new contacts start at zero; matched ones inherit impulses, penalties, stick and anchors
+    float4 lam = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 kt = make_float2(0.f, 0.f);
+    uint32_t stick = 0, wc = 0, fp = m.fp[c];
+    float3 aa = make_float3(0.f, 0.f, 0.f), ab = make_float3(0.f, 0.f, 0.f);
+    const int j = get_src(c);
+    if (j >= 0) {
+      const uint32_t oi = ob + uint32_t(j);
+      const bool p2 = (pass2 >> c) & 1u;
+      const float4 ol = d.c_lam[prv][oi], okt = d.c_kt[prv][oi], oaa = d.c_anc_a[prv][oi];
+      lam = p2 ? make_float4(ol.x, ol.y * sgn, ol.z, ol.w) : ol;
+      kt = make_float2(okt.x, okt.y);
+      stick = __float_as_uint(okt.z);
+      if (stick != 0) {
+        const float3 a0 = f3(oaa), b0 = f3(d.c_anc_b[prv][oi]);
+        aa = (p2 && swapped) ? b0 : a0;
+        ab = (p2 && swapped) ? a0 : b0;
+      }
+      if (p2) fp = __float_as_uint(oaa.w);
+      wc = warm_inc(__float_as_uint(okt.w));
+    }
+    d.c_pos[cur][cb + c] = f4(m.pos[c], m.pen[c]);
+    d.c_lam[cur][cb + c] = lam;
+    d.c_kt[cur][cb + c] = make_float4(kt.x, kt.y, __uint_as_float(stick), __uint_as_float(wc));
+    d.c_anc_a[cur][cb + c] = f4(aa, __uint_as_float(fp));
+    d.c_anc_b[cur][cb + c] = f4(ab, 0.f);
   }
   d.hit[k] = 1;
 }

@@ -195,6 +195,8 @@ struct bb_world_impl {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   uint32_t cap_n = 0, cap_p = 0, n = 0, n_dyn = 0;
+  uint32_t max_world_n = 0;  // batched worlds: bodies of the largest world
+  uint32_t max_world_bodies() const { return d.n_worlds > 1 ? max_world_n : n; }
   std::vector<Shape> shapes;
   std::vector<float> restitution;
   bb_solver_params params;
@@ -354,7 +356,7 @@ struct bb_world_impl {
     const int cur = parity ^ 1;
     k_begin_substep<<<1, 32, 0, stream>>>(d.ctr);
     cudaMemsetAsync(scratch_base, 0, scratch_bytes, stream);
-    bb_front_end(stream, d, params, n, sc, sms, cur);
+    bb_front_end(stream, d, params, n, sc, sms, cur, max_world_bodies());
     if (stop_stage >= 2) bb_narrow_phase(stream, d, params, n, sc, sms, cur, warm);
     last_cur = cur;
     if (stop_stage < 3) return;
@@ -502,6 +504,7 @@ bb_status bb_world_clear(void* world) {
   CU(cudaStreamSynchronize(w->stream));
   w->n = 0;
   w->n_dyn = 0;
+  w->max_world_n = 0;
   w->shapes.clear();
   w->restitution.clear();
   w->vox_table.clear();
@@ -736,6 +739,7 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
   CU(cudaMemcpyAsync(w->d.world_bounds + 2 * widx, bnd, sizeof(bnd), cudaMemcpyHostToDevice, w->stream));
   CU(cudaStreamSynchronize(w->stream));
   w->d.n_worlds = widx + 1;
+  w->max_world_n = std::max(w->max_world_n, count);
   w->invalidate_graphs();
   if (out_world_index) *out_world_index = widx;
   if (out_first_id) *out_first_id = first;
@@ -859,7 +863,7 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
       k_begin_substep<<<1, 32, 0, w->stream>>>(w->d.ctr);
       cudaMemsetAsync(w->scratch_base, 0, w->scratch_bytes, w->stream);
       cudaEventRecord(ev[0], w->stream);
-      bb_front_end(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur);
+      bb_front_end(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->max_world_bodies());
       cudaEventRecord(ev[1], w->stream);
       bb_narrow_phase(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, s == 0 ? warm_first : warm_rest);
       cudaEventRecord(ev[2], w->stream);

@@ -66,6 +66,20 @@ def workload(args):
     return sc, name
 
 
+def run_sort(args, rank: int, local_rank: int):
+    """The onesweep pair sort alone (bb_radix_sort_pairs on --sort-keys random keys): one JSON
+    line with sorted keys/s and its HBM roofline (68 algorithmic bytes per key)."""
+    if rank != 0:
+        return
+    pk = peaks()
+    r = sort_roofline(local_rank, float(pk.get("hbm_gbs", 6650.0)), n=args.sort_keys, reps=max(args.steps, 1))
+    print(json.dumps({"metric": "sorted keys/s", "value": r["keys"] / (r["ms_per_sort"] / 1000.0), "unit": "keys/s",
+                      "n_gpus": 1, "steps": max(args.steps, 1), "warmup": 1, "higher_is_better": True,
+                      "dtype": "u32", "data": "synthetic (uniform random 31-bit keys, seed 0)",
+                      "config": {"workload": f"bb_radix_sort_pairs: {r['keys']} 32-bit keys + 32-bit values"},
+                      "roofline": r}), flush=True)
+
+
 def sort_roofline(local_rank: int, peak_gbs: float, n: int = 1 << 26, reps: int = 5) -> dict:
     """The onesweep pair sort (the step's a4 kernels, through bb_radix_sort_pairs) on 2^26 random
     32-bit keys with 32-bit values, 1 GB in and out, so every pass streams from HBM.  Algorithmic
@@ -546,7 +560,7 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
     arrays = [bb.scene_request_arrays(sc) for sc in templates]
     p_pgs = bb.make_params(solver=bb.SOLVER_PGS_SOFT, iterations=10, relax_iterations=10, quirks=bb.QUIRKS_PHYSICAL)
     p_avbd = bb.make_params(solver=bb.SOLVER_AVBD, avbd_iterations=4, avbd_beta=10.0, quirks=bb.QUIRKS_PHYSICAL)
-    srv = bb.Server(hbm_budget_bytes=120 << 30, max_active=args.max_active, pairs_per_body=8, device=local_rank)
+    srv = bb.Server(hbm_budget_bytes=120 << 30, max_active=args.max_active, pairs_per_body=16, device=local_rank)
     clocks = sample_clocks(local_rank)
     rates = [float(x) for x in args.rates.split(",")]
     per_rate = []
@@ -583,7 +597,11 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
         ok = [r for r in res if r["result"] == bb.OK]
         lat = np.array([r["finish_s"] - r["submit_s"] for r in ok])
         span = max(r["finish_s"] for r in res) - min(r["submit_s"] for r in res)
-        per_rate.append({"rate_req_s": lam, "requests": len(res), "failed": len(res) - len(ok),
+        codes: dict = {}
+        for r in res:
+            if r["result"] != bb.OK:
+                codes[str(r["result"])] = codes.get(str(r["result"]), 0) + 1
+        per_rate.append({"rate_req_s": lam, "requests": len(res), "failed": len(res) - len(ok), "fail_codes": codes,
                          "body_steps_per_s": bodies / span if span > 0 else None,
                          "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
                          "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
@@ -621,9 +639,10 @@ def main():
                          "box_grid: the 1000-box grid; voxel_pile: concave voxel bodies")
     ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "sort"],
                     help="plain: one world (default); batched: config-4 batch of independent worlds; "
-                         "served: config-5 serving loop")
+                         "served: config-5 serving loop; sort: the a4 pair sort alone on --sort-keys keys")
+    ap.add_argument("--sort-keys", type=int, default=1 << 26)
     ap.add_argument("--rates", default="200,500,1000,2000,5000")
     ap.add_argument("--requests", type=int, default=60, help="requests per arrival rate (served mode)")
     ap.add_argument("--max-active", type=int, default=64)
@@ -643,6 +662,8 @@ def main():
     elif args.mode == "served":
         if rank == 0:
             run_served(args, rank, world_size, local_rank)
+    elif args.mode == "sort":
+        run_sort(args, rank, local_rank)
     else:
         run_ours(args, rank, world_size, local_rank)
 
