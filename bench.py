@@ -645,7 +645,7 @@ def main():
     ap.add_argument("--sort-keys", type=int, default=1 << 26)
     ap.add_argument("--rates", default="200,500,1000,2000,5000")
     ap.add_argument("--requests", type=int, default=60, help="requests per arrival rate (served mode)")
-    ap.add_argument("--max-active", type=int, default=64)
+    ap.add_argument("--max-active", type=int, default=8)
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--plain-stride", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
