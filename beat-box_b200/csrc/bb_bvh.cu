@@ -233,13 +233,95 @@ __global__ void k_refit(const DevState d, uint32_t n) {
 #define BB_HEAVY_CAP 8192u
 #define BB_FRONTIER 256
 
-// Child ch is worth visiting from query qi: it holds leaves in (qi, wend) and its box
-// overlaps the query box.  wend = n for one world; the end of the query's world otherwise.
-__device__ __forceinline__ bool bp_take(const DevState& d, int ch, int leaf0, int qi, int wend, float4 qmn, float4 qmx) {
-  bool take = ch >= leaf0 ? ((ch - leaf0) > qi && (ch - leaf0) < wend)
-                          : (d.range_last[ch] > qi && d.range_first[ch] < wend);
-  return take && box_overlap(qmn, qmx, d.node_box[2 * ch], d.node_box[2 * ch + 1]);
+// Internal node records for the traversals: both children's boxes, indices and leaf ranges in
+// one 80-byte record (5 float4), built after the refit.  A visit is then one dependent load
+// (instead of the child indices, then each child's range and box), and a leaf child is tested
+// from its parent's record without being visited.  Layout: (lmin.xyz, lmax.x), (lmax.yz,
+// rmin.xy), (rmin.z, rmax.xyz), (left, right, left last leaf, right last leaf), (left first
+// leaf, right first leaf, -, -).
+__global__ void k_node_recs(const DevState d, uint32_t n) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < 2 || p >= n - 1) return;
+  const int leaf0 = int(n) - 1;
+  const int2 c = d.child[p];
+  const float4 lmn = d.node_box[2 * c.x], lmx = d.node_box[2 * c.x + 1];
+  const float4 rmn = d.node_box[2 * c.y], rmx = d.node_box[2 * c.y + 1];
+  const int lf = c.x >= leaf0 ? c.x - leaf0 : d.range_first[c.x], ll = c.x >= leaf0 ? c.x - leaf0 : d.range_last[c.x];
+  const int rf = c.y >= leaf0 ? c.y - leaf0 : d.range_first[c.y], rl = c.y >= leaf0 ? c.y - leaf0 : d.range_last[c.y];
+  float4* r = d.node_rec + 5 * size_t(p);
+  r[0] = make_float4(lmn.x, lmn.y, lmn.z, lmx.x);
+  r[1] = make_float4(lmx.y, lmx.z, rmn.x, rmn.y);
+  r[2] = make_float4(rmn.z, rmx.x, rmx.y, rmx.z);
+  r[3] = make_float4(__int_as_float(c.x), __int_as_float(c.y), __int_as_float(ll), __int_as_float(rl));
+  r[4] = make_float4(__int_as_float(lf), __int_as_float(rf), 0.f, 0.f);
 }
+
+struct Kids {
+  int l, r;       // child nodes
+  bool tl, tr;    // worth visiting from query qi: leaves in (qi, wend) and a box overlapping the query's
+  int lspan, rspan;  // leaves under each
+};
+// wend = n for one world; the end of the query's world otherwise
+__device__ __forceinline__ Kids rec_take(const DevState& d, int p, int qi, int wend, float4 qmn, float4 qmx) {
+  const float4* r = d.node_rec + 5 * size_t(p);
+  const float4 a = r[0], b = r[1], c = r[2], e = r[3], f = r[4];
+  Kids k;
+  k.l = __float_as_int(e.x);
+  k.r = __float_as_int(e.y);
+  const int ll = __float_as_int(e.z), rl = __float_as_int(e.w), lf = __float_as_int(f.x), rf = __float_as_int(f.y);
+  k.lspan = ll - lf + 1;
+  k.rspan = rl - rf + 1;
+  k.tl = ll > qi && lf < wend &&
+         box_overlap(qmn, qmx, make_float4(a.x, a.y, a.z, 0.f), make_float4(a.w, b.x, b.y, 0.f));
+  k.tr = rl > qi && rf < wend &&
+         box_overlap(qmn, qmx, make_float4(b.z, b.w, c.x, 0.f), make_float4(c.y, c.z, c.w, 0.f));
+  return k;
+}
+
+// Left-first walk of the subtree at `root` (taken by the query already) for query qi: calls
+// leaf(j) for every partner j in ascending order.  Taken leaf children are reported from their
+// parent's record at once when nothing to their left is still pending; a right leaf child whose
+// left sibling subtree is pending goes on the stack as a marker.  Stops and returns false after
+// `budget` pops (the caller hands the query to a wider path).
+template <class F>
+__device__ __forceinline__ bool walk_query(const DevState& d, int root, int leaf0, int qi, int wend, float4 qmn,
+                                           float4 qmx, uint32_t budget, F&& leaf) {
+  if (root >= leaf0) {
+    leaf(uint32_t(root - leaf0));
+    return true;
+  }
+  int stack[BB_BVH_STACK];
+  int sp = 0;
+  stack[sp++] = root;
+  uint32_t pops = 0;
+  while (sp > 0) {
+    if (++pops > budget) return false;
+    const int node = stack[--sp];
+    if (node >= leaf0) {  // a marker: a taken leaf whose left neighbours are done
+      leaf(uint32_t(node - leaf0));
+      continue;
+    }
+    const Kids k = rec_take(d, node, qi, wend, qmn, qmx);
+    const bool l_leaf = k.l >= leaf0, r_leaf = k.r >= leaf0;
+    const bool l_push = k.tl && !l_leaf;
+    if (k.tl && l_leaf) leaf(uint32_t(k.l - leaf0));
+    if (k.tr) {
+      if (r_leaf && !l_push) {
+        leaf(uint32_t(k.r - leaf0));
+      } else if (sp < BB_BVH_STACK) {
+        stack[sp++] = k.r;
+      } else {
+        raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+      }
+    }
+    if (l_push) {
+      if (sp < BB_BVH_STACK) stack[sp++] = k.l;
+      else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
+    }
+  }
+  return true;
+}
+
 __device__ __forceinline__ int world_end(const DevState& d, uint32_t qi, uint32_t n) {
   if (d.n_worlds <= 1) return int(n);
   uint32_t w = d.sworld[qi];
@@ -265,44 +347,28 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
   const int leaf0 = N - 1;
   float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
   const int wend = world_end(d, i, n);
-  uint32_t out = EMIT ? d.pair_off[i] : 0u;
+  const uint32_t out = EMIT ? d.pair_off[i] : 0u;
   const uint32_t cap = d.pair_capacity;
-  uint32_t count = 0, visits = 0;
-  bool budgeted = !EMIT;
-  int stack[BB_BVH_STACK];
-  int sp = 0;
-  stack[sp++] = 0;
-  while (sp > 0) {
-    if (budgeted && ++visits > BB_BP_BUDGET) {
-      uint32_t slot = atomicAdd(&d.ctr->pad[4], 1u);
-      if (slot < BB_HEAVY_CAP) {
-        d.heavy_list[slot] = i;
-        d.is_heavy[i] = 1;
-        return;  // pair_cnt[i] is written by k_broad_heavy
-      }
-      budgeted = false;  // heavy list full: finish serially
+  uint32_t count = 0;
+  auto leaf = [&](uint32_t j) {
+    if (EMIT) {
+      const uint32_t k = out + count;
+      if (k < cap) d.pairs[k] = make_uint2(i, j);
+      else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+    } else if (count < BB_BP_STAGE) {
+      d.bp_stage[size_t(i) * BB_BP_STAGE + count] = j;
     }
-    int node = stack[--sp];
-    if (node >= leaf0) {
-      if (EMIT) {
-        uint32_t k = out + count;
-        if (k < cap) d.pairs[k] = make_uint2(i, uint32_t(node - leaf0));
-        else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
-      } else if (count < BB_BP_STAGE) {
-        d.bp_stage[size_t(i) * BB_BP_STAGE + count] = uint32_t(node - leaf0);
-      }
-      ++count;
-      continue;
+    ++count;
+  };
+  if (!walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, EMIT ? 0xFFFFFFFFu : BB_BP_BUDGET, leaf)) {
+    const uint32_t slot = atomicAdd(&d.ctr->pad[4], 1u);
+    if (slot < BB_HEAVY_CAP) {
+      d.heavy_list[slot] = i;
+      d.is_heavy[i] = 1;
+      return;  // pair_cnt[i] is written by the heavy path
     }
-    int2 c = d.child[node];
-    int kids[2] = {c.y, c.x};  // right first: the left child is popped first
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      int ch = kids[k];
-      if (!bp_take(d, ch, leaf0, int(i), wend, qmn, qmx)) continue;
-      if (sp < BB_BVH_STACK) stack[sp++] = ch;
-      else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
-    }
+    count = 0;  // heavy list full: walk it here after all
+    walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, 0xFFFFFFFFu, leaf);
   }
   if (!EMIT) {
     d.pair_cnt[i] = count;
@@ -384,9 +450,9 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
     if (node >= leaf0) {
       kid[c++] = node;  // a leaf entry stays in place
     } else if (node >= 0) {
-      int2 ch = d.child[node];
-      if (bp_take(d, ch.x, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.x;
-      if (bp_take(d, ch.y, leaf0, int(qi), wend, qmn, qmx)) kid[c++] = ch.y;
+      const Kids k = rec_take(d, node, int(qi), wend, qmn, qmx);
+      if (k.tl) kid[c++] = k.l;
+      if (k.tr) kid[c++] = k.r;
     }
     uint32_t total;
     const uint32_t pos = block_excl_scan(c, s_warp, total);
@@ -411,30 +477,14 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
     // EMIT: pass 0 counts (for the scan), pass 1 writes
     uint32_t cnt = 0;
     if (root >= 0) {
-      int stack[BB_BVH_STACK];
-      int sp = 0;
-      stack[sp++] = root;
-      while (sp > 0) {
-        int node = stack[--sp];
-        if (node >= leaf0) {
-          if (EMIT && pass == 1) {
-            uint32_t k = out + cnt;
-            if (k < d.pair_capacity) d.pairs[k] = make_uint2(qi, uint32_t(node - leaf0));
-            else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
-          }
-          ++cnt;
-          continue;
+      walk_query(d, root, leaf0, int(qi), wend, qmn, qmx, 0xFFFFFFFFu, [&](uint32_t j) {
+        if (EMIT && pass == 1) {
+          const uint32_t k = out + cnt;
+          if (k < d.pair_capacity) d.pairs[k] = make_uint2(qi, j);
+          else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
         }
-        int2 c = d.child[node];
-        if (bp_take(d, c.y, leaf0, int(qi), wend, qmn, qmx)) {
-          if (sp < BB_BVH_STACK) stack[sp++] = c.y;
-          else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
-        }
-        if (bp_take(d, c.x, leaf0, int(qi), wend, qmn, qmx)) {
-          if (sp < BB_BVH_STACK) stack[sp++] = c.x;
-          else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
-        }
-      }
+        ++cnt;
+      });
     }
     count = cnt;
     if (EMIT && pass == 0) {
@@ -500,28 +550,23 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
         const uint32_t idx = uint32_t(t) * BB_HV_PER_THREAD + e;
         node[e] = idx < size ? s_fr[cur][idx] : -1;
       }
-#pragma unroll
-      for (int e = 0; e < BB_HV_PER_THREAD; ++e)
-        ch[e] = (node[e] >= 0 && node[e] < leaf0) ? d.child[node[e]] : make_int2(-1, -1);
-      // take test of both children of every internal entry; leaves stay in place
+      // take test of both children of every internal entry (one record load each, issued
+      // together); leaves stay in place
       bool tk[2 * BB_HV_PER_THREAD];
       uint32_t span[2 * BB_HV_PER_THREAD];
       uint32_t c = 0;
 #pragma unroll
-      for (int e = 0; e < 2 * BB_HV_PER_THREAD; ++e) {
-        const int k = (e & 1) ? ch[e >> 1].y : ch[e >> 1].x;
-        tk[e] = false;
-        span[e] = 0;
-        if (k < 0) continue;
-        bool in_range;
-        if (k >= leaf0) {
-          in_range = (k - leaf0) > int(qi) && (k - leaf0) < wend;
-        } else {
-          const int rf = d.range_first[k], rl = d.range_last[k];
-          in_range = rl > int(qi) && rf < wend;
-          span[e] = uint32_t(rl - rf + 1);
-        }
-        tk[e] = in_range && box_overlap(qmn, qmx, d.node_box[2 * k], d.node_box[2 * k + 1]);
+      for (int e = 0; e < BB_HV_PER_THREAD; ++e) {
+        tk[2 * e] = tk[2 * e + 1] = false;
+        span[2 * e] = span[2 * e + 1] = 0;
+        ch[e] = make_int2(-1, -1);
+        if (node[e] < 0 || node[e] >= leaf0) continue;
+        const Kids k = rec_take(d, node[e], int(qi), wend, qmn, qmx);
+        ch[e] = make_int2(k.l, k.r);
+        tk[2 * e] = k.tl;
+        tk[2 * e + 1] = k.tr;
+        span[2 * e] = k.l >= leaf0 ? 0u : uint32_t(k.lspan);
+        span[2 * e + 1] = k.r >= leaf0 ? 0u : uint32_t(k.rspan);
       }
 #pragma unroll
       for (int e = 0; e < BB_HV_PER_THREAD; ++e) c += node[e] >= leaf0 ? 1u : uint32_t(tk[2 * e]) + uint32_t(tk[2 * e + 1]);
@@ -613,30 +658,14 @@ __global__ void k_heavy_walk(const DevState d, uint32_t n) {
     uint32_t out = 0;
     if (EMIT) out = d.pair_off[qi] + d.hv_off[e] - d.hv_off[d.hv_first[slot]];
     uint32_t cnt = 0;
-    int stack[BB_BVH_STACK];
-    int sp = 0;
-    stack[sp++] = int(d.hv_pool[e]);
-    while (sp > 0) {
-      const int node = stack[--sp];
-      if (node >= leaf0) {
-        if (EMIT) {
-          const uint32_t k = out + cnt;
-          if (k < d.pair_capacity) d.pairs[k] = make_uint2(qi, uint32_t(node - leaf0));
-          else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
-        }
-        ++cnt;
-        continue;
+    walk_query(d, int(d.hv_pool[e]), leaf0, int(qi), wend, qmn, qmx, 0xFFFFFFFFu, [&](uint32_t j) {
+      if (EMIT) {
+        const uint32_t k = out + cnt;
+        if (k < d.pair_capacity) d.pairs[k] = make_uint2(qi, j);
+        else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
       }
-      const int2 c = d.child[node];
-      if (bp_take(d, c.y, leaf0, int(qi), wend, qmn, qmx)) {
-        if (sp < BB_BVH_STACK) stack[sp++] = c.y;
-        else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
-      }
-      if (bp_take(d, c.x, leaf0, int(qi), wend, qmn, qmx)) {
-        if (sp < BB_BVH_STACK) stack[sp++] = c.x;
-        else raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
-      }
-    }
+      ++cnt;
+    });
     if (!EMIT) d.hv_cnt[e] = cnt;
   }
 }
@@ -672,6 +701,7 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   }
   k_build<<<blocks, T, 0, s>>>(d, n);
   k_refit<<<blocks, T, 0, s>>>(d, n);
+  k_node_recs<<<blocks, T, 0, s>>>(d, n);
   const uint32_t bt = p.broad_threads ? p.broad_threads : 128u;
   uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);

@@ -90,6 +90,7 @@ struct DevState {
   uint32_t *keys[2], *vals[2];  // vals[0] holds the sorted ids (= next substep's order)
   uint32_t* rank;               // body id -> sorted position
   float4* node_box;             // 2 float4 per node (min, max); internal 0..N-2, leaves N-1..
+  float4* node_rec;             // 5 float4 per internal node: both children's boxes, indices, leaf ranges
   int2* child;                  // internal node children
   int32_t* parent;              // parent of every node (root: -1)
   int32_t* range_last;          // last leaf covered by each internal node

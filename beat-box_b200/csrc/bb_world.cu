@@ -250,6 +250,7 @@ struct bb_world_impl {
     for (int k = 0; k < 2; ++k) { d.keys[k] = u32(N); d.vals[k] = u32(N); }
     d.rank = u32(N);
     d.node_box = f4(4 * N);
+    d.node_rec = f4(5 * N);
     d.child = dalloc<int2>(N, owned, err, stream);
     d.parent = dalloc<int32_t>(2 * N, owned, err, stream);
     d.range_last = dalloc<int32_t>(N, owned, err, stream);
