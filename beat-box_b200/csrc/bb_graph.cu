@@ -266,13 +266,22 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   // outcome depends only on its set, since the highest priority wins every contested colour).
   const int lane = threadIdx.x & 31;
   const uint32_t warp0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  // Once the uncoloured list fits in one block, block 0 runs the remaining rounds alone with
+  // block barriers (the other blocks go straight to the final grid barrier): the same rounds
+  // on the same sets, so the same colours, without two grid barriers per round.
+  bool local = false;
   for (uint32_t r = 1; r <= p.gc_rounds; ++r) {
     const uint32_t* L = r == 1 ? nullptr : d.gc_list[r & 1];
     const uint32_t nL = r == 1 ? M : *(volatile uint32_t*)&c->gc_list_n[r & 1];
     if (nL == 0) break;
-    if (tid == 0) c->gc_list_n[(r + 1) & 1] = 0;  // the list this round fills (last read two rounds ago)
+    if (!local && nL <= blockDim.x) {
+      local = true;
+      if (blockIdx.x != 0) break;
+    }
+    const uint32_t rtid = local ? threadIdx.x : tid, rstride = local ? blockDim.x : stride;
+    if (rtid == 0) c->gc_list_n[(r + 1) & 1] = 0;  // the list this round fills (last read two rounds ago)
     const unsigned long long tag = (unsigned long long)(epoch + r) << 32;
-    for (uint32_t i = tid; i < nL; i += stride) {
+    for (uint32_t i = rtid; i < nL; i += rstride) {
       const uint32_t m = L ? L[i] : i;
       const uint4 rec = d.gc_rec[m];
       const bool sa = rec.w & 1u, sb = rec.w & 2u;
@@ -284,9 +293,10 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
       if (!sa) atomicMax(&d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col], v);
       if (!sb) atomicMax(&d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col], v);
     }
-    grid_sync(c, sync, ep);
+    if (local) __syncthreads();
+    else grid_sync(c, sync, ep);
     uint32_t* next = d.gc_list[(r + 1) & 1];
-    for (uint32_t base = warp0; base < nL; base += stride) {  // warp-uniform trip count
+    for (uint32_t base = local ? (threadIdx.x & ~31u) : warp0; base < nL; base += rstride) {  // warp-uniform trips
       const uint32_t i = base + lane;
       bool keep = false;
       uint32_t m = 0;
@@ -317,8 +327,10 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
         if (keep) next[off + __popc(mask & ((1u << lane) - 1u))] = m;
       }
     }
-    grid_sync(c, sync, ep);
+    if (local) __syncthreads();
+    else grid_sync(c, sync, ep);
   }
+  if (local) grid_sync(c, sync, ep);  // block 0's rounds are done before anyone reads the colours
   uint32_t over = 0;
   for (uint32_t m = tid; m < M; m += stride) {
     uint32_t col = d.gc_color[m];

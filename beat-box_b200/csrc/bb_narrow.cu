@@ -1111,23 +1111,33 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
   }
 }
 
-// man_slot[man_index[k]] = k for every slot that collided; per-manifold statistics.
+// man_slot[man_index[k]] = k for every slot that collided; per-manifold statistics, reduced
+// over each warp before one atomic per warp.
 __global__ void k_compact(const DevState d, int cur) {
   const uint32_t S = slot_total(d);
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
-    if (!d.hit[k]) continue;
-    d.man_slot[cur][d.man_index[k]] = k;
-    int cc = d.m_keycc[cur][k].y;
-    uint32_t fresh = 0;
-    float deep = 0.f;
-    for (int c = 0; c < cc; ++c) {
-      const uint32_t ci = k * BB_MAX_CONTACTS + c;
-      if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
-      deep = fmaxf(deep, -d.c_pos[cur][ci].w);
+  const uint32_t lane = threadIdx.x & 31u, stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < S; base += stride) {  // warp-uniform
+    const uint32_t k = base + lane;
+    uint32_t cc = 0, fresh = 0, deep_bits = 0;
+    if (k < S && d.hit[k]) {
+      d.man_slot[cur][d.man_index[k]] = k;
+      cc = uint32_t(d.m_keycc[cur][k].y);
+      float deep = 0.f;
+      for (uint32_t c = 0; c < cc; ++c) {
+        const uint32_t ci = k * BB_MAX_CONTACTS + c;
+        if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
+        deep = fmaxf(deep, -d.c_pos[cur][ci].w);
+      }
+      deep_bits = deep > 0.f ? __float_as_uint(deep) : 0u;  // positive floats order as their bits
     }
-    atomicAdd(&d.ctr->contact_count, uint32_t(cc));
-    if (fresh) atomicAdd(&d.ctr->fresh, fresh);
-    if (deep > 0.f) atomicMax(&d.ctr->max_pen_bits, __float_as_uint(deep));
+    cc = __reduce_add_sync(0xFFFFFFFFu, cc);
+    fresh = __reduce_add_sync(0xFFFFFFFFu, fresh);
+    deep_bits = __reduce_max_sync(0xFFFFFFFFu, deep_bits);
+    if (lane == 0) {
+      if (cc) atomicAdd(&d.ctr->contact_count, cc);
+      if (fresh) atomicAdd(&d.ctr->fresh, fresh);
+      if (deep_bits) atomicMax(&d.ctr->max_pen_bits, deep_bits);
+    }
   }
 }
 
