@@ -161,3 +161,29 @@ def test_voxel_shape_inertia_from_the_shape_matches_scene():
     a = w.debug_read("body_inertia")
     k = int(np.nonzero((sc["shape"] == scenes.SHAPE_VOXEL) & (sc["voxel"] == 0))[0][0])
     assert np.array_equal(a[0, :3], sc["inv_inertia"][k]) and np.array_equal(a[0, 3:6], sc["inv_inertia_off"][k])
+
+
+def test_voxel_worlds_are_the_same_alone_and_in_a_batch():
+    """Two voxel piles stepped as independent worlds of one batch give the bits of each pile
+    stepped alone (six-slot voxel pairs, world-local colouring, world-prefixed sort)."""
+    a, b = scenes.voxel_pile(12, seed=5), scenes.voxel_pile(15, seed=6)
+    p = bb.make_params(solver=bb.SOLVER_PGS_SOFT, quirks=bb.QUIRKS_PHYSICAL)
+    alone = []
+    for sc in (a, b):
+        w = bb.World(sc["n"], pairs_per_body=64)
+        w.add_world(sc, sc["bounds"][0], sc["bounds"][1])
+        w.set_params(p)
+        for _ in range(40):
+            w.step(DT, 4)
+        alone.append(w.read_state())
+    w = bb.World(a["n"] + b["n"], pairs_per_body=64)
+    w.add_world(a, a["bounds"][0], a["bounds"][1])
+    w.add_world(b, b["bounds"][0], b["bounds"][1])
+    w.set_params(p)
+    for _ in range(40):
+        w.step(DT, 4)
+    both = w.read_state()
+    assert w.stats()["error_flags"] == 0
+    for k in both:
+        assert np.array_equal(both[k][: a["n"]], alone[0][k]), k
+        assert np.array_equal(both[k][a["n"]:], alone[1][k]), k

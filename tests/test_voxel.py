@@ -182,3 +182,8 @@ def test_voxel_resting_contacts_keep_their_identity(oracle_lib):
         assert o.stats()["fresh_contacts"] == 0
     # every contact inherited its impulses in each of the 20 substeps
     assert np.array_equal(oread(o, 9)["warm_start"][:4], np.minimum(w0 + 20, 255))
+
+
+def test_served_worlds_take_boxes_and_spheres_only():
+    with pytest.raises(ValueError):
+        bb.scene_request_arrays(scenes.voxel_pile(3))
