@@ -331,57 +331,48 @@ __device__ __forceinline__ int world_end(const DevState& d, uint32_t qi, uint32_
 // Left-first traversal for sorted query i.  EMIT=false counts every partner and keeps the first
 // BB_BP_STAGE of them in bp_stage (so k_broad_copy can place them once offsets are known);
 // EMIT=true re-walks only the queries that had more (is_heavy == 2) and writes their pairs.
-// EMIT=false: count every query's partners and stage the first BB_BP_STAGE of them; the block's
-// 128 rows of staged partners are collected in shared memory and flushed to bp_stage row by row,
-// one warp per row (coalesced), so k_broad_copy can place them once offsets are known.
-// EMIT=true: re-walk the queries with more partners (is_heavy == 2) and write their pairs.
-#define BB_BP_THREADS 128
 template <bool EMIT>
-__global__ void __launch_bounds__(BB_BP_THREADS) k_broad(const DevState d, uint32_t n) {
-  __shared__ uint32_t s_stage[EMIT ? 1 : BB_BP_THREADS * BB_BP_STAGE];
-  __shared__ uint32_t s_cnt[EMIT ? 1 : BB_BP_THREADS];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (n < 2) {
+    if (!EMIT) {
+      d.pair_cnt[i] = 0;
+      d.is_heavy[i] = 0;
+    }
+    return;
+  }
+  if (EMIT && d.is_heavy[i] != 2u) return;
   const int N = int(n);
   const int leaf0 = N - 1;
+  float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
+  const int wend = world_end(d, i, n);
+  const uint32_t out = EMIT ? d.pair_off[i] : 0u;
+  const uint32_t cap = d.pair_capacity;
   uint32_t count = 0;
-  if (i < n && n >= 2 && (!EMIT || d.is_heavy[i] == 2u)) {
-    const float4 qmn = d.node_box[2 * (leaf0 + i)], qmx = d.node_box[2 * (leaf0 + i) + 1];
-    const int wend = world_end(d, i, n);
-    const uint32_t out = EMIT ? d.pair_off[i] : 0u;
-    const uint32_t cap = d.pair_capacity;
-    auto leaf = [&](uint32_t j) {
-      if (EMIT) {
-        const uint32_t k = out + count;
-        if (k < cap) d.pairs[k] = make_uint2(i, j);
-        else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
-      } else if (count < BB_BP_STAGE) {
-        s_stage[threadIdx.x * BB_BP_STAGE + count] = j;
-      }
-      ++count;
-    };
-    if (!walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, EMIT ? 0xFFFFFFFFu : BB_BP_BUDGET, leaf)) {
-      const uint32_t slot = atomicAdd(&d.ctr->pad[4], 1u);
-      if (slot < BB_HEAVY_CAP) {
-        d.heavy_list[slot] = i;
-        d.is_heavy[i] = 1;
-        count = BB_NONE;  // pair_cnt[i] is written by the heavy path
-      } else {
-        count = 0;  // heavy list full: walk it here after all
-        walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, 0xFFFFFFFFu, leaf);
-      }
+  auto leaf = [&](uint32_t j) {
+    if (EMIT) {
+      const uint32_t k = out + count;
+      if (k < cap) d.pairs[k] = make_uint2(i, j);
+      else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+    } else if (count < BB_BP_STAGE) {
+      d.bp_stage[size_t(i) * BB_BP_STAGE + count] = j;
     }
+    ++count;
+  };
+  if (!walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, EMIT ? 0xFFFFFFFFu : BB_BP_BUDGET, leaf)) {
+    const uint32_t slot = atomicAdd(&d.ctr->pad[4], 1u);
+    if (slot < BB_HEAVY_CAP) {
+      d.heavy_list[slot] = i;
+      d.is_heavy[i] = 1;
+      return;  // pair_cnt[i] is written by the heavy path
+    }
+    count = 0;  // heavy list full: walk it here after all
+    walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, 0xFFFFFFFFu, leaf);
   }
-  if (EMIT) return;
-  if (i < n && count != BB_NONE) {
+  if (!EMIT) {
     d.pair_cnt[i] = count;
     d.is_heavy[i] = count > BB_BP_STAGE ? 2u : 0u;
-  }
-  s_cnt[threadIdx.x] = (i < n && count != BB_NONE) ? min(count, BB_BP_STAGE) : 0u;
-  __syncthreads();
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  for (uint32_t r = warp; r < blockDim.x; r += blockDim.x / 32u) {  // blockDim.x: 32, 64 or 128
-    const uint32_t q = blockIdx.x * blockDim.x + r;
-    if (q < n && lane < s_cnt[r]) d.bp_stage[size_t(q) * BB_BP_STAGE + lane] = s_stage[r * BB_BP_STAGE + lane];
   }
 }
 

@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
     for (uint32_t base = local ? (threadIdx.x & ~31u) : warp0; base < nL; base += rstride) {  // warp-uniform trips
       const uint32_t i = base + lane;
       bool keep = false;
-      uint32_t m = 0;
+      uint32_t m = 0, used = 0;  // used: colour + 1 of a committed manifold
       if (i < nL) {
         m = L ? L[i] : i;
         const uint32_t col = d.gc_choice[m];
@@ -314,11 +314,13 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
             d.gc_color[m] = col;
             if (!sa) atomicOr(&d.gc_mask[rec.x], 1u << col);
             if (!sb) atomicOr(&d.gc_mask[rec.y], 1u << col);
-            atomicMax(&c->gc_colors, col + 1u);
+            used = col + 1u;
             keep = false;
           }
         }
       }
+      used = __reduce_max_sync(0xFFFFFFFFu, used);  // one colour-count update per warp
+      if (lane == 0 && used) atomicMax(&c->gc_colors, used);
       const unsigned mask = __ballot_sync(0xFFFFFFFFu, keep);
       if (mask) {
         uint32_t off = 0;

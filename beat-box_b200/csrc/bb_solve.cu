@@ -384,7 +384,10 @@ __global__ void k_pgs_count(const DevState d, int cur) {
     const uint2 b = d.m_bodies[cur][slot];
     const bool skip = !awake(d.flags[b.x]) && !awake(d.flags[b.y]);
     d.pgs_cnt[k] = skip ? 0u : uint32_t(d.m_keycc[cur][slot].y);
-    if (!skip) d.colour_awake[min(d.gc_color[list[k]], uint32_t(BB_MAX_COLORS))] = 1u;
+    if (!skip) {  // set once: most threads only read the flag (33 hot words otherwise take every store)
+      uint32_t* f = &d.colour_awake[min(d.gc_color[list[k]], uint32_t(BB_MAX_COLORS))];
+      if (*f == 0u) *f = 1u;
+    }
   }
 }
 
