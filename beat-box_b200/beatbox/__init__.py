@@ -36,6 +36,8 @@ QUIRKS_REFERENCE, QUIRKS_PHYSICAL = 7, 0
 BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
 SCHEDULE_DATAFLOW, SCHEDULE_COLOUR_BARRIER = 0, 1
 SORT_STATIC_MAX_KEYS = 262144
+EDGE_COLOR_OVERFLOW = 0xFFFFFFFF
+EDGE_COLOR_RESTING = 0xFFFFFFFE  # the manifold's island has no awake body: not coloured, not solved
 DBG = dict(morton=1, sorted_keys=2, sorted_ids=3, lbvh_child=4, leaf_aabb=5, node_aabb=6, pairs=7,
            manifolds=8, contacts=9, edge_colors=10, body_colors=11, islands=12, support_depth=13, body_inertia=14)
 

@@ -19,7 +19,8 @@
 
 #define BB_MAX_CONTACTS 8
 #define BB_MAX_COLORS 32
-#define BB_UNCOLORED 0xFFFFFFFFu
+#define BB_UNCOLORED BB_EDGE_COLOR_OVERFLOW
+#define BB_RESTING BB_EDGE_COLOR_RESTING  // a manifold whose island has no awake body (not coloured)
 #define BB_NONE 0xFFFFFFFFu
 #define BB_SLEEP_VETO 0x80000000u
 #define BB_SLEEP_MASK 0x7FFFFFFFu
@@ -64,6 +65,7 @@ struct DevCounters {
   uint32_t gc_list_n[2];   // edge colouring: sizes of the alternating uncoloured-manifold lists
   uint32_t hv_pool_n;      // broad phase: frontier entries of the heavy queries
   uint32_t slot_count;     // worlds with voxel shapes: manifold slots (6 per voxel pair, else 1)
+  uint32_t slots_of[2];    // manifold slots of the narrow phase that last wrote contact buffer 0 / 1
 };
 
 // Voxel shape on the device (VoxelShape, include/shared.inl:938-951) with the body-frame box
@@ -141,6 +143,7 @@ struct DevState {
   uint32_t* man_index;   // per pair slot: exclusive scan of hit
   // islands
   uint32_t *uf_parent, *is_root, *root_rank, *island;
+  uint32_t* cc_mark;       // per body id: substep number when its old component must start over
   uint32_t* island_start;  // per-island path: first sorted manifold of each island
   // colouring
   uint32_t* gc_color;    // per compact manifold
@@ -149,6 +152,7 @@ struct DevState {
   uint4* gc_rec;         // per compact manifold: body a, body b, pair hash, static bits
   uint32_t* gc_list[2];  // manifolds still uncoloured after a round (alternating)
   uint32_t* gc_mask;     // per body
+  uint32_t* gc_island_tag; // per island: colouring epoch + 1 when one of its bodies is awake
   unsigned long long* gc_owner; // per body x 32 colours: (epoch << 32) | priority
   uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies
   uint32_t* bucket_start; // 34 + 32*L entries

@@ -66,10 +66,30 @@ __global__ void __launch_bounds__(BB_CC_THREADS, 1) k_components(const DevState 
   uint32_t* changed = &c->pad[2];  // two alternating per-round flags (the AVBD colouring reuses them later)
   uint32_t ep = 0;
   uint32_t* parent = d.uf_parent;
-  for (uint32_t i = tid; i < n; i += stride) parent[i] = (d.flags[i] & BB_BODY_DYNAMIC) ? i : BB_NONE;
+  // Start from the last substep's roots where that is exact.  A last-substep component whose
+  // bodies are all dynamic and were not awake at either narrow phase (frozen bit 1) keeps every
+  // one of its manifolds (two such bodies keep their poses, so their pairs and manifolds
+  // persist), so it lies inside one component now, and its root (its smallest id) is a valid
+  // parent for its bodies: parents stay <= ids within the component, and the rounds below
+  // converge to the same smallest ids.  Every other body starts alone, and any body that is not
+  // such a body marks its old root, so its old component starts over.  Marks carry this
+  // substep's number; a stale mark or a stray old parent can only make a component start over.
+  const uint32_t mark = c->substeps;
+  for (uint32_t i = tid; i < n; i += stride) {
+    const bool keep = (d.flags[i] & BB_BODY_DYNAMIC) && (d.frozen[i] & 2u);
+    const uint32_t old = parent[i];
+    if (!keep && old < n) d.cc_mark[old] = mark;
+  }
   if (tid == 0) {
     changed[0] = 0;
     changed[1] = 0;
+  }
+  grid_sync(c, sync, ep);
+  for (uint32_t i = tid; i < n; i += stride) {  // each thread reads and writes only parent[i]
+    const bool dyn = d.flags[i] & BB_BODY_DYNAMIC;
+    const uint32_t old = parent[i];
+    const bool keep = dyn && (d.frozen[i] & 2u) && old < n && d.cc_mark[old] != mark;
+    parent[i] = !dyn ? BB_NONE : keep ? old : i;
   }
   grid_sync(c, sync, ep);
   uint32_t r = 0;
@@ -243,36 +263,71 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   uint32_t* sync = &c->sync_count[0];
   uint32_t ep = 0;
-  for (uint32_t i = tid; i < n; i += stride) d.gc_mask[i] = 0;
-  for (uint32_t m = tid; m < M; m += stride) {
-    const uint32_t slot = d.man_slot[cur][m];
-    uint2 b = d.m_bodies[cur][slot];
-    int key = d.m_keycc[cur][slot].x;
-    const uint32_t la = local_id(d, b.x), lb = local_id(d, b.y);
-    uint32_t lo = min(la, lb), hi = max(la, lb);
-    const uint32_t pid = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
-    d.gc_pid[m] = pid;
-    d.gc_color[m] = BB_UNCOLORED;
-    const uint32_t st = ((d.flags[b.x] & BB_BODY_DYNAMIC) ? 0u : 1u) | ((d.flags[b.y] & BB_BODY_DYNAMIC) ? 0u : 2u);
-    d.gc_rec[m] = make_uint4(b.x, b.y, pid, st);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  // Islands with an awake body get this launch's tag.  The rounds below are local to a
+  // connected component of the conflict graph (manifolds sharing a dynamic body), and those
+  // components are exactly the islands' manifold sets (k_components links every manifold).  So
+  // leaving out the manifolds of islands with no awake body changes no other manifold's colour;
+  // the solve skips those manifolds anyway (both bodies asleep or static), so they are marked
+  // BB_RESTING and sorted behind the overflow bucket without being coloured.
+  const uint32_t itag = epoch + 1u;  // never 0 (epochs step by 64), so zeroed tags never match
+  for (uint32_t i = tid; i < n; i += stride) {
+    d.gc_mask[i] = 0;
+    const uint32_t f = d.flags[i];
+    if ((f & BB_BODY_DYNAMIC) && !(f & BB_BODY_SLEEPING)) {
+      const uint32_t isl = d.island[i];
+      if (isl != BB_NONE && d.gc_island_tag[isl] != itag) d.gc_island_tag[isl] = itag;
+    }
   }
   if (tid == 0) {
     c->gc_colors = 0;
     c->gc_list_n[0] = 0;
+    c->gc_list_n[1] = 0;
   }
   grid_sync(c, sync, ep);
-  // Round r bids and commits over the manifolds still uncoloured when it starts: all of them in
-  // round 1, afterwards the list the previous round's commit left (in any order: a round's
-  // outcome depends only on its set, since the highest priority wins every contested colour).
-  const int lane = threadIdx.x & 31;
-  const uint32_t warp0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  // round 1's list: the manifolds of islands with an awake body (a warp appends its lanes at once)
+  for (uint32_t base = warp0; base < M; base += stride) {  // warp-uniform trips
+    const uint32_t m = base + lane;
+    bool colour = false;
+    if (m < M) {
+      const uint32_t slot = d.man_slot[cur][m];
+      uint2 b = d.m_bodies[cur][slot];
+      int key = d.m_keycc[cur][slot].x;
+      const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+      const bool da = fa & BB_BODY_DYNAMIC, db = fb & BB_BODY_DYNAMIC;
+      const uint32_t isl = da ? d.island[b.x] : db ? d.island[b.y] : BB_NONE;
+      colour = isl != BB_NONE && d.gc_island_tag[isl] == itag;
+      if (colour) {
+        const uint32_t la = local_id(d, b.x), lb = local_id(d, b.y);
+        uint32_t lo = min(la, lb), hi = max(la, lb);
+        const uint32_t pid = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
+        d.gc_pid[m] = pid;
+        d.gc_rec[m] = make_uint4(b.x, b.y, pid, (da ? 0u : 1u) | (db ? 0u : 2u));
+      }
+      d.gc_color[m] = colour ? BB_UNCOLORED : BB_RESTING;
+    }
+    const unsigned mask = __ballot_sync(0xFFFFFFFFu, colour);
+    if (mask) {
+      uint32_t off = 0;
+      if (lane == 0) off = atomicAdd(&c->gc_list_n[1], uint32_t(__popc(mask)));
+      off = __shfl_sync(0xFFFFFFFFu, off, 0);
+      if (colour) d.gc_list[1][off + __popc(mask & ((1u << lane) - 1u))] = m;
+    }
+  }
+  grid_sync(c, sync, ep);
+  // Round r bids and commits over the manifolds still uncoloured when it starts: in round 1 all
+  // manifolds of islands with an awake body (the identity list when that is all of them),
+  // afterwards the list the previous round's commit left (in any order: a round's outcome
+  // depends only on its set, since the highest priority wins every contested colour).
+  const uint32_t n1 = *(volatile uint32_t*)&c->gc_list_n[1];
   // Once the uncoloured list fits in one block, block 0 runs the remaining rounds alone with
   // block barriers (the other blocks go straight to the final grid barrier): the same rounds
   // on the same sets, so the same colours, without two grid barriers per round.
   bool local = false;
   for (uint32_t r = 1; r <= p.gc_rounds; ++r) {
-    const uint32_t* L = r == 1 ? nullptr : d.gc_list[r & 1];
-    const uint32_t nL = r == 1 ? M : *(volatile uint32_t*)&c->gc_list_n[r & 1];
+    const uint32_t* L = r == 1 && n1 == M ? nullptr : d.gc_list[r & 1];
+    const uint32_t nL = r == 1 ? n1 : *(volatile uint32_t*)&c->gc_list_n[r & 1];
     if (nL == 0) break;
     if (!local && nL <= blockDim.x) {
       local = true;
@@ -334,17 +389,17 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   }
   if (local) grid_sync(c, sync, ep);  // block 0's rounds are done before anyone reads the colours
   uint32_t over = 0;
-  for (uint32_t m = tid; m < M; m += stride) {
+  for (uint32_t m = tid; m < M; m += stride) {  // keys: colour, 32 = overflow, 33 = resting
     uint32_t col = d.gc_color[m];
     if (col == BB_UNCOLORED) ++over;
-    d.bucket_keys[0][m] = col == BB_UNCOLORED ? BB_MAX_COLORS : col;
+    d.bucket_keys[0][m] = col == BB_UNCOLORED ? BB_MAX_COLORS : col == BB_RESTING ? BB_MAX_COLORS + 1 : col;
     d.bucket_vals[0][m] = m;
   }
   if (over) atomicAdd(&c->gc_overflow, over);
   if (tid == 0) c->gc_epoch = epoch + 64u;
 }
 
-// bucket_start[0..33]: start of colour c (32 = overflow), [33] = M
+// bucket_start[0..34]: start of colour c (32 = overflow, 33 = resting manifolds), [34] = M
 __global__ void k_bucket_starts(const uint32_t* hist_scan, const uint32_t* n_ptr, uint32_t* starts, int nb) {
   int t = threadIdx.x;
   if (t < nb) starts[t] = hist_scan[t];
@@ -368,5 +423,5 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
   uint32_t* hist = sc.sort_hist + 1 * BB_HIST_REGION;
   bb_launch_sort(s, keys, vals, &d.ctr->manifold_count, d.pair_capacity, 1, 0, hist,
                  sc.sort_status + 6 * size_t(sc.sort_tiles) * 256, sc.sort_tile_ctr + 6, d.ctr, sms);
-  k_bucket_starts<<<1, 64, 0, s>>>(hist + 8 * 256, &d.ctr->manifold_count, d.bucket_start, BB_MAX_COLORS + 1);
+  k_bucket_starts<<<1, 64, 0, s>>>(hist + 8 * 256, &d.ctr->manifold_count, d.bucket_start, BB_MAX_COLORS + 2);
 }

@@ -423,6 +423,7 @@ __device__ __forceinline__ bool np_awake(uint32_t f) { return (f & BB_BODY_DYNAM
 __global__ void k_np_classify(const DevState d, int cur, int warm) {
   const uint32_t S = slot_total(d);
   const int lane = threadIdx.x & 31;
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.ctr->slots_of[cur] = S;  // read by the next substep's carry
   for (uint32_t base = blockIdx.x * blockDim.x; base < S; base += gridDim.x * blockDim.x) {
     const uint32_t k = base + threadIdx.x;
     int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body, 3 frozen
@@ -463,42 +464,89 @@ __global__ void k_np_classify(const DevState d, int cur, int warm) {
 // impulses, penalties, stick anchors -- with warm-start counts + 1 and the extraction trend 0,
 // which is what recomputing the same poses and matching every contact by feature gives.  A
 // frozen pair without a manifold last substep goes to the ordinary lists and is computed.
+__device__ __forceinline__ void carry_contact(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni) {
+  d.c_pos[cur][ni] = d.c_pos[prv][oi];
+  d.c_lam[cur][ni] = d.c_lam[prv][oi];
+  float4 kt = d.c_kt[prv][oi];
+  kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
+  d.c_kt[cur][ni] = kt;
+  const bool stick = __float_as_uint(kt.z) != 0u;
+  const float4 aa = d.c_anc_a[prv][oi], ab = d.c_anc_b[prv][oi];
+  d.c_anc_a[cur][ni] = stick ? aa : make_float4(0.f, 0.f, 0.f, aa.w);
+  d.c_anc_b[cur][ni] = stick ? make_float4(ab.x, ab.y, ab.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Every load of a manifold's header and of its first four contacts is issued before the first
+// store (the stores could alias the loads as far as the compiler knows), so the copy costs one
+// memory round trip rather than one per contact.
 __device__ __forceinline__ void carry_copy(const DevState& d, int cur, uint32_t os, uint32_t dst, uint32_t ida,
                                            uint32_t idb) {
   const int prv = cur ^ 1;
   const int2 kc = d.m_keycc[prv][os];
-  const float4 n4 = d.m_normal[prv][os];
+  const float4 n4 = d.m_normal[prv][os], t04 = d.m_t0[prv][os], t14 = d.m_t1[prv][os];
+  const float4 pa = d.pos[ida], pb = d.pos[idb];
+  float4 cp[4], cl[4], ck[4], ca[4], cb[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (c < kc.y) {
+      const uint32_t oi = os * BB_MAX_CONTACTS + c;
+      cp[c] = d.c_pos[prv][oi];
+      cl[c] = d.c_lam[prv][oi];
+      ck[c] = d.c_kt[prv][oi];
+      ca[c] = d.c_anc_a[prv][oi];
+      cb[c] = d.c_anc_b[prv][oi];
+    }
+  }
   d.m_bodies[cur][dst] = make_uint2(ida, idb);
   d.m_keycc[cur][dst] = kc;
   d.m_normal[cur][dst] = make_float4(n4.x, n4.y, n4.z, __int_as_float(0));
-  d.m_t0[cur][dst] = d.m_t0[prv][os];
-  d.m_t1[cur][dst] = d.m_t1[prv][os];
-  const float4 pa = d.pos[ida], pb = d.pos[idb];
+  d.m_t0[cur][dst] = t04;
+  d.m_t1[cur][dst] = t14;
   d.m_anchor_a[cur][dst] = make_float4(pa.x, pa.y, pa.z, 0.f);
   d.m_anchor_b[cur][dst] = make_float4(pb.x, pb.y, pb.z, 0.f);
-  for (int c = 0; c < kc.y; ++c) {
-    const uint32_t oi = os * BB_MAX_CONTACTS + c, ni = dst * BB_MAX_CONTACTS + c;
-    d.c_pos[cur][ni] = d.c_pos[prv][oi];
-    d.c_lam[cur][ni] = d.c_lam[prv][oi];
-    float4 kt = d.c_kt[prv][oi];
-    kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
-    d.c_kt[cur][ni] = kt;
-    const bool stick = __float_as_uint(kt.z) != 0u;
-    const float4 aa = d.c_anc_a[prv][oi], ab = d.c_anc_b[prv][oi];
-    d.c_anc_a[cur][ni] = stick ? aa : make_float4(0.f, 0.f, 0.f, aa.w);
-    d.c_anc_b[cur][ni] = stick ? make_float4(ab.x, ab.y, ab.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (c < kc.y) {
+      const uint32_t ni = dst * BB_MAX_CONTACTS + c;
+      d.c_pos[cur][ni] = cp[c];
+      d.c_lam[cur][ni] = cl[c];
+      float4 kt = ck[c];
+      kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
+      d.c_kt[cur][ni] = kt;
+      const bool stick = __float_as_uint(kt.z) != 0u;
+      d.c_anc_a[cur][ni] = stick ? ca[c] : make_float4(0.f, 0.f, 0.f, ca[c].w);
+      d.c_anc_b[cur][ni] = stick ? make_float4(cb[c].x, cb[c].y, cb[c].z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
   }
+  for (int c = 4; c < kc.y; ++c) carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c);
   d.hit[dst] = 1;
 }
 
+// A frozen pair's manifold of the previous substep is found at the pair's own slot when the
+// slot held a manifold of the same two bodies in the same order then: that is the pair's only
+// non-voxel manifold (key < 90; a voxel pair's keys are 90..95), the one the search through the
+// body's manifold list would find.  While no pair ahead of it came or went, every frozen pair
+// takes this path; the others search.  Slots past the previous substep's count are not read
+// (they hold older manifolds).
 __global__ void k_narrow_carry(const DevState d, int cur) {
   const int prv = cur ^ 1;
   const uint32_t S = slot_total(d);
+  const uint32_t S_prv = min(d.ctr->slots_of[prv], d.pair_capacity);
   const uint32_t nc = d.ctr->np_counts[3];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
     const uint32_t s = d.carry_list[t];
     const uint2 pr = d.pairs[slot_pair_of(d, s)];
+    int2 okc = make_int2(-1, 0);
+    uint2 ob = make_uint2(BB_NONE, BB_NONE);
+    if (s < S_prv) {
+      okc = d.m_keycc[prv][s];
+      ob = d.m_bodies[prv][s];
+    }
     const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
+    if (okc.x >= 0 && okc.x < 90 && ob.x == ida && ob.y == idb) {
+      carry_copy(d, cur, s, s, ida, idb);
+      continue;
+    }
     const uint32_t fa = d.flags[ida];
     const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
     const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
@@ -1123,10 +1171,13 @@ __global__ void k_compact(const DevState d, int cur) {
       d.man_slot[cur][d.man_index[k]] = k;
       cc = uint32_t(d.m_keycc[cur][k].y);
       float deep = 0.f;
-      for (uint32_t c = 0; c < cc; ++c) {
-        const uint32_t ci = k * BB_MAX_CONTACTS + c;
-        if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
-        deep = fmaxf(deep, -d.c_pos[cur][ci].w);
+#pragma unroll
+      for (uint32_t c = 0; c < BB_MAX_CONTACTS; ++c) {  // unrolled: the contacts' loads go out together
+        if (c < cc) {
+          const uint32_t ci = k * BB_MAX_CONTACTS + c;
+          if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
+          deep = fmaxf(deep, -d.c_pos[cur][ci].w);
+        }
       }
       deep_bits = deep > 0.f ? __float_as_uint(deep) : 0u;  // positive floats order as their bits
     }
@@ -1161,7 +1212,11 @@ __global__ void k_csr_fill(const DevState d, int cur) {
 __global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  d.frozen[i] = np_awake(d.flags[i]) ? 0u : 1u;  // read by the next substep's classification
+  // bit 0: not awake now (read by the next substep's classification); bit 1: not awake at the
+  // last narrow phase either, so every pair of two such bodies is carried or recomputed from
+  // unchanged poses (read by this substep's connected components)
+  const uint32_t now = np_awake(d.flags[i]) ? 0u : 1u;
+  d.frozen[i] = now | ((d.frozen[i] & now) << 1);
   uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
   uint32_t* L = d.csr_list[cur];
   for (uint32_t a = s0 + 1; a < s1; ++a) {

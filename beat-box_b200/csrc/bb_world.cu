@@ -293,6 +293,7 @@ struct bb_world_impl {
     d.uf_parent = u32(N); d.is_root = u32(N); d.root_rank = u32(N); d.island = u32(N);
     d.island_start = u32(N + 2);
     d.gc_color = u32(P); d.gc_pid = u32(P); d.gc_choice = u32(P); d.gc_mask = u32(N);
+    d.gc_island_tag = u32(N); d.cc_mark = u32(N);
     d.gc_owner = dalloc<unsigned long long>(N * BB_MAX_COLORS, owned, err, stream);
     for (int k = 0; k < 2; ++k) { d.bucket_keys[k] = u32(P); d.bucket_vals[k] = u32(P); }
     d.bucket_start = u32(64);

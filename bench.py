@@ -492,6 +492,14 @@ def run_batched(args, rank: int, world_size: int, local_rank: int):
     if dist is not None:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = sum(sizes) * e2e_steps / float(e2e_t.item())
+    # per-stage CUDA-event split over a few profiled steps (after the timed and end-to-end runs)
+    prof_steps = max(1, min(args.steps, 5))
+    w.set_profiling(True)
+    for _ in range(prof_steps):
+        w.step(DT, SUBSTEPS)
+    w.sync()
+    stages = {k: v / (prof_steps * SUBSTEPS) for k, v in w.stage_times().items()}
+    w.set_profiling(False)
     w.close()
 
     # plain path: every plain_stride-th of this rank's worlds alone, same kernels, same step window
@@ -534,7 +542,8 @@ def run_batched(args, rank: int, world_size: int, local_rank: int):
                 "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": total * 52,
                         "d2h_bytes_per_step": total * 52, "steps": e2e_steps,
                         "what": "bb_write_state + bb_step + bb_read_state of the whole batch, pinned host buffers"},
-                "gpu_launches": launches, "clocks": clk, "step_stats": st}
+                "gpu_launches": launches, "clocks": clk, "step_stats": st,
+                "stage_ms_per_substep": stages}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -211,7 +211,10 @@ typedef struct bb_step_stats {
 #define BB_DBG_PAIRS 7u        /* u32 x 2P: (sorted a, sorted b), a < b */
 #define BB_DBG_MANIFOLDS 8u    /* bb_manifold_info x M */
 #define BB_DBG_CONTACTS 9u     /* bb_contact_info x 8M (slot j of manifold m at 8m+j) */
-#define BB_DBG_EDGE_COLORS 10u /* u32 x M (0xFFFFFFFF = overflow) */
+#define BB_DBG_EDGE_COLORS 10u /* u32 x M (0xFFFFFFFF = overflow, 0xFFFFFFFE = resting: the manifold's
+                                  island has no awake body, so it is neither coloured nor solved) */
+#define BB_EDGE_COLOR_OVERFLOW 0xFFFFFFFFu
+#define BB_EDGE_COLOR_RESTING 0xFFFFFFFEu
 #define BB_DBG_BODY_COLORS 11u /* u32 x N by body id (AVBD colouring) */
 #define BB_DBG_ISLANDS 12u     /* u32 x N by body id (0xFFFFFFFF = static / no island) */
 #define BB_DBG_SUPPORT_DEPTH 13u /* u32 x N by body id (AVBD shock-propagation depth) */

@@ -359,3 +359,73 @@ def test_sleeping_bodies_carry_their_manifolds_like_the_oracle(oracle_lib, solve
     after = w.read_state()
     for k in before:
         assert np.array_equal(before[k], after[k]), k  # asleep: frozen in place
+
+
+def test_resting_islands_are_left_uncoloured(oracle_lib):
+    """The 18 boxes of the resting scene fall asleep while a three-box stack is in free fall
+    elsewhere.  The edge colouring skips the islands with no awake body (their manifolds read
+    EDGE_COLOR_RESTING and are not solved); every other manifold keeps the colour the oracle,
+    which colours all manifolds, gives it, because the colouring rounds are local to an island."""
+    sc = resting_scene()
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50])
+    sb.add(sc["pos"][1:], sc["quat"][1:], sc["half"][1:], scenes.SHAPE_BOX,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1000.0)
+    stack = np.array([[12.0, 5.0, 0.0], [12.0, 5.999, 0.0], [12.0, 6.998, 0.0]])
+    sb.add(stack, np.tile([0, 0, 0, 1.0], (3, 1)), np.full((3, 3), 0.5), scenes.SHAPE_BOX,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1000.0)
+    sc = sb.build()
+    p = params_for(oracle_lib, sc, solver=bb.SOLVER_PGS_SOFT, quirks=0, iterations=8, relax_iterations=8)
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    for _ in range(20):
+        w.step(DT, 4)
+        o.step(DT, 4)
+    w.sync()
+    assert w.stats()["sleeping_count"] == o.stats()["sleeping_count"] == 18
+    gm, rm = w.debug_read("manifolds"), oread(o, 8, None)
+    assert len(gm) == len(rm)
+    for f in ("body_a", "body_b", "key", "contact_count"):
+        assert np.array_equal(gm[f], rm[f]), f
+    gcol, rcol = w.debug_read("edge_colors"), oread(o, 10, np.uint32)
+    in_stack = (gm["body_a"] >= 19) | (gm["body_b"] >= 19)
+    assert in_stack.sum() == 2  # the stack's two inner manifolds, sharing the middle box
+    assert (gcol[~in_stack] == bb.EDGE_COLOR_RESTING).all()
+    assert np.array_equal(gcol[in_stack], rcol[in_stack])
+    assert sorted(gcol[in_stack].tolist()) == [0, 1]
+    assert w.stats()["graph_color_count"] == 2 and w.stats()["error_flags"] == 0
+
+
+def test_islands_start_from_last_roots_like_a_fresh_union_find(oracle_lib):
+    """Connected components start from the last substep's roots for components whose bodies
+    were not awake at two narrow phases in a row.  A three-box stack falls onto the sleeping
+    two-box stack of the resting scene and wakes it; the island of every body must equal the
+    oracle's union-find from scratch at every step whose manifolds agree (most of them)."""
+    sc = resting_scene()
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([0, -50, 0], [50, 50, 50])
+    sb.add(sc["pos"][1:], sc["quat"][1:], sc["half"][1:], scenes.SHAPE_BOX,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1000.0)
+    stack = np.array([[4.0, 4.0, 0.0], [4.0, 4.999, 0.0], [4.0, 5.998, 0.0]])
+    sb.add(stack, np.tile([0, 0, 0, 1.0], (3, 1)), np.full((3, 3), 0.5), scenes.SHAPE_BOX,
+           scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY, 1000.0)
+    sc = sb.build()
+    p = params_for(oracle_lib, sc, solver=bb.SOLVER_PGS_SOFT, quirks=0, iterations=8, relax_iterations=8)
+    w = bb.world_from_scene(sc, params=p)
+    o = oracle_for(oracle_lib, sc, p)
+    compared, merged, slept = 0, 0, 0
+    for _ in range(70):
+        w.step(DT, 4)
+        o.step(DT, 4)
+        w.sync()
+        gm, rm = w.debug_read("manifolds"), oread(o, 8, None)
+        if len(gm) != len(rm) or not all(np.array_equal(gm[f], rm[f]) for f in ("body_a", "body_b")):
+            continue
+        gi, ri = w.debug_read("islands"), oread(o, 12, np.uint32)
+        assert np.array_equal(gi, ri)
+        assert w.stats()["island_count"] == o.stats()["island_count"]
+        compared += 1
+        slept += w.stats()["sleeping_count"] >= 16
+        merged += gi[17] == gi[19]  # the lower stack and the falling stack share an island
+    assert compared >= 50 and slept >= 20 and merged >= 5, (compared, slept, merged)
+    assert w.stats()["error_flags"] == 0
