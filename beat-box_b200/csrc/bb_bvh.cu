@@ -376,16 +376,45 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
   }
 }
 
-// pairs of the queries whose partners all fit in bp_stage, one thread per staged slot
+// pairs of the queries whose partners all fit in bp_stage.  A warp takes 32 consecutive queries,
+// scans their counts, and its lanes then write the warp's pairs 32 at a time, each lane finding
+// its query by a binary search over the scanned counts (shuffles): every lane has work, and a
+// pair's place pair_off[i] + k and value are those of the staged slot.
 __global__ void k_broad_copy(const DevState d, uint32_t n) {
-  const size_t total = size_t(n) * BB_BP_STAGE;
   const uint32_t cap = d.pair_capacity;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
-    const uint32_t i = uint32_t(t / BB_BP_STAGE), k = uint32_t(t % BB_BP_STAGE);
-    if (d.is_heavy[i] != 0u || k >= d.pair_cnt[i]) continue;
-    const uint32_t o = d.pair_off[i] + k;
-    if (o < cap) d.pairs[o] = make_uint2(i, d.bp_stage[t]);
-    else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+  const int lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t q0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; q0 < n; q0 += nwarps * 32u) {  // warp-uniform
+    const uint32_t i = q0 + lane;
+    uint32_t cnt = 0, off = 0;
+    if (i < n && d.is_heavy[i] == 0u) {
+      cnt = d.pair_cnt[i];
+      off = d.pair_off[i];
+    }
+    uint32_t inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+    const uint32_t exc = inc - cnt;
+    for (uint32_t r0 = 0; r0 < total; r0 += 32u) {
+      const uint32_t r = r0 + uint32_t(lane);
+      int j = 0;  // the first lane whose inclusive count exceeds r
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, j + step - 1);
+        if (v <= r) j += step;
+      }
+      const uint32_t ej = __shfl_sync(0xFFFFFFFFu, exc, j), oj = __shfl_sync(0xFFFFFFFFu, off, j);
+      if (r < total) {
+        const uint32_t k = r - ej, o = oj + k;
+        const uint32_t partner = d.bp_stage[size_t(q0 + uint32_t(j)) * BB_BP_STAGE + k];
+        if (o < cap) d.pairs[o] = make_uint2(q0 + uint32_t(j), partner);
+        else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+      }
+    }
   }
 }
 

@@ -420,11 +420,13 @@ __device__ __forceinline__ bool np_awake(uint32_t f) { return (f & BB_BODY_DYNAM
 // keeps the warps of k_narrow on one code path (the box-box clip is long, the sphere cases
 // short); the outputs go to each slot's own place, so the order in which the lists fill does
 // not matter.
-__global__ void k_np_classify(const DevState d, int cur, int warm) {
+#define BB_CLS_WARPS 8  // k_np_classify runs 256-thread blocks
+__global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevState d, int cur, int warm) {
+  __shared__ uint32_t s_cnt[4][BB_CLS_WARPS];  // per kind, per warp: entries, then the warp's first index
   const uint32_t S = slot_total(d);
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (blockIdx.x == 0 && threadIdx.x == 0) d.ctr->slots_of[cur] = S;  // read by the next substep's carry
-  for (uint32_t base = blockIdx.x * blockDim.x; base < S; base += gridDim.x * blockDim.x) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < S; base += gridDim.x * blockDim.x) {  // block-uniform
     const uint32_t k = base + threadIdx.x;
     int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body, 3 frozen
     if (k < S) {
@@ -442,20 +444,36 @@ __global__ void k_np_classify(const DevState d, int cur, int warm) {
         else kind = (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1;
       }
     }
+    // one list append per kind and block: warp counts, a block scan by four threads, one atomic each
+    unsigned my_mask = 0;
 #pragma unroll
     for (int kd = 0; kd < 4; ++kd) {
       const unsigned mask = __ballot_sync(0xFFFFFFFFu, kind == kd);
-      if (!mask) continue;
-      uint32_t off = 0;
-      if (lane == 0) off = atomicAdd(&d.ctr->np_counts[kd], uint32_t(__popc(mask)));
-      off = __shfl_sync(0xFFFFFFFFu, off, 0);
-      if (kind == kd) {
-        const uint32_t r = off + uint32_t(__popc(mask & ((1u << lane) - 1u)));
-        if (kd == 3) d.carry_list[r] = k;
-        else if (kd == 2) d.vox_list[r] = k;
-        else d.np_list[kd == 0 ? r : S - 1 - r] = k;
-      }
+      if (kind == kd) my_mask = mask;
+      if (lane == 0) s_cnt[kd][warp] = uint32_t(__popc(mask));
     }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      const int kd = threadIdx.x;
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < BB_CLS_WARPS; ++w) {
+        const uint32_t c = s_cnt[kd][w];
+        s_cnt[kd][w] = run;
+        run += c;
+      }
+      const uint32_t first = run ? atomicAdd(&d.ctr->np_counts[kd], run) : 0u;
+#pragma unroll
+      for (int w = 0; w < BB_CLS_WARPS; ++w) s_cnt[kd][w] += first;
+    }
+    __syncthreads();
+    if (kind >= 0) {
+      const uint32_t r = s_cnt[kind][warp] + uint32_t(__popc(my_mask & ((1u << lane) - 1u)));
+      if (kind == 3) d.carry_list[r] = k;
+      else if (kind == 2) d.vox_list[r] = k;
+      else d.np_list[kind == 0 ? r : S - 1 - r] = k;
+    }
+    __syncthreads();  // s_cnt is rewritten by the next trip
   }
 }
 
@@ -465,75 +483,54 @@ __global__ void k_np_classify(const DevState d, int cur, int warm) {
 // which is what recomputing the same poses and matching every contact by feature gives.  A
 // frozen pair without a manifold last substep goes to the ordinary lists and is computed.
 __device__ __forceinline__ void carry_contact(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni) {
-  d.c_pos[cur][ni] = d.c_pos[prv][oi];
-  d.c_lam[cur][ni] = d.c_lam[prv][oi];
+  const float4 cp = d.c_pos[prv][oi], cl = d.c_lam[prv][oi], aa = d.c_anc_a[prv][oi];
   float4 kt = d.c_kt[prv][oi];
-  kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
-  d.c_kt[cur][ni] = kt;
   const bool stick = __float_as_uint(kt.z) != 0u;
-  const float4 aa = d.c_anc_a[prv][oi], ab = d.c_anc_b[prv][oi];
+  // the second anchor only of a sticking contact (else it is written as 0)
+  const float4 ab = stick ? d.c_anc_b[prv][oi] : make_float4(0.f, 0.f, 0.f, 0.f);
+  kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
+  d.c_pos[cur][ni] = cp;
+  d.c_lam[cur][ni] = cl;
+  d.c_kt[cur][ni] = kt;
   d.c_anc_a[cur][ni] = stick ? aa : make_float4(0.f, 0.f, 0.f, aa.w);
-  d.c_anc_b[cur][ni] = stick ? make_float4(ab.x, ab.y, ab.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+  d.c_anc_b[cur][ni] = make_float4(ab.x, ab.y, ab.z, 0.f);
 }
 
-// Every load of a manifold's header and of its first four contacts is issued before the first
-// store (the stores could alias the loads as far as the compiler knows), so the copy costs one
-// memory round trip rather than one per contact.
-__device__ __forceinline__ void carry_copy(const DevState& d, int cur, uint32_t os, uint32_t dst, uint32_t ida,
-                                           uint32_t idb) {
+// Lane q (0..3) of the quad that carries a pair: the header (q = 0) and contacts q, q + 4.  The
+// quad's four lanes read each contact array over 64 contiguous bytes.
+__device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t os, uint32_t dst, uint32_t ida,
+                                           uint32_t idb, uint32_t q) {
   const int prv = cur ^ 1;
   const int2 kc = d.m_keycc[prv][os];
-  const float4 n4 = d.m_normal[prv][os], t04 = d.m_t0[prv][os], t14 = d.m_t1[prv][os];
-  const float4 pa = d.pos[ida], pb = d.pos[idb];
-  float4 cp[4], cl[4], ck[4], ca[4], cb[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    if (c < kc.y) {
-      const uint32_t oi = os * BB_MAX_CONTACTS + c;
-      cp[c] = d.c_pos[prv][oi];
-      cl[c] = d.c_lam[prv][oi];
-      ck[c] = d.c_kt[prv][oi];
-      ca[c] = d.c_anc_a[prv][oi];
-      cb[c] = d.c_anc_b[prv][oi];
-    }
+  if (q == 0) {
+    const float4 n4 = d.m_normal[prv][os], t04 = d.m_t0[prv][os], t14 = d.m_t1[prv][os];
+    const float4 pa = d.pos[ida], pb = d.pos[idb];
+    d.m_bodies[cur][dst] = make_uint2(ida, idb);
+    d.m_keycc[cur][dst] = kc;
+    d.m_normal[cur][dst] = make_float4(n4.x, n4.y, n4.z, __int_as_float(0));
+    d.m_t0[cur][dst] = t04;
+    d.m_t1[cur][dst] = t14;
+    d.m_anchor_a[cur][dst] = make_float4(pa.x, pa.y, pa.z, 0.f);
+    d.m_anchor_b[cur][dst] = make_float4(pb.x, pb.y, pb.z, 0.f);
+    d.hit[dst] = 1;
   }
-  d.m_bodies[cur][dst] = make_uint2(ida, idb);
-  d.m_keycc[cur][dst] = kc;
-  d.m_normal[cur][dst] = make_float4(n4.x, n4.y, n4.z, __int_as_float(0));
-  d.m_t0[cur][dst] = t04;
-  d.m_t1[cur][dst] = t14;
-  d.m_anchor_a[cur][dst] = make_float4(pa.x, pa.y, pa.z, 0.f);
-  d.m_anchor_b[cur][dst] = make_float4(pb.x, pb.y, pb.z, 0.f);
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    if (c < kc.y) {
-      const uint32_t ni = dst * BB_MAX_CONTACTS + c;
-      d.c_pos[cur][ni] = cp[c];
-      d.c_lam[cur][ni] = cl[c];
-      float4 kt = ck[c];
-      kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
-      d.c_kt[cur][ni] = kt;
-      const bool stick = __float_as_uint(kt.z) != 0u;
-      d.c_anc_a[cur][ni] = stick ? ca[c] : make_float4(0.f, 0.f, 0.f, ca[c].w);
-      d.c_anc_b[cur][ni] = stick ? make_float4(cb[c].x, cb[c].y, cb[c].z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  }
-  for (int c = 4; c < kc.y; ++c) carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c);
-  d.hit[dst] = 1;
+  for (uint32_t c = q; c < uint32_t(kc.y); c += 4u)
+    carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c);
 }
 
-// A frozen pair's manifold of the previous substep is found at the pair's own slot when the
-// slot held a manifold of the same two bodies in the same order then: that is the pair's only
-// non-voxel manifold (key < 90; a voxel pair's keys are 90..95), the one the search through the
-// body's manifold list would find.  While no pair ahead of it came or went, every frozen pair
-// takes this path; the others search.  Slots past the previous substep's count are not read
-// (they hold older manifolds).
+// One quad of lanes per frozen pair.  The pair's manifold of the previous substep is found at
+// the pair's own slot when the slot held a manifold of the same two bodies in the same order
+// then: that is the pair's only non-voxel manifold (key < 90; a voxel pair's keys are 90..95),
+// the one the search through the body's manifold list would find.  While no pair ahead of it
+// came or went, every frozen pair takes this path; the others search.  Slots past the previous
+// substep's count are not read (they hold older manifolds).
 __global__ void k_narrow_carry(const DevState d, int cur) {
   const int prv = cur ^ 1;
   const uint32_t S = slot_total(d);
   const uint32_t S_prv = min(d.ctr->slots_of[prv], d.pair_capacity);
   const uint32_t nc = d.ctr->np_counts[3];
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
+  const uint32_t q = threadIdx.x & 3u, quads = (gridDim.x * blockDim.x) >> 2;
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < nc; t += quads) {  // quad-uniform
     const uint32_t s = d.carry_list[t];
     const uint2 pr = d.pairs[slot_pair_of(d, s)];
     int2 okc = make_int2(-1, 0);
@@ -544,7 +541,7 @@ __global__ void k_narrow_carry(const DevState d, int cur) {
     }
     const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
     if (okc.x >= 0 && okc.x < 90 && ob.x == ida && ob.y == idb) {
-      carry_copy(d, cur, s, s, ida, idb);
+      carry_part(d, cur, s, s, ida, idb, q);
       continue;
     }
     const uint32_t fa = d.flags[ida];
@@ -560,15 +557,15 @@ __global__ void k_narrow_carry(const DevState d, int cur) {
       const int key = d.m_keycc[prv][os].x;
       if (vox) {
         if (key < 90 || key > 95) continue;
-        carry_copy(d, cur, os, s + uint32_t(key - 90), ida, idb);
+        carry_part(d, cur, os, s + uint32_t(key - 90), ida, idb, q);
         any = true;
       } else {
-        carry_copy(d, cur, os, s, ida, idb);
+        carry_part(d, cur, os, s, ida, idb, q);
         any = true;
         break;
       }
     }
-    if (any) continue;
+    if (any || q != 0) continue;
     // no manifold last substep: compute the pair with the others
     if (vox) {
       d.vox_list[atomicAdd(&d.ctr->np_counts[2], 1u)] = s;
@@ -1159,33 +1156,49 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
   }
 }
 
-// man_slot[man_index[k]] = k for every slot that collided; per-manifold statistics, reduced
-// over each warp before one atomic per warp.
+// man_slot[man_index[k]] = k for every slot that collided; per-manifold statistics summed by
+// each thread over its slots, then reduced over the block before one atomic per block (a few
+// thousand updates of three counters instead of one per warp and slot group).
 __global__ void k_compact(const DevState d, int cur) {
+  __shared__ uint32_t s_red[3][32];
   const uint32_t S = slot_total(d);
-  const uint32_t lane = threadIdx.x & 31u, stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < S; base += stride) {  // warp-uniform
-    const uint32_t k = base + lane;
-    uint32_t cc = 0, fresh = 0, deep_bits = 0;
-    if (k < S && d.hit[k]) {
-      d.man_slot[cur][d.man_index[k]] = k;
-      cc = uint32_t(d.m_keycc[cur][k].y);
-      float deep = 0.f;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, stride = gridDim.x * blockDim.x;
+  uint32_t cc_sum = 0, fresh = 0, deep_bits = 0;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += stride) {
+    if (!d.hit[k]) continue;
+    d.man_slot[cur][d.man_index[k]] = k;
+    const uint32_t cc = uint32_t(d.m_keycc[cur][k].y);
+    cc_sum += cc;
+    float deep = 0.f;
 #pragma unroll
-      for (uint32_t c = 0; c < BB_MAX_CONTACTS; ++c) {  // unrolled: the contacts' loads go out together
-        if (c < cc) {
-          const uint32_t ci = k * BB_MAX_CONTACTS + c;
-          if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
-          deep = fmaxf(deep, -d.c_pos[cur][ci].w);
-        }
+    for (uint32_t c = 0; c < BB_MAX_CONTACTS; ++c) {  // unrolled: the contacts' loads go out together
+      if (c < cc) {
+        const uint32_t ci = k * BB_MAX_CONTACTS + c;
+        if (__float_as_uint(d.c_kt[cur][ci].w) == 0u) ++fresh;
+        deep = fmaxf(deep, -d.c_pos[cur][ci].w);
       }
-      deep_bits = deep > 0.f ? __float_as_uint(deep) : 0u;  // positive floats order as their bits
     }
-    cc = __reduce_add_sync(0xFFFFFFFFu, cc);
+    if (deep > 0.f) deep_bits = max(deep_bits, __float_as_uint(deep));  // positive floats order as their bits
+  }
+  cc_sum = __reduce_add_sync(0xFFFFFFFFu, cc_sum);
+  fresh = __reduce_add_sync(0xFFFFFFFFu, fresh);
+  deep_bits = __reduce_max_sync(0xFFFFFFFFu, deep_bits);
+  if (lane == 0) {
+    s_red[0][warp] = cc_sum;
+    s_red[1][warp] = fresh;
+    s_red[2][warp] = deep_bits;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t nw = blockDim.x >> 5;
+    cc_sum = lane < nw ? s_red[0][lane] : 0u;
+    fresh = lane < nw ? s_red[1][lane] : 0u;
+    deep_bits = lane < nw ? s_red[2][lane] : 0u;
+    cc_sum = __reduce_add_sync(0xFFFFFFFFu, cc_sum);
     fresh = __reduce_add_sync(0xFFFFFFFFu, fresh);
     deep_bits = __reduce_max_sync(0xFFFFFFFFu, deep_bits);
     if (lane == 0) {
-      if (cc) atomicAdd(&d.ctr->contact_count, cc);
+      if (cc_sum) atomicAdd(&d.ctr->contact_count, cc_sum);
       if (fresh) atomicAdd(&d.ctr->fresh, fresh);
       if (deep_bits) atomicMax(&d.ctr->max_pen_bits, deep_bits);
     }
@@ -1219,6 +1232,37 @@ __global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
   d.frozen[i] = now | ((d.frozen[i] & now) << 1);
   uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
   uint32_t* L = d.csr_list[cur];
+  if (s1 - s0 <= 8u) {  // short list: registers, a 19-comparator sorting network, loads issued together
+    const uint32_t len = s1 - s0;
+    uint32_t v[8];
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) v[j] = j < len ? L[s0 + j] : 0xFFFFFFFFu;
+    auto cx = [&](int a, int b) {
+      const uint32_t lo = min(v[a], v[b]), hi = max(v[a], v[b]);
+      v[a] = lo;
+      v[b] = hi;
+    };
+    cx(0, 2); cx(1, 3); cx(4, 6); cx(5, 7);
+    cx(0, 4); cx(1, 5); cx(2, 6); cx(3, 7);
+    cx(0, 1); cx(2, 3); cx(4, 5); cx(6, 7);
+    cx(2, 4); cx(3, 5);
+    cx(1, 4); cx(3, 6);
+    cx(1, 2); cx(3, 4); cx(5, 6);
+    uint32_t slot[8];
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) slot[j] = j < len ? d.man_slot[cur][v[j]] : 0u;
+    uint2 b[8];
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) b[j] = j < len ? d.m_bodies[cur][slot[j]] : make_uint2(0u, 0u);
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) {
+      if (j < len) {
+        L[s0 + j] = v[j];
+        d.csr_partner[cur][s0 + j] = b[j].x == i ? b[j].y : b[j].x;
+      }
+    }
+    return;
+  }
   for (uint32_t a = s0 + 1; a < s1; ++a) {
     uint32_t v = L[a];
     uint32_t b = a;
@@ -1245,7 +1289,7 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
                    sc.scan_status + 6 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 6, d.ctr);
     k_slot_fill<<<grid, T, 0, s>>>(d);
   }
-  k_np_classify<<<sms * 8, 256, 0, s>>>(d, cur, warm ? 1 : 0);
+  k_np_classify<<<sms * 8, 32 * BB_CLS_WARPS, 0, s>>>(d, cur, warm ? 1 : 0);
   k_narrow_carry<<<sms * 8, 256, 0, s>>>(d, cur);
   k_narrow<<<sms * (p.narrow_blocks_per_sm ? p.narrow_blocks_per_sm : 16u), 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
   if (d.vox_on) k_voxel_narrow<<<sms * 8, 256, 0, s>>>(d, p, cur, warm ? 1 : 0);
