@@ -318,10 +318,20 @@ struct PgsItem {
 // thread's slot of dynamic shared memory with cp.async at prefetch time, so the run does not
 // pay one global round trip per extra contact.  Slot layout: [contact][R1, R2, K, lam].
 #define BB_PGS_EXTRA (BB_MAX_CONTACTS - 4)
-#define BB_PGS_SMEM (BB_PGS_THREADS * BB_PGS_EXTRA * 4 * 16)
+// Next-item staging (k_pgs_soft): the item a thread runs after the current one in the same
+// colour -- masses, frame, up to four contacts' rows and impulses, and both bodies' velocities
+// and world inverse inertias -- copied with cp.async while the current item computes.  Element e
+// of thread t sits at e * BB_PGS_THREADS + t, so a warp's 16-byte accesses hit distinct banks.
+#define BB_PGS_NEXT 28  // float4 per thread: mass, n, t0, t1, 4 x (R1, R2, K, lam), 8 body words
+#define BB_PGS_SMEM_EXTRA (BB_PGS_THREADS * BB_PGS_EXTRA * 4 * 16)
+#define BB_PGS_SMEM (BB_PGS_SMEM_EXTRA + BB_PGS_THREADS * BB_PGS_NEXT * 16)
 __device__ __forceinline__ float4* pgs_extra_slot() {
   extern __shared__ float4 s_pgs_extra[];
   return s_pgs_extra + threadIdx.x * (BB_PGS_EXTRA * 4);
+}
+__device__ __forceinline__ float4* pgs_next_base() {
+  extern __shared__ float4 s_pgs_extra[];
+  return s_pgs_extra + BB_PGS_THREADS * BB_PGS_EXTRA * 4 + threadIdx.x;
 }
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const uint32_t s = uint32_t(__cvta_generic_to_shared(smem));
@@ -429,16 +439,35 @@ __device__ void pgs_item_build(const DevState& d, int cur, uint32_t k, uint32_t 
   }
 }
 
-// mode 0: warm start, 1: solve sweep (soft bias), 2: relax sweep
+// an item's two bodies: velocities and world inverse inertias
+struct PgsBodies {
+  float4 va, wa, ia0, ia1, vb, wb, ib0, ib1;
+};
+__device__ __forceinline__ PgsBodies pgs_bodies_load(const DevState& d, uint32_t a, uint32_t b) {
+  PgsBodies B;
+  B.va = d.vel[a];
+  B.wa = d.omega[a];
+  B.ia0 = d.iw[2 * a];
+  B.ia1 = d.iw[2 * a + 1];
+  B.vb = d.vel[b];
+  B.wb = d.omega[b];
+  B.ib0 = d.iw[2 * b];
+  B.ib1 = d.iw[2 * b + 1];
+  return B;
+}
+
+// mode 0: warm start, 1: solve sweep (soft bias), 2: relax sweep; B holds the item's bodies
 template <int PF, bool STAGED = true>
-__device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p, int cur, PgsItem<PF>& x, int mode) {
+__device__ __forceinline__ void pgs_item_compute(const DevState& d, const Params& p, PgsItem<PF>& x,
+                                                 const PgsBodies& B, int mode) {
   if (x.rec.w & BB_PGS_SKIP) return;
   const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
   if (mode == 0 && !accum) return;
   const uint32_t a = x.rec.y, b = x.rec.z, c0 = x.rec.x, cc = x.rec.w & 0xFFu;
-  float4 va4 = d.vel[a], vb4 = d.vel[b];
-  float3 va = f3(va4), wa = f3(d.omega[a]), vb = f3(vb4), wb = f3(d.omega[b]);
-  const Sym3 IA = load_iw(d, a), IB = load_iw(d, b);
+  const float4 va4 = B.va, vb4 = B.vb;
+  float3 va = f3(va4), wa = f3(B.wa), vb = f3(vb4), wb = f3(B.wb);
+  const Sym3 IA{B.ia0.x, B.ia0.y, B.ia0.z, B.ia0.w, B.ia1.x, B.ia1.y};
+  const Sym3 IB{B.ib0.x, B.ib0.y, B.ib0.z, B.ib0.w, B.ib1.x, B.ib1.y};
   const float ima = x.mass.x, imb = x.mass.y, mu = x.mass.z;
   const float3 n = f3(x.n), t0 = f3(x.t0), t1 = f3(x.t1);
 #pragma unroll
@@ -480,6 +509,84 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
   }
 }
 
+template <int PF, bool STAGED = true>
+__device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p, int cur, PgsItem<PF>& x, int mode) {
+  (void)cur;
+  if (x.rec.w & BB_PGS_SKIP) return;
+  if (mode == 0 && !(p.flags & BB_SIM_ACCUM_IMPULSE)) return;
+  const PgsBodies B = pgs_bodies_load(d, x.rec.y, x.rec.z);
+  pgs_item_compute<PF, STAGED>(d, p, x, B, mode);
+}
+
+// cp.async of the next item k (record r) of this thread's colour into its staging slot: the
+// bodies cannot change before this thread runs the item (the colour's items share no body),
+// and the rows and impulses are only written by the item itself.
+template <int PF>
+__device__ __forceinline__ void pgs_stage_next(const DevState& d, uint32_t k, uint4 r) {
+  float4* nb = pgs_next_base();
+  const uint32_t T = BB_PGS_THREADS, c0 = r.x, cc = min(r.w & 0xFFu, uint32_t(PF)), a = r.y, b = r.z;
+  cp_async16(nb + 0 * T, d.pgs_mass + k);
+  cp_async16(nb + 1 * T, d.pgs_frame + 3 * k);
+  cp_async16(nb + 2 * T, d.pgs_frame + 3 * k + 1);
+  cp_async16(nb + 3 * T, d.pgs_frame + 3 * k + 2);
+  for (uint32_t j = 0; j < cc; ++j) {
+    cp_async16(nb + (4 + 4 * j) * T, d.c_r1 + c0 + j);
+    cp_async16(nb + (5 + 4 * j) * T, d.c_r2 + c0 + j);
+    cp_async16(nb + (6 + 4 * j) * T, d.c_k + c0 + j);
+    cp_async16(nb + (7 + 4 * j) * T, d.pgs_lam + c0 + j);
+  }
+  cp_async16(nb + 20 * T, d.vel + a);
+  cp_async16(nb + 21 * T, d.omega + a);
+  cp_async16(nb + 22 * T, d.iw + 2 * a);
+  cp_async16(nb + 23 * T, d.iw + 2 * a + 1);
+  cp_async16(nb + 24 * T, d.vel + b);
+  cp_async16(nb + 25 * T, d.omega + b);
+  cp_async16(nb + 26 * T, d.iw + 2 * b);
+  cp_async16(nb + 27 * T, d.iw + 2 * b + 1);
+  cp_async_commit();
+}
+
+// the staged item into registers (after cp.async.wait_all); its contacts beyond PF are staged
+// in the extra slot as pgs_item_fill does
+template <int PF>
+__device__ __forceinline__ void pgs_take_next(const DevState& d, uint4 r, PgsItem<PF>& x, PgsBodies& B) {
+  const float4* nb = pgs_next_base();
+  const uint32_t T = BB_PGS_THREADS, cc = r.w & 0xFFu;
+  x.rec = r;
+  x.mass = nb[0];
+  x.n = nb[T];
+  x.t0 = nb[2 * T];
+  x.t1 = nb[3 * T];
+#pragma unroll
+  for (int j = 0; j < PF; ++j) {
+    if (uint32_t(j) < cc) {
+      x.R1[j] = nb[(4 + 4 * j) * T];
+      x.R2[j] = nb[(5 + 4 * j) * T];
+      x.K[j] = nb[(6 + 4 * j) * T];
+      x.lam[j] = nb[(7 + 4 * j) * T];
+    }
+  }
+  B.va = nb[20 * T];
+  B.wa = nb[21 * T];
+  B.ia0 = nb[22 * T];
+  B.ia1 = nb[23 * T];
+  B.vb = nb[24 * T];
+  B.wb = nb[25 * T];
+  B.ib0 = nb[26 * T];
+  B.ib1 = nb[27 * T];
+  if (cc > uint32_t(PF)) {
+    float4* slot = pgs_extra_slot();
+    for (uint32_t j = PF; j < cc; ++j) {
+      float4* e = slot + (j - PF) * 4;
+      cp_async16(e + 0, d.c_r1 + r.x + j);
+      cp_async16(e + 1, d.c_r2 + r.x + j);
+      cp_async16(e + 2, d.c_k + r.x + j);
+      cp_async16(e + 3, d.pgs_lam + r.x + j);
+    }
+    cp_async_commit();
+  }
+}
+
 // one sweep over colours 0..C-1 and the overflow bucket.  On entry x holds this thread's first
 // item of colour 0 and rec_next the record of its first item of colour 1 (or of colour 0 when
 // C == 1); on exit both are set the same way for the next sweep.  Records run one colour ahead
@@ -488,7 +595,7 @@ __device__ __forceinline__ void pgs_item_run(const DevState& d, const Params& p,
 // wait for them either.
 __device__ __forceinline__ uint32_t pgs_next_colour(uint32_t c, uint32_t C) { return c + 1 < C ? c + 1 : 0u; }
 
-template <int PF>
+template <int PF, bool STAGE_NEXT>
 __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode, const uint32_t* bs, const uint32_t* aw,
                           uint32_t C, PgsItem<PF>& x, uint4& rec_next, uint32_t& epoch) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
@@ -497,12 +604,38 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
     // A colour whose manifolds all sleep has no work (every item is skipped) and needs no
     // barrier: its neighbours are ordered by the barriers of the colours that do run.
     const bool run = aw[c] != 0;
-    if (run) {
+    if (run && !STAGE_NEXT) {  // later items of the colour load after the one before has run
       const uint32_t end = bs[c + 1];
       for (uint32_t k = bs[c] + tid; k < end;) {
         pgs_item_run(d, p, cur, x, mode);
         k += stride;
         if (k < end) pgs_item_load(d, k, x);
+      }
+    } else if (run) {
+      // The colour's first item is in x.  Its bodies and the next item's record load now; each
+      // later item (with its bodies) is staged by cp.async while the one before computes, and
+      // the record after it loads meanwhile, so a later item costs no dependent round trip.
+      const uint32_t end = bs[c + 1];
+      uint32_t k = bs[c] + tid;
+      if (k < end) {
+        uint4 rn = make_uint4(0, 0, 0, 0);
+        if (k + stride < end) rn = d.pgs_rec[k + stride];
+        PgsBodies B = pgs_bodies_load(d, x.rec.y, x.rec.z);
+        for (;;) {
+          const uint32_t kn = k + stride;
+          const bool more = kn < end;
+          uint4 rnn = make_uint4(0, 0, 0, 0);
+          if (more) {
+            pgs_stage_next<PF>(d, kn, rn);
+            if (kn + stride < end) rnn = d.pgs_rec[kn + stride];
+          }
+          pgs_item_compute<PF>(d, p, x, B, mode);
+          if (!more) break;
+          cp_async_wait_all();
+          pgs_take_next<PF>(d, rn, x, B);
+          rn = rnn;
+          k = kn;
+        }
       }
     }
     const uint32_t cn = pgs_next_colour(c, C), cnn = pgs_next_colour(cn, C);
@@ -541,7 +674,7 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
 // PF = 4 contacts held per item (one 255-register block per SM).  Holding fewer would let
 // two blocks share an SM but puts the other contacts' loads on the critical path, one round
 // trip each.
-template <int PF>
+template <int PF, bool STAGE_NEXT>
 __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   __shared__ uint32_t bs[BB_MAX_COLORS + 2];
   __shared__ uint32_t aw[BB_MAX_COLORS + 1];
@@ -569,14 +702,14 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(co
     const uint32_t c1 = pgs_next_colour(0, C);
     if (bs[c1] + tid < bs[c1 + 1]) rec_next = d.pgs_rec[bs[c1] + tid];
   }
-  pgs_sweep(d, p, cur, 0, bs, aw, C, x, rec_next, epoch);
-  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep(d, p, cur, 1, bs, aw, C, x, rec_next, epoch);
+  pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 0, bs, aw, C, x, rec_next, epoch);
+  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 1, bs, aw, C, x, rec_next, epoch);
   if (p.flags & BB_SIM_ADVECTION) {
     for (uint32_t i = tid; i < n; i += stride)
       if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
     grid_sync(d.ctr, sync, epoch);
   }
-  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep(d, p, cur, 2, bs, aw, C, x, rec_next, epoch);
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 2, bs, aw, C, x, rec_next, epoch);
   // impulses back to the persistent contacts (every sweep ended with a grid barrier)
   const uint32_t M = d.ctr->manifold_count;
   for (uint32_t k = tid; k < M; k += stride) {
@@ -711,9 +844,10 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_flow(co
 }
 
 int bb_pgs_soft_blocks(int sms) {
-  cudaFuncSetAttribute((const void*)k_pgs_soft<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM);
-  cudaFuncSetAttribute((const void*)k_pgs_flow<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM);
-  return bb_coop_blocks((const void*)k_pgs_soft<4>, BB_PGS_THREADS, sms);
+  cudaFuncSetAttribute((const void*)k_pgs_soft<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM_EXTRA);
+  cudaFuncSetAttribute((const void*)k_pgs_soft<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM);
+  cudaFuncSetAttribute((const void*)k_pgs_flow<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_SMEM_EXTRA);
+  return bb_coop_blocks((const void*)k_pgs_soft<4, false>, BB_PGS_THREADS, sms);
 }
 
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
@@ -732,7 +866,7 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
     float hh = h;
     void* args[] = {&dd, &pp, &cc, &nn, &hh};
     const void* kern = (const void*)k_pgs_flow<4>;
-    bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
+    bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM_EXTRA);
     return;
   }
   DevState dd = d;
@@ -741,8 +875,10 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
-  const void* kern = (const void*)k_pgs_soft<4>;
-  bb_launch_coop(kern, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
+  // staging the next item needs 112 KB more shared memory (less L1): it pays when threads run
+  // several items per colour (large worlds), which is what the autotuner measures
+  if (p.pgs_stage_next) bb_launch_coop((const void*)k_pgs_soft<4, true>, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
+  else bb_launch_coop((const void*)k_pgs_soft<4, false>, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM_EXTRA);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -414,7 +414,7 @@ void bb_default_solver_params(bb_solver_params* p) {
   p->schedule = BB_SCHEDULE_COLOUR_BARRIER;
   p->broad_threads = 128;
   p->narrow_blocks_per_sm = 16;
-  p->flow_blocks_per_sm = 8;
+  p->pgs_stage_next = 0;
   p->bounds_mode = BB_BOUNDS_FIXED;
   for (int k = 0; k < 3; ++k) {
     p->world_min[k] = -64.0f;
@@ -775,15 +775,14 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
     if (!(p->world_extent[k] > 0)) return fail(BB_E_INVALID, "world_extent must be positive");
   if (p->schedule > BB_SCHEDULE_COLOUR_BARRIER) return fail(BB_E_INVALID, "unknown schedule");
   if ((p->broad_threads != 0 && p->broad_threads != 32 && p->broad_threads != 64 && p->broad_threads != 128) ||
-      p->narrow_blocks_per_sm > 64 || p->flow_blocks_per_sm > 8)
-    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, flow <= 8)");
+      p->narrow_blocks_per_sm > 64 || p->pgs_stage_next > 1)
+    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, pgs_stage_next 0/1)");
   // contact geometry depends on these: no pair keeps last substep's manifolds as they were
   if (p->quirks != w->params.quirks || p->penetration_cap != w->params.penetration_cap)
     CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * (w->cap_n + 1), w->stream));
   w->params = *p;
   if (!w->params.broad_threads) w->params.broad_threads = 128;
   if (!w->params.narrow_blocks_per_sm) w->params.narrow_blocks_per_sm = 16;
-  if (!w->params.flow_blocks_per_sm) w->params.flow_blocks_per_sm = 8;
   return BB_OK;
 }
 
@@ -1254,33 +1253,34 @@ bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_s
     CU(cudaEventElapsedTime(ms, e0, e1));
     return bb_sync(world);
   };
-  float best_ms = 0.f;
-  bb_status st = trial(best, &best_ms);
+  bb_status st = BB_OK;
   struct Axis {
     uint32_t bb_solver_params::*field;
     std::vector<uint32_t> values;
-    bool pgs_only, dataflow_only;
+    bool pgs_only, barrier_only;
   };
   const std::vector<Axis> axes = {
       {&bb_solver_params::schedule, {BB_SCHEDULE_DATAFLOW, BB_SCHEDULE_COLOUR_BARRIER}, true, false},
       {&bb_solver_params::broad_threads, {32, 64, 128}, false, false},
       {&bb_solver_params::narrow_blocks_per_sm, {4, 8, 16, 32}, false, false},
+      {&bb_solver_params::pgs_stage_next, {0, 1}, true, true},
   };
   for (const Axis& ax : axes) {
     if (st != BB_OK) break;
     if (ax.pgs_only && best.solver != BB_SOLVER_PGS_SOFT) continue;
-    if (ax.dataflow_only && best.schedule != BB_SCHEDULE_DATAFLOW) continue;
+    if (ax.barrier_only && best.schedule != BB_SCHEDULE_COLOUR_BARRIER) continue;
     for (uint32_t v : ax.values) {
       if (best.*ax.field == v) continue;
       bb_solver_params cand = best;
       cand.*ax.field = v;
-      float ms = 0.f;
-      st = trial(cand, &ms);
+      // the world's step cost drifts as it evolves, so the candidate runs between two runs of
+      // the incumbent and is compared with their mean
+      float before = 0.f, ms = 0.f, after = 0.f;
+      st = trial(best, &before);
+      if (st == BB_OK) st = trial(cand, &ms);
+      if (st == BB_OK) st = trial(best, &after);
       if (st != BB_OK) break;
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = cand;
-      }
+      if (ms < 0.5f * (before + after)) best = cand;
     }
   }
   cudaEventDestroy(e0);

@@ -134,7 +134,8 @@ typedef struct bb_solver_params {
   /* launch geometry (results are identical for every value; 0 = default; bb_autotune picks) */
   uint32_t broad_threads;        /* broad-phase block size: 32, 64 or 128 (default 128) */
   uint32_t narrow_blocks_per_sm; /* narrow-phase grid, 128-thread blocks per SM: 1..64 (default 16) */
-  uint32_t flow_blocks_per_sm;   /* not used (kept for layout); the dataflow kernel is cooperative */
+  uint32_t pgs_stage_next;       /* colour-barrier PGS_SOFT: 1 stages each thread's next item of a colour in shared
+                                    memory while the current one computes (large worlds); 0 loads it after (default) */
   /* Morton normalisation */
   uint32_t bounds_mode;        /* BB_BOUNDS_* */
   float world_min[3];          /* default -64 */
@@ -383,9 +384,10 @@ bb_status bb_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* va
                                      uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
 
 /* Pick the launch geometry and colour-sweep schedule of this world by timing candidates
- * (coordinate descent over bb_solver_params.schedule, broad_threads,
- * narrow_blocks_per_sm).  All candidates give bit-identical results, so the trial steps are
- * ordinary steps (about 8 x (trial_steps + 1) of them): use it in place of warm-up.  The
+ * (coordinate descent over bb_solver_params.schedule, broad_threads, narrow_blocks_per_sm,
+ * pgs_stage_next; each candidate timed between two runs of the incumbent).  All candidates
+ * give bit-identical results, so the trial steps are ordinary steps (about 21 x
+ * (trial_steps + 1) of them): use it in place of warm-up.  The
  * winner is set on the world and copied to *chosen (may be NULL).  The reference has no
  * autotuner (its dispatch sizes are fixed in the task graph, src/rigid_body_manager.cpp:1284-1427). */
 bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_steps, bb_solver_params* chosen);

@@ -213,7 +213,7 @@ inline void default_params(bb_solver_params* p) {
   p->schedule = BB_SCHEDULE_COLOUR_BARRIER;  // execution details of the CUDA library; ignored here
   p->broad_threads = 128;
   p->narrow_blocks_per_sm = 16;
-  p->flow_blocks_per_sm = 8;
+  p->pgs_stage_next = 0;
   p->bounds_mode = BB_BOUNDS_FIXED;
   for (int i = 0; i < 3; ++i) {
     p->world_min[i] = -64.0f;

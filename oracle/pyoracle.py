@@ -30,7 +30,7 @@ class SolverParams(ctypes.Structure):
         ("avbd_stick_thresh", ctypes.c_float), ("avbd_stick_slop", ctypes.c_float),
         ("avbd_color_rounds", ctypes.c_uint32), ("avbd_shock_layers", ctypes.c_uint32),
         ("avbd_post_stab_sweeps", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("broad_threads", ctypes.c_uint32),
-        ("narrow_blocks_per_sm", ctypes.c_uint32), ("flow_blocks_per_sm", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
+        ("narrow_blocks_per_sm", ctypes.c_uint32), ("pgs_stage_next", ctypes.c_uint32), ("bounds_mode", ctypes.c_uint32),
         ("world_min", ctypes.c_float * 3), ("world_extent", ctypes.c_float * 3),
     ]
 

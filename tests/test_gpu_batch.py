@@ -148,6 +148,30 @@ def test_dataflow_schedule_equals_colour_barrier(name):
         assert np.array_equal(outs[0][k], outs[1][k]), k
 
 
+@pytest.mark.parametrize("name", ["mixed_3000", "pyramids_200x1000"])
+def test_staging_the_next_item_equals_loading_it(name):
+    """The colour-barrier kernel that stages each thread's next item of a colour in shared memory
+    while the current one computes runs the same arithmetic on the same data.  In the 200k-box
+    pyramids (over 400k manifolds in about a dozen colours, on at most 148 x 256 threads) the
+    threads run several items of the largest colours, so the staged path carries them."""
+    big = name == "pyramids_200x1000"
+    sc = scenes.pyramids(n_pyramids=200, boxes_per=1000, seed=0) if big else scenes.mixed_column(n_bodies=3000, seed=2)
+    outs = []
+    for stage in (0, 1):
+        p = params(bb.SOLVER_PGS_SOFT, schedule=bb.SCHEDULE_COLOUR_BARRIER, pgs_stage_next=stage)
+        w = bb.world_from_scene(sc, params=p)
+        for _ in range(4 if big else 40):
+            w.step(DT, 4)
+        outs.append(w.read_state())
+        st = w.stats()
+        assert st["error_flags"] == 0
+        if big:
+            assert st["manifold_count"] > 400_000  # the largest colours hold more items than the grid has threads
+        w.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
 def test_world_added_to_a_running_batch_leaves_the_others_unchanged():
     """Serving pattern: world B joins after A has run 10 steps; A continues exactly as alone
     (its warm-start contacts and sort order survive the join) and B runs as if alone."""
