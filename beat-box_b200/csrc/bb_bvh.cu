@@ -87,6 +87,7 @@ __device__ __forceinline__ bool box_overlap(float4 amn, float4 amx, float4 bmn, 
 
 // ---- kernels ---------------------------------------------------------------------------------
 __global__ void k_bounds(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 p = d.pos[i];
@@ -100,6 +101,7 @@ __global__ void k_bounds(const DevState d, uint32_t n) {
 
 // keys[0][i] = Morton code of body vals[0][i] (the previous substep's sorted order).
 __global__ void k_morton(const DevState d, uint32_t n, Params p) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float wmin[3], wext[3];
@@ -130,6 +132,7 @@ __global__ void k_morton(const DevState d, uint32_t n, Params p) {
 
 // world of every sorted position (batched worlds only)
 __global__ void k_sorted_world(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) d.sworld[i] = d.world_of[d.vals[0][i]];
 }
@@ -153,6 +156,7 @@ __device__ __forceinline__ int clz_delta(const uint32_t* codes, const uint32_t* 
 
 // leaves in sorted order + Karras internal nodes (LBVH.slang:155-221, RB_sim.slang:206-278)
 __global__ void k_build(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t* codes = d.keys[0];
@@ -201,6 +205,7 @@ __global__ void k_build(const DevState d, uint32_t n) {
 
 // bottom-up refit: the second child to arrive at a node merges both boxes and climbs on
 __global__ void k_refit(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || n < 2) return;
   int node = d.parent[n - 1 + i];
@@ -240,6 +245,7 @@ __global__ void k_refit(const DevState d, uint32_t n) {
 // rmin.xy), (rmin.z, rmax.xyz), (left, right, left last leaf, right last leaf), (left first
 // leaf, right first leaf, -, -).
 __global__ void k_node_recs(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (n < 2 || p >= n - 1) return;
   const int leaf0 = int(n) - 1;
@@ -333,6 +339,7 @@ __device__ __forceinline__ int world_end(const DevState& d, uint32_t qi, uint32_
 // EMIT=true re-walks only the queries that had more (is_heavy == 2) and writes their pairs.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (n < 2) {
@@ -381,6 +388,7 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
 // its query by a binary search over the scanned counts (shuffles): every lane has work, and a
 // pair's place pair_off[i] + k and value are those of the staged slot.
 __global__ void k_broad_copy(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   const uint32_t cap = d.pair_capacity;
   const int lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -455,6 +463,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp
 // ascending partner order.
 template <bool EMIT>
 __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, uint32_t n, int all) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   __shared__ int s_fr[2][BB_FRONTIER];
   __shared__ uint32_t s_warp[BB_FRONTIER / 32];
   __shared__ uint32_t s_size;
@@ -547,6 +556,7 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
 #define BB_HV_FRONTIER (BB_HV_THREADS * BB_HV_PER_THREAD)
 
 __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   __shared__ int s_fr[2][BB_HV_FRONTIER];
   __shared__ uint32_t s_warp[BB_HV_THREADS / 32];
   __shared__ uint32_t s_size, s_off, s_fits;
@@ -673,6 +683,7 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
 // EMIT=false: partners under each pool entry; EMIT=true: write them
 template <bool EMIT>
 __global__ void k_heavy_walk(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   const uint32_t E = min(d.ctr->hv_pool_n, d.hv_cap);
   const int N = int(n), leaf0 = N - 1;
   for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
@@ -701,6 +712,7 @@ __global__ void k_heavy_walk(const DevState d, uint32_t n) {
 
 // pair count of every heavy query with a pool frontier
 __global__ void k_heavy_totals(const DevState d) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
   const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
   for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < hc; slot += gridDim.x * blockDim.x) {
     const uint32_t m = d.hv_n[slot];
@@ -722,11 +734,11 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   uint32_t* vals[2] = {d.vals[0], d.vals[1]};
   if (d.n_worlds > 1) {
     // stable sort by code, then by world id (two digits of world_of[id]): key order (world, code)
-    bb_launch_sort(s, keys, vals, nullptr, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms,
-                   d.world_of, 2);
+    bb_launch_sort(s, keys, vals, &d.ctr->front_n, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr,
+                   sms, d.world_of, 2);
     k_sorted_world<<<blocks, T, 0, s>>>(d, n);
   } else {
-    bb_launch_sort(s, keys, vals, nullptr, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms);
+    bb_launch_sort(s, keys, vals, &d.ctr->front_n, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms);
   }
   k_build<<<blocks, T, 0, s>>>(d, n);
   k_refit<<<blocks, T, 0, s>>>(d, n);
@@ -744,11 +756,12 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
     k_heavy_frontier<<<min(hb, 2u * uint32_t(sms)), BB_HV_THREADS, 0, s>>>(d, n);
     k_heavy_walk<false><<<sms * 8, 128, 0, s>>>(d, n);
     bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr,
-                   sc.scan_status + 5 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 5, d.ctr);
+                   sc.scan_status + 5 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 5, d.ctr, &d.ctr->front_skip);
     k_heavy_totals<<<(hb + 255) / 256, 256, 0, s>>>(d);
   }
   k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n, pool ? 0 : 1);
-  bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr);
+  bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr,
+                 &d.ctr->front_skip);
   k_broad_copy<<<sms * 16, 256, 0, s>>>(d, n);
   k_broad<true><<<bb, bt, 0, s>>>(d, n);
   k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n, pool ? 0 : 1);

@@ -66,6 +66,11 @@ struct DevCounters {
   uint32_t hv_pool_n;      // broad phase: frontier entries of the heavy queries
   uint32_t slot_count;     // worlds with voxel shapes: manifold slots (6 per voxel pair, else 1)
   uint32_t slots_of[2];    // manifold slots of the narrow phase that last wrote contact buffer 0 / 1
+  // Front-end skip: when no body was awake after the last substep's sleep stage, nothing was
+  // integrated, so every pose (and the sort, tree and pair list built from them) is as the last
+  // front end left it.  front_valid is cleared by every host-side change of bodies, poses or
+  // parameters; front_n is the front-end sort's key count (0 when skipped, else all).
+  uint32_t front_skip, front_valid, front_n, sleep_ran, awake_after;
 };
 
 // Voxel shape on the device (VoxelShape, include/shared.inl:938-951) with the body-frame box

@@ -201,6 +201,7 @@ __global__ void k_sleep_veto(const DevState d, Params p, int cur) {
 }
 __global__ void k_sleep_apply(const DevState d, uint32_t n, Params p) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) d.ctr->sleep_ran = 1u;  // with awake_after: the next substep may skip its front end
   if (i >= n) return;
   uint32_t f = d.flags[i];
   if (!(f & BB_BODY_DYNAMIC)) return;
@@ -216,8 +217,9 @@ __global__ void k_sleep_apply(const DevState d, uint32_t n, Params p) {
       d.flags[i] = f | BB_BODY_SLEEPING;
     }
     atomicAdd(&d.ctr->sleeping, 1u);
-  } else if (was) {
-    d.flags[i] = f & ~BB_BODY_SLEEPING;
+  } else {
+    if (was) d.flags[i] = f & ~BB_BODY_SLEEPING;
+    if (d.ctr->awake_after == 0u) d.ctr->awake_after = 1u;  // this body is integrated: poses move
   }
 }
 

@@ -3,8 +3,10 @@
 #include "bb_common.cuh"
 
 // bb_scan_sort.cu
+// skip (device word, may be null): when non-zero the scan does nothing (not even its total)
 void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint32_t n_cap,
-                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr);
+                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr,
+                    const uint32_t* skip = nullptr);
 uint32_t bb_scan_tiles(uint32_t n_cap);
 uint32_t bb_sort_tiles(uint32_t n_cap);
 #define BB_SORT_TILE 4096  // keys per onesweep tile

@@ -29,9 +29,10 @@ constexpr uint32_t kValMask = (1u << 30) - 1u;
 __global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
                                                    const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
                                                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr,
-                                                   DevCounters* ctr) {
+                                                   DevCounters* ctr, const uint32_t* __restrict__ skip) {
   __shared__ uint32_t s_tile, s_excl;
   __shared__ uint32_t s_warp[kThreads / 32];
+  if (skip && *skip) return;
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
   __syncthreads();
   const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
@@ -322,10 +323,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_onesweep(const uint32_t* __rest
 // ---------------------------------------------------------------------------------------
 // host launchers
 void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint32_t n_cap,
-                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr) {
+                    uint32_t* total, unsigned long long* status, uint32_t* tile_ctr, DevCounters* ctr,
+                    const uint32_t* skip) {
   uint32_t tiles = (n_cap + kTile - 1) / kTile;
   if (tiles == 0) tiles = 1;
-  k_scan<<<tiles, kThreads, 0, s>>>(in, out, n_dev, n_cap, total, status, tile_ctr, ctr);
+  k_scan<<<tiles, kThreads, 0, s>>>(in, out, n_dev, n_cap, total, status, tile_ctr, ctr, skip);
 }
 
 uint32_t bb_scan_tiles(uint32_t n_cap) { return n_cap / kTile + 1; }

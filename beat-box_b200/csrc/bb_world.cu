@@ -124,6 +124,7 @@ __global__ void k_extend_contacts(const DevState d, uint32_t o, uint32_t count) 
   if (i >= count) return;
   d.vals[0][o + i] = o + i;
   d.frozen[o + i] = 0;
+  if (i == 0) d.ctr->front_valid = 0;
   for (int k = 0; k < 2; ++k) d.csr_start[k][o + 1 + i] = d.csr_start[k][o];
 }
 
@@ -158,7 +159,20 @@ __global__ void k_contact_points(const DevState d, int cur, float4* out) {
 
 __global__ void k_begin_substep(DevCounters* c) {
   if (threadIdx.x != 0) return;
-  c->pair_count = 0;
+  const bool still = c->front_valid != 0u && c->sleep_ran != 0u && c->awake_after == 0u;
+  c->front_skip = still ? 1u : 0u;
+  c->front_n = still ? 0u : 0xFFFFFFFFu;
+  c->front_valid = 1u;
+  c->sleep_ran = 0;
+  c->awake_after = 0;
+  if (!still) {  // the skipped front end's outputs stay: its pair count and bounds
+    c->pair_count = 0;
+    c->hv_pool_n = 0;
+    for (int k = 0; k < 3; ++k) {
+      c->bounds_min[k] = 0xFFFFFFFFu;
+      c->bounds_max[k] = 0u;
+    }
+  }
   c->manifold_count = 0;
   c->contact_count = 0;
   c->fresh = 0;
@@ -172,10 +186,6 @@ __global__ void k_begin_substep(DevCounters* c) {
   c->avbd_violations = 0;
   c->stick = 0;
   c->barrier_count = 0;
-  for (int k = 0; k < 3; ++k) {
-    c->bounds_min[k] = 0xFFFFFFFFu;
-    c->bounds_max[k] = 0u;
-  }
   for (int k = 0; k < 6; ++k) c->pad[k] = 0;
   for (int k = 0; k < 8; ++k) c->sync_count[k] = 0;
   c->np_counts[0] = 0;
@@ -185,7 +195,6 @@ __global__ void k_begin_substep(DevCounters* c) {
   c->slot_count = 0;
   c->gc_list_n[0] = 0;
   c->gc_list_n[1] = 0;
-  c->hv_pool_n = 0;
   c->substeps += 1;
 }
 
@@ -332,6 +341,7 @@ struct bb_world_impl {
 
   void reset_contacts() {
     cudaMemsetAsync(d.frozen, 0, sizeof(uint32_t) * (cap_n + 1), stream);
+    cudaMemsetAsync(&d.ctr->front_valid, 0, sizeof(uint32_t), stream);
     cudaMemsetAsync(d.csr_start[0], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     cudaMemsetAsync(d.csr_start[1], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     std::vector<uint32_t> ident(n);
@@ -780,6 +790,7 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
   // contact geometry depends on these: no pair keeps last substep's manifolds as they were
   if (p->quirks != w->params.quirks || p->penetration_cap != w->params.penetration_cap)
     CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * (w->cap_n + 1), w->stream));
+  CU(cudaMemsetAsync(&w->d.ctr->front_valid, 0, sizeof(uint32_t), w->stream));  // bounds, modes
   w->params = *p;
   if (!w->params.broad_threads) w->params.broad_threads = 128;
   if (!w->params.narrow_blocks_per_sm) w->params.narrow_blocks_per_sm = 16;
@@ -989,7 +1000,10 @@ bb_status bb_write_state(void* world, const float* position, const float* rotati
   if (omega) { CU(cudaMemcpyAsync(st + 10ull * n, omega, 12ull * n, cudaMemcpyHostToDevice, w->stream)); mask |= 8; }
   k_unpack_state<<<(n + 255) / 256, 256, 0, w->stream>>>(w->d, n, st, mask);
   // moved poses: no body keeps last substep's manifolds as they were
-  if (mask & 3u) CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * n, w->stream));
+  if (mask & 3u) {
+    CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * n, w->stream));
+    CU(cudaMemsetAsync(&w->d.ctr->front_valid, 0, sizeof(uint32_t), w->stream));
+  }
   // the caller may reuse its buffers as soon as this returns
   CU(cudaStreamSynchronize(w->stream));
   return BB_OK;

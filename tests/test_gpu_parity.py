@@ -429,3 +429,36 @@ def test_islands_start_from_last_roots_like_a_fresh_union_find(oracle_lib):
         merged += gi[17] == gi[19]  # the lower stack and the falling stack share an island
     assert compared >= 50 and slept >= 20 and merged >= 5, (compared, slept, merged)
     assert w.stats()["error_flags"] == 0
+
+
+def test_front_end_skipped_while_everything_sleeps_keeps_its_outputs():
+    """Once every body sleeps nothing is integrated, so the front end (Morton codes, sort, tree,
+    pairs) is skipped and its last outputs stand.  They must equal what a fresh world computes
+    from the same poses, and a pose write must bring the front end back."""
+    sc = resting_scene()
+    p = bb.make_params(solver=bb.SOLVER_PGS_SOFT, quirks=bb.QUIRKS_PHYSICAL, iterations=8, relax_iterations=8)
+    w = bb.world_from_scene(sc, params=p)
+    for _ in range(40):
+        w.step(DT, 4)
+    w.sync()
+    assert w.stats()["sleeping_count"] == 18
+    keys, ids, pairs = w.debug_read("sorted_keys"), w.debug_read("sorted_ids"), w.debug_read("pairs")
+    st = w.read_state()
+    sc2 = dict(sc)
+    sc2["pos"], sc2["quat"] = st["pos"].copy(), st["quat"].copy()
+    sc2["vel"], sc2["omega"] = np.zeros_like(st["vel"]), np.zeros_like(st["omega"])
+    fresh = bb.world_from_scene(sc2, params=p)
+    fresh.debug_collide(2)
+    assert np.array_equal(fresh.debug_read("sorted_keys"), keys)
+    assert np.array_equal(fresh.debug_read("sorted_ids"), ids)
+    n_pairs = w.stats()["pair_count"]
+    assert n_pairs == fresh.stats()["pair_count"] > 0
+    assert np.array_equal(fresh.debug_read("pairs")[: 2 * n_pairs], pairs[: 2 * n_pairs])
+    # lift one single box far above the others: its ground pair must go
+    pos = st["pos"].copy()
+    pos[1, 1] += 20.0
+    w.write_state(pos=pos)
+    w.step(DT, 1)
+    w.sync()
+    assert w.stats()["pair_count"] == n_pairs - 1
+    assert w.stats()["error_flags"] == 0
