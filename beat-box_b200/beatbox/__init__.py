@@ -131,7 +131,8 @@ class StepStats(ctypes.Structure):
         "graph_color_count", "graph_color_overflow", "graph_color_violations", "avbd_color_count",
         "avbd_violations", "sleeping_count", "fresh_contacts", "stick_count")] + [
         ("max_penetration", ctypes.c_float), ("error_flags", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
-        ("substeps_run", ctypes.c_uint32)]
+        ("substeps_run", ctypes.c_uint32), ("solved_manifolds", ctypes.c_uint32),
+        ("solved_contacts", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -171,12 +172,14 @@ _SIG = {
     "bb_skip_warm_starting_once": (ctypes.c_int32, [_P]),
     "bb_debug_collide": (ctypes.c_int32, [_P, _U32]),
     "bb_debug_read": (ctypes.c_int32, [_P, _U32, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "bb_debug_wait_limit": (ctypes.c_int32, [_P, _U32, _U32]),
     "bb_world_stream": (ctypes.c_void_p, [_P]),
     "bb_set_profiling": (ctypes.c_int32, [_P, ctypes.c_int32]),
     "bb_read_stage_times": (ctypes.c_int32, [_P, _P, _U32, ctypes.POINTER(_U32), _P, _U32]),
     "bb_kernel_launch_count": (ctypes.c_uint64, [_P]),
     "bb_radix_sort_pairs": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
     "bb_radix_sort_pairs_static": (ctypes.c_int32, [_P, _P, _P, _P, _U32, _U32, _P]),
+    "bb_radix_sort_error_flags": (ctypes.c_int32, [_U32, _P, ctypes.POINTER(_U32)]),
     "bb_autotune": (ctypes.c_int32, [_P, ctypes.c_float, _U32, _U32, ctypes.POINTER(SolverParams)]),
     "bb_update_transforms": (ctypes.c_int32, [_P]),
     "bb_transforms_device": (ctypes.c_void_p, [_P]),
@@ -438,6 +441,16 @@ class World:
 
     def debug_collide(self, stage: int):
         _check(self.L.bb_debug_collide(self.h, stage))
+
+    def debug_wait_limit(self, polls: int, abandon_block: bool = False):
+        """Bound of the persistent kernels' grid-barrier waits (0 = default); abandon_block makes
+        the colour-sweep kernel's last block leave so the other blocks' waits run out."""
+        _check(self.L.bb_debug_wait_limit(self.h, polls, 1 if abandon_block else 0))
+
+    def clear(self):
+        """Remove every body and shape (device buffers kept); clears the device error bits."""
+        self._shape_cache = {}
+        _check(self.L.bb_world_clear(self.h))
 
     def debug_read(self, which: str):
         code = DBG[which]

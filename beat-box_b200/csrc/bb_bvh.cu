@@ -203,17 +203,29 @@ __global__ void k_build(const DevState d, uint32_t n) {
   d.visit[i] = 0;
 }
 
-// bottom-up refit: the second child to arrive at a node merges both boxes and climbs on
+__device__ __forceinline__ uint32_t atom_add_acq_rel_gpu(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// Bottom-up refit: the second child to arrive at a node merges both boxes and climbs on.  The
+// arrival counter is one acquire-release atomic: its release publishes the arriving thread's
+// box, its acquire makes the sibling's box visible to the second arriver.  The thread that
+// merges a node also writes the node's traversal record (below), so the records cost no pass
+// of their own over the node boxes.
+__device__ __forceinline__ void write_node_rec(const DevState& d, int p, int2 c, int leaf0, float4 lmn, float4 lmx,
+                                               float4 rmn, float4 rmx);
+
 __global__ void k_refit(const DevState d, uint32_t n) {
   if (d.ctr->front_skip) return;  // nothing moved since the last front end
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || n < 2) return;
-  int node = d.parent[n - 1 + i];
+  const int leaf0 = int(n) - 1;
+  int node = d.parent[leaf0 + i];
   uint32_t guard = 0;
   while (node >= 0) {
-    __threadfence();
-    if (atomicAdd(&d.visit[node], 1u) == 0u) return;  // first arriver: sibling not ready
-    __threadfence();
+    if (atom_add_acq_rel_gpu(&d.visit[node], 1u) == 0u) return;  // first arriver: sibling not ready
     int2 c = d.child[node];
     float4 amn = __ldcg(&d.node_box[2 * c.x]), amx = __ldcg(&d.node_box[2 * c.x + 1]);
     float4 bmn = __ldcg(&d.node_box[2 * c.y]), bmx = __ldcg(&d.node_box[2 * c.y + 1]);
@@ -223,6 +235,7 @@ __global__ void k_refit(const DevState d, uint32_t n) {
                             bmx.z > amx.z ? bmx.z : amx.z, 0.f);
     __stcg(&d.node_box[2 * node], mn);
     __stcg(&d.node_box[2 * node + 1], mx);
+    write_node_rec(d, node, c, leaf0, amn, amx, bmn, bmx);
     node = d.parent[node];
     if (++guard > 128u) {  // a Karras tree over 30-bit codes + 32 index bits is < 64 deep
       raise_error(d.ctr, BB_ERRF_STACK_OVERFLOW);
@@ -239,19 +252,13 @@ __global__ void k_refit(const DevState d, uint32_t n) {
 #define BB_FRONTIER 256
 
 // Internal node records for the traversals: both children's boxes, indices and leaf ranges in
-// one 80-byte record (5 float4), built after the refit.  A visit is then one dependent load
-// (instead of the child indices, then each child's range and box), and a leaf child is tested
-// from its parent's record without being visited.  Layout: (lmin.xyz, lmax.x), (lmax.yz,
-// rmin.xy), (rmin.z, rmax.xyz), (left, right, left last leaf, right last leaf), (left first
-// leaf, right first leaf, -, -).
-__global__ void k_node_recs(const DevState d, uint32_t n) {
-  if (d.ctr->front_skip) return;  // nothing moved since the last front end
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n < 2 || p >= n - 1) return;
-  const int leaf0 = int(n) - 1;
-  const int2 c = d.child[p];
-  const float4 lmn = d.node_box[2 * c.x], lmx = d.node_box[2 * c.x + 1];
-  const float4 rmn = d.node_box[2 * c.y], rmx = d.node_box[2 * c.y + 1];
+// one 80-byte record (5 float4), written by the refit when it merges the node.  A visit is then
+// one dependent load (instead of the child indices, then each child's range and box), and a
+// leaf child is tested from its parent's record without being visited.  Layout: (lmin.xyz,
+// lmax.x), (lmax.yz, rmin.xy), (rmin.z, rmax.xyz), (left, right, left last leaf, right last
+// leaf), (left first leaf, right first leaf, -, -).
+__device__ __forceinline__ void write_node_rec(const DevState& d, int p, int2 c, int leaf0, float4 lmn, float4 lmx,
+                                               float4 rmn, float4 rmx) {
   const int lf = c.x >= leaf0 ? c.x - leaf0 : d.range_first[c.x], ll = c.x >= leaf0 ? c.x - leaf0 : d.range_last[c.x];
   const int rf = c.y >= leaf0 ? c.y - leaf0 : d.range_first[c.y], rl = c.y >= leaf0 ? c.y - leaf0 : d.range_last[c.y];
   float4* r = d.node_rec + 5 * size_t(p);
@@ -723,13 +730,14 @@ __global__ void k_heavy_totals(const DevState d) {
 }
 
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
-                  int cur, uint32_t max_world_bodies) {
+                  int cur, uint32_t max_world_bodies, cudaEvent_t* marks) {
   (void)cur;
   if (n == 0) return;
   const int T = BB_THREADS;
   uint32_t blocks = (n + T - 1) / T;
   if (p.bounds_mode == BB_BOUNDS_AUTO) k_bounds<<<blocks, T, 0, s>>>(d, n);
   k_morton<<<blocks, T, 0, s>>>(d, n, p);
+  if (marks) cudaEventRecord(marks[0], s);
   uint32_t* keys[2] = {d.keys[0], d.keys[1]};
   uint32_t* vals[2] = {d.vals[0], d.vals[1]};
   if (d.n_worlds > 1) {
@@ -740,9 +748,11 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   } else {
     bb_launch_sort(s, keys, vals, &d.ctr->front_n, n, 4, 0, sc.sort_hist, sc.sort_status, sc.sort_tile_ctr, d.ctr, sms);
   }
+  if (marks) cudaEventRecord(marks[1], s);
   k_build<<<blocks, T, 0, s>>>(d, n);
+  if (marks) cudaEventRecord(marks[2], s);
   k_refit<<<blocks, T, 0, s>>>(d, n);
-  k_node_recs<<<blocks, T, 0, s>>>(d, n);
+  if (marks) cudaEventRecord(marks[3], s);
   const uint32_t bt = p.broad_threads ? p.broad_threads : 128u;
   uint32_t bb = (n + bt - 1) / bt;
   uint32_t hb = min(n, BB_HEAVY_CAP);

@@ -57,7 +57,11 @@ struct DevCounters {
   uint32_t bounds_max[3];
   uint32_t avbd_body_count;
   uint32_t substeps;       // substeps run since the world was created
-  uint32_t pad[6];
+  uint32_t wait_limit;     // polls before a bounded device wait gives up (0 = BB_SPIN_LIMIT)
+  uint32_t abandon_block;  // test switch: the PGS solver's last block leaves before its first barrier
+  uint32_t pgs_manifolds;  // per substep: colour-sweep items with an awake body (solved manifolds)
+  uint32_t pgs_contacts;   // their contacts
+  uint32_t pad[2];
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
                            // 7 connected components
@@ -352,6 +356,19 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
 }
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
+// Bound of every grid-barrier wait: checked once per 64 polls (a barrier that completes within
+// them never reads it).  Gives up past the world's wait_limit (BB_SPIN_LIMIT when 0), raising
+// BB_ERRF_SPIN_LIMIT, or at once when another wait of the launch already gave up.
+__device__ __forceinline__ bool spin_gave_up(DevCounters* c, uint32_t spins) {
+  if ((spins & 63u) != 0u) return false;
+  const uint32_t lim = *reinterpret_cast<volatile const uint32_t*>(&c->wait_limit);
+  if (spins > (lim ? lim : BB_SPIN_LIMIT)) {
+    atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
+    return true;
+  }
+  return (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT) != 0;
+}
+
 __device__ __forceinline__ void grid_barrier(DevCounters* c) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -364,13 +381,8 @@ __device__ __forceinline__ void grid_barrier(DevCounters* c) {
       atomicAdd(&c->barrier_gen, 1u);
     } else {
       uint32_t spins = 0;
-      while (ld_acquire_gpu(&c->barrier_gen) == g) {
-        if (++spins > BB_SPIN_LIMIT) {
-          atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
-          break;
-        }
-        if ((spins & 1023u) == 0u && (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT)) break;
-      }
+      while (ld_acquire_gpu(&c->barrier_gen) == g)
+        if (spin_gave_up(c, ++spins)) break;
     }
     fence_acq_rel_gpu();
   }
@@ -393,13 +405,8 @@ __device__ __forceinline__ void grid_sync(DevCounters* c, uint32_t* count, uint3
     red_relaxed_add(count, 1u);
     const uint32_t target = epoch * gridDim.x;
     uint32_t spins = 0;
-    while (ld_acquire_gpu(count) < target) {
-      if (++spins > BB_SPIN_LIMIT) {
-        atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
-        break;
-      }
-      if ((spins & 1023u) == 0u && (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT)) break;
-    }
+    while (ld_acquire_gpu(count) < target)
+      if (spin_gave_up(c, ++spins)) break;
   }
   __syncthreads();
 }
@@ -419,13 +426,8 @@ __device__ __forceinline__ void grid_wait(DevCounters* c, const uint32_t* count,
   if (threadIdx.x == 0 && gridDim.x > 1) {
     const uint32_t target = epoch * gridDim.x;
     uint32_t spins = 0;
-    while (ld_acquire_gpu(count) < target) {
-      if (++spins > BB_SPIN_LIMIT) {
-        atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
-        break;
-      }
-      if ((spins & 1023u) == 0u && (ld_acquire_gpu(&c->error_flags) & BB_ERRF_SPIN_LIMIT)) break;
-    }
+    while (ld_acquire_gpu(count) < target)
+      if (spin_gave_up(c, ++spins)) break;
   }
   __syncthreads();
 }

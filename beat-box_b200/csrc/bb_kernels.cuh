@@ -30,10 +30,10 @@ struct StepScratch {
   uint32_t sort_tiles;
 };
 
-// bb_bvh.cu: Morton codes -> sort -> Karras LBVH -> refit -> broad phase
+// bb_bvh.cu: Morton codes -> sort -> Karras LBVH -> refit -> broad phase.  marks (may be
+// null): four events recorded after the Morton codes, the sort, the tree build and the refit.
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
-                  int cur,
-                  uint32_t max_world_bodies);
+                  int cur, uint32_t max_world_bodies, cudaEvent_t* marks = nullptr);
 
 // bb_narrow.cu: narrow phase + warm start + manifold compaction + per-body lists
 void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc,
@@ -60,6 +60,7 @@ void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t 
 bb_status bb_fail(bb_status code, const char* msg);
 
 // stand-alone radix sort helpers (bb_sort_api.cu)
+char* bb_sort_scratch_base();
 bb_status bb_check_sort_args(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                              uint32_t n, uint32_t key_bits);
 void bb_sort_carve(char* base, uint32_t n, int passes, DevCounters** ctr, uint32_t** hist, uint32_t** tile_ctr,

@@ -394,6 +394,8 @@ __global__ void k_pgs_count(const DevState d, int cur) {
     const uint2 b = d.m_bodies[cur][slot];
     const bool skip = !awake(d.flags[b.x]) && !awake(d.flags[b.y]);
     d.pgs_cnt[k] = skip ? 0u : uint32_t(d.m_keycc[cur][slot].y);
+    const uint32_t act = __ballot_sync(__activemask(), !skip);
+    if ((threadIdx.x & 31u) == uint32_t(__ffs(__activemask()) - 1) && act) atomicAdd(&d.ctr->pgs_manifolds, __popc(act));
     if (!skip) {  // set once: most threads only read the flag (33 hot words otherwise take every store)
       uint32_t* f = &d.colour_awake[min(d.gc_color[list[k]], uint32_t(BB_MAX_COLORS))];
       if (*f == 0u) *f = 1u;
@@ -678,6 +680,9 @@ template <int PF, bool STAGE_NEXT>
 __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   __shared__ uint32_t bs[BB_MAX_COLORS + 2];
   __shared__ uint32_t aw[BB_MAX_COLORS + 1];
+  // test switch (bb_debug_wait_limit): the last block leaves, so the others' first grid barrier
+  // waits for a block that never arrives until its bounded wait gives up
+  if (gridDim.x > 1 && blockIdx.x == gridDim.x - 1 && d.ctr->abandon_block) return;
   if (threadIdx.x < BB_MAX_COLORS + 2) bs[threadIdx.x] = d.bucket_start[threadIdx.x];
   if (threadIdx.x < BB_MAX_COLORS + 1) aw[threadIdx.x] = d.colour_awake[threadIdx.x];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
@@ -742,12 +747,8 @@ __device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v) {
 }
 __device__ __forceinline__ void flow_wait(DevCounters* c, const uint32_t* ctr, uint32_t target) {
   uint32_t spins = 0;
-  while (ld_acquire_gpu(ctr) < target) {
-    if (++spins > BB_SPIN_LIMIT) {
-      atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
-      return;
-    }
-  }
+  while (ld_acquire_gpu(ctr) < target)
+    if (spin_gave_up(c, ++spins)) return;
 }
 
 // per colour-ordered item k: (rank_a | rank_b << 16, deg_a | deg_b << 16) where rank_x is the
@@ -854,7 +855,7 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
                        const StepScratch& sc, int coop_blocks, int sms) {
   cudaMemsetAsync(d.colour_awake, 0, sizeof(uint32_t) * (BB_MAX_COLORS + 1), s);
   k_pgs_count<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
-  bb_launch_scan(s, d.pgs_cnt, d.pgs_coff, &d.ctr->manifold_count, d.pair_capacity, nullptr,
+  bb_launch_scan(s, d.pgs_cnt, d.pgs_coff, &d.ctr->manifold_count, d.pair_capacity, &d.ctr->pgs_contacts,
                  sc.scan_status + 4 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 4, d.ctr);
   if (p.schedule == BB_SCHEDULE_DATAFLOW) {
     k_flow_prep<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);

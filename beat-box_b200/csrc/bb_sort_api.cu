@@ -46,6 +46,16 @@ void bb_sort_carve(char* base, uint32_t n, int passes, DevCounters** ctr, uint32
   *tmp_vals = *tmp_keys + n;
 }
 
+// Scratch block of bb_radix_sort_pairs on the current device (nullptr before its first call).
+char* bb_sort_scratch_base() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_sort_mu);
+  for (auto& c : g_sort_cache)
+    if (c.device == dev) return c.base;
+  return nullptr;
+}
+
 bb_status bb_check_sort_args(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                              uint32_t n, uint32_t key_bits) {
   if (key_bits == 0 || key_bits > 32) return bb_fail(BB_E_INVALID, "radix sort: key_bits must be 1..32");

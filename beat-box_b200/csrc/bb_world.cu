@@ -175,6 +175,8 @@ __global__ void k_begin_substep(DevCounters* c) {
   }
   c->manifold_count = 0;
   c->contact_count = 0;
+  c->pgs_manifolds = 0;
+  c->pgs_contacts = 0;
   c->fresh = 0;
   c->max_pen_bits = 0;
   c->island_count = 0;
@@ -532,6 +534,10 @@ bb_status bb_world_clear(void* world) {
   w->invalidate_graphs();
   uint32_t nn[2] = {0, 0};
   CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
+  // the next substep rebuilds the front end whatever the bodies added later; the sticky
+  // device error bits of earlier steps go with the bodies
+  CU(cudaMemsetAsync(&w->d.ctr->front_valid, 0, sizeof(uint32_t), w->stream));
+  CU(cudaMemsetAsync(&w->d.ctr->error_flags, 0, sizeof(uint32_t), w->stream));
   CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
@@ -863,38 +869,41 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
   }
   if (w->profiling) {
     // per-stage timing: run the substeps stage by stage with events
-    static const char* names[] = {"front_end", "narrow_phase", "advect", "islands", "sleep", "edge_coloring", "solve"};
-    if (w->stage_ms.size() != 7) {
-      w->stage_ms.assign(7, 0.f);
-      w->stage_names.assign(names, names + 7);
+    // the front end is split at its sort, tree build and refit (their own rooflines)
+    static const char* names[] = {"morton", "sort", "lbvh_build", "refit", "broad_phase", "narrow_phase", "advect",
+                                  "islands", "sleep", "edge_coloring", "solve"};
+    constexpr int kStages = 11;
+    if (w->stage_ms.size() != kStages) {
+      w->stage_ms.assign(kStages, 0.f);
+      w->stage_names.assign(names, names + kStages);
     }
     for (uint32_t s = 0; s < substeps; ++s) {
       const int cur = w->parity ^ 1;
-      cudaEvent_t ev[8];
+      cudaEvent_t ev[kStages + 1];
       for (auto& e : ev) cudaEventCreate(&e);
       k_begin_substep<<<1, 32, 0, w->stream>>>(w->d.ctr);
       cudaMemsetAsync(w->scratch_base, 0, w->scratch_bytes, w->stream);
       cudaEventRecord(ev[0], w->stream);
-      bb_front_end(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->max_world_bodies());
-      cudaEventRecord(ev[1], w->stream);
-      bb_narrow_phase(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, s == 0 ? warm_first : warm_rest);
-      cudaEventRecord(ev[2], w->stream);
-      bb_advect(w->stream, w->d, w->params, w->n, h, w->sms);
-      cudaEventRecord(ev[3], w->stream);
-      bb_islands(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_cc);
-      cudaEventRecord(ev[4], w->stream);
-      bb_sleep(w->stream, w->d, w->params, w->n, w->sms, cur);
+      bb_front_end(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->max_world_bodies(), ev + 1);
       cudaEventRecord(ev[5], w->stream);
+      bb_narrow_phase(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, s == 0 ? warm_first : warm_rest);
+      cudaEventRecord(ev[6], w->stream);
+      bb_advect(w->stream, w->d, w->params, w->n, h, w->sms);
+      cudaEventRecord(ev[7], w->stream);
+      bb_islands(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_cc);
+      cudaEventRecord(ev[8], w->stream);
+      bb_sleep(w->stream, w->d, w->params, w->n, w->sms, cur);
+      cudaEventRecord(ev[9], w->stream);
       const bool coloured = (w->params.flags & BB_SIM_USE_GRAPH_COLORING) != 0;
       if (coloured || w->params.solver == BB_SOLVER_AVBD)
         bb_edge_coloring(w->stream, w->d, w->params, w->n, w->sc, w->sms, cur, w->coop_edge);
-      cudaEventRecord(ev[6], w->stream);
+      cudaEventRecord(ev[10], w->stream);
       if (w->params.solver == BB_SOLVER_AVBD) bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
       else if (!coloured) bb_solve_islands(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->sms);
       else bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->sms);
-      cudaEventRecord(ev[7], w->stream);
-      CU(cudaEventSynchronize(ev[7]));
-      for (int k = 0; k < 7; ++k) {
+      cudaEventRecord(ev[11], w->stream);
+      CU(cudaEventSynchronize(ev[11]));
+      for (int k = 0; k < kStages; ++k) {
         float ms = 0;
         cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
         w->stage_ms[k] += ms;
@@ -1044,6 +1053,8 @@ bb_status bb_read_stats(void* world, bb_step_stats* s) {
   s->error_flags = c.error_flags;
   s->pair_capacity = w->cap_p;
   s->substeps_run = c.substeps;
+  s->solved_manifolds = c.pgs_manifolds;
+  s->solved_contacts = c.pgs_contacts;
   return BB_OK;
 }
 
@@ -1201,6 +1212,15 @@ bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_byt
   if (st != BB_OK) return st;
   if (dst) std::memcpy(dst, out.data(), std::min<uint64_t>(out.size(), max_bytes));
   if (count) *count = cnt;
+  return BB_OK;
+}
+
+bb_status bb_debug_wait_limit(void* world, uint32_t polls, uint32_t abandon_block) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "null world");
+  const uint32_t v[2] = {polls, abandon_block ? 1u : 0u};
+  CU(cudaMemcpyAsync(&w->d.ctr->wait_limit, v, sizeof(v), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
 

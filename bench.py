@@ -1,17 +1,21 @@
 """Benchmark of the B200 rigid-body step (body-steps/s), one JSON line on rank 0.
 
-Workload (default): 100,000 mixed bodies (60% boxes with half extents U[0.2, 0.8], 40% spheres
-with lognormal radii) dropped from a 60x60x200 m column into a 5-wall container; FP32 state,
-dt = 1/60 s, 4 substeps, PGS_SOFT 10 solve + 10 relax iterations, physical arithmetic (the
-reference's gravity / SAT-frame / inertia quirks off).  Synthetic seeded scene (seed 0): no
-public dataset exists for this workload.  A "step" is one bb_step(dt, 4) of the whole world.
+Workload (default): 1,000,000 unit boxes in 1,000 pyramids of 1,000 boxes (base 18x18, tapering)
+on a 32x32 grid of cells 20 m apart over a ground box, initial velocity N(0, 0.01) m/s per
+component; FP32 state, dt = 1/60 s, 4 substeps, PGS_SOFT 10 solve + 10 relax iterations,
+physical arithmetic (the reference's gravity / SAT-frame / inertia quirks off).  Seeded synthetic
+scene (seed 0): no public dataset exists for this workload.  A "step" is one bb_step(dt, 4) of
+the whole world.
 
-Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the world's
-stream; L2 is flushed (256 MB write) before every timed step, outside the events.  Multi-GPU
-(torchrun): a single world does not shard, so every rank steps its own replica; the time is
-the max over ranks and value = all ranks' body-steps / that time.
+Timing: the run starts from the scene at rest; W untimed warm-up steps, then the next K steps,
+each bracketed by CUDA events on the world's stream (the awake settling phase of the pyramids:
+every front-end, colouring and solver stage runs at full size); L2 is flushed (256 MB write)
+before every timed step, outside the events.  Multi-GPU (torchrun): a single world does not
+shard, so every rank steps its own replica; the time is the max over ranks and value = all
+ranks' body-steps / that time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solver pgs|avbd]
+                  [--scene pyramids|mixed_column|box_grid|voxel_pile] [--mode plain|batched|served|sort]
 """
 from __future__ import annotations
 
@@ -32,23 +36,24 @@ from beatbox import ranks, scenes  # noqa: E402
 
 DT = 1.0 / 60.0
 SUBSTEPS = 4
-N_BODIES = 100_000
 L2_BYTES = 126 * 1024 * 1024
-# DRAM bytes (read + write) of one k_pgs_soft launch on the 100k mixed column, from one ncu
-# capture at step ~298 of the run (dram__bytes_read.sum + dram__bytes_write.sum; the capture
-# command is in profiles/k_pgs_soft_k_narrow_k_components_mixed_column_100k.md)
-SOLVER_TRAFFIC_MIXED_100K = 114.5e6 + 24.1e6
+DEFAULT_BODIES = {"pyramids": 1_000_000, "mixed_column": 100_000, "box_grid": 1000, "voxel_pile": 20_000}
+# DRAM bytes (read + write) of one launch, from ncu captures of the same workloads; the capture
+# commands are in profiles/ (k_pgs_soft on the 100k mixed column at step ~298 of its run)
+SOLVER_TRAFFIC = {("mixed_column", 100_000): 114.5e6 + 24.1e6}
 
 
-def workload(args):
+def workload(args, n_bodies: int | None = None):
+    """The scene and its one-line description; n_bodies overrides --bodies (samples)."""
+    nb = args.bodies if n_bodies is None else n_bodies
     if args.scene == "pyramids":
-        n_pyr = max(1, args.bodies // 1000)
+        n_pyr = max(1, nb // 1000)
         sc = scenes.pyramids(n_pyramids=n_pyr, boxes_per=1000, seed=0)
         name = (f"pyramids_{n_pyr}x1000: {n_pyr} pyramids of 1000 unit boxes (base 18x18) on a 32x32 grid, "
                 f"velocity N(0, 0.01) m/s, dt=1/60, {SUBSTEPS} substeps, ")
     elif args.scene == "voxel_pile":
-        sc = scenes.voxel_pile(n_bodies=args.bodies, seed=0)
-        name = (f"voxel_pile_{args.bodies // 1000}k: {args.bodies} concave voxel bodies (L / cross / frame, "
+        sc = scenes.voxel_pile(n_bodies=nb, seed=0)
+        name = (f"voxel_pile_{nb // 1000}k: {nb} concave voxel bodies (L / cross / frame, "
                 f"0.2 m cells, random orientation) in 3 layers over a ground box, dt=1/60, {SUBSTEPS} substeps, ")
     elif args.scene == "box_grid":
         sc = scenes.box_grid(n_side=10, seed=0)
@@ -56,8 +61,8 @@ def workload(args):
         name = (f"box_grid_1000: 1000 unit boxes (10x10x10, 1.1 m spacing, jitter 0.05 m, random yaw) "
                 f"dropped on a ground box, dt=1/60, {SUBSTEPS} substeps, ")
     else:
-        sc = scenes.mixed_column(n_bodies=args.bodies, seed=0)
-        name = (f"mixed_column_{args.bodies // 1000}k: {args.bodies} bodies (60% boxes / 40% spheres) in a "
+        sc = scenes.mixed_column(n_bodies=nb, seed=0)
+        name = (f"mixed_column_{nb // 1000}k: {nb} bodies (60% boxes / 40% spheres) in a "
                 f"60x60x200 m column, 5-wall container, dt=1/60, {SUBSTEPS} substeps, ")
     if args.solver == "pgs":
         name += f"PGS_SOFT {pgs_iterations(args)} iterations ({args.schedule} schedule)"
@@ -126,7 +131,11 @@ def pgs_iterations(args) -> int:
 
 
 def timed_window(args) -> int:
-    """First timed step: centred on the run, never before the W warm-up steps."""
+    """First timed step.  Pyramids: right after the W warm-up steps (the awake settling phase,
+    where the sort, tree, colouring and solver work at full size).  Other scenes: centred on
+    the run (their piles form as they fall), never before the W warm-up steps."""
+    if args.scene == "pyramids":
+        return args.warmup
     return max(args.warmup, run_steps(args) // 2 - args.steps // 2)
 
 
@@ -184,63 +193,163 @@ def peaks() -> dict:
 
 def solver_bytes(st: dict, n: int, args) -> float:
     """Algorithmic HBM bytes of one solver launch (one substep), SoA float4 model: body
-    state 64 B, props 48 B, contact row 64 B, manifold header 32 B."""
-    M, K = st["manifold_count"], st["contact_count"]
+    state 64 B, props 48 B, contact row 64 B, manifold header 32 B.  PGS: the manifolds and
+    contacts the colour sweeps solve (those with an awake body); AVBD: all of them."""
     if args.solver == "pgs":
-        it = 10
+        M, K = st["solved_manifolds"], st["solved_contacts"]
+        it = pgs_iterations(args)
         pre = 64 * K + 4 * 32 * M + 2 * 48 * M
         sweep = 64 * K + 128 * M
         return pre + 2 * it * sweep + 128 * n
+    M, K = st["manifold_count"], st["contact_count"]
     it = 4
     sweeps = it + 12 + 3  # main iterations + post-stabilisation (cascade + plain sweeps)
     return 2 * 192 * n + sweeps * (64 * n + 2 * (32 * M + 64 * K)) + it * (32 * M + 76 * K)
 
 
-def run_reference(args, rank: int, world_size: int):
-    """Times the reference's CPU implementation of the step: the oracle (a restatement of the
-    reference's Slang passes; the reference itself needs Vulkan/Daxa and cannot run here) in
-    FP32 on all host cores."""
-    if rank != 0:
-        return
+def cpu_sample_pyramids(args) -> int:
+    return max(1, min(args.cpu_sample_pyramids, args.bodies // 1000))
+
+
+def cpu_sample(args, threads: int) -> dict:
+    """The step on the host cores: the oracle (a restatement of the reference's Slang passes;
+    the reference itself needs Vulkan/Daxa and cannot run here) in FP32 on `threads` threads,
+    over a bounded sample of the timed workload: the same steps (W untimed, then up to K timed,
+    at most --cpu-budget-s seconds of them) of a world holding the first pyramids of the scene
+    (their bodies start exactly as in the full world; pyramids 20 m apart never touch), or of
+    the whole world for the other scenes."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
     pyoracle.build()
-    sc, name = workload(args)
-    threads = os.cpu_count() or 1
+    if args.scene == "pyramids":
+        n_pyr = cpu_sample_pyramids(args)
+        sc, _ = workload(args, n_bodies=n_pyr * 1000)
+        what = f"pyramids 0..{n_pyr - 1} of the {args.bodies // 1000} ({sc['n']} bodies with the ground)"
+    else:
+        sc, _ = workload(args)
+        what = f"the full {sc['n']}-body world"
     p = pyoracle.default_params()
     for k, v in solver_fields(args).items():
         setattr(p, k, v)
     p.world_min[:] = sc["bounds"][0]
     p.world_extent[:] = sc["bounds"][1]
     o = pyoracle.Oracle(sc, double=False, threads=threads, params=p)
-    budget = args.ref_budget_s
     first = timed_window(args)
     t0 = time.time()
-    done = 0  # untimed steps: pre-roll to the timed window (bounded by the budget), then warm-up
-    while done < first and (first - done <= args.warmup or time.time() - t0 < budget):
+    done = 0
+    while done < first and (first - done <= args.warmup or time.time() - t0 < args.cpu_budget_s):
         o.step(DT, SUBSTEPS)
         done += 1
     t1 = time.time()
     steps = 0
-    while steps < args.steps:
+    while steps < args.steps and (steps == 0 or time.time() - t1 < args.cpu_budget_s):
         o.step(DT, SUBSTEPS)
         steps += 1
-        if time.time() - t1 > budget:
-            break
     el = time.time() - t1
     v = sc["n"] * steps / el
-    sample = (f"steps {done}..{done + steps - 1} of the {run_steps(args)}-step run ({steps} of the {args.steps} "
-              f"timed steps; the window starts at step {first}, fewer if the {budget:.0f} s pre-roll budget ran out) "
-              f"of the full {sc['n']}-body world, FP32 oracle, {threads} threads")
-    warm = done
+    sample = (f"steps {done}..{done + steps - 1} (the timed window starts at step {first}) of {what}, "
+              f"FP32 oracle, {threads} threads")
+    return {"value": v, "unit": "body-steps/s", "cores": threads, "kind": "port", "sample": sample,
+            "steps": steps, "first_step": done, "same_steps": done == first and steps == args.steps,
+            "ms_per_step": 1000 * el / max(steps, 1), "bodies": int(sc["n"])}
+
+
+def run_reference(args, rank: int, world_size: int):
+    """Times the reference's CPU implementation of the step on the host cores (all threads):
+    the oracle port, on a bounded sample of this bench's workload and step window."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    _, name = workload(args)
+    cb = cpu_sample(args, threads)
+    v = cb["value"]
     line = {"impl": "reference", "metric": "body-steps/s", "value": v, "unit": "body-steps/s", "n_gpus": world_size,
-            "steps": steps, "warmup": warm, "ms_per_step": 1000 * el / max(steps, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
-            "config": {"workload": name, "bodies": sc["n"], "substeps": SUBSTEPS, "dt": DT},
-            "cpu_baseline": {"value": v, "unit": "body-steps/s", "cores": threads, "kind": "port", "sample": sample},
+            "steps": cb["steps"], "warmup": cb["first_step"], "ms_per_step": cb["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene, seed 0)",
+            "config": {"workload": name, "bodies": int(workload(args)[0]["n"]), "substeps": SUBSTEPS, "dt": DT,
+                       "timed_steps": f"steps {timed_window(args)}..{timed_window(args) + args.steps - 1}"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "same_steps")},
             "e2e": {"value": v, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def make_world(bb, args, sc, local_rank: int):
+    # a voxel pair takes six manifold slots (one per face direction)
+    w = bb.World(sc["n"], pairs_per_body=64 if args.scene == "voxel_pile" else 16, device=local_rank)
+    w.add_scene(sc)
+    p = bb.default_params()
+    p.world_min[:] = sc["bounds"][0]
+    p.world_extent[:] = sc["bounds"][1]
+    w.set_params(p, **solver_fields(args))
+    return w
+
+
+def time_steps(torch, w, steps: int, flush, dev: str):
+    """Device time (ms) of each of `steps` steps: CUDA events on the world's stream, L2 flushed
+    (outside the events) before each."""
+    stream = torch.cuda.ExternalStream(w.stream, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        evs[k][0].record(stream)
+        w.step(DT, SUBSTEPS)
+        evs[k][1].record(stream)
+    w.sync()
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
+
+
+def kernel_roof(kernel: str, bytes_total: float, ms_total: float, launches: int, peak_gbs: float, traffic=None,
+                model: str = "") -> dict:
+    achieved = bytes_total / (ms_total / 1000.0) / 1e9 if ms_total > 0 else 0.0
+    return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+            "frac": achieved / peak_gbs, "traffic": traffic,
+            "algorithmic_bytes_per_launch": bytes_total / max(launches, 1),
+            "ms_per_launch": ms_total / max(launches, 1), "launches": launches, "model": model}
+
+
+def profiled_window(bb, args, sc, local_rank: int, first: int, steps: int, peak_gbs: float, traffic=None) -> dict:
+    """A second world with the same deterministic history, profiled over the timed steps:
+    per-stage CUDA-event times (a substep run stage by stage with events between) and the
+    rooflines of the solver, the sort and the refit from their own event times and the
+    algorithmic bytes of the same substeps (live counts after each step)."""
+    w = make_world(bb, args, sc, local_rank)
+    for _ in range(first):
+        w.step(DT, SUBSTEPS)
+    w.sync()
+    n = w.n
+    n_dyn = int(w.stats()["active_body_count"])
+    w.set_profiling(True)
+    solve_b = sort_b = refit_b = 0.0
+    front_runs = 0
+    for _ in range(steps):
+        w.step(DT, SUBSTEPS)
+        st = w.stats()
+        solve_b += SUBSTEPS * solver_bytes(st, n, args)
+        if st["sleeping_count"] < n_dyn:  # the front end ran (it is skipped once every body sleeps)
+            front_runs += SUBSTEPS
+    stages = w.stage_times()
+    w.set_profiling(False)
+    w.close()
+    sort_b, refit_b = 68.0 * n * front_runs, 52.0 * n * front_runs
+    subs = steps * SUBSTEPS
+    solver_name = "k_pgs_soft" if args.solver == "pgs" else "AVBD kernels"
+    roofs = {
+        "solve": kernel_roof(f"solve ({solver_name})", solve_b, stages.get("solve", 0.0), subs, peak_gbs, traffic,
+                             "PGS_SOFT: pre-step 64K + 224M, each of 2I sweeps 64K + 128M, integrate 128N bytes "
+                             "(K contacts, M manifolds solved this substep)"),
+        "sort": kernel_roof("sort (k_sort_hist + 4x k_onesweep)", sort_b, stages.get("sort", 0.0), max(front_runs, 1),
+                            peak_gbs, None, "68 B per body: histogram read 4 B + 4 passes x 16 B"),
+        "refit": kernel_roof("refit (k_refit, node records fused)", refit_b, stages.get("refit", 0.0),
+                             max(front_runs, 1), peak_gbs, None, "52 B per body: leaf boxes read 24 B, internal "
+                             "boxes written 24 B, parents 4 B"),
+    }
+    return {"stage_ms_per_substep": {k: v / subs for k, v in stages.items()}, "rooflines": roofs,
+            "front_end_substeps": front_runs}
 
 
 def run_ours(args, rank: int, world_size: int, local_rank: int):
@@ -249,6 +358,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     import beatbox as bb
 
     torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
     dist = None
     if world_size > 1:
         import datetime
@@ -257,112 +367,110 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     sc, name = workload(args)
-    fields = solver_fields(args)
-
-    def make_world():
-        # a voxel pair takes six manifold slots (one per face direction)
-        w = bb.World(sc["n"], pairs_per_body=64 if args.scene == "voxel_pile" else 16, device=local_rank)
-        w.add_scene(sc)
-        p = bb.default_params()
-        p.world_min[:] = sc["bounds"][0]
-        p.world_extent[:] = sc["bounds"][1]
-        w.set_params(p, **fields)
-        return w
-
-    # The configuration is a run of RUN_STEPS steps whose cost per step grows as the pile forms;
-    # K timed steps are centred on that run (untimed pre-roll first), so a short K still
-    # measures a representative part of it, and K >= RUN_STEPS - W times the whole run.
     first = timed_window(args)
+    pk = peaks()
+    peak_gbs = float(pk.get("hbm_gbs", 6650.0))
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
-    def roll(world):
-        for _ in range(first):
-            world.step(DT, SUBSTEPS)
-        world.sync()
-
-    w = make_world()
-    stream = torch.cuda.ExternalStream(w.stream)
-    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
-    roll(w)
-    warm_state = w.read_state()
-    warm_flags = w.read_flags()
+    w = make_world(bb, args, sc, local_rank)
+    for _ in range(first):  # the W warm-up steps (and, for the other scenes, the pre-roll)
+        w.step(DT, SUBSTEPS)
+    w.sync()
     n = w.n
     launches0 = w.launches()
     clocks = sample_clocks(local_rank)
     if dist is not None:
         dist.barrier()
-    torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        evs[k][0].record(stream)
-        w.step(DT, SUBSTEPS)
-        evs[k][1].record(stream)
-    w.sync()
-    torch.cuda.synchronize()
+    ms = time_steps(torch, w, args.steps, flush, dev)
     clk = finish_clocks(clocks)
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    total_ms = sum(ms)
     launches = w.launches() - launches0
     stats = w.stats()
-    t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
+    t = torch.tensor([total_ms], device=dev)
     if dist is not None:
         dist.barrier()
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
     value = world_size * n * args.steps / (max_ms / 1000.0)
 
-    # end to end through the public API with pinned host buffers: upload state, step, read back
-    w2 = make_world()
-    roll(w2)  # the same deterministic history: both measurements cover the same steps
+    extras = {}
+    if world_size == 1 and args.scene == "pyramids" and not args.no_extras:
+        # the same world later in its run, once every body sleeps (front end skipped, frozen
+        # pairs carried, no island coloured): steps 145..154 of the 300-step run
+        done = first + args.steps
+        for _ in range(max(0, 145 - done)):
+            w.step(DT, SUBSTEPS)
+        w.sync()
+        sms = time_steps(torch, w, 10, flush, dev)
+        extras["asleep_window"] = {"value": n * 10 / (sum(sms) / 1000.0), "unit": "body-steps/s",
+                                   "ms_per_step": sum(sms) / 10, "steps": f"steps {max(done, 145)}..{max(done, 145) + 9}",
+                                   "sleeping_count": w.stats()["sleeping_count"]}
+    w.close()
+
+    # end to end through the public API with pinned host buffers: upload state, step, read back,
+    # over the same steps (a second world with the same deterministic history)
+    w2 = make_world(bb, args, sc, local_rank)
+    for _ in range(first):
+        w2.step(DT, SUBSTEPS)
+    w2.sync()
     pin = lambda shape: torch.empty(shape, dtype=torch.float32).pin_memory().numpy()  # noqa: E731
-    host = {k: pin(v.shape) for k, v in warm_state.items()}
+    st0 = w2.read_state()
+    host = {k: pin(v.shape) for k, v in st0.items()}
     for k in host:
-        host[k][...] = w2.read_state()[k]
-    e2e_steps = args.steps  # the same steps as the device-timed run
+        host[k][...] = st0[k]
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         w2.write_state(host["pos"], host["quat"], host["vel"], host["omega"])
         w2.step(DT, SUBSTEPS)
         w2.read_state(host)
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+    w2.close()
+    e2e_t = torch.tensor([e2e_s], device=dev)
     if dist is not None:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world_size * n * e2e_steps / float(e2e_t.item())
+    e2e_value = world_size * n * args.steps / float(e2e_t.item())
     io_bytes = n * (12 + 16 + 12 + 12)
-    w2.close()
 
-    # roofline of the dominant stage: per-stage CUDA-event times over a profiled pass
-    prof_steps = max(1, min(args.steps, 20))
-    w.set_profiling(True)
-    for _ in range(prof_steps):
-        w.step(DT, SUBSTEPS)
-    w.sync()
-    stages = w.stage_times()
-    w.set_profiling(False)
-    st_now = w.stats()
-    launches_per_stage = prof_steps * SUBSTEPS
-    dom = max(stages, key=stages.get) if stages else "solve"
-    pk = peaks()
-    peak_gbs = float(pk.get("hbm_gbs", 6650.0))
-    solve_ms = stages.get("solve", 0.0) / launches_per_stage
-    sb = solver_bytes(st_now, n, args)
-    achieved = sb / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else 0.0
-    roof = {"kernel": "solve (k_pgs_soft)" if args.solver == "pgs" else "solve (AVBD kernels)", "bound": "hbm",
-            "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
-            "peak_source": "measured" if not pk.get("fallback") else "fallback",
-            "traffic": (SOLVER_TRAFFIC_MIXED_100K if args.solver == "pgs" and args.scene == "mixed_column"
-                        and args.bodies == N_BODIES else None),
-            "algorithmic_bytes_per_launch": sb, "ms_per_launch": solve_ms,
-            "stage_ms_per_substep": {k: v / launches_per_stage for k, v in stages.items()}, "dominant_stage": dom}
+    # per-stage split and per-kernel rooflines on the timed steps
+    prof = profiled_window(bb, args, sc, local_rank, first, args.steps, peak_gbs,
+                           SOLVER_TRAFFIC.get((args.scene, args.bodies)) if args.solver == "pgs" else None)
+    stage = prof["stage_ms_per_substep"]
+    dom = max(stage, key=stage.get) if stage else "solve"
+    roof = dict(prof["rooflines"]["solve"])
+    roof.update({"peak_source": "measured" if not pk.get("fallback") else "fallback",
+                 "stage_ms_per_substep": stage, "dominant_stage": dom})
 
-    sort_roof = sort_roofline(local_rank, peak_gbs) if rank == 0 else None
+    if world_size == 1 and args.scene == "pyramids" and not args.no_extras:
+        # config 2 beside it: the 100k mixed column at the centre of its 600-step run
+        class A:  # noqa: N801
+            pass
+
+        a2 = A()
+        a2.__dict__.update(vars(args))
+        a2.scene, a2.bodies = "mixed_column", DEFAULT_BODIES["mixed_column"]
+        sc2, name2 = workload(a2)
+        f2 = timed_window(a2)
+        wc = make_world(bb, a2, sc2, local_rank)
+        for _ in range(f2):
+            wc.step(DT, SUBSTEPS)
+        wc.sync()
+        ms2 = time_steps(torch, wc, args.steps, flush, dev)
+        wc.close()
+        p2 = profiled_window(bb, a2, sc2, local_rank, f2, args.steps, peak_gbs,
+                             SOLVER_TRAFFIC.get((a2.scene, a2.bodies)))
+        extras["mixed_column_100k"] = {"workload": name2, "value": sc2["n"] * args.steps / (sum(ms2) / 1000.0),
+                                       "unit": "body-steps/s", "ms_per_step": sum(ms2) / args.steps,
+                                       "timed_steps": f"steps {f2}..{f2 + args.steps - 1} of the 600-step run",
+                                       "stage_ms_per_substep": p2["stage_ms_per_substep"],
+                                       "rooflines": p2["rooflines"]}
+
+    sort_roof = sort_roofline(local_rank, peak_gbs) if rank == 0 and not args.no_extras else None
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, sc, warm_state, warm_flags)
+        cpu = cpu_sample(args, os.cpu_count() or 1)
     if rank == 0:
         line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world_size,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
@@ -371,46 +479,18 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                 "config": {"workload": name, "bodies": n, "substeps": SUBSTEPS, "dt": DT,
                            "parallelism": f"replicas x{world_size}", "l2": "flushed before every timed step",
                            "timed_steps": f"steps {first}..{first + args.steps - 1} of the {run_steps(args)}-step run "
-                                          f"(the last {args.warmup} untimed steps before them are the warm-up)"},
+                                          f"(after {first} untimed steps from rest, the last {args.warmup} of them "
+                                          f"the warm-up)"},
                 "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": io_bytes,
-                        "d2h_bytes_per_step": io_bytes, "steps": e2e_steps,
-                        "what": "bb_write_state + bb_step + bb_read_state with pinned host buffers"},
-                "gpu_launches": launches, "roofline": roof, "sort_roofline": sort_roof, "cpu_baseline": cpu,
-                "clocks": clk,
-                "step_stats": stats}
+                        "d2h_bytes_per_step": io_bytes, "steps": args.steps,
+                        "what": "bb_write_state + bb_step + bb_read_state with pinned host buffers, same steps"},
+                "gpu_launches": launches, "roofline": roof, "rooflines": prof["rooflines"],
+                "sort_roofline": sort_roof, "cpu_baseline": cpu, "clocks": clk,
+                "ms_per_timed_step": [round(x, 3) for x in ms], "step_stats": stats, **extras}
         print(json.dumps(line), flush=True)
-    w.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-
-
-def cpu_baseline(args, sc, state, flags) -> dict:
-    """Oracle (FP32, all host threads) continued from the GPU's post-warm-up state for about
-    15 s of CPU time: a bounded sample of the timed workload."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
-
-    pyoracle.build()
-    sc2 = dict(sc)
-    sc2["pos"], sc2["quat"], sc2["vel"], sc2["omega"] = state["pos"], state["quat"], state["vel"], state["omega"]
-    sc2["flags"] = flags
-    threads = os.cpu_count() or 1
-    p = pyoracle.default_params()
-    for k, v in solver_fields(args).items():
-        setattr(p, k, v)
-    p.world_min[:] = sc["bounds"][0]
-    p.world_extent[:] = sc["bounds"][1]
-    o = pyoracle.Oracle(sc2, double=False, threads=threads, params=p)
-    t0 = time.time()
-    steps = 0
-    while steps < args.steps and (steps == 0 or time.time() - t0 < 15.0):
-        o.step(DT, SUBSTEPS)
-        steps += 1
-    el = time.time() - t0
-    return {"value": sc["n"] * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{steps} steps of the {sc['n']}-body world continued from the GPU state after "
-                      f"{args.warmup} warm-up steps (cold warm start), FP32 oracle"}
 
 
 def batched_scenes(n_worlds: int):
@@ -638,14 +718,14 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="pgs", choices=["pgs", "avbd"])
-    ap.add_argument("--bodies", type=int, default=N_BODIES)
-    ap.add_argument("--scene", default="mixed_column", choices=["mixed_column", "pyramids", "box_grid", "voxel_pile"],
-                    help="mixed_column: the 100k mixed column (default); pyramids: bodies/1000 box pyramids; "
-                         "box_grid: the 1000-box grid; voxel_pile: concave voxel bodies")
+    ap.add_argument("--bodies", type=int, default=None, help="bodies of the scene (default: its configuration's)")
+    ap.add_argument("--scene", default="pyramids", choices=["pyramids", "mixed_column", "box_grid", "voxel_pile"],
+                    help="pyramids: bodies/1000 box pyramids (default, 1M boxes); mixed_column: the 100k mixed "
+                         "column; box_grid: the 1000-box grid; voxel_pile: concave voxel bodies")
     ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "sort"],
@@ -658,9 +738,14 @@ def main():
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--plain-stride", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-budget-s", type=float, default=150.0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the asleep window, config 2 and the sort alone")
+    ap.add_argument("--cpu-sample-pyramids", type=int, default=16,
+                    help="pyramids in the CPU baseline's sample world (pyramids scene)")
+    ap.add_argument("--cpu-budget-s", type=float, default=60.0, help="bound on the CPU baseline's timed steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.bodies is None:
+        args.bodies = DEFAULT_BODIES[args.scene]
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -193,6 +193,8 @@ typedef struct bb_step_stats {
   uint32_t error_flags;           /* BB_ERRF_* bits raised on the device */
   uint32_t pair_capacity;
   uint32_t substeps_run;          /* substeps run since the world was created */
+  uint32_t solved_manifolds;      /* last substep's colour sweeps: manifolds with an awake body */
+  uint32_t solved_contacts;       /* and their contacts (0 under AVBD and the per-island path) */
 } bb_step_stats;
 
 /* device error bits (bb_step_stats.error_flags) */
@@ -344,6 +346,17 @@ bb_status bb_debug_collide(void* world, uint32_t stage);
  * receives the element count; at most max_bytes are written. */
 bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_bytes, uint64_t* count);
 
+/* Bounded device waits, for tests of the failure path.  polls: how many polls a grid-barrier
+ * wait of this world's persistent kernels makes before it gives up (0 = the default, 2^22),
+ * raising BB_ERRF_SPIN_LIMIT so that bb_sync returns BB_E_DEVICE_LIMIT.  abandon_block = 1
+ * makes the last block of the PGS_SOFT colour-sweep kernel leave before its first grid barrier
+ * (when the kernel runs on more than one block), so the other blocks wait for a block that
+ * never arrives until their bounded waits give up; the step's results are then undefined, and
+ * bb_world_clear (which also clears the error bits) makes the world usable again.  No
+ * counterpart in the reference: its bounded loops (avbd.slang:559, collision_detection.slang:921,
+ * LBVH.slang:226,278) stop without reporting. */
+bb_status bb_debug_wait_limit(void* world, uint32_t polls, uint32_t abandon_block);
+
 /* CUDA stream the world runs on (cudaStream_t). */
 void* bb_world_stream(void* world);
 /* Per-stage device timing (ms, summed over substeps since the last reset) for profiling.
@@ -378,10 +391,20 @@ bb_status bb_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, 
  * array's address up; make it before any stream capture.  Every call clears the part of the
  * scratch that must start at zero on `stream` itself.  Calls on one device share the scratch:
  * calls that overlap in time (different streams without ordering, several host threads) race
- * and give wrong results.  No counterpart in the reference. */
+ * and give wrong results.  The looked-up address is kept with the id of the CUDA context; after
+ * cudaDeviceReset (a new context) the next call looks it up again.  No counterpart in the
+ * reference. */
 #define BB_SORT_STATIC_MAX_KEYS 262144u
 bb_status bb_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                      uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
+
+/* BB_OK from either sort means its work was launched, not that it finished: a look-back wait
+ * that reached its bound (BB_ERRF_SPIN_LIMIT) leaves the output undefined.  This waits for
+ * `stream` and returns in *error_flags the device error bits (BB_ERRF_*) of the last sort on the
+ * current device: static_scratch = 1 for bb_radix_sort_pairs_static, 0 for bb_radix_sort_pairs.
+ * 0 means that sort ran to the end.  Allocates nothing.  No counterpart in the reference (its
+ * sort passes clamp silently, LBVH.slang:34-152). */
+bb_status bb_radix_sort_error_flags(uint32_t static_scratch, void* stream, uint32_t* error_flags);
 
 /* Pick the launch geometry and colour-sweep schedule of this world by timing candidates
  * (coordinate descent over bb_solver_params.schedule, broad_threads, narrow_blocks_per_sm,

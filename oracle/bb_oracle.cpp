@@ -237,6 +237,19 @@ void orc_set_carry_frozen(void* hp, int on) {
   else h->f->carry_frozen = on != 0;
 }
 
+// The next substep's narrow phase uses these n manifolds (bb_manifold_info, pair order) and
+// their contacts (bb_contact_info, MAX_CONTACTS per manifold) as its geometry (no voxel keys).
+void orc_inject_manifolds(void* hp, const bb_manifold_info* m, const bb_contact_info* c, uint32_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  auto set = [&](auto& w) {
+    w.inj_m.assign(m, m + n);
+    w.inj_c.assign(c, c + size_t(n) * MAX_CONTACTS);
+    w.inj = true;
+  };
+  if (h->dbl) set(*h->d);
+  else set(*h->f);
+}
+
 void orc_skip_warm_starting_once(void* hp) {
   Handle* h = static_cast<Handle*>(hp);
   if (h->dbl) h->d->skip_warm_once = true;

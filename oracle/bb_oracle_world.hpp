@@ -26,6 +26,13 @@ template <class R> class World {
   std::vector<uint8_t> frozen;
   bool carry_frozen = true;
   bool skip_warm_once = false;
+  // Test hook: the next narrow phase takes these manifolds' geometry (identity, key, normal,
+  // contact points, depths, features) instead of computing it, so two implementations whose
+  // near-degenerate contact decisions could differ solve the same contact set.  Warm-start
+  // matching, anchors and tangent bases are still the oracle's own.
+  std::vector<bb_manifold_info> inj_m;
+  std::vector<bb_contact_info> inj_c;
+  bool inj = false;
 
   // products of the last substep (debug readback)
   std::vector<uint32_t> morton;       // code of body order[i]
@@ -260,7 +267,54 @@ template <class R> class World {
 
   // ------------------------------------------------------------------------------------
   // Narrow phase + warm start (collision_detection.slang:1514-1755).
+  void narrow_from_injected() {
+    const bool warm = (p.flags & BB_SIM_WARM_STARTING) && !skip_warm_once;
+    manifolds.clear();
+    for (size_t k = 0; k < inj_m.size(); ++k) {
+      const bb_manifold_info& mi = inj_m[k];
+      Manifold<R> m;
+      m.a = mi.body_a;
+      m.b = mi.body_b;
+      m.sa = rank[m.a];
+      m.sb = rank[m.b];
+      m.key = mi.key;
+      m.cc = mi.contact_count;
+      m.normal = Vec3<R>(R(mi.normal[0]), R(mi.normal[1]), R(mi.normal[2]));
+      for (int c = 0; c < m.cc; ++c) {
+        const bb_contact_info& ci = inj_c[k * MAX_CONTACTS + c];
+        Contact<R> ct;
+        ct.pos = Vec3<R>(R(ci.position[0]), R(ci.position[1]), R(ci.position[2]));
+        ct.pen = R(ci.penetration);
+        ct.fp.in_ref = ci.feature & 0xFF;
+        ct.fp.out_ref = (ci.feature >> 8) & 0xFF;
+        ct.fp.in_inc = (ci.feature >> 16) & 0xFF;
+        ct.fp.out_inc = ci.feature >> 24;
+        m.c[c] = ct;
+      }
+      m.anchor_a = bodies[m.a].pos;
+      m.anchor_b = bodies[m.b].pos;
+      m.error = 0x7FFFFFFF;
+      compute_basis(m);
+      if (warm) {
+        uint64_t key = (uint64_t(std::min(m.a, m.b)) << 32) | std::max(m.a, m.b);
+        auto it = prev_pair_index.find(key);
+        if (it != prev_pair_index.end()) {
+          const Manifold<R>& old = prev_manifolds[it->second];
+          update_from_old(m, old, old.a != m.a);
+        }
+      }
+      manifolds.push_back(m);
+    }
+    frozen.assign(n(), 0);
+    for (size_t i = 0; i < n(); ++i) frozen[i] = awake(bodies[i]) ? 0 : 1;
+    inj = false;
+  }
+
   void narrow_phase() {
+    if (inj) {
+      narrow_from_injected();
+      return;
+    }
     const size_t P = pair_a.size();
     // up to six manifolds per pair (voxel pairs, one per face direction); one otherwise
     std::vector<std::array<Manifold<R>, 6>> per(P);

@@ -41,7 +41,7 @@ class StepStats(ctypes.Structure):
         "graph_color_count", "graph_color_overflow", "graph_color_violations", "avbd_color_count",
         "avbd_violations", "sleeping_count", "fresh_contacts", "stick_count")] + [
         ("max_penetration", ctypes.c_float), ("error_flags", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
-        ("substeps_run", ctypes.c_uint32)]
+        ("substeps_run", ctypes.c_uint32), ("solved_manifolds", ctypes.c_uint32), ("solved_contacts", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -77,6 +77,7 @@ def lib():
         L.orc_step.argtypes = [P, ctypes.c_float, ctypes.c_uint32]
         L.orc_collide.argtypes = [P, ctypes.c_uint32]
         L.orc_skip_warm_starting_once.argtypes = [P]
+        L.orc_inject_manifolds.argtypes = [P, P, P, ctypes.c_uint32]
         L.orc_set_carry_frozen.argtypes = [P, ctypes.c_int]
         L.orc_read_state.argtypes = [P, P, P, P, P, P]
         L.orc_read_stats.argtypes = [P, ctypes.POINTER(StepStats)]
@@ -153,6 +154,15 @@ class Oracle:
 
     def skip_warm_starting_once(self):
         lib().orc_skip_warm_starting_once(self.h)
+
+    def inject_manifolds(self, manifolds: np.ndarray, contacts: np.ndarray):
+        """The next substep's narrow phase takes this geometry (records in the library's
+        bb_manifold_info / bb_contact_info layouts, 8 contacts per manifold) instead of its own."""
+        m = np.ascontiguousarray(manifolds)
+        c = np.ascontiguousarray(contacts)
+        assert c.size == 8 * m.size
+        self._keep["inj"] = (m, c)
+        lib().orc_inject_manifolds(self.h, _ptr(m), _ptr(c), int(m.size))
 
     def state(self):
         pos = np.zeros((self.n, 3))

@@ -60,6 +60,12 @@ def test_ctypes_layout_matches_header(struct, cls):
     assert _c_sizeof(struct) == ctypes.sizeof(cls)
 
 
+def test_oracle_stats_struct_matches_header():
+    import pyoracle
+
+    assert _c_sizeof("bb_step_stats") == ctypes.sizeof(pyoracle.StepStats)
+
+
 def test_record_dtypes_match_header():
     assert _c_sizeof("bb_manifold_info") == beatbox.MANIFOLD_DTYPE.itemsize
     assert _c_sizeof("bb_contact_info") == beatbox.CONTACT_DTYPE.itemsize

@@ -25,6 +25,10 @@ def sort_on_gpu(fn, keys, vals, bits):
     code = fn(dptr(kin), dptr(vin), dptr(kout), dptr(vout), len(keys), bits, None)
     assert code == bb.OK, bb.load_library().bb_last_error_string()
     torch.cuda.synchronize()
+    flags = ctypes.c_uint32(0xFFFFFFFF)
+    static = 1 if fn is bb.load_library().bb_radix_sort_pairs_static else 0
+    assert bb.load_library().bb_radix_sort_error_flags(static, None, ctypes.byref(flags)) == bb.OK
+    assert flags.value == 0  # the look-back waits all ended
     return kout.cpu().numpy().view(np.uint32), vout.cpu().numpy().view(np.uint32), kin, vin
 
 

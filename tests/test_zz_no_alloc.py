@@ -54,6 +54,9 @@ def test_static_sort_matches_allocating_sort_twice_in_a_row():
     torch.cuda.synchronize()
     free_after = torch.cuda.mem_get_info()[0]
     assert free_after == free_before
+    flags = ctypes.c_uint32(0xFFFFFFFF)
+    assert lib.bb_radix_sort_error_flags(1, stream, ctypes.byref(flags)) == bb.OK
+    assert flags.value == 0  # the second static sort's look-back waits all ended
     for n, bits, k, v, kin, vin, outs in bufs:
         assert lib.bb_radix_sort_pairs(dptr(kin), dptr(vin), dptr(outs[2]), dptr(outs[3]), n, bits,
                                        stream) == bb.OK, lib.bb_last_error_string()
