@@ -305,7 +305,10 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
         uint32_t lo = min(la, lb), hi = max(la, lb);
         const uint32_t pid = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
         d.gc_pid[m] = pid;
-        d.gc_rec[m] = make_uint4(b.x, b.y, pid, (da ? 0u : 1u) | (db ? 0u : 2u));
+        // bit 2: neither body awake (both asleep or static); the sweeps have nothing to do there
+        const bool idle = !((fa & BB_BODY_DYNAMIC) && !(fa & BB_BODY_SLEEPING)) &&
+                          !((fb & BB_BODY_DYNAMIC) && !(fb & BB_BODY_SLEEPING));
+        d.gc_rec[m] = make_uint4(b.x, b.y, pid, (da ? 0u : 1u) | (db ? 0u : 2u) | (idle ? 4u : 0u));
       }
       d.gc_color[m] = colour ? BB_UNCOLORED : BB_RESTING;
     }
@@ -390,11 +393,20 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
     else grid_sync(c, sync, ep);
   }
   if (local) grid_sync(c, sync, ep);  // block 0's rounds are done before anyone reads the colours
+  // Keys: colour, 32 = overflow, 33 = not swept.  Under the colour-barrier schedule a coloured
+  // manifold whose two bodies are both asleep or static is also keyed 33: its sweep items would
+  // do nothing (both bodies are frozen this substep), and leaving them out of the colour lists
+  // saves the sweeps from walking them.  Its colour (gc_color) is kept.  The dataflow schedule
+  // ranks every manifold on a body's list, so there every coloured manifold stays in its colour.
+  const bool drop_idle = p.schedule == BB_SCHEDULE_COLOUR_BARRIER;
   uint32_t over = 0;
-  for (uint32_t m = tid; m < M; m += stride) {  // keys: colour, 32 = overflow, 33 = resting
+  for (uint32_t m = tid; m < M; m += stride) {
     uint32_t col = d.gc_color[m];
     if (col == BB_UNCOLORED) ++over;
-    d.bucket_keys[0][m] = col == BB_UNCOLORED ? BB_MAX_COLORS : col == BB_RESTING ? BB_MAX_COLORS + 1 : col;
+    uint32_t key = col == BB_UNCOLORED ? BB_MAX_COLORS : col == BB_RESTING ? BB_MAX_COLORS + 1 : col;
+    if (drop_idle && key <= BB_MAX_COLORS && (reinterpret_cast<const uint32_t*>(d.gc_rec + m)[3] & 4u))
+      key = BB_MAX_COLORS + 1;
+    d.bucket_keys[0][m] = key;
     d.bucket_vals[0][m] = m;
   }
   if (over) atomicAdd(&c->gc_overflow, over);

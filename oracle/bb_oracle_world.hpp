@@ -305,16 +305,36 @@ template <class R> class World {
       }
       manifolds.push_back(m);
     }
-    frozen.assign(n(), 0);
-    for (size_t i = 0; i < n(); ++i) frozen[i] = awake(bodies[i]) ? 0 : 1;
     inj = false;
   }
 
   void narrow_phase() {
-    if (inj) {
-      narrow_from_injected();
-      return;
+    if (inj) narrow_from_injected();
+    else narrow_manifolds();
+    frozen.assign(n(), 0);
+    for (size_t i = 0; i < n(); ++i) frozen[i] = awake(bodies[i]) ? 0 : 1;
+    skip_warm_once = false;
+    // per-body manifold lists in ascending manifold order (body_link_manifold :881-905)
+    lists.assign(n(), {});
+    uint32_t fresh = 0;
+    float maxpen = 0;
+    uint32_t contacts = 0;
+    for (uint32_t m = 0; m < manifolds.size(); ++m) {
+      lists[manifolds[m].a].push_back(m);
+      lists[manifolds[m].b].push_back(m);
+      for (int c = 0; c < manifolds[m].cc; ++c) {
+        if (manifolds[m].c[c].warm == 0) ++fresh;
+        maxpen = std::max(maxpen, float(-manifolds[m].c[c].pen));
+        ++contacts;
+      }
     }
+    stats.manifold_count = uint32_t(manifolds.size());
+    stats.contact_count = contacts;
+    stats.fresh_contacts = fresh;
+    stats.max_penetration = maxpen;
+  }
+
+  void narrow_manifolds() {
     const size_t P = pair_a.size();
     // up to six manifolds per pair (voxel pairs, one per face direction); one otherwise
     std::vector<std::array<Manifold<R>, 6>> per(P);
@@ -380,27 +400,6 @@ template <class R> class World {
     for (size_t k = 0; k < P; ++k)
       for (uint32_t code = 0; code < 6; ++code)
         if (have[k] & (1u << code)) manifolds.push_back(per[k][code]);
-    frozen.assign(n(), 0);
-    for (size_t i = 0; i < n(); ++i) frozen[i] = awake(bodies[i]) ? 0 : 1;
-    skip_warm_once = false;
-    // per-body manifold lists in ascending manifold order (body_link_manifold :881-905)
-    lists.assign(n(), {});
-    uint32_t fresh = 0;
-    float maxpen = 0;
-    uint32_t contacts = 0;
-    for (uint32_t m = 0; m < manifolds.size(); ++m) {
-      lists[manifolds[m].a].push_back(m);
-      lists[manifolds[m].b].push_back(m);
-      for (int c = 0; c < manifolds[m].cc; ++c) {
-        if (manifolds[m].c[c].warm == 0) ++fresh;
-        maxpen = std::max(maxpen, float(-manifolds[m].c[c].pen));
-        ++contacts;
-      }
-    }
-    stats.manifold_count = uint32_t(manifolds.size());
-    stats.contact_count = contacts;
-    stats.fresh_contacts = fresh;
-    stats.max_penetration = maxpen;
   }
 
   // ------------------------------------------------------------------------------------

@@ -210,3 +210,62 @@ def test_autotune_keeps_results_bit_identical():
     a, b = w.read_state(), ref.read_state()
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+def resting_boxes(x0):
+    """Four boxes resting on a ground box from the start: they fall asleep after the quiet time."""
+    sb = scenes.SceneBuilder()
+    sb.add_static_box([x0, -50, 0], [50, 50, 50])
+    pos = [[x0 - 2.4 + 1.6 * k, 0.499, 0.0] for k in range(4)]
+    sb.add(pos, [[0, 0, 0, 1.0]] * 4, [[0.5] * 3] * 4, scenes.SHAPE_BOX, scenes.BODY_DYNAMIC | scenes.BODY_GRAVITY,
+           1000.0)
+    return sb.build()
+
+
+def test_batched_worlds_asleep_keep_their_front_end_outputs():
+    """Once every body of every world sleeps, the batched front end (two-digit world-id sort,
+    world-bounded traversal) is skipped and its outputs stand: they must equal a fresh batch's
+    on the same poses, and a pose written into one world must bring the front end back."""
+    scs = [resting_boxes(0.0), resting_boxes(200.0), resting_boxes(400.0)]
+    p = params(bb.SOLVER_PGS_SOFT, iterations=8, relax_iterations=8)
+    total = sum(int(s["n"]) for s in scs)
+
+    boxes = [scene_bounds(sc, margin=60.0) for sc in scs]  # the same Morton box for both batches
+
+    def batch(worlds):
+        w = bb.World(total)
+        for sc, box in zip(worlds, boxes):
+            w.add_world(sc, *box)
+        w.set_params(p)
+        return w
+
+    w = batch(scs)
+    for _ in range(40):
+        w.step(DT, 4)
+    w.sync()
+    assert w.stats()["sleeping_count"] == 12
+    keys, ids, pairs = w.debug_read("sorted_keys"), w.debug_read("sorted_ids"), w.debug_read("pairs")
+    n_pairs = w.stats()["pair_count"]
+    st = w.read_state()
+    rest, first = [], 0
+    for sc in scs:
+        n = int(sc["n"])
+        s2 = dict(sc)
+        s2["pos"], s2["quat"] = st["pos"][first:first + n].copy(), st["quat"][first:first + n].copy()
+        s2["vel"], s2["omega"] = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32)
+        rest.append(s2)
+        first += n
+    fresh = batch(rest)
+    fresh.debug_collide(2)
+    assert np.array_equal(fresh.debug_read("sorted_keys"), keys)
+    assert np.array_equal(fresh.debug_read("sorted_ids"), ids)
+    assert n_pairs == fresh.stats()["pair_count"] > 0
+    assert np.array_equal(fresh.debug_read("pairs")[: 2 * n_pairs], pairs[: 2 * n_pairs])
+    # lift one box of the second world far above its ground: its ground pair must go
+    pos = st["pos"].copy()
+    pos[int(scs[0]["n"]) + 1, 1] += 20.0
+    w.write_state(pos=pos)
+    w.step(DT, 1)
+    w.sync()
+    assert w.stats()["pair_count"] == n_pairs - 1
+    assert w.stats()["error_flags"] == 0

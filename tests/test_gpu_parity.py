@@ -209,19 +209,78 @@ def energy_stats(state, sc):
                 mom=float(np.abs((m[:, None] * v).sum(0)).sum()), ymean=float(y.mean()))
 
 
+def quat_matrix(q):
+    x, y, z, w = (q[:, k] for k in range(4))
+    return np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], 1),
+                     np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], 1),
+                     np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], 1)], 1)
+
+
+def dynamics(state, sc):
+    """Total linear momentum P, angular momentum L about the dynamic bodies' centre of mass,
+    and energy E = kinetic (linear + rotational) + potential (g = 9.81 m/s^2)."""
+    dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+    m = sc["mass"][dyn].astype(np.float64)
+    x = state["pos"][dyn].astype(np.float64)
+    v = state["vel"][dyn].astype(np.float64)
+    w = state["omega"][dyn].astype(np.float64)
+    ii = sc["inv_inertia"][dyn].astype(np.float64)
+    inertia = np.where(ii > 0, 1.0 / np.where(ii > 0, ii, 1.0), 0.0)  # body-frame diagonal
+    R = quat_matrix(state["quat"][dyn].astype(np.float64))
+    wb = np.einsum("nji,nj->ni", R, w)  # angular velocity in the body frame
+    com = (m[:, None] * x).sum(0) / m.sum()
+    P = (m[:, None] * v).sum(0)
+    L = (np.cross(x - com, m[:, None] * v) + np.einsum("nij,nj->ni", R, inertia * wb)).sum(0)
+    E = 0.5 * (m * (v ** 2).sum(1)).sum() + 0.5 * (inertia * wb ** 2).sum() + (m * 9.81 * x[:, 1]).sum()
+    return P, L, E
+
+
+def mean_penetration(manifolds, contacts):
+    mask = (np.arange(8)[None, :] < manifolds["contact_count"][:, None]).ravel()
+    pen = contacts["penetration"][mask]
+    pen = pen[pen < 0]
+    return float(pen.mean()) if len(pen) else 0.0
+
+
 def test_300_step_statistics(oracle_lib):
     """1,000-box grid, PGS 8 iterations, 4 substeps, 300 steps: GPU (FP32) vs oracle (FP64).
-    The trajectories are chaotic, so aggregate quantities are compared:
-    mean height within 2 cm, potential energy within 1%, max penetration within 1 cm,
-    sleeping fraction within 0.1, final kinetic energy both small."""
+    The trajectories are chaotic, so statistics are compared, every step, within bands set
+    several times wider than the oracle's own FP32 build lands from its FP64 build:
+      * total linear momentum within 2% of M g (1 s) (M: the pile's mass);
+      * angular momentum about the pile's centre of mass within 2% of M g (1 s) R0 (R0: the
+        grid's RMS radius about that centre at the start);
+      * energy (kinetic + potential) within 5% of the energy the oracle's run dissipates;
+      * mean penetration of the penetrating contacts, averaged over steps 100..299, within 1 mm;
+    and at the end: mean height within 2 cm, potential energy within 1%, max penetration within
+    1 cm, sleeping count within 100, kinetic energy small on both."""
     sc = scenes.box_grid()
     p = params_for(oracle_lib, sc, solver=1, quirks=0, iterations=8, relax_iterations=8)
     w = bb.world_from_scene(sc, params=p)
     o = oracle_for(oracle_lib, sc, p)
-    for _ in range(300):
+    dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
+    M = float(sc["mass"][dyn].sum())
+    x0 = sc["pos"][dyn].astype(np.float64)
+    R0 = float(np.sqrt(((x0 - x0.mean(0)) ** 2).sum(1).mean()))
+    E0 = dynamics(o.state(), sc)[2]
+    dP, dL, dE, pen_g, pen_r = [], [], [], [], []
+    for k in range(300):
         w.step(DT, 4)
         o.step(DT, 4)
+        Pg, Lg, Eg = dynamics(w.read_state(), sc)
+        Pr, Lr, Er = dynamics(o.state(), sc)
+        dP.append(np.abs(Pg - Pr).max())
+        dL.append(np.abs(Lg - Lr).max())
+        dE.append(abs(Eg - Er))
+        if k >= 100:
+            pen_g.append(mean_penetration(w.debug_read("manifolds"), w.debug_read("contacts")))
+            pen_r.append(mean_penetration(oread(o, 8, None), oread(o, 9, None)))
     w.sync()
+    dissipated = E0 - Er
+    assert dissipated > 0
+    assert max(dP) <= 0.02 * M * 9.81, (max(dP), M * 9.81)
+    assert max(dL) <= 0.02 * M * 9.81 * R0, (max(dL), M * 9.81 * R0)
+    assert max(dE) <= 0.05 * dissipated, (max(dE), dissipated)
+    assert abs(np.mean(pen_g) - np.mean(pen_r)) <= 1e-3, (np.mean(pen_g), np.mean(pen_r))
     g, r = energy_stats(w.read_state(), sc), energy_stats(o.state(), sc)
     gs, rs = w.stats(), o.stats()
     assert abs(g["ymean"] - r["ymean"]) < 0.02
