@@ -35,6 +35,7 @@ QUIRK_GRAVITY_IMPULSE, QUIRK_SAT_FRAME, QUIRK_INERTIA_TRANSPOSE = 1, 2, 4
 QUIRKS_REFERENCE, QUIRKS_PHYSICAL = 7, 0
 BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
 SCHEDULE_DATAFLOW, SCHEDULE_COLOUR_BARRIER = 0, 1
+PGS_PIPE_AUTO, PGS_PIPE_STAGED, PGS_PIPE_STREAM, PGS_PIPE_HELD = 0, 1, 2, 3  # bb_solver_params.pgs_stage_next
 SORT_STATIC_MAX_KEYS = 262144
 EDGE_COLOR_OVERFLOW = 0xFFFFFFFF
 EDGE_COLOR_RESTING = 0xFFFFFFFE  # the manifold's island has no awake body: not coloured, not solved
@@ -114,7 +115,8 @@ class Request(ctypes.Structure):
 
 class RequestStatus(ctypes.Structure):
     _fields_ = [("done", ctypes.c_uint32), ("result", ctypes.c_int32), ("submit_s", ctypes.c_double),
-                ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double)]
+                ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double), ("error_flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -159,6 +161,8 @@ _SIG = {
     "bb_add_world": (ctypes.c_int32, [_P, ctypes.POINTER(BatchWorldDesc), ctypes.POINTER(BodyDesc), _U32,
                                       ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "bb_world_count": (_U32, [_P]),
+    "bb_world_pause": (ctypes.c_int32, [_P, _U32, _U32]),
+    "bb_world_refill": (ctypes.c_int32, [_P, _U32, ctypes.POINTER(BatchWorldDesc), ctypes.POINTER(BodyDesc), _U32]),
     "bb_set_material": (ctypes.c_int32, [_P, _U32, _U32, ctypes.c_float, ctypes.c_float]),
     "bb_set_solver_params": (ctypes.c_int32, [_P, ctypes.POINTER(SolverParams)]),
     "bb_get_solver_params": (ctypes.c_int32, [_P, ctypes.POINTER(SolverParams)]),
@@ -187,6 +191,9 @@ _SIG = {
     "bb_read_contact_points": (ctypes.c_int32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
     "bb_world_device_bytes": (ctypes.c_uint64, [_P]),
     "bb_world_clear": (ctypes.c_int32, [_P]),
+    "bb_world_save_state": (ctypes.c_int32, [_P, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "bb_world_set_auto_regrow": (ctypes.c_int32, [_P, _U32]),
+    "bb_world_load_state": (ctypes.c_int32, [_P, _P, ctypes.c_uint64]),
     "bb_world_bytes_for": (ctypes.c_uint64, [_U32, _U32]),
     "bb_server_create": (ctypes.c_int32, [ctypes.POINTER(ServerDesc), ctypes.POINTER(ctypes.c_void_p)]),
     "bb_server_destroy": (ctypes.c_int32, [_P]),
@@ -342,6 +349,18 @@ class World:
         _check(self.L.bb_add_world(self.h, ctypes.byref(wd), descs, n, ctypes.byref(wi), ctypes.byref(first)))
         return wi.value, first.value
 
+    def pause_world(self, index: int, paused: bool = True):
+        """Pause (or resume) world `index` of a batch: while paused it is left exactly as it is."""
+        _check(self.L.bb_world_pause(self.h, index, 1 if paused else 0))
+
+    def refill_world(self, index: int, scene: dict, world_min, world_extent, inertia_mode: int = INERTIA_EXPLICIT):
+        """Replace the bodies of world `index`'s slot by a new scene (at most the slot's size)."""
+        descs, n = self._scene_descs(scene, inertia_mode)
+        wd = BatchWorldDesc()
+        wd.world_min[:] = [float(v) for v in world_min]
+        wd.world_extent[:] = [float(v) for v in world_extent]
+        _check(self.L.bb_world_refill(self.h, index, ctypes.byref(wd), descs, n))
+
     @property
     def n_worlds(self) -> int:
         return int(self.L.bb_world_count(self.h))
@@ -446,6 +465,23 @@ class World:
         """Bound of the persistent kernels' grid-barrier waits (0 = default); abandon_block makes
         the colour-sweep kernel's last block leave so the other blocks' waits run out."""
         _check(self.L.bb_debug_wait_limit(self.h, polls, 1 if abandon_block else 0))
+
+    def set_auto_regrow(self, max_pairs_per_body: int):
+        """Rerun steps that overflowed the pair capacity with more capacity (0 = off)."""
+        _check(self.L.bb_world_set_auto_regrow(self.h, max_pairs_per_body))
+
+    def save_state(self) -> np.ndarray:
+        """Image of the world's state (uint8): poses, velocities, persistent contacts, lists..."""
+        n = ctypes.c_uint64()
+        _check(self.L.bb_world_save_state(self.h, None, 0, ctypes.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        _check(self.L.bb_world_save_state(self.h, _ptr(buf), buf.nbytes, ctypes.byref(n)))
+        return buf
+
+    def load_state(self, image: np.ndarray):
+        """Restore an image from save_state into this world (same capacity, same bodies)."""
+        buf = np.ascontiguousarray(image, np.uint8)
+        _check(self.L.bb_world_load_state(self.h, _ptr(buf), buf.nbytes))
 
     def clear(self):
         """Remove every body and shape (device buffers kept); clears the device error bits."""
@@ -599,13 +635,13 @@ class Server:
         st = RequestStatus()
         _check(self.L.bb_server_poll(self.h, ticket, ctypes.byref(st)))
         return dict(done=bool(st.done), result=st.result, submit_s=st.submit_s, start_s=st.start_s,
-                    finish_s=st.finish_s)
+                    finish_s=st.finish_s, error_flags=st.error_flags)
 
     def wait(self, ticket: int) -> dict:
         st = RequestStatus()
         _check(self.L.bb_server_wait(self.h, ticket, ctypes.byref(st)))
         return dict(done=bool(st.done), result=st.result, submit_s=st.submit_s, start_s=st.start_s,
-                    finish_s=st.finish_s)
+                    finish_s=st.finish_s, error_flags=st.error_flags)
 
     def read_state(self, world: int, n: int) -> dict:
         out = dict(pos=np.empty((n, 3), np.float32), quat=np.empty((n, 4), np.float32),

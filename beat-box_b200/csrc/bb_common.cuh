@@ -25,6 +25,7 @@
 #define BB_SLEEP_VETO 0x80000000u
 #define BB_SLEEP_MASK 0x7FFFFFFFu
 #define BB_SPIN_LIMIT (1u << 22)
+#define BB_BODY_PAUSE_AWAKE (1u << 6)  // a paused body that was awake when its world was paused
 #define BB_BVH_STACK 64
 
 #define BB_KEY_SPHERE_SPHERE 20

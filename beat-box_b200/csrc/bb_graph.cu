@@ -157,7 +157,7 @@ __global__ void k_sleep_reduce(const DevState d, Params p, uint32_t n, int cur) 
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t f = d.flags[i];
-  if (!(f & BB_BODY_DYNAMIC)) return;
+  if (!(f & BB_BODY_DYNAMIC) || (f & BB_BODY_PAUSED)) return;  // a paused world keeps its timers
   if (!(p.flags & BB_SIM_SLEEPING_ENABLED)) {
     d.sleep[i] = 0;
     d.flags[i] = f & ~BB_BODY_SLEEPING;
@@ -181,6 +181,7 @@ __global__ void k_sleep_veto(const DevState d, Params p, int cur) {
     uint32_t slot = d.man_slot[cur][m];
     uint2 b = d.m_bodies[cur][slot];
     uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+    if ((fa | fb) & BB_BODY_PAUSED) continue;
     bool ad = fa & BB_BODY_DYNAMIC, bd = fb & BB_BODY_DYNAMIC;
     bool a_loud = ad && (d.sleep[b.x] & BB_SLEEP_MASK) < p.sleep_steps;
     bool b_loud = bd && (d.sleep[b.y] & BB_SLEEP_MASK) < p.sleep_steps;
@@ -204,7 +205,7 @@ __global__ void k_sleep_apply(const DevState d, uint32_t n, Params p) {
   if (i == 0) d.ctr->sleep_ran = 1u;  // with awake_after: the next substep may skip its front end
   if (i >= n) return;
   uint32_t f = d.flags[i];
-  if (!(f & BB_BODY_DYNAMIC)) return;
+  if (!(f & BB_BODY_DYNAMIC) || (f & BB_BODY_PAUSED)) return;
   uint32_t t = d.sleep[i];
   bool vetoed = (t & BB_SLEEP_VETO) != 0;
   bool quiet = (t & BB_SLEEP_MASK) >= p.sleep_steps;
@@ -258,6 +259,7 @@ __device__ __forceinline__ uint32_t gc_priority(uint32_t pid, uint32_t round) {
 // into one record up front, so a round touches rec -> body masks -> owner words only; the
 // grid barrier is the arrival-counter kind (counter 0 of the substep).
 #define BB_GC_THREADS 1024
+#define GC_UNROLL 3  // list entries a thread takes per trip of a round
 __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
   DevCounters* c = d.ctr;
   const uint32_t M = c->manifold_count;
@@ -341,53 +343,88 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
     const uint32_t rtid = local ? threadIdx.x : tid, rstride = local ? blockDim.x : stride;
     if (rtid == 0) c->gc_list_n[(r + 1) & 1] = 0;  // the list this round fills (last read two rounds ago)
     const unsigned long long tag = (unsigned long long)(epoch + r) << 32;
-    for (uint32_t i = rtid; i < nL; i += rstride) {
-      const uint32_t m = L ? L[i] : i;
-      const uint4 rec = d.gc_rec[m];
-      const bool sa = rec.w & 1u, sb = rec.w & 2u;
-      uint32_t avail = ~((sa ? 0u : d.gc_mask[rec.x]) | (sb ? 0u : d.gc_mask[rec.y]));
-      uint32_t col = avail == 0u ? BB_MAX_COLORS : uint32_t(__ffs(avail) - 1);
-      d.gc_choice[m] = col;
-      if (col >= BB_MAX_COLORS) continue;
-      unsigned long long v = tag | gc_priority(rec.z, r);
-      if (!sa) atomicMax(&d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col], v);
-      if (!sb) atomicMax(&d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col], v);
+    // A thread takes GC_UNROLL list entries per trip and issues each stage's loads (list entry,
+    // record, body masks) for all of them before using any: the rounds are chains of dependent
+    // loads, and this keeps several chains in flight per thread.  A round's outcome depends only
+    // on its set of manifolds, not on the order in which they are taken.
+    for (uint32_t i0 = rtid; i0 < nL; i0 += GC_UNROLL * rstride) {
+      uint32_t m[GC_UNROLL];
+      uint4 rec[GC_UNROLL];
+      uint32_t ma[GC_UNROLL], mb[GC_UNROLL];
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        const uint32_t i = i0 + uint32_t(u) * rstride;
+        m[u] = i < nL ? (L ? L[i] : i) : BB_NONE;
+      }
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) rec[u] = m[u] != BB_NONE ? d.gc_rec[m[u]] : make_uint4(0, 0, 0, 3u);
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        ma[u] = (rec[u].w & 1u) ? 0u : d.gc_mask[rec[u].x];
+        mb[u] = (rec[u].w & 2u) ? 0u : d.gc_mask[rec[u].y];
+      }
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        if (m[u] == BB_NONE) continue;
+        const bool sa = rec[u].w & 1u, sb = rec[u].w & 2u;
+        const uint32_t avail = ~(ma[u] | mb[u]);
+        const uint32_t col = avail == 0u ? BB_MAX_COLORS : uint32_t(__ffs(avail) - 1);
+        d.gc_choice[m[u]] = col;
+        if (col >= BB_MAX_COLORS) continue;
+        const unsigned long long v = tag | gc_priority(rec[u].z, r);
+        if (!sa) atomicMax(&d.gc_owner[size_t(rec[u].x) * BB_MAX_COLORS + col], v);
+        if (!sb) atomicMax(&d.gc_owner[size_t(rec[u].y) * BB_MAX_COLORS + col], v);
+      }
     }
     if (local) __syncthreads();
     else grid_sync(c, sync, ep);
     uint32_t* next = d.gc_list[(r + 1) & 1];
-    for (uint32_t base = local ? (threadIdx.x & ~31u) : warp0; base < nL; base += rstride) {  // warp-uniform trips
-      const uint32_t i = base + lane;
-      bool keep = false;
-      uint32_t m = 0, used = 0;  // used: colour + 1 of a committed manifold
-      if (i < nL) {
-        m = L ? L[i] : i;
-        const uint32_t col = d.gc_choice[m];
-        keep = true;
-        if (col < BB_MAX_COLORS) {
-          const uint4 rec = d.gc_rec[m];
-          const bool sa = rec.w & 1u, sb = rec.w & 2u;
-          unsigned long long v = tag | gc_priority(rec.z, r);
-          bool wa = sa || d.gc_owner[size_t(rec.x) * BB_MAX_COLORS + col] == v;
-          bool wb = sb || d.gc_owner[size_t(rec.y) * BB_MAX_COLORS + col] == v;
+    for (uint32_t base = local ? (threadIdx.x & ~31u) : warp0; base < nL; base += GC_UNROLL * rstride) {  // warp-uniform trips
+      uint32_t m[GC_UNROLL], col[GC_UNROLL];
+      uint4 rec[GC_UNROLL];
+      unsigned long long oa[GC_UNROLL], ob[GC_UNROLL];
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        const uint32_t i = base + uint32_t(u) * rstride + lane;
+        m[u] = i < nL ? (L ? L[i] : i) : BB_NONE;
+      }
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        col[u] = m[u] != BB_NONE ? d.gc_choice[m[u]] : BB_MAX_COLORS;
+        rec[u] = m[u] != BB_NONE ? d.gc_rec[m[u]] : make_uint4(0, 0, 0, 3u);
+      }
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        const bool live = col[u] < BB_MAX_COLORS;
+        oa[u] = live && !(rec[u].w & 1u) ? d.gc_owner[size_t(rec[u].x) * BB_MAX_COLORS + col[u]] : 0ull;
+        ob[u] = live && !(rec[u].w & 2u) ? d.gc_owner[size_t(rec[u].y) * BB_MAX_COLORS + col[u]] : 0ull;
+      }
+      uint32_t used = 0;  // colour + 1 of a committed manifold
+#pragma unroll
+      for (int u = 0; u < GC_UNROLL; ++u) {
+        bool keep = m[u] != BB_NONE;
+        if (keep && col[u] < BB_MAX_COLORS) {
+          const bool sa = rec[u].w & 1u, sb = rec[u].w & 2u;
+          const unsigned long long v = tag | gc_priority(rec[u].z, r);
+          const bool wa = sa || oa[u] == v, wb = sb || ob[u] == v;
           if (wa && wb) {
-            d.gc_color[m] = col;
-            if (!sa) atomicOr(&d.gc_mask[rec.x], 1u << col);
-            if (!sb) atomicOr(&d.gc_mask[rec.y], 1u << col);
-            used = col + 1u;
+            d.gc_color[m[u]] = col[u];
+            if (!sa) atomicOr(&d.gc_mask[rec[u].x], 1u << col[u]);
+            if (!sb) atomicOr(&d.gc_mask[rec[u].y], 1u << col[u]);
+            used = max(used, col[u] + 1u);
             keep = false;
           }
+        }
+        const unsigned mask = __ballot_sync(0xFFFFFFFFu, keep);
+        if (mask) {
+          uint32_t off = 0;
+          if (lane == 0) off = atomicAdd(&c->gc_list_n[(r + 1) & 1], uint32_t(__popc(mask)));
+          off = __shfl_sync(0xFFFFFFFFu, off, 0);
+          if (keep) next[off + __popc(mask & ((1u << lane) - 1u))] = m[u];
         }
       }
       used = __reduce_max_sync(0xFFFFFFFFu, used);  // one colour-count update per warp
       if (lane == 0 && used) atomicMax(&c->gc_colors, used);
-      const unsigned mask = __ballot_sync(0xFFFFFFFFu, keep);
-      if (mask) {
-        uint32_t off = 0;
-        if (lane == 0) off = atomicAdd(&c->gc_list_n[(r + 1) & 1], uint32_t(__popc(mask)));
-        off = __shfl_sync(0xFFFFFFFFu, off, 0);
-        if (keep) next[off + __popc(mask & ((1u << lane) - 1u))] = m;
-      }
     }
     if (local) __syncthreads();
     else grid_sync(c, sync, ep);

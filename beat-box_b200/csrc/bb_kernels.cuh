@@ -52,9 +52,14 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
 void bb_solve_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                       const StepScratch& sc, int sms);
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
-                       const StepScratch& sc, int coop_blocks, int sms);
+                       const StepScratch& sc, int coop_blocks, int coop_stream, int sms);
 void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,
                    int sms, int cur, int coop_blocks);
+
+// serving loop helpers (bb_world.cu): one batch slot's state, the device error word
+bb_status bb_world_read_range(void* world, uint32_t first, uint32_t count, float* position, float* rotation,
+                              float* velocity, float* omega, uint32_t* flags);
+const uint32_t* bb_world_error_word(void* world);
 
 // thread-local last-error message behind bb_last_error_string (bb_world.cu)
 bb_status bb_fail(bb_status code, const char* msg);
@@ -69,6 +74,7 @@ void bb_sort_carve(char* base, uint32_t n, int passes, DevCounters** ctr, uint32
 // co-resident block counts of the persistent cooperative kernels
 int bb_edge_coloring_blocks(int sms);
 int bb_pgs_soft_blocks(int sms);
+int bb_pgs_stream_blocks(int sms);
 int bb_avbd_blocks(int sms);
 
 // occupancy helpers (bb_world.cu)

@@ -439,7 +439,9 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
         const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
         const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
         const bool first = !vox || (d.slot_pair[k] & 7u) == 0u;  // a voxel pair is listed once
-        if (warm && !np_awake(fa) && !np_awake(fb) && d.frozen[ida] && d.frozen[idb]) kind = first ? 3 : -1;
+        // a paused world's pairs are always carried (exactly: see k_narrow_carry)
+        if ((fa | fb) & BB_BODY_PAUSED) kind = first ? 3 : -1;
+        else if (warm && !np_awake(fa) && !np_awake(fb) && d.frozen[ida] && d.frozen[idb]) kind = first ? 3 : -1;
         else if (vox) kind = first ? 2 : -1;
         else kind = (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) ? 0 : 1;
       }
@@ -496,12 +498,37 @@ __device__ __forceinline__ void carry_contact(const DevState& d, int prv, int cu
   d.c_anc_b[cur][ni] = make_float4(ab.x, ab.y, ab.z, 0.f);
 }
 
+// A paused world's manifold is carried as it is, every field (warm-start counts, trend, anchors,
+// stick data), so the world resumes exactly where it stopped.
+__device__ __forceinline__ void carry_exact_contact(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni) {
+  d.c_pos[cur][ni] = d.c_pos[prv][oi];
+  d.c_lam[cur][ni] = d.c_lam[prv][oi];
+  d.c_kt[cur][ni] = d.c_kt[prv][oi];
+  d.c_anc_a[cur][ni] = d.c_anc_a[prv][oi];
+  d.c_anc_b[cur][ni] = d.c_anc_b[prv][oi];
+}
+
 // Lane q (0..3) of the quad that carries a pair: the header (q = 0) and contacts q, q + 4.  The
 // quad's four lanes read each contact array over 64 contiguous bytes.
 __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t os, uint32_t dst, uint32_t ida,
-                                           uint32_t idb, uint32_t q) {
+                                           uint32_t idb, uint32_t q, bool exact) {
   const int prv = cur ^ 1;
   const int2 kc = d.m_keycc[prv][os];
+  if (exact) {
+    if (q == 0) {
+      d.m_bodies[cur][dst] = d.m_bodies[prv][os];
+      d.m_keycc[cur][dst] = kc;
+      d.m_normal[cur][dst] = d.m_normal[prv][os];
+      d.m_t0[cur][dst] = d.m_t0[prv][os];
+      d.m_t1[cur][dst] = d.m_t1[prv][os];
+      d.m_anchor_a[cur][dst] = d.m_anchor_a[prv][os];
+      d.m_anchor_b[cur][dst] = d.m_anchor_b[prv][os];
+      d.hit[dst] = 1;
+    }
+    for (uint32_t c = q; c < uint32_t(kc.y); c += 4u)
+      carry_exact_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c);
+    return;
+  }
   if (q == 0) {
     const float4 n4 = d.m_normal[prv][os], t04 = d.m_t0[prv][os], t14 = d.m_t1[prv][os];
     const float4 pa = d.pos[ida], pb = d.pos[idb];
@@ -540,11 +567,15 @@ __global__ void k_narrow_carry(const DevState d, int cur) {
       ob = d.m_bodies[prv][s];
     }
     const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
-    if (okc.x >= 0 && okc.x < 90 && ob.x == ida && ob.y == idb) {
-      carry_part(d, cur, s, s, ida, idb, q);
+    const uint32_t fa = d.flags[ida];
+    // A paused world's manifold is kept in the body order it was stored in: the first paused
+    // substep sorts with the poses its world's last step integrated, which can swap a pair.
+    const bool exact = ((fa | d.flags[idb]) & BB_BODY_PAUSED) != 0;
+    if (okc.x >= 0 && okc.x < 90 &&
+        ((ob.x == ida && ob.y == idb) || (exact && ob.x == idb && ob.y == ida))) {
+      carry_part(d, cur, s, s, ida, idb, q, exact);
       continue;
     }
-    const uint32_t fa = d.flags[ida];
     const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
     const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
     const uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb, other = x == ida ? idb : ida;
@@ -553,20 +584,21 @@ __global__ void k_narrow_carry(const DevState d, int cur) {
     for (uint32_t e = s0; e < s1; ++e) {
       if (d.csr_partner[prv][e] != other) continue;
       const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
-      if (d.m_bodies[prv][os].x != ida) continue;  // same body order only
+      if (!exact && d.m_bodies[prv][os].x != ida) continue;  // same body order only
       const int key = d.m_keycc[prv][os].x;
       if (vox) {
         if (key < 90 || key > 95) continue;
-        carry_part(d, cur, os, s + uint32_t(key - 90), ida, idb, q);
+        carry_part(d, cur, os, s + uint32_t(key - 90), ida, idb, q, exact);
         any = true;
       } else {
-        carry_part(d, cur, os, s, ida, idb, q);
+        carry_part(d, cur, os, s, ida, idb, q, exact);
         any = true;
         break;
       }
     }
-    if (any || q != 0) continue;
-    // no manifold last substep: compute the pair with the others
+    // no manifold last substep: compute the pair with the others (a paused pair had none when
+    // its world stopped, and keeps none)
+    if (any || q != 0 || exact) continue;
     if (vox) {
       d.vox_list[atomicAdd(&d.ctr->np_counts[2], 1u)] = s;
     } else if (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) {

@@ -45,7 +45,10 @@ struct Shape {
 thread_local size_t t_alloc_bytes = 0;  // device bytes allocated by dalloc on this thread
 thread_local bool t_count_only = false;  // dalloc only counts (bb_world_bytes_for)
 
-template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& err, cudaStream_t stream) {
+// device arrays of a world with their sizes (a saved state is an image of all of them)
+typedef std::vector<std::pair<void*, size_t>> Owned;
+
+template <class T> T* dalloc(size_t n, Owned& owned, cudaError_t& err, cudaStream_t stream) {
   void* p = nullptr;
   if (n == 0) n = 1;
   t_alloc_bytes += n * sizeof(T);
@@ -56,7 +59,7 @@ template <class T> T* dalloc(size_t n, std::vector<void*>& owned, cudaError_t& e
     return nullptr;
   }
   cudaMemsetAsync(p, 0, n * sizeof(T), stream);
-  owned.push_back(p);
+  owned.emplace_back(p, n * sizeof(T));
   return static_cast<T*>(p);
 }
 
@@ -106,6 +109,24 @@ __global__ void k_pack_state(const DevState d, uint32_t n, float* st) {
   V[3 * i] = v.x; V[3 * i + 1] = v.y; V[3 * i + 2] = v.z;
   W[3 * i] = w.x; W[3 * i + 1] = w.y; W[3 * i + 2] = w.z;
 }
+// bodies [o, o + n) into the staging buffer (the k_pack_state layout for n bodies), and their
+// flags as the caller sees them: a paused body reads asleep as it was when its world stopped
+__global__ void k_pack_range(const DevState d, uint32_t o, uint32_t n, float* st, uint32_t* flags) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t b = o + i;
+  float4 p = d.pos[b], q = d.rot[b], v = d.vel[b], w = d.omega[b];
+  float* P = st + 4 * size_t(n);
+  float* V = st + 7 * size_t(n);
+  float* W = st + 10 * size_t(n);
+  P[3 * i] = p.x; P[3 * i + 1] = p.y; P[3 * i + 2] = p.z;
+  reinterpret_cast<float4*>(st)[i] = q;
+  V[3 * i] = v.x; V[3 * i + 1] = v.y; V[3 * i + 2] = v.z;
+  W[3 * i] = w.x; W[3 * i + 1] = w.y; W[3 * i + 2] = w.z;
+  uint32_t f = d.flags[b];
+  if (f & BB_BODY_PAUSED) f = (f & BB_BODY_PAUSE_AWAKE) ? (f & ~BB_BODY_SLEEPING) : f;
+  flags[i] = f & (BB_BODY_DYNAMIC | BB_BODY_GRAVITY | BB_BODY_SLEEPING);
+}
 __global__ void k_unpack_state(const DevState d, uint32_t n, const float* st, uint32_t mask) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -126,6 +147,45 @@ __global__ void k_extend_contacts(const DevState d, uint32_t o, uint32_t count) 
   d.frozen[o + i] = 0;
   if (i == 0) d.ctr->front_valid = 0;
   for (int k = 0; k < 2; ++k) d.csr_start[k][o + 1 + i] = d.csr_start[k][o];
+}
+
+// Pause (on = 1) or resume the dynamic bodies [o, o + count): a paused body is flagged asleep
+// and remembers whether it was awake, so resuming gives back its flags exactly.
+__global__ void k_pause(const DevState d, uint32_t o, uint32_t count, uint32_t on) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) d.ctr->front_valid = 0;
+  if (i >= count) return;
+  const uint32_t f = d.flags[o + i];
+  if (!(f & BB_BODY_DYNAMIC)) return;
+  if (on && !(f & BB_BODY_PAUSED)) {
+    d.flags[o + i] = f | BB_BODY_PAUSED | BB_BODY_SLEEPING | ((f & BB_BODY_SLEEPING) ? 0u : BB_BODY_PAUSE_AWAKE);
+  } else if (!on && (f & BB_BODY_PAUSED)) {
+    uint32_t g = f & ~(BB_BODY_PAUSED | BB_BODY_PAUSE_AWAKE);
+    if (f & BB_BODY_PAUSE_AWAKE) g &= ~BB_BODY_SLEEPING;
+    d.flags[o + i] = g;
+  }
+}
+
+// Bodies [o, o + count) were replaced (a refilled batch slot): the manifolds of both buffers
+// that involve them are dropped from the warm-start lookups (per-body list entries and the
+// manifold's bodies), they start unfrozen, and their sorted order restarts as the identity, as
+// for a world just added.
+__global__ void k_refill_contacts(const DevState d, uint32_t o, uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) d.ctr->front_valid = 0;
+  if (i >= count) return;
+  const uint32_t id = o + i;
+  d.vals[0][id] = id;
+  d.frozen[id] = 0;
+  for (int k = 0; k < 2; ++k) {
+    const uint32_t s0 = d.csr_start[k][id], s1 = d.csr_start[k][id + 1];
+    for (uint32_t e = s0; e < s1; ++e) {
+      const uint32_t slot = d.man_slot[k][d.csr_list[k][e]];
+      d.m_bodies[k][slot] = make_uint2(BB_NONE, BB_NONE);
+      d.m_keycc[k][slot] = make_int2(-1, 0);
+      d.csr_partner[k][e] = BB_NONE;
+    }
+  }
 }
 
 // Render feed: per body the affine transform [R | t] (3 x 4, row-major: the layout of a ray
@@ -210,15 +270,28 @@ struct bb_world_impl {
   uint32_t max_world_bodies() const { return d.n_worlds > 1 ? max_world_n : n; }
   std::vector<Shape> shapes;
   std::vector<float> restitution;
+  // batched worlds: first body id, body count (the slot's capacity) and dynamic bodies of each
+  std::vector<uint32_t> wfirst, wcount, wdyn;
+  uint32_t park_shape = 0xFFFFFFFFu;  // tiny box that parks a refilled slot's unused bodies
+  // capacity regrow (bb_world_set_auto_regrow): a device snapshot of every array before the first
+  // step since the last bb_sync, the steps issued since, and the host fields the steps change
+  uint32_t ppb = 16, regrow_max_ppb = 0, regrows = 0;
+  void* shadow = nullptr;
+  size_t shadow_cap = 0;
+  std::vector<size_t> shadow_sizes;
+  std::vector<std::pair<float, uint32_t>> step_log;
+  bool snapped = false;
+  int snap_parity = 0, snap_last_cur = 0;
+  bool snap_ran_any = false, snap_skip_warm = false;
   bb_solver_params params;
   DevState d = {};
   StepScratch sc = {};
-  std::vector<void*> owned;
+  Owned owned;
   int parity = 0;    // manifold buffer of the last committed substep
   int last_cur = 0;  // manifold buffer the last (partial or full) substep wrote
   bool skip_warm_once = false;
   bool ran_any = false;
-  int coop_edge = 0, coop_pgs = 0, coop_avbd = 0, coop_cc = 0;
+  int coop_edge = 0, coop_pgs = 0, coop_pgs_stream = 0, coop_avbd = 0, coop_cc = 0;
   size_t scratch_bytes = 0;
   void* scratch_base = nullptr;
   size_t dev_bytes = 0;  // device memory held by this world
@@ -244,9 +317,10 @@ struct bb_world_impl {
   ~bb_world_impl() {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
-    for (void* p : owned) cudaFree(p);
+    for (auto& o : owned) cudaFree(o.first);
     if (vox_buf) cudaFree(vox_buf);
     if (slot_buf) cudaFree(slot_buf);
+    if (shadow) cudaFree(shadow);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 
@@ -315,7 +389,7 @@ struct bb_world_impl {
     for (int k = 0; k < 2; ++k) { d.a_bucket_keys[k] = u32(N); d.a_bucket_vals[k] = u32(N); }
     d.a_bucket_start = u32(64 * BB_MAX_COLORS + 2);
     d.ctr = dalloc<DevCounters>(1, owned, err, stream);
-    d.staging = dalloc<float>(13 * N + 4, owned, err, stream);
+    d.staging = dalloc<float>(14 * N + 4, owned, err, stream);  // 13 floats of state + flags per body
     xforms = dalloc<float>(12 * N, owned, err, stream);
     d.pair_capacity = cap_p;
     d.body_capacity = cap_n;
@@ -359,6 +433,85 @@ struct bb_world_impl {
     cudaStreamSynchronize(stream);
   }
 
+  // device copy of every array (and the host fields a step changes), taken on the world's stream
+  bb_status snapshot() {
+    size_t total = 0;
+    for (auto& o : owned) total += o.second;
+    if (shadow_cap < total) {
+      if (shadow) cudaFree(shadow);
+      shadow = nullptr;
+      shadow_cap = 0;
+      cudaError_t e = cudaMalloc(&shadow, total);
+      if (e != cudaSuccess) return fail(BB_E_CUDA, std::string("auto-regrow snapshot: ") + cudaGetErrorString(e));
+      shadow_cap = total;
+    }
+    shadow_sizes.clear();
+    size_t off = 0;
+    for (auto& o : owned) {
+      cudaMemcpyAsync(static_cast<char*>(shadow) + off, o.first, o.second, cudaMemcpyDeviceToDevice, stream);
+      shadow_sizes.push_back(o.second);
+      off += o.second;
+    }
+    snap_parity = parity;
+    snap_last_cur = last_cur;
+    snap_ran_any = ran_any;
+    snap_skip_warm = skip_warm_once;
+    snapped = true;
+    step_log.clear();
+    return BB_OK;
+  }
+  void forget_snapshot() {
+    snapped = false;
+    step_log.clear();
+  }
+
+  // Pair capacity raised to new_ppb pairs per body: every array reallocated, the snapshot copied
+  // back into it (pair-, slot- and contact-indexed arrays keep their indices, so each array takes
+  // the snapshot's bytes up to the smaller size), host fields back to the snapshot's.
+  bb_status regrow(uint32_t new_ppb) {
+    CU(cudaStreamSynchronize(stream));
+    const DevState keep = d;
+    for (auto& o : owned) cudaFree(o.first);
+    owned.clear();
+    ppb = new_ppb;
+    cap_p = uint32_t(std::min<uint64_t>(uint64_t(ppb) * cap_n + 1024, 0x3FFFFFFFull));
+    t_alloc_bytes = 0;
+    bb_status st = allocate();
+    if (st != BB_OK) return st;
+    dev_bytes = t_alloc_bytes;
+    d.n_worlds = keep.n_worlds;
+    d.vox = keep.vox;
+    d.vox_occ = keep.vox_occ;
+    d.vox_surf = keep.vox_surf;
+    d.vox_on = keep.vox_on;
+    d.full_inertia = keep.full_inertia;
+    if (slot_buf) {
+      cudaFree(slot_buf);
+      slot_buf = nullptr;
+      CU(cudaMalloc(&slot_buf, 16ull * cap_p));
+      uint32_t* sb = static_cast<uint32_t*>(slot_buf);
+      d.slot_cnt = sb;
+      d.slot_off = sb + cap_p;
+      d.slot_pair = sb + 2ull * cap_p;
+      d.vox_list = sb + 3ull * cap_p;
+      dev_bytes += 16ull * cap_p;
+    }
+    if (owned.size() != shadow_sizes.size()) return fail(BB_E_CUDA, "auto-regrow: array layout changed");
+    size_t off = 0;
+    for (size_t k = 0; k < owned.size(); ++k) {
+      CU(cudaMemcpyAsync(owned[k].first, static_cast<char*>(shadow) + off, std::min(owned[k].second, shadow_sizes[k]),
+                         cudaMemcpyDeviceToDevice, stream));
+      off += shadow_sizes[k];
+    }
+    parity = snap_parity;
+    last_cur = snap_last_cur;
+    ran_any = snap_ran_any;
+    skip_warm_once = snap_skip_warm;
+    invalidate_graphs();
+    ++regrows;
+    return BB_OK;
+  }
+
   void invalidate_graphs() {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
@@ -381,7 +534,7 @@ struct bb_world_impl {
     if (coloured || params.solver == BB_SOLVER_AVBD) bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
     if (params.solver == BB_SOLVER_AVBD) bb_solve_avbd(stream, d, params, n, h, sc, sms, cur, coop_avbd);
     else if (!coloured) bb_solve_islands(stream, d, params, n, h, cur, sc, sms);
-    else bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, sms);
+    else bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, coop_pgs_stream, sms);
     if (commit) parity = cur;
   }
 };
@@ -389,6 +542,24 @@ struct bb_world_impl {
 using World = bb_world_impl;
 
 static World* W(void* w) { return static_cast<World*>(w); }
+
+namespace {
+struct StateHeader {
+  uint32_t magic, version;
+  uint32_t cap_n, cap_p, n, n_dyn, n_worlds, vox_on, full_inertia;
+  int32_t parity, last_cur;
+  uint32_t ran_any, skip_warm_once, arrays;
+  uint64_t slot_bytes, total;
+  bb_solver_params params;
+};
+constexpr uint32_t kStateMagic = 0x31534242u;  // "BBS1"
+uint64_t state_bytes(const World* w) {
+  uint64_t t = sizeof(StateHeader) + 8ull * w->owned.size();
+  for (auto& o : w->owned) t += o.second;
+  if (w->slot_buf) t += 16ull * w->cap_p;
+  return t;
+}
+}  // namespace
 
 extern "C" {
 
@@ -458,6 +629,7 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   }
   w->cap_n = desc->max_bodies;
   uint32_t ppb = desc->pairs_per_body ? desc->pairs_per_body : 16;
+  w->ppb = ppb;
   w->cap_p = uint32_t(std::min<uint64_t>(uint64_t(ppb) * w->cap_n + 1024, 0x3FFFFFFFull));
   bb_default_solver_params(&w->params);
   t_alloc_bytes = 0;
@@ -476,6 +648,7 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   };
   w->coop_edge = fit(bb_edge_coloring_blocks(w->sms), w->cap_n, 1024);
   w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), w->cap_n / 2, 256);
+  w->coop_pgs_stream = fit(bb_pgs_stream_blocks(w->sms), w->cap_n / 2, 256);
   w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n / 2, 512);
   w->coop_cc = fit(bb_components_blocks(w->sms), w->cap_n, 512);
   cudaError_t e = cudaStreamSynchronize(w->stream);  // the zero fills (no device-wide wait)
@@ -521,6 +694,10 @@ bb_status bb_world_clear(void* world) {
   w->max_world_n = 0;
   w->shapes.clear();
   w->restitution.clear();
+  w->wfirst.clear();
+  w->wcount.clear();
+  w->wdyn.clear();
+  w->park_shape = 0xFFFFFFFFu;
   w->vox_table.clear();
   w->vox_occ.clear();
   w->vox_surf.clear();
@@ -531,6 +708,7 @@ bb_status bb_world_clear(void* world) {
   w->last_cur = 0;
   w->skip_warm_once = false;
   w->ran_any = false;
+  w->forget_snapshot();
   w->invalidate_graphs();
   uint32_t nn[2] = {0, 0};
   CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
@@ -640,14 +818,26 @@ bb_status bb_add_voxel_shape(void* world, uint32_t nx, uint32_t ny, uint32_t nz,
   return BB_OK;
 }
 
-static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id,
-                                 bool keep_contacts = false) {
-  if (!w || (!bodies && count)) return fail(BB_E_INVALID, "bb_add_bodies: bad arguments");
-  if (uint64_t(w->n) + count > w->cap_n) return fail(BB_E_CAPACITY, "bb_add_bodies: max_bodies exceeded");
-  std::vector<float4> pos(count), rot(count), vel(count), om(count), shp(count), ii(count), io(count);
-  std::vector<uint32_t> fl(count), zero(count, 0);
+// Bodies converted to the device layout (SoA float4 rows), ready to upload at some offset.
+struct BodyRows {
+  std::vector<float4> pos, rot, vel, om, shp, ii, io;
+  std::vector<uint32_t> fl;
+  std::vector<float> restitution;
   bool any_off = false;
   uint32_t ndyn = 0;
+  void resize(uint32_t count) {
+    for (auto* v : {&pos, &rot, &vel, &om, &shp, &ii, &io}) v->assign(count, make_float4(0.f, 0.f, 0.f, 0.f));
+    fl.assign(count, 0u);
+    restitution.assign(count, 0.f);
+  }
+};
+
+static bb_status pack_bodies(World* w, const bb_body_desc* bodies, uint32_t count, BodyRows& r) {
+  r.resize(count);
+  std::vector<float4>&pos = r.pos, &rot = r.rot, &vel = r.vel, &om = r.om, &shp = r.shp, &ii = r.ii, &io = r.io;
+  std::vector<uint32_t>& fl = r.fl;
+  bool& any_off = r.any_off;
+  uint32_t& ndyn = r.ndyn;
   for (uint32_t i = 0; i < count; ++i) {
     const bb_body_desc& b = bodies[i];
     if (b.shape >= w->shapes.size()) return fail(BB_E_INVALID, "bb_add_bodies: unknown shape handle");
@@ -702,9 +892,18 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
     if (inv_o[0] != 0.f || inv_o[1] != 0.f || inv_o[2] != 0.f) any_off = true;
     fl[i] = b.flags & (BB_BODY_DYNAMIC | BB_BODY_GRAVITY | BB_BODY_SLEEPING);
     if (dyn) ++ndyn;
-    w->restitution.push_back(b.restitution);
+    r.restitution[i] = b.restitution;
   }
-  const uint32_t o = w->n;
+  return BB_OK;
+}
+
+// rows of `r` into body ids [o, o + count) on the world's stream (sleep timers start at 0);
+// waits for the copies, since the rows are host memory that dies with the caller
+static bb_status upload_bodies(World* w, uint32_t o, const BodyRows& r) {
+  const uint32_t count = uint32_t(r.fl.size());
+  const std::vector<uint32_t> zero(count, 0u);
+  const std::vector<float4>&pos = r.pos, &rot = r.rot, &vel = r.vel, &om = r.om, &shp = r.shp, &ii = r.ii, &io = r.io;
+  const std::vector<uint32_t>& fl = r.fl;
   cudaStreamSynchronize(w->stream);
   CU(cudaMemcpyAsync(w->d.pos + o, pos.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.rot + o, rot.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
@@ -714,9 +913,25 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
   CU(cudaMemcpyAsync(w->d.shape + o, shp.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.iinv + o, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.iinv_off + o, io.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  if (any_off) w->d.full_inertia = 1;
+  if (r.any_off) w->d.full_inertia = 1;
   CU(cudaMemcpyAsync(w->d.flags + o, fl.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.sleep + o, zero.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  return BB_OK;
+}
+
+static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id,
+                                 bool keep_contacts = false) {
+  if (!w || (!bodies && count)) return fail(BB_E_INVALID, "bb_add_bodies: bad arguments");
+  if (uint64_t(w->n) + count > w->cap_n) return fail(BB_E_CAPACITY, "bb_add_bodies: max_bodies exceeded");
+  BodyRows r;
+  bb_status st = pack_bodies(w, bodies, count, r);
+  if (st != BB_OK) return st;
+  const uint32_t o = w->n;
+  st = upload_bodies(w, o, r);
+  if (st != BB_OK) return st;
+  w->restitution.insert(w->restitution.end(), r.restitution.begin(), r.restitution.end());
+  const uint32_t ndyn = r.ndyn;
   w->n += count;
   w->n_dyn += ndyn;
   if (out_first_id) *out_first_id = o;
@@ -733,6 +948,7 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
 
 bb_status bb_add_bodies(void* world, const bb_body_desc* bodies, uint32_t count, uint32_t* out_first_id) {
   World* w = W(world);
+  if (w) w->forget_snapshot();
   if (w && w->d.n_worlds > 0) return fail(BB_E_INVALID, "bb_add_bodies: this object holds batched worlds");
   return add_bodies_impl(w, bodies, count, out_first_id);
 }
@@ -741,13 +957,18 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
                        uint32_t* out_world_index, uint32_t* out_first_id) {
   World* w = W(world);
   if (!w || !desc || count == 0) return fail(BB_E_INVALID, "bb_add_world: bad arguments");
+  w->forget_snapshot();
   if (w->d.n_worlds == 0 && w->n > 0) return fail(BB_E_INVALID, "bb_add_world: object already holds a plain world");
   for (int k = 0; k < 3; ++k)
     if (!(desc->world_extent[k] > 0)) return fail(BB_E_INVALID, "bb_add_world: world_extent must be positive");
   uint32_t first = 0;
+  const uint32_t dyn_before = w->n_dyn;
   bb_status st = add_bodies_impl(w, bodies, count, &first, w->d.n_worlds > 0);
   if (st != BB_OK) return st;
   const uint32_t widx = w->d.n_worlds;
+  w->wfirst.push_back(first);
+  w->wcount.push_back(count);
+  w->wdyn.push_back(w->n_dyn - dyn_before);
   std::vector<uint32_t> wof(count, widx);
   CU(cudaMemcpyAsync(w->d.world_of + first, wof.data(), 4ull * count, cudaMemcpyHostToDevice, w->stream));
   CU(cudaMemcpyAsync(w->d.world_first + widx, &first, 4, cudaMemcpyHostToDevice, w->stream));
@@ -766,10 +987,82 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
 
 uint32_t bb_world_count(void* world) { return world ? W(world)->d.n_worlds : 0; }
 
+// body id range of world `widx` of a batch, or of the whole plain world (widx 0)
+static bool world_range(World* w, uint32_t widx, uint32_t* first, uint32_t* count) {
+  if (w->d.n_worlds == 0) {
+    if (widx != 0) return false;
+    *first = 0;
+    *count = w->n;
+    return true;
+  }
+  if (widx >= w->wfirst.size()) return false;
+  *first = w->wfirst[widx];
+  *count = w->wcount[widx];
+  return true;
+}
+
+bb_status bb_world_pause(void* world, uint32_t world_index, uint32_t paused) {
+  World* w = W(world);
+  uint32_t first = 0, count = 0;
+  if (!w || !world_range(w, world_index, &first, &count)) return fail(BB_E_INVALID, "bb_world_pause: bad world index");
+  w->forget_snapshot();
+  if (count == 0) return BB_OK;
+  k_pause<<<(count + 255) / 256, 256, 0, w->stream>>>(w->d, first, count, paused ? 1u : 0u);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(BB_E_CUDA, std::string("bb_world_pause: ") + cudaGetErrorString(e));
+  return BB_OK;
+}
+
+bb_status bb_world_refill(void* world, uint32_t world_index, const bb_batch_world_desc* desc,
+                          const bb_body_desc* bodies, uint32_t count) {
+  World* w = W(world);
+  if (!w || !desc || (!bodies && count)) return fail(BB_E_INVALID, "bb_world_refill: bad arguments");
+  if (w->d.n_worlds == 0 || world_index >= w->wfirst.size())
+    return fail(BB_E_INVALID, "bb_world_refill: not a world of this batch");
+  for (int k = 0; k < 3; ++k)
+    if (!(desc->world_extent[k] > 0)) return fail(BB_E_INVALID, "bb_world_refill: world_extent must be positive");
+  const uint32_t first = w->wfirst[world_index], slot = w->wcount[world_index];
+  if (count > slot) return fail(BB_E_CAPACITY, "bb_world_refill: more bodies than the world's slot holds");
+  w->forget_snapshot();
+  if (w->park_shape == 0xFFFFFFFFu) {
+    w->shapes.push_back(Shape{BB_SHAPE_BOX, {0.001f, 0.001f, 0.001f}});
+    w->park_shape = uint32_t(w->shapes.size() - 1);
+  }
+  // the slot's unused bodies are parked: static specks on a line well outside the world's box
+  std::vector<bb_body_desc> all(slot);
+  for (uint32_t i = 0; i < count; ++i) all[i] = bodies[i];
+  for (uint32_t i = count; i < slot; ++i) {
+    bb_body_desc& b = all[i];
+    std::memset(&b, 0, sizeof(b));
+    b.position[0] = desc->world_min[0] - 1000.0f - 0.01f * float(i - count);
+    b.position[1] = desc->world_min[1] - 1000.0f;
+    b.position[2] = desc->world_min[2] - 1000.0f;
+    b.rotation[3] = 1.0f;
+    b.shape = w->park_shape;
+  }
+  BodyRows r;
+  bb_status st = pack_bodies(w, all.data(), slot, r);
+  if (st != BB_OK) return st;
+  st = upload_bodies(w, first, r);
+  if (st != BB_OK) return st;
+  for (uint32_t i = 0; i < slot; ++i) w->restitution[first + i] = r.restitution[i];
+  w->n_dyn = w->n_dyn - w->wdyn[world_index] + r.ndyn;
+  w->wdyn[world_index] = r.ndyn;
+  float4 bnd[2] = {make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
+                   make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f)};
+  CU(cudaMemcpyAsync(w->d.world_bounds + 2 * world_index, bnd, sizeof(bnd), cudaMemcpyHostToDevice, w->stream));
+  k_refill_contacts<<<(slot + 255) / 256, 256, 0, w->stream>>>(w->d, first, slot);
+  uint32_t nn[2] = {w->n, w->n_dyn};
+  CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));  // bnd and nn are host locals
+  return BB_OK;
+}
+
 bb_status bb_set_material(void* world, uint32_t first, uint32_t count, float friction, float restitution) {
   World* w = W(world);
   if (!w || uint64_t(first) + count > w->n) return fail(BB_E_INVALID, "bb_set_material: bad range");
   cudaStreamSynchronize(w->stream);
+  w->forget_snapshot();
   std::vector<float4> ii(count);
   CU(cudaMemcpy(ii.data(), w->d.iinv + first, count * sizeof(float4), cudaMemcpyDeviceToHost));
   for (auto& v : ii) v.w = friction;
@@ -782,6 +1075,7 @@ bb_status bb_set_material(void* world, uint32_t first, uint32_t count, float fri
 bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
   World* w = W(world);
   if (!w || !p) return fail(BB_E_INVALID, "bb_set_solver_params: bad arguments");
+  w->forget_snapshot();
   if (p->solver == BB_SOLVER_PGS && (p->flags & BB_SIM_USE_GRAPH_COLORING))
     return fail(BB_E_INVALID, "BB_SOLVER_PGS runs on the per-island path only: clear BB_SIM_USE_GRAPH_COLORING");
   if (p->solver > BB_SOLVER_AVBD) return fail(BB_E_INVALID, "unknown solver");
@@ -791,8 +1085,8 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
     if (!(p->world_extent[k] > 0)) return fail(BB_E_INVALID, "world_extent must be positive");
   if (p->schedule > BB_SCHEDULE_COLOUR_BARRIER) return fail(BB_E_INVALID, "unknown schedule");
   if ((p->broad_threads != 0 && p->broad_threads != 32 && p->broad_threads != 64 && p->broad_threads != 128) ||
-      p->narrow_blocks_per_sm > 64 || p->pgs_stage_next > 1)
-    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, pgs_stage_next 0/1)");
+      p->narrow_blocks_per_sm > 64 || p->pgs_stage_next > BB_PGS_PIPE_HELD)
+    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, pgs_stage_next 0..3)");
   // contact geometry depends on these: no pair keeps last substep's manifolds as they were
   if (p->quirks != w->params.quirks || p->penetration_cap != w->params.penetration_cap)
     CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * (w->cap_n + 1), w->stream));
@@ -819,6 +1113,13 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
   World* w = W(world);
   if (!w || !(dt > 0) || substeps == 0 || substeps > 64) return fail(BB_E_INVALID, "bb_step: bad arguments");
   if (w->n == 0) return BB_OK;
+  if (w->regrow_max_ppb) {  // auto-regrow: snapshot before the first step since the last sync
+    if (!w->snapped) {
+      bb_status st = w->snapshot();
+      if (st != BB_OK) return st;
+    }
+    w->step_log.emplace_back(dt, substeps);
+  }
   const float h = dt / float(substeps);
   const bool warm_first = (w->params.flags & BB_SIM_WARM_STARTING) && !w->skip_warm_once;
   const bool warm_rest = (w->params.flags & BB_SIM_WARM_STARTING) != 0;
@@ -900,7 +1201,7 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
       cudaEventRecord(ev[10], w->stream);
       if (w->params.solver == BB_SOLVER_AVBD) bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
       else if (!coloured) bb_solve_islands(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->sms);
-      else bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->sms);
+      else bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->coop_pgs_stream, w->sms);
       cudaEventRecord(ev[11], w->stream);
       CU(cudaEventSynchronize(ev[11]));
       for (int k = 0; k < kStages; ++k) {
@@ -928,6 +1229,22 @@ bb_status bb_sync(void* world) {
   CU(cudaStreamSynchronize(w->stream));
   uint32_t flags = 0;
   CU(cudaMemcpy(&flags, &w->d.ctr->error_flags, 4, cudaMemcpyDeviceToHost));
+  // auto-regrow: a pair overflow in the steps since the last sync reruns them from the snapshot
+  // with twice the pair capacity, as often as the limit allows
+  while ((flags & (BB_ERRF_PAIR_OVERFLOW | BB_ERRF_CONTACT_OVERFLOW)) && w->regrow_max_ppb && w->snapped &&
+         w->ppb < w->regrow_max_ppb) {
+    bb_status st = w->regrow(std::min(2 * w->ppb, w->regrow_max_ppb));
+    if (st != BB_OK) return st;
+    const std::vector<std::pair<float, uint32_t>> log = w->step_log;
+    w->step_log.clear();
+    for (auto& s : log) {
+      st = bb_step(world, s.first, s.second);
+      if (st != BB_OK) return st;
+    }
+    CU(cudaStreamSynchronize(w->stream));
+    CU(cudaMemcpy(&flags, &w->d.ctr->error_flags, 4, cudaMemcpyDeviceToHost));
+  }
+  if (!(flags & (BB_ERRF_PAIR_OVERFLOW | BB_ERRF_CONTACT_OVERFLOW))) w->forget_snapshot();
   if (flags & (BB_ERRF_PAIR_OVERFLOW | BB_ERRF_CONTACT_OVERFLOW))
     return fail(BB_E_CAPACITY, "pair capacity exceeded: create the world with a larger pairs_per_body");
   if (flags & (BB_ERRF_SPIN_LIMIT | BB_ERRF_STACK_OVERFLOW | BB_ERRF_CAS_LIMIT))
@@ -999,6 +1316,7 @@ bb_status bb_write_state(void* world, const float* position, const float* rotati
                          const float* omega) {
   World* w = W(world);
   if (!w) return fail(BB_E_INVALID, "null world");
+  w->forget_snapshot();
   const uint32_t n = w->n;
   if (n == 0) return BB_OK;
   float* st = w->d.staging;
@@ -1215,6 +1533,106 @@ bb_status bb_debug_read(void* world, uint32_t which, void* dst, uint64_t max_byt
   return BB_OK;
 }
 
+// ---- saved state ----------------------------------------------------------------------------
+// Image of a world: a header with the host fields that steer the next step, the byte size of
+// every device array in allocation order, then the arrays themselves (and the voxel slot buffer).
+// Loading it into a world created with the same capacity and holding the same bodies (same
+// shapes, same order, hence the same allocation sequence) restores every bit the step reads:
+// poses, velocities, flags and sleep timers, both manifold buffers with their contacts,
+// impulses and anchors, per-body lists, sort order, frozen bits, last island roots, counters.
+
+bb_status bb_world_save_state(void* world, void* dst, uint64_t max_bytes, uint64_t* bytes) {
+  World* w = W(world);
+  if (!w || !bytes) return fail(BB_E_INVALID, "bb_world_save_state: bad arguments");
+  const uint64_t total = state_bytes(w);
+  *bytes = total;
+  if (!dst) return BB_OK;
+  if (max_bytes < total) return fail(BB_E_INVALID, "bb_world_save_state: buffer smaller than the state");
+  CU(cudaStreamSynchronize(w->stream));
+  StateHeader h{};
+  h.magic = kStateMagic;
+  h.version = 1;
+  h.cap_n = w->cap_n;
+  h.cap_p = w->cap_p;
+  h.n = w->n;
+  h.n_dyn = w->n_dyn;
+  h.n_worlds = w->d.n_worlds;
+  h.vox_on = w->d.vox_on;
+  h.full_inertia = w->d.full_inertia;
+  h.parity = w->parity;
+  h.last_cur = w->last_cur;
+  h.ran_any = w->ran_any ? 1u : 0u;
+  h.skip_warm_once = w->skip_warm_once ? 1u : 0u;
+  h.arrays = uint32_t(w->owned.size());
+  h.slot_bytes = w->slot_buf ? 16ull * w->cap_p : 0ull;
+  h.total = total;
+  h.params = w->params;
+  char* out = static_cast<char*>(dst);
+  std::memcpy(out, &h, sizeof(h));
+  uint64_t* sizes = reinterpret_cast<uint64_t*>(out + sizeof(h));
+  char* p = out + sizeof(h) + 8ull * w->owned.size();
+  for (size_t k = 0; k < w->owned.size(); ++k) {
+    sizes[k] = w->owned[k].second;
+    CU(cudaMemcpyAsync(p, w->owned[k].first, w->owned[k].second, cudaMemcpyDeviceToHost, w->stream));
+    p += w->owned[k].second;
+  }
+  if (h.slot_bytes) CU(cudaMemcpyAsync(p, w->slot_buf, h.slot_bytes, cudaMemcpyDeviceToHost, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  return BB_OK;
+}
+
+bb_status bb_world_load_state(void* world, const void* src, uint64_t bytes) {
+  World* w = W(world);
+  if (!w || !src || bytes < sizeof(StateHeader)) return fail(BB_E_INVALID, "bb_world_load_state: bad arguments");
+  StateHeader h;
+  std::memcpy(&h, src, sizeof(h));
+  if (h.magic != kStateMagic || h.version != 1 || h.total != bytes)
+    return fail(BB_E_INVALID, "bb_world_load_state: not a saved world state");
+  if (h.cap_n != w->cap_n || h.cap_p != w->cap_p || h.n != w->n || h.n_dyn != w->n_dyn ||
+      h.n_worlds != w->d.n_worlds || h.vox_on != w->d.vox_on || h.full_inertia != w->d.full_inertia ||
+      h.arrays != w->owned.size() || h.slot_bytes != (w->slot_buf ? 16ull * w->cap_p : 0ull) ||
+      state_bytes(w) != bytes)
+    return fail(BB_E_INVALID,
+                "bb_world_load_state: the world differs from the saved one (create it with the same capacity and "
+                "add the same bodies first)");
+  const char* in = static_cast<const char*>(src);
+  const uint64_t* sizes = reinterpret_cast<const uint64_t*>(in + sizeof(h));
+  for (size_t k = 0; k < w->owned.size(); ++k)
+    if (sizes[k] != w->owned[k].second) return fail(BB_E_INVALID, "bb_world_load_state: array sizes differ");
+  CU(cudaStreamSynchronize(w->stream));
+  w->forget_snapshot();
+  const char* p = in + sizeof(h) + 8ull * w->owned.size();
+  for (auto& o : w->owned) {
+    CU(cudaMemcpyAsync(o.first, p, o.second, cudaMemcpyHostToDevice, w->stream));
+    p += o.second;
+  }
+  if (h.slot_bytes) CU(cudaMemcpyAsync(w->slot_buf, p, h.slot_bytes, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  w->parity = h.parity;
+  w->last_cur = h.last_cur;
+  w->ran_any = h.ran_any != 0;
+  w->skip_warm_once = h.skip_warm_once != 0;
+  w->params = h.params;
+  w->invalidate_graphs();
+  return BB_OK;
+}
+
+bb_status bb_world_set_auto_regrow(void* world, uint32_t max_pairs_per_body) {
+  World* w = W(world);
+  if (!w) return fail(BB_E_INVALID, "bb_world_set_auto_regrow: null world");
+  if (max_pairs_per_body && max_pairs_per_body < w->ppb)
+    return fail(BB_E_INVALID, "bb_world_set_auto_regrow: the limit is below the current pairs per body");
+  CU(cudaStreamSynchronize(w->stream));
+  w->regrow_max_ppb = max_pairs_per_body;
+  w->forget_snapshot();
+  if (!max_pairs_per_body && w->shadow) {
+    cudaFree(w->shadow);
+    w->shadow = nullptr;
+    w->shadow_cap = 0;
+  }
+  return BB_OK;
+}
+
 bb_status bb_debug_wait_limit(void* world, uint32_t polls, uint32_t abandon_block) {
   World* w = W(world);
   if (!w) return fail(BB_E_INVALID, "null world");
@@ -1254,6 +1672,29 @@ bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint3
 uint64_t bb_kernel_launch_count(void* world) { return world ? W(world)->launches : 0; }
 
 }  // extern "C"
+
+// State of bodies [first, first + count) (the serving loop's view of one batch slot): xyz
+// positions, xyzw rotations, velocities, angular velocities, flags (may each be null).
+bb_status bb_world_read_range(void* world, uint32_t first, uint32_t count, float* position, float* rotation,
+                              float* velocity, float* omega, uint32_t* flags) {
+  World* w = W(world);
+  if (!w || uint64_t(first) + count > w->n) return fail(BB_E_INVALID, "bb_world_read_range: bad range");
+  if (count == 0) return BB_OK;
+  float* st = w->d.staging;
+  uint32_t* fl = reinterpret_cast<uint32_t*>(st + 13ull * count);
+  k_pack_range<<<(count + 255) / 256, 256, 0, w->stream>>>(w->d, first, count, st, fl);
+  if (position) CU(cudaMemcpyAsync(position, st + 4ull * count, 12ull * count, cudaMemcpyDeviceToHost, w->stream));
+  if (rotation) CU(cudaMemcpyAsync(rotation, st, 16ull * count, cudaMemcpyDeviceToHost, w->stream));
+  if (velocity) CU(cudaMemcpyAsync(velocity, st + 7ull * count, 12ull * count, cudaMemcpyDeviceToHost, w->stream));
+  if (omega) CU(cudaMemcpyAsync(omega, st + 10ull * count, 12ull * count, cudaMemcpyDeviceToHost, w->stream));
+  if (flags) CU(cudaMemcpyAsync(flags, fl, 4ull * count, cudaMemcpyDeviceToHost, w->stream));
+  CU(cudaStreamSynchronize(w->stream));
+  return BB_OK;
+}
+
+// device word of the world's sticky error bits (BB_ERRF_*)
+const uint32_t* bb_world_error_word(void* world) { return world ? &W(world)->d.ctr->error_flags : nullptr; }
+
 
 // ---- autotuner ------------------------------------------------------------------------------
 // Coordinate descent over the launch-geometry fields and the colour-sweep schedule of
@@ -1297,7 +1738,7 @@ bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_s
       {&bb_solver_params::schedule, {BB_SCHEDULE_DATAFLOW, BB_SCHEDULE_COLOUR_BARRIER}, true, false},
       {&bb_solver_params::broad_threads, {32, 64, 128}, false, false},
       {&bb_solver_params::narrow_blocks_per_sm, {4, 8, 16, 32}, false, false},
-      {&bb_solver_params::pgs_stage_next, {0, 1}, true, true},
+      {&bb_solver_params::pgs_stage_next, {BB_PGS_PIPE_HELD, BB_PGS_PIPE_STREAM, BB_PGS_PIPE_STAGED}, true, true},
   };
   for (const Axis& ax : axes) {
     if (st != BB_OK) break;

@@ -37,6 +37,10 @@ typedef int32_t bb_status;
 #define BB_BODY_DYNAMIC (1u << 1)
 #define BB_BODY_GRAVITY (1u << 2)
 #define BB_BODY_SLEEPING (1u << 3)
+/* Set by bb_world_pause on every dynamic body of a paused (sub-)world: the body counts as
+ * asleep, and the step leaves it and its contacts exactly as they are (no sleep-timer update,
+ * contacts carried over unchanged) until the world is resumed.  No reference counterpart. */
+#define BB_BODY_PAUSED (1u << 5)
 
 /* ---- shapes ---------------------------------------------------------------------- */
 #define BB_SHAPE_BOX 0u    /* reference OBB body: RigidBody::minimum/maximum (shared.inl:349-352) */
@@ -101,6 +105,19 @@ typedef int32_t bb_status;
  * bb_default_solver_params) is the reference value; replaces StatusManager::set_solver /
  * flag toggles (src/status_manager.hpp:204-373) and the compile-time constants of
  * include/shared.inl:77-83,760-839 and include/defines.hpp:352-364. */
+/* Item pipelines of the colour-barrier PGS_SOFT sweeps (bb_solver_params.pgs_stage_next); the
+ * results are the same bits for each.  HELD: a thread holds its next colour's item (up to four
+ * contacts) in registers across the barrier, one block per SM -- for colours of about one item
+ * per thread, where the barrier latency dominates.  STAGED: HELD plus the thread's next item of
+ * the same colour copied into shared memory while the current one computes.  STREAM: nothing
+ * held, two blocks per SM, each contact's rows loaded while the one before computes -- for
+ * colours of several items per thread.  AUTO: STREAM for worlds of 262,144 bodies or more, else
+ * HELD. */
+#define BB_PGS_PIPE_AUTO 0u
+#define BB_PGS_PIPE_STAGED 1u
+#define BB_PGS_PIPE_STREAM 2u
+#define BB_PGS_PIPE_HELD 3u
+
 typedef struct bb_solver_params {
   uint32_t solver;             /* BB_SOLVER_* (default AVBD) */
   uint32_t flags;              /* BB_SIM_* (default BB_SIM_DEFAULT_FLAGS) */
@@ -134,8 +151,7 @@ typedef struct bb_solver_params {
   /* launch geometry (results are identical for every value; 0 = default; bb_autotune picks) */
   uint32_t broad_threads;        /* broad-phase block size: 32, 64 or 128 (default 128) */
   uint32_t narrow_blocks_per_sm; /* narrow-phase grid, 128-thread blocks per SM: 1..64 (default 16) */
-  uint32_t pgs_stage_next;       /* colour-barrier PGS_SOFT: 1 stages each thread's next item of a colour in shared
-                                    memory while the current one computes (large worlds); 0 loads it after (default) */
+  uint32_t pgs_stage_next;       /* colour-barrier PGS_SOFT item pipeline, BB_PGS_PIPE_* (default AUTO) */
   /* Morton normalisation */
   uint32_t bounds_mode;        /* BB_BOUNDS_* */
   float world_min[3];          /* default -64 */
@@ -304,6 +320,27 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
                        uint32_t* out_world_index, uint32_t* out_first_id);
 uint32_t bb_world_count(void* world);
 
+/* Batch slots for continuous batching.  A batch is one object stepped as a whole; these two
+ * calls let a serving loop keep worlds resident in it while they have no work, and reuse the
+ * slot of a finished world for a new one, without touching the other worlds.
+ *
+ * bb_world_pause: paused = 1 pauses world `world_index` of the batch (0 for a plain world):
+ * its dynamic bodies count as asleep (BB_BODY_PAUSED), and every later step leaves the world
+ * exactly as it is -- poses, velocities, sleep timers, and its contacts, which are carried from
+ * substep to substep unchanged.  paused = 0 resumes it: it then steps bit for bit as if the
+ * steps taken while it was paused had not happened.  Asynchronous on the world's stream.
+ *
+ * bb_world_refill: puts `count` new bodies into world `world_index`'s slot (ids
+ * [first, first + slot size), slot size = the body count the world was added with), with new
+ * Morton bounds; the slot's unused bodies are parked as static specks far outside the box.  The
+ * slot's old bodies, their contacts and their sorted order are discarded: the new world starts
+ * as a world just added does (and steps as it would alone).  count above the slot size returns
+ * BB_E_CAPACITY.  Waits for the world's stream.  No reference counterpart (the reference steps
+ * one scene, src/rigid_body_manager.cpp:1606-1622). */
+bb_status bb_world_pause(void* world, uint32_t world_index, uint32_t paused);
+bb_status bb_world_refill(void* world, uint32_t world_index, const bb_batch_world_desc* desc,
+                          const bb_body_desc* bodies, uint32_t count);
+
 /* Change the friction/restitution of bodies [first, first+n).  No separate reference
  * entry point (materials are per body, shared.inl:360-361). */
 bb_status bb_set_material(void* world, uint32_t first, uint32_t n, float friction, float restitution);
@@ -372,6 +409,32 @@ uint64_t bb_world_bytes_for(uint32_t max_bodies, uint32_t pairs_per_body);
  * object can hold a different scene (bodies added next restart the persistent state).  No
  * reference counterpart (the reference reloads a scene into fixed buffers, RBM:224-254). */
 bb_status bb_world_clear(void* world);
+
+/* Saved world state, for checkpoints and for resuming evicted worlds bit for bit.
+ * bb_world_save_state writes an image of the world (its device arrays and the host fields that
+ * steer the next step: manifold parity, solver parameters, pending warm-start skip) into dst;
+ * with dst = NULL it only returns the size in *bytes.  The image holds the persistent contacts
+ * (both manifold buffers with impulses, anchors and warm-start counters), per-body lists, sort
+ * order, sleep timers and island roots, so a world loaded from it steps exactly as the saved
+ * world would have.  Its size is the world's device footprint (bb_world_device_bytes).
+ * bb_world_load_state restores an image into a world created with the same bb_world_desc
+ * capacity that holds the same bodies (the same shapes and bodies added in the same order);
+ * anything else returns BB_E_INVALID.  Both wait for the world's stream.  The reference's
+ * counterpart is a pause of the whole step (src/status_manager.hpp:133-152); it saves nothing. */
+/* Automatic regrow of the pair capacity.  With max_pairs_per_body > 0, bb_step first copies
+ * the world's device state (once, before the first step since the last bb_sync; the copy needs as
+ * much device memory again as the world holds), and when bb_sync finds that a step overflowed the
+ * pair or manifold capacity it reallocates the world with twice the pairs per body (up to the
+ * limit), restores the copy and runs the steps issued since again: the world then steps exactly
+ * as a world created with the larger capacity would.  bb_sync returns BB_E_CAPACITY only when the
+ * limit is reached.  Calls that change bodies, poses or parameters between a step and its
+ * bb_sync drop the copy (an overflow before them is then reported, not repaired).  0 turns it
+ * off (the default).  The reference instead clamps silently at its N^2 buffer sizes
+ * (include/shared.inl:770-776, RB_sim.slang:454,466). */
+bb_status bb_world_set_auto_regrow(void* world, uint32_t max_pairs_per_body);
+
+bb_status bb_world_save_state(void* world, void* dst, uint64_t max_bytes, uint64_t* bytes);
+bb_status bb_world_load_state(void* world, const void* src, uint64_t bytes);
 
 /* Number of kernels this library launched on the world's stream since creation. */
 uint64_t bb_kernel_launch_count(void* world);
@@ -456,6 +519,8 @@ typedef struct bb_request_status {
   double submit_s;   /* server clock, seconds since bb_server_create */
   double start_s;
   double finish_s;
+  uint32_t error_flags; /* BB_ERRF_* seen in the world's batch by the end of the request's last step */
+  uint32_t reserved;
 } bb_request_status;
 
 typedef struct bb_server_stats {

@@ -149,15 +149,18 @@ def test_dataflow_schedule_equals_colour_barrier(name):
 
 
 @pytest.mark.parametrize("name", ["mixed_3000", "pyramids_200x1000"])
-def test_staging_the_next_item_equals_loading_it(name):
-    """The colour-barrier kernel that stages each thread's next item of a colour in shared memory
-    while the current one computes runs the same arithmetic on the same data.  In the 200k-box
-    pyramids (over 400k manifolds in about a dozen colours, on at most 148 x 256 threads) the
-    threads run several items of the largest colours, so the staged path carries them."""
+def test_item_pipelines_give_the_same_bits(name):
+    """The colour-barrier sweeps' three item pipelines -- the next colour's item held in registers
+    across the barrier, that plus the thread's next item of the same colour staged in shared
+    memory, and streaming (nothing held, two blocks per SM, rows loaded contact by contact) --
+    run the same arithmetic on the same data in the same order.  In the 200k-box pyramids (over
+    400k manifolds in about a dozen colours) threads run several items of the largest colours, so
+    the staged and streaming loops carry them; the 3000-body column has colours of a few hundred
+    items, where the CTA-barrier shortcut and the overflow bucket come in."""
     big = name == "pyramids_200x1000"
     sc = scenes.pyramids(n_pyramids=200, boxes_per=1000, seed=0) if big else scenes.mixed_column(n_bodies=3000, seed=2)
     outs = []
-    for stage in (0, 1):
+    for stage in (bb.PGS_PIPE_HELD, bb.PGS_PIPE_STAGED, bb.PGS_PIPE_STREAM):
         p = params(bb.SOLVER_PGS_SOFT, schedule=bb.SCHEDULE_COLOUR_BARRIER, pgs_stage_next=stage)
         w = bb.world_from_scene(sc, params=p)
         for _ in range(4 if big else 40):
@@ -168,8 +171,9 @@ def test_staging_the_next_item_equals_loading_it(name):
         if big:
             assert st["manifold_count"] > 400_000  # the largest colours hold more items than the grid has threads
         w.close()
-    for k in outs[0]:
-        assert np.array_equal(outs[0][k], outs[1][k]), k
+    for o in outs[1:]:
+        for k in outs[0]:
+            assert np.array_equal(outs[0][k], o[k]), k
 
 
 def test_world_added_to_a_running_batch_leaves_the_others_unchanged():
@@ -269,3 +273,69 @@ def test_batched_worlds_asleep_keep_their_front_end_outputs():
     w.sync()
     assert w.stats()["pair_count"] == n_pairs - 1
     assert w.stats()["error_flags"] == 0
+
+
+def alone(sc, p, steps, substeps):
+    out, _ = run_batch([sc], p, steps=steps, substeps=substeps)
+    return out[0]
+
+
+@pytest.mark.parametrize("solver", [bb.SOLVER_PGS_SOFT, bb.SOLVER_AVBD])
+def test_paused_world_resumes_as_if_never_paused(solver):
+    """World 1 of a batch is paused for 15 steps while the others step, then resumed: it ends
+    bit for bit where the same world stepped alone for only its active steps ends, and the
+    others are unaffected."""
+    scs = [WORLDS[0](), WORLDS[1](), WORLDS[3]()]
+    p = params(solver)
+    total = sum(int(s["n"]) for s in scs)
+    w = bb.World(total)
+    firsts = [w.add_world(sc, *scene_bounds(sc))[1] for sc in scs]
+    w.set_params(p)
+    for _ in range(10):
+        w.step(DT, 2)
+    w.pause_world(1)
+    for _ in range(15):
+        w.step(DT, 2)
+    w.pause_world(1, False)
+    for _ in range(10):
+        w.step(DT, 2)
+    st = w.read_state()
+    assert w.stats()["error_flags"] == 0
+    w.close()
+    active = {0: 35, 1: 20, 2: 35}
+    for k, sc in enumerate(scs):
+        ref = alone(sc, p, active[k], 2)
+        n = int(sc["n"])
+        for key in ref:
+            assert np.array_equal(st[key][firsts[k]:firsts[k] + n], ref[key]), (k, key)
+
+
+def test_refilled_slot_steps_like_a_world_added():
+    """The slot of world 1 is refilled with a smaller, different scene after 10 steps: the new
+    world steps bit for bit as it would alone, and the other worlds are unaffected."""
+    scs = [WORLDS[0](), WORLDS[1](), WORLDS[3]()]
+    new = tiny_stack()
+    assert new["n"] < scs[1]["n"]
+    p = params(bb.SOLVER_PGS_SOFT)
+    total = sum(int(s["n"]) for s in scs)
+    w = bb.World(total)
+    firsts = [w.add_world(sc, *scene_bounds(sc))[1] for sc in scs]
+    w.set_params(p)
+    for _ in range(10):
+        w.step(DT, 2)
+    w.refill_world(1, new, *scene_bounds(new))
+    for _ in range(12):
+        w.step(DT, 2)
+    st = w.read_state()
+    assert w.stats()["error_flags"] == 0
+    w.close()
+    refs = {0: (scs[0], 22), 1: (new, 12), 2: (scs[2], 22)}
+    for k, (sc, steps) in refs.items():
+        ref = alone(sc, p, steps, 2)
+        n = int(sc["n"])
+        for key in ref:
+            assert np.array_equal(st[key][firsts[k]:firsts[k] + n], ref[key]), (k, key)
+    with pytest.raises(bb.BeatboxError):  # a slot holds at most its size
+        w2 = bb.World(total)
+        w2.add_world(new, *scene_bounds(new))
+        w2.refill_world(0, scs[1], *scene_bounds(scs[1]))

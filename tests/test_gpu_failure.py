@@ -57,3 +57,47 @@ def test_a_grid_barrier_wait_that_runs_out_is_reported_and_the_world_recovers():
     a, b = w.read_state(), fresh.read_state()
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_capacity_overflow_regrows_and_equals_a_large_world():
+    """A world created with one pair per body on overlapping boxes overflows its pair capacity;
+    with auto-regrow bb_sync reallocates it with more pairs per body, restores the state from
+    before the steps since the last sync and runs them again, so it ends bit for bit where a
+    world created with the large capacity ends."""
+    sc = scenes.pyramids(n_pyramids=1, boxes_per=1000, gap=-0.002)  # every box overlaps its neighbours
+    worlds = []
+    for ppb in (1, 64):
+        w = bb.World(sc["n"], pairs_per_body=ppb)
+        w.add_scene(sc)
+        w.set_params(params(sc))
+        worlds.append(w)
+    small, big = worlds
+    small.set_auto_regrow(64)
+    cap0 = small.stats()["pair_capacity"]
+    for k in range(6):
+        small.step(DT, 4)
+        big.step(DT, 4)
+        if k % 2 == 1:  # the first overflow is repaired with two steps to rerun
+            small.sync()
+    small.sync()
+    big.sync()
+    st = small.stats()
+    assert st["error_flags"] == 0 and st["pair_capacity"] > cap0
+    assert st["pair_count"] == big.stats()["pair_count"] > sc["n"]
+    a, b = small.read_state(), big.read_state()
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
+    for what in ("manifolds", "contacts"):
+        assert np.array_equal(small.debug_read(what), big.debug_read(what)), what
+
+
+def test_overflow_without_regrow_is_still_reported():
+    sc = scenes.pyramids(n_pyramids=1, boxes_per=1000, gap=-0.002)
+    w = bb.World(sc["n"], pairs_per_body=1)
+    w.add_scene(sc)
+    w.set_params(params(sc))
+    w.set_auto_regrow(2)  # a limit too low to hold the pairs
+    w.step(DT, 1)
+    with pytest.raises(bb.BeatboxError) as e:
+        w.sync()
+    assert e.value.code == bb.E_CAPACITY

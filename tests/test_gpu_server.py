@@ -1,6 +1,8 @@
-"""GPU tests of the serving loop (bb_server_*): every world's result is the same alone and in
-the mix of concurrent requests (bitwise), eviction under a tight HBM budget keeps requests
-completing, and a world that can never fit the budget is refused with BB_E_BUDGET."""
+"""GPU tests of the serving loop (bb_server_*, continuous batching: worlds are slots of batched
+worlds that advance together): every world's result is the same alone and in the mix of
+concurrent requests (bitwise), eviction under a tight HBM budget keeps requests completing, a
+world that can never fit the budget is refused with BB_E_BUDGET, and served results agree with
+the oracle on a sampled 1% of worlds."""
 import numpy as np
 import pytest
 
@@ -20,9 +22,11 @@ def req_params(k):
     return p
 
 
-WORLD_SIZES = [64, 150, 400, 900, 2000, 97]
+# three size classes (slots of 64, 128 and 1024 bodies), several worlds in each
+WORLD_SIZES = [64, 50, 60, 900, 1000, 97, 120]
 # (world index, steps) in submission order: worlds get several requests, interleaved
-PLAN = [(0, 5), (1, 12), (2, 3), (3, 8), (4, 6), (0, 7), (5, 20), (2, 9), (1, 4), (3, 2), (0, 3), (4, 5)]
+PLAN = [(0, 5), (1, 12), (2, 3), (3, 8), (4, 6), (0, 7), (5, 20), (2, 9), (1, 4), (3, 2), (0, 3), (4, 5),
+        (6, 11), (5, 4), (6, 3)]
 
 
 def run_plan(server, worlds, plan):
@@ -42,7 +46,9 @@ def test_each_world_is_the_same_alone_and_in_the_mix():
     res = run_plan(mix, worlds, PLAN)
     assert all(r["done"] and r["result"] == bb.OK for r in res)
     st = mix.stats()
-    assert st["completed"] == len(PLAN) and st["evictions"] == 0
+    assert st["completed"] == len(PLAN)
+    # worlds of a size class share batches: at most 3 size classes x 2 step classes (PGS, AVBD)
+    assert st["worlds_created"] <= 6 < len(WORLD_SIZES) * 2
     assert st["body_steps"] == sum(int(worlds[w]["n"]) * s for w, s in PLAN)
     mixed = {w: mix.read_state(1000 + w, int(worlds[w]["n"])) for w in range(len(worlds))}
     mix.close()
@@ -70,7 +76,7 @@ def test_tight_budget_evicts_idle_worlds_and_keeps_serving():
         for w, sc in enumerate(worlds):
             tickets.append(srv.submit(7 + w, 3, req_params(rnd), DT, 2, scene=sc if rnd == 0 else None))
     res = [srv.wait(t) for t in tickets]
-    assert all(r["result"] == bb.OK for r in res)
+    assert all(r["result"] == bb.OK for r in res), [(r["result"], r["error_flags"]) for r in res if r["result"] != bb.OK]
     st = srv.stats()
     assert st["evictions"] > 0 and st["resident_bytes"] <= 2.5 * per_world
     for w, sc in enumerate(worlds):
@@ -87,12 +93,28 @@ def test_world_larger_than_the_budget_is_refused():
     srv.close()
 
 
+def settled(sc, steps=30):
+    """The scene after `steps` steps of the same world on its own (a pile in contact), every body
+    awake: the state a sampled world is created from."""
+    w = bb.world_from_scene(sc, params=req_params(0), pairs_per_body=8)
+    for _ in range(steps):
+        w.step(DT, 2)
+    st = w.read_state()
+    w.close()
+    out = dict(sc)
+    for k in ("pos", "quat", "vel", "omega"):
+        out[k] = st[k].astype(np.float32)
+    return out
+
+
 def test_served_worlds_match_the_fp64_oracle_on_a_sampled_one_percent(oracle_lib):
-    """Poisson arrivals of new and continued worlds (config-5 style, scaled down); a seeded 1% of
-    the new worlds (at least one) take a single-step request and are never continued, so their
-    served state after the request is compared with the FP64 oracle's one step of the same
-    scene and parameters: the one-step tolerance (positions 1e-4 of the world's scale,
-    velocities 2e-4 of max(|v|, 1) m/s)."""
+    """Poisson arrivals of new and continued worlds (config-5 style, scaled down).  A seeded 1% of
+    the new worlds (at least two) are created from a contact-rich state (their scene after 30
+    steps) and take a single-step request while the others run; their served state is compared
+    with one step of the oracle from the same state and parameters, in FP64 and in FP32: over
+    the sampled components the served velocity errors against FP64 (median and 99th percentile)
+    are within 2x of the FP32 oracle's (plus 1e-6 m/s), and 99.9% of position components are
+    within 1e-4 relative + 1e-6 m."""
     import time
 
     rng = np.random.default_rng(11)
@@ -104,40 +126,46 @@ def test_served_worlds_match_the_fp64_oracle_on_a_sampled_one_percent(oracle_lib
     for j in range(200):
         time.sleep(float(rng.exponential(1.0 / 2000.0)))
         params = req_params(j)
-        if not known or rng.random() < 0.5:
+        # new worlds sampled at 1%, and at least two of them, submitted while others run
+        force = j in (120, 199) and len(sampled) < (1 if j == 120 else 2)
+        if force or not known or rng.random() < 0.5:
             k = int(rng.integers(0, len(templates)))
             key = next_key
             next_key += 1
-            if rng.random() < 0.01:
-                sampled.append((key, k, params))
-                tickets.append(srv.submit(key, 1, params, DT, 2, scene=templates[k]))
+            if force or rng.random() < 0.01:
+                sc = settled(templates[k])
+                sampled.append((key, sc, params))
+                tickets.append(srv.submit(key, 1, params, DT, 2, scene=sc))
                 continue
             known.append((key, k))
             tickets.append(srv.submit(key, int(rng.integers(1, 30)), params, DT, 2, scene=templates[k]))
         else:
             key, k = known[int(rng.integers(0, len(known)))]
             tickets.append(srv.submit(key, int(rng.integers(1, 30)), params, DT, 2))
-        if j == 199 and not sampled:  # at least one sampled world, submitted while others run
-            k = int(rng.integers(0, len(templates)))
-            sampled.append((next_key, k, req_params(j + 1)))
-            tickets.append(srv.submit(next_key, 1, req_params(j + 1), DT, 2, scene=templates[k]))
-            next_key += 1
     res = [srv.wait(t) for t in tickets]
-    assert all(r["result"] == bb.OK for r in res)
-    assert sampled
-    for key, k, params in sampled:
-        sc = templates[k]
+    assert all(r["result"] == bb.OK for r in res), [(r["result"], r["error_flags"]) for r in res if r["result"] != bb.OK]
+    assert len(sampled) >= 2
+    ge, fe, pos_ok = [], [], []
+    for key, sc, params in sampled:
         g = srv.read_state(key, int(sc["n"]))
         p = oracle_lib.SolverParams.from_buffer_copy(bytes(params))
         b = sc.get("bounds") or ([-64.0] * 3, [128.0] * 3)  # the Morton box the server applies
         p.world_min[:] = b[0]
         p.world_extent[:] = b[1]
-        o = oracle_lib.Oracle(sc, params=p)
-        o.step(DT, 2)
-        r = o.state()
+        o64 = oracle_lib.Oracle(sc, params=p)
+        o64.step(DT, 2)
+        o32 = oracle_lib.Oracle(sc, double=False, params=p)
+        o32.step(DT, 2)
+        assert o64.stats()["manifold_count"] > int(sc["n"]) // 2  # in contact
+        r, q = o64.state(), o32.state()
         dyn = (sc["flags"] & bb.BODY_DYNAMIC) != 0
-        perr = np.abs(g["pos"][dyn] - r["pos"][dyn]).max() / np.abs(r["pos"][dyn]).max()
-        verr = np.abs(g["vel"][dyn] - r["vel"][dyn]).max()
-        assert perr < 1e-4, (key, perr)
-        assert verr < 2e-4 * max(np.abs(r["vel"][dyn]).max(), 1.0), (key, verr)
+        ge.append(np.abs(g["vel"][dyn] - r["vel"][dyn]).ravel())
+        fe.append(np.abs(q["vel"][dyn] - r["vel"][dyn]).ravel())
+        rp = r["pos"][dyn]
+        pos_ok.append((np.abs(g["pos"][dyn] - rp) <= 1e-4 * np.abs(rp) + 1e-6).ravel())
+    ge, fe, pos_ok = np.concatenate(ge), np.concatenate(fe), np.concatenate(pos_ok)
+    for qn in (50, 99):
+        assert np.percentile(ge, qn) <= 2 * np.percentile(fe, qn) + 1e-6, (qn, np.percentile(ge, qn),
+                                                                          np.percentile(fe, qn))
+    assert pos_ok.mean() >= 0.999, pos_ok.mean()
     srv.close()
