@@ -35,7 +35,6 @@ QUIRK_GRAVITY_IMPULSE, QUIRK_SAT_FRAME, QUIRK_INERTIA_TRANSPOSE = 1, 2, 4
 QUIRKS_REFERENCE, QUIRKS_PHYSICAL = 7, 0
 BOUNDS_FIXED, BOUNDS_AUTO = 0, 1
 SCHEDULE_DATAFLOW, SCHEDULE_COLOUR_BARRIER = 0, 1
-PGS_PIPE_AUTO, PGS_PIPE_STAGED, PGS_PIPE_STREAM, PGS_PIPE_HELD = 0, 1, 2, 3  # bb_solver_params.pgs_stage_next
 SORT_STATIC_MAX_KEYS = 262144
 EDGE_COLOR_OVERFLOW = 0xFFFFFFFF
 EDGE_COLOR_RESTING = 0xFFFFFFFE  # the manifold's island has no awake body: not coloured, not solved
@@ -116,7 +115,7 @@ class Request(ctypes.Structure):
 class RequestStatus(ctypes.Structure):
     _fields_ = [("done", ctypes.c_uint32), ("result", ctypes.c_int32), ("submit_s", ctypes.c_double),
                 ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double), ("error_flags", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("error_site", ctypes.c_uint32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -134,7 +133,7 @@ class StepStats(ctypes.Structure):
         "avbd_violations", "sleeping_count", "fresh_contacts", "stick_count")] + [
         ("max_penetration", ctypes.c_float), ("error_flags", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
         ("substeps_run", ctypes.c_uint32), ("solved_manifolds", ctypes.c_uint32),
-        ("solved_contacts", ctypes.c_uint32)]
+        ("solved_contacts", ctypes.c_uint32), ("error_site", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -635,13 +634,13 @@ class Server:
         st = RequestStatus()
         _check(self.L.bb_server_poll(self.h, ticket, ctypes.byref(st)))
         return dict(done=bool(st.done), result=st.result, submit_s=st.submit_s, start_s=st.start_s,
-                    finish_s=st.finish_s, error_flags=st.error_flags)
+                    finish_s=st.finish_s, error_flags=st.error_flags, error_site=st.error_site)
 
     def wait(self, ticket: int) -> dict:
         st = RequestStatus()
         _check(self.L.bb_server_wait(self.h, ticket, ctypes.byref(st)))
         return dict(done=bool(st.done), result=st.result, submit_s=st.submit_s, start_s=st.start_s,
-                    finish_s=st.finish_s, error_flags=st.error_flags)
+                    finish_s=st.finish_s, error_flags=st.error_flags, error_site=st.error_site)
 
     def read_state(self, world: int, n: int) -> dict:
         out = dict(pos=np.empty((n, 3), np.float32), quat=np.empty((n, 4), np.float32),

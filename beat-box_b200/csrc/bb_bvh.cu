@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(128) k_broad(const DevState d, uint32_t n) {
     ++count;
   };
   if (!walk_query(d, 0, leaf0, int(i), wend, qmn, qmx, EMIT ? 0xFFFFFFFFu : BB_BP_BUDGET, leaf)) {
-    const uint32_t slot = atomicAdd(&d.ctr->pad[4], 1u);
+    const uint32_t slot = atomicAdd(&d.ctr->heavy_n, 1u);
     if (slot < BB_HEAVY_CAP) {
       d.heavy_list[slot] = i;
       d.is_heavy[i] = 1;
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
   __shared__ int s_fr[2][BB_FRONTIER];
   __shared__ uint32_t s_warp[BB_FRONTIER / 32];
   __shared__ uint32_t s_size;
-  const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
+  const uint32_t hc = min(d.ctr->heavy_n, BB_HEAVY_CAP);
   if (blockIdx.x >= hc || (!all && d.hv_n[blockIdx.x] != BB_NONE)) return;  // pool path took this query
   const uint32_t qi = d.heavy_list[blockIdx.x];
   const int N = int(n), leaf0 = N - 1;
@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
   __shared__ int s_fr[2][BB_HV_FRONTIER];
   __shared__ uint32_t s_warp[BB_HV_THREADS / 32];
   __shared__ uint32_t s_size, s_off, s_fits;
-  const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
+  const uint32_t hc = min(d.ctr->heavy_n, BB_HEAVY_CAP);
   const int N = int(n), leaf0 = N - 1;
   const int t = threadIdx.x;
   for (uint32_t slot = blockIdx.x; slot < hc; slot += gridDim.x) {
@@ -720,7 +720,7 @@ __global__ void k_heavy_walk(const DevState d, uint32_t n) {
 // pair count of every heavy query with a pool frontier
 __global__ void k_heavy_totals(const DevState d) {
   if (d.ctr->front_skip) return;  // nothing moved since the last front end
-  const uint32_t hc = min(d.ctr->pad[4], BB_HEAVY_CAP);
+  const uint32_t hc = min(d.ctr->heavy_n, BB_HEAVY_CAP);
   for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < hc; slot += gridDim.x * blockDim.x) {
     const uint32_t m = d.hv_n[slot];
     if (m == BB_NONE) continue;

@@ -62,7 +62,9 @@ struct DevCounters {
   uint32_t abandon_block;  // test switch: the PGS solver's last block leaves before its first barrier
   uint32_t pgs_manifolds;  // per substep: colour-sweep items with an awake body (solved manifolds)
   uint32_t pgs_contacts;   // their contacts
-  uint32_t pad[2];
+  uint32_t round_flags[2]; // per-round flags / counters: components' "changed", then the AVBD colouring's uncoloured counts
+  uint32_t heavy_n;        // broad phase: heavy queries of this substep
+  uint32_t error_site;     // where the first bounded wait gave up (bb_step_stats.error_site)
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
                            // 7 connected components
@@ -327,7 +329,21 @@ __device__ __forceinline__ Sym3 body_world_inv_inertia(const float4* iinv, const
   return world_inv_inertia(q, f3(iinv[i]), tq);
 }
 
+// Sites of bounded waits, recorded in DevCounters::error_site by the first one that gives up
+// (bb_step_stats.error_site): the sort's and the scan's look-backs, the dataflow PGS wait,
+// the generation barrier, and BB_SITE_GRID + k for the grid barrier on sync_count[k] (0 edge colouring, 1
+// PGS_SOFT, 2 AVBD colouring, 3..5 AVBD solve phases, 7 connected components).
+#define BB_SITE_SORT 1u
+#define BB_SITE_FLOW 2u
+#define BB_SITE_GEN_BARRIER 3u
+#define BB_SITE_SCAN 4u
+#define BB_SITE_GRID 16u
 __device__ __forceinline__ void raise_error(DevCounters* c, uint32_t bit) { atomicOr(&c->error_flags, bit); }
+// a bounded wait at `site` (BB_SITE_*) gave up
+__device__ __forceinline__ void raise_wait_error(DevCounters* c, uint32_t site) {
+  atomicCAS(&c->error_site, 0u, site);
+  atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
+}
 
 // id of a body inside its own world (batched worlds hash world-local ids, so a world's
 // colouring does not depend on where it sits in the batch)
@@ -360,10 +376,11 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 // Bound of every grid-barrier wait: checked once per 64 polls (a barrier that completes within
 // them never reads it).  Gives up past the world's wait_limit (BB_SPIN_LIMIT when 0), raising
 // BB_ERRF_SPIN_LIMIT, or at once when another wait of the launch already gave up.
-__device__ __forceinline__ bool spin_gave_up(DevCounters* c, uint32_t spins) {
+__device__ __forceinline__ bool spin_gave_up(DevCounters* c, uint32_t spins, uint32_t site) {
   if ((spins & 63u) != 0u) return false;
   const uint32_t lim = *reinterpret_cast<volatile const uint32_t*>(&c->wait_limit);
   if (spins > (lim ? lim : BB_SPIN_LIMIT)) {
+    atomicCAS(&c->error_site, 0u, site);
     atomicOr(&c->error_flags, BB_ERRF_SPIN_LIMIT);
     return true;
   }
@@ -383,7 +400,7 @@ __device__ __forceinline__ void grid_barrier(DevCounters* c) {
     } else {
       uint32_t spins = 0;
       while (ld_acquire_gpu(&c->barrier_gen) == g)
-        if (spin_gave_up(c, ++spins)) break;
+        if (spin_gave_up(c, ++spins, BB_SITE_GEN_BARRIER)) break;
     }
     fence_acq_rel_gpu();
   }
@@ -407,7 +424,7 @@ __device__ __forceinline__ void grid_sync(DevCounters* c, uint32_t* count, uint3
     const uint32_t target = epoch * gridDim.x;
     uint32_t spins = 0;
     while (ld_acquire_gpu(count) < target)
-      if (spin_gave_up(c, ++spins)) break;
+      if (spin_gave_up(c, ++spins, BB_SITE_GRID + uint32_t(count - c->sync_count))) break;
   }
   __syncthreads();
 }
@@ -428,7 +445,7 @@ __device__ __forceinline__ void grid_wait(DevCounters* c, const uint32_t* count,
     const uint32_t target = epoch * gridDim.x;
     uint32_t spins = 0;
     while (ld_acquire_gpu(count) < target)
-      if (spin_gave_up(c, ++spins)) break;
+      if (spin_gave_up(c, ++spins, BB_SITE_GRID + uint32_t(count - c->sync_count))) break;
   }
   __syncthreads();
 }

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(BB_CC_THREADS, 1) k_components(const DevState 
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const uint32_t M = c->manifold_count;
   uint32_t* sync = &c->sync_count[7];
-  uint32_t* changed = &c->pad[2];  // two alternating per-round flags (the AVBD colouring reuses them later)
+  uint32_t* changed = c->round_flags;  // two alternating per-round flags (the AVBD colouring reuses them later)
   uint32_t ep = 0;
   uint32_t* parent = d.uf_parent;
   // Start from the last substep's roots where that is exact.  A last-substep component whose

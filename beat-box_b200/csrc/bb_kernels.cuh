@@ -52,7 +52,7 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
 void bb_solve_islands(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
                       const StepScratch& sc, int sms);
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
-                       const StepScratch& sc, int coop_blocks, int coop_stream, int sms);
+                       const StepScratch& sc, int coop_blocks, int sms);
 void bb_solve_avbd(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, const StepScratch& sc,
                    int sms, int cur, int coop_blocks);
 
@@ -74,7 +74,6 @@ void bb_sort_carve(char* base, uint32_t n, int passes, DevCounters** ctr, uint32
 // co-resident block counts of the persistent cooperative kernels
 int bb_edge_coloring_blocks(int sms);
 int bb_pgs_soft_blocks(int sms);
-int bb_pgs_stream_blocks(int sms);
 int bb_avbd_blocks(int sms);
 
 // occupancy helpers (bb_world.cu)

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ 
         uint32_t flag = uint32_t(w >> 32);
         if (flag == 0) {
           if (++spins > BB_SPIN_LIMIT) {
-            raise_error(ctr, BB_ERRF_SPIN_LIMIT);
+            raise_wait_error(ctr, BB_SITE_SCAN);
             break;
           }
           continue;
@@ -210,7 +210,7 @@ __device__ __forceinline__ uint32_t sort_lookback(volatile uint32_t* st, uint32_
     }
     j -= k;
     if (k < kLookback && ++spins > BB_SPIN_LIMIT) {
-      raise_error(ctr, BB_ERRF_SPIN_LIMIT);
+      raise_wait_error(ctr, BB_SITE_SORT);
       return excl;
     }
   }

@@ -51,6 +51,7 @@ bb_status bb_fail(bb_status code, const char* msg);
 bb_status bb_world_read_range(void* world, uint32_t first, uint32_t count, float* position, float* rotation,
                               float* velocity, float* omega, uint32_t* flags);
 const uint32_t* bb_world_error_word(void* world);
+const uint32_t* bb_world_error_site_word(void* world);
 
 namespace {
 
@@ -102,7 +103,7 @@ struct Batch {
   std::map<std::tuple<uint32_t, float, float, float>, uint32_t> shape_handle;
   uint32_t park_shape = 0;
   std::deque<cudaEvent_t> inflight;
-  uint32_t* err_host = nullptr;  // pinned copy of the batch's error word after each step
+  uint32_t* err_host = nullptr;  // pinned copies of the batch's error bits and error site after each step
   uint64_t bytes = 0, last_use = 0;
   uint32_t running = 0;
 };
@@ -115,7 +116,7 @@ struct Req {
   std::vector<bb_body_desc> bodies;
   double submit_s = 0, start_s = 0, finish_s = 0;
   bb_status result = BB_OK;
-  uint32_t error_flags = 0;
+  uint32_t error_flags = 0, error_site = 0;
   bool done = false;
   cudaEvent_t ev = nullptr;  // after the request's last step
   Batch* batch = nullptr;
@@ -250,13 +251,13 @@ struct bb_server_impl {
     }
     bb_status s = bb_set_solver_params(b->w, &p);
     if (s == BB_OK) s = bb_add_box_shape(b->w, 0.001f, 0.001f, 0.001f, &b->park_shape);
-    if (s == BB_OK && cudaMallocHost(&b->err_host, sizeof(uint32_t)) != cudaSuccess) s = BB_E_CUDA;
+    if (s == BB_OK && cudaMallocHost(&b->err_host, 2 * sizeof(uint32_t)) != cudaSuccess) s = BB_E_CUDA;
     if (s != BB_OK) {
       bb_world_destroy(b->w);
       *err = s;
       return nullptr;
     }
-    *b->err_host = 0;
+    b->err_host[0] = b->err_host[1] = 0;
     b->bytes = bb_world_device_bytes(b->w);
     held_bytes += b->bytes;
     ++st.worlds_created;
@@ -405,8 +406,9 @@ struct bb_server_impl {
       for (size_t i = 0; i < issued.size();) {
         Req* q = issued[i];
         if (cudaEventQuery(q->ev) == cudaSuccess) {
-          const uint32_t e = *q->batch->err_host;
+          const uint32_t e = q->batch->err_host[0];
           q->error_flags = e;
+          q->error_site = q->batch->err_host[1];
           bb_status res = BB_OK;
           if (e & (BB_ERRF_PAIR_OVERFLOW | BB_ERRF_CONTACT_OVERFLOW)) res = BB_E_CAPACITY;
           else if (e) res = BB_E_DEVICE_LIMIT;
@@ -463,6 +465,8 @@ struct bb_server_impl {
             bb_status s = bb_step(b->w, b->dt, b->substeps);
             cudaMemcpyAsync(b->err_host, bb_world_error_word(b->w), sizeof(uint32_t), cudaMemcpyDeviceToHost,
                             b->stream);
+            cudaMemcpyAsync(b->err_host + 1, bb_world_error_site_word(b->w), sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, b->stream);
             cudaEvent_t ev = nullptr;
             cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
             cudaEventRecord(ev, b->stream);
@@ -595,6 +599,7 @@ static void fill_status(const Req& q, bb_request_status* out) {
   out->start_s = q.start_s;
   out->finish_s = q.finish_s;
   out->error_flags = q.error_flags;
+  out->error_site = q.error_site;
 }
 
 bb_status bb_server_poll(void* server, uint64_t ticket, bb_request_status* out) {

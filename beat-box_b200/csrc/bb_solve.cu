@@ -673,105 +673,13 @@ __device__ void pgs_sweep(const DevState& d, const Params& p, int cur, int mode,
   }
 }
 
-// Streaming schedule of the same sweeps, for colours with several items per thread (worlds of a
-// few hundred thousand bodies and more).  Nothing is held across a barrier, so a thread needs
-// about half the registers and BB_PGS_STREAM_BLOCKS blocks share an SM: more warps have their
-// loads in flight.  An item's record loads while the item before it runs; then its first four
-// contacts' rows and impulses are copied into the thread's shared-memory slot with cp.async
-// while its masses, frame and bodies load, so the item waits for one round trip.  The
-// arithmetic is the same calls in the same order as pgs_item_compute: the same bits.
-#ifndef BB_PGS_STREAM_BLOCKS
-#define BB_PGS_STREAM_BLOCKS 3
-#endif
-#define BB_PGS_STREAM_MIN_BODIES 262144u  // BB_PGS_PIPE_AUTO's switch to streaming
-#define BB_PGS_STREAM_HELD 4              // contacts per item staged in shared memory
-#define BB_PGS_STREAM_SMEM (BB_PGS_THREADS * BB_PGS_STREAM_HELD * 4 * 16)
-__device__ __forceinline__ float4* pgs_stream_base() {  // element e of thread t at e * BB_PGS_THREADS + t
-  extern __shared__ float4 s_pgs_extra[];
-  return s_pgs_extra + threadIdx.x;
-}
-__device__ __forceinline__ void pgs_item_stream(const DevState& d, const Params& p, uint4 r, uint32_t k, int mode) {
-  if (r.w & BB_PGS_SKIP) return;
-  const bool accum = p.flags & BB_SIM_ACCUM_IMPULSE, fric = p.flags & BB_SIM_FRICTION;
-  if (mode == 0 && !accum) return;
-  const uint32_t a = r.y, b = r.z, c0 = r.x, cc = r.w & 0xFFu, T = BB_PGS_THREADS;
-  float4* sb = pgs_stream_base();
-  const uint32_t held = min(cc, uint32_t(BB_PGS_STREAM_HELD));
-  for (uint32_t j = 0; j < held; ++j) {
-    cp_async16(sb + (4 * j + 0) * T, d.c_r1 + c0 + j);
-    cp_async16(sb + (4 * j + 1) * T, d.c_r2 + c0 + j);
-    if (mode != 0) cp_async16(sb + (4 * j + 2) * T, d.c_k + c0 + j);
-    cp_async16(sb + (4 * j + 3) * T, d.pgs_lam + c0 + j);
-  }
-  cp_async_commit();
-  const float4 m4 = d.pgs_mass[k];
-  const float3 n = f3(d.pgs_frame[3 * k]), t0 = f3(d.pgs_frame[3 * k + 1]), t1 = f3(d.pgs_frame[3 * k + 2]);
-  const PgsBodies B = pgs_bodies_load(d, a, b);
-  const float4 va4 = B.va, vb4 = B.vb;
-  float3 va = f3(va4), wa = f3(B.wa), vb = f3(vb4), wb = f3(B.wb);
-  const Sym3 IA{B.ia0.x, B.ia0.y, B.ia0.z, B.ia0.w, B.ia1.x, B.ia1.y};
-  const Sym3 IB{B.ib0.x, B.ib0.y, B.ib0.z, B.ib0.w, B.ib1.x, B.ib1.y};
-  const float ima = m4.x, imb = m4.y, mu = m4.z;
-  cp_async_wait_all();
-  for (uint32_t j = 0; j < cc; ++j) {
-    const bool sm = j < held;
-    const float4 R1 = sm ? sb[(4 * j + 0) * T] : d.c_r1[c0 + j], R2 = sm ? sb[(4 * j + 1) * T] : d.c_r2[c0 + j];
-    float4 lam = sm ? sb[(4 * j + 3) * T] : d.pgs_lam[c0 + j];
-    if (mode == 0) {
-      pgs_contact_warm(f3(R1), f3(R2), lam, n, t0, t1, fric, ima, imb, IA, IB, va, wa, vb, wb);
-    } else {
-      const float4 K = sm ? sb[(4 * j + 2) * T] : d.c_k[c0 + j];
-      pgs_contact_solve(R1, R2, K, lam, n, t0, t1, mu, mode == 1, accum, fric, ima, imb, IA, IB, va, wa, vb, wb);
-      d.pgs_lam[c0 + j] = lam;
-    }
-  }
-  if (r.w & (1u << 8)) {
-    d.vel[a] = f4(va, va4.w);
-    d.omega[a] = f4(wa, 0.f);
-  }
-  if (r.w & (1u << 9)) {
-    d.vel[b] = f4(vb, vb4.w);
-    d.omega[b] = f4(wb, 0.f);
-  }
-}
-
-// one sweep over colours 0..C-1 and the overflow bucket, streaming (barriers as in pgs_sweep)
-__device__ __forceinline__ void pgs_sweep_stream(const DevState& d, const Params& p, int mode, const uint32_t* bs, const uint32_t* aw,
-                                 uint32_t C, uint32_t& epoch) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  uint32_t* sync = &d.ctr->sync_count[1];
-  for (uint32_t c = 0; c < C; ++c) {
-    if (!aw[c]) continue;
-    const uint32_t end = bs[c + 1];
-    uint32_t k = bs[c] + tid;
-    uint4 r = k < end ? d.pgs_rec[k] : make_uint4(0, 0, 0, 0);
-    while (k < end) {
-      const uint32_t kn = k + stride;
-      const uint4 rn = kn < end ? d.pgs_rec[kn] : make_uint4(0, 0, 0, 0);
-      pgs_item_stream(d, p, r, k, mode);
-      r = rn;
-      k = kn;
-    }
-    uint32_t ne = c + 1;
-    while (ne < C && !aw[ne]) ++ne;
-    const bool local = ne < C && bs[c + 1] - bs[c] <= blockDim.x && bs[ne + 1] - bs[ne] <= blockDim.x;
-    if (local) __syncthreads();
-    else grid_sync(d.ctr, sync, epoch);
-  }
-  const uint32_t o0 = bs[BB_MAX_COLORS], o1 = bs[BB_MAX_COLORS + 1];
-  if (o0 != o1) {  // overflow bucket: serial, in manifold order
-    if (tid == 0)
-      for (uint32_t k = o0; k < o1; ++k) pgs_item_stream(d, p, d.pgs_rec[k], k, mode);
-    grid_sync(d.ctr, sync, epoch);
-  }
-}
-
 // PF = 4 contacts held per item (one 255-register block per SM).  Holding fewer would let
 // two blocks share an SM but puts the other contacts' loads on the critical path, one round
-// trip each.  STREAM: the streaming schedule above instead (PF and STAGE_NEXT unused).
-template <int PF, bool STAGE_NEXT, bool STREAM = false>
-__global__ void __launch_bounds__(BB_PGS_THREADS, STREAM ? BB_PGS_STREAM_BLOCKS : (PF == 4 ? 1 : 2))
-    k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
+// trip each.  A streaming variant that held nothing across barriers (each item's contacts
+// copied to shared memory by cp.async while its bodies load) ran 2 or 3 blocks per SM and
+// measured slower on the 1M-box pyramids (solve 3.32 and 6.55 against 3.23 ms per substep).
+template <int PF, bool STAGE_NEXT>
+__global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(const DevState d, Params p, int cur, uint32_t n, float h) {
   __shared__ uint32_t bs[BB_MAX_COLORS + 2];
   __shared__ uint32_t aw[BB_MAX_COLORS + 1];
   // test switch (bb_debug_wait_limit): the last block leaves, so the others' first grid barrier
@@ -794,32 +702,21 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, STREAM ? BB_PGS_STREAM_BLOCKS 
     for (uint32_t k = bs[c] + tid; k < bs[c + 1]; k += stride) pgs_item_build(d, cur, k, list[k], h, hertz);
   if (tid == 0)
     for (uint32_t k = bs[BB_MAX_COLORS]; k < bs[BB_MAX_COLORS + 1]; ++k) pgs_item_build(d, cur, k, list[k], h, hertz);
-  if constexpr (STREAM) {
-    pgs_sweep_stream(d, p, 0, bs, aw, C, epoch);
-    for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep_stream(d, p, 1, bs, aw, C, epoch);
-    if (p.flags & BB_SIM_ADVECTION) {
-      for (uint32_t i = tid; i < n; i += stride)
-        if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
-      grid_sync(d.ctr, sync, epoch);
-    }
-    for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep_stream(d, p, 2, bs, aw, C, epoch);
-  } else {
-    PgsItem<PF> x;
-    uint4 rec_next = make_uint4(0, 0, 0, 0);
-    if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, bs[0] + tid, x);
-    if (C > 0) {
-      const uint32_t c1 = pgs_next_colour(0, C);
-      if (bs[c1] + tid < bs[c1 + 1]) rec_next = d.pgs_rec[bs[c1] + tid];
-    }
-    pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 0, bs, aw, C, x, rec_next, epoch);
-    for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 1, bs, aw, C, x, rec_next, epoch);
-    if (p.flags & BB_SIM_ADVECTION) {
-      for (uint32_t i = tid; i < n; i += stride)
-        if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
-      grid_sync(d.ctr, sync, epoch);
-    }
-    for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 2, bs, aw, C, x, rec_next, epoch);
+  PgsItem<PF> x;
+  uint4 rec_next = make_uint4(0, 0, 0, 0);
+  if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, bs[0] + tid, x);
+  if (C > 0) {
+    const uint32_t c1 = pgs_next_colour(0, C);
+    if (bs[c1] + tid < bs[c1 + 1]) rec_next = d.pgs_rec[bs[c1] + tid];
   }
+  pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 0, bs, aw, C, x, rec_next, epoch);
+  for (uint32_t it = 0; it < p.iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 1, bs, aw, C, x, rec_next, epoch);
+  if (p.flags & BB_SIM_ADVECTION) {
+    for (uint32_t i = tid; i < n; i += stride)
+      if (awake(d.flags[i])) pgs_integrate(d, i, h, tq);
+    grid_sync(d.ctr, sync, epoch);
+  }
+  for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 2, bs, aw, C, x, rec_next, epoch);
   // impulses back to the persistent contacts (every sweep ended with a grid barrier)
   const uint32_t M = d.ctr->manifold_count;
   for (uint32_t k = tid; k < M; k += stride) {
@@ -853,7 +750,7 @@ __device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ void flow_wait(DevCounters* c, const uint32_t* ctr, uint32_t target) {
   uint32_t spins = 0;
   while (ld_acquire_gpu(ctr) < target)
-    if (spin_gave_up(c, ++spins)) return;
+    if (spin_gave_up(c, ++spins, BB_SITE_FLOW)) return;
 }
 
 // per colour-ordered item k: (rank_a | rank_b << 16, deg_a | deg_b << 16) where rank_x is the
@@ -956,18 +853,8 @@ int bb_pgs_soft_blocks(int sms) {
   return bb_coop_blocks((const void*)k_pgs_soft<4, false>, BB_PGS_THREADS, sms);
 }
 
-// grid of the streaming schedule: BB_PGS_STREAM_BLOCKS blocks per SM (fewer if the occupancy
-// calculator says they do not fit: the launch is cooperative)
-int bb_pgs_stream_blocks(int sms) {
-  const void* kern = (const void*)k_pgs_soft<4, false, true>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, BB_PGS_STREAM_SMEM);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BB_PGS_THREADS, BB_PGS_STREAM_SMEM);
-  return sms * std::max(1, std::min(per_sm, BB_PGS_STREAM_BLOCKS));
-}
-
 void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, float h, int cur,
-                       const StepScratch& sc, int coop_blocks, int coop_stream, int sms) {
+                       const StepScratch& sc, int coop_blocks, int sms) {
   cudaMemsetAsync(d.colour_awake, 0, sizeof(uint32_t) * (BB_MAX_COLORS + 1), s);
   k_pgs_count<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
   bb_launch_scan(s, d.pgs_cnt, d.pgs_coff, &d.ctr->manifold_count, d.pair_capacity, &d.ctr->pgs_contacts,
@@ -991,15 +878,10 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
-  // Item pipeline: held items for worlds whose colours give a thread about one item (the
-  // barrier latency dominates), streaming where threads run several items per colour; staging
-  // the next item needs 112 KB more shared memory (less L1).  The autotuner measures all three.
-  uint32_t pipe = p.pgs_stage_next;
-  if (pipe == BB_PGS_PIPE_AUTO) pipe = n >= BB_PGS_STREAM_MIN_BODIES ? BB_PGS_PIPE_STREAM : BB_PGS_PIPE_HELD;
-  if (pipe == BB_PGS_PIPE_STAGED)
+  // staging the next item needs 112 KB more shared memory (less L1): it pays when threads run
+  // several items per colour (large worlds), which is what the autotuner measures
+  if (p.pgs_stage_next)
     bb_launch_coop((const void*)k_pgs_soft<4, true>, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
-  else if (pipe == BB_PGS_PIPE_STREAM)
-    bb_launch_coop((const void*)k_pgs_soft<4, false, true>, coop_stream, BB_PGS_THREADS, args, s, BB_PGS_STREAM_SMEM);
   else bb_launch_coop((const void*)k_pgs_soft<4, false>, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM_EXTRA);
 }
 
@@ -1210,7 +1092,7 @@ __device__ __forceinline__ float3 avbd_q_rotate(Quatf q, float3 u) {
 __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_color(const DevState d, Params p, int cur, uint32_t n) {
   DevCounters* c = d.ctr;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  uint32_t* uncol = &c->pad[2];
+  uint32_t* uncol = c->round_flags;
   uint32_t* sync = &c->sync_count[2];
   uint32_t ep = 0;
   for (uint32_t i = tid; i < n; i += stride) d.body_color[i] = BB_UNCOLORED;
@@ -1295,7 +1177,11 @@ __global__ void k_avbd_warmstart(const DevState d, Params p, int cur) {
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
     const uint32_t slot = d.man_slot[cur][m];
     const uint2 b = d.m_bodies[cur][slot];
-    bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
+    const uint32_t fa = d.flags[b.x], fb = d.flags[b.y];
+    // a paused world's manifolds are carried unchanged (no penalty decay, no new anchors), so
+    // the world resumes exactly as it stopped
+    if ((fa | fb) & BB_BODY_PAUSED) continue;
+    bool d1 = awake(fa), d2 = awake(fb);
     float3 c1 = d1 ? f3(d.a_pos_start[b.x]) : f3(d.pos[b.x]);
     float3 c2 = d2 ? f3(d.a_pos_start[b.y]) : f3(d.pos[b.y]);
     Quatf q1c = q_conj(d1 ? q_from(d.a_rot_start[b.x]) : q_from(d.rot[b.x]));

@@ -248,7 +248,9 @@ __global__ void k_begin_substep(DevCounters* c) {
   c->avbd_violations = 0;
   c->stick = 0;
   c->barrier_count = 0;
-  for (int k = 0; k < 6; ++k) c->pad[k] = 0;
+  c->round_flags[0] = 0;
+  c->round_flags[1] = 0;
+  c->heavy_n = 0;
   for (int k = 0; k < 8; ++k) c->sync_count[k] = 0;
   c->np_counts[0] = 0;
   c->np_counts[1] = 0;
@@ -291,7 +293,7 @@ struct bb_world_impl {
   int last_cur = 0;  // manifold buffer the last (partial or full) substep wrote
   bool skip_warm_once = false;
   bool ran_any = false;
-  int coop_edge = 0, coop_pgs = 0, coop_pgs_stream = 0, coop_avbd = 0, coop_cc = 0;
+  int coop_edge = 0, coop_pgs = 0, coop_avbd = 0, coop_cc = 0;
   size_t scratch_bytes = 0;
   void* scratch_base = nullptr;
   size_t dev_bytes = 0;  // device memory held by this world
@@ -534,7 +536,7 @@ struct bb_world_impl {
     if (coloured || params.solver == BB_SOLVER_AVBD) bb_edge_coloring(stream, d, params, n, sc, sms, cur, coop_edge);
     if (params.solver == BB_SOLVER_AVBD) bb_solve_avbd(stream, d, params, n, h, sc, sms, cur, coop_avbd);
     else if (!coloured) bb_solve_islands(stream, d, params, n, h, cur, sc, sms);
-    else bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, coop_pgs_stream, sms);
+    else bb_solve_pgs_soft(stream, d, params, n, h, cur, sc, coop_pgs, sms);
     if (commit) parity = cur;
   }
 };
@@ -648,7 +650,6 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   };
   w->coop_edge = fit(bb_edge_coloring_blocks(w->sms), w->cap_n, 1024);
   w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), w->cap_n / 2, 256);
-  w->coop_pgs_stream = fit(bb_pgs_stream_blocks(w->sms), w->cap_n / 2, 256);
   w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n / 2, 512);
   w->coop_cc = fit(bb_components_blocks(w->sms), w->cap_n, 512);
   cudaError_t e = cudaStreamSynchronize(w->stream);  // the zero fills (no device-wide wait)
@@ -716,6 +717,7 @@ bb_status bb_world_clear(void* world) {
   // device error bits of earlier steps go with the bodies
   CU(cudaMemsetAsync(&w->d.ctr->front_valid, 0, sizeof(uint32_t), w->stream));
   CU(cudaMemsetAsync(&w->d.ctr->error_flags, 0, sizeof(uint32_t), w->stream));
+  CU(cudaMemsetAsync(&w->d.ctr->error_site, 0, sizeof(uint32_t), w->stream));
   CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
@@ -1085,8 +1087,8 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
     if (!(p->world_extent[k] > 0)) return fail(BB_E_INVALID, "world_extent must be positive");
   if (p->schedule > BB_SCHEDULE_COLOUR_BARRIER) return fail(BB_E_INVALID, "unknown schedule");
   if ((p->broad_threads != 0 && p->broad_threads != 32 && p->broad_threads != 64 && p->broad_threads != 128) ||
-      p->narrow_blocks_per_sm > 64 || p->pgs_stage_next > BB_PGS_PIPE_HELD)
-    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, pgs_stage_next 0..3)");
+      p->narrow_blocks_per_sm > 64 || p->pgs_stage_next > 1)
+    return fail(BB_E_INVALID, "launch geometry out of range (broad_threads 32/64/128, narrow <= 64, pgs_stage_next 0/1)");
   // contact geometry depends on these: no pair keeps last substep's manifolds as they were
   if (p->quirks != w->params.quirks || p->penetration_cap != w->params.penetration_cap)
     CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * (w->cap_n + 1), w->stream));
@@ -1201,7 +1203,7 @@ bb_status bb_step(void* world, float dt, uint32_t substeps) {
       cudaEventRecord(ev[10], w->stream);
       if (w->params.solver == BB_SOLVER_AVBD) bb_solve_avbd(w->stream, w->d, w->params, w->n, h, w->sc, w->sms, cur, w->coop_avbd);
       else if (!coloured) bb_solve_islands(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->sms);
-      else bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->coop_pgs_stream, w->sms);
+      else bb_solve_pgs_soft(w->stream, w->d, w->params, w->n, h, cur, w->sc, w->coop_pgs, w->sms);
       cudaEventRecord(ev[11], w->stream);
       CU(cudaEventSynchronize(ev[11]));
       for (int k = 0; k < kStages; ++k) {
@@ -1373,6 +1375,7 @@ bb_status bb_read_stats(void* world, bb_step_stats* s) {
   s->substeps_run = c.substeps;
   s->solved_manifolds = c.pgs_manifolds;
   s->solved_contacts = c.pgs_contacts;
+  s->error_site = c.error_site;
   return BB_OK;
 }
 
@@ -1694,6 +1697,7 @@ bb_status bb_world_read_range(void* world, uint32_t first, uint32_t count, float
 
 // device word of the world's sticky error bits (BB_ERRF_*)
 const uint32_t* bb_world_error_word(void* world) { return world ? &W(world)->d.ctr->error_flags : nullptr; }
+const uint32_t* bb_world_error_site_word(void* world) { return world ? &W(world)->d.ctr->error_site : nullptr; }
 
 
 // ---- autotuner ------------------------------------------------------------------------------
@@ -1738,7 +1742,7 @@ bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_s
       {&bb_solver_params::schedule, {BB_SCHEDULE_DATAFLOW, BB_SCHEDULE_COLOUR_BARRIER}, true, false},
       {&bb_solver_params::broad_threads, {32, 64, 128}, false, false},
       {&bb_solver_params::narrow_blocks_per_sm, {4, 8, 16, 32}, false, false},
-      {&bb_solver_params::pgs_stage_next, {BB_PGS_PIPE_HELD, BB_PGS_PIPE_STREAM, BB_PGS_PIPE_STAGED}, true, true},
+      {&bb_solver_params::pgs_stage_next, {0, 1}, true, true},
   };
   for (const Axis& ax : axes) {
     if (st != BB_OK) break;

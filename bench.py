@@ -139,13 +139,10 @@ def timed_window(args) -> int:
     return max(args.warmup, run_steps(args) // 2 - args.steps // 2)
 
 
-PGS_PIPES = {"auto": 0, "staged": 1, "stream": 2, "held": 3}  # bb_solver_params.pgs_stage_next
-
-
 def solver_fields(args) -> dict:
     if args.solver == "pgs":
         return dict(solver=1, iterations=pgs_iterations(args), relax_iterations=pgs_iterations(args), quirks=0,
-                    schedule=0 if args.schedule == "dataflow" else 1, pgs_stage_next=PGS_PIPES[args.pgs_pipe])
+                    schedule=0 if args.schedule == "dataflow" else 1)
     return dict(solver=2, avbd_iterations=4, avbd_beta=10.0, quirks=0)
 
 
@@ -481,7 +478,6 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                 "data": "synthetic (seeded scene, seed 0)",
                 "config": {"workload": name, "bodies": n, "substeps": SUBSTEPS, "dt": DT,
                            "parallelism": f"replicas x{world_size}", "l2": "flushed before every timed step",
-                           "pgs_pipe": args.pgs_pipe if args.solver == "pgs" else None,
                            "timed_steps": f"steps {first}..{first + args.steps - 1} of the {run_steps(args)}-step run "
                                           f"(after {first} untimed steps from rest, the last {args.warmup} of them "
                                           f"the warm-up)"},
@@ -697,9 +693,10 @@ def run_served(args, rank: int, world_size: int, local_rank: int):
         for r in res:
             if r["result"] != bb.OK:
                 codes[str(r["result"])] = codes.get(str(r["result"]), 0) + 1
-                flags[str(r["error_flags"])] = flags.get(str(r["error_flags"]), 0) + 1
+                fk = f'{r["error_flags"]}@{r["error_site"]}'
+                flags[fk] = flags.get(fk, 0) + 1
         per_rate.append({"rate_req_s": lam, "requests": len(res), "failed": len(res) - len(ok), "fail_codes": codes,
-                         "fail_error_flags": flags,
+                         "fail_error_flags_at_site": flags,
                          "body_steps_per_s": bodies / span if span > 0 else None,
                          "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
                          "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
@@ -737,8 +734,6 @@ def main():
                          "column; box_grid: the 1000-box grid; voxel_pile: concave voxel bodies")
     ap.add_argument("--schedule", default="barrier", choices=["dataflow", "barrier"],
                     help="PGS schedule: per-body dataflow counters or a grid barrier per colour")
-    ap.add_argument("--pgs-pipe", default="auto", choices=list(PGS_PIPES),
-                    help="colour-sweep item pipeline (same results): auto (by world size), held, staged, stream")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "sort"],
                     help="plain: one world (default); batched: config-4 batch of independent worlds; "
                          "served: config-5 serving loop; sort: the a4 pair sort alone on --sort-keys keys")

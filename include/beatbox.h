@@ -105,19 +105,6 @@ typedef int32_t bb_status;
  * bb_default_solver_params) is the reference value; replaces StatusManager::set_solver /
  * flag toggles (src/status_manager.hpp:204-373) and the compile-time constants of
  * include/shared.inl:77-83,760-839 and include/defines.hpp:352-364. */
-/* Item pipelines of the colour-barrier PGS_SOFT sweeps (bb_solver_params.pgs_stage_next); the
- * results are the same bits for each.  HELD: a thread holds its next colour's item (up to four
- * contacts) in registers across the barrier, one block per SM -- for colours of about one item
- * per thread, where the barrier latency dominates.  STAGED: HELD plus the thread's next item of
- * the same colour copied into shared memory while the current one computes.  STREAM: nothing
- * held, two blocks per SM, each contact's rows loaded while the one before computes -- for
- * colours of several items per thread.  AUTO: STREAM for worlds of 262,144 bodies or more, else
- * HELD. */
-#define BB_PGS_PIPE_AUTO 0u
-#define BB_PGS_PIPE_STAGED 1u
-#define BB_PGS_PIPE_STREAM 2u
-#define BB_PGS_PIPE_HELD 3u
-
 typedef struct bb_solver_params {
   uint32_t solver;             /* BB_SOLVER_* (default AVBD) */
   uint32_t flags;              /* BB_SIM_* (default BB_SIM_DEFAULT_FLAGS) */
@@ -151,7 +138,8 @@ typedef struct bb_solver_params {
   /* launch geometry (results are identical for every value; 0 = default; bb_autotune picks) */
   uint32_t broad_threads;        /* broad-phase block size: 32, 64 or 128 (default 128) */
   uint32_t narrow_blocks_per_sm; /* narrow-phase grid, 128-thread blocks per SM: 1..64 (default 16) */
-  uint32_t pgs_stage_next;       /* colour-barrier PGS_SOFT item pipeline, BB_PGS_PIPE_* (default AUTO) */
+  uint32_t pgs_stage_next;       /* colour-barrier PGS_SOFT: 1 stages each thread's next item of a colour in shared
+                                    memory while the current one computes (large worlds); 0 loads it after (default) */
   /* Morton normalisation */
   uint32_t bounds_mode;        /* BB_BOUNDS_* */
   float world_min[3];          /* default -64 */
@@ -211,6 +199,10 @@ typedef struct bb_step_stats {
   uint32_t substeps_run;          /* substeps run since the world was created */
   uint32_t solved_manifolds;      /* last substep's colour sweeps: manifolds with an awake body */
   uint32_t solved_contacts;       /* and their contacts (0 under AVBD and the per-island path) */
+  uint32_t error_site;            /* where the first bounded wait gave up (BB_ERRF_SPIN_LIMIT): 0 none,
+                                     1 sort look-back, 2 dataflow PGS wait, 3 generation barrier, 4 scan
+                                     look-back, 16 + k grid barrier k (0 edge colouring, 1 PGS_SOFT, 2 AVBD
+                                     colouring, 3..5 AVBD solve phases, 7 connected components) */
 } bb_step_stats;
 
 /* device error bits (bb_step_stats.error_flags) */
@@ -520,7 +512,7 @@ typedef struct bb_request_status {
   double start_s;
   double finish_s;
   uint32_t error_flags; /* BB_ERRF_* seen in the world's batch by the end of the request's last step */
-  uint32_t reserved;
+  uint32_t error_site;  /* bb_step_stats.error_site of the batch at that point */
 } bb_request_status;
 
 typedef struct bb_server_stats {

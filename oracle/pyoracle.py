@@ -41,7 +41,8 @@ class StepStats(ctypes.Structure):
         "graph_color_count", "graph_color_overflow", "graph_color_violations", "avbd_color_count",
         "avbd_violations", "sleeping_count", "fresh_contacts", "stick_count")] + [
         ("max_penetration", ctypes.c_float), ("error_flags", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
-        ("substeps_run", ctypes.c_uint32), ("solved_manifolds", ctypes.c_uint32), ("solved_contacts", ctypes.c_uint32)]
+        ("substeps_run", ctypes.c_uint32), ("solved_manifolds", ctypes.c_uint32), ("solved_contacts", ctypes.c_uint32),
+        ("error_site", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}

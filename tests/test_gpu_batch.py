@@ -149,18 +149,15 @@ def test_dataflow_schedule_equals_colour_barrier(name):
 
 
 @pytest.mark.parametrize("name", ["mixed_3000", "pyramids_200x1000"])
-def test_item_pipelines_give_the_same_bits(name):
-    """The colour-barrier sweeps' three item pipelines -- the next colour's item held in registers
-    across the barrier, that plus the thread's next item of the same colour staged in shared
-    memory, and streaming (nothing held, two blocks per SM, rows loaded contact by contact) --
-    run the same arithmetic on the same data in the same order.  In the 200k-box pyramids (over
-    400k manifolds in about a dozen colours) threads run several items of the largest colours, so
-    the staged and streaming loops carry them; the 3000-body column has colours of a few hundred
-    items, where the CTA-barrier shortcut and the overflow bucket come in."""
+def test_staging_the_next_item_equals_loading_it(name):
+    """The colour-barrier kernel that stages each thread's next item of a colour in shared memory
+    while the current one computes runs the same arithmetic on the same data.  In the 200k-box
+    pyramids (over 400k manifolds in about a dozen colours, on at most 148 x 256 threads) the
+    threads run several items of the largest colours, so the staged path carries them."""
     big = name == "pyramids_200x1000"
     sc = scenes.pyramids(n_pyramids=200, boxes_per=1000, seed=0) if big else scenes.mixed_column(n_bodies=3000, seed=2)
     outs = []
-    for stage in (bb.PGS_PIPE_HELD, bb.PGS_PIPE_STAGED, bb.PGS_PIPE_STREAM):
+    for stage in (0, 1):
         p = params(bb.SOLVER_PGS_SOFT, schedule=bb.SCHEDULE_COLOUR_BARRIER, pgs_stage_next=stage)
         w = bb.world_from_scene(sc, params=p)
         for _ in range(4 if big else 40):
@@ -308,6 +305,35 @@ def test_paused_world_resumes_as_if_never_paused(solver):
         n = int(sc["n"])
         for key in ref:
             assert np.array_equal(st[key][firsts[k]:firsts[k] + n], ref[key]), (k, key)
+
+
+@pytest.mark.parametrize("solver", [bb.SOLVER_PGS_SOFT, bb.SOLVER_AVBD])
+def test_paused_world_is_unchanged_by_a_world_added_meanwhile(solver):
+    """A pile in contact with the ground is paused after 8 steps; another world joins the batch
+    and the batch steps 3 times; after the pile resumes and steps twice it equals the same pile
+    stepped 10 times alone (its contacts, penalties and anchors were carried untouched)."""
+    a, b = scenes.pile(900, seed=4), scenes.pile(1000, seed=5)
+    p = params(solver)
+    w = bb.World(int(a["n"]) + int(b["n"]))
+    fa = w.add_world(a, *a["bounds"])[1]
+    w.set_params(p)
+    for _ in range(8):
+        w.step(DT, 2)
+    assert w.stats()["manifold_count"] > 0
+    w.pause_world(0)
+    w.add_world(b, *b["bounds"])
+    for _ in range(3):
+        w.step(DT, 2)
+    w.pause_world(0, False)
+    for _ in range(2):
+        w.step(DT, 2)
+    st = w.read_state()
+    assert w.stats()["error_flags"] == 0
+    w.close()
+    ref = alone(a, p, 10, 2)
+    n = int(a["n"])
+    for key in ref:
+        assert np.array_equal(st[key][fa:fa + n], ref[key]), key
 
 
 def test_refilled_slot_steps_like_a_world_added():

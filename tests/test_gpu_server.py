@@ -76,7 +76,7 @@ def test_tight_budget_evicts_idle_worlds_and_keeps_serving():
         for w, sc in enumerate(worlds):
             tickets.append(srv.submit(7 + w, 3, req_params(rnd), DT, 2, scene=sc if rnd == 0 else None))
     res = [srv.wait(t) for t in tickets]
-    assert all(r["result"] == bb.OK for r in res), [(r["result"], r["error_flags"]) for r in res if r["result"] != bb.OK]
+    assert all(r["result"] == bb.OK for r in res), [(r["result"], r["error_flags"], r["error_site"]) for r in res if r["result"] != bb.OK]
     st = srv.stats()
     assert st["evictions"] > 0 and st["resident_bytes"] <= 2.5 * per_world
     for w, sc in enumerate(worlds):
@@ -143,7 +143,7 @@ def test_served_worlds_match_the_fp64_oracle_on_a_sampled_one_percent(oracle_lib
             key, k = known[int(rng.integers(0, len(known)))]
             tickets.append(srv.submit(key, int(rng.integers(1, 30)), params, DT, 2))
     res = [srv.wait(t) for t in tickets]
-    assert all(r["result"] == bb.OK for r in res), [(r["result"], r["error_flags"]) for r in res if r["result"] != bb.OK]
+    assert all(r["result"] == bb.OK for r in res), [(r["result"], r["error_flags"], r["error_site"]) for r in res if r["result"] != bb.OK]
     assert len(sampled) >= 2
     ge, fe, pos_ok = [], [], []
     for key, sc, params in sampled:
