@@ -46,7 +46,7 @@ struct DevCounters {
   uint32_t gc_colors;
   uint32_t gc_overflow;
   uint32_t gc_violations;
-  uint32_t gc_uncolored;   // working counter of the colouring rounds
+  uint32_t gc_rounds_run;  // colouring rounds the last edge colouring ran
   uint32_t avbd_colors;
   uint32_t avbd_violations;
   uint32_t stick;

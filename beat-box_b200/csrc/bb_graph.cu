@@ -332,6 +332,7 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   // block barriers (the other blocks go straight to the final grid barrier): the same rounds
   // on the same sets, so the same colours, without two grid barriers per round.
   bool local = false;
+  uint32_t ran = 0;
   for (uint32_t r = 1; r <= p.gc_rounds; ++r) {
     const uint32_t* L = r == 1 && n1 == M ? nullptr : d.gc_list[r & 1];
     const uint32_t nL = r == 1 ? n1 : *(volatile uint32_t*)&c->gc_list_n[r & 1];
@@ -340,6 +341,7 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
       local = true;
       if (blockIdx.x != 0) break;
     }
+    ran = r;
     const uint32_t rtid = local ? threadIdx.x : tid, rstride = local ? blockDim.x : stride;
     if (rtid == 0) c->gc_list_n[(r + 1) & 1] = 0;  // the list this round fills (last read two rounds ago)
     const unsigned long long tag = (unsigned long long)(epoch + r) << 32;
@@ -430,6 +432,7 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
     else grid_sync(c, sync, ep);
   }
   if (local) grid_sync(c, sync, ep);  // block 0's rounds are done before anyone reads the colours
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->gc_rounds_run = ran;
   // Keys: colour, 32 = overflow, 33 = not swept.  Under the colour-barrier schedule a coloured
   // manifold whose two bodies are both asleep or static is also keyed 33: its sweep items would
   // do nothing (both bodies are frozen this substep), and leaving them out of the colour lists

@@ -51,6 +51,8 @@ bb_status bb_fail(bb_status code, const char* msg);
 bb_status bb_world_read_range(void* world, uint32_t first, uint32_t count, float* position, float* rotation,
                               float* velocity, float* omega, uint32_t* flags);
 const uint32_t* bb_world_error_word(void* world);
+bb_status bb_world_move_in(void* dst_world, uint32_t widx, const bb_batch_world_desc* desc, void* src_world,
+                           uint32_t src_widx, uint32_t count);
 const uint32_t* bb_world_error_site_word(void* world);
 
 namespace {
@@ -293,16 +295,27 @@ struct bb_server_impl {
   // world wr into slot k of batch b: a refill of a used slot, or a new world of the batch
   // padded to the slot's size with parked bodies
   bb_status place(Batch* b, uint32_t k, WorldRec* wr) {
+    // A world still resident in a batch of another step class moves by device copies (same
+    // stream, so after that batch's queued steps); its host copy is stale and not needed.
+    Batch* from = wr->batch;
     std::vector<bb_body_desc> bodies;
-    bb_status s = batch_bodies(b, wr, bodies);
-    if (s != BB_OK) return s;
+    bb_status s = BB_OK;
+    if (from) {
+      bodies.resize(b->slot_cap);  // a new slot starts parked, then takes the moved bodies
+    } else {
+      s = batch_bodies(b, wr, bodies);
+      if (s != BB_OK) return s;
+    }
     bb_batch_world_desc wd = {};
     std::memcpy(wd.world_min, wr->wmin, sizeof(wd.world_min));
     std::memcpy(wd.world_extent, wr->wext, sizeof(wd.world_extent));
-    if (k < b->slots.size()) {
+    const uint32_t n_real = uint32_t(wr->bodies.size());
+    if (from && k < b->slots.size()) {
+      s = bb_world_move_in(b->w, k, &wd, from->w, wr->slot, n_real);
+    } else if (k < b->slots.size()) {
       s = bb_world_refill(b->w, k, &wd, bodies.data(), uint32_t(bodies.size()));
     } else {
-      const uint32_t n = uint32_t(bodies.size());
+      const uint32_t n = from ? 0u : uint32_t(bodies.size());
       bodies.resize(b->slot_cap);
       for (uint32_t i = n; i < b->slot_cap; ++i) {
         bb_body_desc& d = bodies[i];
@@ -316,8 +329,10 @@ struct bb_server_impl {
       uint32_t widx = 0, first = 0;
       s = bb_add_world(b->w, &wd, bodies.data(), b->slot_cap, &widx, &first);
       if (s == BB_OK) b->slots.emplace_back();
+      if (s == BB_OK && from) s = bb_world_move_in(b->w, k, &wd, from->w, wr->slot, n_real);
     }
     if (s != BB_OK) return s;
+    if (from) from->slots[wr->slot].world = nullptr;
     b->slots[k].world = wr;
     wr->batch = b;
     wr->slot = k;
@@ -335,7 +350,8 @@ struct bb_server_impl {
       if (s != BB_OK) *fail = s;
       return true;
     }
-    if (b) save_world(wr);  // another step class: it moves (its warm starts restart)
+    // otherwise it moves to a batch of its new step class (its warm starts restart there); it
+    // stays registered in its old slot until placed, so a batch destroyed to make room saves it
     const uint32_t cls = class_of(uint32_t(wr->bodies.size()));
     Batch* best = nullptr;
     uint32_t best_k = 0;

@@ -11,6 +11,7 @@
 // the device.  Persistent solver kernels are launched cooperatively.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -147,6 +148,66 @@ __global__ void k_extend_contacts(const DevState d, uint32_t o, uint32_t count) 
   d.frozen[o + i] = 0;
   if (i == 0) d.ctr->front_valid = 0;
   for (int k = 0; k < 2; ++k) d.csr_start[k][o + 1 + i] = d.csr_start[k][o];
+}
+
+// host-side counts and one world's range and Morton box of a batch, as kernel parameters (no
+// host buffer to keep alive while the stream catches up)
+__global__ void k_set_counts(const DevState d, uint32_t n, uint32_t n_dyn) {
+  d.ctr->n_bodies = n;
+  d.ctr->n_dynamic = n_dyn;
+}
+__global__ void k_set_world(const DevState d, uint32_t widx, uint32_t first, uint32_t count, float4 lo, float4 ext) {
+  d.world_first[widx] = first;
+  d.world_count[widx] = count;
+  d.world_bounds[2 * widx] = lo;
+  d.world_bounds[2 * widx + 1] = ext;
+}
+__global__ void k_fill_u32(uint32_t* p, uint32_t count, uint32_t v) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) p[i] = v;
+}
+__global__ void k_iota(uint32_t* p, uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) p[i] = i;
+}
+
+// Bodies [so, so + count) of world `s` into [o, o + count) of world `d` (both on one stream), as
+// an upload of the same bodies would write them: flags as the caller sees them, the previous
+// velocity equal to the velocity, sleep timers at zero.  Bodies [o + count, o + slot) are
+// parked as static specks on a line well outside the Morton box starting at `lo`, as
+// bb_world_refill parks them.
+__global__ void k_move_bodies(const DevState d, const DevState s, uint32_t o, uint32_t so, uint32_t count,
+                              uint32_t slot, float3 lo, float4 park_shape) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= slot) return;
+  const uint32_t b = o + i;
+  if (i < count) {
+    const uint32_t a = so + i;
+    const float4 v = s.vel[a];
+    d.pos[b] = s.pos[a];
+    d.rot[b] = s.rot[a];
+    d.vel[b] = v;
+    d.pvel[b] = v;
+    d.omega[b] = s.omega[a];
+    d.shape[b] = s.shape[a];
+    d.iinv[b] = s.iinv[a];
+    d.iinv_off[b] = s.iinv_off[a];
+    uint32_t f = s.flags[a];
+    if (f & BB_BODY_PAUSED) f = (f & BB_BODY_PAUSE_AWAKE) ? (f & ~BB_BODY_SLEEPING) : f;
+    d.flags[b] = f & (BB_BODY_DYNAMIC | BB_BODY_GRAVITY | BB_BODY_SLEEPING);
+  } else {
+    const float z = 0.f;
+    d.pos[b] = make_float4(lo.x - 1000.0f - 0.01f * float(i - count), lo.y - 1000.0f, lo.z - 1000.0f, z);
+    d.rot[b] = make_float4(z, z, z, 1.0f);
+    d.vel[b] = make_float4(z, z, z, z);
+    d.pvel[b] = make_float4(z, z, z, z);
+    d.omega[b] = make_float4(z, z, z, z);
+    d.shape[b] = park_shape;
+    d.iinv[b] = make_float4(z, z, z, z);
+    d.iinv_off[b] = make_float4(z, z, z, z);
+    d.flags[b] = 0u;
+  }
+  d.sleep[b] = 0u;
 }
 
 // Pause (on = 1) or resume the dynamic bodies [o, o + count): a paused body is flagged asleep
@@ -298,6 +359,54 @@ struct bb_world_impl {
   void* scratch_base = nullptr;
   size_t dev_bytes = 0;  // device memory held by this world
   float* xforms = nullptr;  // render feed: 12 floats per body
+  // Pinned host staging for uploads issued while steps may be queued on the stream: a chunk is
+  // reused once the copies issued from it have run (its event), so adding, refilling or
+  // writing bodies does not wait for the queued steps.
+  struct Stage {
+    char* p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+  };
+  std::vector<Stage> stages;
+  char* stage_get(size_t bytes, int* idx) {
+    for (size_t k = 0; k < stages.size(); ++k)
+      if (stages[k].cap >= bytes && cudaEventQuery(stages[k].ev) == cudaSuccess) {
+        *idx = int(k);
+        return stages[k].p;
+      }
+    if (stages.size() < 8) {
+      Stage s;
+      s.cap = std::max<size_t>(bytes, size_t(1) << 20);
+      if (cudaMallocHost(&s.p, s.cap) != cudaSuccess) return nullptr;
+      if (cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaFreeHost(s.p);
+        return nullptr;
+      }
+      stages.push_back(s);
+      *idx = int(stages.size() - 1);
+      return stages.back().p;
+    }
+    Stage& s = stages[0];  // all in flight: wait for the oldest, grow it if needed
+    cudaEventSynchronize(s.ev);
+    if (s.cap < bytes) {
+      cudaFreeHost(s.p);
+      s.p = nullptr;
+      s.cap = 0;
+      if (cudaMallocHost(&s.p, bytes) != cudaSuccess) return nullptr;
+      s.cap = bytes;
+    }
+    std::rotate(stages.begin(), stages.begin() + 1, stages.end());
+    *idx = int(stages.size() - 1);
+    return stages.back().p;
+  }
+  void stage_done(int idx) { cudaEventRecord(stages[size_t(idx)].ev, stream); }
+  void stages_free() {
+    for (auto& s : stages) {
+      if (s.ev) cudaEventDestroy(s.ev);
+      if (s.p) cudaFreeHost(s.p);
+    }
+    stages.clear();
+  }
   // graph cache
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
@@ -317,6 +426,7 @@ struct bb_world_impl {
   std::vector<float> stage_ms;
 
   ~bb_world_impl() {
+    stages_free();
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
     for (auto& o : owned) cudaFree(o.first);
@@ -422,17 +532,13 @@ struct bb_world_impl {
     cudaMemsetAsync(&d.ctr->front_valid, 0, sizeof(uint32_t), stream);
     cudaMemsetAsync(d.csr_start[0], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     cudaMemsetAsync(d.csr_start[1], 0, sizeof(uint32_t) * (cap_n + 2), stream);
-    std::vector<uint32_t> ident(n);
-    for (uint32_t i = 0; i < n; ++i) ident[i] = i;
-    cudaMemcpyAsync(d.vals[0], ident.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream);
-    cudaStreamSynchronize(stream);
+    if (n) k_iota<<<(n + 255) / 256, 256, 0, stream>>>(d.vals[0], n);
   }
 
   // bodies [o, o + count) were appended: they start with empty contact lists and take the
   // next sorted positions; existing bodies keep their warm-start state and order
   void extend_contacts(uint32_t o, uint32_t count) {
     k_extend_contacts<<<(count + 255) / 256, 256, 0, stream>>>(d, o, count);
-    cudaStreamSynchronize(stream);
   }
 
   // device copy of every array (and the host fields a step changes), taken on the world's stream
@@ -652,7 +758,10 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), w->cap_n / 2, 256);
   w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n / 2, 512);
   w->coop_cc = fit(bb_components_blocks(w->sms), w->cap_n, 512);
-  cudaError_t e = cudaStreamSynchronize(w->stream);  // the zero fills (no device-wide wait)
+  // The zero fills run on the world's stream ahead of everything the world does later.  On a
+  // stream of its own, wait for them here (no device-wide wait); on the caller's stream, which may
+  // hold queued work of other worlds, only check that they were issued.
+  cudaError_t e = w->own_stream ? cudaStreamSynchronize(w->stream) : cudaGetLastError();
   if (e != cudaSuccess) {
     delete w;
     return fail(BB_E_CUDA, std::string("create: ") + cudaGetErrorString(e));
@@ -899,26 +1008,25 @@ static bb_status pack_bodies(World* w, const bb_body_desc* bodies, uint32_t coun
   return BB_OK;
 }
 
-// rows of `r` into body ids [o, o + count) on the world's stream (sleep timers start at 0);
-// waits for the copies, since the rows are host memory that dies with the caller
+// rows of `r` into body ids [o, o + count) on the world's stream (sleep timers start at 0),
+// copied through the world's pinned staging: nothing waits for the steps queued before
 static bb_status upload_bodies(World* w, uint32_t o, const BodyRows& r) {
   const uint32_t count = uint32_t(r.fl.size());
-  const std::vector<uint32_t> zero(count, 0u);
-  const std::vector<float4>&pos = r.pos, &rot = r.rot, &vel = r.vel, &om = r.om, &shp = r.shp, &ii = r.ii, &io = r.io;
-  const std::vector<uint32_t>& fl = r.fl;
-  cudaStreamSynchronize(w->stream);
-  CU(cudaMemcpyAsync(w->d.pos + o, pos.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.rot + o, rot.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.vel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.pvel + o, vel.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.omega + o, om.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.shape + o, shp.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.iinv + o, ii.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.iinv_off + o, io.data(), count * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+  if (count == 0) return BB_OK;
+  const size_t f4 = size_t(count) * sizeof(float4);
+  int si = 0;
+  char* h = w->stage_get(8 * f4 + size_t(count) * sizeof(uint32_t), &si);
+  if (!h) return fail(BB_E_CUDA, "upload: pinned staging could not be allocated");
+  const std::vector<float4>* rows[7] = {&r.pos, &r.rot, &r.vel, &r.om, &r.shp, &r.ii, &r.io};
+  for (int k = 0; k < 7; ++k) std::memcpy(h + k * f4, rows[k]->data(), f4);
+  std::memcpy(h + 7 * f4, r.fl.data(), size_t(count) * sizeof(uint32_t));
+  float4* dst[7] = {w->d.pos, w->d.rot, w->d.vel, w->d.omega, w->d.shape, w->d.iinv, w->d.iinv_off};
+  for (int k = 0; k < 7; ++k) CU(cudaMemcpyAsync(dst[k] + o, h + k * f4, f4, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.pvel + o, h + 2 * f4, f4, cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemcpyAsync(w->d.flags + o, h + 7 * f4, size_t(count) * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
+  CU(cudaMemsetAsync(w->d.sleep + o, 0, size_t(count) * sizeof(uint32_t), w->stream));
+  w->stage_done(si);
   if (r.any_off) w->d.full_inertia = 1;
-  CU(cudaMemcpyAsync(w->d.flags + o, fl.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.sleep + o, zero.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaStreamSynchronize(w->stream));
   return BB_OK;
 }
 
@@ -942,9 +1050,8 @@ static bb_status add_bodies_impl(World* w, const bb_body_desc* bodies, uint32_t 
   if (keep_contacts) w->extend_contacts(o, count);
   else w->reset_contacts();
   w->invalidate_graphs();
-  uint32_t nn[2] = {w->n, w->n_dyn};
-  CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaStreamSynchronize(w->stream));  // the host arrays above die on return
+  k_set_counts<<<1, 1, 0, w->stream>>>(w->d, w->n, w->n_dyn);
+  CU(cudaGetLastError());
   return BB_OK;
 }
 
@@ -971,14 +1078,11 @@ bb_status bb_add_world(void* world, const bb_batch_world_desc* desc, const bb_bo
   w->wfirst.push_back(first);
   w->wcount.push_back(count);
   w->wdyn.push_back(w->n_dyn - dyn_before);
-  std::vector<uint32_t> wof(count, widx);
-  CU(cudaMemcpyAsync(w->d.world_of + first, wof.data(), 4ull * count, cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.world_first + widx, &first, 4, cudaMemcpyHostToDevice, w->stream));
-  CU(cudaMemcpyAsync(w->d.world_count + widx, &count, 4, cudaMemcpyHostToDevice, w->stream));
-  float4 bnd[2] = {make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
-                   make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f)};
-  CU(cudaMemcpyAsync(w->d.world_bounds + 2 * widx, bnd, sizeof(bnd), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaStreamSynchronize(w->stream));
+  k_fill_u32<<<(count + 255) / 256, 256, 0, w->stream>>>(w->d.world_of + first, count, widx);
+  k_set_world<<<1, 1, 0, w->stream>>>(w->d, widx, first, count,
+                                      make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
+                                      make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f));
+  CU(cudaGetLastError());
   w->d.n_worlds = widx + 1;
   w->max_world_n = std::max(w->max_world_n, count);
   w->invalidate_graphs();
@@ -1050,13 +1154,12 @@ bb_status bb_world_refill(void* world, uint32_t world_index, const bb_batch_worl
   for (uint32_t i = 0; i < slot; ++i) w->restitution[first + i] = r.restitution[i];
   w->n_dyn = w->n_dyn - w->wdyn[world_index] + r.ndyn;
   w->wdyn[world_index] = r.ndyn;
-  float4 bnd[2] = {make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
-                   make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f)};
-  CU(cudaMemcpyAsync(w->d.world_bounds + 2 * world_index, bnd, sizeof(bnd), cudaMemcpyHostToDevice, w->stream));
+  k_set_world<<<1, 1, 0, w->stream>>>(w->d, world_index, first, slot,
+                                      make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
+                                      make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f));
   k_refill_contacts<<<(slot + 255) / 256, 256, 0, w->stream>>>(w->d, first, slot);
-  uint32_t nn[2] = {w->n, w->n_dyn};
-  CU(cudaMemcpyAsync(w->d.ctr, nn, sizeof(nn), cudaMemcpyHostToDevice, w->stream));
-  CU(cudaStreamSynchronize(w->stream));  // bnd and nn are host locals
+  k_set_counts<<<1, 1, 0, w->stream>>>(w->d, w->n, w->n_dyn);
+  CU(cudaGetLastError());
   return BB_OK;
 }
 
@@ -1376,6 +1479,7 @@ bb_status bb_read_stats(void* world, bb_step_stats* s) {
   s->solved_manifolds = c.pgs_manifolds;
   s->solved_contacts = c.pgs_contacts;
   s->error_site = c.error_site;
+  s->graph_color_rounds = c.gc_rounds_run;
   return BB_OK;
 }
 
@@ -1675,6 +1779,45 @@ bb_status bb_read_stage_times(void* world, float* ms, uint32_t max_stages, uint3
 uint64_t bb_kernel_launch_count(void* world) { return world ? W(world)->launches : 0; }
 
 }  // extern "C"
+
+// Serving: the first `count` bodies of world `src_widx` of batch `src` moved into slot `widx` of
+// batch `dst` by device copies, with new Morton bounds -- the same bodies a bb_world_refill with
+// their current state would write, without the round trip through host memory.  Both batches
+// must step on one stream (the copy is ordered after the source's queued steps and before the
+// destination's next).  The destination slot restarts as a refilled slot does; the source slot
+// is left as it is (the caller reuses it).
+bb_status bb_world_move_in(void* dst_world, uint32_t widx, const bb_batch_world_desc* desc, void* src_world,
+                           uint32_t src_widx, uint32_t count) {
+  World* w = W(dst_world);
+  World* s = W(src_world);
+  if (!w || !s || !desc || w == s) return fail(BB_E_INVALID, "bb_world_move_in: bad arguments");
+  if (w->stream != s->stream) return fail(BB_E_INVALID, "bb_world_move_in: the batches step on different streams");
+  if (w->d.n_worlds == 0 || widx >= w->wfirst.size() || s->d.n_worlds == 0 || src_widx >= s->wfirst.size())
+    return fail(BB_E_INVALID, "bb_world_move_in: not a world of these batches");
+  const uint32_t first = w->wfirst[widx], slot = w->wcount[widx], src_first = s->wfirst[src_widx];
+  if (count > slot || count > s->wcount[src_widx])
+    return fail(BB_E_CAPACITY, "bb_world_move_in: more bodies than the slot holds");
+  w->forget_snapshot();
+  const uint32_t tbits = BB_SHAPE_BOX;
+  float tf;
+  std::memcpy(&tf, &tbits, 4);
+  k_move_bodies<<<(slot + 255) / 256, 256, 0, w->stream>>>(
+      w->d, s->d, first, src_first, count, slot, make_float3(desc->world_min[0], desc->world_min[1], desc->world_min[2]),
+      make_float4(0.001f, 0.001f, 0.001f, tf));
+  for (uint32_t i = 0; i < slot; ++i) w->restitution[first + i] = i < count ? s->restitution[src_first + i] : 0.f;
+  const uint32_t ndyn = s->wdyn[src_widx];
+  w->n_dyn = w->n_dyn - w->wdyn[widx] + ndyn;
+  w->wdyn[widx] = ndyn;
+  if (s->d.full_inertia) w->d.full_inertia = 1;
+  k_set_world<<<1, 1, 0, w->stream>>>(w->d, widx, first, slot,
+                                      make_float4(desc->world_min[0], desc->world_min[1], desc->world_min[2], 0.f),
+                                      make_float4(desc->world_extent[0], desc->world_extent[1], desc->world_extent[2], 0.f));
+  k_refill_contacts<<<(slot + 255) / 256, 256, 0, w->stream>>>(w->d, first, slot);
+  k_set_counts<<<1, 1, 0, w->stream>>>(w->d, w->n, w->n_dyn);
+  CU(cudaGetLastError());
+  return BB_OK;
+}
+
 
 // State of bodies [first, first + count) (the serving loop's view of one batch slot): xyz
 // positions, xyzw rotations, velocities, angular velocities, flags (may each be null).

@@ -199,6 +199,7 @@ typedef struct bb_step_stats {
   uint32_t substeps_run;          /* substeps run since the world was created */
   uint32_t solved_manifolds;      /* last substep's colour sweeps: manifolds with an awake body */
   uint32_t solved_contacts;       /* and their contacts (0 under AVBD and the per-island path) */
+  uint32_t graph_color_rounds;    /* bid/commit rounds the last edge colouring ran (at most gc_rounds) */
   uint32_t error_site;            /* where the first bounded wait gave up (BB_ERRF_SPIN_LIMIT): 0 none,
                                      1 sort look-back, 2 dataflow PGS wait, 3 generation barrier, 4 scan
                                      look-back, 16 + k grid barrier k (0 edge colouring, 1 PGS_SOFT, 2 AVBD

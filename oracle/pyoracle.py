@@ -42,7 +42,7 @@ class StepStats(ctypes.Structure):
         "avbd_violations", "sleeping_count", "fresh_contacts", "stick_count")] + [
         ("max_penetration", ctypes.c_float), ("error_flags", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
         ("substeps_run", ctypes.c_uint32), ("solved_manifolds", ctypes.c_uint32), ("solved_contacts", ctypes.c_uint32),
-        ("error_site", ctypes.c_uint32)]
+        ("graph_color_rounds", ctypes.c_uint32), ("error_site", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
