@@ -165,7 +165,7 @@ struct DevState {
   uint32_t* gc_list[2];  // manifolds still uncoloured after a round (alternating)
   uint32_t* gc_mask;     // per body
   uint32_t* gc_island_tag; // per island: colouring epoch + 1 when one of its bodies is awake
-  unsigned long long* gc_owner; // per body x 32 colours: (epoch << 32) | priority
+  unsigned long long* gc_owner; // 32 colours x (body capacity + 1) bodies: (epoch << 32) | priority
   uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies
   uint32_t* bucket_start; // 34 + 32*L entries
   uint32_t* colour_awake; // per colour (32 = overflow): 1 if one of its manifolds has an awake body

@@ -260,6 +260,12 @@ __device__ __forceinline__ uint32_t gc_priority(uint32_t pid, uint32_t round) {
 // grid barrier is the arrival-counter kind (counter 0 of the substep).
 #define BB_GC_THREADS 1024
 #define GC_UNROLL 3  // list entries a thread takes per trip of a round
+// Owner word of (body, colour), colour-major: a round's bids go mostly to the lowest free colours,
+// so the words in use (8 bytes per body for each colour bid) stay in L2, where a body-major
+// table (256 bytes per body) spread every round's random atomics over the whole table in DRAM.
+__device__ __forceinline__ size_t gc_owner_at(const DevState& d, uint32_t body, uint32_t col) {
+  return size_t(col) * (size_t(d.body_capacity) + 1u) + body;
+}
 __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState d, Params p, int cur, uint32_t n) {
   DevCounters* c = d.ctr;
   const uint32_t M = c->manifold_count;
@@ -374,8 +380,8 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
         d.gc_choice[m[u]] = col;
         if (col >= BB_MAX_COLORS) continue;
         const unsigned long long v = tag | gc_priority(rec[u].z, r);
-        if (!sa) atomicMax(&d.gc_owner[size_t(rec[u].x) * BB_MAX_COLORS + col], v);
-        if (!sb) atomicMax(&d.gc_owner[size_t(rec[u].y) * BB_MAX_COLORS + col], v);
+        if (!sa) atomicMax(&d.gc_owner[gc_owner_at(d, rec[u].x, col)], v);
+        if (!sb) atomicMax(&d.gc_owner[gc_owner_at(d, rec[u].y, col)], v);
       }
     }
     if (local) __syncthreads();
@@ -398,8 +404,8 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
 #pragma unroll
       for (int u = 0; u < GC_UNROLL; ++u) {
         const bool live = col[u] < BB_MAX_COLORS;
-        oa[u] = live && !(rec[u].w & 1u) ? d.gc_owner[size_t(rec[u].x) * BB_MAX_COLORS + col[u]] : 0ull;
-        ob[u] = live && !(rec[u].w & 2u) ? d.gc_owner[size_t(rec[u].y) * BB_MAX_COLORS + col[u]] : 0ull;
+        oa[u] = live && !(rec[u].w & 1u) ? d.gc_owner[gc_owner_at(d, rec[u].x, col[u])] : 0ull;
+        ob[u] = live && !(rec[u].w & 2u) ? d.gc_owner[gc_owner_at(d, rec[u].y, col[u])] : 0ull;
       }
       uint32_t used = 0;  // colour + 1 of a committed manifold
 #pragma unroll
