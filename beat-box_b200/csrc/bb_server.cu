@@ -7,14 +7,17 @@
 // worlds in slots, and one graph launch per step advances all of them.
 //
 //   * Requests are grouped by step class (solver parameters, dt, substeps: one batch steps with
-//     one set) and size class (slot capacity, a power of two >= the world's bodies, 64 at least).
-//     A batch of a (step class, size class) holds up to max(2^16 / slot, 1) slots (fewer when a
-//     batch that size would take more than half of the HBM budget).
+//     one set).  A batch of a step class holds worlds of every size, each in a slot of its size
+//     class (a power of two >= the world's bodies, 64 at least), up to 2^19 bodies (fewer when a
+//     batch that size would take more than half of the HBM budget).  A step of a batch costs
+//     nearly the same for a few small worlds as for many (the colour sweeps and AVBD's
+//     per-colour passes are latency-bound), so one batch per step class advances the most
+//     worlds per step.
 //   * A request is admitted as soon as a slot and the budget allow: its world is put into a free
-//     slot (bb_world_refill, or bb_add_world for a slot never used) or, when it is already
-//     resident in a batch of its step class, resumed in place (bb_world_pause(.., 0)).  From
-//     then on it advances with every step of its batch; requests that arrive while others run
-//     join at the next step boundary.
+//     slot of its size class (bb_world_refill), a new slot where the batch has room
+//     (bb_add_world), or, when it is already resident in a batch of its step class, resumed in
+//     place (bb_world_pause(.., 0)).  From then on it advances with every step of its batch;
+//     requests that arrive while others run join at the next step boundary.
 //   * After its last step a world is paused in its slot: it keeps its device state (bodies,
 //     warm-start contacts, sort order) exactly until its next request, whatever the other
 //     slots do.  A world's results therefore do not depend on what else is in flight.
@@ -58,7 +61,7 @@ const uint32_t* bb_world_error_site_word(void* world);
 namespace {
 
 using Clock = std::chrono::steady_clock;
-constexpr uint32_t kBatchBodies = 1u << 16;  // bodies of one batch (at least one slot)
+constexpr uint32_t kBatchBodies = 1u << 19;  // body capacity of one batch (at least its largest slot)
 constexpr uint32_t kInFlight = 2;           // steps a batch may have queued on its stream
 
 uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
@@ -92,6 +95,7 @@ struct Slot {
   WorldRec* world = nullptr;  // resident world (running or paused), nullptr = free
   Req* req = nullptr;         // running request
   uint32_t remaining = 0;     // its steps not yet enqueued
+  uint32_t cls = 0, first = 0;  // size class (2^cls bodies) and first body id in the batch
 };
 
 struct Batch {
@@ -100,7 +104,7 @@ struct Batch {
   uint64_t step_key = 0;
   float dt = 0;
   uint32_t substeps = 1;
-  uint32_t cls = 0, slot_cap = 0, max_slots = 0;
+  uint32_t cap = 0, used = 0;  // body capacity, bodies taken by its slots
   std::vector<Slot> slots;
   std::map<std::tuple<uint32_t, float, float, float>, uint32_t> shape_handle;
   uint32_t park_shape = 0;
@@ -165,7 +169,7 @@ struct bb_server_impl {
   void save_world(WorldRec* wr) {
     Batch* b = wr->batch;
     const uint32_t n = uint32_t(wr->bodies.size());
-    const uint32_t first = wr->slot * b->slot_cap;
+    const uint32_t first = b->slots[wr->slot].first;
     std::vector<float> pos(3 * size_t(n)), rot(4 * size_t(n)), vel(3 * size_t(n)), om(3 * size_t(n));
     std::vector<uint32_t> fl(n);
     if (bb_world_read_range(b->w, first, n, pos.data(), rot.data(), vel.data(), om.data(), fl.data()) == BB_OK) {
@@ -215,11 +219,11 @@ struct bb_server_impl {
   }
 
   Batch* create_batch(const Req* q, uint32_t cls, bb_status* err) {
-    const uint32_t cap = 1u << cls;
-    uint32_t slots = std::max(1u, kBatchBodies / cap);
-    // under a small budget, smaller batches: one batch should not take more than half of it
-    while (slots > 1 && bb_world_bytes_for(cap * slots, ppb()) > desc.hbm_budget_bytes / 2) slots /= 2;
-    const uint64_t need = bb_world_bytes_for(cap * slots, ppb());
+    // capacity kBatchBodies, at least the first slot's size; under a small budget smaller: one
+    // batch should not take more than half of it
+    uint32_t cap = std::max(kBatchBodies, 1u << cls);
+    while (cap > (1u << cls) && bb_world_bytes_for(cap, ppb()) > desc.hbm_budget_bytes / 2) cap /= 2;
+    const uint64_t need = bb_world_bytes_for(cap, ppb());
     if (need > desc.hbm_budget_bytes) {
       *err = BB_E_BUDGET;
       return nullptr;
@@ -230,7 +234,7 @@ struct bb_server_impl {
     }
     auto b = std::make_unique<Batch>();
     bb_world_desc wd = {};
-    wd.max_bodies = cap * slots;
+    wd.max_bodies = cap;
     wd.pairs_per_body = ppb();
     wd.device = desc.device;
     wd.stream = stream;
@@ -242,9 +246,7 @@ struct bb_server_impl {
     b->step_key = q->step_key;
     b->dt = q->r.dt;
     b->substeps = q->r.substeps;
-    b->cls = cls;
-    b->slot_cap = cap;
-    b->max_slots = slots;
+    b->cap = cap;
     bb_solver_params p = q->r.params;
     p.bounds_mode = BB_BOUNDS_FIXED;
     for (int k = 0; k < 3; ++k) {
@@ -292,16 +294,17 @@ struct bb_server_impl {
     return BB_OK;
   }
 
-  // world wr into slot k of batch b: a refill of a used slot, or a new world of the batch
-  // padded to the slot's size with parked bodies
-  bb_status place(Batch* b, uint32_t k, WorldRec* wr) {
+  // world wr into slot k of batch b: a refill of a free slot of its size class, or a new slot
+  // of 2^cls bodies (k == slots.size()) padded with parked bodies
+  bb_status place(Batch* b, uint32_t k, uint32_t cls, WorldRec* wr) {
+    const uint32_t slot_cap = 1u << cls;
     // A world still resident in a batch of another step class moves by device copies (same
     // stream, so after that batch's queued steps); its host copy is stale and not needed.
     Batch* from = wr->batch;
     std::vector<bb_body_desc> bodies;
     bb_status s = BB_OK;
     if (from) {
-      bodies.resize(b->slot_cap);  // a new slot starts parked, then takes the moved bodies
+      bodies.resize(slot_cap);  // a new slot starts parked, then takes the moved bodies
     } else {
       s = batch_bodies(b, wr, bodies);
       if (s != BB_OK) return s;
@@ -316,8 +319,8 @@ struct bb_server_impl {
       s = bb_world_refill(b->w, k, &wd, bodies.data(), uint32_t(bodies.size()));
     } else {
       const uint32_t n = from ? 0u : uint32_t(bodies.size());
-      bodies.resize(b->slot_cap);
-      for (uint32_t i = n; i < b->slot_cap; ++i) {
+      bodies.resize(slot_cap);
+      for (uint32_t i = n; i < slot_cap; ++i) {
         bb_body_desc& d = bodies[i];
         std::memset(&d, 0, sizeof(d));
         d.position[0] = wr->wmin[0] - 1000.0f - 0.01f * float(i - n);
@@ -327,8 +330,13 @@ struct bb_server_impl {
         d.shape = b->park_shape;
       }
       uint32_t widx = 0, first = 0;
-      s = bb_add_world(b->w, &wd, bodies.data(), b->slot_cap, &widx, &first);
-      if (s == BB_OK) b->slots.emplace_back();
+      s = bb_add_world(b->w, &wd, bodies.data(), slot_cap, &widx, &first);
+      if (s == BB_OK) {
+        b->slots.emplace_back();
+        b->slots.back().cls = cls;
+        b->slots.back().first = first;
+        b->used += slot_cap;
+      }
       if (s == BB_OK && from) s = bb_world_move_in(b->w, k, &wd, from->w, wr->slot, n_real);
     }
     if (s != BB_OK) return s;
@@ -352,26 +360,38 @@ struct bb_server_impl {
     }
     // otherwise it moves to a batch of its new step class (its warm starts restart there); it
     // stays registered in its old slot until placed, so a batch destroyed to make room saves it
+    // A free slot of its size class in a batch of its step class (the busiest such batch: more
+    // worlds per step), else a new slot where a batch has room, else the slot of an idle world
+    // of that size class (saved to the host), else a new batch.
     const uint32_t cls = class_of(uint32_t(wr->bodies.size()));
     Batch* best = nullptr;
     uint32_t best_k = 0;
     for (auto& c : batches) {
-      if (c->step_key != q->step_key || c->cls != cls) continue;
+      if (c->step_key != q->step_key) continue;
       uint32_t k = 0;
-      while (k < c->slots.size() && c->slots[k].world) ++k;
-      if (k >= c->max_slots) continue;
-      if (!best || c->running > best->running) {  // join the busiest batch: more worlds per step
+      while (k < c->slots.size() && (c->slots[k].world || c->slots[k].cls != cls)) ++k;
+      if (k == c->slots.size()) continue;
+      if (!best || c->running > best->running) {
         best = c.get();
         best_k = k;
       }
     }
     if (!best) {
-      // a free slot holding an idle paused world of this class can be taken over
       for (auto& c : batches) {
-        if (c->step_key != q->step_key || c->cls != cls) continue;
+        if (c->step_key != q->step_key || c->used + (1u << cls) > c->cap) continue;
+        if (!best || c->running > best->running) {
+          best = c.get();
+          best_k = uint32_t(c->slots.size());
+        }
+      }
+    }
+    if (!best) {
+      // a slot of this size class holding an idle paused world can be taken over
+      for (auto& c : batches) {
+        if (c->step_key != q->step_key) continue;
         for (uint32_t k = 0; k < c->slots.size(); ++k) {
           Slot& sl = c->slots[k];
-          if (sl.world && !sl.world->busy && !sl.world->reading && !sl.req) {
+          if (sl.cls == cls && sl.world && !sl.world->busy && !sl.world->reading && !sl.req) {
             save_world(sl.world);
             best = c.get();
             best_k = k;
@@ -391,7 +411,7 @@ struct bb_server_impl {
       best_k = 0;
     }
     const auto t = Clock::now();
-    bb_status s = place(best, best_k, wr);
+    bb_status s = place(best, best_k, cls, wr);
     st.materialise_s += std::chrono::duration<double>(Clock::now() - t).count();
     if (s != BB_OK) *fail = s;
     return true;
@@ -654,7 +674,7 @@ bb_status bb_server_read_state(void* server, uint64_t world, float* position, fl
   if (wr->batch) {  // resident (paused in its slot): copy its range out of the batch
     wr->reading = true;
     Batch* b = wr->batch;
-    const uint32_t first = wr->slot * b->slot_cap;
+    const uint32_t first = b->slots[wr->slot].first;
     lk.unlock();
     bb_status st;
     {

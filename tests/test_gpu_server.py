@@ -22,7 +22,7 @@ def req_params(k):
     return p
 
 
-# three size classes (slots of 64, 128 and 1024 bodies), several worlds in each
+# three size classes (slots of 64, 128 and 1024 bodies), several worlds in each, all in one batch per step class
 WORLD_SIZES = [64, 50, 60, 900, 1000, 97, 120]
 # (world index, steps) in submission order: worlds get several requests, interleaved
 PLAN = [(0, 5), (1, 12), (2, 3), (3, 8), (4, 6), (0, 7), (5, 20), (2, 9), (1, 4), (3, 2), (0, 3), (4, 5),
@@ -47,8 +47,8 @@ def test_each_world_is_the_same_alone_and_in_the_mix():
     assert all(r["done"] and r["result"] == bb.OK for r in res)
     st = mix.stats()
     assert st["completed"] == len(PLAN)
-    # worlds of a size class share batches: at most 3 size classes x 2 step classes (PGS, AVBD)
-    assert st["worlds_created"] <= 6 < len(WORLD_SIZES) * 2
+    # every world of a step class shares one batch: PGS_SOFT and AVBD
+    assert st["worlds_created"] == 2
     assert st["body_steps"] == sum(int(worlds[w]["n"]) * s for w, s in PLAN)
     mixed = {w: mix.read_state(1000 + w, int(worlds[w]["n"])) for w in range(len(worlds))}
     mix.close()
