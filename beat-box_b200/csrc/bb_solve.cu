@@ -689,19 +689,12 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(co
   if (threadIdx.x < BB_MAX_COLORS + 1) aw[threadIdx.x] = d.colour_awake[threadIdx.x];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
-  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
-  const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
   uint32_t* sync = &d.ctr->sync_count[1];
   uint32_t epoch = 0;
-  for (uint32_t i = tid; i < n; i += stride) pgs_world_inertia(d, i, tq);
-  grid_sync(d.ctr, sync, epoch);  // also makes bs visible block-wide
+  // the world inverse inertias and the items' records and rows were written by k_pgs_inertia
+  // and k_pgs_build before this launch
+  __syncthreads();  // bs and aw
   const uint32_t C = d.ctr->gc_colors;
-  const uint32_t* list = d.bucket_vals[1];
-  // records and rows, each item by the thread that runs it in every sweep (no barrier needed)
-  for (uint32_t c = 0; c < C; ++c)
-    for (uint32_t k = bs[c] + tid; k < bs[c + 1]; k += stride) pgs_item_build(d, cur, k, list[k], h, hertz);
-  if (tid == 0)
-    for (uint32_t k = bs[BB_MAX_COLORS]; k < bs[BB_MAX_COLORS + 1]; ++k) pgs_item_build(d, cur, k, list[k], h, hertz);
   PgsItem<PF> x;
   uint4 rec_next = make_uint4(0, 0, 0, 0);
   if (C > 0 && bs[0] + tid < bs[1]) pgs_item_load(d, bs[0] + tid, x);
@@ -717,9 +710,28 @@ __global__ void __launch_bounds__(BB_PGS_THREADS, PF == 4 ? 1 : 2) k_pgs_soft(co
     grid_sync(d.ctr, sync, epoch);
   }
   for (uint32_t it = 0; it < p.relax_iterations; ++it) pgs_sweep<PF, STAGE_NEXT>(d, p, cur, 2, bs, aw, C, x, rec_next, epoch);
-  // impulses back to the persistent contacts (every sweep ended with a grid barrier)
+  // k_pgs_writeback copies the impulses back to the persistent contacts after this launch
+}
+
+// Before k_pgs_soft, at full occupancy (the persistent kernel runs one 256-thread block per
+// SM, where these passes of one item or body per thread were latency-bound): the world
+// inverse inertias, then the records and rows of every swept item (colours and the overflow
+// bucket, [0, bucket_start[33])).  After it, the impulses back to the persistent contacts.
+__global__ void k_pgs_inertia(const DevState d, uint32_t n, Params p) {
+  const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pgs_world_inertia(d, i, tq);
+}
+__global__ void k_pgs_build(const DevState d, Params p, int cur, float h) {
+  const float inv_h = h > 0.f ? 1.0f / h : 0.f;
+  const float hertz = fminf(p.contact_hertz, inv_h * 0.3333333333333333f);
+  const uint32_t end = d.bucket_start[BB_MAX_COLORS + 1];
+  const uint32_t* list = d.bucket_vals[1];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < end; k += gridDim.x * blockDim.x)
+    pgs_item_build(d, cur, k, list[k], h, hertz);
+}
+__global__ void k_pgs_writeback(const DevState d, int cur) {
   const uint32_t M = d.ctr->manifold_count;
-  for (uint32_t k = tid; k < M; k += stride) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
     const uint32_t cc = d.pgs_cnt[k];
     if (cc == 0) continue;
     const uint32_t slot = d.pgs_slot[k], c0 = d.pgs_coff[k];
@@ -878,11 +890,14 @@ void bb_solve_pgs_soft(cudaStream_t s, const DevState& d, const Params& p, uint3
   uint32_t nn = n;
   float hh = h;
   void* args[] = {&dd, &pp, &cc, &nn, &hh};
+  if (n) k_pgs_inertia<<<(n + BB_THREADS - 1) / BB_THREADS, BB_THREADS, 0, s>>>(d, n, p);
+  k_pgs_build<<<sms * 8, BB_THREADS, 0, s>>>(d, p, cur, h);
   // staging the next item needs 112 KB more shared memory (less L1): it pays when threads run
   // several items per colour (large worlds), which is what the autotuner measures
   if (p.pgs_stage_next)
     bb_launch_coop((const void*)k_pgs_soft<4, true>, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM);
   else bb_launch_coop((const void*)k_pgs_soft<4, false>, coop_blocks, BB_PGS_THREADS, args, s, BB_PGS_SMEM_EXTRA);
+  k_pgs_writeback<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
 }
 
 // ---------------------------------------------------------------------------------------
