@@ -5,7 +5,7 @@
 // src/shaders/simulation/LBVH.slang:34-152, RBM:1288-1295) with:
 //   * one histogram kernel that counts all digit positions in a single read of the keys,
 //   * one onesweep kernel per digit: tiles of 4096 keys rank themselves with warp-level
-//     multisplit (__match_any_sync), publish per-digit tile totals, resolve their global
+//     multisplit (one ballot per digit bit), publish per-digit tile totals, resolve their global
 //     offsets by decoupled look-back over the preceding tiles, reorder the tile by digit in
 //     shared memory and write each digit's run contiguously (coalesced stores).
 // Both are stable, so the result equals a stable sort by key -- the reference's semantics.
@@ -252,17 +252,32 @@ __global__ void __launch_bounds__(kThreads, 3) k_onesweep(const uint32_t* __rest
     key[k] = i < n ? keys_in[i] : 0u;
     val[k] = i < n ? vals_in[i] : 0u;
   }
-  // warp-level multisplit: rank of each key among its warp's keys of the same digit, in order
+  // warp-level multisplit: rank of each key among its warp's keys of the same digit, in order.
+  // The lanes holding the same digit are found with one ballot per digit bit (plus one for the
+  // keys past n); only the lowest of them reads and advances the warp's count of that digit, and
+  // the others take the old count from it by a shuffle.
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
-    const uint32_t d = first + k * 32 < n ? sort_digit(key[k], val[k], lut, shift) : 256u;
-    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-    uint32_t prior = d < 256u ? s_warp_hist[warp][d] : 0u;
+    const bool valid = first + k * 32 < n;
+    const uint32_t d = valid ? sort_digit(key[k], val[k], lut, shift) : 0u;
+    uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+    if (!valid) peers = ~peers;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
+      peers &= ((d >> b) & 1u) ? bal : ~bal;
+    }
+    const int leader = __ffs(peers) - 1;
+    uint32_t prior = 0;
+    if (valid && lane == leader) {
+      prior = s_warp_hist[warp][d];
+      s_warp_hist[warp][d] = prior + __popc(peers);
+    }
+    prior = __shfl_sync(0xFFFFFFFFu, prior, leader);
     rank[k] = prior + __popc(peers & lt_mask);
     __syncwarp();
-    if (d < 256u && lane == __ffs(peers) - 1) s_warp_hist[warp][d] = prior + __popc(peers);
-    __syncwarp();
   }
+
   __syncthreads();
   // per digit t: exclusive prefix over warps, and the tile's count of digit t
   const uint32_t t = threadIdx.x;
