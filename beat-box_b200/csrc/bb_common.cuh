@@ -65,6 +65,8 @@ struct DevCounters {
   uint32_t round_flags[2]; // per-round flags / counters: components' "changed", then the AVBD colouring's uncoloured counts
   uint32_t heavy_n;        // broad phase: heavy queries of this substep
   uint32_t error_site;     // where the first bounded wait gave up (bb_step_stats.error_site)
+  uint32_t prev_manifolds; // manifold count of the last substep (its buffer is the previous one)
+  uint32_t gc_coloured;    // substep number of the last edge colouring (0: none to reuse)
   uint32_t sync_count[8];  // grid_sync arrival counters, one per persistent launch of a substep
                            // (zeroed at substep start): 0 edge colouring, 1 PGS, 2.. AVBD,
                            // 7 connected components
@@ -169,6 +171,13 @@ struct DevState {
   uint32_t *bucket_keys[2], *bucket_vals[2]; // colour sort of manifolds / bodies
   uint32_t* bucket_start; // 34 + 32*L entries
   uint32_t* colour_awake; // per colour (32 = overflow): 1 if one of its manifolds has an awake body
+  // colour reuse: an island whose manifolds (bodies and key) are exactly last substep's keeps
+  // last substep's colours (the colouring of an island depends on that set alone)
+  uint32_t* gc_slot_color[2]; // per manifold slot of each buffer: the colour the colouring gave it
+  uint32_t* gc_reuse;      // per slot of this substep: the colour of the same manifold last substep, or BB_NONE
+  uint32_t* gc_survived;   // per slot of the previous buffer: substep number when a manifold took it over
+  uint32_t* gc_body_chg;   // per body: substep number when one of its manifolds of last substep ended
+  uint32_t* gc_island_chg; // per island: colouring epoch + 1 when it must be coloured afresh
   // AVBD
   uint32_t* body_color;   // per body
   uint32_t* body_color_round;

@@ -282,12 +282,31 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   // the solve skips those manifolds anyway (both bodies asleep or static), so they are marked
   // BB_RESTING and sorted behind the overflow bucket without being coloured.
   const uint32_t itag = epoch + 1u;  // never 0 (epochs step by 64), so zeroed tags never match
+  // Colour reuse.  The colours of an island depend only on its set of manifolds (their bodies
+  // and keys).  When every manifold of an island is one of last substep's (matched in the narrow
+  // phase, gc_reuse) and none of last substep's manifolds on its bodies ended (gc_body_chg),
+  // the set is last substep's and so are its colours: the island skips the rounds.  Islands
+  // marked here (gc_island_chg) are coloured afresh.  Only right after a colouring.
+  const uint32_t sub_tag = c->substeps;
+  const bool reuse = c->gc_coloured + 1u == sub_tag;
   for (uint32_t i = tid; i < n; i += stride) {
     d.gc_mask[i] = 0;
     const uint32_t f = d.flags[i];
+    const uint32_t isl = d.island[i];
     if ((f & BB_BODY_DYNAMIC) && !(f & BB_BODY_SLEEPING)) {
-      const uint32_t isl = d.island[i];
       if (isl != BB_NONE && d.gc_island_tag[isl] != itag) d.gc_island_tag[isl] = itag;
+    }
+    if (reuse && isl != BB_NONE && d.gc_body_chg[i] == sub_tag && d.gc_island_chg[isl] != itag)
+      d.gc_island_chg[isl] = itag;
+  }
+  if (reuse) {  // manifolds that are not last substep's (or were not coloured then)
+    for (uint32_t m = tid; m < M; m += stride) {
+      const uint32_t slot = d.man_slot[cur][m];
+      const uint32_t old = d.gc_reuse[slot];
+      if (old != BB_NONE && old != BB_RESTING) continue;
+      const uint2 b = d.m_bodies[cur][slot];
+      const uint32_t isl = (d.flags[b.x] & BB_BODY_DYNAMIC) ? d.island[b.x] : d.island[b.y];
+      if (isl != BB_NONE && d.gc_island_chg[isl] != itag) d.gc_island_chg[isl] = itag;
     }
   }
   if (tid == 0) {
@@ -297,6 +316,7 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
   }
   grid_sync(c, sync, ep);
   // round 1's list: the manifolds of islands with an awake body (a warp appends its lanes at once)
+  uint32_t used0 = 0;  // colour + 1 of the reused colours
   for (uint32_t base = warp0; base < M; base += stride) {  // warp-uniform trips
     const uint32_t m = base + lane;
     bool colour = false;
@@ -308,7 +328,12 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
       const bool da = fa & BB_BODY_DYNAMIC, db = fb & BB_BODY_DYNAMIC;
       const uint32_t isl = da ? d.island[b.x] : db ? d.island[b.y] : BB_NONE;
       colour = isl != BB_NONE && d.gc_island_tag[isl] == itag;
-      if (colour) {
+      uint32_t kept = BB_NONE;  // a reused colour
+      if (colour && reuse && d.gc_island_chg[isl] != itag) {
+        kept = d.gc_reuse[slot];
+        colour = false;
+      }
+      if (colour || kept != BB_NONE) {
         const uint32_t la = local_id(d, b.x), lb = local_id(d, b.y);
         uint32_t lo = min(la, lb), hi = max(la, lb);
         const uint32_t pid = gc_hash(lo * 0x9e3779b9u + hi * 0x85ebca6bu + uint32_t(key) * 0xc2b2ae35u);
@@ -318,7 +343,8 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
                           !((fb & BB_BODY_DYNAMIC) && !(fb & BB_BODY_SLEEPING));
         d.gc_rec[m] = make_uint4(b.x, b.y, pid, (da ? 0u : 1u) | (db ? 0u : 2u) | (idle ? 4u : 0u));
       }
-      d.gc_color[m] = colour ? BB_UNCOLORED : BB_RESTING;
+      d.gc_color[m] = kept != BB_NONE ? kept : colour ? BB_UNCOLORED : BB_RESTING;
+      if (kept < BB_MAX_COLORS) used0 = max(used0, kept + 1u);
     }
     const unsigned mask = __ballot_sync(0xFFFFFFFFu, colour);
     if (mask) {
@@ -328,6 +354,8 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
       if (colour) d.gc_list[1][off + __popc(mask & ((1u << lane) - 1u))] = m;
     }
   }
+  used0 = __reduce_max_sync(0xFFFFFFFFu, used0);
+  if (lane == 0 && used0) atomicMax(&c->gc_colors, used0);
   grid_sync(c, sync, ep);
   // Round r bids and commits over the manifolds still uncoloured when it starts: in round 1 all
   // manifolds of islands with an awake body (the identity list when that is all of them),
@@ -454,9 +482,13 @@ __global__ void __launch_bounds__(BB_GC_THREADS, 1) k_edge_color(const DevState 
       key = BB_MAX_COLORS + 1;
     d.bucket_keys[0][m] = key;
     d.bucket_vals[0][m] = m;
+    d.gc_slot_color[cur][d.man_slot[cur][m]] = col;  // for the next substep's colour reuse
   }
   if (over) atomicAdd(&c->gc_overflow, over);
-  if (tid == 0) c->gc_epoch = epoch + 64u;
+  if (tid == 0) {
+    c->gc_epoch = epoch + 64u;
+    c->gc_coloured = sub_tag;
+  }
 }
 
 // bucket_start[0..34]: start of colour c (32 = overflow, 33 = resting manifolds), [34] = M
@@ -464,6 +496,22 @@ __global__ void k_bucket_starts(const uint32_t* hist_scan, const uint32_t* n_ptr
   int t = threadIdx.x;
   if (t < nb) starts[t] = hist_scan[t];
   if (t == nb) starts[t] = *n_ptr;
+}
+
+// Colour reuse: the bodies of last substep's manifolds that no manifold of this substep took
+// over (their pair ended, or its key changed) mark their islands for a fresh colouring.
+__global__ void k_gc_ended(const DevState d, int cur) {
+  const int prv = cur ^ 1;
+  const uint32_t tag = d.ctr->substeps;
+  if (d.ctr->gc_coloured + 1u != tag) return;  // no reuse this substep
+  const uint32_t Mp = min(d.ctr->prev_manifolds, d.pair_capacity);
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < Mp; m += gridDim.x * blockDim.x) {
+    const uint32_t os = d.man_slot[prv][m];
+    if (d.gc_survived[os] == tag) continue;
+    const uint2 b = d.m_bodies[prv][os];
+    if (b.x != BB_NONE) d.gc_body_chg[b.x] = tag;
+    if (b.y != BB_NONE) d.gc_body_chg[b.y] = tag;
+  }
 }
 
 int bb_edge_coloring_blocks(int sms) { return bb_coop_blocks((const void*)k_edge_color, BB_GC_THREADS, sms); }
@@ -475,6 +523,7 @@ void bb_edge_coloring(cudaStream_t s, const DevState& d, const Params& p, uint32
   uint32_t nn = n;
   DevState dd = d;
   void* args[] = {&dd, &pp, &cc, &nn};
+  k_gc_ended<<<sms * 8, BB_THREADS, 0, s>>>(d, cur);
   bb_launch_coop((const void*)k_edge_color, coop_blocks, BB_GC_THREADS, args, s);
   // stable bucket sort of manifold ids by colour (one 8-bit digit)
   uint32_t* keys[2] = {d.bucket_keys[0], d.bucket_keys[1]};

@@ -514,6 +514,12 @@ __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t 
                                            uint32_t idb, uint32_t q, bool exact) {
   const int prv = cur ^ 1;
   const int2 kc = d.m_keycc[prv][os];
+  if (q == 0) {  // the same manifold as last substep: its colour carries over (colour reuse)
+    const uint32_t sub_tag = d.ctr->substeps;
+    const bool reuse_ok = d.ctr->gc_coloured + 1u == sub_tag;
+    d.gc_reuse[dst] = reuse_ok ? d.gc_slot_color[prv][os] : BB_NONE;
+    if (reuse_ok) d.gc_survived[os] = sub_tag;
+  }
   if (exact) {
     if (q == 0) {
       d.m_bodies[cur][dst] = d.m_bodies[prv][os];
@@ -643,6 +649,11 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
   bool swapped = false;
   float sgn = 1.f;
   int32_t err = 0x7FFFFFFF;
+  // Colour reuse: the same manifold (bodies and key) as last substep carries its colour, and
+  // the old manifold is marked as taken over (an old manifold nobody takes over has ended).
+  uint32_t reuse = BB_NONE;
+  const uint32_t sub_tag = d.ctr->substeps;
+  const bool reuse_ok = d.ctr->gc_coloured + 1u == sub_tag;
   if (warm) {
     // find the pair's manifold of the previous substep on the dynamic body's list
     uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb;
@@ -660,6 +671,10 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
     if (old_slot != BB_NONE) {
       // Manifold::update_from_old (extensions.slang:306-473)
       int2 okc = d.m_keycc[prv][old_slot];
+      if (reuse_ok && !vox && okc.x == m.key) {
+        reuse = d.gc_slot_color[prv][old_slot];
+        d.gc_survived[old_slot] = sub_tag;
+      }
       float4 on4 = d.m_normal[prv][old_slot];
       sgn = swapped ? -1.f : 1.f;
       bool cross_key = m.key != okc.x || swapped;
@@ -751,6 +766,7 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
     d.c_anc_b[cur][cb + c] = f4(ab, 0.f);
   }
   d.hit[k] = 1;
+  d.gc_reuse[k] = reuse;
 }
 
 // Narrow phase + warm start: one thread per listed pair.

@@ -294,6 +294,7 @@ __global__ void k_begin_substep(DevCounters* c) {
       c->bounds_max[k] = 0u;
     }
   }
+  c->prev_manifolds = c->manifold_count;
   c->manifold_count = 0;
   c->contact_count = 0;
   c->pgs_manifolds = 0;
@@ -495,6 +496,9 @@ struct bb_world_impl {
     for (int k = 0; k < 2; ++k) { d.bucket_keys[k] = u32(P); d.bucket_vals[k] = u32(P); }
     d.bucket_start = u32(64);
     d.colour_awake = u32(BB_MAX_COLORS + 1);
+    d.gc_slot_color[0] = u32(P); d.gc_slot_color[1] = u32(P);
+    d.gc_reuse = u32(P); d.gc_survived = u32(P);
+    d.gc_body_chg = u32(N); d.gc_island_chg = u32(N);
     d.body_color = u32(N); d.body_color_round = u32(N);
     d.a_pos_start = f4(N); d.a_rot_start = f4(N); d.a_pos_tilde = f4(N); d.a_rot_tilde = f4(N);
     d.a_depth = u32(N);
@@ -530,6 +534,7 @@ struct bb_world_impl {
   void reset_contacts() {
     cudaMemsetAsync(d.frozen, 0, sizeof(uint32_t) * (cap_n + 1), stream);
     cudaMemsetAsync(&d.ctr->front_valid, 0, sizeof(uint32_t), stream);
+    cudaMemsetAsync(&d.ctr->gc_coloured, 0, sizeof(uint32_t), stream);
     cudaMemsetAsync(d.csr_start[0], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     cudaMemsetAsync(d.csr_start[1], 0, sizeof(uint32_t) * (cap_n + 2), stream);
     if (n) k_iota<<<(n + 255) / 256, 256, 0, stream>>>(d.vals[0], n);
@@ -1196,6 +1201,8 @@ bb_status bb_set_solver_params(void* world, const bb_solver_params* p) {
   if (p->quirks != w->params.quirks || p->penetration_cap != w->params.penetration_cap)
     CU(cudaMemsetAsync(w->d.frozen, 0, 4ull * (w->cap_n + 1), w->stream));
   CU(cudaMemsetAsync(&w->d.ctr->front_valid, 0, sizeof(uint32_t), w->stream));  // bounds, modes
+  // the colouring rounds (gc_rounds) may change: the next colouring starts afresh
+  CU(cudaMemsetAsync(&w->d.ctr->gc_coloured, 0, sizeof(uint32_t), w->stream));
   w->params = *p;
   if (!w->params.broad_threads) w->params.broad_threads = 128;
   if (!w->params.narrow_blocks_per_sm) w->params.narrow_blocks_per_sm = 16;

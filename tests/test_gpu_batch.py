@@ -365,3 +365,30 @@ def test_refilled_slot_steps_like_a_world_added():
         w2 = bb.World(total)
         w2.add_world(new, *scene_bounds(new))
         w2.refill_world(0, scs[1], *scene_bounds(scs[1]))
+
+
+@pytest.mark.parametrize("name", ["mixed_3000", "pyramids_4x300"])
+def test_colour_reuse_gives_the_same_bits(name):
+    """Islands whose manifolds are exactly last substep's keep last substep's colours instead of
+    running the colouring rounds.  Setting the parameters before every single-substep step makes
+    every colouring start afresh; both worlds must give the same bits, through piles that form
+    and break apart (mixed column) and piles that settle (pyramids)."""
+    sc = (scenes.mixed_column(n_bodies=3000, seed=2) if name == "mixed_3000"
+          else scenes.pyramids(n_pyramids=4, boxes_per=300, gap=-0.002))
+    p = params(bb.SOLVER_PGS_SOFT)
+    reused = bb.world_from_scene(sc, params=p)
+    fresh = bb.world_from_scene(sc, params=p)
+    applied = bb.SolverParams.from_buffer_copy(bytes(fresh.params))  # with the scene's Morton box
+    rounds = []
+    for _ in range(160):
+        reused.step(DT / 4, 1)
+        fresh.set_params(applied)
+        fresh.step(DT / 4, 1)
+        rounds.append(reused.stats()["graph_color_rounds"])
+    a, b = reused.read_state(), fresh.read_state()
+    assert reused.stats()["error_flags"] == 0 and fresh.stats()["error_flags"] == 0
+    assert min(rounds[40:]) < max(rounds)  # some substeps reused every island's colours
+    reused.close()
+    fresh.close()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
