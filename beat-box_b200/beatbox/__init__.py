@@ -123,7 +123,8 @@ class ServerStats(ctypes.Structure):
                 ("body_steps", ctypes.c_uint64), ("evictions", ctypes.c_uint64), ("worlds_created", ctypes.c_uint64),
                 ("resident_bytes", ctypes.c_uint64), ("active", ctypes.c_uint32), ("queued", ctypes.c_uint32),
                 ("resident_worlds", ctypes.c_uint32), ("known_worlds", ctypes.c_uint32),
-                ("materialise_s", ctypes.c_double), ("issue_s", ctypes.c_double)]
+                ("materialise_s", ctypes.c_double), ("issue_s", ctypes.c_double), ("batch_steps", ctypes.c_uint64),
+                ("slot_steps", ctypes.c_uint64)]
 
 
 class StepStats(ctypes.Structure):

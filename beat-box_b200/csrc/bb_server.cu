@@ -499,6 +499,7 @@ struct bb_server_impl {
             for (auto& sl : b->slots) any |= sl.req && sl.remaining > 0;
             if (!any) break;
             bb_status s = bb_step(b->w, b->dt, b->substeps);
+            ++st.batch_steps;
             cudaMemcpyAsync(b->err_host, bb_world_error_word(b->w), sizeof(uint32_t), cudaMemcpyDeviceToHost,
                             b->stream);
             cudaMemcpyAsync(b->err_host + 1, bb_world_error_site_word(b->w), sizeof(uint32_t),
@@ -511,6 +512,7 @@ struct bb_server_impl {
             for (uint32_t k = 0; k < b->slots.size(); ++k) {
               Slot& sl = b->slots[k];
               if (!sl.req || sl.remaining == 0) continue;
+              ++st.slot_steps;
               if (s != BB_OK) sl.req->result = s;
               if (--sl.remaining == 0) {  // its last step: stop the world after it, then retire
                 Req* q = sl.req;

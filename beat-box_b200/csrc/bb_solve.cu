@@ -1335,7 +1335,78 @@ __device__ float avbd_dir_C(const DevState& d, const Params& p, int cur, uint32_
 }
 
 // entry_avbd_primal (avbd.slang:478-658): Gauss-Newton step of body i on its 6 DoF.
-__device__ void avbd_primal(const DevState& d, const Params& p, int cur, uint32_t i, float dt, float alpha) {
+// One warp per body.  The lanes take the body's contacts (eight lanes per manifold of its list,
+// four manifolds at a time) and each sums its contacts' gradient and Hessian terms; a butterfly
+// over the lanes adds the sums (a fixed order, so the result does not depend on scheduling; it
+// differs from a serial sum in the last bits), and lane 0 adds the inertial terms, solves the
+// 6x6 system and moves the body.  Serially, a body's contact loop was one dependent chain per
+// colour step (16 contacts of a box in a pile: 15-30 us), which set the AVBD sweeps' pace.
+// H is kept as its lower triangle, row-major: entry (a, b), b <= a, at a * (a + 1) / 2 + b.
+__device__ __forceinline__ int avbd_lt(int a, int b) { return a * (a + 1) / 2 + b; }
+__device__ __forceinline__ void avbd_primal(const DevState& d, const Params& p, int cur, uint32_t i, float dt, float alpha) {
+  const int lane = threadIdx.x & 31;
+  float g[6], H[21];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) g[a] = 0.f;
+#pragma unroll
+  for (int a = 0; a < 21; ++a) H[a] = 0.f;
+  const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
+  for (uint32_t e0 = s0; e0 < s1; e0 += 4) {
+    const uint32_t e = e0 + uint32_t(lane >> 3);
+    const int j = lane & 7;
+    if (e >= s1) continue;
+    const uint32_t slot = d.man_slot[cur][d.csr_list[cur][e]];
+    const int cc = d.m_keycc[cur][slot].y;
+    if (j >= cc) continue;
+    const uint2 b = d.m_bodies[cur][slot];
+    const bool i1 = b.x == i;
+    const bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
+    const float mu = sqrtf(fmaxf(d.iinv[b.x].w, 0.f) * fmaxf(d.iinv[b.y].w, 0.f));
+    const float3 n = f3(d.m_normal[cur][slot]);
+    const float3 td[2] = {f3(d.m_t0[cur][slot]), f3(d.m_t1[cur][slot])};
+    const uint32_t ci = slot * BB_MAX_CONTACTS + uint32_t(j);
+    float3 rr1, rr2;
+    const float C = avbd_contact_C(d, p, cur, slot, ci, b, d1, d2, alpha, n, rr1, rr2);
+    const float4 lam = d.c_lam[cur][ci];
+    const float4 kt = d.c_kt[cur][ci];
+    const float f = fminf(lam.w * C + lam.x, 0.f);
+    const float3 Jl = i1 ? -n : n;
+    const float3 Ja = i1 ? -cross3(rr1, n) : cross3(rr2, n);
+    const float J[6] = {Jl.x, Jl.y, Jl.z, Ja.x, Ja.y, Ja.z};
+#pragma unroll
+    for (int a = 0; a < 6; ++a) g[a] += f * J[a];
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+      for (int bb = 0; bb <= a; ++bb) H[avbd_lt(a, bb)] += lam.w * J[a] * J[bb];
+    const float bound = mu * fabsf(lam.x);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      float3 ar1, ar2;
+      float C0t;
+      const float Ct = avbd_dir_C(d, p, cur, ci, b, d1, d2, alpha, td[t], ar1, ar2, C0t);
+      const float ktt = t == 0 ? kt.x : kt.y;
+      const float lt = t == 0 ? lam.y : lam.z;
+      const float ft = fminf(fmaxf(ktt * Ct + lt, -bound), bound);
+      const float3 Jlt = i1 ? -td[t] : td[t];
+      const float3 Jat = i1 ? -cross3(ar1, td[t]) : cross3(ar2, td[t]);
+      const float Jt[6] = {Jlt.x, Jlt.y, Jlt.z, Jat.x, Jat.y, Jat.z};
+#pragma unroll
+      for (int a = 0; a < 6; ++a) g[a] += ft * Jt[a];
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int bb = 0; bb <= a; ++bb) H[avbd_lt(a, bb)] += ktt * Jt[a] * Jt[bb];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) g[a] += __shfl_xor_sync(0xFFFFFFFFu, g[a], o);
+#pragma unroll
+    for (int a = 0; a < 21; ++a) H[a] += __shfl_xor_sync(0xFFFFFFFFu, H[a], o);
+  }
+  if (lane != 0) return;
   const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
   const float inv_dt2 = dt > 0.f ? 1.0f / (dt * dt) : 0.f;
   const float m_lin = d.vel[i].w * inv_dt2;
@@ -1349,118 +1420,65 @@ __device__ void avbd_primal(const DevState& d, const Params& p, int cur, uint32_
   r0 = r0 * inv;
   r1 = r1 * inv;
   r2 = r2 * inv;
-  float H[6][6];
-  float g[6];
-#pragma unroll
-  for (int a = 0; a < 6; ++a) {
-    g[a] = 0.f;
-#pragma unroll
-    for (int bb = 0; bb < 6; ++bb) H[a][bb] = 0.f;
-  }
-  H[0][0] = H[1][1] = H[2][2] = m_lin;
-  float Iw[3][3] = {{r0.x, r0.y, r0.z}, {r1.x, r1.y, r1.z}, {r2.x, r2.y, r2.z}};
+  const float Iw[3][3] = {{r0.x, r0.y, r0.z}, {r1.x, r1.y, r1.z}, {r2.x, r2.y, r2.z}};
+  H[avbd_lt(0, 0)] += m_lin;
+  H[avbd_lt(1, 1)] += m_lin;
+  H[avbd_lt(2, 2)] += m_lin;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int bb = 0; bb < 3; ++bb) H[3 + a][3 + bb] = Iw[a][bb] * inv_dt2;
-  float3 dpos = f3(d.pos[i]) - f3(d.a_pos_tilde[i]);
-  float3 dth = small_angle_delta(rot, q_from(d.a_rot_tilde[i]));
-  g[0] = m_lin * dpos.x;
-  g[1] = m_lin * dpos.y;
-  g[2] = m_lin * dpos.z;
-  float3 ga = make_float3(Iw[0][0] * dth.x + Iw[0][1] * dth.y + Iw[0][2] * dth.z,
-                          Iw[1][0] * dth.x + Iw[1][1] * dth.y + Iw[1][2] * dth.z,
-                          Iw[2][0] * dth.x + Iw[2][1] * dth.y + Iw[2][2] * dth.z) * inv_dt2;
-  g[3] = ga.x;
-  g[4] = ga.y;
-  g[5] = ga.z;
-  const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
-  for (uint32_t e = s0; e < s1; ++e) {
-    const uint32_t slot = d.man_slot[cur][d.csr_list[cur][e]];
-    const uint2 b = d.m_bodies[cur][slot];
-    const bool i1 = b.x == i;
-    const bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
-    const float mu = sqrtf(fmaxf(d.iinv[b.x].w, 0.f) * fmaxf(d.iinv[b.y].w, 0.f));
-    const float3 n = f3(d.m_normal[cur][slot]);
-    const float3 td[2] = {f3(d.m_t0[cur][slot]), f3(d.m_t1[cur][slot])};
-    const int cc = d.m_keycc[cur][slot].y;
-    for (int j = 0; j < cc; ++j) {
-      const uint32_t ci = slot * BB_MAX_CONTACTS + j;
-      float3 rr1, rr2;
-      float C = avbd_contact_C(d, p, cur, slot, ci, b, d1, d2, alpha, n, rr1, rr2);
-      const float4 lam = d.c_lam[cur][ci];
-      const float4 kt = d.c_kt[cur][ci];
-      float f = fminf(lam.w * C + lam.x, 0.f);
-      float3 Jl = i1 ? -n : n;
-      float3 Ja = i1 ? -cross3(rr1, n) : cross3(rr2, n);
-      float J[6] = {Jl.x, Jl.y, Jl.z, Ja.x, Ja.y, Ja.z};
-#pragma unroll
-      for (int a = 0; a < 6; ++a) g[a] += f * J[a];
-#pragma unroll
-      for (int a = 0; a < 6; ++a)
-#pragma unroll
-        for (int bb = 0; bb < 6; ++bb) H[a][bb] += lam.w * J[a] * J[bb];
-      const float bound = mu * fabsf(lam.x);
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        float3 ar1, ar2;
-        float C0t;
-        float Ct = avbd_dir_C(d, p, cur, ci, b, d1, d2, alpha, td[t], ar1, ar2, C0t);
-        const float ktt = t == 0 ? kt.x : kt.y;
-        const float lt = t == 0 ? lam.y : lam.z;
-        float ft = fminf(fmaxf(ktt * Ct + lt, -bound), bound);
-        float3 Jlt = i1 ? -td[t] : td[t];
-        float3 Jat = i1 ? -cross3(ar1, td[t]) : cross3(ar2, td[t]);
-        float Jt[6] = {Jlt.x, Jlt.y, Jlt.z, Jat.x, Jat.y, Jat.z};
-#pragma unroll
-        for (int a = 0; a < 6; ++a) g[a] += ft * Jt[a];
-#pragma unroll
-        for (int a = 0; a < 6; ++a)
-#pragma unroll
-          for (int bb = 0; bb < 6; ++bb) H[a][bb] += ktt * Jt[a] * Jt[bb];
-      }
-    }
-  }
+    for (int bb = 0; bb <= a; ++bb) H[avbd_lt(3 + a, 3 + bb)] += Iw[a][bb] * inv_dt2;
+  const float3 dpos = f3(d.pos[i]) - f3(d.a_pos_tilde[i]);
+  const float3 dth = small_angle_delta(rot, q_from(d.a_rot_tilde[i]));
+  g[0] += m_lin * dpos.x;
+  g[1] += m_lin * dpos.y;
+  g[2] += m_lin * dpos.z;
+  const float3 ga = make_float3(Iw[0][0] * dth.x + Iw[0][1] * dth.y + Iw[0][2] * dth.z,
+                                Iw[1][0] * dth.x + Iw[1][1] * dth.y + Iw[1][2] * dth.z,
+                                Iw[2][0] * dth.x + Iw[2][1] * dth.y + Iw[2][2] * dth.z) * inv_dt2;
+  g[3] += ga.x;
+  g[4] += ga.y;
+  g[5] += ga.z;
   // avbd_solve6: in-place LDL^T, diagonal floor 1e-8
   float x[6], rhs[6];
 #pragma unroll
   for (int a = 0; a < 6; ++a) rhs[a] = -g[a];
 #pragma unroll
   for (int jj = 0; jj < 6; ++jj) {
-    float dd = H[jj][jj];
+    float dd = H[avbd_lt(jj, jj)];
 #pragma unroll
     for (int kk = 0; kk < 6; ++kk)
-      if (kk < jj) dd -= H[jj][kk] * H[jj][kk] * H[kk][kk];
+      if (kk < jj) dd -= H[avbd_lt(jj, kk)] * H[avbd_lt(jj, kk)] * H[avbd_lt(kk, kk)];
     dd = fmaxf(dd, 1e-8f);
-    H[jj][jj] = dd;
+    H[avbd_lt(jj, jj)] = dd;
 #pragma unroll
     for (int ii = 0; ii < 6; ++ii) {
       if (ii > jj) {
-        float s = H[ii][jj];
+        float sm = H[avbd_lt(ii, jj)];
 #pragma unroll
         for (int kk = 0; kk < 6; ++kk)
-          if (kk < jj) s -= H[ii][kk] * H[jj][kk] * H[kk][kk];
-        H[ii][jj] = s / dd;
+          if (kk < jj) sm -= H[avbd_lt(ii, kk)] * H[avbd_lt(jj, kk)] * H[avbd_lt(kk, kk)];
+        H[avbd_lt(ii, jj)] = sm / dd;
       }
     }
   }
 #pragma unroll
   for (int ii = 0; ii < 6; ++ii) {
-    float s = rhs[ii];
+    float sm = rhs[ii];
 #pragma unroll
     for (int kk = 0; kk < 6; ++kk)
-      if (kk < ii) s -= H[ii][kk] * rhs[kk];
-    rhs[ii] = s;
+      if (kk < ii) sm -= H[avbd_lt(ii, kk)] * rhs[kk];
+    rhs[ii] = sm;
   }
 #pragma unroll
-  for (int ii = 0; ii < 6; ++ii) rhs[ii] /= H[ii][ii];
+  for (int ii = 0; ii < 6; ++ii) rhs[ii] /= H[avbd_lt(ii, ii)];
 #pragma unroll
   for (int ii = 5; ii >= 0; --ii) {
-    float s = rhs[ii];
+    float sm = rhs[ii];
 #pragma unroll
     for (int kk = 0; kk < 6; ++kk)
-      if (kk > ii) s -= H[kk][ii] * x[kk];
-    x[ii] = s;
+      if (kk > ii) sm -= H[avbd_lt(kk, ii)] * x[kk];
+    x[ii] = sm;
   }
   float4 ps = d.pos[i];
   d.pos[i] = make_float4(ps.x + x[0], ps.y + x[1], ps.z + x[2], ps.w);
@@ -1537,6 +1555,7 @@ __device__ void avbd_finalize(const DevState& d, int cur, uint32_t i, float dt) 
 __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevState d, Params p, int cur, uint32_t n, float dt,
                                                            int phase) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const uint32_t wid = tid >> 5, nwarps = stride >> 5;  // a body per warp in the primal sweeps
   const uint32_t* list = d.a_bucket_vals[1];
   uint32_t* sync = &d.ctr->sync_count[3 + phase];
   uint32_t ep = 0;
@@ -1547,7 +1566,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
       for (uint32_t c = 0; c < C; ++c) {
         uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
         if (s0 == s1) continue;
-        for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 1.0f);
+        for (uint32_t k = s0 + wid; k < s1; k += nwarps) avbd_primal(d, p, cur, list[k], dt, 1.0f);
         grid_sync(d.ctr, sync, ep);
       }
       for (uint32_t m = tid; m < M; m += stride) avbd_dual(d, p, cur, m);
@@ -1560,7 +1579,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
     for (uint32_t key = 0; key < nb; ++key) {
       uint32_t s0 = d.a_bucket_start[key], s1 = d.a_bucket_start[key + 1];
       if (s0 == s1) continue;
-      for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 0.0f);
+      for (uint32_t k = s0 + wid; k < s1; k += nwarps) avbd_primal(d, p, cur, list[k], dt, 0.0f);
       grid_sync(d.ctr, sync, ep);
     }
   } else {
@@ -1569,7 +1588,7 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
       for (uint32_t c = 0; c < C; ++c) {
         uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
         if (s0 == s1) continue;
-        for (uint32_t k = s0 + tid; k < s1; k += stride) avbd_primal(d, p, cur, list[k], dt, 0.0f);
+        for (uint32_t k = s0 + wid; k < s1; k += nwarps) avbd_primal(d, p, cur, list[k], dt, 0.0f);
         grid_sync(d.ctr, sync, ep);
       }
     }

@@ -524,6 +524,8 @@ typedef struct bb_server_stats {
   uint32_t active, queued, resident_worlds, known_worlds;
   double materialise_s;      /* worker time spent creating / loading worlds */
   double issue_s;            /* worker time spent enqueueing steps (includes graph captures) */
+  uint64_t batch_steps;      /* steps of batched worlds enqueued */
+  uint64_t slot_steps;       /* world-steps they advanced (running requests per batch step, summed) */
 } bb_server_stats;
 
 bb_status bb_server_create(const bb_server_desc* desc, void** out_server);
