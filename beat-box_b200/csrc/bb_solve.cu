@@ -1335,78 +1335,81 @@ __device__ float avbd_dir_C(const DevState& d, const Params& p, int cur, uint32_
 }
 
 // entry_avbd_primal (avbd.slang:478-658): Gauss-Newton step of body i on its 6 DoF.
-// One warp per body.  The lanes take the body's contacts (eight lanes per manifold of its list,
-// four manifolds at a time) and each sums its contacts' gradient and Hessian terms; a butterfly
-// over the lanes adds the sums (a fixed order, so the result does not depend on scheduling; it
-// differs from a serial sum in the last bits), and lane 0 adds the inertial terms, solves the
-// 6x6 system and moves the body.  Serially, a body's contact loop was one dependent chain per
-// colour step (16 contacts of a box in a pile: 15-30 us), which set the AVBD sweeps' pace.
+// A group of AVBD_LANES lanes per body.  Lane l of the group takes manifolds l, l + AVBD_LANES, ...
+// of the body's list and sums their contacts' gradient and Hessian terms in order; a butterfly
+// over the group adds the lanes' sums (a fixed order, so the result does not depend on
+// scheduling or on which bodies share a warp; it differs from a serial sum in the last bits),
+// and the group's lane 0 adds the inertial terms, solves the 6x6 system and moves the body.
+// Serially, a body's whole contact loop was one dependent chain per colour step (a box in a
+// pile: 15-30 us); a warp per body cut the chain but left too few bodies in flight where a
+// colour holds tens of thousands of them.  i == BB_NONE: the group only takes part in the
+// shuffles (the trips over a colour's bodies are warp-uniform).
 // H is kept as its lower triangle, row-major: entry (a, b), b <= a, at a * (a + 1) / 2 + b.
+#define AVBD_LANES 8
+#define AVBD_GROUPS (32 / AVBD_LANES)
 __device__ __forceinline__ int avbd_lt(int a, int b) { return a * (a + 1) / 2 + b; }
 __device__ __forceinline__ void avbd_primal(const DevState& d, const Params& p, int cur, uint32_t i, float dt, float alpha) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (AVBD_LANES - 1);
   float g[6], H[21];
 #pragma unroll
   for (int a = 0; a < 6; ++a) g[a] = 0.f;
 #pragma unroll
   for (int a = 0; a < 21; ++a) H[a] = 0.f;
-  const uint32_t s0 = d.csr_start[cur][i], s1 = d.csr_start[cur][i + 1];
-  for (uint32_t e0 = s0; e0 < s1; e0 += 4) {
-    const uint32_t e = e0 + uint32_t(lane >> 3);
-    const int j = lane & 7;
-    if (e >= s1) continue;
+  const uint32_t s0 = i == BB_NONE ? 0u : d.csr_start[cur][i], s1 = i == BB_NONE ? 0u : d.csr_start[cur][i + 1];
+  for (uint32_t e = s0 + uint32_t(lane); e < s1; e += AVBD_LANES) {
     const uint32_t slot = d.man_slot[cur][d.csr_list[cur][e]];
     const int cc = d.m_keycc[cur][slot].y;
-    if (j >= cc) continue;
     const uint2 b = d.m_bodies[cur][slot];
     const bool i1 = b.x == i;
     const bool d1 = awake(d.flags[b.x]), d2 = awake(d.flags[b.y]);
     const float mu = sqrtf(fmaxf(d.iinv[b.x].w, 0.f) * fmaxf(d.iinv[b.y].w, 0.f));
     const float3 n = f3(d.m_normal[cur][slot]);
     const float3 td[2] = {f3(d.m_t0[cur][slot]), f3(d.m_t1[cur][slot])};
-    const uint32_t ci = slot * BB_MAX_CONTACTS + uint32_t(j);
-    float3 rr1, rr2;
-    const float C = avbd_contact_C(d, p, cur, slot, ci, b, d1, d2, alpha, n, rr1, rr2);
-    const float4 lam = d.c_lam[cur][ci];
-    const float4 kt = d.c_kt[cur][ci];
-    const float f = fminf(lam.w * C + lam.x, 0.f);
-    const float3 Jl = i1 ? -n : n;
-    const float3 Ja = i1 ? -cross3(rr1, n) : cross3(rr2, n);
-    const float J[6] = {Jl.x, Jl.y, Jl.z, Ja.x, Ja.y, Ja.z};
+    for (int j = 0; j < cc; ++j) {
+      const uint32_t ci = slot * BB_MAX_CONTACTS + uint32_t(j);
+      float3 rr1, rr2;
+      const float C = avbd_contact_C(d, p, cur, slot, ci, b, d1, d2, alpha, n, rr1, rr2);
+      const float4 lam = d.c_lam[cur][ci];
+      const float4 kt = d.c_kt[cur][ci];
+      const float f = fminf(lam.w * C + lam.x, 0.f);
+      const float3 Jl = i1 ? -n : n;
+      const float3 Ja = i1 ? -cross3(rr1, n) : cross3(rr2, n);
+      const float J[6] = {Jl.x, Jl.y, Jl.z, Ja.x, Ja.y, Ja.z};
 #pragma unroll
-    for (int a = 0; a < 6; ++a) g[a] += f * J[a];
-#pragma unroll
-    for (int a = 0; a < 6; ++a)
-#pragma unroll
-      for (int bb = 0; bb <= a; ++bb) H[avbd_lt(a, bb)] += lam.w * J[a] * J[bb];
-    const float bound = mu * fabsf(lam.x);
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      float3 ar1, ar2;
-      float C0t;
-      const float Ct = avbd_dir_C(d, p, cur, ci, b, d1, d2, alpha, td[t], ar1, ar2, C0t);
-      const float ktt = t == 0 ? kt.x : kt.y;
-      const float lt = t == 0 ? lam.y : lam.z;
-      const float ft = fminf(fmaxf(ktt * Ct + lt, -bound), bound);
-      const float3 Jlt = i1 ? -td[t] : td[t];
-      const float3 Jat = i1 ? -cross3(ar1, td[t]) : cross3(ar2, td[t]);
-      const float Jt[6] = {Jlt.x, Jlt.y, Jlt.z, Jat.x, Jat.y, Jat.z};
-#pragma unroll
-      for (int a = 0; a < 6; ++a) g[a] += ft * Jt[a];
+      for (int a = 0; a < 6; ++a) g[a] += f * J[a];
 #pragma unroll
       for (int a = 0; a < 6; ++a)
 #pragma unroll
-        for (int bb = 0; bb <= a; ++bb) H[avbd_lt(a, bb)] += ktt * Jt[a] * Jt[bb];
+        for (int bb = 0; bb <= a; ++bb) H[avbd_lt(a, bb)] += lam.w * J[a] * J[bb];
+      const float bound = mu * fabsf(lam.x);
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        float3 ar1, ar2;
+        float C0t;
+        const float Ct = avbd_dir_C(d, p, cur, ci, b, d1, d2, alpha, td[t], ar1, ar2, C0t);
+        const float ktt = t == 0 ? kt.x : kt.y;
+        const float lt = t == 0 ? lam.y : lam.z;
+        const float ft = fminf(fmaxf(ktt * Ct + lt, -bound), bound);
+        const float3 Jlt = i1 ? -td[t] : td[t];
+        const float3 Jat = i1 ? -cross3(ar1, td[t]) : cross3(ar2, td[t]);
+        const float Jt[6] = {Jlt.x, Jlt.y, Jlt.z, Jat.x, Jat.y, Jat.z};
+#pragma unroll
+        for (int a = 0; a < 6; ++a) g[a] += ft * Jt[a];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+          for (int bb = 0; bb <= a; ++bb) H[avbd_lt(a, bb)] += ktt * Jt[a] * Jt[bb];
+      }
     }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
+  for (int o = AVBD_LANES / 2; o > 0; o >>= 1) {
 #pragma unroll
     for (int a = 0; a < 6; ++a) g[a] += __shfl_xor_sync(0xFFFFFFFFu, g[a], o);
 #pragma unroll
     for (int a = 0; a < 21; ++a) H[a] += __shfl_xor_sync(0xFFFFFFFFu, H[a], o);
   }
-  if (lane != 0) return;
+  if (lane != 0 || i == BB_NONE) return;
   const bool tq = p.quirks & BB_QUIRK_INERTIA_TRANSPOSE;
   const float inv_dt2 = dt > 0.f ? 1.0f / (dt * dt) : 0.f;
   const float m_lin = d.vel[i].w * inv_dt2;
@@ -1555,7 +1558,8 @@ __device__ void avbd_finalize(const DevState& d, int cur, uint32_t i, float dt) 
 __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevState d, Params p, int cur, uint32_t n, float dt,
                                                            int phase) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  const uint32_t wid = tid >> 5, nwarps = stride >> 5;  // a body per warp in the primal sweeps
+  // primal sweeps: AVBD_GROUPS bodies per warp (AVBD_LANES lanes each), warp-uniform trips
+  const uint32_t wid = tid >> 5, nwarps = stride >> 5, grp = (threadIdx.x & 31u) / AVBD_LANES;
   const uint32_t* list = d.a_bucket_vals[1];
   uint32_t* sync = &d.ctr->sync_count[3 + phase];
   uint32_t ep = 0;
@@ -1566,7 +1570,8 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
       for (uint32_t c = 0; c < C; ++c) {
         uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
         if (s0 == s1) continue;
-        for (uint32_t k = s0 + wid; k < s1; k += nwarps) avbd_primal(d, p, cur, list[k], dt, 1.0f);
+        for (uint32_t kw = s0 + wid * AVBD_GROUPS; kw < s1; kw += nwarps * AVBD_GROUPS)
+          avbd_primal(d, p, cur, kw + grp < s1 ? list[kw + grp] : BB_NONE, dt, 1.0f);
         grid_sync(d.ctr, sync, ep);
       }
       for (uint32_t m = tid; m < M; m += stride) avbd_dual(d, p, cur, m);
@@ -1579,7 +1584,8 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
     for (uint32_t key = 0; key < nb; ++key) {
       uint32_t s0 = d.a_bucket_start[key], s1 = d.a_bucket_start[key + 1];
       if (s0 == s1) continue;
-      for (uint32_t k = s0 + wid; k < s1; k += nwarps) avbd_primal(d, p, cur, list[k], dt, 0.0f);
+      for (uint32_t kw = s0 + wid * AVBD_GROUPS; kw < s1; kw += nwarps * AVBD_GROUPS)
+        avbd_primal(d, p, cur, kw + grp < s1 ? list[kw + grp] : BB_NONE, dt, 0.0f);
       grid_sync(d.ctr, sync, ep);
     }
   } else {
@@ -1588,7 +1594,8 @@ __global__ void __launch_bounds__(BB_COOP_THREADS, 1) k_avbd_solve(const DevStat
       for (uint32_t c = 0; c < C; ++c) {
         uint32_t s0 = d.a_bucket_start[c], s1 = d.a_bucket_start[c + 1];
         if (s0 == s1) continue;
-        for (uint32_t k = s0 + wid; k < s1; k += nwarps) avbd_primal(d, p, cur, list[k], dt, 0.0f);
+        for (uint32_t kw = s0 + wid * AVBD_GROUPS; kw < s1; kw += nwarps * AVBD_GROUPS)
+          avbd_primal(d, p, cur, kw + grp < s1 ? list[kw + grp] : BB_NONE, dt, 0.0f);
         grid_sync(d.ctr, sync, ep);
       }
     }
