@@ -473,13 +473,15 @@ bb_status bb_autotune(void* world, float dt, uint32_t substeps, uint32_t trial_s
 
 /* ---- serving loop ---------------------------------------------------------------------
  * Step requests for many worlds, kept resident on the device between requests, admitted by an
- * HBM budget; requests that arrive while others run start as soon as a slot and memory are
- * free, and their steps overlap on the device (one stream per world).  A request either
- * creates a world (its key not seen before; shapes and bodies given) or continues one.  A
- * world runs its requests one after another in submission order; its result does not depend
- * on the other requests in flight.  Idle worlds may be evicted to make room: their body state
- * is kept on the host and reloaded (warm-start contacts restart).  No reference counterpart:
- * the reference steps one scene per frame from its render loop (src/renderer_manager.cpp:254). */
+ * HBM budget (continuous batching).  Worlds of one step class (solver parameters, dt,
+ * substeps) sit as slots of one batched world, and each step of that batch advances every
+ * running request in it; requests that arrive while others run join at the next step.  A
+ * request either creates a world (its key not seen before; shapes and bodies given) or
+ * continues one.  A world runs its requests one after another in submission order; its result
+ * does not depend on the other requests in flight.  A world that changes step class moves to
+ * that class's batch (warm-start contacts restart); idle worlds may be evicted to make room
+ * (their body state is kept on the host).  No reference counterpart: the reference steps one
+ * scene per frame from its render loop (src/renderer_manager.cpp:254). */
 typedef struct bb_shape_desc {
   uint32_t type;   /* BB_SHAPE_BOX or BB_SHAPE_SPHERE */
   float half[3];   /* half extents; sphere radius in half[0] */
