@@ -9,7 +9,8 @@ void bb_launch_scan(cudaStream_t s, const uint32_t* in, uint32_t* out, const uin
                     const uint32_t* skip = nullptr);
 uint32_t bb_scan_tiles(uint32_t n_cap);
 uint32_t bb_sort_tiles(uint32_t n_cap);
-#define BB_SORT_TILE 4096  // keys per onesweep tile
+void onesweep_smem_attr();  // k_onesweep's dynamic shared memory size, once per device
+#define BB_SORT_TILE 8192  // keys per onesweep tile
 // hist regions are BB_HIST_REGION words: 8 rows of counts + 8 rows of exclusive starts
 #define BB_HIST_REGION (2 * 8 * 256)
 void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,

@@ -4,7 +4,7 @@
 // transfer between passes, src/shaders/simulation/RB_sim.slang:113-203,
 // src/shaders/simulation/LBVH.slang:34-152, RBM:1288-1295) with:
 //   * one histogram kernel that counts all digit positions in a single read of the keys,
-//   * one onesweep kernel per digit: tiles of 4096 keys rank themselves with warp-level
+//   * one onesweep kernel per digit: tiles of 8192 keys rank themselves with warp-level
 //     multisplit (one ballot per digit bit), publish per-digit tile totals, resolve their global
 //     offsets by decoupled look-back over the preceding tiles, reorder the tile by digit in
 //     shared memory and write each digit's run contiguously (coalesced stores).
@@ -17,8 +17,9 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kItems = 8;
 constexpr int kTile = kThreads * kItems;  // 2048 (scan)
-constexpr int kSortItems = BB_SORT_TILE / kThreads;  // 16 keys per thread in a onesweep tile
-static_assert(kSortItems * kThreads == BB_SORT_TILE, "onesweep tile");
+constexpr int kSortThreads = 512;  // onesweep block
+constexpr int kSortItems = BB_SORT_TILE / kSortThreads;  // 16 keys per thread in a onesweep tile
+static_assert(kSortItems * kSortThreads == BB_SORT_TILE, "onesweep tile");
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1u;
@@ -218,25 +219,33 @@ __device__ __forceinline__ uint32_t sort_lookback(volatile uint32_t* st, uint32_
 }
 
 // one stable onesweep pass on digit (key >> shift) & 255, or (lut[value] >> shift) & 255
-// when lut is given
-__global__ void __launch_bounds__(kThreads, 3) k_onesweep(const uint32_t* __restrict__ keys_in,
-                                                          const uint32_t* __restrict__ vals_in,
-                                                          uint32_t* __restrict__ keys_out,
-                                                          uint32_t* __restrict__ vals_out,
-                                                          const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
-                                                          const uint32_t* __restrict__ digit_start, int shift,
-                                                          const uint32_t* __restrict__ lut, uint32_t* status,
-                                                          uint32_t* tile_ctr, DevCounters* ctr) {
+// when lut is given.  A tile is BB_SORT_TILE = 8192 keys on kSortThreads = 512 threads (16 keys
+// each), so each digit's run in a tile averages 32 keys (128-byte lines when written out).  The
+// values are read when the tile is reordered, not held through the ranking (registers: two
+// blocks per SM); with a lut the digit needs the value, which the ranking reads then.
+// Shared memory (dynamic, kSortSmem bytes): per-warp digit counts 16 x 256, keys and values of
+// the tile, the digit of each reordered position.
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr size_t kSortSmem = size_t(kSortWarps) * 256 * 4 + size_t(BB_SORT_TILE) * (4 + 4 + 1);
+__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __restrict__ keys_in,
+                                                              const uint32_t* __restrict__ vals_in,
+                                                              uint32_t* __restrict__ keys_out,
+                                                              uint32_t* __restrict__ vals_out,
+                                                              const uint32_t* __restrict__ n_ptr, uint32_t n_fixed,
+                                                              const uint32_t* __restrict__ digit_start, int shift,
+                                                              const uint32_t* __restrict__ lut, uint32_t* status,
+                                                              uint32_t* tile_ctr, DevCounters* ctr) {
+  extern __shared__ __align__(16) uint8_t s_dyn[];
+  uint32_t(*s_warp_hist)[256] = reinterpret_cast<uint32_t(*)[256]>(s_dyn);
+  uint32_t* s_keys = reinterpret_cast<uint32_t*>(s_dyn + size_t(kSortWarps) * 256 * 4);
+  uint32_t* s_vals = s_keys + BB_SORT_TILE;
+  uint8_t* s_dig = reinterpret_cast<uint8_t*>(s_vals + BB_SORT_TILE);
   __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_warp_hist[kThreads / 32][256];
   __shared__ uint32_t s_offset[256];  // global position of this tile's first key of digit d
   __shared__ uint32_t s_local[256];   // tile position of its first key of digit d
-  __shared__ uint32_t s_wsum[kThreads / 32];
-  __shared__ uint32_t s_keys[BB_SORT_TILE];
-  __shared__ uint32_t s_vals[BB_SORT_TILE];
-  __shared__ uint8_t s_dig[BB_SORT_TILE];
+  __shared__ uint32_t s_wsum[8];
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
-  for (int i = threadIdx.x; i < (kThreads / 32) * 256; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&s_warp_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
   const uint32_t tile = s_tile;
@@ -245,21 +254,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_onesweep(const uint32_t* __rest
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t first = base + warp * (32 * kSortItems) + lane;
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const uint32_t i = first + k * 32;
     key[k] = i < n ? keys_in[i] : 0u;
-    val[k] = i < n ? vals_in[i] : 0u;
   }
   // warp-level multisplit: rank of each key among its warp's keys of the same digit, in order.
   // The lanes holding the same digit are found with one ballot per digit bit (plus one for the
   // keys past n); only the lowest of them reads and advances the warp's count of that digit, and
-  // the others take the old count from it by a shuffle.
+  // the others take the old count from it by a shuffle.  rank keeps the digit in its top 8 bits.
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const bool valid = first + k * 32 < n;
-    const uint32_t d = valid ? sort_digit(key[k], val[k], lut, shift) : 0u;
+    const uint32_t d = valid ? sort_digit(key[k], lut ? vals_in[first + k * 32] : 0u, lut, shift) : 0u;
     uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
     if (!valid) peers = ~peers;
 #pragma unroll
@@ -274,64 +282,78 @@ __global__ void __launch_bounds__(kThreads, 3) k_onesweep(const uint32_t* __rest
       s_warp_hist[warp][d] = prior + __popc(peers);
     }
     prior = __shfl_sync(0xFFFFFFFFu, prior, leader);
-    rank[k] = prior + __popc(peers & lt_mask);
+    rank[k] = (d << 24) | (prior + __popc(peers & lt_mask));
     __syncwarp();
   }
-
   __syncthreads();
-  // per digit t: exclusive prefix over warps, and the tile's count of digit t
+  // per digit t (threads 0..255): exclusive prefix over warps, and the tile's count of digit t
   const uint32_t t = threadIdx.x;
-  uint32_t sum = 0;
-#pragma unroll
-  for (int w = 0; w < kThreads / 32; ++w) {
-    uint32_t c = s_warp_hist[w][t];
-    s_warp_hist[w][t] = sum;
-    sum += c;
-  }
   volatile uint32_t* st = status;
-  // publish the tile's counts first, so that later tiles can look past this one early
-  st[tile * 256 + t] = (tile == 0 ? kFlagPrefix : kFlagAgg) | sum;
-  // tile-local start of each digit: block exclusive scan of the counts
-  {
-    uint32_t x = sum;
+  uint32_t sum = 0, x = 0;
+  if (t < 256) {
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = s_warp_hist[w][t];
+      s_warp_hist[w][t] = sum;
+      sum += c;
+    }
+    // publish the tile's counts first, so that later tiles can look past this one early
+    st[tile * 256 + t] = (tile == 0 ? kFlagPrefix : kFlagAgg) | sum;
+    // tile-local start of each digit: block exclusive scan of the counts (warps 0..7)
+    x = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
       if (lane >= o) x += y;
     }
     if (lane == 31) s_wsum[warp] = x;
-    __syncthreads();
+  }
+  __syncthreads();
+  if (t < 256) {
     uint32_t wo = 0;
     for (int w = 0; w < warp; ++w) wo += s_wsum[w];
     s_local[t] = wo + x - sum;
+    // keys of digit t in the preceding tiles
+    uint32_t excl = 0;
+    if (tile > 0) {
+      excl = sort_lookback(st, tile, t, ctr);
+      st[tile * 256 + t] = kFlagPrefix | (excl + sum);
+    }
+    s_offset[t] = digit_start[t] + excl;
   }
-  // keys of digit t in the preceding tiles
-  uint32_t excl = 0;
-  if (tile > 0) {
-    excl = sort_lookback(st, tile, t, ctr);
-    st[tile * 256 + t] = kFlagPrefix | (excl + sum);
-  }
-  s_offset[t] = digit_start[t] + excl;
   __syncthreads();
   // reorder the tile by digit (stable: warps and ranks follow the input order) ...
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
-    if (first + k * 32 < n) {
-      const uint32_t d = sort_digit(key[k], val[k], lut, shift);
-      const uint32_t lp = s_local[d] + s_warp_hist[warp][d] + rank[k];
+    const uint32_t i = first + k * 32;
+    if (i < n) {
+      const uint32_t d = rank[k] >> 24;
+      const uint32_t lp = s_local[d] + s_warp_hist[warp][d] + (rank[k] & 0xFFFFFFu);
       s_keys[lp] = key[k];
-      s_vals[lp] = val[k];
+      s_vals[lp] = vals_in[i];
       s_dig[lp] = uint8_t(d);
     }
   }
   __syncthreads();
   // ... and write each digit's run of the tile contiguously
   const uint32_t nt = min(uint32_t(BB_SORT_TILE), n - base);
-  for (uint32_t i = t; i < nt; i += kThreads) {
+  for (uint32_t i = t; i < nt; i += kSortThreads) {
     const uint32_t d = s_dig[i];
     const uint32_t dst = s_offset[d] + (i - s_local[d]);
     keys_out[dst] = s_keys[i];
     vals_out[dst] = s_vals[i];
+  }
+}
+
+// dynamic shared memory of k_onesweep above the 48 KB default: set once per device (the first
+// sort on a device should come before any stream capture; bb_world_create makes that call)
+void onesweep_smem_attr() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !done[dev]) {
+    cudaFuncSetAttribute((const void*)k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSortSmem));
+    done[dev] = true;
   }
 }
 
@@ -355,6 +377,7 @@ uint32_t bb_sort_tiles(uint32_t n_cap) { return n_cap / BB_SORT_TILE + 1; }
 void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* dst_keys[2],
                        uint32_t* dst_vals[2], uint32_t n, int passes, uint32_t* hist, uint32_t* status,
                        uint32_t* tile_ctr, DevCounters* ctr, int sms) {
+  onesweep_smem_attr();
   uint32_t tiles = (n + BB_SORT_TILE - 1) / BB_SORT_TILE;
   if (tiles == 0) tiles = 1;
   k_sort_hist<<<sms * 4, kThreads, 0, s>>>(keys_in, vals_in, nullptr, nullptr, n, hist, passes, 0, 0);
@@ -363,7 +386,7 @@ void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* 
   const uint32_t* iv = vals_in;
   for (int p = 0; p < passes; ++p) {
     int o = (passes - 1 - p) & 1;
-    k_onesweep<<<tiles, kThreads, 0, s>>>(ik, iv, dst_keys[o], dst_vals[o], nullptr, n, hist + 8 * 256 + p * 256, 8 * p,
+    k_onesweep<<<tiles, kSortThreads, kSortSmem, s>>>(ik, iv, dst_keys[o], dst_vals[o], nullptr, n, hist + 8 * 256 + p * 256, 8 * p,
                                           nullptr, status + size_t(p) * tiles * 256, tile_ctr + p, ctr);
     ik = dst_keys[o];
     iv = dst_vals[o];
@@ -377,6 +400,7 @@ void bb_launch_sort_to(cudaStream_t s, const uint32_t* keys_in, const uint32_t* 
 void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const uint32_t* n_dev, uint32_t n_cap,
                     int passes, int shift0, uint32_t* hist, uint32_t* status, uint32_t* tile_ctr, DevCounters* ctr,
                     int sms, const uint32_t* lut, int lut_passes) {
+  onesweep_smem_attr();
   uint32_t tiles = (n_cap + BB_SORT_TILE - 1) / BB_SORT_TILE;
   if (tiles == 0) tiles = 1;
   const int total = passes + (lut ? lut_passes : 0);
@@ -386,7 +410,7 @@ void bb_launch_sort(cudaStream_t s, uint32_t* keys[2], uint32_t* vals[2], const 
   for (int p = 0; p < total; ++p) {
     int in = p & 1, out = in ^ 1;
     bool by_lut = p >= passes;
-    k_onesweep<<<tiles, kThreads, 0, s>>>(keys[in], vals[in], keys[out], vals[out], n_dev, n_cap,
+    k_onesweep<<<tiles, kSortThreads, kSortSmem, s>>>(keys[in], vals[in], keys[out], vals[out], n_dev, n_cap,
                                           hist + 8 * 256 + p * 256, by_lut ? 8 * (p - passes) : shift0 + 8 * p,
                                           by_lut ? lut : nullptr, status + size_t(p) * tiles * 256, tile_ctr + p,
                                           ctr);

@@ -761,6 +761,7 @@ bb_status bb_world_create(const bb_world_desc* desc, void** out_world) {
   };
   w->coop_edge = fit(bb_edge_coloring_blocks(w->sms), w->cap_n, 1024);
   w->coop_pgs = fit(bb_pgs_soft_blocks(w->sms), w->cap_n / 2, 256);
+  onesweep_smem_attr();
   w->coop_avbd = fit(bb_avbd_blocks(w->sms), w->cap_n / 2, 512);
   w->coop_cc = fit(bb_components_blocks(w->sms), w->cap_n, 512);
   // The zero fills run on the world's stream ahead of everything the world does later.  On a

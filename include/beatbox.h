@@ -441,7 +441,7 @@ uint64_t bb_kernel_launch_count(void* world);
 bb_status bb_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                               uint32_t* vals_out, uint32_t n, uint32_t key_bits, void* stream);
 
-/* bb_radix_sort_pairs with the same results that allocates nothing: its scratch (about 2.4 MB)
+/* bb_radix_sort_pairs with the same results that allocates nothing: its scratch (about 2.3 MB)
  * is a fixed device array in the library, so n is limited to BB_SORT_STATIC_MAX_KEYS (larger n
  * returns BB_E_INVALID).  The first call on a device (with that device current) looks the
  * array's address up; make it before any stream capture.  Every call clears the part of the
