@@ -49,6 +49,8 @@ def test_each_world_is_the_same_alone_and_in_the_mix():
     assert st["completed"] == len(PLAN)
     # every world of a step class shares one batch: PGS_SOFT and AVBD
     assert st["worlds_created"] == 2
+    # every request's steps were advanced by batch steps, several worlds per step at times
+    assert st["slot_steps"] == sum(s for _, s in PLAN) and 0 < st["batch_steps"] < st["slot_steps"]
     assert st["body_steps"] == sum(int(worlds[w]["n"]) * s for w, s in PLAN)
     mixed = {w: mix.read_state(1000 + w, int(worlds[w]["n"])) for w in range(len(worlds))}
     mix.close()
