@@ -148,7 +148,10 @@ __device__ __forceinline__ float3 xrel(float3 r1, float3 r2, float3 va, float3 w
   return xsub(xadd(vb, xcross(wb, r2)), xadd(va, xcross(wa, r1)));
 }
 
-// one contact of PGS_SOFT::solve (solvers.slang:209-277): two friction rows, then the normal row
+// one contact of PGS_SOFT::solve (solvers.slang:209-277): two friction rows, then the normal row.
+// Both friction rows take their impulse from the same relative velocity (computed once, before
+// either is applied, as the reference does), so their two impulses are applied as one sum: the
+// same result up to rounding, with one body update instead of two.
 __device__ __forceinline__ void pgs_contact_solve(float4 R1, float4 R2, float4 K, float4& lam, float3 n, float3 t0,
                                                   float3 t1, float mu, bool use_bias, bool accum, bool fric, float ima,
                                                   float imb, const Sym3& IA, const Sym3& IB, float3& va, float3& wa,
@@ -156,22 +159,22 @@ __device__ __forceinline__ void pgs_contact_solve(float4 R1, float4 R2, float4 K
   const float3 r1 = f3(R1), r2 = f3(R2);
   if (fric) {
     const float3 rv = xrel(r1, r2, va, wa, vb, wb);
-    float imp_t[2] = {lam.y, lam.z};
+    float imp_t[2] = {lam.y, lam.z}, ti[2];
     const float tmass[2] = {R2.w, K.x};
     const float maxf = __fmul_rn(mu, lam.x);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const float3 t = k == 0 ? t0 : t1;
-      float ti = __fmul_rn(tmass[k], -xdot(rv, t));
+      ti[k] = __fmul_rn(tmass[k], -xdot(rv, t));
       if (accum) {
         const float old = imp_t[k];
-        imp_t[k] = fminf(fmaxf(__fadd_rn(old, ti), -maxf), maxf);
-        ti = __fsub_rn(imp_t[k], old);
+        imp_t[k] = fminf(fmaxf(__fadd_rn(old, ti[k]), -maxf), maxf);
+        ti[k] = __fsub_rn(imp_t[k], old);
       } else {
-        ti = fminf(fmaxf(ti, -maxf), maxf);
+        ti[k] = fminf(fmaxf(ti[k], -maxf), maxf);
       }
-      xapply(xscale(t, ti), r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
     }
+    xapply(xaxpy(t1, ti[1], xscale(t0, ti[0])), r1, r2, ima, imb, IA, IB, va, wa, vb, wb);
     lam.y = imp_t[0];
     lam.z = imp_t[1];
   }
