@@ -216,7 +216,8 @@ struct DevState {
   uint32_t* vox_list;      // narrow-phase work list of the voxel slots
   float4* iinv_off;        // per body: body-frame inverse inertia off-diagonal (xy, xz, yz, -)
   uint32_t* frozen;        // per body: 1 if asleep or static at the last narrow phase, state unwritten since
-  uint32_t* carry_list;    // narrow-phase work list of the frozen pairs
+  uint32_t* carry_list;    // narrow-phase work list of the frozen pairs: slot | paused << 31
+  uint2* carry_ids;        // the two bodies of each carry_list entry
 };
 
 // ---- small vector helpers -------------------------------------------------------------------

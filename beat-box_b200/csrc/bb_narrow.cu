@@ -69,14 +69,37 @@ struct CV {
   uint32_t f;
 };
 
-struct Contacts {
+// A manifold under construction.  Contact i lives at p[i * ST] (position, depth) and f[i * ST]
+// (feature word): k_narrow points p and f at the thread's column of shared-memory buffers
+// (ST = the block size), so the contact and clip arrays, which are indexed by run-time counts,
+// stay on chip instead of in local memory; the voxel kernel's lanes use local arrays (ST = 1).
+template <int ST>
+struct ContactsT {
   int cc;
   int key;
   float3 normal;
-  float3 pos[BB_MAX_CONTACTS];
-  float pen[BB_MAX_CONTACTS];
-  uint32_t fp[BB_MAX_CONTACTS];
+  float4* p;
+  uint32_t* f;
+  __device__ __forceinline__ float3 pos(int i) const { return f3(p[i * ST]); }
+  __device__ __forceinline__ float pen(int i) const { return p[i * ST].w; }
+  __device__ __forceinline__ uint32_t fp(int i) const { return f[i * ST]; }
+  __device__ __forceinline__ void set(int i, float3 v, float depth, uint32_t feature) {
+    p[i * ST] = f4(v, depth);
+    f[i * ST] = feature;
+  }
+  __device__ __forceinline__ void set_pos(int i, float3 v) { p[i * ST] = f4(v, p[i * ST].w); }
+  __device__ __forceinline__ void set_pen(int i, float depth) { p[i * ST].w = depth; }
 };
+// clip vertex i of a column buffer: position and feature word
+template <int ST>
+__device__ __forceinline__ CV cv_get(const float4* b, int i) {
+  const float4 x = b[i * ST];
+  return CV{make_float3(x.x, x.y, x.z), __float_as_uint(x.w)};
+}
+template <int ST>
+__device__ __forceinline__ void cv_put(float4* b, int i, const CV& c) {
+  b[i * ST] = make_float4(c.v.x, c.v.y, c.v.z, __uint_as_float(c.f));
+}
 
 // compute_incident_face (collision_detection.slang:123-243)
 __device__ void incident_face(const Xf& itx, float3 e, float3 n, CV out[4]) {
@@ -141,29 +164,31 @@ __device__ void reference_edges(float3 er, const Xf& rtx, float3 n, int axis, ui
   basis.p = rtx.p;
 }
 
-// ortographic_clip (collision_detection.slang:352-387); output capped at 8
-__device__ int ortho_clip(float sign, float e, int axis, uint32_t clip_edge, const CV* in, int in_count, CV* out) {
+// ortographic_clip (collision_detection.slang:352-387); output capped at 8.  in and out are
+// column buffers (vertex i at [i * ST]).
+template <int ST>
+__device__ int ortho_clip(float sign, float e, int axis, uint32_t clip_edge, const float4* in, int in_count, float4* out) {
   const float TH = 0.005f;
   int oc = 0;
-  CV a = in[in_count - 1];
+  CV a = cv_get<ST>(in, in_count - 1);
   for (int i = 0; i < in_count; ++i) {
-    CV b = in[i];
+    CV b = cv_get<ST>(in, i);
     float da = sign * comp(a.v, axis) - e;
     float db = sign * comp(b.v, axis) - e;
     bool on_a = da < TH && da > -TH, on_b = db < TH && db > -TH;
     if ((da < 0.f && db < 0.f) || on_a || on_b) {
-      if (oc < BB_MAX_CONTACTS) out[oc++] = b;
+      if (oc < BB_MAX_CONTACTS) cv_put<ST>(out, oc++, b);
     } else if (da < 0.f && db >= 0.f) {
       CV cv;
       cv.f = fp_set_out_ref(b.f, clip_edge);
       cv.v = a.v + (b.v - a.v) * (da / (da - db));
-      if (oc < BB_MAX_CONTACTS) out[oc++] = cv;
+      if (oc < BB_MAX_CONTACTS) cv_put<ST>(out, oc++, cv);
     } else if (da >= 0.f && db < 0.f) {
       CV cv;
       cv.f = fp_set_in_ref(a.f, clip_edge);
       cv.v = a.v + (b.v - a.v) * (da / (da - db));
-      if (oc < BB_MAX_CONTACTS) out[oc++] = cv;
-      if (oc < BB_MAX_CONTACTS) out[oc++] = b;
+      if (oc < BB_MAX_CONTACTS) cv_put<ST>(out, oc++, cv);
+      if (oc < BB_MAX_CONTACTS) cv_put<ST>(out, oc++, b);
     }
     a = b;
   }
@@ -209,8 +234,12 @@ __device__ void edges_contact(float3 pa, float3 qa, float3 pb, float3 qb, float3
   cb = pb + db * tb;
 }
 
-// OBBvsOBBCollision::collision_detection (collision_detection.slang:562-876)
-__device__ bool box_box(Quatf qa, float3 pa, float3 ea, Quatf qb, float3 pb, float3 eb, bool sat_quirk, Contacts& out) {
+// OBBvsOBBCollision::collision_detection (collision_detection.slang:562-876).  The clip runs
+// between the column buffer buf and the output's own buffer out.p: four passes end in buf, and
+// the contacts are then written to out.p.
+template <int ST>
+__device__ bool box_box(Quatf qa, float3 pa, float3 ea, Quatf qb, float3 pb, float3 eb, bool sat_quirk, float4* buf,
+                        ContactsT<ST>& out) {
   out.cc = 0;
   out.key = -1;
   Xf txa, txb;
@@ -288,27 +317,24 @@ __device__ bool box_box(Quatf qa, float3 pa, float3 ea, Quatf qb, float3 pb, flo
     Xf basis;
     float3 e;
     reference_edges(er, rtx, normal, axis, clip, basis, e);
-    CV in[BB_MAX_CONTACTS], outv[BB_MAX_CONTACTS];
+    float4* in = buf;
+    float4* outv = out.p;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      in[i].v = xf_transform_t(basis, inc[i].v);
-      in[i].f = inc[i].f;
-    }
-    int oc = ortho_clip(1.f, e.x, 0, clip[0], in, 4, outv);
+    for (int i = 0; i < 4; ++i) cv_put<ST>(in, i, CV{xf_transform_t(basis, inc[i].v), inc[i].f});
+    int oc = ortho_clip<ST>(1.f, e.x, 0, clip[0], in, 4, outv);
     if (oc == 0) return false;
-    int ic = ortho_clip(1.f, e.y, 1, clip[1], outv, oc, in);
+    int ic = ortho_clip<ST>(1.f, e.y, 1, clip[1], outv, oc, in);
     if (ic == 0) return false;
-    oc = ortho_clip(-1.f, e.x, 0, clip[2], in, ic, outv);
+    oc = ortho_clip<ST>(-1.f, e.x, 0, clip[2], in, ic, outv);
     if (oc == 0) return false;
-    ic = ortho_clip(-1.f, e.y, 1, clip[3], outv, oc, in);
+    ic = ortho_clip<ST>(-1.f, e.y, 1, clip[3], outv, oc, in);
     if (ic == 0) return false;
     int n = 0;
     for (int i = 0; i < ic; ++i) {
-      float dd = in[i].v.z - e.z;
+      const CV v = cv_get<ST>(in, i);
+      float dd = v.v.z - e.z;
       if (dd <= 0.f) {
-        out.pos[n] = xf_transform(basis, in[i].v);
-        out.pen[n] = dd;
-        out.fp[n] = flip ? fp_swap_roles(in[i].f) : in[i].f;
+        out.set(n, xf_transform(basis, v.v), dd, flip ? fp_swap_roles(v.f) : v.f);
         ++n;
       }
     }
@@ -325,16 +351,15 @@ __device__ bool box_box(Quatf qa, float3 pa, float3 ea, Quatf qb, float3 pb, flo
     edges_contact(p0, q0, p1, q1, ca, cb);
     out.cc = 1;
     out.normal = normal;
-    out.pos[0] = (ca + cb) * 0.5f;
-    out.pen[0] = s_max;
-    out.fp[0] = fp_pack(axis, axis, axis, axis);
+    out.set(0, (ca + cb) * 0.5f, s_max, fp_pack(axis, axis, axis, axis));
   }
   out.key = axis;
   return out.cc > 0;
 }
 
 // Sphere contacts (first principles; the reference has no sphere collider).
-__device__ bool sphere_sphere(float3 pa, float ra, float3 pb, float rb, Contacts& out) {
+template <int ST>
+__device__ bool sphere_sphere(float3 pa, float ra, float3 pb, float rb, ContactsT<ST>& out) {
   float3 d = pb - pa;
   float dist = len3(d);
   if (dist > ra + rb) return false;
@@ -343,9 +368,8 @@ __device__ bool sphere_sphere(float3 pa, float ra, float3 pb, float rb, Contacts
   out.cc = 1;
   out.key = BB_KEY_SPHERE_SPHERE;
   out.normal = n;
-  out.pen[0] = pen;
-  out.pos[0] = pa + n * (ra + pen * 0.5f);
-  out.fp[0] = fp_pack(BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE);
+  out.set(0, pa + n * (ra + pen * 0.5f), pen,
+          fp_pack(BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE, BB_KEY_SPHERE_SPHERE));
   return true;
 }
 __device__ bool box_sphere_core(Quatf qx, float3 px, float3 e, float3 ps, float r, float3& n, float& pen, float3& pos) {
@@ -429,12 +453,16 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
   for (uint32_t base = blockIdx.x * blockDim.x; base < S; base += gridDim.x * blockDim.x) {  // block-uniform
     const uint32_t k = base + threadIdx.x;
     int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body, 3 frozen
+    uint2 ids = make_uint2(0u, 0u);
+    bool paused = false;
     if (k < S) {
       d.hit[k] = 0;
       d.m_keycc[cur][k] = make_int2(-1, 0);
       const uint2 pr = d.pairs[slot_pair_of(d, k)];
       const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
       const uint32_t fa = d.flags[ida], fb = d.flags[idb];
+      ids = make_uint2(ida, idb);
+      paused = ((fa | fb) & BB_BODY_PAUSED) != 0u;
       if ((fa & BB_BODY_DYNAMIC) || (fb & BB_BODY_DYNAMIC)) {
         const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
         const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
@@ -471,8 +499,10 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
     __syncthreads();
     if (kind >= 0) {
       const uint32_t r = s_cnt[kind][warp] + uint32_t(__popc(my_mask & ((1u << lane) - 1u)));
-      if (kind == 3) d.carry_list[r] = k;
-      else if (kind == 2) d.vox_list[r] = k;
+      if (kind == 3) {  // slot | paused << 31, and the two bodies, so the carry's loads start at once
+        d.carry_list[r] = k | (paused ? 0x80000000u : 0u);
+        d.carry_ids[r] = ids;
+      } else if (kind == 2) d.vox_list[r] = k;
       else d.np_list[kind == 0 ? r : S - 1 - r] = k;
     }
     __syncthreads();  // s_cnt is rewritten by the next trip
@@ -484,28 +514,29 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
 // impulses, penalties, stick anchors -- with warm-start counts + 1 and the extraction trend 0,
 // which is what recomputing the same poses and matching every contact by feature gives.  A
 // frozen pair without a manifold last substep goes to the ordinary lists and is computed.
-__device__ __forceinline__ void carry_contact(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni) {
-  const float4 cp = d.c_pos[prv][oi], cl = d.c_lam[prv][oi], aa = d.c_anc_a[prv][oi];
-  float4 kt = d.c_kt[prv][oi];
+// Old contact oi (its position, impulses, penalties and first anchor already loaded) written as
+// new contact ni.  A paused world's manifold (exact) is carried as it is, every field
+// (warm-start counts, trend, anchors, stick data), so the world resumes exactly where it stopped.
+__device__ __forceinline__ void carry_loaded(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni, float4 cp,
+                                             float4 cl, float4 kt, float4 aa, bool exact) {
+  d.c_pos[cur][ni] = cp;
+  d.c_lam[cur][ni] = cl;
+  if (exact) {
+    d.c_kt[cur][ni] = kt;
+    d.c_anc_a[cur][ni] = aa;
+    d.c_anc_b[cur][ni] = d.c_anc_b[prv][oi];
+    return;
+  }
   const bool stick = __float_as_uint(kt.z) != 0u;
   // the second anchor only of a sticking contact (else it is written as 0)
   const float4 ab = stick ? d.c_anc_b[prv][oi] : make_float4(0.f, 0.f, 0.f, 0.f);
   kt.w = __uint_as_float(min(255u, __float_as_uint(kt.w) + 1u));
-  d.c_pos[cur][ni] = cp;
-  d.c_lam[cur][ni] = cl;
   d.c_kt[cur][ni] = kt;
   d.c_anc_a[cur][ni] = stick ? aa : make_float4(0.f, 0.f, 0.f, aa.w);
   d.c_anc_b[cur][ni] = make_float4(ab.x, ab.y, ab.z, 0.f);
 }
-
-// A paused world's manifold is carried as it is, every field (warm-start counts, trend, anchors,
-// stick data), so the world resumes exactly where it stopped.
-__device__ __forceinline__ void carry_exact_contact(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni) {
-  d.c_pos[cur][ni] = d.c_pos[prv][oi];
-  d.c_lam[cur][ni] = d.c_lam[prv][oi];
-  d.c_kt[cur][ni] = d.c_kt[prv][oi];
-  d.c_anc_a[cur][ni] = d.c_anc_a[prv][oi];
-  d.c_anc_b[cur][ni] = d.c_anc_b[prv][oi];
+__device__ __forceinline__ void carry_contact(const DevState& d, int prv, int cur, uint32_t oi, uint32_t ni, bool exact) {
+  carry_loaded(d, prv, cur, oi, ni, d.c_pos[prv][oi], d.c_lam[prv][oi], d.c_kt[prv][oi], d.c_anc_a[prv][oi], exact);
 }
 
 // Lane q (0..3) of the quad that carries a pair: the header (q = 0) and contacts q, q + 4.  The
@@ -532,7 +563,7 @@ __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t 
       d.hit[dst] = 1;
     }
     for (uint32_t c = q; c < uint32_t(kc.y); c += 4u)
-      carry_exact_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c);
+      carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c, true);
     return;
   }
   if (q == 0) {
@@ -548,7 +579,7 @@ __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t 
     d.hit[dst] = 1;
   }
   for (uint32_t c = q; c < uint32_t(kc.y); c += 4u)
-    carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c);
+    carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, dst * BB_MAX_CONTACTS + c, false);
 }
 
 // One quad of lanes per frozen pair.  The pair's manifold of the previous substep is found at
@@ -557,31 +588,70 @@ __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t 
 // the one the search through the body's manifold list would find.  While no pair ahead of it
 // came or went, every frozen pair takes this path; the others search.  Slots past the previous
 // substep's count are not read (they hold older manifolds).
-__global__ void k_narrow_carry(const DevState d, int cur) {
+//
+// The list entry carries the two bodies and the paused bit, so every load of the slot's own old
+// manifold is issued at once, before the check: the quad's lanes split the header (lane 0 the
+// key and colour, 1 the normal and first tangent, 2 the second tangent and first anchor, 3 the
+// second anchor) and lane q takes contact q.  A pair then waits for one round of loads after
+// its list entry instead of a chain through the pair, the sorted ids and the flags.
+__global__ void __launch_bounds__(256) k_narrow_carry(const DevState d, int cur) {
   const int prv = cur ^ 1;
   const uint32_t S = slot_total(d);
   const uint32_t S_prv = min(d.ctr->slots_of[prv], d.pair_capacity);
   const uint32_t nc = d.ctr->np_counts[3];
+  const uint32_t sub_tag = d.ctr->substeps;
+  const bool reuse_ok = d.ctr->gc_coloured + 1u == sub_tag;
   const uint32_t q = threadIdx.x & 3u, quads = (gridDim.x * blockDim.x) >> 2;
   for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < nc; t += quads) {  // quad-uniform
-    const uint32_t s = d.carry_list[t];
-    const uint2 pr = d.pairs[slot_pair_of(d, s)];
-    int2 okc = make_int2(-1, 0);
-    uint2 ob = make_uint2(BB_NONE, BB_NONE);
-    if (s < S_prv) {
-      okc = d.m_keycc[prv][s];
-      ob = d.m_bodies[prv][s];
-    }
-    const uint32_t ida = d.vals[0][pr.x], idb = d.vals[0][pr.y];
-    const uint32_t fa = d.flags[ida];
+    const uint32_t entry = d.carry_list[t];
+    const uint2 ids = d.carry_ids[t];
+    const uint32_t s = entry & 0x7FFFFFFFu, ida = ids.x, idb = ids.y;
     // A paused world's manifold is kept in the body order it was stored in: the first paused
     // substep sorts with the poses its world's last step integrated, which can swap a pair.
-    const bool exact = ((fa | d.flags[idb]) & BB_BODY_PAUSED) != 0;
-    if (okc.x >= 0 && okc.x < 90 &&
-        ((ob.x == ida && ob.y == idb) || (exact && ob.x == idb && ob.y == ida))) {
-      carry_part(d, cur, s, s, ida, idb, q, exact);
-      continue;
+    const bool exact = (entry >> 31) != 0u;
+    if (s < S_prv) {
+      const int2 okc = d.m_keycc[prv][s];
+      const uint2 ob = d.m_bodies[prv][s];
+      float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = h0;
+      uint32_t colour = BB_NONE;
+      if (q == 0) {
+        if (reuse_ok) colour = d.gc_slot_color[prv][s];
+      } else if (q == 1) {
+        h0 = d.m_normal[prv][s];
+        h1 = d.m_t0[prv][s];
+      } else if (q == 2) {
+        h0 = d.m_t1[prv][s];
+        h1 = exact ? d.m_anchor_a[prv][s] : d.pos[ida];
+      } else {
+        h1 = exact ? d.m_anchor_b[prv][s] : d.pos[idb];
+      }
+      const uint32_t oi = s * BB_MAX_CONTACTS + q;
+      const float4 cp = d.c_pos[prv][oi], cl = d.c_lam[prv][oi], kt = d.c_kt[prv][oi], aa = d.c_anc_a[prv][oi];
+      if (okc.x >= 0 && okc.x < 90 &&
+          ((ob.x == ida && ob.y == idb) || (exact && ob.x == idb && ob.y == ida))) {
+        // the same writes as carry_part(d, cur, s, s, ida, idb, q, exact)
+        if (q == 0) {  // the same manifold as last substep: its colour carries over (colour reuse)
+          d.gc_reuse[s] = colour;
+          if (reuse_ok) d.gc_survived[s] = sub_tag;
+          d.m_bodies[cur][s] = ob;
+          d.m_keycc[cur][s] = okc;
+          d.hit[s] = 1;
+        } else if (q == 1) {
+          d.m_normal[cur][s] = exact ? h0 : make_float4(h0.x, h0.y, h0.z, __int_as_float(0));
+          d.m_t0[cur][s] = h1;
+        } else if (q == 2) {
+          d.m_t1[cur][s] = h0;
+          d.m_anchor_a[cur][s] = exact ? h1 : make_float4(h1.x, h1.y, h1.z, 0.f);
+        } else {
+          d.m_anchor_b[cur][s] = exact ? h1 : make_float4(h1.x, h1.y, h1.z, 0.f);
+        }
+        if (q < uint32_t(okc.y)) carry_loaded(d, prv, cur, oi, oi, cp, cl, kt, aa, exact);
+        for (uint32_t c = q + 4u; c < uint32_t(okc.y); c += 4u)
+          carry_contact(d, prv, cur, s * BB_MAX_CONTACTS + c, s * BB_MAX_CONTACTS + c, exact);
+        continue;
+      }
     }
+    const uint32_t fa = d.flags[ida];
     const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
     const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
     const uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb, other = x == ida ? idb : ida;
@@ -620,9 +690,12 @@ __global__ void k_narrow_carry(const DevState d, int cur) {
 // the write of slot k.  Voxel manifolds (vox) inherit only from the old manifold of the same
 // key in the same body order, match features by the whole voxel/corner id, and keep their
 // own depth caps; other manifolds take the pair's old manifold under any key, either order.
+// old_p / old_f are column buffers (stride ST) that receive the old manifold's contacts
+// (position and depth, feature word) once, for the matching loops below.
+template <int ST>
 __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int cur, int warm, uint32_t k,
-                                         uint32_t ida, uint32_t idb, uint32_t fa, float3 pa, float3 pb, Contacts& m,
-                                         bool vox) {
+                                         uint32_t ida, uint32_t idb, uint32_t fa, float3 pa, float3 pb,
+                                         ContactsT<ST>& m, bool vox, float4* old_p, uint32_t* old_f) {
   const int prv = cur ^ 1;
   // compute_basis (extensions.slang:262-272)
   float3 n = m.normal, t0;
@@ -631,7 +704,8 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
   t0 = t0 * (1.0f / len3(t0));
   float3 t1 = cross3(t0, n);
   const int cc = m.cc;
-  for (int c = 0; c < cc; ++c) m.pen[c] = vox ? m.pen[c] : fmaxf(m.pen[c], p.penetration_cap);  // extraction cap (:1575-1578)
+  if (!vox)
+    for (int c = 0; c < cc; ++c) m.set_pen(c, fmaxf(m.pen(c), p.penetration_cap));  // extraction cap (:1575-1578)
   // Each new contact records the old contact it inherits from (src, -1: none) and whether the
   // proximity pass gave it (pass2: then the old features, the tangent sign and anchor roles of
   // a swapped pair apply); the inherited fields are read from the old contact when written.
@@ -683,20 +757,24 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
         const int occ = okc.y;
         uint32_t used_old = 0, matched_new = 0;
         ob = old_slot * BB_MAX_CONTACTS;
+        for (int j = 0; j < occ; ++j) {
+          old_p[j * ST] = d.c_pos[prv][ob + j];
+          if (!cross_key) old_f[j * ST] = __float_as_uint(d.c_anc_a[prv][ob + j].w);
+        }
         if (!cross_key) {
           for (int i = 0; i < cc; ++i) {
             for (int j = 0; j < occ; ++j) {
               if (used_old & (1u << j)) continue;
-              float4 op = d.c_pos[prv][ob + j];
-              uint32_t ofp = __float_as_uint(d.c_anc_a[prv][ob + j].w);
-              bool feat = vox ? ofp == m.fp[i]
-                              : (fp_in_inc(ofp) == fp_in_inc(m.fp[i]) && fp_out_inc(ofp) == fp_out_inc(m.fp[i]));
-              float3 dp = f3(op) - m.pos[i];
+              float4 op = old_p[j * ST];
+              uint32_t ofp = old_f[j * ST];
+              const uint32_t nfp = m.fp(i);
+              bool feat = vox ? ofp == nfp : (fp_in_inc(ofp) == fp_in_inc(nfp) && fp_out_inc(ofp) == fp_out_inc(nfp));
+              float3 dp = f3(op) - m.pos(i);
               bool close = dot3(dp, dp) < 0.1f * 0.1f;
               if (feat && close) {
                 set_src(i, j);
-                float3 d2 = m.pos[i] - f3(op);
-                if (dot3(d2, d2) < 0.01f) m.pos[i] = f3(op);
+                float3 d2 = m.pos(i) - f3(op);
+                if (dot3(d2, d2) < 0.01f) m.set_pos(i, f3(op));
                 used_old |= 1u << j;
                 matched_new |= 1u << i;
                 break;
@@ -711,7 +789,7 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
             if (matched_new & (1u << i)) continue;
             for (int j = 0; j < occ; ++j) {
               if (used_old & (1u << j)) continue;
-              float3 dp = m.pos[i] - f3(d.c_pos[prv][ob + j]);
+              float3 dp = m.pos(i) - f3(old_p[j * ST]);
               float d2 = dot3(dp, dp);
               if (d2 < best) { best = d2; bi = i; bj = j; }
             }
@@ -723,8 +801,8 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
           used_old |= 1u << bj;
         }
         float deep_new = 0.f, deep_old = 0.f;
-        for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, m.pen[i]);
-        for (int j = 0; j < occ; ++j) deep_old = fminf(deep_old, d.c_pos[prv][ob + j].w);
+        for (int i = 0; i < cc; ++i) deep_new = fminf(deep_new, m.pen(i));
+        for (int j = 0; j < occ; ++j) deep_old = fminf(deep_old, old_p[j * ST].w);
         err = int32_t(fminf(fmaxf((deep_new - deep_old) * 10000.0f, -32000.0f), 32000.0f));
       }
     }
@@ -741,7 +819,7 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
     // new contacts start at zero; matched ones inherit impulses, penalties, stick and anchors
     float4 lam = make_float4(0.f, 0.f, 0.f, 0.f);
     float2 kt = make_float2(0.f, 0.f);
-    uint32_t stick = 0, wc = 0, fp = m.fp[c];
+    uint32_t stick = 0, wc = 0, fp = m.fp(c);
     float3 aa = make_float3(0.f, 0.f, 0.f), ab = make_float3(0.f, 0.f, 0.f);
     const int j = get_src(c);
     if (j >= 0) {
@@ -759,7 +837,7 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
       if (p2) fp = __float_as_uint(oaa.w);
       wc = warm_inc(__float_as_uint(okt.w));
     }
-    d.c_pos[cur][cb + c] = f4(m.pos[c], m.pen[c]);
+    d.c_pos[cur][cb + c] = f4(m.pos(c), m.pen(c));
     d.c_lam[cur][cb + c] = lam;
     d.c_kt[cur][cb + c] = make_float4(kt.x, kt.y, __uint_as_float(stick), __uint_as_float(wc));
     d.c_anc_a[cur][cb + c] = f4(aa, __uint_as_float(fp));
@@ -769,8 +847,16 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
   d.gc_reuse[k] = reuse;
 }
 
-// Narrow phase + warm start: one thread per listed pair.
-__global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int cur, int warm) {
+// Narrow phase + warm start: one thread per listed pair.  Each thread owns a column of three
+// shared-memory buffers of eight entries: the clip polygon ping-pongs between columns 0 and 1,
+// the contacts end in column 1 with their feature words beside them, and column 0 then takes
+// the old manifold's contacts for the warm-start match (36 KB per 128-thread block).
+#define BB_NARROW_THREADS 128
+__global__ void __launch_bounds__(BB_NARROW_THREADS) k_narrow(const DevState d, Params p, int cur, int warm) {
+  __shared__ float4 s_col[2][BB_MAX_CONTACTS][BB_NARROW_THREADS];
+  __shared__ uint32_t s_feat[2][BB_MAX_CONTACTS][BB_NARROW_THREADS];
+  constexpr int ST = BB_NARROW_THREADS;
+  float4* const buf = &s_col[0][0][threadIdx.x];
   const uint32_t S = slot_total(d);
   const uint32_t nbb = d.ctr->np_counts[0], ntot = nbb + d.ctr->np_counts[1];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += gridDim.x * blockDim.x) {
@@ -783,12 +869,14 @@ __global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int 
     Quatf qa = q_from(d.rot[ida]), qb = q_from(d.rot[idb]);
     float3 pa = f3(pa4), pb = f3(pb4);
     uint32_t ta = __float_as_uint(sa.w), tb = __float_as_uint(sb.w);
-    Contacts m;
+    ContactsT<ST> m;
+    m.p = &s_col[1][0][threadIdx.x];
+    m.f = &s_feat[1][0][threadIdx.x];
     bool hit;
     if (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) {
-      hit = box_box(qa, pa, f3(sa), qb, pb, f3(sb), (p.quirks & BB_QUIRK_SAT_FRAME) != 0, m);
+      hit = box_box<ST>(qa, pa, f3(sa), qb, pb, f3(sb), (p.quirks & BB_QUIRK_SAT_FRAME) != 0, buf, m);
     } else if (ta == BB_SHAPE_SPHERE && tb == BB_SHAPE_SPHERE) {
-      hit = sphere_sphere(pa, sa.x, pb, sb.x, m);
+      hit = sphere_sphere<ST>(pa, sa.x, pb, sb.x, m);
     } else {
       float3 n, pos;
       float pen;
@@ -803,13 +891,11 @@ __global__ void __launch_bounds__(128) k_narrow(const DevState d, Params p, int 
       if (hit) {
         m.cc = 1;
         m.normal = n;
-        m.pen[0] = pen;
-        m.pos[0] = pos;
-        m.fp[0] = fp_pack(m.key, m.key, m.key, m.key);
+        m.set(0, pos, pen, fp_pack(m.key, m.key, m.key, m.key));
       }
     }
     if (!hit) continue;
-    np_store(d, p, cur, warm, k, ida, idb, fa, pa, pb, m, false);
+    np_store<ST>(d, p, cur, warm, k, ida, idb, fa, pa, pb, m, false, buf, &s_feat[0][0][threadIdx.x]);
   }
 }
 
@@ -1132,7 +1218,11 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
       const uint32_t code = lane, axk = code >> 1;
       const float3 n_sep = mat_col(r2.R, int(axk)) * ((code & 1u) ? 1.f : -1.f);  // the face normal, world
       bool store = true;
-      Contacts m;
+      float4 lp[BB_MAX_CONTACTS], lo[BB_MAX_CONTACTS];
+      uint32_t lf[BB_MAX_CONTACTS], lof[BB_MAX_CONTACTS];
+      ContactsT<1> m;
+      m.p = lp;
+      m.f = lf;
       m.cc = 0;
       m.key = 90 + int(code);
       if (my_samples == 0) {
@@ -1141,9 +1231,7 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
         const float3 dd = r1.p - r2.p;
         const float3 n_res = dot3(dd, dd) > 1e-8f ? dd * (1.0f / len3(dd)) : make_float3(0.f, 1.f, 0.f);
         m.normal = flip ? n_res : -n_res;
-        m.pos[0] = (r1.p + r2.p) * 0.5f;
-        m.pen[0] = -0.5f * vs1;
-        m.fp[0] = 0xFFFFFFu;
+        m.set(0, (r1.p + r2.p) * 0.5f, -0.5f * vs1, 0xFFFFFFu);
         m.cc = 1;
       } else {
         // voxel_emit_manifold (:1330-1448); every sample of a pass has the normal n_sep
@@ -1189,16 +1277,14 @@ __global__ void __launch_bounds__(256) k_voxel_narrow(const DevState d, Params p
             }
             if (dup) continue;
             emitted[en++] = pt;
-            m.pos[n_emit] = pt;
-            m.pen[n_emit] = wo.pen * align;
-            m.fp[n_emit] = wo.fa | (c << 24);
+            m.set(n_emit, pt, wo.pen * align, wo.fa | (c << 24));
             ++n_emit;
           }
         }
         m.cc = n_emit;
         store = n_emit > 0;
       }
-      if (store) np_store(d, p, cur, warm, slot0 + code, ida, idb, d.flags[ida], A.p, B.p, m, true);
+      if (store) np_store<1>(d, p, cur, warm, slot0 + code, ida, idb, d.flags[ida], A.p, B.p, m, true, lo, lof);
     }
     __syncwarp();
   }

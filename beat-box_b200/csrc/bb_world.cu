@@ -474,6 +474,7 @@ struct bb_world_impl {
     d.flow_rec = dalloc<uint4>(P, owned, err, stream);
     d.pgs_rec = dalloc<uint4>(P, owned, err, stream);
     d.np_list = u32(P); d.carry_list = u32(P);
+    d.carry_ids = dalloc<uint2>(P, owned, err, stream);
     d.gc_rec = dalloc<uint4>(P, owned, err, stream);
     d.gc_list[0] = u32(P); d.gc_list[1] = u32(P);
     d.pgs_mass = f4(P);
