@@ -152,6 +152,7 @@ struct DevState {
   uint32_t* csr_start[2];
   uint32_t* csr_list[2];
   uint32_t* csr_partner[2];  // other body of each list entry
+  uint32_t* csr_slot[2];     // slot of each list entry's manifold
   uint32_t* csr_cursor;
   uint32_t* hit;         // per pair slot: 1 if it produced a manifold
   uint32_t* man_index;   // per pair slot: exclusive scan of hit
@@ -218,6 +219,7 @@ struct DevState {
   uint32_t* frozen;        // per body: 1 if asleep or static at the last narrow phase, state unwritten since
   uint32_t* carry_list;    // narrow-phase work list of the frozen pairs: slot | paused << 31
   uint2* carry_ids;        // the two bodies of each carry_list entry
+  uint32_t* carry_tag;     // per slot: the substep that last carried it in place (short carry)
 };
 
 // ---- small vector helpers -------------------------------------------------------------------

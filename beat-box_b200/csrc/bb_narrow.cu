@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
     const uint32_t k = base + threadIdx.x;
     int kind = -1;  // 0 box-box, 1 with a sphere, 2 with a voxel body, 3 frozen
     uint2 ids = make_uint2(0u, 0u);
-    bool paused = false;
+    bool paused = false, dyn_a = false;
     if (k < S) {
       d.hit[k] = 0;
       d.m_keycc[cur][k] = make_int2(-1, 0);
@@ -463,6 +463,7 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
       const uint32_t fa = d.flags[ida], fb = d.flags[idb];
       ids = make_uint2(ida, idb);
       paused = ((fa | fb) & BB_BODY_PAUSED) != 0u;
+      dyn_a = (fa & BB_BODY_DYNAMIC) != 0u;
       if ((fa & BB_BODY_DYNAMIC) || (fb & BB_BODY_DYNAMIC)) {
         const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
         const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
@@ -499,8 +500,8 @@ __global__ void __launch_bounds__(32 * BB_CLS_WARPS) k_np_classify(const DevStat
     __syncthreads();
     if (kind >= 0) {
       const uint32_t r = s_cnt[kind][warp] + uint32_t(__popc(my_mask & ((1u << lane) - 1u)));
-      if (kind == 3) {  // slot | paused << 31, and the two bodies, so the carry's loads start at once
-        d.carry_list[r] = k | (paused ? 0x80000000u : 0u);
+      if (kind == 3) {  // slot | paused << 31 | body a dynamic << 30, and the two bodies
+        d.carry_list[r] = k | (paused ? 0x80000000u : 0u) | (dyn_a ? 0x40000000u : 0u);
         d.carry_ids[r] = ids;
       } else if (kind == 2) d.vox_list[r] = k;
       else d.np_list[kind == 0 ? r : S - 1 - r] = k;
@@ -594,93 +595,144 @@ __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t 
 // key and colour, 1 the normal and first tangent, 2 the second tangent and first anchor, 3 the
 // second anchor) and lane q takes contact q.  A pair then waits for one round of loads after
 // its list entry instead of a chain through the pair, the sorted ids and the flags.
-__global__ void __launch_bounds__(256) k_narrow_carry(const DevState d, int cur) {
+//
+// Short carry.  When this slot was carried the same way last substep (carry_tag = last
+// substep), last substep's manifold was made from the one this substep writes over, and nothing
+// has written either since: the frozen pair is not solved, and host calls that change contacts
+// either reset both buffers' headers (refill), restore every array (state load, regrow) or
+// unfreeze the bodies.  Its contacts then differ from last substep's only in the warm-start
+// count, so only that word is rewritten (the header is written in full).  Not under AVBD
+// (lazy_ok = 0), whose warm start decays the penalties and re-anchors every manifold, sleeping
+// ones included; not for a paused world's exact carry.
+__global__ void __launch_bounds__(256) k_narrow_carry(const DevState d, int cur, int lazy_ok) {
   const int prv = cur ^ 1;
   const uint32_t S = slot_total(d);
   const uint32_t S_prv = min(d.ctr->slots_of[prv], d.pair_capacity);
   const uint32_t nc = d.ctr->np_counts[3];
   const uint32_t sub_tag = d.ctr->substeps;
   const bool reuse_ok = d.ctr->gc_coloured + 1u == sub_tag;
+  const bool lazy_on = lazy_ok != 0 && sub_tag > 1u;  // tags start at 0: substep 1 never matches
   const uint32_t q = threadIdx.x & 3u, quads = (gridDim.x * blockDim.x) >> 2;
+  const uint32_t qbase = threadIdx.x & 28u;  // this quad's first lane
+  const unsigned qmask = 0xFu << qbase;
   for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < nc; t += quads) {  // quad-uniform
     const uint32_t entry = d.carry_list[t];
     const uint2 ids = d.carry_ids[t];
-    const uint32_t s = entry & 0x7FFFFFFFu, ida = ids.x, idb = ids.y;
+    const uint32_t s = entry & 0x3FFFFFFFu, ida = ids.x, idb = ids.y;
     // A paused world's manifold is kept in the body order it was stored in: the first paused
     // substep sorts with the poses its world's last step integrated, which can swap a pair.
     const bool exact = (entry >> 31) != 0u;
+    const uint32_t x = (entry & 0x40000000u) ? ida : idb, other = x == ida ? idb : ida;
+    // one round of loads: the old manifold at the pair's own slot, and the bounds of the dynamic
+    // body's list of old manifolds
+    int2 okc = make_int2(-1, 0);
+    uint2 ob = make_uint2(BB_NONE, BB_NONE);
     if (s < S_prv) {
-      const int2 okc = d.m_keycc[prv][s];
-      const uint2 ob = d.m_bodies[prv][s];
-      float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = h0;
-      uint32_t colour = BB_NONE;
-      if (q == 0) {
-        if (reuse_ok) colour = d.gc_slot_color[prv][s];
-      } else if (q == 1) {
-        h0 = d.m_normal[prv][s];
-        h1 = d.m_t0[prv][s];
-      } else if (q == 2) {
-        h0 = d.m_t1[prv][s];
-        h1 = exact ? d.m_anchor_a[prv][s] : d.pos[ida];
-      } else {
-        h1 = exact ? d.m_anchor_b[prv][s] : d.pos[idb];
-      }
-      const uint32_t oi = s * BB_MAX_CONTACTS + q;
-      const float4 cp = d.c_pos[prv][oi], cl = d.c_lam[prv][oi], kt = d.c_kt[prv][oi], aa = d.c_anc_a[prv][oi];
-      if (okc.x >= 0 && okc.x < 90 &&
-          ((ob.x == ida && ob.y == idb) || (exact && ob.x == idb && ob.y == ida))) {
-        // the same writes as carry_part(d, cur, s, s, ida, idb, q, exact)
-        if (q == 0) {  // the same manifold as last substep: its colour carries over (colour reuse)
-          d.gc_reuse[s] = colour;
-          if (reuse_ok) d.gc_survived[s] = sub_tag;
-          d.m_bodies[cur][s] = ob;
-          d.m_keycc[cur][s] = okc;
-          d.hit[s] = 1;
-        } else if (q == 1) {
-          d.m_normal[cur][s] = exact ? h0 : make_float4(h0.x, h0.y, h0.z, __int_as_float(0));
-          d.m_t0[cur][s] = h1;
-        } else if (q == 2) {
-          d.m_t1[cur][s] = h0;
-          d.m_anchor_a[cur][s] = exact ? h1 : make_float4(h1.x, h1.y, h1.z, 0.f);
-        } else {
-          d.m_anchor_b[cur][s] = exact ? h1 : make_float4(h1.x, h1.y, h1.z, 0.f);
+      okc = d.m_keycc[prv][s];
+      ob = d.m_bodies[prv][s];
+    }
+    const uint32_t l0 = d.csr_start[prv][x], l1 = d.csr_start[prv][x + 1];
+    const bool in_place = okc.x >= 0 && okc.x < 90 &&
+                          ((ob.x == ida && ob.y == idb) || (exact && ob.x == idb && ob.y == ida));
+    uint32_t os = s;
+    uint32_t ta = BB_SHAPE_BOX, tb = BB_SHAPE_BOX;
+    if (!in_place) {
+      ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w));
+      tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
+      const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
+      os = BB_NONE;
+      if (vox) {  // each face key into its own slot, in list order
+        bool any = false;
+        for (uint32_t e = l0; e < l1; ++e) {
+          if (d.csr_partner[prv][e] != other) continue;
+          const uint32_t vs = d.csr_slot[prv][e];
+          if (!exact && d.m_bodies[prv][vs].x != ida) continue;  // same body order only
+          const int key = d.m_keycc[prv][vs].x;
+          if (key < 90 || key > 95) continue;
+          carry_part(d, cur, vs, s + uint32_t(key - 90), ida, idb, q, exact);
+          any = true;
         }
-        if (q < uint32_t(okc.y)) carry_loaded(d, prv, cur, oi, oi, cp, cl, kt, aa, exact);
-        for (uint32_t c = q + 4u; c < uint32_t(okc.y); c += 4u)
-          carry_contact(d, prv, cur, s * BB_MAX_CONTACTS + c, s * BB_MAX_CONTACTS + c, exact);
+        // no manifold last substep: compute the pair with the others (a paused pair had none
+        // when its world stopped, and keeps none)
+        if (!any && q == 0 && !exact) d.vox_list[atomicAdd(&d.ctr->np_counts[2], 1u)] = s;
         continue;
       }
-    }
-    const uint32_t fa = d.flags[ida];
-    const uint32_t ta = BB_SHAPE_KIND(__float_as_uint(d.shape[ida].w)), tb = BB_SHAPE_KIND(__float_as_uint(d.shape[idb].w));
-    const bool vox = ta == BB_SHAPE_VOXEL || tb == BB_SHAPE_VOXEL;
-    const uint32_t x = (fa & BB_BODY_DYNAMIC) ? ida : idb, other = x == ida ? idb : ida;
-    const uint32_t s0 = d.csr_start[prv][x], s1 = d.csr_start[prv][x + 1];
-    bool any = false;
-    for (uint32_t e = s0; e < s1; ++e) {
-      if (d.csr_partner[prv][e] != other) continue;
-      const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
-      if (!exact && d.m_bodies[prv][os].x != ida) continue;  // same body order only
-      const int key = d.m_keycc[prv][os].x;
-      if (vox) {
-        if (key < 90 || key > 95) continue;
-        carry_part(d, cur, os, s + uint32_t(key - 90), ida, idb, q, exact);
-        any = true;
-      } else {
-        carry_part(d, cur, os, s, ida, idb, q, exact);
-        any = true;
-        break;
+      // Not a voxel pair: one slot, so at most one old manifold, the entry of x's list whose
+      // partner is the other body.  The quad's lanes split the list.
+      uint32_t mine = BB_NONE;
+      for (uint32_t e = l0 + q; e < l1; e += 4u) {
+        const uint32_t pe = d.csr_partner[prv][e], se = d.csr_slot[prv][e];
+        if (pe == other) mine = se;
       }
+      const unsigned found = __ballot_sync(qmask, mine != BB_NONE) & qmask;
+      if (found) os = __shfl_sync(qmask, mine, __ffs(found) - 1);
     }
-    // no manifold last substep: compute the pair with the others (a paused pair had none when
-    // its world stopped, and keeps none)
-    if (any || q != 0 || exact) continue;
-    if (vox) {
-      d.vox_list[atomicAdd(&d.ctr->np_counts[2], 1u)] = s;
-    } else if (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) {
-      d.np_list[atomicAdd(&d.ctr->np_counts[0], 1u)] = s;
+    // the old manifold os, every load at once: the header split over the quad (lane 0 the key,
+    // bodies and colour, 1 the normal and first tangent, 2 the second tangent and first anchor,
+    // 3 the second anchor), contact q on lane q
+    int2 kc = okc;
+    uint2 ob2 = ob;
+    float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = h0, kt = h0;
+    uint32_t colour = BB_NONE, tag = 0u;
+    if (os != BB_NONE) {
+      if (!in_place) {
+        kc = d.m_keycc[prv][os];
+        ob2 = d.m_bodies[prv][os];
+      }
+      if (q == 0) {
+        if (reuse_ok) colour = d.gc_slot_color[prv][os];
+        if (lazy_on && in_place) tag = d.carry_tag[s];
+      } else if (q == 1) {
+        h0 = d.m_normal[prv][os];
+        h1 = d.m_t0[prv][os];
+      } else if (q == 2) {
+        h0 = d.m_t1[prv][os];
+        h1 = exact ? d.m_anchor_a[prv][os] : d.pos[ida];
+      } else {
+        h1 = exact ? d.m_anchor_b[prv][os] : d.pos[idb];
+      }
+      kt = d.c_kt[prv][os * BB_MAX_CONTACTS + q];
+    }
+    if (os == BB_NONE || (!exact && ob2.x != ida)) {  // same body order only
+      // no manifold last substep: compute the pair with the others (a paused pair had none
+      // when its world stopped, and keeps none)
+      if (q != 0 || exact) continue;
+      if (ta == BB_SHAPE_BOX && tb == BB_SHAPE_BOX) d.np_list[atomicAdd(&d.ctr->np_counts[0], 1u)] = s;
+      else d.np_list[S - 1 - atomicAdd(&d.ctr->np_counts[1], 1u)] = s;
+      continue;
+    }
+    const bool lazy = in_place && lazy_on && !exact && __shfl_sync(qmask, tag, qbase) == sub_tag - 1u;
+    // the same writes as carry_part(d, cur, os, s, ida, idb, q, exact)
+    if (q == 0) {  // the same manifold as last substep: its colour carries over (colour reuse)
+      d.gc_reuse[s] = colour;
+      if (reuse_ok) d.gc_survived[os] = sub_tag;
+      d.m_bodies[cur][s] = exact ? ob2 : make_uint2(ida, idb);
+      d.m_keycc[cur][s] = kc;
+      d.hit[s] = 1;
+      if (in_place && lazy_on && !exact) d.carry_tag[s] = sub_tag;
+    } else if (q == 1) {
+      d.m_normal[cur][s] = exact ? h0 : make_float4(h0.x, h0.y, h0.z, __int_as_float(0));
+      d.m_t0[cur][s] = h1;
+    } else if (q == 2) {
+      d.m_t1[cur][s] = h0;
+      d.m_anchor_a[cur][s] = exact ? h1 : make_float4(h1.x, h1.y, h1.z, 0.f);
     } else {
-      d.np_list[S - 1 - atomicAdd(&d.ctr->np_counts[1], 1u)] = s;
+      d.m_anchor_b[cur][s] = exact ? h1 : make_float4(h1.x, h1.y, h1.z, 0.f);
+    }
+    if (lazy) {  // in place, carried in place last substep too: warm-start counts only
+      for (uint32_t c = q; c < uint32_t(kc.y); c += 4u) {
+        const uint32_t ci = s * BB_MAX_CONTACTS + c;
+        float4 k4 = c == q ? kt : d.c_kt[prv][ci];
+        k4.w = __uint_as_float(min(255u, __float_as_uint(k4.w) + 1u));
+        d.c_kt[cur][ci] = k4;
+      }
+    } else {
+      const uint32_t oi = os * BB_MAX_CONTACTS + q;
+      if (q < uint32_t(kc.y))
+        carry_loaded(d, prv, cur, oi, s * BB_MAX_CONTACTS + q, d.c_pos[prv][oi], d.c_lam[prv][oi], kt,
+                     d.c_anc_a[prv][oi], exact);
+      for (uint32_t c = q + 4u; c < uint32_t(kc.y); c += 4u)
+        carry_contact(d, prv, cur, os * BB_MAX_CONTACTS + c, s * BB_MAX_CONTACTS + c, exact);
     }
   }
 }
@@ -736,7 +788,7 @@ __device__ __forceinline__ void np_store(const DevState& d, const Params& p, int
     uint32_t old_slot = BB_NONE;
     for (uint32_t e = s0; e < s1; ++e) {
       if (d.csr_partner[prv][e] != other) continue;
-      const uint32_t os = d.man_slot[prv][d.csr_list[prv][e]];
+      const uint32_t os = d.csr_slot[prv][e];
       if (vox && (d.m_keycc[prv][os].x != m.key || d.m_bodies[prv][os].x != ida)) continue;
       old_slot = os;
       swapped = d.m_bodies[prv][os].x != ida;
@@ -1393,6 +1445,7 @@ __global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
       if (j < len) {
         L[s0 + j] = v[j];
         d.csr_partner[cur][s0 + j] = b[j].x == i ? b[j].y : b[j].x;
+        d.csr_slot[cur][s0 + j] = slot[j];
       }
     }
     return;
@@ -1406,10 +1459,12 @@ __global__ void k_csr_sort(const DevState d, int cur, uint32_t n) {
     }
     L[b] = v;
   }
-  // partner body of every entry, so lookups by pair scan one contiguous array
+  // partner body and slot of every entry, so lookups by pair scan contiguous arrays
   for (uint32_t e = s0; e < s1; ++e) {
-    const uint2 b = d.m_bodies[cur][d.man_slot[cur][L[e]]];
+    const uint32_t slot = d.man_slot[cur][L[e]];
+    const uint2 b = d.m_bodies[cur][slot];
     d.csr_partner[cur][e] = b.x == i ? b.y : b.x;
+    d.csr_slot[cur][e] = slot;
   }
 }
 
@@ -1424,7 +1479,7 @@ void bb_narrow_phase(cudaStream_t s, const DevState& d, const Params& p, uint32_
     k_slot_fill<<<grid, T, 0, s>>>(d);
   }
   k_np_classify<<<sms * 8, 32 * BB_CLS_WARPS, 0, s>>>(d, cur, warm ? 1 : 0);
-  k_narrow_carry<<<sms * 8, 256, 0, s>>>(d, cur);
+  k_narrow_carry<<<sms * 8, 256, 0, s>>>(d, cur, p.solver != BB_SOLVER_AVBD ? 1 : 0);
   k_narrow<<<sms * (p.narrow_blocks_per_sm ? p.narrow_blocks_per_sm : 16u), 128, 0, s>>>(d, p, cur, warm ? 1 : 0);
   if (d.vox_on) k_voxel_narrow<<<sms * 8, 256, 0, s>>>(d, p, cur, warm ? 1 : 0);
   // compact order: exclusive scan of the hit flags over the slots

@@ -469,12 +469,14 @@ struct bb_world_impl {
       d.csr_start[k] = u32(N + 1);
       d.csr_list[k] = u32(2 * P);
       d.csr_partner[k] = u32(2 * P);
+      d.csr_slot[k] = u32(2 * P);
     }
     d.c_r1 = f4(C); d.c_r2 = f4(C); d.c_k = f4(C);
     d.flow_rec = dalloc<uint4>(P, owned, err, stream);
     d.pgs_rec = dalloc<uint4>(P, owned, err, stream);
     d.np_list = u32(P); d.carry_list = u32(P);
     d.carry_ids = dalloc<uint2>(P, owned, err, stream);
+    d.carry_tag = u32(P);
     d.gc_rec = dalloc<uint4>(P, owned, err, stream);
     d.gc_list[0] = u32(P); d.gc_list[1] = u32(P);
     d.pgs_mass = f4(P);
