@@ -561,6 +561,10 @@ __global__ void __launch_bounds__(BB_FRONTIER) k_broad_heavy(const DevState d, u
 // traversal k_broad_heavy: its 256-entry frontier then leaves at most 512 leaves per walk.
 #define BB_HV_BLOCK_LEAVES (512u * BB_FRONTIER)
 #define BB_HV_FRONTIER (BB_HV_THREADS * BB_HV_PER_THREAD)
+// With at most BB_FLAT_MAX heavy queries (a floor and a few walls) the flat pass below answers
+// them all; their slots read hv_n = BB_HV_FLAT and the pool and block paths leave them alone.
+#define BB_FLAT_MAX 4u
+#define BB_HV_FLAT 0xFFFFFFFEu
 
 __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState d, uint32_t n) {
   if (d.ctr->front_skip) return;  // nothing moved since the last front end
@@ -571,6 +575,11 @@ __global__ void __launch_bounds__(BB_HV_THREADS) k_heavy_frontier(const DevState
   const int N = int(n), leaf0 = N - 1;
   const int t = threadIdx.x;
   for (uint32_t slot = blockIdx.x; slot < hc; slot += gridDim.x) {
+    if (d.ctr->heavy_n <= BB_FLAT_MAX) {  // few heavy queries: the flat pass takes them
+      if (t == 0) d.hv_n[slot] = BB_HV_FLAT;
+      __syncthreads();
+      continue;
+    }
     const uint32_t qi = d.heavy_list[slot];
     const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
     const int wend = world_end(d, qi, n);
@@ -723,10 +732,103 @@ __global__ void k_heavy_totals(const DevState d) {
   const uint32_t hc = min(d.ctr->heavy_n, BB_HEAVY_CAP);
   for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < hc; slot += gridDim.x * blockDim.x) {
     const uint32_t m = d.hv_n[slot];
-    if (m == BB_NONE) continue;
+    if (m == BB_NONE || m == BB_HV_FLAT) continue;
     const uint32_t f = d.hv_first[slot];
     d.pair_cnt[d.heavy_list[slot]] = m ? d.hv_off[f + m - 1] + d.hv_cnt[f + m - 1] - d.hv_off[f] : 0u;
   }
+}
+
+// ---- a few heavy queries: one flat pass over the leaves ------------------------------------------
+// With at most BB_FLAT_MAX heavy queries, each is answered by testing every leaf j of its range
+// (qi, world end) against the query box.  That is the traversal's answer: every internal box is
+// the exact min/max union of its children's, so no ancestor of an overlapping leaf is pruned
+// (only a non-finite box could make the two differ), and ascending j is the traversal's order.
+// Block b takes tiles of BB_FLAT_TILE leaves, thread t leaves j0 + k * BB_FLAT_THREADS + t, so
+// the reads coalesce and leaf order is (k, warp, lane).  EMIT=false counts per (query, tile)
+// into flat_cnt; k_heavy_flat_scan turns the counts into offsets and the query's pair count;
+// EMIT=true runs the same tests and writes the pairs.  One read of every leaf box per query
+// replaces the pool's frontier levels and walks, which for a floor cover most of the world.
+#define BB_FLAT_THREADS 256
+#define BB_FLAT_PER 8
+#define BB_FLAT_TILE (BB_FLAT_THREADS * BB_FLAT_PER)
+template <bool EMIT>
+__global__ void __launch_bounds__(BB_FLAT_THREADS) k_heavy_flat(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
+  const uint32_t hc = d.ctr->heavy_n;
+  if (hc == 0 || hc > BB_FLAT_MAX) return;
+  __shared__ uint32_t s_cnt[BB_FLAT_PER][BB_FLAT_THREADS / 32];
+  const int leaf0 = int(n) - 1;
+  const uint32_t tiles = (n + BB_FLAT_TILE - 1) / BB_FLAT_TILE;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t h = 0; h < hc; ++h) {
+    const uint32_t qi = d.heavy_list[h];
+    const float4 qmn = d.node_box[2 * (leaf0 + qi)], qmx = d.node_box[2 * (leaf0 + qi) + 1];
+    const uint32_t wend = uint32_t(world_end(d, qi, n));
+    const uint32_t out = EMIT ? d.pair_off[qi] : 0u;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {  // block-uniform
+      const uint32_t j0 = tile * BB_FLAT_TILE;
+      if (j0 + BB_FLAT_TILE <= qi + 1u || j0 >= wend) {  // no leaf of the tile in (qi, wend)
+        if (!EMIT && threadIdx.x == 0) d.flat_cnt[h * tiles + tile] = 0;
+        continue;
+      }
+      bool f[BB_FLAT_PER];
+#pragma unroll
+      for (int k = 0; k < BB_FLAT_PER; ++k) {
+        const uint32_t j = j0 + uint32_t(k) * BB_FLAT_THREADS + threadIdx.x;
+        f[k] = false;
+        if (j > qi && j < wend)
+          f[k] = box_overlap(qmn, qmx, d.node_box[2 * (leaf0 + j)], d.node_box[2 * (leaf0 + j) + 1]);
+      }
+      unsigned m[BB_FLAT_PER];
+#pragma unroll
+      for (int k = 0; k < BB_FLAT_PER; ++k) {
+        m[k] = __ballot_sync(0xFFFFFFFFu, f[k]);
+        if (lane == 0) s_cnt[k][warp] = uint32_t(__popc(m[k]));
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {  // exclusive prefix in leaf order (k, then warp); the tile's count
+        uint32_t run = 0;
+        for (int k = 0; k < BB_FLAT_PER; ++k)
+          for (int w = 0; w < BB_FLAT_THREADS / 32; ++w) {
+            const uint32_t c = s_cnt[k][w];
+            s_cnt[k][w] = run;
+            run += c;
+          }
+        if (!EMIT) d.flat_cnt[h * tiles + tile] = run;
+      }
+      __syncthreads();
+      if (EMIT) {
+        const uint32_t base = out + d.flat_off[h * tiles + tile];
+#pragma unroll
+        for (int k = 0; k < BB_FLAT_PER; ++k) {
+          if (!f[k]) continue;
+          const uint32_t j = j0 + uint32_t(k) * BB_FLAT_THREADS + threadIdx.x;
+          const uint32_t o = base + s_cnt[k][warp] + uint32_t(__popc(m[k] & ((1u << lane) - 1u)));
+          if (o < d.pair_capacity) d.pairs[o] = make_uint2(qi, j);
+          else raise_error(d.ctr, BB_ERRF_PAIR_OVERFLOW);
+        }
+      }
+      __syncthreads();  // s_cnt is rewritten by the next tile
+    }
+  }
+}
+// block h: exclusive scan of query h's tile counts into flat_off, and its pair count
+__global__ void __launch_bounds__(1024) k_heavy_flat_scan(const DevState d, uint32_t n) {
+  if (d.ctr->front_skip) return;  // nothing moved since the last front end
+  const uint32_t hc = d.ctr->heavy_n;
+  if (hc == 0 || hc > BB_FLAT_MAX || blockIdx.x >= hc) return;
+  __shared__ uint32_t s_warp[32];
+  const uint32_t tiles = (n + BB_FLAT_TILE - 1) / BB_FLAT_TILE, h = blockIdx.x;
+  uint32_t carry = 0;
+  for (uint32_t b = 0; b < tiles; b += blockDim.x) {  // block-uniform
+    const uint32_t i = b + threadIdx.x;
+    const uint32_t v = i < tiles ? d.flat_cnt[h * tiles + i] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_scan_nt<1024>(v, s_warp, total);
+    if (i < tiles) d.flat_off[h * tiles + i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) d.pair_cnt[d.heavy_list[h]] = carry;
 }
 
 void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n, const StepScratch& sc, int sms,
@@ -768,6 +870,8 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
     bb_launch_scan(s, d.hv_cnt, d.hv_off, &d.ctr->hv_pool_n, d.hv_cap, nullptr,
                    sc.scan_status + 5 * size_t(sc.scan_tiles), sc.scan_tile_ctr + 5, d.ctr, &d.ctr->front_skip);
     k_heavy_totals<<<(hb + 255) / 256, 256, 0, s>>>(d);
+    k_heavy_flat<false><<<min((n + BB_FLAT_TILE - 1) / BB_FLAT_TILE, uint32_t(sms) * 8u), BB_FLAT_THREADS, 0, s>>>(d, n);
+    k_heavy_flat_scan<<<BB_FLAT_MAX, 1024, 0, s>>>(d, n);
   }
   k_broad_heavy<false><<<hb, BB_FRONTIER, 0, s>>>(d, n, pool ? 0 : 1);
   bb_launch_scan(s, d.pair_cnt, d.pair_off, nullptr, n, &d.ctr->pair_count, sc.scan_status, sc.scan_tile_ctr, d.ctr,
@@ -775,5 +879,8 @@ void bb_front_end(cudaStream_t s, const DevState& d, const Params& p, uint32_t n
   k_broad_copy<<<sms * 16, 256, 0, s>>>(d, n);
   k_broad<true><<<bb, bt, 0, s>>>(d, n);
   k_broad_heavy<true><<<hb, BB_FRONTIER, 0, s>>>(d, n, pool ? 0 : 1);
-  if (pool) k_heavy_walk<true><<<sms * 8, 128, 0, s>>>(d, n);
+  if (pool) {
+    k_heavy_walk<true><<<sms * 8, 128, 0, s>>>(d, n);
+    k_heavy_flat<true><<<min((n + BB_FLAT_TILE - 1) / BB_FLAT_TILE, uint32_t(sms) * 8u), BB_FLAT_THREADS, 0, s>>>(d, n);
+  }
 }

@@ -117,6 +117,7 @@ struct DevState {
   // heavy queries split over the whole GPU: per slot its frontier range in the pool; per pool
   // entry the subtree root, the slot, the partner count and its exclusive scan
   uint32_t *hv_first, *hv_n, *hv_pool, *hv_slot, *hv_cnt, *hv_off;
+  uint32_t *flat_cnt, *flat_off;  // flat pass of a few heavy queries: per (query, leaf tile) counts, offsets
   uint32_t hv_cap;              // pool entries
   uint2* pairs;                 // (sorted a, sorted b)
   uint32_t* np_list;            // narrow-phase work list (pair indices; see k_np_classify)

@@ -459,6 +459,7 @@ struct bb_world_impl {
     d.hv_first = u32(8192); d.hv_n = u32(8192);
     d.hv_cap = uint32_t(P);
     d.hv_pool = u32(P); d.hv_slot = u32(P); d.hv_cnt = u32(P); d.hv_off = u32(P);
+    d.flat_cnt = u32(4 * (N / 2048 + 2)); d.flat_off = u32(4 * (N / 2048 + 2));  // 4 queries x leaf tiles
     d.pairs = dalloc<uint2>(P, owned, err, stream);
     for (int k = 0; k < 2; ++k) {
       d.m_bodies[k] = dalloc<uint2>(P, owned, err, stream);
