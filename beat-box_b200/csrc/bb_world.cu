@@ -670,6 +670,7 @@ struct StateHeader {
   bb_solver_params params;
 };
 constexpr uint32_t kStateMagic = 0x31534242u;  // "BBS1"
+constexpr uint32_t kStateVersion = 2;  // the array set of this build (frozen-pair carry and list slots)
 uint64_t state_bytes(const World* w) {
   uint64_t t = sizeof(StateHeader) + 8ull * w->owned.size();
   for (auto& o : w->owned) t += o.second;
@@ -1670,7 +1671,7 @@ bb_status bb_world_save_state(void* world, void* dst, uint64_t max_bytes, uint64
   CU(cudaStreamSynchronize(w->stream));
   StateHeader h{};
   h.magic = kStateMagic;
-  h.version = 1;
+  h.version = kStateVersion;
   h.cap_n = w->cap_n;
   h.cap_p = w->cap_p;
   h.n = w->n;
@@ -1705,8 +1706,10 @@ bb_status bb_world_load_state(void* world, const void* src, uint64_t bytes) {
   if (!w || !src || bytes < sizeof(StateHeader)) return fail(BB_E_INVALID, "bb_world_load_state: bad arguments");
   StateHeader h;
   std::memcpy(&h, src, sizeof(h));
-  if (h.magic != kStateMagic || h.version != 1 || h.total != bytes)
+  if (h.magic != kStateMagic || h.total != bytes)
     return fail(BB_E_INVALID, "bb_world_load_state: not a saved world state");
+  if (h.version != kStateVersion)
+    return fail(BB_E_INVALID, "bb_world_load_state: saved by another version of the library (different arrays)");
   if (h.cap_n != w->cap_n || h.cap_p != w->cap_p || h.n != w->n || h.n_dyn != w->n_dyn ||
       h.n_worlds != w->d.n_worlds || h.vox_on != w->d.vox_on || h.full_inertia != w->d.full_inertia ||
       h.arrays != w->owned.size() || h.slot_bytes != (w->slot_buf ? 16ull * w->cap_p : 0ull) ||
