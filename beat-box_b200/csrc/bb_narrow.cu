@@ -590,11 +590,13 @@ __device__ __forceinline__ void carry_part(const DevState& d, int cur, uint32_t 
 // came or went, every frozen pair takes this path; the others search.  Slots past the previous
 // substep's count are not read (they hold older manifolds).
 //
-// The list entry carries the two bodies and the paused bit, so every load of the slot's own old
-// manifold is issued at once, before the check: the quad's lanes split the header (lane 0 the
-// key and colour, 1 the normal and first tangent, 2 the second tangent and first anchor, 3 the
-// second anchor) and lane q takes contact q.  A pair then waits for one round of loads after
-// its list entry instead of a chain through the pair, the sorted ids and the flags.
+// The list entry carries the two bodies, the paused bit and whether body a is dynamic, so the
+// probe of the pair's own slot and the bounds of the dynamic body's old list load in one round,
+// with no chain through the pair, the sorted ids and the flags.  A pair whose slot moved searches
+// that list with the quad's lanes splitting it (each entry carries its slot, csr_slot).  Then
+// every load of the old manifold is issued at once: the quad's lanes split the header (lane 0
+// the key, bodies and colour, 1 the normal and first tangent, 2 the second tangent and first
+// anchor, 3 the second anchor) and lane q takes contact q.
 //
 // Short carry.  When this slot was carried the same way last substep (carry_tag = last
 // substep), last substep's manifold was made from the one this substep writes over, and nothing
